@@ -1,0 +1,22 @@
+"""B200-native dense ZNCC tracker with AutoRIFT.jl's API.
+
+Loaded under the module name ``autorift_b200`` (the directory name is not an identifier);
+``__graft_entry__.load_package()`` registers it.
+"""
+
+from . import _lib, synthetic
+from .methods import (GardnerFilter, Highpass, NCC, NoOutlierFilter, NoPreprocess, NoQuantize,
+                      NoRefine, Params, PyramidRefine, QuantizeUInt8, Wallis, ZNCC, chip_sizes,
+                      params, upsampling)
+from .points import (PointSet, gridpoints, gridpoints_xy, nsearchable, npoints, pointset,
+                     sanitize)
+from .track import (DisplacementField, ImagePair, correlate, displacement_field, nmeasured,
+                    refine_patches, track)
+
+__all__ = [
+    "GardnerFilter", "Highpass", "NCC", "NoOutlierFilter", "NoPreprocess", "NoQuantize",
+    "NoRefine", "Params", "PyramidRefine", "QuantizeUInt8", "Wallis", "ZNCC", "chip_sizes",
+    "params", "upsampling", "PointSet", "gridpoints", "gridpoints_xy", "nsearchable", "npoints",
+    "pointset", "sanitize", "DisplacementField", "ImagePair", "correlate", "displacement_field",
+    "nmeasured", "refine_patches", "track",
+]

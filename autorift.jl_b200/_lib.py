@@ -1,0 +1,124 @@
+"""ctypes binding of libautorift_gpu.so (include/autorift_gpu.h).
+
+The library is the only compute path: if it is missing or no GPU is visible, every call that
+would compute raises. There is no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libautorift_gpu.so"
+
+AR_OK, AR_ERR_ARG, AR_ERR_SIZE, AR_ERR_OOM, AR_ERR_TIMEOUT, AR_ERR_CUDA, AR_ERR_UNSUPPORTED = range(7)
+AR_U8, AR_U16, AR_F32, AR_I16, AR_F64 = range(5)
+AR_ZNCC, AR_NCC = 0, 1
+
+# Every symbol include/autorift_gpu.h declares, with (restype, argtypes).
+_p = ctypes.c_void_p
+_i32 = ctypes.c_int
+_i64 = ctypes.c_int64
+_sz = ctypes.c_size_t
+
+
+class ArPoints(ctypes.Structure):
+    """`ar_points`: the eight PointSet fields (src/points.jl:50-74) plus the count."""
+
+    _fields_ = [("x", _p), ("y", _p), ("radius_x", _p), ("radius_y", _p),
+                ("dx_prior", _p), ("dy_prior", _p), ("chip_size_x", _p), ("chip_size_y", _p),
+                ("n", _i64)]
+
+
+SIGNATURES = {
+    "ar_version": (_i32, []),
+    "ar_ctx_create": (_i32, [_i32, ctypes.POINTER(_p)]),
+    "ar_ctx_destroy": (_i32, [_p]),
+    "ar_last_error": (_i32, [_p, ctypes.c_char_p, _sz]),
+    "ar_pair_upload": (_i32, [_p, _p, _p, _p, _p, _i64, _i64, _i32, ctypes.POINTER(_p)]),
+    "ar_pair_destroy": (_i32, [_p]),
+    "ar_pair_info": (_i32, [_p, ctypes.POINTER(_i32), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+    "ar_track": (_i32, [_p, _p, ctypes.POINTER(ArPoints), _i32, _i32, _p, _p, _p, _p]),
+    "ar_track_device": (_i32, [_p, _p, ctypes.POINTER(ArPoints), _i32, _i32, _p, _p, _p, _p, _p]),
+    "ar_correlate": (_i32, [_p, _p, _p, _i32, _i64, _i64, _i64, _i64, _i32, _p,
+                            ctypes.POINTER(_i32)]),
+    "ar_refine_patches": (_i32, [_p, _p, _i64, _i32, _p, _p, _p]),
+    "ar_synchronize": (_i32, [_p]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+class ArError(RuntimeError):
+    """A non-zero status from the library, with its message."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+
+
+def load(path: Path | None = None):
+    """Load the shared library and declare every exported signature."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            p = Path(path) if path else LIB_PATH
+            if not p.exists():
+                raise RuntimeError(
+                    f"{p.name} is not built; run __graft_entry__.build() (nvcc for sm_100a). "
+                    "There is no CPU fallback.")
+            L = ctypes.CDLL(str(p))
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(L, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = L
+    return _lib
+
+
+class Context:
+    """An `ar_ctx` on one CUDA device (owns its stream and scratch)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        h = _p()
+        rc = self.lib.ar_ctx_create(int(device), ctypes.byref(h))
+        if rc != AR_OK:
+            raise ArError(rc, f"ar_ctx_create(device={device}) failed: no usable CUDA device")
+        self.handle = h
+        self.device = int(device)
+
+    def check(self, rc: int):
+        if rc != AR_OK:
+            buf = ctypes.create_string_buffer(512)
+            self.lib.ar_last_error(self.handle, buf, 512)
+            raise ArError(rc, buf.value.decode(errors="replace"))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.ar_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx = {}
+
+
+def default_context(device: int = 0) -> Context:
+    """One shared context per device for the convenience API."""
+    with _lock:
+        ctx = _default_ctx.get(device)
+    if ctx is None:
+        ctx = Context(device)
+        with _lock:
+            _default_ctx.setdefault(device, ctx)
+            ctx = _default_ctx[device]
+    return ctx

@@ -1,0 +1,510 @@
+// C ABI of libautorift_gpu: contexts, device-resident image pairs and the track entry points.
+// Declared in include/autorift_gpu.h, where each entry point cites the reference interface it
+// replaces.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "ar_internal.cuh"
+
+struct ar_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::mutex mu;  // one call at a time per context
+    ar::TrackScratch scratch;
+    // Pinned staging for host<->device copies of caller-owned (pageable) arrays.
+    unsigned char* pinned = nullptr;
+    size_t pinned_bytes = 0;
+    cudaEvent_t staged[2] = {nullptr, nullptr};
+    // Device buffers for host point sets and outputs, grown on demand.
+    void* dbuf = nullptr;
+    size_t dbuf_bytes = 0;
+};
+
+struct ar_pair {
+    ar_ctx* ctx = nullptr;
+    int dtype = 0;
+    int64_t nrows = 0, ncols = 0;
+    void* ref = nullptr;
+    void* sec = nullptr;
+    uint8_t* valid = nullptr;  // ref_valid .& sec_valid
+};
+
+namespace {
+
+constexpr size_t kStageBytes = 32u << 20;  // two halves of 16 MiB
+
+size_t elem_size(int dtype) {
+    switch (dtype) {
+        case AR_U8: return 1;
+        case AR_U16: return 2;
+        case AR_I16: return 2;
+        case AR_F32: return 4;
+        case AR_F64: return 8;
+        default: return 0;
+    }
+}
+
+int fail(ar_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int cuda_fail(ar_ctx* ctx, cudaError_t e, const char* what) {
+    const int code = e == cudaErrorMemoryAllocation ? AR_ERR_OOM : AR_ERR_CUDA;
+    return fail(ctx, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+cudaError_t ensure_pinned(ar_ctx* c) {
+    if (c->pinned) return cudaSuccess;
+    cudaError_t e = cudaMallocHost(&c->pinned, kStageBytes);
+    if (e != cudaSuccess) return e;
+    c->pinned_bytes = kStageBytes;
+    for (auto& ev : c->staged) {
+        e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// Host (pageable) -> device through the two pinned halves, so the CPU copy of one chunk
+// overlaps the DMA of the previous one. Stream-ordered; returns once all chunks are queued.
+cudaError_t stage_h2d(ar_ctx* c, void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return cudaSuccess;
+    cudaError_t e = ensure_pinned(c);
+    if (e != cudaSuccess) return e;
+    const size_t half = c->pinned_bytes / 2;
+    size_t off = 0;
+    int slot = 0;
+    while (off < bytes) {
+        const size_t n = std::min(half, bytes - off);
+        e = cudaEventSynchronize(c->staged[slot]);  // the slot's previous DMA has finished
+        if (e != cudaSuccess) return e;
+        unsigned char* buf = c->pinned + slot * half;
+        std::memcpy(buf, static_cast<const unsigned char*>(src) + off, n);
+        e = cudaMemcpyAsync(static_cast<unsigned char*>(dst) + off, buf, n, cudaMemcpyHostToDevice,
+                            c->stream);
+        if (e != cudaSuccess) return e;
+        e = cudaEventRecord(c->staged[slot], c->stream);
+        if (e != cudaSuccess) return e;
+        off += n;
+        slot ^= 1;
+    }
+    return cudaSuccess;
+}
+
+// Device -> host (pageable) through the pinned halves; synchronous.
+cudaError_t stage_d2h(ar_ctx* c, void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return cudaSuccess;
+    cudaError_t e = ensure_pinned(c);
+    if (e != cudaSuccess) return e;
+    const size_t half = c->pinned_bytes / 2;
+    size_t off = 0;
+    int slot = 0;
+    size_t pending_off[2] = {0, 0}, pending_n[2] = {0, 0};
+    while (off < bytes || pending_n[0] || pending_n[1]) {
+        if (off < bytes) {
+            e = cudaEventSynchronize(c->staged[slot]);
+            if (e != cudaSuccess) return e;
+            if (pending_n[slot]) {
+                std::memcpy(static_cast<unsigned char*>(dst) + pending_off[slot],
+                            c->pinned + slot * half, pending_n[slot]);
+                pending_n[slot] = 0;
+            }
+            const size_t n = std::min(half, bytes - off);
+            e = cudaMemcpyAsync(c->pinned + slot * half, static_cast<const unsigned char*>(src) + off,
+                                n, cudaMemcpyDeviceToHost, c->stream);
+            if (e != cudaSuccess) return e;
+            e = cudaEventRecord(c->staged[slot], c->stream);
+            if (e != cudaSuccess) return e;
+            pending_off[slot] = off;
+            pending_n[slot] = n;
+            off += n;
+            slot ^= 1;
+        } else {
+            for (int s = 0; s < 2; ++s) {
+                if (!pending_n[s]) continue;
+                e = cudaEventSynchronize(c->staged[s]);
+                if (e != cudaSuccess) return e;
+                std::memcpy(static_cast<unsigned char*>(dst) + pending_off[s], c->pinned + s * half,
+                            pending_n[s]);
+                pending_n[s] = 0;
+            }
+        }
+    }
+    return cudaSuccess;
+}
+
+cudaError_t ensure_dbuf(ar_ctx* c, size_t bytes) {
+    if (c->dbuf_bytes >= bytes) return cudaSuccess;
+    cudaFree(c->dbuf);
+    c->dbuf = nullptr;
+    c->dbuf_bytes = 0;
+    cudaError_t e = cudaMalloc(&c->dbuf, bytes);
+    if (e != cudaSuccess) return e;
+    c->dbuf_bytes = bytes;
+    return cudaSuccess;
+}
+
+template <typename T>
+__global__ void k_make_valid(const T* ref, const T* sec, const uint8_t* rv, const uint8_t* sv,
+                             uint8_t* out, int64_t n) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    bool a, b;
+    if (rv) a = rv[i] != 0; else a = isfinite(static_cast<double>(ref[i]));
+    if (sv) b = sv[i] != 0; else b = isfinite(static_cast<double>(sec[i]));
+    out[i] = (a && b) ? 1 : 0;
+}
+
+template <typename T>
+cudaError_t launch_make_valid(const void* ref, const void* sec, const uint8_t* rv,
+                              const uint8_t* sv, uint8_t* out, int64_t n, cudaStream_t s) {
+    const int threads = 256;
+    k_make_valid<T><<<static_cast<unsigned>((n + threads - 1) / threads), threads, 0, s>>>(
+        static_cast<const T*>(ref), static_cast<const T*>(sec), rv, sv, out, n);
+    return cudaGetLastError();
+}
+
+bool is_pow2(int v) { return v >= 1 && (v & (v - 1)) == 0; }
+
+}  // namespace
+
+extern "C" {
+
+int ar_version(void) { return 100; }
+
+int ar_ctx_create(int device, ar_ctx** out) {
+    if (!out) return AR_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+        return AR_ERR_ARG;
+    DeviceGuard g(device);
+    ar_ctx* c = new ar_ctx();
+    c->device = device;
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return AR_ERR_CUDA;
+    }
+    *out = c;
+    return AR_OK;
+}
+
+int ar_ctx_destroy(ar_ctx* c) {
+    if (!c) return AR_ERR_ARG;
+    {
+        DeviceGuard g(c->device);
+        std::lock_guard<std::mutex> lk(c->mu);
+        cudaStreamSynchronize(c->stream);
+        cudaFree(c->scratch.sub_count);
+        cudaFree(c->scratch.sub_point);
+        cudaFree(c->scratch.sub_origin);
+        cudaFree(c->scratch.sub_patch);
+        cudaFree(c->scratch.geom);
+        cudaFree(c->dbuf);
+        if (c->pinned) cudaFreeHost(c->pinned);
+        for (auto& ev : c->staged)
+            if (ev) cudaEventDestroy(ev);
+        cudaStreamDestroy(c->stream);
+    }
+    delete c;
+    return AR_OK;
+}
+
+int ar_last_error(const ar_ctx* c, char* buf, size_t size) {
+    if (!c || !buf || size == 0) return AR_ERR_ARG;
+    const size_t n = std::min(size - 1, c->err.size());
+    std::memcpy(buf, c->err.data(), n);
+    buf[n] = '\0';
+    return AR_OK;
+}
+
+int ar_pair_upload(ar_ctx* c, const void* ref, const void* sec, const uint8_t* ref_valid,
+                   const uint8_t* sec_valid, int64_t nrows, int64_t ncols, int dtype,
+                   ar_pair** out) {
+    if (!c || !ref || !sec || !out) return fail(c, AR_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (nrows <= 0 || ncols <= 0) return fail(c, AR_ERR_SIZE, "image extents must be positive");
+    const size_t es = elem_size(dtype);
+    if (es == 0 || dtype == AR_F64) return fail(c, AR_ERR_UNSUPPORTED, "unsupported element type");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    const int64_t n = nrows * ncols;
+    ar_pair* p = new ar_pair();
+    p->ctx = c;
+    p->dtype = dtype;
+    p->nrows = nrows;
+    p->ncols = ncols;
+    cudaError_t e = cudaMalloc(&p->ref, n * es);
+    if (e == cudaSuccess) e = cudaMalloc(&p->sec, n * es);
+    if (e == cudaSuccess) e = cudaMalloc(&p->valid, n);
+    uint8_t* dmask = nullptr;
+    if (e == cudaSuccess && (ref_valid || sec_valid)) e = cudaMalloc(&dmask, 2 * n);
+    if (e == cudaSuccess) e = stage_h2d(c, p->ref, ref, n * es);
+    if (e == cudaSuccess) e = stage_h2d(c, p->sec, sec, n * es);
+    if (e == cudaSuccess && ref_valid) e = stage_h2d(c, dmask, ref_valid, n);
+    if (e == cudaSuccess && sec_valid) e = stage_h2d(c, dmask + n, sec_valid, n);
+    if (e == cudaSuccess) {
+        const uint8_t* rv = ref_valid ? dmask : nullptr;
+        const uint8_t* sv = sec_valid ? dmask + n : nullptr;
+        switch (dtype) {
+            case AR_U8: e = launch_make_valid<uint8_t>(p->ref, p->sec, rv, sv, p->valid, n, c->stream); break;
+            case AR_U16: e = launch_make_valid<uint16_t>(p->ref, p->sec, rv, sv, p->valid, n, c->stream); break;
+            case AR_I16: e = launch_make_valid<int16_t>(p->ref, p->sec, rv, sv, p->valid, n, c->stream); break;
+            case AR_F32: e = launch_make_valid<float>(p->ref, p->sec, rv, sv, p->valid, n, c->stream); break;
+        }
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(dmask);
+    if (e != cudaSuccess) {
+        cudaFree(p->ref);
+        cudaFree(p->sec);
+        cudaFree(p->valid);
+        delete p;
+        return cuda_fail(c, e, "ar_pair_upload");
+    }
+    *out = p;
+    return AR_OK;
+}
+
+int ar_pair_destroy(ar_pair* p) {
+    if (!p) return AR_ERR_ARG;
+    {
+        DeviceGuard g(p->ctx->device);
+        std::lock_guard<std::mutex> lk(p->ctx->mu);
+        cudaStreamSynchronize(p->ctx->stream);
+        cudaFree(p->ref);
+        cudaFree(p->sec);
+        cudaFree(p->valid);
+    }
+    delete p;
+    return AR_OK;
+}
+
+int ar_pair_info(const ar_pair* p, int* dtype, int64_t* nrows, int64_t* ncols) {
+    if (!p) return AR_ERR_ARG;
+    if (dtype) *dtype = p->dtype;
+    if (nrows) *nrows = p->nrows;
+    if (ncols) *ncols = p->ncols;
+    return AR_OK;
+}
+
+static int check_track_args(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up, int measure) {
+    if (!c || !p || !pts) return fail(c, AR_ERR_ARG, "null argument");
+    if (p->ctx != c) return fail(c, AR_ERR_ARG, "the pair belongs to another context");
+    if (pts->n < 0) return fail(c, AR_ERR_SIZE, "negative point count");
+    if (pts->n > 0 && (!pts->x || !pts->y || !pts->radius_x || !pts->radius_y || !pts->dx_prior ||
+                       !pts->dy_prior || !pts->chip_size_x || !pts->chip_size_y))
+        return fail(c, AR_ERR_ARG, "null point-set field");
+    if (!is_pow2(up) || up > 128)
+        return fail(c, AR_ERR_ARG, "`upsampling` must be 1 or a power of 2 up to 128");
+    if (measure != AR_ZNCC && measure != AR_NCC) return fail(c, AR_ERR_ARG, "unknown measure");
+    return AR_OK;
+}
+
+int ar_track(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up, int measure, float* dx,
+             float* dy, float* corr, uint8_t* searched) {
+    int rc = check_track_args(c, p, pts, up, measure);
+    if (rc != AR_OK) return rc;
+    const int64_t n = pts->n;
+    if (n > 0 && (!dx || !dy || !corr || !searched)) return fail(c, AR_ERR_ARG, "null output");
+    if (n == 0) return AR_OK;
+    for (int64_t k = 0; k < n; ++k) {
+        if (!std::isfinite(pts->x[k]) || !std::isfinite(pts->y[k]) ||
+            !std::isfinite(pts->dx_prior[k]) || !std::isfinite(pts->dy_prior[k]))
+            return fail(c, AR_ERR_ARG, "point coordinates and priors must be finite");
+    }
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    const ar::PassGeometry geom = ar::pass_geometry_host(*pts, p->nrows, p->ncols);
+    // One device block: 4 f64 + 4 i64 fields, then the outputs.
+    const size_t fb = static_cast<size_t>(n) * 8;
+    const size_t need = 8 * fb + 3 * static_cast<size_t>(n) * 4 + static_cast<size_t>(n) + 64;
+    cudaError_t e = ensure_dbuf(c, need);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ar_track: device buffers");
+    unsigned char* base = static_cast<unsigned char*>(c->dbuf);
+    ar::DevPoints dp;
+    dp.x = reinterpret_cast<const double*>(base + 0 * fb);
+    dp.y = reinterpret_cast<const double*>(base + 1 * fb);
+    dp.rx = reinterpret_cast<const int64_t*>(base + 2 * fb);
+    dp.ry = reinterpret_cast<const int64_t*>(base + 3 * fb);
+    dp.dx0 = reinterpret_cast<const double*>(base + 4 * fb);
+    dp.dy0 = reinterpret_cast<const double*>(base + 5 * fb);
+    dp.csx = reinterpret_cast<const int64_t*>(base + 6 * fb);
+    dp.csy = reinterpret_cast<const int64_t*>(base + 7 * fb);
+    dp.n = n;
+    ar::DevOutputs dout;
+    dout.dx = reinterpret_cast<float*>(base + 8 * fb);
+    dout.dy = dout.dx + n;
+    dout.corr = dout.dy + n;
+    dout.searched = reinterpret_cast<uint8_t*>(dout.corr + n);
+    const void* srcs[8] = {pts->x, pts->y, pts->radius_x, pts->radius_y,
+                           pts->dx_prior, pts->dy_prior, pts->chip_size_x, pts->chip_size_y};
+    for (int f = 0; f < 8 && e == cudaSuccess; ++f) e = stage_h2d(c, base + f * fb, srcs[f], fb);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ar_track: upload points");
+    std::string err;
+    e = ar::launch_track(p->dtype, p->ref, p->sec, p->valid, p->nrows, p->ncols, dp, geom, up,
+                         measure, dout, c->scratch, c->num_sms, c->stream, &err);
+    if (e != cudaSuccess)
+        return err.empty() ? cuda_fail(c, e, "ar_track") : fail(c, AR_ERR_UNSUPPORTED, err);
+    // The three float outputs are contiguous on the device, as is `searched`.
+    std::vector<float> tmp;
+    e = stage_d2h(c, dx, dout.dx, n * 4);
+    if (e == cudaSuccess) e = stage_d2h(c, dy, dout.dy, n * 4);
+    if (e == cudaSuccess) e = stage_d2h(c, corr, dout.corr, n * 4);
+    if (e == cudaSuccess) e = stage_d2h(c, searched, dout.searched, n);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ar_track: download results");
+    return AR_OK;
+}
+
+int ar_track_device(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up, int measure,
+                    float* dx, float* dy, float* corr, uint8_t* searched, void* stream) {
+    int rc = check_track_args(c, p, pts, up, measure);
+    if (rc != AR_OK) return rc;
+    const int64_t n = pts->n;
+    if (n > 0 && (!dx || !dy || !corr || !searched)) return fail(c, AR_ERR_ARG, "null output");
+    if (n == 0) return AR_OK;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    ar::DevPoints dp{pts->x, pts->y, pts->radius_x, pts->radius_y, pts->dx_prior,
+                     pts->dy_prior, pts->chip_size_x, pts->chip_size_y, n};
+    ar::PassGeometry geom;
+    cudaError_t e = ar::pass_geometry_device(dp, p->nrows, p->ncols, c->scratch, s, &geom);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ar_track_device: pass geometry");
+    ar::DevOutputs dout{dx, dy, corr, searched};
+    std::string err;
+    e = ar::launch_track(p->dtype, p->ref, p->sec, p->valid, p->nrows, p->ncols, dp, geom, up,
+                         measure, dout, c->scratch, c->num_sms, s, &err);
+    if (e != cudaSuccess)
+        return err.empty() ? cuda_fail(c, e, "ar_track_device") : fail(c, AR_ERR_UNSUPPORTED, err);
+    return AR_OK;
+}
+
+int ar_correlate(ar_ctx* c, const void* search, const void* chip, int dtype, int64_t ch,
+                 int64_t cw, int64_t rx, int64_t ry, int measure, float* surface,
+                 int* degenerate) {
+    if (!c || !search || !chip || !surface) return fail(c, AR_ERR_ARG, "null argument");
+    if (ch <= 0 || cw <= 0 || rx <= 0 || ry <= 0 || (ch & 1) || (cw & 1))
+        return fail(c, AR_ERR_SIZE, "chip extents must be positive and even, radii positive");
+    if (measure != AR_ZNCC && measure != AR_NCC) return fail(c, AR_ERR_ARG, "unknown measure");
+    const size_t es = elem_size(dtype);
+    if (es == 0 || dtype == AR_F64) return fail(c, AR_ERR_UNSUPPORTED, "unsupported element type");
+    // One point on a pair whose reference is the search window and whose secondary holds the
+    // chip at the window's zero-displacement position. The point sits at 1-based
+    // (ry + ch/2 + 0.5, rx + cw/2 + 0.5): after the grid loop's +0.5 shift its window starts
+    // at row 1, column 1 and its chip at row ry + 1, column rx + 1 (src/points.jl:358-395).
+    const int64_t wr = ch + 2 * ry - 1, wc = cw + 2 * rx - 1;
+    std::vector<unsigned char> secimg(static_cast<size_t>(wr * wc) * es, 0);
+    const unsigned char* cp = static_cast<const unsigned char*>(chip);
+    for (int64_t j = 0; j < cw; ++j)
+        std::memcpy(secimg.data() + (ry + (rx + j) * wr) * es, cp + j * ch * es, ch * es);
+    std::vector<uint8_t> mask(static_cast<size_t>(wr * wc), 1);
+    ar_pair* pair = nullptr;
+    int rc = ar_pair_upload(c, search, secimg.data(), mask.data(), mask.data(), wr, wc, dtype, &pair);
+    if (rc != AR_OK) return rc;
+    const double x = static_cast<double>(rx + cw / 2) + 0.5;
+    const double y = static_cast<double>(ry + ch / 2) + 0.5;
+    const int64_t rxx = rx, ryy = ry, csx = cw, csy = ch;
+    const double zero = 0.0;
+    ar_points pts{&x, &y, &rxx, &ryy, &zero, &zero, &csx, &csy, 1};
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        const ar::PassGeometry geom = ar::pass_geometry_host(pts, wr, wc);
+        const int64_t ns = 2 * ry * 2 * rx;
+        cudaError_t e = ensure_dbuf(c, 8 * 8 + 16 + static_cast<size_t>(ns) * 4 + 256);
+        unsigned char* base = static_cast<unsigned char*>(c->dbuf);
+        double* dd = reinterpret_cast<double*>(base);
+        int64_t* di = reinterpret_cast<int64_t*>(base);
+        const double hostd[8] = {x, y, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        const int64_t hosti[4] = {rxx, ryy, csx, csy};
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(dd, hostd, sizeof(hostd), cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(di + 8, hosti, sizeof(hosti), cudaMemcpyHostToDevice, c->stream);
+        ar::DevPoints dp{dd + 0, dd + 1, di + 8, di + 9, dd + 2, dd + 3, di + 10, di + 11, 1};
+        float* fo = reinterpret_cast<float*>(base + 128);
+        ar::DevOutputs dout{fo, fo + 1, fo + 2, reinterpret_cast<uint8_t*>(fo + 3)};
+        float* dsurf = reinterpret_cast<float*>(base + 256);
+        if (e == cudaSuccess) e = cudaMemsetAsync(dsurf, 0, ns * 4, c->stream);
+        std::string err;
+        if (e == cudaSuccess)
+            e = ar::launch_track(dtype, pair->ref, pair->sec, pair->valid, wr, wc, dp, geom, 1,
+                                 measure, dout, c->scratch, c->num_sms, c->stream, &err, dsurf);
+        float outs[4];
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(outs, fo, sizeof(outs), cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = stage_d2h(c, surface, dsurf, ns * 4);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) {
+            rc = err.empty() ? cuda_fail(c, e, "ar_correlate") : fail(c, AR_ERR_UNSUPPORTED, err);
+        } else {
+            uint8_t sr;
+            std::memcpy(&sr, &outs[3], 1);
+            if (degenerate) *degenerate = (sr && std::isnan(outs[2])) ? 1 : 0;
+        }
+    }
+    ar_pair_destroy(pair);
+    return rc;
+}
+
+int ar_refine_patches(ar_ctx* c, const float* patches, int64_t count, int up, int32_t* row,
+                      int32_t* col, float* value) {
+    if (!c || (count > 0 && (!patches || !row || !col || !value)))
+        return fail(c, AR_ERR_ARG, "null argument");
+    if (!is_pow2(up) || up < 2 || up > 128)
+        return fail(c, AR_ERR_ARG, "`upsampling` must be a power of 2 in [2, 128]");
+    if (count <= 0) return AR_OK;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    const size_t need = static_cast<size_t>(count) * (25 * 4 + 4 + 4 + 4) + 64;
+    cudaError_t e = ensure_dbuf(c, need);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ar_refine_patches: device buffers");
+    float* dpatch = static_cast<float*>(c->dbuf);
+    int32_t* drow = reinterpret_cast<int32_t*>(dpatch + count * 25);
+    int32_t* dcol = drow + count;
+    float* dval = reinterpret_cast<float*>(dcol + count);
+    e = stage_h2d(c, dpatch, patches, count * 25 * sizeof(float));
+    if (e == cudaSuccess)
+        e = ar::launch_refine_patches(dpatch, count, up, drow, dcol, dval, c->num_sms, c->stream);
+    if (e == cudaSuccess) e = stage_d2h(c, row, drow, count * 4);
+    if (e == cudaSuccess) e = stage_d2h(c, col, dcol, count * 4);
+    if (e == cudaSuccess) e = stage_d2h(c, value, dval, count * 4);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ar_refine_patches");
+    return AR_OK;
+}
+
+int ar_synchronize(ar_ctx* c) {
+    if (!c) return AR_ERR_ARG;
+    DeviceGuard g(c->device);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    return e == cudaSuccess ? AR_OK : cuda_fail(c, e, "ar_synchronize");
+}
+
+}  // extern "C"

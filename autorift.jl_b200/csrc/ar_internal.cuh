@@ -1,0 +1,71 @@
+// Internal declarations shared by the CUDA translation units of libautorift_gpu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "autorift_gpu.h"
+
+namespace ar {
+
+// Pass geometry: the summary of a point set that sizes a launch (src/track.jl:176-197).
+struct PassGeometry {
+    int64_t max_ch = 0, max_cw = 0;  // effective chip extents (2 * (size / 2))
+    int64_t max_nr = 0, max_nc = 0;  // surface extents (2 * radius)
+    int64_t padx = 0, pady = 0;      // virtual zero padding, 0 when every window fits
+    int64_t searchable = 0;          // points with both radii > 0
+};
+
+// Device-resident point set (same field order as ar_points).
+struct DevPoints {
+    const double* x;
+    const double* y;
+    const int64_t* rx;
+    const int64_t* ry;
+    const double* dx0;
+    const double* dy0;
+    const int64_t* csx;
+    const int64_t* csy;
+    int64_t n;
+};
+
+struct DevOutputs {
+    float* dx;
+    float* dy;
+    float* corr;
+    uint8_t* searched;
+};
+
+// Scratch the track launch needs, owned by the context and grown on demand.
+struct TrackScratch {
+    int* sub_count = nullptr;       // number of points queued for sub-pixel refinement
+    int64_t* sub_point = nullptr;   // point index per queued item
+    int32_t* sub_origin = nullptr;  // (i0, j0) of the 5x5 patch, 0-based, per item
+    float* sub_patch = nullptr;     // 25 floats per item, column-major
+    int64_t capacity = 0;
+    int64_t* geom = nullptr;        // device-side pass geometry (8 int64)
+};
+
+// Host-side pass geometry of a host point set.
+PassGeometry pass_geometry_host(const ar_points& p, int64_t nrows, int64_t ncols);
+
+// Enqueue the track kernels. `geom` must describe `pts` (host- or device-computed).
+// `surf_out`, when given, receives every searched point's surface (max_nr x max_nc floats per
+// point, column-major with leading dimension nr of that point).
+cudaError_t launch_track(int dtype, const void* ref, const void* sec, const uint8_t* valid,
+                         int64_t nrows, int64_t ncols, const DevPoints& pts,
+                         const PassGeometry& geom, int up, int measure, const DevOutputs& out,
+                         TrackScratch& scratch, int num_sms, cudaStream_t stream,
+                         std::string* err, float* surf_out = nullptr);
+
+// Device-side pass geometry for a device point set (one small synchronising read).
+cudaError_t pass_geometry_device(const DevPoints& pts, int64_t nrows, int64_t ncols,
+                                 TrackScratch& scratch, cudaStream_t stream, PassGeometry* out);
+
+// Refine `count` patches already on the device.
+cudaError_t launch_refine_patches(const float* patches, int64_t count, int up, int32_t* row,
+                                  int32_t* col, float* value, int num_sms, cudaStream_t stream);
+
+}  // namespace ar

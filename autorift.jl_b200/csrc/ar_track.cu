@@ -1,0 +1,1039 @@
+// The track pass on sm_100a: one CTA per search point computes the ZNCC surface in shared
+// memory, its row-major argmax and the 5x5 refinement patch; a second kernel runs the pyrUp
+// cascade on the patches. The surface never leaves shared memory.
+//
+// Reference (AutoRIFT.jl): src/track.jl:103-152, 249-305 (the grid loop), src/points.jl:358-395
+// (chip and window bounds), src/correlate.jl:423-453 (prepare_chip!), 575-630 (ZNCC / NCC
+// normalisation), 785-848 (numerator), src/integral.jl:141-170, 244-247 (per-window sums),
+// src/peak.jl:32-61, 102-106, 196-324, 456-522 (peak and sub-pixel cascade).
+//
+// Numerics.
+//  * Numerator: FP32 products accumulated in FP32 over a few chip columns, then flushed into
+//    an FP64 accumulator. For UInt8 imagery the chip and window are staged as raw integers
+//    and the flush interval keeps every FP32 partial below 2^24, so the numerator
+//    sum(T*W) - mean(T)*sum(W) is exact -- the value the reference's FP32 FFT approximates.
+//    Other element types stage the mean-removed chip and a centred window (W - c).
+//  * Denominator: window box sums from per-window prefix tables built by warp scans in
+//    shared memory -- exact integers (uint32) for UInt8, FP64 otherwise -- and
+//    wvar = max(s2 - s1*s1/n, 0), den = cnorm*sqrt(wvar), surface = Float32(num/den), each
+//    operation an explicitly rounded FP64 intrinsic, as in src/correlate.jl:591-600.
+//  * Cascade: every pyrUp sample is fl(fl(0.75*b) + fl(0.125*fl(a+c))) or
+//    fl(0.5*fl(b+c)) with __fmul_rn/__fadd_rn, so no step is fused into an FMA and the result
+//    is bit-identical to the reference's Float32 arithmetic on the same patch.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <climits>
+#include <cmath>
+#include <cstdint>
+#include <string>
+
+#include "ar_internal.cuh"
+
+namespace ar {
+namespace {
+
+constexpr int kMI = 10;        // surface rows per thread item
+constexpr int kUA = 16;        // chip rows per inner step
+constexpr int kCorrThreads = 256;
+constexpr int kRefineThreads = 256;
+constexpr int kChunk = 16;     // rows of the penultimate cascade level per streaming chunk
+constexpr unsigned kFull = 0xffffffffu;
+
+template <typename T>
+struct Traits;
+template <>
+struct Traits<uint8_t> {
+    static constexpr bool raw = true;  // exact integer numerator
+    static constexpr bool integer = true;
+    typedef uint32_t ph_t;
+};
+template <>
+struct Traits<uint16_t> {
+    static constexpr bool raw = false;
+    static constexpr bool integer = true;
+    typedef double ph_t;
+};
+template <>
+struct Traits<int16_t> {
+    static constexpr bool raw = false;
+    static constexpr bool integer = true;
+    typedef double ph_t;
+};
+template <>
+struct Traits<float> {
+    static constexpr bool raw = false;
+    static constexpr bool integer = false;
+    typedef double ph_t;
+};
+
+// ----------------------------------------------------------------------------------------------
+// Reductions
+
+// Key for a row-major first strict maximum (src/peak.jl:32-61): the larger value wins, and
+// among equal values the smaller row-major index. NaN never wins; -0 equals +0.
+__device__ __forceinline__ unsigned long long argmax_key(float v, unsigned rowmajor) {
+    if (v != v) return 0ull;
+    if (v == 0.0f) v = 0.0f;
+    unsigned u = __float_as_uint(v);
+    u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    return (static_cast<unsigned long long>(u) << 32) | (0xffffffffu - rowmajor);
+}
+
+__device__ __forceinline__ float key_value(unsigned long long key) {
+    unsigned u = static_cast<unsigned>(key >> 32);
+    u = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+    return __uint_as_float(u);
+}
+
+// Decode to (row-major index, value); the reference returns (1,1) when nothing beats -Inf.
+__device__ __forceinline__ bool key_decode(unsigned long long key, unsigned* rowmajor,
+                                          float* value) {
+    if (key == 0ull) return false;
+    const float v = key_value(key);
+    if (v == -INFINITY) return false;
+    *rowmajor = 0xffffffffu - static_cast<unsigned>(key & 0xffffffffull);
+    *value = v;
+    return true;
+}
+
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long w = __shfl_xor_sync(kFull, v, o);
+        v = w > v ? w : v;
+    }
+    return v;
+}
+
+// Block-wide max; every thread gets the result. `red` holds >= 32 entries.
+__device__ unsigned long long block_max_u64(unsigned long long v, unsigned long long* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+    v = warp_max_u64(v);
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    unsigned long long r = lane < nw ? red[lane] : 0ull;
+    r = warp_max_u64(r);
+    return r;
+}
+
+__device__ __forceinline__ double warp_sum_f64(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = __dadd_rn(v, __shfl_xor_sync(kFull, v, o));
+    return v;
+}
+
+// Block-wide sum of up to three doubles; every thread gets the results.
+template <int N>
+__device__ void block_sum_f64(double (&v)[N], double* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int q = 0; q < N; ++q) v[q] = warp_sum_f64(v[q]);
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < N; ++q) red[q * 32 + warp] = v[q];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+        double r = lane < nw ? red[q * 32 + lane] : 0.0;
+        v[q] = warp_sum_f64(r);
+    }
+}
+
+template <typename V>
+__device__ __forceinline__ V warp_inclusive_scan(V v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const V w = __shfl_up_sync(kFull, v, o);
+        if (lane >= o) v = v + w;
+    }
+    return v;
+}
+
+// ----------------------------------------------------------------------------------------------
+// pyrUp taps (src/peak.jl:312-324, 374-382), 0-based.
+
+__device__ __forceinline__ int reflect101_0(int p, int n) {
+    if (n == 1) return 0;
+    const int m = n - 1;
+    while (p < 0 || p > m) {
+        if (p < 0) p = -p;
+        if (p > m) p = 2 * m - p;
+    }
+    return p;
+}
+
+// Source taps of output position p on an axis whose source length is n: returns the number
+// of taps (3 on a sample, 2 between samples) and the minus/centre/plus source indices.
+__device__ __forceinline__ int pyr_taps(int p, int n, int* m, int* c, int* q) {
+    if ((p & 1) == 0) {
+        *c = p >> 1;
+        *m = reflect101_0(p - 2, 2 * n) >> 1;
+        *q = reflect101_0(p + 2, 2 * n) >> 1;
+        return 3;
+    }
+    *c = reflect101_0(p - 1, 2 * n) >> 1;
+    *m = *c;
+    *q = reflect101_0(p + 1, 2 * n) >> 1;
+    return 2;
+}
+
+// One pyrUp sample in the reference's operation order (src/peak.jl:266-292).
+__device__ __forceinline__ float pyr_sample(int nt, float a, float b, float c) {
+    return nt == 3 ? __fadd_rn(__fmul_rn(0.75f, b), __fmul_rn(0.125f, __fadd_rn(a, c)))
+                   : __fmul_rn(0.5f, __fadd_rn(b, c));
+}
+
+// ----------------------------------------------------------------------------------------------
+// Correlation kernel
+
+struct CorrArgs {
+    const void* ref;
+    const void* sec;
+    const uint8_t* valid;
+    int64_t nrows, ncols;
+    DevPoints pts;
+    int64_t padx, pady;
+    int up, measure;
+    int TI, TJ;   // surface tile; TI a multiple of kMI and (TI/kMI)*TJ <= blockDim
+    int CHP;      // chip smem stride (rows), >= every point's ch rounded up to 16
+    int CWM;      // largest chip width
+    int WS;       // window smem stride (floats): even, WS/2 odd, >= TI + CHP
+    int PHS;      // prefix-table stride (entries), >= TI + largest ch
+    int NRS;      // surface smem stride (rows), >= largest nr
+    int NCM;      // largest nc
+    unsigned off_win, off_ph1, off_ph2, off_surf, off_red;  // byte offsets, chip at 0
+    DevOutputs out;
+    int* sub_count;
+    int64_t* sub_point;
+    int32_t* sub_origin;
+    float* sub_patch;
+    float* surf_out;  // optional: each point's surface, NRS x NCM floats per point
+};
+
+template <typename T>
+__device__ __forceinline__ double pixel(const T* img, int64_t nrows, int64_t ncols, int64_t r,
+                                        int64_t c) {
+    if (r < 0 || r >= nrows || c < 0 || c >= ncols) return 0.0;
+    return static_cast<double>(img[r + c * nrows]);
+}
+
+template <typename PH>
+__device__ __forceinline__ PH ph_of(float w);
+template <>
+__device__ __forceinline__ uint32_t ph_of<uint32_t>(float w) {
+    return static_cast<uint32_t>(w);
+}
+template <>
+__device__ __forceinline__ double ph_of<double>(float w) {
+    return static_cast<double>(w);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kCorrThreads, 2) k_corr(const CorrArgs A) {
+    typedef Traits<T> Tr;
+    typedef typename Tr::ph_t PH;
+    extern __shared__ __align__(16) unsigned char smem[];
+    float* s_chip = reinterpret_cast<float*>(smem);
+    float* s_win = reinterpret_cast<float*>(smem + A.off_win);
+    PH* s_ph1 = reinterpret_cast<PH*>(smem + A.off_ph1);
+    PH* s_ph2 = reinterpret_cast<PH*>(smem + A.off_ph2);
+    float* s_surf = reinterpret_cast<float*>(smem + A.off_surf);
+    double* s_red = reinterpret_cast<double*>(smem + A.off_red);
+    __shared__ int s_slot;
+
+    const int tid = threadIdx.x, bd = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = bd >> 5;
+    const T* ref = static_cast<const T*>(A.ref);
+    const T* sec = static_cast<const T*>(A.sec);
+    const int64_t NR = A.nrows + 2 * A.pady, NC = A.ncols + 2 * A.padx;
+    const double shx = static_cast<double>(A.padx) + 0.5;
+    const double shy = static_cast<double>(A.pady) + 0.5;
+
+    for (int64_t k = blockIdx.x; k < A.pts.n; k += gridDim.x) {
+        __syncthreads();  // shared buffers of the previous point are no longer read
+        const int64_t prx = A.pts.rx[k], pry = A.pts.ry[k];
+        if (!(prx > 0 && pry > 0)) continue;  // issearchable (src/points.jl:116-117)
+
+        // Geometry in padded 1-based coordinates (src/track.jl:207-210, src/points.jl:358-395).
+        const double xs = A.pts.x[k] + shx, ys = A.pts.y[k] + shy;
+        const int64_t hx = A.pts.csx[k] / 2, hy = A.pts.csy[k] / 2;
+        const int64_t ccx = static_cast<int64_t>(floor(__dsub_rn(xs, A.pts.dx0[k])));
+        const int64_t ccy = static_cast<int64_t>(floor(__dsub_rn(ys, A.pts.dy0[k])));
+        const int64_t wcx = static_cast<int64_t>(floor(xs)), wcy = static_cast<int64_t>(floor(ys));
+        const int64_t cr0 = ccy - hy, cr1 = ccy + hy - 1, cc0 = ccx - hx, cc1 = ccx + hx - 1;
+        const int64_t wr0 = wcy - hy - pry, wr1 = wcy + hy + pry - 2;
+        const int64_t wc0 = wcx - hx - prx, wc1 = wcx + hx + prx - 2;
+        // checkbounds (src/track.jl:271-272): an empty range is always in bounds.
+        const bool chip_in = (cr1 < cr0 || cc1 < cc0) ||
+                             (cr0 >= 1 && cr1 <= NR && cc0 >= 1 && cc1 <= NC);
+        const bool win_in = (wr1 < wr0 || wc1 < wc0) ||
+                            (wr0 >= 1 && wr1 <= NR && wc0 >= 1 && wc1 <= NC);
+        if (!chip_in || !win_in) continue;
+        const int ch = static_cast<int>(2 * hy), cw = static_cast<int>(2 * hx);
+        const int nr = static_cast<int>(2 * pry), nc = static_cast<int>(2 * prx);
+        if (ch <= 0 || cw <= 0) continue;  // an empty chip has no valid pixel
+        if (ch > A.CHP || cw > A.CWM || nr > A.NRS || nc > A.NCM) continue;  // not sized for
+        const int64_t chip_r = cr0 - 1 - A.pady, chip_c = cc0 - 1 - A.padx;
+        const int64_t win_r = wr0 - 1 - A.pady, win_c = wc0 - 1 - A.padx;
+
+        // _any_valid over the chip (src/track.jl:416-421).
+        int any = 0;
+        for (int e = tid; e < ch * cw; e += bd) {
+            const int64_t r = chip_r + e % ch, c = chip_c + e / ch;
+            if (r >= 0 && r < A.nrows && c >= 0 && c < A.ncols && A.valid[r + c * A.nrows])
+                any = 1;
+        }
+        if (!__syncthreads_or(any)) continue;
+        if (tid == 0) A.out.searched[k] = 1;
+
+        // prepare_chip! (src/correlate.jl:423-453): FP64 mean, then the mean-removed Float32
+        // copy, its FP64 sum of squares, and the FP64 sum of the rounded copy.
+        double st[1] = {0.0};
+        for (int e = tid; e < ch * cw; e += bd)
+            st[0] = __dadd_rn(st[0], pixel(sec, A.nrows, A.ncols, chip_r + e % ch, chip_c + e / ch));
+        block_sum_f64<1>(st, s_red);
+        const double nn = static_cast<double>(ch * cw);
+        const double mean = __ddiv_rn(st[0], nn);
+        const int chp = (ch + kUA - 1) & ~(kUA - 1);
+        double acc2[2] = {0.0, 0.0};
+        for (int e = tid; e < chp * cw; e += bd) {
+            const int a = e % chp, b = e / chp;
+            float staged = 0.0f;
+            if (a < ch) {
+                const double v = pixel(sec, A.nrows, A.ncols, chip_r + a, chip_c + b);
+                const double d = __dsub_rn(v, mean);
+                const float df = __double2float_rn(d);
+                acc2[0] = __dadd_rn(acc2[0], __dmul_rn(d, d));
+                acc2[1] = __dadd_rn(acc2[1], static_cast<double>(df));
+                staged = Tr::raw ? static_cast<float>(v) : df;
+            }
+            s_chip[b * A.CHP + a] = staged;
+        }
+        block_sum_f64<2>(acc2, s_red);
+        const double sq = acc2[0], sumd = acc2[1];
+        if (!(sq > __dmul_rn(__dmul_rn(DBL_EPSILON, static_cast<double>(ch)),
+                             static_cast<double>(cw))))
+            continue;  // degenerate chip: searched, no measurement (src/track.jl:286)
+        const double cnorm = __dsqrt_rn(sq);
+        // Centring constant for the window of non-raw element types.
+        double cshift = 0.0;
+        if (!Tr::raw) cshift = Tr::integer ? rint(mean) : static_cast<double>(__double2float_rn(mean));
+
+        const int F = Tr::raw ? max(1, 16777216 / (chp * 65025)) : 2;
+
+        for (int ti = 0; ti < nr; ti += A.TI) {
+            const int trows = min(A.TI, nr - ti);
+            const int trows_p = (trows + kMI - 1) / kMI * kMI;
+            const int srows = trows_p + chp;  // staged window rows (<= WS)
+            const int wrows = trows + ch - 1; // rows the box sums use
+            for (int tj = 0; tj < nc; tj += A.TJ) {
+                const int tcols = min(A.TJ, nc - tj);
+                const int xcols = tcols + cw - 1;
+                __syncthreads();
+                // Stage the window block column-major, zero outside the image and below the
+                // window's last row.
+                for (int e = tid; e < xcols * srows; e += bd) {
+                    const int r = e % srows, x = e / srows;
+                    float v = 0.0f;
+                    if (r < wrows) {
+                        const double pv =
+                            pixel(ref, A.nrows, A.ncols, win_r + ti + r, win_c + tj + x);
+                        v = Tr::raw ? static_cast<float>(pv)
+                                    : __double2float_rn(__dsub_rn(pv, cshift));
+                    }
+                    s_win[x * A.WS + r] = v;
+                }
+                __syncthreads();
+                // Per-window sums of W and W^2 over cw columns for every row the tile uses
+                // (integral_both!, src/integral.jl:141-170), stored at slot r + 1.
+                const int nseg = (tcols + 15) >> 4;
+                for (int task = tid; task < wrows * nseg; task += bd) {
+                    const int r = task % wrows, seg = task / wrows;
+                    const int j0s = seg << 4, j1s = min(j0s + 16, tcols);
+                    PH h1 = 0, h2 = 0;
+                    for (int b = 0; b < cw; ++b) {
+                        const PH w = ph_of<PH>(s_win[(j0s + b) * A.WS + r]);
+                        h1 = h1 + w;
+                        h2 = h2 + w * w;
+                    }
+                    s_ph1[j0s * A.PHS + r + 1] = h1;
+                    s_ph2[j0s * A.PHS + r + 1] = h2;
+                    for (int jl = j0s + 1; jl < j1s; ++jl) {
+                        const PH wo = ph_of<PH>(s_win[(jl - 1) * A.WS + r]);
+                        const PH wn = ph_of<PH>(s_win[(jl - 1 + cw) * A.WS + r]);
+                        h1 = h1 + wn - wo;
+                        h2 = h2 + wn * wn - wo * wo;
+                        s_ph1[jl * A.PHS + r + 1] = h1;
+                        s_ph2[jl * A.PHS + r + 1] = h2;
+                    }
+                }
+                __syncthreads();
+                // Exclusive prefix down each column by warp scans: ph[jl][q] = sum_{r<q} H[r].
+                for (int jl = warp; jl < tcols; jl += nwarps) {
+                    PH c1 = 0, c2 = 0;
+                    for (int q = 1; q <= wrows; q += 32) {
+                        const int idx = q + lane;
+                        PH v1 = idx <= wrows ? s_ph1[jl * A.PHS + idx] : PH(0);
+                        PH v2 = idx <= wrows ? s_ph2[jl * A.PHS + idx] : PH(0);
+                        v1 = warp_inclusive_scan(v1) + c1;
+                        v2 = warp_inclusive_scan(v2) + c2;
+                        if (idx <= wrows) {
+                            s_ph1[jl * A.PHS + idx] = v1;
+                            s_ph2[jl * A.PHS + idx] = v2;
+                        }
+                        c1 = __shfl_sync(kFull, v1, 31);
+                        c2 = __shfl_sync(kFull, v2, 31);
+                    }
+                    if (lane == 0) {
+                        s_ph1[jl * A.PHS] = PH(0);
+                        s_ph2[jl * A.PHS] = PH(0);
+                    }
+                }
+                __syncthreads();
+
+                // Numerator: item = (row group, column), kMI surface rows per thread.
+                const int ig = tid / A.TJ, jl = tid % A.TJ;
+                if (ig * kMI < trows && jl < tcols) {
+                    const int il = ig * kMI;
+                    float acc[kMI];
+                    double acc64[kMI];
+#pragma unroll
+                    for (int m = 0; m < kMI; ++m) { acc[m] = 0.0f; acc64[m] = 0.0; }
+                    const float* wbase = s_win + jl * A.WS + il;
+                    int fc = 0;
+                    for (int b = 0; b < cw; ++b) {
+                        const float* wc = wbase + b * A.WS;
+                        const float* cc = s_chip + b * A.CHP;
+                        for (int a0 = 0; a0 < chp; a0 += kUA) {
+                            float c[kUA];
+                            float w[kUA + kMI];
+#pragma unroll
+                            for (int q = 0; q < kUA / 4; ++q) {
+                                const float4 v = *reinterpret_cast<const float4*>(cc + a0 + 4 * q);
+                                c[4 * q] = v.x; c[4 * q + 1] = v.y; c[4 * q + 2] = v.z; c[4 * q + 3] = v.w;
+                            }
+#pragma unroll
+                            for (int q = 0; q < (kUA + kMI) / 2; ++q) {
+                                const float2 v = *reinterpret_cast<const float2*>(wc + a0 + 2 * q);
+                                w[2 * q] = v.x; w[2 * q + 1] = v.y;
+                            }
+#pragma unroll
+                            for (int a = 0; a < kUA; ++a)
+#pragma unroll
+                                for (int m = 0; m < kMI; ++m) acc[m] = fmaf(c[a], w[m + a], acc[m]);
+                        }
+                        if (++fc == F) {
+#pragma unroll
+                            for (int m = 0; m < kMI; ++m) {
+                                acc64[m] = __dadd_rn(acc64[m], static_cast<double>(acc[m]));
+                                acc[m] = 0.0f;
+                            }
+                            fc = 0;
+                        }
+                    }
+#pragma unroll
+                    for (int m = 0; m < kMI; ++m)
+                        acc64[m] = __dadd_rn(acc64[m], static_cast<double>(acc[m]));
+
+                    // Normalisation (src/correlate.jl:591-600, 624-628).
+#pragma unroll
+                    for (int m = 0; m < kMI; ++m) {
+                        const int ir = il + m;
+                        if (ir < trows) {
+                            const PH p1 = s_ph1[jl * A.PHS + ir + ch] - s_ph1[jl * A.PHS + ir];
+                            const PH p2 = s_ph2[jl * A.PHS + ir + ch] - s_ph2[jl * A.PHS + ir];
+                            double s1, s2, num;
+                            if (Tr::raw) {
+                                s1 = static_cast<double>(p1);
+                                s2 = static_cast<double>(p2);
+                                num = __dsub_rn(acc64[m], __dmul_rn(mean, s1));
+                            } else {
+                                const double s1c = static_cast<double>(p1);
+                                const double s2c = static_cast<double>(p2);
+                                s1 = __dadd_rn(s1c, __dmul_rn(nn, cshift));
+                                s2 = __dadd_rn(__dadd_rn(s2c, __dmul_rn(__dmul_rn(2.0, cshift), s1c)),
+                                               __dmul_rn(__dmul_rn(nn, cshift), cshift));
+                                num = __dadd_rn(acc64[m], __dmul_rn(cshift, sumd));
+                            }
+                            double den;
+                            if (A.measure == AR_NCC) {
+                                den = __dmul_rn(cnorm, __dsqrt_rn(s2 > 0.0 ? s2 : 0.0));
+                            } else {
+                                double wvar = __dsub_rn(s2, __ddiv_rn(__dmul_rn(s1, s1), nn));
+                                if (!(wvar > 0.0)) wvar = 0.0;
+                                den = __dmul_rn(cnorm, __dsqrt_rn(wvar));
+                            }
+                            const float sv = den > 0.0 ? __double2float_rn(__ddiv_rn(num, den)) : 0.0f;
+                            s_surf[(ti + ir) + (tj + jl) * A.NRS] = sv;
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (A.surf_out) {
+            float* so = A.surf_out + k * static_cast<int64_t>(A.NRS) * A.NCM;
+            for (int e = tid; e < nr * nc; e += bd) so[e] = s_surf[(e % nr) + (e / nr) * A.NRS];
+        }
+
+        // Integer peak (src/peak.jl:32-61).
+        unsigned long long best = 0ull;
+        for (int e = tid; e < nr * nc; e += bd) {
+            const int i = e % nr, j = e / nr;
+            const unsigned long long kk =
+                argmax_key(s_surf[i + j * A.NRS], static_cast<unsigned>(i * nc + j));
+            best = kk > best ? kk : best;
+        }
+        best = block_max_u64(best, reinterpret_cast<unsigned long long*>(s_red));
+        unsigned rm = 0;
+        float pv = 0.0f;
+        int pi = 0, pj = 0;
+        if (key_decode(best, &rm, &pv)) {
+            pi = static_cast<int>(rm / nc);
+            pj = static_cast<int>(rm % nc);
+        }
+        if (A.up == 1 || nr < 5 || nc < 5) {
+            // peak_offset (src/peak.jl:102-106) and the output write (src/track.jl:293-295).
+            if (tid == 0) {
+                const float v = s_surf[pi + pj * A.NRS];
+                A.out.dx[k] = __double2float_rn(
+                    __dadd_rn(static_cast<double>(pj - static_cast<int>(prx)), A.pts.dx0[k]));
+                A.out.dy[k] = __double2float_rn(
+                    __dadd_rn(static_cast<double>(pi - static_cast<int>(pry)), A.pts.dy0[k]));
+                A.out.corr[k] = v;
+            }
+        } else {
+            // The clamped 5x5 patch of subpixel_peak (src/peak.jl:473-482), queued.
+            const int pi0 = min(max(pi - 2, 0), max(nr - 5, 0));
+            const int pj0 = min(max(pj - 2, 0), max(nc - 5, 0));
+            if (tid == 0) s_slot = atomicAdd(A.sub_count, 1);
+            __syncthreads();
+            const int slot = s_slot;
+            if (tid < 25) {
+                const int a = tid % 5, b = tid / 5;
+                A.sub_patch[static_cast<int64_t>(slot) * 25 + tid] =
+                    s_surf[(pi0 + a) + (pj0 + b) * A.NRS];
+            }
+            if (tid == 0) {
+                A.sub_point[slot] = k;
+                A.sub_origin[2 * slot] = pi0;
+                A.sub_origin[2 * slot + 1] = pj0;
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------------------------
+// Sub-pixel cascade kernel (src/peak.jl:456-522 from the patch onward).
+
+struct RefineArgs {
+    const int* count;       // device count of queued items (or null: use n_items)
+    int64_t n_items;
+    const int64_t* point;   // point index per item (null for bare patches)
+    const int32_t* origin;  // patch origin per item (null for bare patches)
+    const float* patch;     // 25 floats per item
+    DevPoints pts;
+    DevOutputs out;
+    int32_t* orow;          // bare-patch outputs (when point is null)
+    int32_t* ocol;
+    float* oval;
+    int levels;             // log2(upsampling) >= 1
+    int nmat;               // size of the last materialised level
+    unsigned off_B, off_T, off_P, off_C;  // float offsets: A at 0
+};
+
+// One pyrUp step over shared memory, src (sh x sw) -> dst (2sh x 2sw) via tmp (2sh x sw);
+// all column-major. The vertical then horizontal order of src/peak.jl:261-292.
+__device__ void pyrup_block(const float* src, int sh, int sw, float* dst, float* tmp) {
+    const int th = 2 * sh;
+    for (int e = threadIdx.x; e < th * sw; e += blockDim.x) {
+        const int i = e % th, j = e / th;
+        int m, c, q;
+        const int nt = pyr_taps(i, sh, &m, &c, &q);
+        const float* s = src + j * sh;
+        tmp[i + j * th] = pyr_sample(nt, s[m], s[c], s[q]);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < th * 2 * sw; e += blockDim.x) {
+        const int i = e % th, j = e / th;
+        int m, c, q;
+        const int nt = pyr_taps(j, sw, &m, &c, &q);
+        dst[i + j * th] = pyr_sample(nt, tmp[i + m * th], tmp[i + c * th], tmp[i + q * th]);
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kRefineThreads) k_refine(const RefineArgs A) {
+    extern __shared__ __align__(16) float rsm[];
+    float* sA = rsm;
+    float* sB = rsm + A.off_B;
+    float* sT = rsm + A.off_T;
+    float* sP = rsm + A.off_P;
+    float* sC = rsm + A.off_C;  // streaming chunk buffers (alias sB/sT)
+    __shared__ unsigned long long red[32];
+
+    const int tid = threadIdx.x, bd = blockDim.x;
+    const int64_t count = A.count ? static_cast<int64_t>(*A.count) : A.n_items;
+    const int L = A.levels;
+    const int nmat_levels = L <= 2 ? L : L - 2;
+
+    for (int64_t item = blockIdx.x; item < count; item += gridDim.x) {
+        __syncthreads();
+        if (tid < 25) sP[tid] = A.patch[item * 25 + tid];
+        __syncthreads();
+        const float* cur = sP;
+        int n = 5;
+        for (int lev = 1; lev <= nmat_levels; ++lev) {
+            float* dst = ((nmat_levels - lev) & 1) == 0 ? sA : sB;
+            pyrup_block(cur, n, n, dst, sT);
+            cur = dst;
+            n *= 2;
+        }
+        unsigned long long best = 0ull;
+        int nfinal;
+        if (L <= 2) {
+            nfinal = n;
+            for (int e = tid; e < n * n; e += bd) {
+                const int i = e % n, j = e / n;
+                const unsigned long long kk = argmax_key(cur[i + j * n], static_cast<unsigned>(i * n + j));
+                best = kk > best ? kk : best;
+            }
+        } else {
+            // Stream the last two levels from the materialised one (n x n in sA): rows of the
+            // penultimate level (2n wide) are built a chunk at a time, the final level (4n) is
+            // reduced on the fly and never stored.
+            const int N1 = 2 * n, N2 = 4 * n;
+            nfinal = N2;
+            float* TA = sC;                       // (kChunk + 2) x n
+            float* RB = TA + (kChunk + 2) * n;    // (kChunk + 2) x N1
+            float* TB = RB + (kChunk + 2) * N1;   // 2*kChunk x N1
+            for (int q0 = 0; q0 < N1; q0 += kChunk) {
+                const int q1 = min(q0 + kChunk, N1);
+                const int qa = max(q0 - 1, 0), qb = min(q1, N1 - 1);
+                const int nq = qb - qa + 1;
+                const int np = 2 * (q1 - q0);
+                // Vertical taps of the penultimate rows qa..qb over the materialised level.
+                for (int e = tid; e < nq * n; e += bd) {
+                    const int qq = e / n, jj = e % n;
+                    int m, c, q;
+                    const int nt = pyr_taps(qa + qq, n, &m, &c, &q);
+                    TA[qq * n + jj] = pyr_sample(nt, cur[m + jj * n], cur[c + jj * n], cur[q + jj * n]);
+                }
+                __syncthreads();
+                // Horizontal: the penultimate rows themselves.
+                for (int e = tid; e < nq * N1; e += bd) {
+                    const int qq = e / N1, cc = e % N1;
+                    int m, c, q;
+                    const int nt = pyr_taps(cc, n, &m, &c, &q);
+                    RB[qq * N1 + cc] = pyr_sample(nt, TA[qq * n + m], TA[qq * n + c], TA[qq * n + q]);
+                }
+                __syncthreads();
+                // Vertical taps of the final rows 2q0 .. 2q1-1 over the penultimate rows.
+                for (int e = tid; e < np * N1; e += bd) {
+                    const int pp = e / N1, cc = e % N1;
+                    int m, c, q;
+                    const int nt = pyr_taps(2 * q0 + pp, N1, &m, &c, &q);
+                    TB[pp * N1 + cc] = pyr_sample(nt, RB[(m - qa) * N1 + cc], RB[(c - qa) * N1 + cc],
+                                                  RB[(q - qa) * N1 + cc]);
+                }
+                __syncthreads();
+                // Horizontal: final samples, reduced to the row-major first maximum.
+                for (int e = tid; e < np * N2; e += bd) {
+                    const int pp = e / N2, c4 = e % N2;
+                    int m, c, q;
+                    const int nt = pyr_taps(c4, N1, &m, &c, &q);
+                    const float v = pyr_sample(nt, TB[pp * N1 + m], TB[pp * N1 + c], TB[pp * N1 + q]);
+                    const unsigned long long kk =
+                        argmax_key(v, static_cast<unsigned>((2 * q0 + pp) * N2 + c4));
+                    best = kk > best ? kk : best;
+                }
+                __syncthreads();
+            }
+        }
+        best = block_max_u64(best, red);
+        if (tid == 0) {
+            unsigned rm = 0;
+            float v = 0.0f;
+            int si = 0, sj = 0;
+            if (key_decode(best, &rm, &v)) {
+                si = static_cast<int>(rm / nfinal);
+                sj = static_cast<int>(rm % nfinal);
+            } else {
+                v = cur[0];  // (1,1) of a level with nothing above -Inf; only reachable if materialised
+            }
+            if (A.point) {
+                const int64_t k = A.point[item];
+                const int i0 = A.origin[2 * item], j0 = A.origin[2 * item + 1];
+                const double factor = static_cast<double>(1 << L);
+                const double row = __dadd_rn(__ddiv_rn(static_cast<double>(si), factor), static_cast<double>(i0));
+                const double col = __dadd_rn(__ddiv_rn(static_cast<double>(sj), factor), static_cast<double>(j0));
+                const double dx = __dsub_rn(col, static_cast<double>(A.pts.rx[k]));
+                const double dy = __dsub_rn(row, static_cast<double>(A.pts.ry[k]));
+                A.out.dx[k] = __double2float_rn(__dadd_rn(dx, A.pts.dx0[k]));
+                A.out.dy[k] = __double2float_rn(__dadd_rn(dy, A.pts.dy0[k]));
+                A.out.corr[k] = v;
+            } else {
+                A.orow[item] = si;
+                A.ocol[item] = sj;
+                A.oval[item] = v;
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------------------------
+// Small helpers
+
+__global__ void k_init_outputs(DevOutputs out, int64_t n, int* sub_count) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i == 0 && sub_count) *sub_count = 0;
+    if (i < n) {
+        out.dx[i] = __int_as_float(0x7fc00000);
+        out.dy[i] = __int_as_float(0x7fc00000);
+        out.corr[i] = __int_as_float(0x7fc00000);
+        out.searched[i] = 0;
+    }
+}
+
+// geom: [0] max ch, [1] max cw, [2] max nr, [3] max nc, [4] max px term, [5] max py term,
+// [6] 1 while every window fits, [7] searchable count. Reductions by atomics.
+__global__ void k_pass_geometry(DevPoints p, int64_t nrows, int64_t ncols, long long* geom) {
+    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (k >= p.n) return;
+    const int64_t rx = p.rx[k], ry = p.ry[k];
+    if (!(rx > 0 && ry > 0)) return;
+    const int64_t hx = p.csx[k] / 2, hy = p.csy[k] / 2;
+    atomicMax(&geom[0], static_cast<long long>(2 * hy));
+    atomicMax(&geom[1], static_cast<long long>(2 * hx));
+    atomicMax(&geom[2], static_cast<long long>(2 * ry));
+    atomicMax(&geom[3], static_cast<long long>(2 * rx));
+    atomicMax(&geom[4], static_cast<long long>(hx + rx + static_cast<int64_t>(ceil(fabs(p.dx0[k])))));
+    atomicMax(&geom[5], static_cast<long long>(hy + ry + static_cast<int64_t>(ceil(fabs(p.dy0[k])))));
+    const int64_t wcx = static_cast<int64_t>(floor(p.x[k])), wcy = static_cast<int64_t>(floor(p.y[k]));
+    const bool inb = (wcy - hy - ry) >= 1 && (wcy + hy + ry - 2) <= nrows &&
+                     (wcx - hx - rx) >= 1 && (wcx + hx + rx - 2) <= ncols;
+    if (!inb) atomicMin(&geom[6], 0ll);
+    atomicAdd(reinterpret_cast<unsigned long long*>(&geom[7]), 1ull);
+}
+
+inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// Window stride: even with an odd half, so that 16 lanes reading float2 at consecutive
+// columns hit 16 distinct 8-byte bank pairs.
+inline int window_stride(int rows) {
+    int s = round_up(rows, 2);
+    if ((s / 2) % 2 == 0) s += 2;
+    return s;
+}
+
+struct CorrPlan {
+    int TI, TJ, CHP, CWM, WS, PHS, NRS, NCM;
+    unsigned off_win, off_ph1, off_ph2, off_surf, off_red;
+    size_t smem;
+};
+
+bool plan_corr(const PassGeometry& g, size_t ph_bytes, size_t smem_cap, CorrPlan* P) {
+    const int ch = static_cast<int>(g.max_ch), cw = static_cast<int>(g.max_cw);
+    const int nr = static_cast<int>(g.max_nr), nc = static_cast<int>(g.max_nc);
+    P->CHP = round_up(std::max(ch, 1), kUA);
+    P->CWM = std::max(cw, 1);
+    P->NRS = std::max(nr, 1);
+    P->NCM = std::max(nc, 1);
+    // Columns per tile: as many as fit one thread each with at least one row group, rows to
+    // fill the block. Shrink until the shared-memory budget is met.
+    for (int TJ = std::min(nc, kCorrThreads); TJ >= 1; TJ = (TJ > 8 ? TJ - 8 : TJ - 1)) {
+        const int groups = std::max(1, kCorrThreads / TJ);
+        for (int TI = std::min(round_up(nr, kMI), groups * kMI); TI >= kMI; TI -= kMI) {
+            const int WS = window_stride(TI + P->CHP);
+            const int PHS = TI + ch + 1;
+            size_t off = static_cast<size_t>(P->CHP) * P->CWM * 4;
+            off = (off + 15) & ~size_t(15);
+            const unsigned off_win = static_cast<unsigned>(off);
+            off += static_cast<size_t>(WS) * (TJ + P->CWM - 1) * 4;
+            off = (off + 15) & ~size_t(15);
+            const unsigned off_ph1 = static_cast<unsigned>(off);
+            off += static_cast<size_t>(PHS) * TJ * ph_bytes;
+            off = (off + 15) & ~size_t(15);
+            const unsigned off_ph2 = static_cast<unsigned>(off);
+            off += static_cast<size_t>(PHS) * TJ * ph_bytes;
+            off = (off + 15) & ~size_t(15);
+            const unsigned off_surf = static_cast<unsigned>(off);
+            off += static_cast<size_t>(P->NRS) * P->NCM * 4;
+            off = (off + 15) & ~size_t(15);
+            const unsigned off_red = static_cast<unsigned>(off);
+            off += 3 * 32 * 8;
+            if (off <= smem_cap) {
+                P->TI = TI;
+                P->TJ = TJ;
+                P->WS = WS;
+                P->PHS = PHS;
+                P->off_win = off_win;
+                P->off_ph1 = off_ph1;
+                P->off_ph2 = off_ph2;
+                P->off_surf = off_surf;
+                P->off_red = off_red;
+                P->smem = off;
+                return true;
+            }
+        }
+        if (TJ == 1) break;
+    }
+    return false;
+}
+
+int ilog2_exact(int up) {
+    int L = 0;
+    while ((1 << L) < up) ++L;
+    return (1 << L) == up ? L : -1;
+}
+
+struct RefinePlan {
+    int levels, nmat;
+    unsigned off_B, off_T, off_P, off_C;
+    size_t smem;
+};
+
+RefinePlan plan_refine(int up) {
+    RefinePlan R{};
+    R.levels = ilog2_exact(up);
+    const int L = R.levels;
+    const int nm = L <= 2 ? 5 << L : 5 << (L - 2);
+    R.nmat = nm;
+    const size_t a = static_cast<size_t>(nm) * nm;
+    const size_t b = static_cast<size_t>(nm / 2) * (nm / 2);
+    const size_t t = static_cast<size_t>(nm) * (nm / 2);
+    size_t chunk = 0;
+    if (L > 2) chunk = static_cast<size_t>(kChunk + 2) * nm + static_cast<size_t>(kChunk + 2) * 2 * nm +
+                       static_cast<size_t>(2 * kChunk) * 2 * nm;
+    R.off_B = static_cast<unsigned>(a);
+    R.off_T = static_cast<unsigned>(a + b);
+    R.off_C = static_cast<unsigned>(a);  // the chunk buffers reuse B and T once materialised
+    const size_t tail = std::max(b + t, chunk);
+    R.off_P = static_cast<unsigned>(a + tail);
+    R.smem = (a + tail + 32) * sizeof(float);
+    return R;
+}
+
+template <typename T>
+cudaError_t launch_corr_t(const CorrArgs& A, const CorrPlan& P, int grid, cudaStream_t stream) {
+    cudaError_t e = cudaFuncSetAttribute(k_corr<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(P.smem));
+    if (e != cudaSuccess) return e;
+    k_corr<T><<<grid, kCorrThreads, P.smem, stream>>>(A);
+    return cudaGetLastError();
+}
+
+cudaError_t ensure_scratch(TrackScratch& s, int64_t n) {
+    if (!s.geom) {
+        cudaError_t e = cudaMalloc(&s.geom, 8 * sizeof(int64_t));
+        if (e != cudaSuccess) return e;
+    }
+    if (!s.sub_count) {
+        cudaError_t e = cudaMalloc(&s.sub_count, sizeof(int));
+        if (e != cudaSuccess) return e;
+    }
+    if (s.capacity >= n) return cudaSuccess;
+    cudaFree(s.sub_point);
+    cudaFree(s.sub_origin);
+    cudaFree(s.sub_patch);
+    s.sub_point = nullptr;
+    s.sub_origin = nullptr;
+    s.sub_patch = nullptr;
+    s.capacity = 0;
+    const int64_t cap = std::max<int64_t>(n, 1024);
+    cudaError_t e = cudaMalloc(&s.sub_point, cap * sizeof(int64_t));
+    if (e == cudaSuccess) e = cudaMalloc(&s.sub_origin, cap * 2 * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&s.sub_patch, cap * 25 * sizeof(float));
+    if (e != cudaSuccess) return e;
+    s.capacity = cap;
+    return cudaSuccess;
+}
+
+}  // namespace
+
+PassGeometry pass_geometry_host(const ar_points& p, int64_t nrows, int64_t ncols) {
+    PassGeometry g;
+    bool fits = true;
+    int64_t px = 0, py = 0;
+    for (int64_t k = 0; k < p.n; ++k) {
+        const int64_t rx = p.radius_x[k], ry = p.radius_y[k];
+        if (!(rx > 0 && ry > 0)) continue;
+        const int64_t hx = p.chip_size_x[k] / 2, hy = p.chip_size_y[k] / 2;
+        g.max_ch = std::max(g.max_ch, 2 * hy);
+        g.max_cw = std::max(g.max_cw, 2 * hx);
+        g.max_nr = std::max(g.max_nr, 2 * ry);
+        g.max_nc = std::max(g.max_nc, 2 * rx);
+        px = std::max(px, hx + rx + static_cast<int64_t>(std::ceil(std::fabs(p.dx_prior[k]))));
+        py = std::max(py, hy + ry + static_cast<int64_t>(std::ceil(std::fabs(p.dy_prior[k]))));
+        const int64_t wcx = static_cast<int64_t>(std::floor(p.x[k]));
+        const int64_t wcy = static_cast<int64_t>(std::floor(p.y[k]));
+        fits = fits && (wcy - hy - ry) >= 1 && (wcy + hy + ry - 2) <= nrows &&
+               (wcx - hx - rx) >= 1 && (wcx + hx + rx - 2) <= ncols;
+        ++g.searchable;
+    }
+    g.padx = fits ? 0 : px + 2;
+    g.pady = fits ? 0 : py + 2;
+    return g;
+}
+
+cudaError_t pass_geometry_device(const DevPoints& pts, int64_t nrows, int64_t ncols,
+                                 TrackScratch& scratch, cudaStream_t stream, PassGeometry* out) {
+    cudaError_t e = ensure_scratch(scratch, 0);
+    if (e != cudaSuccess) return e;
+    long long init[8] = {0, 0, 0, 0, 0, 0, 1, 0};
+    e = cudaMemcpyAsync(scratch.geom, init, sizeof(init), cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return e;
+    if (pts.n > 0) {
+        const int threads = 256;
+        const int64_t blocks = (pts.n + threads - 1) / threads;
+        k_pass_geometry<<<static_cast<unsigned>(blocks), threads, 0, stream>>>(
+            pts, nrows, ncols, reinterpret_cast<long long*>(scratch.geom));
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    long long g[8];
+    e = cudaMemcpyAsync(g, scratch.geom, sizeof(g), cudaMemcpyDeviceToHost, stream);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return e;
+    out->max_ch = g[0];
+    out->max_cw = g[1];
+    out->max_nr = g[2];
+    out->max_nc = g[3];
+    const bool fits = g[6] != 0;
+    out->padx = fits ? 0 : g[4] + 2;
+    out->pady = fits ? 0 : g[5] + 2;
+    out->searchable = g[7];
+    return cudaSuccess;
+}
+
+cudaError_t launch_track(int dtype, const void* ref, const void* sec, const uint8_t* valid,
+                         int64_t nrows, int64_t ncols, const DevPoints& pts,
+                         const PassGeometry& geom, int up, int measure, const DevOutputs& out,
+                         TrackScratch& scratch, int num_sms, cudaStream_t stream,
+                         std::string* err, float* surf_out) {
+    cudaError_t e = ensure_scratch(scratch, pts.n);
+    if (e != cudaSuccess) return e;
+    if (pts.n > 0) {
+        const int threads = 256;
+        k_init_outputs<<<static_cast<unsigned>((pts.n + threads - 1) / threads), threads, 0, stream>>>(
+            out, pts.n, scratch.sub_count);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (geom.searchable == 0 || geom.max_cw == 0 || geom.max_ch == 0) return cudaSuccess;
+
+    const size_t ph_bytes = dtype == AR_U8 ? 4 : 8;
+    CorrPlan P{};
+    if (!plan_corr(geom, ph_bytes, 220 * 1024, &P)) {
+        if (err) *err = "chip and search geometry too large for shared memory";
+        return cudaErrorInvalidValue;
+    }
+    CorrArgs A{};
+    A.ref = ref;
+    A.sec = sec;
+    A.valid = valid;
+    A.nrows = nrows;
+    A.ncols = ncols;
+    A.pts = pts;
+    A.padx = geom.padx;
+    A.pady = geom.pady;
+    A.up = up;
+    A.measure = measure;
+    A.TI = P.TI;
+    A.TJ = P.TJ;
+    A.CHP = P.CHP;
+    A.CWM = P.CWM;
+    A.WS = P.WS;
+    A.PHS = P.PHS;
+    A.NRS = P.NRS;
+    A.NCM = P.NCM;
+    A.off_win = P.off_win;
+    A.off_ph1 = P.off_ph1;
+    A.off_ph2 = P.off_ph2;
+    A.off_surf = P.off_surf;
+    A.off_red = P.off_red;
+    A.out = out;
+    A.sub_count = scratch.sub_count;
+    A.sub_point = scratch.sub_point;
+    A.sub_origin = scratch.sub_origin;
+    A.sub_patch = scratch.sub_patch;
+    A.surf_out = surf_out;
+
+    const int per_sm = P.smem <= 100 * 1024 ? 2 : 1;
+    const int64_t want = static_cast<int64_t>(num_sms) * per_sm * 8;
+    const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(pts.n, want)));
+    switch (dtype) {
+        case AR_U8: e = launch_corr_t<uint8_t>(A, P, grid, stream); break;
+        case AR_U16: e = launch_corr_t<uint16_t>(A, P, grid, stream); break;
+        case AR_I16: e = launch_corr_t<int16_t>(A, P, grid, stream); break;
+        case AR_F32: e = launch_corr_t<float>(A, P, grid, stream); break;
+        default:
+            if (err) *err = "unsupported element type";
+            return cudaErrorInvalidValue;
+    }
+    if (e != cudaSuccess) return e;
+    if (up == 1) return cudaSuccess;
+
+    const RefinePlan R = plan_refine(up);
+    RefineArgs B{};
+    B.count = scratch.sub_count;
+    B.n_items = 0;
+    B.point = scratch.sub_point;
+    B.origin = scratch.sub_origin;
+    B.patch = scratch.sub_patch;
+    B.pts = pts;
+    B.out = out;
+    B.levels = R.levels;
+    B.nmat = R.nmat;
+    B.off_B = R.off_B;
+    B.off_T = R.off_T;
+    B.off_P = R.off_P;
+    B.off_C = R.off_C;
+    e = cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(R.smem));
+    if (e != cudaSuccess) return e;
+    const int rgrid = static_cast<int>(std::max<int64_t>(
+        1, std::min<int64_t>(pts.n, static_cast<int64_t>(num_sms) * 4)));
+    k_refine<<<rgrid, kRefineThreads, R.smem, stream>>>(B);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_refine_patches(const float* patches, int64_t count, int up, int32_t* row,
+                                  int32_t* col, float* value, int num_sms, cudaStream_t stream) {
+    if (count <= 0) return cudaSuccess;
+    const RefinePlan R = plan_refine(up);
+    RefineArgs B{};
+    B.count = nullptr;
+    B.n_items = count;
+    B.point = nullptr;
+    B.origin = nullptr;
+    B.patch = patches;
+    B.orow = row;
+    B.ocol = col;
+    B.oval = value;
+    B.levels = R.levels;
+    B.nmat = R.nmat;
+    B.off_B = R.off_B;
+    B.off_T = R.off_T;
+    B.off_P = R.off_P;
+    B.off_C = R.off_C;
+    cudaError_t e = cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(R.smem));
+    if (e != cudaSuccess) return e;
+    const int grid = static_cast<int>(std::max<int64_t>(
+        1, std::min<int64_t>(count, static_cast<int64_t>(num_sms) * 4)));
+    k_refine<<<grid, kRefineThreads, R.smem, stream>>>(B);
+    return cudaGetLastError();
+}
+
+}  // namespace ar

@@ -1,0 +1,132 @@
+/*
+ * autorift_gpu.h -- C ABI of the B200 (sm_100a) dense ZNCC tracker.
+ *
+ * The drop-in boundary for AutoRIFT.jl's correlator. Every entry point takes plain pointers
+ * and sizes, returns an int status (AR_OK = 0), and never retains a caller's host pointer past
+ * return. Images, masks and point-set fields use Julia's layout: matrices are column-major
+ * (rows fastest), masks are one byte per pixel (Matrix{Bool}, not BitMatrix).
+ *
+ * Citations are to the AutoRIFT.jl source the entry point replaces. The reference's only FFI
+ * is its FFTW binding (src/plans.jl:271-312: const library path, ccall, opaque Ptr{Cvoid}
+ * handles, errors raised on the Julia side); these entry points follow the same idiom.
+ */
+#ifndef AUTORIFT_GPU_H
+#define AUTORIFT_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+enum {
+    AR_OK = 0,
+    AR_ERR_ARG = 1,         /* a null pointer or an out-of-range argument */
+    AR_ERR_SIZE = 2,        /* array extents that do not agree (Julia DimensionMismatch) */
+    AR_ERR_OOM = 3,         /* device allocation failed */
+    AR_ERR_TIMEOUT = 4,     /* a bounded wait ran out */
+    AR_ERR_CUDA = 5,        /* a CUDA runtime error; ar_last_error has the text */
+    AR_ERR_UNSUPPORTED = 6  /* a geometry or element type this build does not handle */
+};
+
+/* Element types of an image pair (the T of ImagePair{T}, src/preprocess.jl:41-62). */
+enum { AR_U8 = 0, AR_U16 = 1, AR_F32 = 2, AR_I16 = 3, AR_F64 = 4 };
+
+/* Similarity measures (ZNCC, NCC of src/types.jl:104-140). */
+enum { AR_ZNCC = 0, AR_NCC = 1 };
+
+typedef struct ar_ctx ar_ctx;   /* one device, its streams and scratch */
+typedef struct ar_pair ar_pair; /* a device-resident image pair with its validity mask */
+
+/*
+ * A point set: the eight SoA fields of PointSet{N} (src/points.jl:50-74), flattened in
+ * Julia's memory order (`scatter`, src/points.jl:276-281). Coordinates are 1-based pixel
+ * positions as in Julia. For ar_track the pointers are host memory; for ar_track_device they
+ * are device memory.
+ */
+typedef struct {
+    const double* x;
+    const double* y;
+    const int64_t* radius_x;
+    const int64_t* radius_y;
+    const double* dx_prior;
+    const double* dy_prior;
+    const int64_t* chip_size_x;
+    const int64_t* chip_size_y;
+    int64_t n;
+} ar_points;
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+int ar_version(void);
+
+/* Create a context on `device` (a CUDA ordinal). Replaces the reference's process-wide FFT
+ * plan cache and workspace pools (src/plans.jl:25-47, src/correlate.jl:294-350). */
+int ar_ctx_create(int device, ar_ctx** out);
+int ar_ctx_destroy(ar_ctx* ctx);
+
+/* Copy the last error message of `ctx` (NUL-terminated, truncated to `size`). */
+int ar_last_error(const ar_ctx* ctx, char* buf, size_t size);
+
+/*
+ * Upload an image pair (ImagePair, src/preprocess.jl:74-79). `ref` and `sec` are
+ * nrows x ncols column-major arrays of `dtype`. `ref_valid`/`sec_valid` may be NULL, which
+ * means finiteness for float types and all-valid for integer types, as ImagePair's default.
+ * The pair keeps `valid(pair) = ref_valid .& sec_valid` (src/preprocess.jl:106).
+ */
+int ar_pair_upload(ar_ctx* ctx, const void* ref, const void* sec, const uint8_t* ref_valid,
+                   const uint8_t* sec_valid, int64_t nrows, int64_t ncols, int dtype,
+                   ar_pair** out);
+int ar_pair_destroy(ar_pair* pair);
+
+/* Element type and extents of an uploaded pair. */
+int ar_pair_info(const ar_pair* pair, int* dtype, int64_t* nrows, int64_t* ncols);
+
+/*
+ * track! (src/track.jl:103-152): correlate `pair` at every searchable point of `pts`.
+ * `upsampling` is 1 for NoRefine or a power of two (PyramidRefine, src/types.jl:215-230);
+ * `measure` is AR_ZNCC or AR_NCC. Outputs are host arrays of length pts->n, overwritten in
+ * full: dx, dy, correlation (NaN where there is no measurement) and searched (0/1), the
+ * fields of DisplacementField (src/track.jl:46-62). Host points and outputs are copied in
+ * and out inside the call; the call returns when the results are on the host.
+ */
+int ar_track(ar_ctx* ctx, const ar_pair* pair, const ar_points* pts, int upsampling,
+             int measure, float* dx, float* dy, float* correlation, uint8_t* searched);
+
+/*
+ * As ar_track with device-resident points and outputs, enqueued on `stream` (a
+ * cudaStream_t, or NULL for the context's stream). Returns after the kernels are enqueued;
+ * one small device-to-host read of the pass geometry (src/track.jl:176-197) synchronises.
+ */
+int ar_track_device(ar_ctx* ctx, const ar_pair* pair, const ar_points* pts_dev,
+                    int upsampling, int measure, float* dx_dev, float* dy_dev,
+                    float* correlation_dev, uint8_t* searched_dev, void* stream);
+
+/*
+ * The surface of one chip against one search window (correlate!, src/correlate.jl:528-557),
+ * for host arrays: `search` is (ch+2ry-1) x (cw+2rx-1), `chip` ch x cw, `surface` 2ry x 2rx,
+ * all column-major of `dtype`/float. `degenerate` receives 1 for a constant chip
+ * (src/correlate.jl:571), whose surface is all zeros.
+ */
+int ar_correlate(ar_ctx* ctx, const void* search, const void* chip, int dtype, int64_t ch,
+                 int64_t cw, int64_t rx, int64_t ry, int measure, float* surface,
+                 int* degenerate);
+
+/*
+ * Sub-pixel refinement of `count` 5x5 patches (the cascade of subpixel_peak,
+ * src/peak.jl:456-522, from the patch copy onward): `patches` holds count x 25 floats, each
+ * patch column-major. Outputs are the row and column of the peak in the upsampled
+ * (5*up) x (5*up) patch (0-based) and its value. Host arrays.
+ */
+int ar_refine_patches(ar_ctx* ctx, const float* patches, int64_t count, int upsampling,
+                      int32_t* row, int32_t* col, float* value);
+
+/* Block until all work the context enqueued has finished. */
+int ar_synchronize(ar_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AUTORIFT_GPU_H */

@@ -1,0 +1,485 @@
+// CPU oracle for the dense ZNCC tracker -- TEST INFRASTRUCTURE ONLY.
+//
+// This file restates, in plain C++17, the algorithm of AutoRIFT.jl's hot path so that the
+// CUDA library can be checked against it. It is never linked into the product: only the
+// tests, the smoke check and the CPU-baseline leg of the benchmark load it.
+//
+// Parity pin: the restatement is checked against the reference's own golden vectors
+// (test/fixtures/matchtemplate/zncc_*, test/fixtures/pyrup/*, test/fixtures/peak/*, read from
+// the reference tree when present) and against golden vectors regenerated with OpenCV in
+// tests/golden/make_golden.py.
+//
+// Every function cites the reference file:line it follows. Arrays are column-major (Julia
+// layout: rows fastest), indices are 0-based here and converted where the reference's 1-based
+// arithmetic matters (floor of a shifted coordinate, peak offsets).
+//
+// Floating point: compiled with -ffp-contract=off so that no a*b+c is fused, matching Julia,
+// which never contracts without @fastmath/@muladd. The numerator is an FP64 direct sum -- the
+// exact value the reference's single-precision FFT approximates (src/correlate.jl:785-848).
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+enum Dtype { OR_U8 = 0, OR_U16 = 1, OR_F32 = 2, OR_I16 = 3, OR_F64 = 4 };
+enum Measure { OR_ZNCC = 0, OR_NCC = 1 };
+
+template <class T>
+inline double as_f64(T v) { return static_cast<double>(v); }
+
+// ---------------------------------------------------------------------------------------------
+// src/correlate.jl:423-453 -- prepare_chip!: FP64 mean, Float32 mean-removed copy, FP64 norm,
+// degenerate when the sum of squares is below eps(Float64) * ch * cw.
+// `get(i, j)` returns the chip element at row i, column j (0-based).
+template <class Get>
+bool prepare_chip(Get get, int64_t ch, int64_t cw, float* dst, double* cnorm) {
+    double s = 0.0;
+    for (int64_t j = 0; j < cw; ++j)
+        for (int64_t i = 0; i < ch; ++i) s += get(i, j);
+    const double mean = s / static_cast<double>(ch * cw);
+    double sq = 0.0;
+    for (int64_t j = 0; j < cw; ++j)
+        for (int64_t i = 0; i < ch; ++i) {
+            const double d = get(i, j) - mean;
+            dst[i + j * ch] = static_cast<float>(d);
+            sq += d * d;
+        }
+    *cnorm = std::sqrt(sq);
+    return sq > (DBL_EPSILON * static_cast<double>(ch)) * static_cast<double>(cw);
+}
+
+// src/integral.jl:141-170 -- integral_both!: per-window summed-area tables of x and x^2, one
+// column-major traversal, (m+1) x (n+1) with a zero first row and column.
+template <class Get>
+void integral_both(Get get, int64_t m, int64_t n, double* S, double* S2) {
+    const int64_t ld = m + 1;
+    for (int64_t j = 0; j <= n; ++j) { S[0 + j * ld] = 0.0; S2[0 + j * ld] = 0.0; }
+    for (int64_t i = 0; i <= m; ++i) { S[i] = 0.0; S2[i] = 0.0; }
+    for (int64_t j = 0; j < n; ++j) {
+        double run = 0.0, runsq = 0.0;
+        for (int64_t i = 0; i < m; ++i) {
+            const double v = get(i, j);
+            run += v;
+            runsq += v * v;
+            S[(i + 1) + (j + 1) * ld] = run + S[(i + 1) + j * ld];
+            S2[(i + 1) + (j + 1) * ld] = runsq + S2[(i + 1) + j * ld];
+        }
+    }
+}
+
+// src/integral.jl:244-247 -- boxsum, 0-based top-left (i, j) of an h x w block.
+inline double boxsum(const double* S, int64_t ld, int64_t i, int64_t j, int64_t h, int64_t w) {
+    return ((S[(i + h) + (j + w) * ld] - S[i + (j + w) * ld]) - S[(i + h) + j * ld]) +
+           S[i + j * ld];
+}
+
+// src/correlate.jl:528-557, 575-630 -- correlate! with the ZNCC or NCC normaliser.
+// The numerator is the FP64 direct sum of src/correlate.jl:799-814 (column-major order over
+// the chip); the reference evaluates the same quantity with a single-precision FFT.
+// Returns false (surface all zeros) for a degenerate chip.
+template <class GetW, class GetC>
+bool correlate(GetW getw, GetC getc, int64_t ch, int64_t cw, int64_t rx, int64_t ry, int measure,
+               float* surface, std::vector<float>& chipbuf, std::vector<double>& S,
+               std::vector<double>& S2, std::vector<double>& num) {
+    const int64_t nr = 2 * ry, nc = 2 * rx;
+    const int64_t wr = ch + 2 * ry - 1, wc = cw + 2 * rx - 1;
+    chipbuf.resize(static_cast<size_t>(ch * cw));
+    double cnorm = 0.0;
+    const bool ok = prepare_chip(getc, ch, cw, chipbuf.data(), &cnorm);
+    if (!ok) {
+        std::fill(surface, surface + nr * nc, 0.0f);
+        return false;
+    }
+    S.resize(static_cast<size_t>((wr + 1) * (wc + 1)));
+    S2.resize(S.size());
+    integral_both(getw, wr, wc, S.data(), S2.data());
+
+    // Numerator: each shift accumulates jj-outer, ii-inner exactly as the direct loop; the
+    // shifts themselves are independent, so the innermost loop runs over them.
+    num.assign(static_cast<size_t>(nr * nc), 0.0);
+    std::vector<double> col(static_cast<size_t>(wr));
+    for (int64_t j = 0; j < nc; ++j) {
+        double* acc = num.data() + j * nr;
+        for (int64_t jj = 0; jj < cw; ++jj) {
+            for (int64_t r = 0; r < wr; ++r) col[r] = getw(r, j + jj);
+            for (int64_t ii = 0; ii < ch; ++ii) {
+                const double c = static_cast<double>(chipbuf[ii + jj * ch]);
+                const double* w = col.data() + ii;
+                for (int64_t i = 0; i < nr; ++i) acc[i] += c * w[i];
+            }
+        }
+    }
+
+    const double n = static_cast<double>(ch * cw);
+    const int64_t ld = wr + 1;
+    for (int64_t j = 0; j < nc; ++j)
+        for (int64_t i = 0; i < nr; ++i) {
+            double den;
+            if (measure == OR_NCC) {
+                const double wsq = boxsum(S2.data(), ld, i, j, ch, cw);
+                den = cnorm * std::sqrt(wsq < 0.0 ? 0.0 : wsq);
+            } else {
+                const double s1 = boxsum(S.data(), ld, i, j, ch, cw);
+                const double s2 = boxsum(S2.data(), ld, i, j, ch, cw);
+                double wvar = s2 - s1 * s1 / n;
+                if (!(wvar > 0.0)) wvar = 0.0;
+                den = cnorm * std::sqrt(wvar);
+            }
+            surface[i + j * nr] =
+                den > 0.0 ? static_cast<float>(num[i + j * nr] / den) : 0.0f;
+        }
+    return true;
+}
+
+// src/peak.jl:32-61 -- row-major first strict maximum, NaN never selected, (0,0) by default.
+void peak_index(const float* s, int64_t nr, int64_t nc, int64_t* bi, int64_t* bj) {
+    int64_t best_i = 0, best_j = 0;
+    float best = -INFINITY;
+    for (int64_t j = 0; j < nc; ++j)
+        for (int64_t i = 0; i < nr; ++i) {
+            const float v = s[i + j * nr];
+            if (v > best || (v == best && (i < best_i || (i == best_i && j < best_j)))) {
+                best = v;
+                best_i = i;
+                best_j = j;
+            }
+        }
+    *bi = best_i;
+    *bj = best_j;
+}
+
+// src/peak.jl:374-382 -- reflect101_0.
+inline int64_t reflect101_0(int64_t p, int64_t n) {
+    if (n == 1) return 0;
+    const int64_t m = n - 1;
+    while (p < 0 || p > m) {
+        if (p < 0) p = -p;
+        if (p > m) p = 2 * m - p;
+    }
+    return p;
+}
+
+// src/peak.jl:312-324 -- _pyrup_taps, returned 0-based: (minus, centre, plus, ntaps).
+inline void pyrup_taps(int64_t k0, int64_t n, int64_t* m, int64_t* c, int64_t* q, int* nt) {
+    const int64_t p = k0;  // 0-based upsampled position
+    if (p % 2 == 0) {
+        *c = p / 2;
+        *m = reflect101_0(p - 2, 2 * n) / 2;
+        *q = reflect101_0(p + 2, 2 * n) / 2;
+        *nt = 3;
+    } else {
+        *c = reflect101_0(p - 1, 2 * n) / 2;
+        *m = *c;
+        *q = reflect101_0(p + 1, 2 * n) / 2;
+        *nt = 2;
+    }
+}
+
+// src/peak.jl:297-299 -- the tap weights.
+constexpr float W_C = 6.0f / 8;
+constexpr float W_S = 1.0f / 8;
+constexpr float W_H = 4.0f / 8;
+
+// src/peak.jl:196-294 -- one pyrUp step, vertical then horizontal, Float32 throughout, in the
+// reference's operation order: W_C*b + W_S*(a+c) for a sample position, W_H*(b+c) between.
+void pyrup(const float* src, int64_t sh, int64_t sw, float* dst, std::vector<float>& tmp) {
+    tmp.resize(static_cast<size_t>(2 * sh * sw));
+    const int64_t th = 2 * sh;
+    for (int64_t j = 0; j < sw; ++j)
+        for (int64_t i = 0; i < th; ++i) {
+            int64_t m, c, q;
+            int nt;
+            pyrup_taps(i, sh, &m, &c, &q, &nt);
+            const float* s = src + j * sh;
+            tmp[i + j * th] = nt == 3 ? W_C * s[c] + W_S * (s[m] + s[q]) : W_H * (s[c] + s[q]);
+        }
+    for (int64_t j = 0; j < 2 * sw; ++j) {
+        int64_t m, c, q;
+        int nt;
+        pyrup_taps(j, sw, &m, &c, &q, &nt);
+        for (int64_t i = 0; i < th; ++i) {
+            const float a = tmp[i + m * th], b = tmp[i + c * th], cc = tmp[i + q * th];
+            dst[i + j * th] = nt == 3 ? W_C * b + W_S * (a + cc) : W_H * (b + cc);
+        }
+    }
+}
+
+// src/peak.jl:102-106 -- peak_offset (1-based peak index minus the surface origin).
+void peak_offset(const float* s, int64_t nr, int64_t nc, int64_t rx, int64_t ry, double* dx,
+                 double* dy, float* v) {
+    int64_t i, j;
+    peak_index(s, nr, nc, &i, &j);
+    *dx = static_cast<double>((j + 1) - rx - 1);
+    *dy = static_cast<double>((i + 1) - ry - 1);
+    *v = s[i + j * nr];
+}
+
+// src/peak.jl:456-522 -- subpixel_peak: clamp a 5x5 patch around the integer peak, cascade
+// log2(up) pyrUp steps, row-major argmax, convert back to a displacement.
+void subpixel_peak(const float* s, int64_t nr, int64_t nc, int64_t rx, int64_t ry, int up,
+                   double* dx, double* dy, float* v, std::vector<float>& a,
+                   std::vector<float>& b, std::vector<float>& tmp) {
+    if (up == 1) { peak_offset(s, nr, nc, rx, ry, dx, dy, v); return; }
+    const int64_t p = 5;
+    int64_t pi, pj;
+    peak_index(s, nr, nc, &pi, &pj);
+    // 1-based clamp(pi - half, 1, max(nr - p + 1, 1)), here on 0-based indices.
+    const int64_t half = p / 2;
+    const int64_t i0 = std::clamp<int64_t>(pi - half, 0, std::max<int64_t>(nr - p, 0));
+    const int64_t j0 = std::clamp<int64_t>(pj - half, 0, std::max<int64_t>(nc - p, 0));
+    if (nr < p || nc < p) { peak_offset(s, nr, nc, rx, ry, dx, dy, v); return; }
+    a.resize(static_cast<size_t>(p * up * p * up));
+    b.resize(a.size());
+    std::vector<float> patch(static_cast<size_t>(p * p));
+    for (int64_t j = 0; j < p; ++j)
+        for (int64_t i = 0; i < p; ++i) patch[i + j * p] = s[(i0 + i) + (j0 + j) * nr];
+    int64_t n = p;
+    int factor = 1;
+    const float* cur = patch.data();
+    bool use_a = true;
+    while (factor < up) {
+        float* dst = use_a ? a.data() : b.data();
+        pyrup(cur, n, n, dst, tmp);
+        n *= 2;
+        factor *= 2;
+        cur = dst;
+        use_a = !use_a;
+    }
+    int64_t si, sj;
+    peak_index(cur, n, n, &si, &sj);
+    *v = cur[si + sj * n];
+    const double row = static_cast<double>(si) / factor + static_cast<double>(i0);
+    const double col = static_cast<double>(sj) / factor + static_cast<double>(j0);
+    *dx = col - static_cast<double>(rx);
+    *dy = row - static_cast<double>(ry);
+}
+
+// ---------------------------------------------------------------------------------------------
+// The grid loop: src/track.jl:103-152 (pass set-up), 176-220 (geometry, +0.5 shift, padding),
+// 249-305 (per point), src/points.jl:358-395 (chip and window bounds), 116-117, 421-425.
+
+struct Points {
+    const double *x, *y, *dx0, *dy0;
+    const int64_t *rx, *ry, *csx, *csy;
+    int64_t n;
+};
+
+inline int64_t floor_i(double v) { return static_cast<int64_t>(std::floor(v)); }
+
+// Julia's `÷` on Int truncates toward zero.
+inline int64_t jdiv(int64_t a, int64_t b) { return a / b; }
+
+template <class T>
+int track_impl(const T* ref, const T* sec, const uint8_t* refv, const uint8_t* secv,
+               int64_t nrows, int64_t ncols, Points pts, int up, int measure, float* odx,
+               float* ody, float* ocorr, uint8_t* osearched, int nthreads) {
+    const int64_t n = pts.n;
+    for (int64_t k = 0; k < n; ++k) {
+        odx[k] = NAN;
+        ody[k] = NAN;
+        ocorr[k] = NAN;
+        osearched[k] = 0;
+    }
+    // _pass_geometry (src/track.jl:176-197), on the unshifted points.
+    int64_t cx = 0, cy = 0, mrx = 0, mry = 0, px = 0, py = 0;
+    bool fits = true;
+    for (int64_t k = 0; k < n; ++k) {
+        if (!(pts.rx[k] > 0 && pts.ry[k] > 0)) continue;
+        cx = std::max(cx, pts.csx[k]);
+        cy = std::max(cy, pts.csy[k]);
+        mrx = std::max(mrx, pts.rx[k]);
+        mry = std::max(mry, pts.ry[k]);
+        px = std::max(px, jdiv(pts.csx[k], 2) + pts.rx[k] +
+                              static_cast<int64_t>(std::ceil(std::fabs(pts.dx0[k]))));
+        py = std::max(py, jdiv(pts.csy[k], 2) + pts.ry[k] +
+                              static_cast<int64_t>(std::ceil(std::fabs(pts.dy0[k]))));
+        // inbounds (src/points.jl:421-425) with search_bounds on the unshifted point.
+        const int64_t hx = jdiv(pts.csx[k], 2), hy = jdiv(pts.csy[k], 2);
+        const int64_t wcx = floor_i(pts.x[k]), wcy = floor_i(pts.y[k]);
+        const bool inb = (wcy - hy - pts.ry[k]) >= 1 && (wcy + hy + pts.ry[k] - 2) <= nrows &&
+                         (wcx - hx - pts.rx[k]) >= 1 && (wcx + hx + pts.rx[k] - 2) <= ncols;
+        fits = fits && inb;
+    }
+    if (cx == 0) return 0;
+    const int64_t padx = fits ? 0 : px + 2, pady = fits ? 0 : py + 2;
+    const int64_t NR = nrows + 2 * pady, NC = ncols + 2 * padx;  // padded extent
+    const double shx = static_cast<double>(padx) + 0.5, shy = static_cast<double>(pady) + 0.5;
+
+    // Padded-image readers (1-based padded coordinates): zero / false outside the image.
+    auto pix = [&](const T* img, int64_t r1, int64_t c1) -> double {
+        const int64_t r = r1 - 1 - pady, c = c1 - 1 - padx;
+        if (r < 0 || r >= nrows || c < 0 || c >= ncols) return 0.0;
+        return as_f64(img[r + c * nrows]);
+    };
+    auto okpix = [&](int64_t r1, int64_t c1) -> bool {
+        const int64_t r = r1 - 1 - pady, c = c1 - 1 - padx;
+        if (r < 0 || r >= nrows || c < 0 || c >= ncols) return false;
+        return refv[r + c * nrows] != 0 && secv[r + c * nrows] != 0;
+    };
+
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel
+#endif
+    {
+        std::vector<float> surface, chipbuf, ba, bb, tmp;
+        std::vector<double> S, S2, num;
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 4)
+#endif
+        for (int64_t k = 0; k < n; ++k) {
+            const int64_t prx = pts.rx[k], pry = pts.ry[k];
+            if (!(prx > 0 && pry > 0)) continue;
+            const double xs = pts.x[k] + shx, ys = pts.y[k] + shy;
+            const int64_t hx = jdiv(pts.csx[k], 2), hy = jdiv(pts.csy[k], 2);
+            // chip_bounds (src/points.jl:358-366)
+            const int64_t ccx = floor_i(xs - pts.dx0[k]), ccy = floor_i(ys - pts.dy0[k]);
+            const int64_t cr0 = ccy - hy, cr1 = ccy + hy - 1, cc0 = ccx - hx, cc1 = ccx + hx - 1;
+            // search_bounds (src/points.jl:385-395)
+            const int64_t wcx = floor_i(xs), wcy = floor_i(ys);
+            const int64_t wr0 = wcy - hy - pry, wr1 = wcy + hy + pry - 2;
+            const int64_t wc0 = wcx - hx - prx, wc1 = wcx + hx + prx - 2;
+            auto inb = [&](int64_t r0, int64_t r1, int64_t c0, int64_t c1) {
+                if (r1 < r0 || c1 < c0) return true;  // empty range: checkbounds is true
+                return r0 >= 1 && r1 <= NR && c0 >= 1 && c1 <= NC;
+            };
+            if (!inb(cr0, cr1, cc0, cc1)) continue;
+            if (!inb(wr0, wr1, wc0, wc1)) continue;
+            // _any_valid (src/track.jl:416-421)
+            bool any = false;
+            for (int64_t c = cc0; c <= cc1 && !any; ++c)
+                for (int64_t r = cr0; r <= cr1; ++r)
+                    if (okpix(r, c)) { any = true; break; }
+            if (!any) continue;
+            osearched[k] = 1;
+            const int64_t ch = 2 * hy, cw = 2 * hx;
+            auto getc = [&](int64_t i, int64_t j) { return pix(sec, cr0 + i, cc0 + j); };
+            auto getw = [&](int64_t i, int64_t j) { return pix(ref, wr0 + i, wc0 + j); };
+            const int64_t nr = 2 * pry, nc = 2 * prx;
+            surface.resize(static_cast<size_t>(nr * nc));
+            if (!correlate(getw, getc, ch, cw, prx, pry, measure, surface.data(), chipbuf, S, S2,
+                           num))
+                continue;  // degenerate: searched, no measurement
+            double dx, dy;
+            float c;
+            subpixel_peak(surface.data(), nr, nc, prx, pry, up, &dx, &dy, &c, ba, bb, tmp);
+            odx[k] = static_cast<float>(dx + pts.dx0[k]);
+            ody[k] = static_cast<float>(dy + pts.dy0[k]);
+            ocorr[k] = c;
+        }
+    }
+    return 0;
+}
+
+template <class T>
+bool correlate_arrays(const T* search, const T* chip, int64_t ch, int64_t cw, int64_t rx,
+                      int64_t ry, int measure, float* surface) {
+    const int64_t wr = ch + 2 * ry - 1;
+    std::vector<float> chipbuf;
+    std::vector<double> S, S2, num;
+    auto getc = [&](int64_t i, int64_t j) { return as_f64(chip[i + j * ch]); };
+    auto getw = [&](int64_t i, int64_t j) { return as_f64(search[i + j * wr]); };
+    return correlate(getw, getc, ch, cw, rx, ry, measure, surface, chipbuf, S, S2, num);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Surface of one chip against one search window (src/correlate.jl:528-557).
+// search: (ch+2ry-1) x (cw+2rx-1), chip: ch x cw, surface: 2ry x 2rx, all column-major.
+// Returns 1 when the chip is degenerate (surface zero-filled), 0 otherwise, <0 on bad dtype.
+int or_correlate(const void* search, const void* chip, int dtype, int64_t ch, int64_t cw,
+                 int64_t rx, int64_t ry, int measure, float* surface) {
+    bool ok;
+    switch (dtype) {
+        case OR_U8: ok = correlate_arrays(static_cast<const uint8_t*>(search),
+                                          static_cast<const uint8_t*>(chip), ch, cw, rx, ry,
+                                          measure, surface); break;
+        case OR_U16: ok = correlate_arrays(static_cast<const uint16_t*>(search),
+                                           static_cast<const uint16_t*>(chip), ch, cw, rx, ry,
+                                           measure, surface); break;
+        case OR_F32: ok = correlate_arrays(static_cast<const float*>(search),
+                                           static_cast<const float*>(chip), ch, cw, rx, ry,
+                                           measure, surface); break;
+        case OR_I16: ok = correlate_arrays(static_cast<const int16_t*>(search),
+                                           static_cast<const int16_t*>(chip), ch, cw, rx, ry,
+                                           measure, surface); break;
+        case OR_F64: ok = correlate_arrays(static_cast<const double*>(search),
+                                           static_cast<const double*>(chip), ch, cw, rx, ry,
+                                           measure, surface); break;
+        default: return -1;
+    }
+    return ok ? 0 : 1;
+}
+
+// src/peak.jl:32-61, returned 0-based.
+void or_peak_index(const float* surface, int64_t nr, int64_t nc, int64_t* i, int64_t* j) {
+    peak_index(surface, nr, nc, i, j);
+}
+
+// src/peak.jl:196-294: dst is (2sh) x (2sw).
+void or_pyrup(const float* src, int64_t sh, int64_t sw, float* dst) {
+    std::vector<float> tmp;
+    pyrup(src, sh, sw, dst, tmp);
+}
+
+// src/peak.jl:456-522.
+void or_subpixel_peak(const float* surface, int64_t nr, int64_t nc, int64_t rx, int64_t ry,
+                      int up, double* dx, double* dy, float* v) {
+    std::vector<float> a, b, tmp;
+    subpixel_peak(surface, nr, nc, rx, ry, up, dx, dy, v, a, b, tmp);
+}
+
+// track! over a point set (src/track.jl:103-152). Images and masks are nrows x ncols
+// column-major; points are 8 SoA arrays of length n; outputs are prefilled by this call.
+// up = 1 is NoRefine, otherwise PyramidRefine(up). nthreads <= 0 uses the OpenMP default.
+int or_track(const void* ref, const void* sec, const uint8_t* refv, const uint8_t* secv,
+             int64_t nrows, int64_t ncols, int dtype, const double* x, const double* y,
+             const int64_t* rx, const int64_t* ry, const double* dx0, const double* dy0,
+             const int64_t* csx, const int64_t* csy, int64_t n, int up, int measure,
+             float* dx, float* dy, float* corr, uint8_t* searched, int nthreads) {
+    Points p{x, y, dx0, dy0, rx, ry, csx, csy, n};
+    switch (dtype) {
+        case OR_U8:
+            return track_impl(static_cast<const uint8_t*>(ref), static_cast<const uint8_t*>(sec),
+                              refv, secv, nrows, ncols, p, up, measure, dx, dy, corr, searched,
+                              nthreads);
+        case OR_U16:
+            return track_impl(static_cast<const uint16_t*>(ref),
+                              static_cast<const uint16_t*>(sec), refv, secv, nrows, ncols, p, up,
+                              measure, dx, dy, corr, searched, nthreads);
+        case OR_F32:
+            return track_impl(static_cast<const float*>(ref), static_cast<const float*>(sec),
+                              refv, secv, nrows, ncols, p, up, measure, dx, dy, corr, searched,
+                              nthreads);
+        case OR_I16:
+            return track_impl(static_cast<const int16_t*>(ref), static_cast<const int16_t*>(sec),
+                              refv, secv, nrows, ncols, p, up, measure, dx, dy, corr, searched,
+                              nthreads);
+        case OR_F64:
+            return track_impl(static_cast<const double*>(ref), static_cast<const double*>(sec),
+                              refv, secv, nrows, ncols, p, up, measure, dx, dy, corr, searched,
+                              nthreads);
+        default: return -1;
+    }
+}
+
+int or_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+}  // extern "C"
