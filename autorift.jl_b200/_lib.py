@@ -24,6 +24,17 @@ _i64 = ctypes.c_int64
 _sz = ctypes.c_size_t
 
 
+class ArPrepareOpts(ctypes.Structure):
+    """`ar_prepare_opts`: preprocess method and width, Wallis floor, quantisation."""
+
+    _fields_ = [("preprocess", _i32), ("width", _i32), ("min_std", ctypes.c_double),
+                ("quantize", _i32)]
+
+
+AR_PRE_NONE, AR_PRE_HIGHPASS, AR_PRE_WALLIS = 0, 1, 2
+AR_QUANT_NONE, AR_QUANT_UINT8 = 0, 1
+
+
 class ArPoints(ctypes.Structure):
     """`ar_points`: the eight PointSet fields (src/points.jl:50-74) plus the count."""
 
@@ -39,12 +50,17 @@ SIGNATURES = {
     "ar_last_error": (_i32, [_p, ctypes.c_char_p, _sz]),
     "ar_pair_upload": (_i32, [_p, _p, _p, _p, _p, _i64, _i64, _i32, ctypes.POINTER(_p)]),
     "ar_pair_destroy": (_i32, [_p]),
+    "ar_prepare": (_i32, [_p, _p, ctypes.POINTER(ArPrepareOpts), ctypes.POINTER(_p)]),
+    "ar_pair_download": (_i32, [_p, _p, _p, _p, _p, _p]),
     "ar_pair_info": (_i32, [_p, ctypes.POINTER(_i32), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "ar_track": (_i32, [_p, _p, ctypes.POINTER(ArPoints), _i32, _i32, _p, _p, _p, _p]),
     "ar_track_device": (_i32, [_p, _p, ctypes.POINTER(ArPoints), _i32, _i32, _p, _p, _p, _p, _p]),
     "ar_correlate": (_i32, [_p, _p, _p, _i32, _i64, _i64, _i64, _i64, _i32, _p,
                             ctypes.POINTER(_i32)]),
     "ar_refine_patches": (_i32, [_p, _p, _i64, _i32, _p, _p, _p]),
+    "ar_ctx_set_timing": (_i32, [_p, _i32]),
+    "ar_kernel_times": (_i32, [_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                               ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "ar_synchronize": (_i32, [_p]),
 }
 
@@ -96,6 +112,17 @@ class Context:
             buf = ctypes.create_string_buffer(512)
             self.lib.ar_last_error(self.handle, buf, 512)
             raise ArError(rc, buf.value.decode(errors="replace"))
+
+    def set_timing(self, enable: bool):
+        self.check(self.lib.ar_ctx_set_timing(self.handle, int(bool(enable))))
+
+    def kernel_times(self):
+        """(corr_ms, refine_ms, track_launches, kernel_launches) since the last call."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        t, n = _i64(), _i64()
+        self.check(self.lib.ar_kernel_times(self.handle, ctypes.byref(a), ctypes.byref(b),
+                                            ctypes.byref(t), ctypes.byref(n)))
+        return a.value, b.value, t.value, n.value
 
     def close(self):
         if getattr(self, "handle", None):

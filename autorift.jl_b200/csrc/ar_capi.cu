@@ -36,6 +36,8 @@ struct ar_pair {
     int64_t nrows = 0, ncols = 0;
     void* ref = nullptr;
     void* sec = nullptr;
+    uint8_t* ref_valid = nullptr;
+    uint8_t* sec_valid = nullptr;
     uint8_t* valid = nullptr;  // ref_valid .& sec_valid
 };
 
@@ -168,23 +170,32 @@ cudaError_t ensure_dbuf(ar_ctx* c, size_t bytes) {
     return cudaSuccess;
 }
 
+// Per-image masks (given ones normalised to 0/1, missing ones from finiteness, the ImagePair
+// default of src/preprocess.jl:74-79) and their intersection, valid(pair).
 template <typename T>
-__global__ void k_make_valid(const T* ref, const T* sec, const uint8_t* rv, const uint8_t* sv,
-                             uint8_t* out, int64_t n) {
+__global__ void k_make_valid(const T* ref, const T* sec, uint8_t* rv, uint8_t* sv, bool have_rv,
+                             bool have_sv, uint8_t* out, int64_t n) {
     const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
-    bool a, b;
-    if (rv) a = rv[i] != 0; else a = isfinite(static_cast<double>(ref[i]));
-    if (sv) b = sv[i] != 0; else b = isfinite(static_cast<double>(sec[i]));
+    const bool a = have_rv ? rv[i] != 0 : isfinite(static_cast<double>(ref[i]));
+    const bool b = have_sv ? sv[i] != 0 : isfinite(static_cast<double>(sec[i]));
+    rv[i] = a ? 1 : 0;
+    sv[i] = b ? 1 : 0;
     out[i] = (a && b) ? 1 : 0;
 }
 
+__global__ void k_and_masks(const uint8_t* a, const uint8_t* b, uint8_t* out, int64_t n) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i < n) out[i] = (a[i] && b[i]) ? 1 : 0;
+}
+
 template <typename T>
-cudaError_t launch_make_valid(const void* ref, const void* sec, const uint8_t* rv,
-                              const uint8_t* sv, uint8_t* out, int64_t n, cudaStream_t s) {
+cudaError_t launch_make_valid(ar_pair* p, bool have_rv, bool have_sv, cudaStream_t s) {
     const int threads = 256;
+    const int64_t n = p->nrows * p->ncols;
     k_make_valid<T><<<static_cast<unsigned>((n + threads - 1) / threads), threads, 0, s>>>(
-        static_cast<const T*>(ref), static_cast<const T*>(sec), rv, sv, out, n);
+        static_cast<const T*>(p->ref), static_cast<const T*>(p->sec), p->ref_valid, p->sec_valid,
+        have_rv, have_sv, p->valid, n);
     return cudaGetLastError();
 }
 
@@ -226,6 +237,9 @@ int ar_ctx_destroy(ar_ctx* c) {
         cudaFree(c->scratch.sub_origin);
         cudaFree(c->scratch.sub_patch);
         cudaFree(c->scratch.geom);
+        for (auto& r : c->scratch.timer.recs)
+            for (auto ev : r) c->scratch.timer.pool.push_back(ev);
+        for (auto ev : c->scratch.timer.pool) cudaEventDestroy(ev);
         cudaFree(c->dbuf);
         if (c->pinned) cudaFreeHost(c->pinned);
         for (auto& ev : c->staged)
@@ -262,25 +276,24 @@ int ar_pair_upload(ar_ctx* c, const void* ref, const void* sec, const uint8_t* r
     p->ncols = ncols;
     cudaError_t e = cudaMalloc(&p->ref, n * es);
     if (e == cudaSuccess) e = cudaMalloc(&p->sec, n * es);
-    if (e == cudaSuccess) e = cudaMalloc(&p->valid, n);
-    uint8_t* dmask = nullptr;
-    if (e == cudaSuccess && (ref_valid || sec_valid)) e = cudaMalloc(&dmask, 2 * n);
+    if (e == cudaSuccess) e = cudaMalloc(&p->valid, 3 * n);
+    if (e == cudaSuccess) {
+        p->ref_valid = p->valid + n;
+        p->sec_valid = p->valid + 2 * n;
+    }
     if (e == cudaSuccess) e = stage_h2d(c, p->ref, ref, n * es);
     if (e == cudaSuccess) e = stage_h2d(c, p->sec, sec, n * es);
-    if (e == cudaSuccess && ref_valid) e = stage_h2d(c, dmask, ref_valid, n);
-    if (e == cudaSuccess && sec_valid) e = stage_h2d(c, dmask + n, sec_valid, n);
+    if (e == cudaSuccess && ref_valid) e = stage_h2d(c, p->ref_valid, ref_valid, n);
+    if (e == cudaSuccess && sec_valid) e = stage_h2d(c, p->sec_valid, sec_valid, n);
     if (e == cudaSuccess) {
-        const uint8_t* rv = ref_valid ? dmask : nullptr;
-        const uint8_t* sv = sec_valid ? dmask + n : nullptr;
         switch (dtype) {
-            case AR_U8: e = launch_make_valid<uint8_t>(p->ref, p->sec, rv, sv, p->valid, n, c->stream); break;
-            case AR_U16: e = launch_make_valid<uint16_t>(p->ref, p->sec, rv, sv, p->valid, n, c->stream); break;
-            case AR_I16: e = launch_make_valid<int16_t>(p->ref, p->sec, rv, sv, p->valid, n, c->stream); break;
-            case AR_F32: e = launch_make_valid<float>(p->ref, p->sec, rv, sv, p->valid, n, c->stream); break;
+            case AR_U8: e = launch_make_valid<uint8_t>(p, ref_valid != nullptr, sec_valid != nullptr, c->stream); break;
+            case AR_U16: e = launch_make_valid<uint16_t>(p, ref_valid != nullptr, sec_valid != nullptr, c->stream); break;
+            case AR_I16: e = launch_make_valid<int16_t>(p, ref_valid != nullptr, sec_valid != nullptr, c->stream); break;
+            case AR_F32: e = launch_make_valid<float>(p, ref_valid != nullptr, sec_valid != nullptr, c->stream); break;
         }
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    cudaFree(dmask);
     if (e != cudaSuccess) {
         cudaFree(p->ref);
         cudaFree(p->sec);
@@ -498,6 +511,133 @@ int ar_refine_patches(ar_ctx* c, const float* patches, int64_t count, int up, in
     if (e == cudaSuccess) e = stage_d2h(c, value, dval, count * 4);
     if (e != cudaSuccess) return cuda_fail(c, e, "ar_refine_patches");
     return AR_OK;
+}
+
+int ar_prepare(ar_ctx* c, const ar_pair* raw, const ar_prepare_opts* opts, ar_pair** out) {
+    if (!c || !raw || !opts || !out) return fail(c, AR_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (raw->ctx != c) return fail(c, AR_ERR_ARG, "the pair belongs to another context");
+    if (opts->preprocess < AR_PRE_NONE || opts->preprocess > AR_PRE_WALLIS)
+        return fail(c, AR_ERR_ARG, "unknown preprocess method");
+    if (opts->quantize != AR_QUANT_NONE && opts->quantize != AR_QUANT_UINT8)
+        return fail(c, AR_ERR_ARG, "unknown quantize method");
+    if (opts->preprocess != AR_PRE_NONE) {
+        if (opts->width < 3 || (opts->width & 1) == 0)
+            return fail(c, AR_ERR_ARG, "filter `width` must be odd and >= 3");
+        if (opts->width > ar::max_filter_width())
+            return fail(c, AR_ERR_UNSUPPORTED, "filter `width` above the supported maximum");
+        if (opts->preprocess == AR_PRE_WALLIS && !(opts->min_std >= 0.0))
+            return fail(c, AR_ERR_ARG, "`min_std` must be >= 0");
+    }
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    const int64_t n = raw->nrows * raw->ncols;
+    const int odt = opts->quantize == AR_QUANT_UINT8 ? AR_U8
+                    : (opts->preprocess != AR_PRE_NONE ? AR_F32 : raw->dtype);
+    const size_t oes = elem_size(odt);
+    ar_pair* p = new ar_pair();
+    p->ctx = c;
+    p->dtype = odt;
+    p->nrows = raw->nrows;
+    p->ncols = raw->ncols;
+    cudaError_t e = cudaMalloc(&p->ref, n * oes);
+    if (e == cudaSuccess) e = cudaMalloc(&p->sec, n * oes);
+    if (e == cudaSuccess) e = cudaMalloc(&p->valid, 3 * n);
+    if (e == cudaSuccess) {
+        p->ref_valid = p->valid + n;
+        p->sec_valid = p->valid + 2 * n;
+    }
+    const bool need_f = opts->preprocess != AR_PRE_NONE && opts->quantize == AR_QUANT_UINT8;
+    const bool need_m = opts->preprocess == AR_PRE_WALLIS;
+    const size_t scratch = (need_f ? n * 4 : 0) + (need_m ? n * 4 : 0) + ar::quant_stats_bytes() + 256;
+    unsigned char* tmp = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&tmp, scratch);
+    for (int side = 0; side < 2 && e == cudaSuccess; ++side) {
+        ar::PrepareJob J{};
+        J.dtype = raw->dtype;
+        J.img = side == 0 ? raw->ref : raw->sec;
+        J.mask = side == 0 ? raw->ref_valid : raw->sec_valid;
+        J.nrows = raw->nrows;
+        J.ncols = raw->ncols;
+        J.preprocess = opts->preprocess;
+        J.width = opts->width;
+        J.min_std = opts->min_std;
+        J.quantize = opts->quantize;
+        J.out = side == 0 ? p->ref : p->sec;
+        J.vout = side == 0 ? p->ref_valid : p->sec_valid;
+        size_t off = 0;
+        J.ftmp = need_f ? reinterpret_cast<float*>(tmp + off) : nullptr;
+        off += need_f ? n * 4 : 0;
+        J.mtmp = need_m ? reinterpret_cast<float*>(tmp + off) : nullptr;
+        off += need_m ? n * 4 : 0;
+        J.stats = reinterpret_cast<ar::QuantStats*>(tmp + ((off + 255) & ~size_t(255)));
+        e = ar::launch_prepare(J, c->stream, &c->scratch.timer.launches);
+    }
+    if (e == cudaSuccess) {
+        const int threads = 256;
+        k_and_masks<<<static_cast<unsigned>((n + threads - 1) / threads), threads, 0, c->stream>>>(
+            p->ref_valid, p->sec_valid, p->valid, n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(tmp);
+    if (e != cudaSuccess) {
+        cudaFree(p->ref);
+        cudaFree(p->sec);
+        cudaFree(p->valid);
+        delete p;
+        return cuda_fail(c, e, "ar_prepare");
+    }
+    *out = p;
+    return AR_OK;
+}
+
+int ar_pair_download(ar_ctx* c, const ar_pair* p, void* ref, void* sec, uint8_t* ref_valid,
+                     uint8_t* sec_valid) {
+    if (!c || !p) return fail(c, AR_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    const int64_t n = p->nrows * p->ncols;
+    const size_t es = elem_size(p->dtype);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess && ref) e = stage_d2h(c, ref, p->ref, n * es);
+    if (e == cudaSuccess && sec) e = stage_d2h(c, sec, p->sec, n * es);
+    if (e == cudaSuccess && ref_valid) e = stage_d2h(c, ref_valid, p->ref_valid, n);
+    if (e == cudaSuccess && sec_valid) e = stage_d2h(c, sec_valid, p->sec_valid, n);
+    return e == cudaSuccess ? AR_OK : cuda_fail(c, e, "ar_pair_download");
+}
+
+int ar_ctx_set_timing(ar_ctx* c, int enable) {
+    if (!c) return AR_ERR_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->scratch.timer.enabled = enable != 0;
+    return AR_OK;
+}
+
+int ar_kernel_times(ar_ctx* c, double* corr_ms, double* refine_ms, int64_t* tracks,
+                    int64_t* launches) {
+    if (!c) return AR_ERR_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    ar::KernelTimer& T = c->scratch.timer;
+    double sc = 0.0, sr = 0.0;
+    cudaError_t e = cudaSuccess;
+    for (auto& r : T.recs) {
+        float a = 0.0f, b = 0.0f;
+        if (e == cudaSuccess) e = cudaEventSynchronize(r[2]);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&a, r[0], r[1]);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&b, r[1], r[2]);
+        sc += a;
+        sr += b;
+        for (auto ev : r) T.pool.push_back(ev);
+    }
+    if (tracks) *tracks = static_cast<int64_t>(T.recs.size());
+    if (launches) *launches = T.launches;
+    T.recs.clear();
+    T.launches = 0;
+    if (corr_ms) *corr_ms = sc;
+    if (refine_ms) *refine_ms = sr;
+    return e == cudaSuccess ? AR_OK : cuda_fail(c, e, "ar_kernel_times");
 }
 
 int ar_synchronize(ar_ctx* c) {

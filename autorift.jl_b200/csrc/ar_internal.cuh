@@ -3,8 +3,10 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "autorift_gpu.h"
 
@@ -39,6 +41,16 @@ struct DevOutputs {
 };
 
 // Scratch the track launch needs, owned by the context and grown on demand.
+// Optional per-kernel timing: events recorded on the launch stream around the correlation and
+// refinement kernels of each track launch, summed when queried. Off unless enabled.
+struct KernelTimer {
+    bool enabled = false;
+    std::vector<std::array<cudaEvent_t, 3>> recs;  // before corr, after corr, after refine
+    std::vector<cudaEvent_t> pool;
+    long long launches = 0;  // kernels this library launched since the last query
+    cudaEvent_t get();
+};
+
 struct TrackScratch {
     int* sub_count = nullptr;       // number of points queued for sub-pixel refinement
     int64_t* sub_point = nullptr;   // point index per queued item
@@ -46,6 +58,7 @@ struct TrackScratch {
     float* sub_patch = nullptr;     // 25 floats per item, column-major
     int64_t capacity = 0;
     int64_t* geom = nullptr;        // device-side pass geometry (8 int64)
+    KernelTimer timer;
 };
 
 // Host-side pass geometry of a host point set.
@@ -63,6 +76,30 @@ cudaError_t launch_track(int dtype, const void* ref, const void* sec, const uint
 // Device-side pass geometry for a device point set (one small synchronising read).
 cudaError_t pass_geometry_device(const DevPoints& pts, int64_t nrows, int64_t ncols,
                                  TrackScratch& scratch, cudaStream_t stream, PassGeometry* out);
+
+// One image through preprocess then quantize (src/api.jl:305-306) on the device.
+// preprocess: 0 none, 1 highpass, 2 Wallis; quantize: 0 none, 1 uint8. `out` holds
+// nrows*ncols elements of the output type (uint8 for quantize 1, float32 when a filter ran,
+// else the input type); `ftmp` and `mtmp` are float scratch of the same length (ftmp used when
+// a filter feeds the quantiser, mtmp by Wallis); `stats` is quant_stats_bytes() of scratch.
+struct QuantStats;
+struct PrepareJob {
+    int dtype;
+    const void* img;
+    const uint8_t* mask;
+    int64_t nrows, ncols;
+    int preprocess, width;
+    double min_std;
+    int quantize;
+    void* out;
+    uint8_t* vout;
+    float* ftmp;
+    float* mtmp;
+    QuantStats* stats;
+};
+size_t quant_stats_bytes();
+int max_filter_width();
+cudaError_t launch_prepare(const PrepareJob& job, cudaStream_t stream, long long* launches);
 
 // Refine `count` patches already on the device.
 cudaError_t launch_refine_patches(const float* patches, int64_t count, int up, int32_t* row,

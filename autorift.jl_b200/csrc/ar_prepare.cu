@@ -1,0 +1,458 @@
+// Pre-correlation filters and UInt8 quantisation on the device: the `_prepare` step of
+// AutoRIFT.jl (src/api.jl:305-311) -- preprocess (src/preprocess.jl:149-160, 275-460) then
+// quantize (src/preprocess.jl:488-592) -- applied to one image at a time.
+//
+// Stencils. The mask-aware box mean (src/preprocess.jl:371-399 over src/window.jl:228-439)
+// is a shared-memory tile: per-pixel values and "contributes" flags (valid and not NaN) for a
+// 32x32 output tile plus its halo, FP64 column sums, then FP64 row sums, divided by the count
+// and rounded to Float32. For integer images and for Float32 images of bounded dynamic range
+// every partial sum is an exact FP64 value, so the mean equals the reference's banded running
+// sum bit for bit. Erosion of the validity mask (src/preprocess.jl:447-460) is the same
+// stencil over the mask, and the highpass / Wallis output, the non-finite clean-up and the
+// mask update of `_filtered` (src/preprocess.jl:275-288) are fused into the final pass.
+//
+// Quantisation. The global mean and Bessel-corrected deviation of `_to_uint8` are reduced in
+// double-double (TwoSum) with a fixed block order -- deterministic, and within an ulp of the
+// exactly rounded sums, which for highpass output of integer imagery equal the reference's
+// sequential FP64 sums exactly. Rounding half to even, as Julia's round(UInt8, x).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+
+#include "ar_internal.cuh"
+
+namespace ar {
+namespace {
+
+constexpr int kTile = 32;
+constexpr int kBoxThreads = 256;
+constexpr int kMaxWidth = 63;
+constexpr int kStatBlocks = 592;
+constexpr int kStatThreads = 256;
+constexpr unsigned kFullMask = 0xffffffffu;
+
+template <typename T>
+__device__ __forceinline__ float as_f32(T v) {
+    return static_cast<float>(v);
+}
+
+// Which per-pixel quantity a box pass averages.
+enum BoxMode { BOX_IMAGE = 0, BOX_DEV2 = 1 };
+
+// Shared-memory layout of one tile with its halo: values, flags, column sums. The window is
+// (wx, wy) after the reference's clamp to the image (src/window.jl:632-637), with the extra
+// element of an even width on the left (src/window.jl:254-257).
+struct BoxSmem {
+    float* val;       // Rr x Rc, Rr = kTile + wy - 1, Rc = kTile + wx - 1, column-major
+    uint8_t* contr;   // contributes to the mean
+    uint8_t* mok;     // mask for erosion (true outside the image)
+    double* vs;       // kTile x Rc column sums
+    int* vc;          // kTile x Rc counts
+    uint8_t* ve;      // kTile x Rc eroded columns
+};
+
+// The Wallis deviation of one pixel (src/preprocess.jl:416-430).
+__device__ __forceinline__ float dev2_of(float x, bool m, float mean, bool* contributes) {
+    if (m && isfinite(mean)) {
+        const float d = __fsub_rn(x, mean);
+        const float v = __fmul_rn(d, d);
+        *contributes = !isnan(v);
+        return v;
+    }
+    *contributes = false;
+    return 0.0f;
+}
+
+// Tile loop of a box pass: for every output pixel of the tile, the FP64 sum and count of
+// contributing neighbours and whether every in-bounds neighbour is valid.
+template <typename T, int MODE, typename Out>
+__device__ void box_tile(const T* img, const uint8_t* mask, const float* mean, int64_t nr,
+                         int64_t nc, int wx, int wy, int64_t r0, int64_t c0, BoxSmem S, Out out) {
+    const int ly = wy / 2, lx = wx / 2;
+    const int Rr = kTile + wy - 1, Rc = kTile + wx - 1;
+    const int tid = threadIdx.x, bd = blockDim.x;
+    for (int e = tid; e < Rr * Rc; e += bd) {
+        const int r = e % Rr, c = e / Rr;
+        const int64_t gr = r0 - ly + r, gc = c0 - lx + c;
+        float v = 0.0f;
+        uint8_t contrib = 0, mk = 1;
+        if (gr >= 0 && gr < nr && gc >= 0 && gc < nc) {
+            const int64_t g = gr + gc * nr;
+            const bool m = mask[g] != 0;
+            mk = m ? 1 : 0;
+            const float x = as_f32(img[g]);
+            if (MODE == BOX_IMAGE) {
+                v = x;
+                contrib = (m && !isnan(x)) ? 1 : 0;
+            } else {
+                bool cb;
+                v = dev2_of(x, m, mean[g], &cb);
+                contrib = cb ? 1 : 0;
+            }
+        }
+        S.val[e] = contrib ? v : 0.0f;
+        S.contr[e] = contrib;
+        S.mok[e] = mk;
+    }
+    __syncthreads();
+    // Column sums over wy rows for each output row of the tile.
+    for (int e = tid; e < kTile * Rc; e += bd) {
+        const int r = e % kTile, c = e / kTile;
+        double s = 0.0;
+        int cnt = 0;
+        uint8_t ok = 1;
+        for (int k = 0; k < wy; ++k) {
+            const int q = (r + k) + c * Rr;
+            s = __dadd_rn(s, static_cast<double>(S.val[q]));
+            cnt += S.contr[q];
+            ok &= S.mok[q];
+        }
+        S.vs[e] = s;
+        S.vc[e] = cnt;
+        S.ve[e] = ok;
+    }
+    __syncthreads();
+    for (int e = tid; e < kTile * kTile; e += bd) {
+        const int r = e % kTile, c = e / kTile;
+        const int64_t gr = r0 + r, gc = c0 + c;
+        if (gr >= nr || gc >= nc) continue;
+        double s = 0.0;
+        int cnt = 0;
+        uint8_t ok = 1;
+        for (int k = 0; k < wx; ++k) {
+            const int q = r + (c + k) * kTile;
+            s = __dadd_rn(s, S.vs[q]);
+            cnt += S.vc[q];
+            ok &= S.ve[q];
+        }
+        out(gr + gc * nr, s, cnt, ok != 0);
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ float box_mean(double s, int cnt) {
+    return cnt > 0 ? __double2float_rn(__ddiv_rn(s, static_cast<double>(cnt))) : __int_as_float(0x7fc00000);
+}
+
+__device__ BoxSmem box_smem(unsigned char* base, int wx, int wy) {
+    const int Rr = kTile + wy - 1, Rc = kTile + wx - 1;
+    BoxSmem S;
+    size_t off = 0;
+    S.vs = reinterpret_cast<double*>(base + off);
+    off += sizeof(double) * kTile * Rc;
+    S.val = reinterpret_cast<float*>(base + off);
+    off += sizeof(float) * Rr * Rc;
+    S.vc = reinterpret_cast<int*>(base + off);
+    off += sizeof(int) * kTile * Rc;
+    S.contr = base + off;
+    off += Rr * Rc;
+    S.mok = base + off;
+    off += Rr * Rc;
+    S.ve = base + off;
+    return S;
+}
+
+size_t box_smem_bytes(int wx, int wy) {
+    const size_t Rr = kTile + wy - 1, Rc = kTile + wx - 1;
+    return sizeof(double) * kTile * Rc + sizeof(float) * Rr * Rc + sizeof(int) * kTile * Rc +
+           2 * Rr * Rc + kTile * Rc + 64;
+}
+
+// Highpass (src/preprocess.jl:304-312) with `_filtered`: out = img - boxmean where valid,
+// zero and invalid elsewhere; the mask erodes by the filter width.
+template <typename T>
+__global__ void __launch_bounds__(kBoxThreads) k_highpass(const T* img, const uint8_t* mask,
+                                                          int64_t nr, int64_t nc, int wx, int wy,
+                                                          float* out, uint8_t* vout) {
+    extern __shared__ __align__(16) unsigned char bsm[];
+    const BoxSmem S = box_smem(bsm, wx, wy);
+    const int64_t r0 = static_cast<int64_t>(blockIdx.x) * kTile;
+    const int64_t c0 = static_cast<int64_t>(blockIdx.y) * kTile;
+    box_tile<T, BOX_IMAGE>(img, mask, nullptr, nr, nc, wx, wy, r0, c0, S,
+                           [&](int64_t g, double s, int cnt, bool eroded) {
+                               const float mean = box_mean(s, cnt);
+                               float o = (mask[g] && isfinite(mean)) ? __fsub_rn(as_f32(img[g]), mean)
+                                                                    : __int_as_float(0x7fc00000);
+                               bool v = eroded;
+                               if (!isfinite(o)) {
+                                   o = 0.0f;
+                                   v = false;
+                               }
+                               out[g] = o;
+                               vout[g] = v ? 1 : 0;
+                           });
+}
+
+// First Wallis pass: the masked box mean (src/preprocess.jl:336).
+template <typename T>
+__global__ void __launch_bounds__(kBoxThreads) k_boxmean(const T* img, const uint8_t* mask,
+                                                         int64_t nr, int64_t nc, int wx, int wy,
+                                                         float* mean) {
+    extern __shared__ __align__(16) unsigned char bsm[];
+    const BoxSmem S = box_smem(bsm, wx, wy);
+    const int64_t r0 = static_cast<int64_t>(blockIdx.x) * kTile;
+    const int64_t c0 = static_cast<int64_t>(blockIdx.y) * kTile;
+    box_tile<T, BOX_IMAGE>(img, mask, nullptr, nr, nc, wx, wy, r0, c0, S,
+                           [&](int64_t g, double s, int cnt, bool) { mean[g] = box_mean(s, cnt); });
+}
+
+// Second Wallis pass (src/preprocess.jl:337-351, 416-438) with `_filtered`.
+template <typename T>
+__global__ void __launch_bounds__(kBoxThreads) k_wallis(const T* img, const uint8_t* mask,
+                                                        const float* mean, int64_t nr,
+                                                        int64_t nc, int wx, int wy, float floor_sd,
+                                                        float* out, uint8_t* vout) {
+    extern __shared__ __align__(16) unsigned char bsm[];
+    const BoxSmem S = box_smem(bsm, wx, wy);
+    const int64_t r0 = static_cast<int64_t>(blockIdx.x) * kTile;
+    const int64_t c0 = static_cast<int64_t>(blockIdx.y) * kTile;
+    box_tile<T, BOX_DEV2>(img, mask, mean, nr, nc, wx, wy, r0, c0, S,
+                          [&](int64_t g, double s, int cnt, bool eroded) {
+                              float msd = box_mean(s, cnt);
+                              // sqrt(max(msd, 0f0)): Julia's max keeps a NaN.
+                              if (!isnan(msd)) msd = __fsqrt_rn(fmaxf(msd, 0.0f));
+                              const float m = mean[g];
+                              float o;
+                              if (!mask[g] || !isfinite(m) || !isfinite(msd)) {
+                                  o = __int_as_float(0x7fc00000);
+                              } else {
+                                  const float sd = fmaxf(msd, floor_sd);
+                                  o = sd > 0.0f ? __fdiv_rn(__fsub_rn(as_f32(img[g]), m), sd)
+                                                : __int_as_float(0x7fc00000);
+                              }
+                              bool v = eroded;
+                              if (!isfinite(o)) {
+                                  o = 0.0f;
+                                  v = false;
+                              }
+                              out[g] = o;
+                              vout[g] = v ? 1 : 0;
+                          });
+}
+
+// ---------------------------------------------------------------------------------------------
+// Quantisation (src/preprocess.jl:546-592)
+
+}  // namespace
+
+// Double-double accumulator and the quantiser's device-side statistics (declared in
+// ar_internal.cuh so the context can size the scratch).
+struct DD {
+    double hi, lo;
+};
+
+__device__ __forceinline__ void dd_add(DD& a, double x) {
+    const double s = __dadd_rn(a.hi, x);
+    const double bb = __dsub_rn(s, a.hi);
+    const double e = __dadd_rn(__dsub_rn(a.hi, __dsub_rn(s, bb)), __dsub_rn(x, bb));
+    a.hi = s;
+    a.lo = __dadd_rn(a.lo, e);
+}
+
+__device__ __forceinline__ void dd_merge(DD& a, const DD& b) {
+    dd_add(a, b.hi);
+    a.lo = __dadd_rn(a.lo, b.lo);
+}
+
+struct QuantStats {
+    double mean, sd, lo, scale;
+    long long n;
+    DD part[kStatBlocks];
+    long long cnt[kStatBlocks];
+};
+
+namespace {
+
+template <typename T>
+__device__ __forceinline__ bool q_ok(const T* img, const uint8_t* mask, int64_t i, double* v) {
+    *v = static_cast<double>(img[i]);
+    return mask[i] && isfinite(*v);
+}
+
+__device__ void block_dd(DD& a, long long& c, DD* sa, long long* sc) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        DD b{__shfl_xor_sync(kFullMask, a.hi, o), __shfl_xor_sync(kFullMask, a.lo, o)};
+        dd_merge(a, b);
+        c += __shfl_xor_sync(kFullMask, c, o);
+    }
+    if (lane == 0) {
+        sa[warp] = a;
+        sc[warp] = c;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < nw; ++k) {
+            dd_merge(a, sa[k]);
+            c += sc[k];
+        }
+    }
+}
+
+// pass 0: sum and count of the valid finite values; pass 1: sum of squared deviations.
+template <typename T, int PASS>
+__global__ void __launch_bounds__(kStatThreads) k_qstats(const T* img, const uint8_t* mask,
+                                                         int64_t n, QuantStats* st) {
+    __shared__ DD sa[32];
+    __shared__ long long sc[32];
+    DD a{0.0, 0.0};
+    long long c = 0;
+    const double mean = PASS == 1 ? st->mean : 0.0;
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double v;
+        if (!q_ok(img, mask, i, &v)) continue;
+        if (PASS == 0) {
+            dd_add(a, v);
+            ++c;
+        } else {
+            const double d = __dsub_rn(v, mean);
+            dd_add(a, __dmul_rn(d, d));
+        }
+    }
+    block_dd(a, c, sa, sc);
+    if (threadIdx.x == 0) {
+        st->part[blockIdx.x] = a;
+        st->cnt[blockIdx.x] = c;
+    }
+}
+
+// Fixed-order combination of the block partials.
+template <int PASS>
+__global__ void k_qfinal(QuantStats* st, int nblocks) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    DD a{0.0, 0.0};
+    long long c = 0;
+    for (int k = 0; k < nblocks; ++k) {
+        dd_merge(a, st->part[k]);
+        c += st->cnt[k];
+    }
+    const double s = __dadd_rn(a.hi, a.lo);
+    if (PASS == 0) {
+        st->n = c;
+        st->mean = c > 0 ? __ddiv_rn(s, static_cast<double>(c)) : 0.0;
+    } else {
+        const long long nn = st->n;
+        const double sd = nn > 1 ? __dsqrt_rn(__ddiv_rn(s, static_cast<double>(nn - 1))) : 0.0;
+        st->sd = sd;
+        st->lo = __dsub_rn(st->mean, __dmul_rn(3.0, sd));
+        st->scale = sd != 0.0 ? __ddiv_rn(255.0, __dmul_rn(6.0, sd)) : 0.0;
+    }
+}
+
+template <typename T>
+__global__ void k_quantize(const T* img, const uint8_t* mask, int64_t n, const QuantStats* st,
+                           uint8_t* out) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    const long long cnt = st->n;
+    if (cnt == 0) {
+        out[i] = 0;
+        return;
+    }
+    if (st->sd == 0.0) {
+        out[i] = mask[i] ? 0x80 : 0x00;
+        return;
+    }
+    double v;
+    if (!q_ok(img, mask, i, &v)) {
+        out[i] = 0;
+        return;
+    }
+    double x = __dmul_rn(__dsub_rn(v, st->lo), st->scale);
+    x = x < 0.0 ? 0.0 : (x > 255.0 ? 255.0 : x);
+    out[i] = static_cast<uint8_t>(__double2uint_rn(x));
+}
+
+// NoQuantize of a float image: non-finite values become zero, the mask is kept
+// (src/preprocess.jl:495-507).
+template <typename T>
+__global__ void k_finite_copy(const T* img, int64_t n, T* out) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    const T v = img[i];
+    out[i] = isfinite(static_cast<double>(v)) ? v : T(0);
+}
+
+template <typename T>
+cudaError_t quantize_u8(const T* img, const uint8_t* mask, int64_t n, QuantStats* st,
+                        uint8_t* out, cudaStream_t s, long long* launches) {
+    k_qstats<T, 0><<<kStatBlocks, kStatThreads, 0, s>>>(img, mask, n, st);
+    k_qfinal<0><<<1, 32, 0, s>>>(st, kStatBlocks);
+    k_qstats<T, 1><<<kStatBlocks, kStatThreads, 0, s>>>(img, mask, n, st);
+    k_qfinal<1><<<1, 32, 0, s>>>(st, kStatBlocks);
+    const int threads = 256;
+    k_quantize<T><<<static_cast<unsigned>((n + threads - 1) / threads), threads, 0, s>>>(img, mask, n, st, out);
+    *launches += 5;
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t prepare_t(const PrepareJob& J, cudaStream_t s, long long* launches) {
+    const T* img = static_cast<const T*>(J.img);
+    const int64_t n = J.nrows * J.ncols;
+    if (J.preprocess == 0) {
+        cudaError_t e = cudaMemcpyAsync(J.vout, J.mask, n, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return e;
+        if (J.quantize == 1)
+            return quantize_u8(img, J.mask, n, J.stats, static_cast<uint8_t*>(J.out), s, launches);
+        const int threads = 256;
+        k_finite_copy<T><<<static_cast<unsigned>((n + threads - 1) / threads), threads, 0, s>>>(
+            img, n, static_cast<T*>(J.out));
+        *launches += 1;
+        return cudaGetLastError();
+    }
+    const dim3 grid(static_cast<unsigned>((J.nrows + kTile - 1) / kTile),
+                    static_cast<unsigned>((J.ncols + kTile - 1) / kTile));
+    // The window clamped to the image (src/window.jl:632-637).
+    const int wx = static_cast<int>(std::min<int64_t>(J.width, J.ncols));
+    const int wy = static_cast<int>(std::min<int64_t>(J.width, J.nrows));
+    const size_t smem = box_smem_bytes(wx, wy);
+    float* filt = J.quantize == 1 ? J.ftmp : static_cast<float*>(J.out);
+    cudaError_t e;
+    if (J.preprocess == 1) {
+        e = cudaFuncSetAttribute(k_highpass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        k_highpass<T><<<grid, kBoxThreads, smem, s>>>(img, J.mask, J.nrows, J.ncols, wx, wy, filt, J.vout);
+        *launches += 1;
+    } else {
+        e = cudaFuncSetAttribute(k_boxmean<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_wallis<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        k_boxmean<T><<<grid, kBoxThreads, smem, s>>>(img, J.mask, J.nrows, J.ncols, wx, wy, J.mtmp);
+        k_wallis<T><<<grid, kBoxThreads, smem, s>>>(img, J.mask, J.mtmp, J.nrows, J.ncols, wx, wy,
+                                                    static_cast<float>(J.min_std), filt, J.vout);
+        *launches += 2;
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess || J.quantize != 1) return e;
+    return quantize_u8(filt, J.vout, n, J.stats, static_cast<uint8_t*>(J.out), s, launches);
+}
+
+}  // namespace
+
+size_t quant_stats_bytes() { return sizeof(QuantStats); }
+
+int max_filter_width() { return kMaxWidth; }
+
+cudaError_t launch_prepare(const PrepareJob& J, cudaStream_t s, long long* launches) {
+    if (J.width > kMaxWidth && J.preprocess != 0) return cudaErrorInvalidValue;
+    switch (J.dtype) {
+        case AR_U8: return prepare_t<uint8_t>(J, s, launches);
+        case AR_U16: return prepare_t<uint16_t>(J, s, launches);
+        case AR_I16: return prepare_t<int16_t>(J, s, launches);
+        case AR_F32: return prepare_t<float>(J, s, launches);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace ar

@@ -39,7 +39,6 @@ constexpr int kMI = 10;        // surface rows per thread item
 constexpr int kUA = 16;        // chip rows per inner step
 constexpr int kCorrThreads = 256;
 constexpr int kRefineThreads = 256;
-constexpr int kChunk = 16;     // rows of the penultimate cascade level per streaming chunk
 constexpr unsigned kFull = 0xffffffffu;
 
 template <typename T>
@@ -159,32 +158,7 @@ __device__ __forceinline__ V warp_inclusive_scan(V v) {
 }
 
 // ----------------------------------------------------------------------------------------------
-// pyrUp taps (src/peak.jl:312-324, 374-382), 0-based.
-
-__device__ __forceinline__ int reflect101_0(int p, int n) {
-    if (n == 1) return 0;
-    const int m = n - 1;
-    while (p < 0 || p > m) {
-        if (p < 0) p = -p;
-        if (p > m) p = 2 * m - p;
-    }
-    return p;
-}
-
-// Source taps of output position p on an axis whose source length is n: returns the number
-// of taps (3 on a sample, 2 between samples) and the minus/centre/plus source indices.
-__device__ __forceinline__ int pyr_taps(int p, int n, int* m, int* c, int* q) {
-    if ((p & 1) == 0) {
-        *c = p >> 1;
-        *m = reflect101_0(p - 2, 2 * n) >> 1;
-        *q = reflect101_0(p + 2, 2 * n) >> 1;
-        return 3;
-    }
-    *c = reflect101_0(p - 1, 2 * n) >> 1;
-    *m = *c;
-    *q = reflect101_0(p + 1, 2 * n) >> 1;
-    return 2;
-}
+// pyrUp arithmetic
 
 // One pyrUp sample in the reference's operation order (src/peak.jl:266-292).
 __device__ __forceinline__ float pyr_sample(int nt, float a, float b, float c) {
@@ -534,6 +508,19 @@ __global__ void __launch_bounds__(kCorrThreads, 2) k_corr(const CorrArgs A) {
 
 // ----------------------------------------------------------------------------------------------
 // Sub-pixel cascade kernel (src/peak.jl:456-522 from the patch onward).
+//
+// Levels up to (5 * up / 4)^2 are materialised in shared memory. The last two levels -- 90%
+// of the samples at up = 64 -- are produced in blocks of the final level, and a block is
+// evaluated only if it can hold the maximum: every pyrUp sample is a rounded convex
+// combination of its taps, so a final sample cannot exceed the largest materialised sample
+// under its two-level footprint by more than a few ulps. Blocks are visited in decreasing
+// order of that bound and the search stops once the best remaining bound is strictly below
+// the maximum found, so the result (value and row-major-first position) is exactly that of
+// the full cascade.
+
+constexpr int kQB = 16;  // penultimate-level rows per final block (32 final rows)
+constexpr int kCB = 64;  // final-level columns per final block
+constexpr int kMaxBlocks = 256;
 
 struct RefineArgs {
     const int* count;       // device count of queued items (or null: use n_items)
@@ -551,25 +538,85 @@ struct RefineArgs {
     unsigned off_B, off_T, off_P, off_C;  // float offsets: A at 0
 };
 
+// Taps of output position p on an axis whose source has n >= 2 samples: the closed form of
+// src/peak.jl:312-324 (reflection in upsampled space only ever folds the first sample's minus
+// tap onto sample 1 and the last samples' plus tap onto sample n-1).
+__device__ __forceinline__ int taps(int p, int n, int& m, int& c, int& q) {
+    c = p >> 1;
+    q = min(c + 1, n - 1);
+    if (p & 1) {
+        m = c;
+        return 2;
+    }
+    m = c == 0 ? 1 : c - 1;
+    return 3;
+}
+
 // One pyrUp step over shared memory, src (sh x sw) -> dst (2sh x 2sw) via tmp (2sh x sw);
-// all column-major. The vertical then horizontal order of src/peak.jl:261-292.
+// all column-major. Vertical then horizontal, as src/peak.jl:261-292. Warps own columns,
+// lanes rows, so no index division is needed.
 __device__ void pyrup_block(const float* src, int sh, int sw, float* dst, float* tmp) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int th = 2 * sh;
-    for (int e = threadIdx.x; e < th * sw; e += blockDim.x) {
-        const int i = e % th, j = e / th;
-        int m, c, q;
-        const int nt = pyr_taps(i, sh, &m, &c, &q);
+    for (int j = warp; j < sw; j += nw) {
         const float* s = src + j * sh;
-        tmp[i + j * th] = pyr_sample(nt, s[m], s[c], s[q]);
+        for (int i = lane; i < th; i += 32) {
+            int m, c, q;
+            const int nt = taps(i, sh, m, c, q);
+            tmp[i + j * th] = pyr_sample(nt, s[m], s[c], s[q]);
+        }
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < th * 2 * sw; e += blockDim.x) {
-        const int i = e % th, j = e / th;
+    for (int j = warp; j < 2 * sw; j += nw) {
         int m, c, q;
-        const int nt = pyr_taps(j, sw, &m, &c, &q);
-        dst[i + j * th] = pyr_sample(nt, tmp[i + m * th], tmp[i + c * th], tmp[i + q * th]);
+        const int nt = taps(j, sw, m, c, q);
+        const float* tm = tmp + m * th;
+        const float* tc = tmp + c * th;
+        const float* tq = tmp + q * th;
+        float* d = dst + j * th;
+        for (int i = lane; i < th; i += 32) d[i] = pyr_sample(nt, tm[i], tc[i], tq[i]);
     }
     __syncthreads();
+}
+
+// (value, row-major index) pairs: larger value wins, equal values go to the smaller index;
+// NaN never wins.
+__device__ __forceinline__ void best_update(float v, int idx, float& bv, int& bi) {
+    if (v > bv || (v == bv && idx < bi)) {
+        bv = v;
+        bi = idx;
+    }
+}
+
+__device__ void block_best(float& bv, int& bi, float* rv, int* ri) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float v2 = __shfl_xor_sync(kFull, bv, o);
+        const int i2 = __shfl_xor_sync(kFull, bi, o);
+        best_update(v2, i2, bv, bi);
+    }
+    __syncthreads();
+    if (lane == 0) {
+        rv[warp] = bv;
+        ri[warp] = bi;
+    }
+    __syncthreads();
+    bv = lane < nw ? rv[lane] : -INFINITY;
+    bi = lane < nw ? ri[lane] : INT_MAX;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float v2 = __shfl_xor_sync(kFull, bv, o);
+        const int i2 = __shfl_xor_sync(kFull, bi, o);
+        best_update(v2, i2, bv, bi);
+    }
+}
+
+// Upper bound on any sample two pyrUp levels above values <= m: rounding in
+// fl(fl(0.75b) + fl(0.125 fl(a+c))) can exceed the largest tap by under 2^-23 relative per
+// level; the slack here is 2^-20 relative plus the smallest normal.
+__device__ __forceinline__ float two_level_bound(float m) {
+    return m + fabsf(m) * 9.5367431640625e-07f + 1.17549435e-38f;
 }
 
 __global__ void __launch_bounds__(kRefineThreads) k_refine(const RefineArgs A) {
@@ -578,10 +625,15 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine(const RefineArgs A) {
     float* sB = rsm + A.off_B;
     float* sT = rsm + A.off_T;
     float* sP = rsm + A.off_P;
-    float* sC = rsm + A.off_C;  // streaming chunk buffers (alias sB/sT)
-    __shared__ unsigned long long red[32];
+    float* sC = rsm + A.off_C;  // block buffers (alias sB/sT once materialised)
+    __shared__ float rv[32];
+    __shared__ int ri[32];
+    __shared__ float sbound[kMaxBlocks];
+    __shared__ float s_best;
+    __shared__ int s_sel;
 
     const int tid = threadIdx.x, bd = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5, nw = bd >> 5;
     const int64_t count = A.count ? static_cast<int64_t>(*A.count) : A.n_items;
     const int L = A.levels;
     const int nmat_levels = L <= 2 ? L : L - 2;
@@ -598,77 +650,139 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine(const RefineArgs A) {
             cur = dst;
             n *= 2;
         }
-        unsigned long long best = 0ull;
+        float bv = -INFINITY;
+        int bi = INT_MAX;
         int nfinal;
         if (L <= 2) {
             nfinal = n;
-            for (int e = tid; e < n * n; e += bd) {
-                const int i = e % n, j = e / n;
-                const unsigned long long kk = argmax_key(cur[i + j * n], static_cast<unsigned>(i * n + j));
-                best = kk > best ? kk : best;
-            }
+            for (int j = warp; j < n; j += nw)
+                for (int i = lane; i < n; i += 32) best_update(cur[i + j * n], i * n + j, bv, bi);
+            block_best(bv, bi, rv, ri);
         } else {
-            // Stream the last two levels from the materialised one (n x n in sA): rows of the
-            // penultimate level (2n wide) are built a chunk at a time, the final level (4n) is
-            // reduced on the fly and never stored.
             const int N1 = 2 * n, N2 = 4 * n;
             nfinal = N2;
-            float* TA = sC;                       // (kChunk + 2) x n
-            float* RB = TA + (kChunk + 2) * n;    // (kChunk + 2) x N1
-            float* TB = RB + (kChunk + 2) * N1;   // 2*kChunk x N1
-            for (int q0 = 0; q0 < N1; q0 += kChunk) {
-                const int q1 = min(q0 + kChunk, N1);
-                const int qa = max(q0 - 1, 0), qb = min(q1, N1 - 1);
-                const int nq = qb - qa + 1;
-                const int np = 2 * (q1 - q0);
-                // Vertical taps of the penultimate rows qa..qb over the materialised level.
-                for (int e = tid; e < nq * n; e += bd) {
-                    const int qq = e / n, jj = e % n;
-                    int m, c, q;
-                    const int nt = pyr_taps(qa + qq, n, &m, &c, &q);
-                    TA[qq * n + jj] = pyr_sample(nt, cur[m + jj * n], cur[c + jj * n], cur[q + jj * n]);
+            const int nqb = (N1 + kQB - 1) / kQB, ncb = (N2 + kCB - 1) / kCB;
+            const int nblk = nqb * ncb;
+            // Bounds: the largest materialised sample under each final block's footprint.
+            for (int blk = warp; blk < nblk; blk += nw) {
+                const int qi = blk % nqb, cj = blk / nqb;
+                const int q0 = qi * kQB, q1 = min(q0 + kQB, N1);
+                const int c0 = cj * kCB, c1 = min(c0 + kCB, N2);
+                const int pr0 = max(q0 - 1, 0), pr1 = min(q1, N1 - 1);
+                const int pc0 = max(c0 / 2 - 1, 0), pc1 = min((c1 - 1) / 2 + 1, N1 - 1);
+                const int sr0 = max(pr0 / 2 - 1, 0), sr1 = min(pr1 / 2 + 1, n - 1);
+                const int sc0 = max(pc0 / 2 - 1, 0), sc1 = min(pc1 / 2 + 1, n - 1);
+                const int nr_ = sr1 - sr0 + 1;
+                float mx = -INFINITY;
+                for (int jj = sc0; jj <= sc1; ++jj)
+                    for (int ii = lane; ii < nr_; ii += 32) mx = fmaxf(mx, cur[(sr0 + ii) + jj * n]);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, o));
+                if (lane == 0) sbound[blk] = two_level_bound(mx);
+            }
+            if (tid == 0) s_best = -INFINITY;
+            __syncthreads();
+            float* TA = sC;                         // (kQB+2) x (kCB/4+4): penultimate rows over S columns
+            float* RB = TA + (kQB + 2) * (kCB / 4 + 4);   // (kQB+2) x (kCB/2+2): penultimate samples
+            float* TB = RB + (kQB + 2) * (kCB / 2 + 2);   // 2kQB x (kCB/2+2): final rows over penultimate columns
+            const int TAS = kCB / 4 + 4, RBS = kCB / 2 + 2;
+            for (int it = 0; it < nblk; ++it) {
+                // Pick the unvisited block with the largest bound (lowest index on ties).
+                if (warp == 0) {
+                    float m = -INFINITY;
+                    int sel = INT_MAX;
+                    for (int b = lane; b < nblk; b += 32) {
+                        const float v = sbound[b];
+                        if (v > m || (v == m && b < sel)) {
+                            m = v;
+                            sel = b;
+                        }
+                    }
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        const float m2 = __shfl_xor_sync(kFull, m, o);
+                        const int s2 = __shfl_xor_sync(kFull, sel, o);
+                        if (m2 > m || (m2 == m && s2 < sel)) {
+                            m = m2;
+                            sel = s2;
+                        }
+                    }
+                    if (lane == 0) {
+                        // Stop once nothing left can reach the maximum found so far.
+                        const bool go = m != -INFINITY && sel < nblk && !(m < s_best);
+                        s_sel = go ? sel : -1;
+                        if (go) sbound[sel] = -INFINITY;
+                    }
                 }
                 __syncthreads();
-                // Horizontal: the penultimate rows themselves.
-                for (int e = tid; e < nq * N1; e += bd) {
-                    const int qq = e / N1, cc = e % N1;
-                    int m, c, q;
-                    const int nt = pyr_taps(cc, n, &m, &c, &q);
-                    RB[qq * N1 + cc] = pyr_sample(nt, TA[qq * n + m], TA[qq * n + c], TA[qq * n + q]);
+                const int blk = s_sel;
+                if (blk < 0) break;
+                const int qi = blk % nqb, cj = blk / nqb;
+                const int q0 = qi * kQB, q1 = min(q0 + kQB, N1);
+                const int c0 = cj * kCB, c1 = min(c0 + kCB, N2);
+                const int pr0 = max(q0 - 1, 0), pr1 = min(q1, N1 - 1);
+                const int pc0 = max(c0 / 2 - 1, 0), pc1 = min((c1 - 1) / 2 + 1, N1 - 1);
+                const int sc0 = max(pc0 / 2 - 1, 0), sc1 = min(pc1 / 2 + 1, n - 1);
+                const int nq = pr1 - pr0 + 1, nsc = sc1 - sc0 + 1, npc = pc1 - pc0 + 1;
+                const int np = 2 * (q1 - q0), ncl = c1 - c0;
+                // Penultimate rows pr0..pr1: vertical taps over the materialised level.
+                for (int e = tid; e < nq * TAS; e += bd) {
+                    const int qq = e / TAS, jj = e - qq * TAS;
+                    if (jj < nsc) {
+                        int m, c, q;
+                        const int nt = taps(pr0 + qq, n, m, c, q);
+                        const float* col = cur + (sc0 + jj) * n;
+                        TA[qq * TAS + jj] = pyr_sample(nt, col[m], col[c], col[q]);
+                    }
                 }
                 __syncthreads();
-                // Vertical taps of the final rows 2q0 .. 2q1-1 over the penultimate rows.
-                for (int e = tid; e < np * N1; e += bd) {
-                    const int pp = e / N1, cc = e % N1;
-                    int m, c, q;
-                    const int nt = pyr_taps(2 * q0 + pp, N1, &m, &c, &q);
-                    TB[pp * N1 + cc] = pyr_sample(nt, RB[(m - qa) * N1 + cc], RB[(c - qa) * N1 + cc],
-                                                  RB[(q - qa) * N1 + cc]);
+                // Horizontal: the penultimate samples.
+                for (int e = tid; e < nq * RBS; e += bd) {
+                    const int qq = e / RBS, cc = e - qq * RBS;
+                    if (cc < npc) {
+                        int m, c, q;
+                        const int nt = taps(pc0 + cc, n, m, c, q);
+                        const float* row = TA + qq * TAS - sc0;
+                        RB[qq * RBS + cc] = pyr_sample(nt, row[m], row[c], row[q]);
+                    }
                 }
                 __syncthreads();
-                // Horizontal: final samples, reduced to the row-major first maximum.
-                for (int e = tid; e < np * N2; e += bd) {
-                    const int pp = e / N2, c4 = e % N2;
-                    int m, c, q;
-                    const int nt = pyr_taps(c4, N1, &m, &c, &q);
-                    const float v = pyr_sample(nt, TB[pp * N1 + m], TB[pp * N1 + c], TB[pp * N1 + q]);
-                    const unsigned long long kk =
-                        argmax_key(v, static_cast<unsigned>((2 * q0 + pp) * N2 + c4));
-                    best = kk > best ? kk : best;
+                // Final rows 2q0 .. 2q1-1: vertical taps over the penultimate rows.
+                for (int e = tid; e < np * RBS; e += bd) {
+                    const int pp = e / RBS, cc = e - pp * RBS;
+                    if (cc < npc) {
+                        int m, c, q;
+                        const int nt = taps(2 * q0 + pp, N1, m, c, q);
+                        TB[pp * RBS + cc] = pyr_sample(nt, RB[(m - pr0) * RBS + cc],
+                                                       RB[(c - pr0) * RBS + cc],
+                                                       RB[(q - pr0) * RBS + cc]);
+                    }
                 }
                 __syncthreads();
+                // Final samples, reduced to the row-major first maximum.
+                for (int e = tid; e < np * kCB; e += bd) {
+                    const int pp = e / kCB, cl = e - pp * kCB;
+                    if (cl < ncl) {
+                        int m, c, q;
+                        const int c4 = c0 + cl;
+                        const int nt = taps(c4, N1, m, c, q);
+                        const float* row = TB + pp * RBS - pc0;
+                        best_update(pyr_sample(nt, row[m], row[c], row[q]),
+                                    (2 * q0 + pp) * N2 + c4, bv, bi);
+                    }
+                }
+                block_best(bv, bi, rv, ri);
+                if (tid == 0) s_best = bv;
             }
         }
-        best = block_max_u64(best, red);
         if (tid == 0) {
-            unsigned rm = 0;
-            float v = 0.0f;
             int si = 0, sj = 0;
-            if (key_decode(best, &rm, &v)) {
-                si = static_cast<int>(rm / nfinal);
-                sj = static_cast<int>(rm % nfinal);
+            float v = bv;
+            if (bi != INT_MAX && bv != -INFINITY) {
+                si = bi / nfinal;
+                sj = bi - si * nfinal;
             } else {
-                v = cur[0];  // (1,1) of a level with nothing above -Inf; only reachable if materialised
+                v = L <= 2 ? cur[0] : NAN;  // nothing above -Inf: the reference reports (1,1)
             }
             if (A.point) {
                 const int64_t k = A.point[item];
@@ -705,24 +819,41 @@ __global__ void k_init_outputs(DevOutputs out, int64_t n, int* sub_count) {
 }
 
 // geom: [0] max ch, [1] max cw, [2] max nr, [3] max nc, [4] max px term, [5] max py term,
-// [6] 1 while every window fits, [7] searchable count. Reductions by atomics.
+// [6] 1 while every window fits, [7] searchable count. Warp reductions, one atomic per warp.
 __global__ void k_pass_geometry(DevPoints p, int64_t nrows, int64_t ncols, long long* geom) {
     const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    if (k >= p.n) return;
-    const int64_t rx = p.rx[k], ry = p.ry[k];
-    if (!(rx > 0 && ry > 0)) return;
-    const int64_t hx = p.csx[k] / 2, hy = p.csy[k] / 2;
-    atomicMax(&geom[0], static_cast<long long>(2 * hy));
-    atomicMax(&geom[1], static_cast<long long>(2 * hx));
-    atomicMax(&geom[2], static_cast<long long>(2 * ry));
-    atomicMax(&geom[3], static_cast<long long>(2 * rx));
-    atomicMax(&geom[4], static_cast<long long>(hx + rx + static_cast<int64_t>(ceil(fabs(p.dx0[k])))));
-    atomicMax(&geom[5], static_cast<long long>(hy + ry + static_cast<int64_t>(ceil(fabs(p.dy0[k])))));
-    const int64_t wcx = static_cast<int64_t>(floor(p.x[k])), wcy = static_cast<int64_t>(floor(p.y[k]));
-    const bool inb = (wcy - hy - ry) >= 1 && (wcy + hy + ry - 2) <= nrows &&
-                     (wcx - hx - rx) >= 1 && (wcx + hx + rx - 2) <= ncols;
-    if (!inb) atomicMin(&geom[6], 0ll);
-    atomicAdd(reinterpret_cast<unsigned long long*>(&geom[7]), 1ull);
+    long long v[6] = {0, 0, 0, 0, 0, 0};
+    int fits = 1, cnt = 0;
+    if (k < p.n) {
+        const int64_t rx = p.rx[k], ry = p.ry[k];
+        if (rx > 0 && ry > 0) {
+            const int64_t hx = p.csx[k] / 2, hy = p.csy[k] / 2;
+            v[0] = 2 * hy;
+            v[1] = 2 * hx;
+            v[2] = 2 * ry;
+            v[3] = 2 * rx;
+            v[4] = hx + rx + static_cast<int64_t>(ceil(fabs(p.dx0[k])));
+            v[5] = hy + ry + static_cast<int64_t>(ceil(fabs(p.dy0[k])));
+            const int64_t wcx = static_cast<int64_t>(floor(p.x[k]));
+            const int64_t wcy = static_cast<int64_t>(floor(p.y[k]));
+            fits = (wcy - hy - ry) >= 1 && (wcy + hy + ry - 2) <= nrows &&
+                   (wcx - hx - rx) >= 1 && (wcx + hx + rx - 2) <= ncols;
+            cnt = 1;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) v[q] = max(v[q], __shfl_xor_sync(kFull, v[q], o));
+        fits &= __shfl_xor_sync(kFull, fits, o);
+        cnt += __shfl_xor_sync(kFull, cnt, o);
+    }
+    if ((threadIdx.x & 31) == 0 && cnt > 0) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) atomicMax(&geom[q], v[q]);
+        if (!fits) atomicMin(&geom[6], 0ll);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&geom[7]), static_cast<unsigned long long>(cnt));
+    }
 }
 
 inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
@@ -811,13 +942,14 @@ RefinePlan plan_refine(int up) {
     const size_t a = static_cast<size_t>(nm) * nm;
     const size_t b = static_cast<size_t>(nm / 2) * (nm / 2);
     const size_t t = static_cast<size_t>(nm) * (nm / 2);
-    size_t chunk = 0;
-    if (L > 2) chunk = static_cast<size_t>(kChunk + 2) * nm + static_cast<size_t>(kChunk + 2) * 2 * nm +
-                       static_cast<size_t>(2 * kChunk) * 2 * nm;
+    size_t blocks = 0;
+    if (L > 2)
+        blocks = static_cast<size_t>(kQB + 2) * (kCB / 4 + 4) + static_cast<size_t>(kQB + 2) * (kCB / 2 + 2) +
+                 static_cast<size_t>(2 * kQB) * (kCB / 2 + 2);
     R.off_B = static_cast<unsigned>(a);
     R.off_T = static_cast<unsigned>(a + b);
-    R.off_C = static_cast<unsigned>(a);  // the chunk buffers reuse B and T once materialised
-    const size_t tail = std::max(b + t, chunk);
+    R.off_C = static_cast<unsigned>(a);  // the block buffers reuse B and T once materialised
+    const size_t tail = std::max(b + t, blocks);
     R.off_P = static_cast<unsigned>(a + tail);
     R.smem = (a + tail + 32) * sizeof(float);
     return R;
@@ -860,6 +992,17 @@ cudaError_t ensure_scratch(TrackScratch& s, int64_t n) {
 
 }  // namespace
 
+cudaEvent_t KernelTimer::get() {
+    if (!pool.empty()) {
+        cudaEvent_t e = pool.back();
+        pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
 PassGeometry pass_geometry_host(const ar_points& p, int64_t nrows, int64_t ncols) {
     PassGeometry g;
     bool fits = true;
@@ -897,6 +1040,7 @@ cudaError_t pass_geometry_device(const DevPoints& pts, int64_t nrows, int64_t nc
         const int64_t blocks = (pts.n + threads - 1) / threads;
         k_pass_geometry<<<static_cast<unsigned>(blocks), threads, 0, stream>>>(
             pts, nrows, ncols, reinterpret_cast<long long*>(scratch.geom));
+        scratch.timer.launches += 1;
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
@@ -927,6 +1071,7 @@ cudaError_t launch_track(int dtype, const void* ref, const void* sec, const uint
         const int threads = 256;
         k_init_outputs<<<static_cast<unsigned>((pts.n + threads - 1) / threads), threads, 0, stream>>>(
             out, pts.n, scratch.sub_count);
+        scratch.timer.launches += 1;
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
@@ -969,6 +1114,14 @@ cudaError_t launch_track(int dtype, const void* ref, const void* sec, const uint
     A.sub_patch = scratch.sub_patch;
     A.surf_out = surf_out;
 
+    KernelTimer& T = scratch.timer;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+    if (T.enabled) {
+        ev0 = T.get();
+        ev1 = T.get();
+        ev2 = T.get();
+        cudaEventRecord(ev0, stream);
+    }
     const int per_sm = P.smem <= 100 * 1024 ? 2 : 1;
     const int64_t want = static_cast<int64_t>(num_sms) * per_sm * 8;
     const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(pts.n, want)));
@@ -982,7 +1135,15 @@ cudaError_t launch_track(int dtype, const void* ref, const void* sec, const uint
             return cudaErrorInvalidValue;
     }
     if (e != cudaSuccess) return e;
-    if (up == 1) return cudaSuccess;
+    T.launches += 1;
+    if (T.enabled) cudaEventRecord(ev1, stream);
+    if (up == 1) {
+        if (T.enabled) {
+            cudaEventRecord(ev2, stream);
+            T.recs.push_back({ev0, ev1, ev2});
+        }
+        return cudaSuccess;
+    }
 
     const RefinePlan R = plan_refine(up);
     RefineArgs B{};
@@ -1005,7 +1166,13 @@ cudaError_t launch_track(int dtype, const void* ref, const void* sec, const uint
     const int rgrid = static_cast<int>(std::max<int64_t>(
         1, std::min<int64_t>(pts.n, static_cast<int64_t>(num_sms) * 4)));
     k_refine<<<rgrid, kRefineThreads, R.smem, stream>>>(B);
-    return cudaGetLastError();
+    e = cudaGetLastError();
+    T.launches += 1;
+    if (T.enabled) {
+        cudaEventRecord(ev2, stream);
+        T.recs.push_back({ev0, ev1, ev2});
+    }
+    return e;
 }
 
 cudaError_t launch_refine_patches(const float* patches, int64_t count, int up, int32_t* row,

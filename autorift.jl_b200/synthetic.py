@@ -130,17 +130,20 @@ def gaussian_bumps(shape, n_bumps: int, max_amp: float, widths=(300.0, 800.0), b
 
 
 def scale_u16_pair(n: int = 4096, seed: int = 11, max_amp: float = 15.0, noise: float = 0.02,
-                   nodata: float = 0.03, sigma: float = 2.0):
+                   nodata: float = 0.03, sigma: float = 2.0, mean: float = 8000.0,
+                   std: float = 1500.0, dtype=np.uint16):
     """UInt16 pair at scale: filtered noise (sigma 2) mapped to mean 8000, std 1500, clipped;
     the secondary is a bicubic warp by a 6-bump field plus 2% Gaussian noise (of the image
-    std) and 3% zero-valued no-data blobs of radius 20-80 px.
+    std) and 3% zero-valued no-data blobs of radius 20-80 px. `mean`, `std` and `dtype`
+    produce the same scene at another bit depth.
 
     Returns (image1, image2, secondary_valid, (fx, fy)) with (fx, fy) the imposed feature
     motion in pixels (the tracker reports its negative)."""
+    hi = float(np.iinfo(dtype).max)
     rng = np.random.default_rng(seed)
     a = _ndi.gaussian_filter(rng.standard_normal((n, n)).astype(np.float32), sigma)
-    a = (a - a.mean()) / a.std() * 1500.0 + 8000.0
-    a = np.clip(a, 0, 65535)
+    a = (a - a.mean()) / a.std() * std + mean
+    a = np.clip(a, 0, hi)
     fx, fy = gaussian_bumps((n, n), 6, max_amp, seed=seed + 1)
     yy, xx = np.meshgrid(np.arange(n, dtype=np.float32), np.arange(n, dtype=np.float32),
                          indexing="ij")
@@ -148,9 +151,9 @@ def scale_u16_pair(n: int = 4096, seed: int = 11, max_amp: float = 15.0, noise: 
     del yy, xx
     b = _ndi.map_coordinates(a, coords, order=3, mode="nearest")
     del coords
-    b = b + rng.normal(0.0, noise * 1500.0, b.shape).astype(np.float32)
-    b = np.clip(np.round(b), 0, 65535).astype(np.uint16)
-    img1 = np.round(a).astype(np.uint16)
+    b = b + rng.normal(0.0, noise * std, b.shape).astype(np.float32)
+    b = np.clip(np.round(b), 0, hi).astype(dtype)
+    img1 = np.round(a).astype(dtype)
     # No-data blobs.
     holes = np.zeros((n, n), bool)
     target = nodata * n * n

@@ -80,6 +80,29 @@ int ar_pair_upload(ar_ctx* ctx, const void* ref, const void* sec, const uint8_t*
                    ar_pair** out);
 int ar_pair_destroy(ar_pair* pair);
 
+/* Pre-correlation filter and quantisation methods (src/types.jl:259-499). */
+enum { AR_PRE_NONE = 0, AR_PRE_HIGHPASS = 1, AR_PRE_WALLIS = 2 };
+enum { AR_QUANT_NONE = 0, AR_QUANT_UINT8 = 1 };
+
+typedef struct {
+    int preprocess;  /* AR_PRE_*: NoPreprocess, Highpass(width), Wallis(width, min_std) */
+    int width;       /* filter width, odd and >= 3 (ignored for AR_PRE_NONE) */
+    double min_std;  /* Wallis divisor floor, >= 0 */
+    int quantize;    /* AR_QUANT_*: NoQuantize or QuantizeUInt8 */
+} ar_prepare_opts;
+
+/*
+ * `_prepare(pair, p)` (src/api.jl:305-311): preprocess then quantize each image of `raw`
+ * (src/preprocess.jl:131-160, 275-460, 477-592) into a new device pair. The result's element
+ * type is UInt8 under AR_QUANT_UINT8, Float32 when a filter ran without quantisation, else the
+ * input type; its masks are the filtered (eroded) masks. `raw` is unchanged.
+ */
+int ar_prepare(ar_ctx* ctx, const ar_pair* raw, const ar_prepare_opts* opts, ar_pair** out);
+
+/* Copy a pair's images and masks back to host arrays (any may be NULL). */
+int ar_pair_download(ar_ctx* ctx, const ar_pair* pair, void* ref, void* sec, uint8_t* ref_valid,
+                     uint8_t* sec_valid);
+
 /* Element type and extents of an uploaded pair. */
 int ar_pair_info(const ar_pair* pair, int* dtype, int64_t* nrows, int64_t* ncols);
 
@@ -121,6 +144,17 @@ int ar_correlate(ar_ctx* ctx, const void* search, const void* chip, int dtype, i
  */
 int ar_refine_patches(ar_ctx* ctx, const float* patches, int64_t count, int upsampling,
                       int32_t* row, int32_t* col, float* value);
+
+/*
+ * Kernel timing, for benchmarks: when enabled, every track launch records CUDA events on its
+ * stream around the correlation kernel and the refinement kernel. ar_kernel_times waits for
+ * the recorded events and returns the summed milliseconds of each kernel, the number of
+ * track launches timed and the number of kernels the library launched, then resets. No
+ * reference counterpart (the reference times from Julia: benchmark/run.jl).
+ */
+int ar_ctx_set_timing(ar_ctx* ctx, int enable);
+int ar_kernel_times(ar_ctx* ctx, double* corr_ms, double* refine_ms, int64_t* tracks,
+                    int64_t* launches);
 
 /* Block until all work the context enqueued has finished. */
 int ar_synchronize(ar_ctx* ctx);

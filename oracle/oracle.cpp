@@ -391,6 +391,267 @@ bool correlate_arrays(const T* search, const T* chip, int64_t ch, int64_t cw, in
     return correlate(getw, getc, ch, cw, rx, ry, measure, surface, chipbuf, S, S2, num);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Pre-correlation filters and quantisation: src/preprocess.jl:275-460, 546-592 and the
+// sliding-window mean of src/window.jl:228-439 (banded running sums, 16-row bands).
+
+// src/window.jl:632-637 -- window clamped to the array; src/window.jl:254-257 -- margins.
+struct Margins { int64_t lx, ly, rx, ry; };
+inline Margins margins(int64_t wx, int64_t wy) {
+    return {wx / 2, wy / 2, wx - 1 - wx / 2, wy - 1 - wy / 2};
+}
+
+// src/window.jl:388-439 -- the dense path: no NaN, counts from the window geometry.
+template <class Get>
+void windowmean_dense(Get A, int64_t nr, int64_t nc, int64_t wx, int64_t wy, float* out) {
+    const Margins m = margins(wx, wy);
+    const int64_t nb = std::min<int64_t>(16, nr);
+    std::vector<double> sums(static_cast<size_t>(nb * nc)), rowbuf(static_cast<size_t>(nc));
+    for (int64_t i0 = 1; i0 <= nr;) {
+        const int64_t i1 = std::min(i0 + nb - 1, nr);
+        for (int64_t j = 1; j <= nc; ++j) {
+            double s = 0.0;
+            for (int64_t i = std::max<int64_t>(i0 - m.ly, 1); i <= std::min(i0 + m.ry, nr); ++i)
+                s += A(i - 1, j - 1);
+            for (int64_t i = i0; i <= i1; ++i) {
+                sums[(i - i0) + (j - 1) * nb] = s;
+                const int64_t oi = i - m.ly;
+                if (1 <= oi && oi <= nr) s -= A(oi - 1, j - 1);
+                const int64_t ii = i + m.ry + 1;
+                if (ii <= nr) s += A(ii - 1, j - 1);
+            }
+        }
+        for (int64_t i = i0; i <= i1; ++i) {
+            const int64_t ci = std::min(i + m.ry, nr) - std::max<int64_t>(i - m.ly, 1) + 1;
+            for (int64_t j = 1; j <= nc; ++j) rowbuf[j - 1] = sums[(i - i0) + (j - 1) * nb];
+            double s = 0.0;
+            for (int64_t j = 1; j <= std::min(m.rx + 1, nc); ++j) s += rowbuf[j - 1];
+            for (int64_t j = 1; j <= nc; ++j) {
+                const int64_t cj = std::min(j + m.rx, nc) - std::max<int64_t>(j - m.lx, 1) + 1;
+                out[(i - 1) + (j - 1) * nr] = static_cast<float>(s / static_cast<double>(ci * cj));
+                const int64_t oj = j - m.lx;
+                if (1 <= oj && oj <= nc) s -= rowbuf[oj - 1];
+                const int64_t jj = j + m.rx + 1;
+                if (jj <= nc) s += rowbuf[jj - 1];
+            }
+        }
+        i0 = i1 + 1;
+    }
+}
+
+// src/window.jl:289-366 -- the masked path: NaN skipped, sums carried with counts.
+template <class Get>
+void windowmean_masked(Get A, int64_t nr, int64_t nc, int64_t wx, int64_t wy, float* out) {
+    const Margins m = margins(wx, wy);
+    const int64_t nb = std::min<int64_t>(16, nr);
+    std::vector<double> sums(static_cast<size_t>(nb * nc)), rowbuf(static_cast<size_t>(nc));
+    std::vector<int32_t> counts(static_cast<size_t>(nb * nc)), cntbuf(static_cast<size_t>(nc));
+    for (int64_t i0 = 1; i0 <= nr;) {
+        const int64_t i1 = std::min(i0 + nb - 1, nr);
+        for (int64_t j = 1; j <= nc; ++j) {
+            double s = 0.0;
+            int32_t c = 0;
+            for (int64_t i = std::max<int64_t>(i0 - m.ly, 1); i <= std::min(i0 + m.ry, nr); ++i) {
+                const double v = A(i - 1, j - 1);
+                if (!std::isnan(v)) { s += v; c += 1; }
+            }
+            for (int64_t i = i0; i <= i1; ++i) {
+                sums[(i - i0) + (j - 1) * nb] = s;
+                counts[(i - i0) + (j - 1) * nb] = c;
+                const int64_t oi = i - m.ly;
+                if (1 <= oi && oi <= nr) {
+                    const double v = A(oi - 1, j - 1);
+                    if (!std::isnan(v)) { s -= v; c -= 1; }
+                }
+                const int64_t ii = i + m.ry + 1;
+                if (ii <= nr) {
+                    const double v = A(ii - 1, j - 1);
+                    if (!std::isnan(v)) { s += v; c += 1; }
+                }
+            }
+        }
+        for (int64_t i = i0; i <= i1; ++i) {
+            for (int64_t j = 1; j <= nc; ++j) {
+                rowbuf[j - 1] = sums[(i - i0) + (j - 1) * nb];
+                cntbuf[j - 1] = counts[(i - i0) + (j - 1) * nb];
+            }
+            double s = 0.0;
+            int64_t c = 0;
+            for (int64_t j = 1; j <= std::min(m.rx + 1, nc); ++j) { s += rowbuf[j - 1]; c += cntbuf[j - 1]; }
+            for (int64_t j = 1; j <= nc; ++j) {
+                out[(i - 1) + (j - 1) * nr] =
+                    c > 0 ? static_cast<float>(s / static_cast<double>(c)) : NAN;
+                const int64_t oj = j - m.lx;
+                if (1 <= oj && oj <= nc) { s -= rowbuf[oj - 1]; c -= cntbuf[oj - 1]; }
+                const int64_t jj = j + m.rx + 1;
+                if (jj <= nc) { s += rowbuf[jj - 1]; c += cntbuf[jj - 1]; }
+            }
+        }
+        i0 = i1 + 1;
+    }
+}
+
+template <class Get>
+void windowmean(Get A, int64_t nr, int64_t nc, int64_t w, bool gaps, float* out) {
+    const int64_t wx = std::min(w, nc), wy = std::min(w, nr);
+    if (gaps) windowmean_masked(A, nr, nc, wx, wy, out);
+    else windowmean_dense(A, nr, nc, wx, wy, out);
+}
+
+// src/preprocess.jl:371-399 -- mask-aware box mean.
+template <class T>
+void masked_boxmean(const T* img, const uint8_t* mask, int64_t nr, int64_t nc, int64_t w,
+                    float* out) {
+    const int64_t n = nr * nc;
+    bool all = true;
+    for (int64_t i = 0; i < n; ++i) all = all && mask[i];
+    if (all) {
+        bool gaps = false;
+        for (int64_t i = 0; i < n && !gaps; ++i) gaps = std::isnan(as_f64(img[i]));
+        windowmean([&](int64_t i, int64_t j) { return as_f64(img[i + j * nr]); }, nr, nc, w,
+                   gaps, out);
+        return;
+    }
+    std::vector<float> masked(static_cast<size_t>(n));
+    for (int64_t i = 0; i < n; ++i) masked[i] = mask[i] ? static_cast<float>(img[i]) : NAN;
+    windowmean([&](int64_t i, int64_t j) { return static_cast<double>(masked[i + j * nr]); },
+               nr, nc, w, true, out);
+}
+
+// src/preprocess.jl:447-460 -- erosion: valid only where the whole (clamped) window is valid.
+void erode_mask(const uint8_t* mask, int64_t nr, int64_t nc, int64_t w, uint8_t* out) {
+    const int64_t n = nr * nc;
+    bool all = true;
+    for (int64_t i = 0; i < n; ++i) all = all && mask[i];
+    if (all) { std::memcpy(out, mask, static_cast<size_t>(n)); return; }
+    const Margins m = margins(std::min(w, nc), std::min(w, nr));
+    std::vector<uint8_t> tmp(static_cast<size_t>(n));
+    for (int64_t j = 0; j < nc; ++j)
+        for (int64_t i = 0; i < nr; ++i) {
+            uint8_t v = 1;
+            for (int64_t q = std::max<int64_t>(i - m.ly, 0); q <= std::min(i + m.ry, nr - 1); ++q)
+                v = v && mask[q + j * nr];
+            tmp[i + j * nr] = v;
+        }
+    for (int64_t j = 0; j < nc; ++j)
+        for (int64_t i = 0; i < nr; ++i) {
+            uint8_t v = 1;
+            for (int64_t q = std::max<int64_t>(j - m.lx, 0); q <= std::min(j + m.rx, nc - 1); ++q)
+                v = v && tmp[i + q * nr];
+            out[i + j * nr] = v;
+        }
+}
+
+// src/preprocess.jl:275-288 -- non-finite outputs become zero and invalid; the mask erodes.
+void filtered(float* out, const uint8_t* mask, int64_t nr, int64_t nc, int64_t w, uint8_t* vout) {
+    erode_mask(mask, nr, nc, w, vout);
+    for (int64_t i = 0; i < nr * nc; ++i)
+        if (!std::isfinite(out[i])) { out[i] = 0.0f; vout[i] = 0; }
+}
+
+// src/preprocess.jl:304-312 -- highpass.
+template <class T>
+void highpass(const T* img, const uint8_t* mask, int64_t nr, int64_t nc, int64_t w, float* out) {
+    masked_boxmean(img, mask, nr, nc, w, out);
+    for (int64_t i = 0; i < nr * nc; ++i)
+        out[i] = (mask[i] && std::isfinite(out[i])) ? static_cast<float>(img[i]) - out[i] : NAN;
+}
+
+// src/preprocess.jl:333-351, 416-438 -- Wallis with the two-pass local deviation.
+template <class T>
+void wallis(const T* img, const uint8_t* mask, int64_t nr, int64_t nc, int64_t w,
+            double min_std, float* out) {
+    const int64_t n = nr * nc;
+    std::vector<float> mean(static_cast<size_t>(n)), dev2(static_cast<size_t>(n)), msd(static_cast<size_t>(n));
+    masked_boxmean(img, mask, nr, nc, w, mean.data());
+    bool gaps = false;
+    for (int64_t i = 0; i < n; ++i) {
+        if (mask[i] && std::isfinite(mean[i])) {
+            const float d = static_cast<float>(img[i]) - mean[i];
+            const float v = d * d;
+            dev2[i] = v;
+            gaps = gaps || std::isnan(v);
+        } else {
+            dev2[i] = NAN;
+            gaps = true;
+        }
+    }
+    windowmean([&](int64_t i, int64_t j) { return static_cast<double>(dev2[i + j * nr]); }, nr,
+               nc, w, gaps, msd.data());
+    // sqrt(max(msd, 0f0)): Julia's max keeps a NaN.
+    for (int64_t i = 0; i < n; ++i)
+        if (!std::isnan(msd[i])) msd[i] = std::sqrt(std::max(msd[i], 0.0f));
+    const float floor_sd = static_cast<float>(min_std);
+    for (int64_t i = 0; i < n; ++i) {
+        if (!mask[i] || !std::isfinite(mean[i]) || !std::isfinite(msd[i])) { out[i] = NAN; continue; }
+        const float s = std::max(msd[i], floor_sd);
+        out[i] = s > 0.0f ? (static_cast<float>(img[i]) - mean[i]) / s : NAN;
+    }
+}
+
+// src/preprocess.jl:546-592 -- _to_uint8: mean +- 3 sd of the valid pixels onto 0..255.
+template <class T>
+void to_uint8(const T* img, const uint8_t* mask, int64_t n, uint8_t* out) {
+    int64_t cnt = 0;
+    double s = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        const double v = as_f64(img[i]);
+        if (mask[i] && std::isfinite(v)) { ++cnt; s += v; }
+    }
+    std::memset(out, 0, static_cast<size_t>(n));
+    if (cnt == 0) return;
+    const double mean = s / static_cast<double>(cnt);
+    double ss = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        const double v = as_f64(img[i]);
+        if (mask[i] && std::isfinite(v)) { const double d = v - mean; ss += d * d; }
+    }
+    const double sd = cnt > 1 ? std::sqrt(ss / static_cast<double>(cnt - 1)) : 0.0;
+    if (sd == 0.0) {
+        for (int64_t i = 0; i < n; ++i) out[i] = mask[i] ? 0x80 : 0x00;
+        return;
+    }
+    const double lo = mean - 3.0 * sd;
+    const double scale = 255.0 / (6.0 * sd);
+    for (int64_t i = 0; i < n; ++i) {
+        const double v = as_f64(img[i]);
+        if (!mask[i] || !std::isfinite(v)) { out[i] = 0; continue; }
+        double x = (v - lo) * scale;
+        x = x < 0.0 ? 0.0 : (x > 255.0 ? 255.0 : x);
+        out[i] = static_cast<uint8_t>(std::nearbyint(x));  // round half to even
+    }
+}
+
+// One image through preprocess then quantize (src/api.jl:305-306).
+// pre: 0 none, 1 highpass, 2 wallis; quant: 0 none, 1 uint8. Output element type: uint8 for
+// quant 1; float32 when a filter ran; otherwise the input type (a copy, non-finite floats
+// replaced by zero, src/preprocess.jl:492-507).
+template <class T>
+void prepare_one(const T* img, const uint8_t* mask, int64_t nr, int64_t nc, int pre, int64_t w,
+                 double min_std, int quant, void* out, uint8_t* vout) {
+    const int64_t n = nr * nc;
+    if (pre == 0) {
+        std::memcpy(vout, mask, static_cast<size_t>(n));
+        if (quant == 1) { to_uint8(img, mask, n, static_cast<uint8_t*>(out)); return; }
+        T* o = static_cast<T*>(out);
+        for (int64_t i = 0; i < n; ++i) {
+            const T v = img[i];
+            o[i] = std::isfinite(as_f64(v)) ? v : T(0);
+        }
+        return;
+    }
+    std::vector<float> f(static_cast<size_t>(n));
+    if (pre == 1) highpass(img, mask, nr, nc, w, f.data());
+    else wallis(img, mask, nr, nc, w, min_std, f.data());
+    filtered(f.data(), mask, nr, nc, w, vout);
+    if (quant == 1) {
+        std::vector<uint8_t> v2(vout, vout + n);
+        to_uint8(f.data(), v2.data(), n, static_cast<uint8_t*>(out));
+    } else {
+        std::memcpy(out, f.data(), static_cast<size_t>(n) * 4);
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -472,6 +733,30 @@ int or_track(const void* ref, const void* sec, const uint8_t* refv, const uint8_
                               nthreads);
         default: return -1;
     }
+}
+
+// preprocess + quantize of one image (src/api.jl:305-306; src/preprocess.jl). `mask` may be
+// NULL (finiteness for float types, all-valid otherwise). `out` must hold nrows*ncols
+// elements of the output type (uint8 when quant = 1, float32 when a filter ran, else the
+// input type); `vout` receives the output mask.
+int or_prepare(const void* img, const uint8_t* mask, int64_t nrows, int64_t ncols, int dtype,
+               int pre, int64_t width, double min_std, int quant, void* out, uint8_t* vout) {
+    const int64_t n = nrows * ncols;
+    std::vector<uint8_t> m(static_cast<size_t>(n), 1);
+    auto run = [&](auto* p) {
+        if (mask) std::memcpy(m.data(), mask, static_cast<size_t>(n));
+        else for (int64_t i = 0; i < n; ++i) m[i] = std::isfinite(as_f64(p[i])) ? 1 : 0;
+        prepare_one(p, m.data(), nrows, ncols, pre, width, min_std, quant, out, vout);
+    };
+    switch (dtype) {
+        case OR_U8: run(static_cast<const uint8_t*>(img)); break;
+        case OR_U16: run(static_cast<const uint16_t*>(img)); break;
+        case OR_F32: run(static_cast<const float*>(img)); break;
+        case OR_I16: run(static_cast<const int16_t*>(img)); break;
+        case OR_F64: run(static_cast<const double*>(img)); break;
+        default: return -1;
+    }
+    return 0;
 }
 
 int or_max_threads(void) {

@@ -53,6 +53,8 @@ def lib():
         L.or_subpixel_peak.restype = None
         L.or_track.argtypes = [p, p, p, p, i64, i64, i32] + [p] * 8 + [i64, i32, i32] + [p] * 4 + [i32]
         L.or_track.restype = i32
+        L.or_prepare.argtypes = [p, p, i64, i64, i32, i32, i64, ctypes.c_double, i32, p, p]
+        L.or_prepare.restype = i32
         L.or_max_threads.argtypes = []
         L.or_max_threads.restype = i32
         _lib = L
@@ -157,6 +159,28 @@ def track(reference, secondary, points, upsampling: int = 64, measure: str = "zn
     if rc != 0:
         raise ValueError(f"or_track failed with {rc}")
     return dx, dy, corr, searched.astype(bool)
+
+
+PREPROCESS = {"none": 0, "highpass": 1, "wallis": 2}
+QUANTIZE = {"none": 0, "uint8": 1}
+
+
+def prepare(img, mask=None, preprocess: str = "highpass", width: int = 5, min_std: float = 0.0,
+            quantize: str = "uint8"):
+    """preprocess then quantize one image (src/api.jl:305-306): returns (image, mask)."""
+    a = _f(img)
+    nr, nc = a.shape
+    m = None if mask is None else _f(mask, np.uint8)
+    pre, q = PREPROCESS[preprocess], QUANTIZE[quantize]
+    odt = np.uint8 if q == 1 else (np.float32 if pre else a.dtype)
+    out = np.empty((nr, nc), dtype=odt, order="F")
+    vout = np.empty((nr, nc), dtype=np.uint8, order="F")
+    rc = lib().or_prepare(_ptr(a), _ptr(m) if m is not None else None, nr, nc,
+                          DTYPE_CODES[a.dtype], pre, int(width), float(min_std), q, _ptr(out),
+                          _ptr(vout))
+    if rc != 0:
+        raise ValueError("unsupported dtype")
+    return out, vout.astype(bool)
 
 
 def max_threads() -> int:
