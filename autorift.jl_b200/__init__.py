@@ -10,13 +10,13 @@ from .methods import (GardnerFilter, Highpass, NCC, NoOutlierFilter, NoPreproces
                       params, upsampling)
 from .points import (PointSet, gridpoints, gridpoints_xy, nsearchable, npoints, pointset,
                      sanitize)
-from .track import (DisplacementField, ImagePair, correlate, displacement_field, nmeasured,
-                    refine_patches, track)
+from .track import (DisplacementField, ImagePair, PreparedPair, correlate, displacement_field,
+                    nmeasured, prepare, refine_patches, track)
 
 __all__ = [
     "GardnerFilter", "Highpass", "NCC", "NoOutlierFilter", "NoPreprocess", "NoQuantize",
     "NoRefine", "Params", "PyramidRefine", "QuantizeUInt8", "Wallis", "ZNCC", "chip_sizes",
     "params", "upsampling", "PointSet", "gridpoints", "gridpoints_xy", "nsearchable", "npoints",
     "pointset", "sanitize", "DisplacementField", "ImagePair", "correlate", "displacement_field",
-    "nmeasured", "refine_patches", "track",
+    "nmeasured", "refine_patches", "track", "PreparedPair", "prepare",
 ]

@@ -1204,3 +1204,4 @@ cudaError_t launch_refine_patches(const float* patches, int64_t count, int up, i
 }
 
 }  // namespace ar
+

@@ -1,0 +1,191 @@
+# AutoRIFTGPU: the Julia side of libautorift_gpu's C ABI (include/autorift_gpu.h).
+#
+# A drop-in for AutoRIFT.jl's correlator: `track!` and `prepare` with the reference's own types
+# (ImagePair, PointSet, Params, DisplacementField), computed on a B200 through `ccall`. The FFI
+# idiom is the reference's FFTW binding (src/plans.jl:271-312): a `const` library path, raw
+# `Ptr{Cvoid}` handles cached under a `ReentrantLock`, no finalizers on the hot path, and a
+# non-zero status turned into a Julia exception naming the failure.
+#
+# Load after AutoRIFT:
+#     using AutoRIFT; include("AutoRIFTGPU.jl"); using .AutoRIFTGPU
+#     out = AutoRIFTGPU.track(pair, pts, p)          # same result type as AutoRIFT.track
+
+module AutoRIFTGPU
+
+using AutoRIFT
+using AutoRIFT: ImagePair, PointSet, Params, DisplacementField, displacement_field,
+                ZNCC, NCC, NoRefine, PyramidRefine, upsampling, scatter,
+                Highpass, Wallis, NoPreprocess, QuantizeUInt8, NoQuantize
+
+const LIB = get(ENV, "AUTORIFT_GPU_LIB", joinpath(@__DIR__, "..", "libautorift_gpu.so"))
+
+const AR_OK = Cint(0)
+const AR_U8, AR_U16, AR_F32, AR_I16 = Cint(0), Cint(1), Cint(2), Cint(3)
+const AR_ZNCC, AR_NCC = Cint(0), Cint(1)
+const AR_PRE_NONE, AR_PRE_HIGHPASS, AR_PRE_WALLIS = Cint(0), Cint(1), Cint(2)
+const AR_QUANT_NONE, AR_QUANT_UINT8 = Cint(0), Cint(1)
+
+# `ar_points` (include/autorift_gpu.h): the eight PointSet fields, flattened, and the count.
+struct ArPoints
+    x::Ptr{Float64}
+    y::Ptr{Float64}
+    radius_x::Ptr{Int64}
+    radius_y::Ptr{Int64}
+    dx_prior::Ptr{Float64}
+    dy_prior::Ptr{Float64}
+    chip_size_x::Ptr{Int64}
+    chip_size_y::Ptr{Int64}
+    n::Int64
+end
+
+struct ArPrepareOpts
+    preprocess::Cint
+    width::Cint
+    min_std::Float64
+    quantize::Cint
+end
+
+# One context per device, created on first use (the plan cache's role, src/plans.jl:25-47).
+const CTX_LOCK = ReentrantLock()
+const CTXS = Dict{Int,Ptr{Cvoid}}()
+
+function context(device::Integer = 0)
+    lock(CTX_LOCK) do
+        get!(CTXS, Int(device)) do
+            h = Ref{Ptr{Cvoid}}(C_NULL)
+            rc = ccall((:ar_ctx_create, LIB), Cint, (Cint, Ref{Ptr{Cvoid}}), device, h)
+            rc == AR_OK || error("ar_ctx_create($device) failed ($rc): no usable CUDA device")
+            h[]
+        end
+    end
+end
+
+function check(ctx::Ptr{Cvoid}, rc::Cint, what::AbstractString)
+    rc == AR_OK && return nothing
+    buf = Vector{UInt8}(undef, 512)
+    ccall((:ar_last_error, LIB), Cint, (Ptr{Cvoid}, Ptr{UInt8}, Csize_t), ctx, buf, length(buf))
+    msg = unsafe_string(pointer(buf))
+    rc == 2 && throw(DimensionMismatch("$what: $msg"))
+    rc == 1 && throw(ArgumentError("$what: $msg"))
+    error("$what failed ($rc): $msg")
+end
+
+eltype_code(::Type{UInt8}) = AR_U8
+eltype_code(::Type{UInt16}) = AR_U16
+eltype_code(::Type{Int16}) = AR_I16
+eltype_code(::Type{Float32}) = AR_F32
+eltype_code(T::Type) = throw(ArgumentError(
+    "element type $T has no GPU correlator; use UInt8, UInt16, Int16 or Float32"))
+
+measure_code(::ZNCC) = AR_ZNCC
+measure_code(::NCC) = AR_NCC
+measure_code(m) = throw(ArgumentError("$(typeof(m)) has no GPU implementation"))
+
+# A device-resident pair, keyed on the identity of the arrays it was made from: the same
+# `===` reuse the reference's Cache makes (src/api.jl:325-335).
+mutable struct DevicePair
+    handle::Ptr{Cvoid}
+    ctx::Ptr{Cvoid}
+end
+
+const PAIR_LOCK = ReentrantLock()
+const PAIRS = IdDict{Any,DevicePair}()
+
+function upload(pair::ImagePair, ctx::Ptr{Cvoid})
+    key = (pair.reference, pair.secondary, pair.reference_valid, pair.secondary_valid)
+    lock(PAIR_LOCK) do
+        get!(PAIRS, key) do
+            T = eltype(pair.reference)
+            ref = collect(pair.reference)          # dense column-major copies
+            sec = collect(pair.secondary)
+            rv = collect(pair.reference_valid)     # Matrix{Bool}: one byte per pixel
+            sv = collect(pair.secondary_valid)
+            h = Ref{Ptr{Cvoid}}(C_NULL)
+            nr, nc = size(ref)
+            rc = ccall((:ar_pair_upload, LIB), Cint,
+                       (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{UInt8}, Ptr{UInt8}, Int64,
+                        Int64, Cint, Ref{Ptr{Cvoid}}),
+                       ctx, ref, sec, rv, sv, nr, nc, eltype_code(T), h)
+            check(ctx, rc, "ar_pair_upload")
+            DevicePair(h[], ctx)
+        end
+    end
+end
+
+"""
+    AutoRIFTGPU.track!(out, pair, pts, p; subpixel = p.subpixel, measure = first(p.similarity))
+
+`AutoRIFT.track!` (src/track.jl:103-152) on the GPU: same arguments, same semantics, same
+`DisplacementField` written in place.
+"""
+function track!(out::DisplacementField, pair::ImagePair, pts::PointSet, p::Params;
+                subpixel = p.subpixel, measure = first(p.similarity), device::Integer = 0)
+    length(out) == length(pts) || throw(DimensionMismatch(
+        "output has $(length(out)) points but the point set has $(length(pts))"))
+    ctx = context(device)
+    dp = upload(pair, ctx)
+    flat = scatter(pts)
+    x, y = collect(flat.x), collect(flat.y)
+    rx, ry = collect(flat.radius_x), collect(flat.radius_y)
+    dx0, dy0 = collect(flat.dx_prior), collect(flat.dy_prior)
+    csx, csy = collect(flat.chip_size_x), collect(flat.chip_size_y)
+    n = length(x)
+    dx = Vector{Float32}(undef, n)
+    dy = Vector{Float32}(undef, n)
+    cc = Vector{Float32}(undef, n)
+    sr = Vector{UInt8}(undef, n)
+    GC.@preserve x y rx ry dx0 dy0 csx csy begin
+        P = Ref(ArPoints(pointer(x), pointer(y), pointer(rx), pointer(ry), pointer(dx0),
+                         pointer(dy0), pointer(csx), pointer(csy), n))
+        rc = ccall((:ar_track, LIB), Cint,
+                   (Ptr{Cvoid}, Ptr{Cvoid}, Ref{ArPoints}, Cint, Cint, Ptr{Float32},
+                    Ptr{Float32}, Ptr{Float32}, Ptr{UInt8}),
+                   ctx, dp.handle, P, upsampling(subpixel), measure_code(measure), dx, dy, cc, sr)
+        check(ctx, rc, "ar_track")
+    end
+    vec(out.dx) .= dx
+    vec(out.dy) .= dy
+    vec(out.correlation) .= cc
+    vec(out.searched) .= sr .!= 0
+    return out
+end
+
+track(pair::ImagePair, pts::PointSet, p::Params; kw...) =
+    track!(displacement_field(pts), pair, pts, p; kw...)
+
+prepare_opts(m::NoPreprocess, q) = ArPrepareOpts(AR_PRE_NONE, 0, 0.0, quant_code(q))
+prepare_opts(m::Highpass, q) = ArPrepareOpts(AR_PRE_HIGHPASS, m.width, 0.0, quant_code(q))
+prepare_opts(m::Wallis, q) = ArPrepareOpts(AR_PRE_WALLIS, m.width, m.min_std, quant_code(q))
+prepare_opts(m, q) = throw(ArgumentError("$(typeof(m)) has no GPU implementation"))
+quant_code(::QuantizeUInt8) = AR_QUANT_UINT8
+quant_code(::NoQuantize) = AR_QUANT_NONE
+
+"""
+    AutoRIFTGPU.prepare(pair, p) -> ImagePair
+
+`_prepare` (src/api.jl:305-311) on the GPU: preprocess then quantize each image, returned as a
+host `ImagePair` of the correlation element type with the filtered masks.
+"""
+function prepare(pair::ImagePair, p::Params; device::Integer = 0)
+    ctx = context(device)
+    dp = upload(pair, ctx)
+    opts = Ref(prepare_opts(p.preprocess, p.quantize))
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    rc = ccall((:ar_prepare, LIB), Cint,
+               (Ptr{Cvoid}, Ptr{Cvoid}, Ref{ArPrepareOpts}, Ref{Ptr{Cvoid}}), ctx, dp.handle, opts, h)
+    check(ctx, rc, "ar_prepare")
+    dt = Ref{Cint}(0); nr = Ref{Int64}(0); nc = Ref{Int64}(0)
+    check(ctx, ccall((:ar_pair_info, LIB), Cint,
+                     (Ptr{Cvoid}, Ref{Cint}, Ref{Int64}, Ref{Int64}), h[], dt, nr, nc), "ar_pair_info")
+    T = dt[] == AR_U8 ? UInt8 : dt[] == AR_F32 ? Float32 : dt[] == AR_U16 ? UInt16 : Int16
+    r = Matrix{T}(undef, nr[], nc[]); s = similar(r)
+    rv = Matrix{Bool}(undef, nr[], nc[]); sv = similar(rv)
+    rc = ccall((:ar_pair_download, LIB), Cint,
+               (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Bool}, Ptr{Bool}),
+               ctx, h[], r, s, rv, sv)
+    ccall((:ar_pair_destroy, LIB), Cint, (Ptr{Cvoid},), h[])
+    check(ctx, rc, "ar_pair_download")
+    return ImagePair(r, s, rv, sv)
+end
+
+end # module

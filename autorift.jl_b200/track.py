@@ -95,6 +95,14 @@ class _DevicePair:
         self.ctx = ctx
         self.handle = handle
 
+    def info(self):
+        dt = ctypes.c_int()
+        nr = ctypes.c_int64()
+        nc = ctypes.c_int64()
+        self.ctx.check(self.ctx.lib.ar_pair_info(self.handle, ctypes.byref(dt), ctypes.byref(nr),
+                                                 ctypes.byref(nc)))
+        return dt.value, (nr.value, nc.value)
+
     def __del__(self):
         try:
             if self.handle:
@@ -102,6 +110,63 @@ class _DevicePair:
                 self.handle = None
         except Exception:
             pass
+
+
+_NP_OF = {_lib.AR_U8: np.uint8, _lib.AR_U16: np.uint16, _lib.AR_F32: np.float32,
+          _lib.AR_I16: np.int16}
+
+
+class PreparedPair:
+    """A filtered and quantised pair resident on the device: the `prepared` ImagePair of the
+    reference's Cache (src/api.jl:30-44), produced by `prepare`."""
+
+    def __init__(self, dev: _DevicePair):
+        self._dev = dev
+        self.dtype_code, self.shape = dev.info()
+        self.dtype = np.dtype(_NP_OF[self.dtype_code])
+
+    def device(self, ctx):
+        if ctx is not self._dev.ctx:
+            raise ValueError("the prepared pair belongs to another context")
+        return self._dev
+
+    def download(self):
+        """(reference, secondary, reference_valid, secondary_valid) as host arrays."""
+        nr, nc = self.shape
+        out = [np.empty((nr, nc), self.dtype, order="F") for _ in range(2)]
+        masks = [np.empty((nr, nc), np.uint8, order="F") for _ in range(2)]
+        ctx = self._dev.ctx
+        ctx.check(ctx.lib.ar_pair_download(ctx.handle, self._dev.handle, out[0].ctypes.data,
+                                           out[1].ctypes.data, masks[0].ctypes.data,
+                                           masks[1].ctypes.data))
+        return out[0], out[1], masks[0].astype(bool), masks[1].astype(bool)
+
+
+def prepare_options(p: Params) -> "_lib.ArPrepareOpts":
+    """The `ar_prepare_opts` of a parameter set's preprocess and quantize methods."""
+    from .methods import Highpass, NoPreprocess, NoQuantize, QuantizeUInt8, Wallis
+    pre = p.preprocess
+    if isinstance(pre, NoPreprocess):
+        kind, width, floor = _lib.AR_PRE_NONE, 0, 0.0
+    elif isinstance(pre, Highpass):
+        kind, width, floor = _lib.AR_PRE_HIGHPASS, pre.width, 0.0
+    elif isinstance(pre, Wallis):
+        kind, width, floor = _lib.AR_PRE_WALLIS, pre.width, pre.min_std
+    else:
+        raise ValueError(f"{type(pre).__name__} has no GPU implementation")
+    q = _lib.AR_QUANT_UINT8 if isinstance(p.quantize, QuantizeUInt8) else _lib.AR_QUANT_NONE
+    return _lib.ArPrepareOpts(kind, width, float(floor), q)
+
+
+def prepare(pair: ImagePair, p: Params | None = None, ctx=None) -> PreparedPair:
+    """Filter and quantise a pair on the device (`_prepare`, src/api.jl:305-311)."""
+    p = p if p is not None else make_params()
+    ctx = ctx or _lib.default_context()
+    raw = pair.device(ctx)
+    out = ctypes.c_void_p()
+    opts = prepare_options(p)
+    ctx.check(ctx.lib.ar_prepare(ctx.handle, raw.handle, ctypes.byref(opts), ctypes.byref(out)))
+    return PreparedPair(_DevicePair(ctx, out))
 
 
 @dataclass
@@ -147,9 +212,10 @@ def _measure_code(m) -> int:
                      "with :zncc or :ncc")
 
 
-def track(pair: ImagePair, pts: PointSet, p: Params | None = None, *, subpixel=None,
+def track(pair, pts: PointSet, p: Params | None = None, *, subpixel=None,
           measure=None, ctx: "_lib.Context | None" = None) -> DisplacementField:
-    """Correlate `pair` at every searchable point of `pts` (src/track.jl:103-160)."""
+    """Correlate `pair` (an ImagePair, uploaded on first use, or a PreparedPair already on the
+    device) at every searchable point of `pts` (src/track.jl:103-160)."""
     p = p if p is not None else make_params()
     sub = p.subpixel if subpixel is None else subpixel
     meas = p.similarity[0] if measure is None else measure
