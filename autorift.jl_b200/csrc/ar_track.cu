@@ -28,6 +28,7 @@
 #include <climits>
 #include <cmath>
 #include <cstdint>
+#include <mutex>
 #include <string>
 
 #include "ar_internal.cuh"
@@ -1205,3 +1206,137 @@ cudaError_t launch_refine_patches(const float* patches, int64_t count, int up, i
 
 }  // namespace ar
 
+// ---------------------------------------------------------------------------------------------
+// Allocation-free track entry point.
+//
+// Some callers cannot allocate device memory at the time they correlate: a host that owns the
+// whole device pool and hands out only the buffers it planned (an embedded or real-time
+// service with a fixed memory budget), code running under another framework's allocator, or
+// a caller that must not trigger cudaMalloc's implicit device synchronisation in the middle
+// of a pipeline. For them the track pass can run with its scratch -- the refinement queue and
+// the pass-geometry words -- in a fixed array in this file instead of context-owned buffers.
+//
+// The array is sized for kStaticMaxPoints points per call (about 3.8 MB, held by every GPU
+// that loads the library until the process exits). Calls share it and it keeps the last
+// call's contents; the queue counter and the geometry words are reset by every call before
+// use. Two calls that overlap on the GPU (different streams, or different host threads) race
+// on it and must not be issued.
+
+namespace ar {
+namespace {
+
+constexpr int64_t kStaticMaxPoints = 32768;
+constexpr size_t kStaticGeomOff = 0;                                   // 8 x int64
+constexpr size_t kStaticCountOff = 64;                                 // int
+constexpr size_t kStaticPointOff = 256;                                // int64 per point
+constexpr size_t kStaticOriginOff = kStaticPointOff + 8 * kStaticMaxPoints;   // 2 x int32
+constexpr size_t kStaticPatchOff = kStaticOriginOff + 8 * kStaticMaxPoints;   // 25 x float
+constexpr size_t kStaticBytes = kStaticPatchOff + 100 * kStaticMaxPoints;
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
+
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mu;
+unsigned char* g_static_addr[kStaticMaxDevices] = {};
+
+// The device address of g_static_scratch on the current device, looked up once per device.
+cudaError_t static_scratch(unsigned char** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kStaticMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    if (!g_static_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess) return e;
+        g_static_addr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_static_addr[dev];
+    return cudaSuccess;
+}
+
+void static_message(char* buf, size_t size, const char* msg) {
+    if (!buf || size == 0) return;
+    size_t n = 0;
+    while (msg[n] && n + 1 < size) {
+        buf[n] = msg[n];
+        ++n;
+    }
+    buf[n] = '\0';
+}
+
+}  // namespace
+}  // namespace ar
+
+extern "C" int ar_track_device_static(const void* ref, const void* sec, const uint8_t* valid,
+                                      int64_t nrows, int64_t ncols, int dtype,
+                                      const ar_points* pts, int upsampling, int measure,
+                                      float* dx, float* dy, float* correlation,
+                                      uint8_t* searched, void* stream, char* err,
+                                      size_t err_size) {
+    using namespace ar;
+    if (!ref || !sec || !valid || !pts || nrows <= 0 || ncols <= 0) {
+        static_message(err, err_size, "null or empty input");
+        return AR_ERR_ARG;
+    }
+    if (pts->n < 0 || pts->n > kStaticMaxPoints) {
+        static_message(err, err_size,
+                       "point count outside [0, 32768], the capacity of the static scratch; "
+                       "split the point set or use ar_track_device");
+        return AR_ERR_SIZE;
+    }
+    if (pts->n > 0 && (!dx || !dy || !correlation || !searched || !pts->x || !pts->y ||
+                       !pts->radius_x || !pts->radius_y || !pts->dx_prior || !pts->dy_prior ||
+                       !pts->chip_size_x || !pts->chip_size_y)) {
+        static_message(err, err_size, "null point-set field or output");
+        return AR_ERR_ARG;
+    }
+    if (upsampling < 1 || upsampling > 128 || (upsampling & (upsampling - 1))) {
+        static_message(err, err_size, "`upsampling` must be 1 or a power of 2 up to 128");
+        return AR_ERR_ARG;
+    }
+    if (measure != AR_ZNCC && measure != AR_NCC) {
+        static_message(err, err_size, "unknown measure");
+        return AR_ERR_ARG;
+    }
+    if (dtype != AR_U8 && dtype != AR_U16 && dtype != AR_I16 && dtype != AR_F32) {
+        static_message(err, err_size, "unsupported element type");
+        return AR_ERR_UNSUPPORTED;
+    }
+    if (pts->n == 0) return AR_OK;
+    unsigned char* base = nullptr;
+    cudaError_t e = static_scratch(&base);
+    if (e != cudaSuccess) {
+        static_message(err, err_size, cudaGetErrorString(e));
+        return AR_ERR_CUDA;
+    }
+    // A view of the static array in the scratch layout the track launch expects. Its capacity
+    // covers the call, so the launch allocates nothing; timing stays off (no events).
+    TrackScratch view;
+    view.geom = reinterpret_cast<int64_t*>(base + kStaticGeomOff);
+    view.sub_count = reinterpret_cast<int*>(base + kStaticCountOff);
+    view.sub_point = reinterpret_cast<int64_t*>(base + kStaticPointOff);
+    view.sub_origin = reinterpret_cast<int32_t*>(base + kStaticOriginOff);
+    view.sub_patch = reinterpret_cast<float*>(base + kStaticPatchOff);
+    view.capacity = kStaticMaxPoints;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    DevPoints dp{pts->x, pts->y, pts->radius_x, pts->radius_y, pts->dx_prior, pts->dy_prior,
+                 pts->chip_size_x, pts->chip_size_y, pts->n};
+    PassGeometry geom;
+    e = pass_geometry_device(dp, nrows, ncols, view, s, &geom);
+    int num_sms = 148;
+    int dev = 0;
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
+    std::string msg;
+    DevOutputs out{dx, dy, correlation, searched};
+    if (e == cudaSuccess)
+        e = launch_track(dtype, ref, sec, valid, nrows, ncols, dp, geom, upsampling, measure, out,
+                         view, num_sms, s, &msg);
+    if (e != cudaSuccess) {
+        static_message(err, err_size, msg.empty() ? cudaGetErrorString(e) : msg.c_str());
+        return msg.empty() ? AR_ERR_CUDA : AR_ERR_UNSUPPORTED;
+    }
+    return AR_OK;
+}

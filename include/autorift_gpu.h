@@ -127,6 +127,31 @@ int ar_track_device(ar_ctx* ctx, const ar_pair* pair, const ar_points* pts_dev,
                     float* correlation_dev, uint8_t* searched_dev, void* stream);
 
 /*
+ * ar_track_device without any device allocation. No counterpart in the reference: it exists
+ * for callers that cannot allocate device memory when they correlate -- a host that owns the
+ * device pool and hands out only planned buffers (a fixed-budget or real-time service), code
+ * running under another framework's allocator, or a pipeline that must not hit cudaMalloc's
+ * implicit synchronisation. The caller passes device pointers for everything it owns: the
+ * images and the combined validity mask (nrows x ncols, column-major, `dtype`), the point
+ * set (as in ar_track_device) and the outputs. No context is needed; the kernels run on
+ * `stream` (NULL is the legacy default stream) of the current device.
+ *
+ * The pass's scratch (the sub-pixel refinement queue and the pass-geometry words) lives in a
+ * static device array of this library sized for at most 32768 points per call (about 3.8 MB,
+ * resident on every GPU that loads the library until the process exits). Larger point sets
+ * return AR_ERR_SIZE; split them. Every call shares the array and resets the parts that must
+ * start at zero; two calls that overlap on the GPU (other streams or host threads) race on it
+ * and must not be issued. The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call before any stream
+ * capture. Like ar_track_device, one small device-to-host read of the pass geometry
+ * synchronises the stream. `err` (may be NULL) receives a message on failure.
+ */
+int ar_track_device_static(const void* ref, const void* sec, const uint8_t* valid, int64_t nrows,
+                           int64_t ncols, int dtype, const ar_points* pts_dev, int upsampling,
+                           int measure, float* dx_dev, float* dy_dev, float* correlation_dev,
+                           uint8_t* searched_dev, void* stream, char* err, size_t err_size);
+
+/*
  * The surface of one chip against one search window (correlate!, src/correlate.jl:528-557),
  * for host arrays: `search` is (ch+2ry-1) x (cw+2rx-1), `chip` ch x cw, `surface` 2ry x 2rx,
  * all column-major of `dtype`/float. `degenerate` receives 1 for a constant chip

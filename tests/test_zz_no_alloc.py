@@ -1,0 +1,101 @@
+"""The allocation-free track entry point (ar_track_device_static) against ar_track_device.
+
+ar_track_device_static is for callers that cannot allocate device memory when they
+correlate; it keeps the pass's scratch in a static device array of the library instead of
+context-owned buffers. This file checks, through the C ABI, that two calls in a row give the
+same dx, dy, correlation and searched as the context-based entry point on the same device
+inputs (bit-identical: the same kernels run on the same data), and that point sets beyond the
+array's capacity are rejected. It sets up everything it needs, so it runs alone in a fresh
+process as well as after the other tests; it is named to be collected last.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _device_points(torch, ar, pts, dev):
+    cols = {f: torch.from_numpy(pts.flat(f)).to(dev) for f in ar.points.FIELDS}
+    st = ar._lib.ArPoints(*(cols[f].data_ptr() for f in ar.points.FIELDS), len(pts))
+    return st, cols
+
+
+def _outputs(torch, n, dev):
+    return [torch.full((n,), 7.0, dtype=torch.float32, device=dev) for _ in range(3)] + [
+        torch.full((n,), 9, dtype=torch.uint8, device=dev)]
+
+
+def _run_context(ar, ctx, pair_handle, st, up, outs, stream):
+    ctx.check(ctx.lib.ar_track_device(ctx.handle, pair_handle, ctypes.byref(st), up,
+                                      ar._lib.AR_ZNCC, *(o.data_ptr() for o in outs),
+                                      ctypes.c_void_p(stream)))
+
+
+def _run_static(ar, lib, dref, dsec, dvalid, shape, st, up, outs, stream):
+    err = ctypes.create_string_buffer(256)
+    rc = lib.ar_track_device_static(dref.data_ptr(), dsec.data_ptr(), dvalid.data_ptr(),
+                                    shape[0], shape[1], ar._lib.AR_U8, ctypes.byref(st), up,
+                                    ar._lib.AR_ZNCC, *(o.data_ptr() for o in outs),
+                                    ctypes.c_void_p(stream), err, 256)
+    assert rc == 0, err.value.decode()
+
+
+def test_static_scratch_matches_context_entry_point_twice(ar):
+    import torch
+
+    import __graft_entry__ as ge
+
+    ge._load_build_ext().build()
+    lib = ar._lib.load()
+    ctx = ar._lib.Context(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    ref, sec = ar.synthetic.shifted_pair(320, (4.4, -2.7), seed=41, dtype=np.uint8)
+    rv = np.ones(ref.shape, bool)
+    rv[40:90, 200:260] = False
+    pair = ar.ImagePair(ref, sec, rv, None)
+    dp = pair.device(ctx)
+    # The same images and combined mask as device buffers owned by the caller.
+    dref = torch.from_numpy(np.asfortranarray(ref).ravel(order="F")).to(dev)
+    dsec = torch.from_numpy(np.asfortranarray(sec).ravel(order="F")).to(dev)
+    dvalid = torch.from_numpy(np.asfortranarray(pair.valid()).ravel(order="F").astype(np.uint8)).to(dev)
+
+    cases = [
+        (ar.gridpoints(ref.shape, 12, chip_size=32, search_radius=12), 16),
+        (ar.pointset(np.linspace(-3, 330, 500), np.linspace(5, 300, 500), chip_size=32,
+                     search_radius=10, dx_prior=2.0), 64),
+    ]
+    with torch.cuda.stream(stream):
+        for pts, up in cases:
+            st, keep = _device_points(torch, ar, pts, dev)
+            want = _outputs(torch, len(pts), dev)
+            _run_context(ar, ctx, dp.handle, st, up, want, stream.cuda_stream)
+            for call in range(2):  # two calls in a row share the static scratch
+                got = _outputs(torch, len(pts), dev)
+                _run_static(ar, lib, dref, dsec, dvalid, ref.shape, st, up, got,
+                            stream.cuda_stream)
+                stream.synchronize()
+                for g, w, name in zip(got, want, ("dx", "dy", "correlation", "searched")):
+                    a, b = g.cpu().numpy(), w.cpu().numpy()
+                    same = (a == b) | (np.isnan(a) & np.isnan(b)) if a.dtype.kind == "f" else (a == b)
+                    assert same.all(), f"call {call}, {name}: {np.count_nonzero(~same)} differ"
+                assert bool(got[3].any())
+
+
+def test_static_scratch_rejects_oversized_point_sets(ar):
+    import torch
+
+    import __graft_entry__ as ge
+
+    ge._load_build_ext().build()
+    lib = ar._lib.load()
+    n = 32769
+    st = ar._lib.ArPoints(1, 1, 1, 1, 1, 1, 1, 1, n)  # never dereferenced: rejected first
+    err = ctypes.create_string_buffer(256)
+    rc = lib.ar_track_device_static(1, 1, 1, 64, 64, ar._lib.AR_U8, ctypes.byref(st), 16,
+                                    ar._lib.AR_ZNCC, 1, 1, 1, 1, None, err, 256)
+    assert rc == ar._lib.AR_ERR_SIZE
+    assert b"32768" in err.value
