@@ -10,6 +10,8 @@ from .methods import (GardnerFilter, Highpass, NCC, NoOutlierFilter, NoPreproces
                       params, upsampling)
 from .points import (PointSet, gridpoints, gridpoints_xy, nsearchable, npoints, pointset,
                      sanitize)
+from .api import (Cache, MultichipResult, autorift, autorift_, build_grid, correlate_multichip,
+                  init, reinit_)
 from .track import (DisplacementField, ImagePair, PreparedPair, correlate, displacement_field,
                     nmeasured, prepare, refine_patches, track)
 
@@ -18,5 +20,7 @@ __all__ = [
     "NoRefine", "Params", "PyramidRefine", "QuantizeUInt8", "Wallis", "ZNCC", "chip_sizes",
     "params", "upsampling", "PointSet", "gridpoints", "gridpoints_xy", "nsearchable", "npoints",
     "pointset", "sanitize", "DisplacementField", "ImagePair", "correlate", "displacement_field",
-    "nmeasured", "refine_patches", "track", "PreparedPair", "prepare",
+    "nmeasured", "refine_patches", "track", "PreparedPair", "prepare", "Cache",
+    "MultichipResult", "autorift", "autorift_", "build_grid", "correlate_multichip", "init",
+    "reinit_",
 ]

@@ -31,6 +31,19 @@ class ArPrepareOpts(ctypes.Structure):
                 ("quantize", _i32)]
 
 
+class ArMultichipParams(ctypes.Structure):
+    """`ar_multichip_params`: the Params fields correlate_multichip reads."""
+
+    _fields_ = [("chip_size_base", _i32), ("chip_size_min", _i32), ("chip_size_max", _i32),
+                ("chip_aspect", ctypes.c_double), ("min_search_radius", _i32),
+                ("coarse_stride", _i32), ("coarse_buffer", _i32),
+                ("min_coarse_valid_fraction", ctypes.c_double), ("upsampling", _i32),
+                ("measure", _i32), ("outliers", _i32), ("outlier_window", _i32),
+                ("outlier_iterations", _i32), ("min_agree_fraction", ctypes.c_double),
+                ("agree_tolerance", ctypes.c_double), ("mad_scale", ctypes.c_double),
+                ("fill_window", _i32)]
+
+
 AR_PRE_NONE, AR_PRE_HIGHPASS, AR_PRE_WALLIS = 0, 1, 2
 AR_QUANT_NONE, AR_QUANT_UINT8 = 0, 1
 
@@ -60,9 +73,12 @@ SIGNATURES = {
     "ar_correlate": (_i32, [_p, _p, _p, _i32, _i64, _i64, _i64, _i64, _i32, _p,
                             ctypes.POINTER(_i32)]),
     "ar_refine_patches": (_i32, [_p, _p, _i64, _i32, _p, _p, _p]),
+    "ar_multichip": (_i32, [_p, _p, ctypes.POINTER(ArPoints), _i64, _i64,
+                            ctypes.POINTER(ArMultichipParams), _p, _p, _p, _p, _p]),
     "ar_ctx_set_timing": (_i32, [_p, _i32]),
     "ar_kernel_times": (_i32, [_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
-                               ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+                               ctypes.POINTER(_i64), ctypes.POINTER(_i64),
+                               ctypes.POINTER(ctypes.c_double)]),
     "ar_synchronize": (_i32, [_p]),
 }
 
@@ -119,12 +135,13 @@ class Context:
         self.check(self.lib.ar_ctx_set_timing(self.handle, int(bool(enable))))
 
     def kernel_times(self):
-        """(corr_ms, refine_ms, track_launches, kernel_launches) since the last call."""
-        a, b = ctypes.c_double(), ctypes.c_double()
+        """(corr_ms, refine_ms, track_launches, kernel_launches, corr_flops) since the last
+        call."""
+        a, b, f = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         t, n = _i64(), _i64()
         self.check(self.lib.ar_kernel_times(self.handle, ctypes.byref(a), ctypes.byref(b),
-                                            ctypes.byref(t), ctypes.byref(n)))
-        return a.value, b.value, t.value, n.value
+                                            ctypes.byref(t), ctypes.byref(n), ctypes.byref(f)))
+        return a.value, b.value, t.value, n.value, f.value
 
     def close(self):
         if getattr(self, "handle", None):

@@ -1,0 +1,176 @@
+"""The public API (src/api.jl): `autorift`, the `init` / `reinit!` / `autorift!` cache
+lifecycle, `correlate_multichip` and `MultichipResult` (src/multichip.jl:74-137), on the GPU.
+
+Python spells Julia's `reinit!` and `autorift!` as `reinit_` and `autorift_`.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .methods import (GardnerFilter, NoOutlierFilter, Params, chip_sizes, params as make_params,
+                      upsampling)
+from .points import PointSet, gridpoints
+from .track import ImagePair, PreparedPair, _measure_code, points_struct, prepare
+
+
+@dataclass
+class MultichipResult:
+    """Displacement over the full grid from all chip-size levels (src/multichip.jl:74-80)."""
+
+    dx: np.ndarray
+    dy: np.ndarray
+    correlation: np.ndarray
+    chip_size: np.ndarray
+    interpolated: np.ndarray
+
+    @property
+    def shape(self):
+        return self.dx.shape
+
+    def __len__(self):
+        return int(self.dx.size)
+
+
+def multichip_params(p: Params) -> "_lib.ArMultichipParams":
+    """The `ar_multichip_params` of a parameter set."""
+    o = p.outliers
+    if isinstance(o, GardnerFilter):
+        kind, w, it, fr, tol, mad = 1, o.window, o.iterations, o.min_agree_fraction, o.agree_tolerance, o.mad_scale
+    elif isinstance(o, NoOutlierFilter):
+        kind, w, it, fr, tol, mad = 0, 5, 3, 8 / 25, 0.2, 4.0
+    else:
+        raise ValueError(f"{type(o).__name__} has no GPU implementation")
+    if len(p.similarity) > len(chip_sizes(p)):
+        raise ValueError(f"`similarity` names {len(p.similarity)} measures but there are only "
+                         f"{len(chip_sizes(p))} chip-size levels.")
+    if len({type(m) for m in p.similarity}) > 1:
+        raise ValueError("per-level similarity tuples are not supported on the GPU")
+    return _lib.ArMultichipParams(
+        p.chip_size_base, p.chip_size_min, p.chip_size_max, p.chip_aspect,
+        p.min_search_radius, p.coarse_stride, p.coarse_buffer, p.min_coarse_valid_fraction,
+        upsampling(p.subpixel), _measure_code(p.similarity[0]), kind, w, it, fr, tol, mad,
+        p.fill_window)
+
+
+def correlate_multichip(pair, grid: PointSet, p: Params | None = None, ctx=None) -> MultichipResult:
+    """Correlate `pair` over the gridded `grid` at every chip-size level, finest first
+    (src/multichip.jl:106-137). `pair` is a prepared pair (ImagePair of the correlation
+    element type, or a PreparedPair already on the device)."""
+    p = p if p is not None else make_params()
+    ctx = ctx or _lib.default_context()
+    if grid.ndim != 2:
+        raise ValueError("correlate_multichip needs a gridded PointSet{2}")
+    gr, gc = grid.shape
+    n = gr * gc
+    out = [np.empty(n, np.float32) for _ in range(3)]
+    cs = np.empty(n, np.uint16)
+    it = np.empty(n, np.uint8)
+    if n:
+        dp = pair.device(ctx)
+        st, keep = points_struct(grid)
+        prm = multichip_params(p)
+        ctx.check(ctx.lib.ar_multichip(ctx.handle, dp.handle, ctypes.byref(st), gr, gc,
+                                       ctypes.byref(prm), out[0].ctypes.data, out[1].ctypes.data,
+                                       out[2].ctypes.data, cs.ctypes.data, it.ctypes.data))
+    shp = lambda a: a.reshape((gr, gc), order="F")
+    return MultichipResult(shp(out[0]), shp(out[1]), shp(out[2]), shp(cs), shp(it).astype(bool))
+
+
+def nmeasured(r) -> int:
+    return int(np.count_nonzero(~np.isnan(r.dx)))
+
+
+def build_grid(imagesize, p: Params) -> PointSet:
+    """The grid when the caller gives none (src/api.jl:339-347)."""
+    return gridpoints(imagesize, p.grid_spacing, chip_size=p.chip_size_max,
+                      chip_aspect=p.chip_aspect, search_radius_x=p.search_radius_x,
+                      search_radius_y=p.search_radius_y, dx_prior=p.dx_prior,
+                      dy_prior=p.dy_prior)
+
+
+class Cache:
+    """Prepared state for correlating many pairs with one configuration (src/api.jl:30-44)."""
+
+    def __init__(self, p: Params, raw: ImagePair, prepared: PreparedPair, grid: PointSet, ctx):
+        self.params = p
+        self.raw = raw
+        self.prepared = prepared
+        self.grid = grid
+        self.result = None
+        self.isfresh = True
+        self.ctx = ctx
+
+
+def init(reference, secondary, *, reference_valid=None, secondary_valid=None, ctx=None,
+         **kw) -> Cache:
+    """Prepare to correlate a pair: resolve parameters, filter and quantise on the device,
+    build the grid (src/api.jl:66-76)."""
+    p = make_params(**kw)
+    ctx = ctx or _lib.default_context()
+    raw = ImagePair(reference, secondary, reference_valid, secondary_valid)
+    prepared = prepare(raw, p, ctx)
+    grid = build_grid(raw.shape, p)
+    return Cache(p, raw, prepared, grid, ctx)
+
+
+def reinit_(cache: Cache, *, reference=None, secondary=None, reference_valid=None,
+            secondary_valid=None) -> Cache:
+    """Point the cache at a new pair of the same size (src/api.jl:104-134): an omitted image
+    keeps its value, an omitted mask follows its image, sizes must match."""
+    if reference is None and secondary is None and reference_valid is None and secondary_valid is None:
+        return cache
+    old = cache.raw
+    ref = old.reference if reference is None else reference
+    sec = old.secondary if secondary is None else secondary
+
+    def maskfor(img):
+        if img is old.reference:
+            return old.reference_valid
+        if img is old.secondary:
+            return old.secondary_valid
+        return None
+
+    rv = maskfor(ref) if reference_valid is None else reference_valid
+    sv = maskfor(sec) if secondary_valid is None else secondary_valid
+    if np.shape(ref) != old.shape or np.shape(sec) != old.shape:
+        raise ValueError(f"new images are {np.shape(ref)} and {np.shape(sec)} but the cache was "
+                         f"built for {old.shape}; build a new cache with `init` for a different "
+                         "image size.")
+    cache.raw = ImagePair(ref, sec, rv, sv)
+    cache.prepared = prepare(cache.raw, cache.params, cache.ctx)
+    cache.isfresh = True
+    cache.result = None
+    return cache
+
+
+def autorift_(cache: Cache) -> MultichipResult:
+    """Correlate the cache's pair; idempotent until the next reinit_ (src/api.jl:165-170)."""
+    if not cache.isfresh and cache.result is not None:
+        return cache.result
+    cache.result = correlate_multichip(cache.prepared, cache.grid, cache.params, cache.ctx)
+    cache.isfresh = False
+    return cache.result
+
+
+def autorift(reference, secondary, grid: PointSet | None = None, *, reference_valid=None,
+             secondary_valid=None, ctx=None, **kw):
+    """Displacement between two co-registered images (src/api.jl:210-274).
+
+    With no grid: the full multi-chip-size search over `grid_spacing` points. With a gridded
+    PointSet: the same search over it. With a scattered PointSet: one scale via `track`.
+    """
+    if grid is None:
+        return autorift_(init(reference, secondary, reference_valid=reference_valid,
+                              secondary_valid=secondary_valid, ctx=ctx, **kw))
+    from .track import track
+    p = make_params(**kw)
+    ctx = ctx or _lib.default_context()
+    prepared = prepare(ImagePair(reference, secondary, reference_valid, secondary_valid), p, ctx)
+    if grid.ndim == 2:
+        return correlate_multichip(prepared, grid, p, ctx)
+    return track(prepared, grid, p, ctx=ctx)

@@ -28,6 +28,9 @@ struct ar_ctx {
     // Device buffers for host point sets and outputs, grown on demand.
     void* dbuf = nullptr;
     size_t dbuf_bytes = 0;
+    // Scratch of the multichip search, grown on demand.
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
 };
 
 struct ar_pair {
@@ -240,7 +243,9 @@ int ar_ctx_destroy(ar_ctx* c) {
         for (auto& r : c->scratch.timer.recs)
             for (auto ev : r) c->scratch.timer.pool.push_back(ev);
         for (auto ev : c->scratch.timer.pool) cudaEventDestroy(ev);
+        cudaFree(c->scratch.timer.flops);
         cudaFree(c->dbuf);
+        cudaFree(c->arena);
         if (c->pinned) cudaFreeHost(c->pinned);
         for (auto& ev : c->staged)
             if (ev) cudaEventDestroy(ev);
@@ -607,15 +612,129 @@ int ar_pair_download(ar_ctx* c, const ar_pair* p, void* ref, void* sec, uint8_t*
     return e == cudaSuccess ? AR_OK : cuda_fail(c, e, "ar_pair_download");
 }
 
+int ar_multichip(ar_ctx* c, const ar_pair* p, const ar_points* grid, int64_t gr, int64_t gc,
+                 const ar_multichip_params* prm, float* dx, float* dy, float* corr,
+                 uint16_t* chip, uint8_t* interp) {
+    if (!c || !p || !grid || !prm) return fail(c, AR_ERR_ARG, "null argument");
+    if (p->ctx != c) return fail(c, AR_ERR_ARG, "the pair belongs to another context");
+    if (gr < 0 || gc < 0 || grid->n != gr * gc)
+        return fail(c, AR_ERR_SIZE, "grid extents do not match the point count");
+    const int64_t n = grid->n;
+    if (n == 0) return AR_OK;
+    if (!dx || !dy || !corr || !chip || !interp || !grid->x || !grid->y || !grid->radius_x ||
+        !grid->radius_y || !grid->dx_prior || !grid->dy_prior)
+        return fail(c, AR_ERR_ARG, "null grid field or output");
+    if (!is_pow2(prm->upsampling) || prm->upsampling > 128)
+        return fail(c, AR_ERR_ARG, "`upsampling` must be 1 or a power of 2 up to 128");
+    if (prm->measure != AR_ZNCC && prm->measure != AR_NCC) return fail(c, AR_ERR_ARG, "unknown measure");
+    if (prm->chip_size_base <= 0 || prm->chip_size_max < prm->chip_size_base || prm->coarse_stride <= 0)
+        return fail(c, AR_ERR_ARG, "invalid chip-size levels or coarse stride");
+    for (int64_t k = 0; k < n; ++k)
+        if (!std::isfinite(grid->x[k]) || !std::isfinite(grid->y[k]) ||
+            !std::isfinite(grid->dx_prior[k]) || !std::isfinite(grid->dy_prior[k]))
+            return fail(c, AR_ERR_ARG, "grid coordinates and priors must be finite");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    // Device copies of the six grid fields and the five outputs.
+    const size_t need = static_cast<size_t>(n) * (6 * 8 + 3 * 4 + 2 + 1) + 16 * 256;
+    cudaError_t e = ensure_dbuf(c, need);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ar_multichip: device buffers");
+    const size_t ab = ar::multichip_arena_bytes(gr, gc);
+    if (c->arena_bytes < ab) {
+        cudaFree(c->arena);
+        c->arena = nullptr;
+        c->arena_bytes = 0;
+        e = cudaMalloc(&c->arena, ab);
+        if (e != cudaSuccess) return cuda_fail(c, e, "ar_multichip: scratch");
+        c->arena_bytes = ab;
+    }
+    unsigned char* base = static_cast<unsigned char*>(c->dbuf);
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        off = (off + 255) & ~size_t(255);
+        unsigned char* q = base + off;
+        off += bytes;
+        return q;
+    };
+    ar::MultichipJob J{};
+    double* gx = reinterpret_cast<double*>(take(n * 8));
+    double* gy = reinterpret_cast<double*>(take(n * 8));
+    int64_t* grx = reinterpret_cast<int64_t*>(take(n * 8));
+    int64_t* gry = reinterpret_cast<int64_t*>(take(n * 8));
+    double* gdx0 = reinterpret_cast<double*>(take(n * 8));
+    double* gdy0 = reinterpret_cast<double*>(take(n * 8));
+    J.dx = reinterpret_cast<float*>(take(n * 4));
+    J.dy = reinterpret_cast<float*>(take(n * 4));
+    J.corr = reinterpret_cast<float*>(take(n * 4));
+    J.chip = reinterpret_cast<uint16_t*>(take(n * 2));
+    J.interp = take(n);
+    const void* srcs[6] = {grid->x, grid->y, grid->radius_x, grid->radius_y, grid->dx_prior, grid->dy_prior};
+    void* dsts[6] = {gx, gy, grx, gry, gdx0, gdy0};
+    for (int f = 0; f < 6 && e == cudaSuccess; ++f) e = stage_h2d(c, dsts[f], srcs[f], n * 8);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ar_multichip: upload grid");
+    J.dtype = p->dtype;
+    J.ref = p->ref;
+    J.sec = p->sec;
+    J.valid = p->valid;
+    J.nrows = p->nrows;
+    J.ncols = p->ncols;
+    J.gx = gx;
+    J.gy = gy;
+    J.grx = grx;
+    J.gry = gry;
+    J.gdx0 = gdx0;
+    J.gdy0 = gdy0;
+    J.gr = gr;
+    J.gc = gc;
+    ar::MultichipParams& P = J.P;
+    P.chip_base = prm->chip_size_base;
+    P.chip_min = prm->chip_size_min;
+    P.chip_max = prm->chip_size_max;
+    P.aspect = prm->chip_aspect;
+    P.min_radius = prm->min_search_radius;
+    P.stride = prm->coarse_stride;
+    P.buffer = prm->coarse_buffer;
+    P.min_frac = prm->min_coarse_valid_fraction;
+    P.up = prm->upsampling;
+    P.measure = prm->measure;
+    P.outliers = prm->outliers;
+    P.gwindow = prm->outlier_window;
+    P.giterations = prm->outlier_iterations;
+    P.gfrac = prm->min_agree_fraction;
+    P.gtol = prm->agree_tolerance;
+    P.gmad = prm->mad_scale;
+    P.fill_window = prm->fill_window;
+    J.arena = c->arena;
+    J.arena_bytes = c->arena_bytes;
+    std::string err;
+    e = ar::run_multichip(J, c->scratch, c->num_sms, c->stream, &err);
+    if (e != cudaSuccess)
+        return err.empty() ? cuda_fail(c, e, "ar_multichip") : fail(c, AR_ERR_UNSUPPORTED, err);
+    e = stage_d2h(c, dx, J.dx, n * 4);
+    if (e == cudaSuccess) e = stage_d2h(c, dy, J.dy, n * 4);
+    if (e == cudaSuccess) e = stage_d2h(c, corr, J.corr, n * 4);
+    if (e == cudaSuccess) e = stage_d2h(c, chip, J.chip, n * 2);
+    if (e == cudaSuccess) e = stage_d2h(c, interp, J.interp, n);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ar_multichip: download");
+    return AR_OK;
+}
+
 int ar_ctx_set_timing(ar_ctx* c, int enable) {
     if (!c) return AR_ERR_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
-    c->scratch.timer.enabled = enable != 0;
+    DeviceGuard g(c->device);
+    ar::KernelTimer& T = c->scratch.timer;
+    if (enable && !T.flops) {
+        cudaError_t e = cudaMalloc(&T.flops, sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaMemsetAsync(T.flops, 0, sizeof(unsigned long long), c->stream);
+        if (e != cudaSuccess) return cuda_fail(c, e, "ar_ctx_set_timing");
+    }
+    T.enabled = enable != 0;
     return AR_OK;
 }
 
 int ar_kernel_times(ar_ctx* c, double* corr_ms, double* refine_ms, int64_t* tracks,
-                    int64_t* launches) {
+                    int64_t* launches, double* corr_flops) {
     if (!c) return AR_ERR_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
     DeviceGuard g(c->device);
@@ -633,6 +752,12 @@ int ar_kernel_times(ar_ctx* c, double* corr_ms, double* refine_ms, int64_t* trac
     }
     if (tracks) *tracks = static_cast<int64_t>(T.recs.size());
     if (launches) *launches = T.launches;
+    unsigned long long fl = 0;
+    if (T.flops) {
+        if (e == cudaSuccess) e = cudaMemcpy(&fl, T.flops, sizeof(fl), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemset(T.flops, 0, sizeof(fl));
+    }
+    if (corr_flops) *corr_flops = static_cast<double>(fl);
     T.recs.clear();
     T.launches = 0;
     if (corr_ms) *corr_ms = sc;

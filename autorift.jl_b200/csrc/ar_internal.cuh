@@ -48,6 +48,7 @@ struct KernelTimer {
     std::vector<std::array<cudaEvent_t, 3>> recs;  // before corr, after corr, after refine
     std::vector<cudaEvent_t> pool;
     long long launches = 0;  // kernels this library launched since the last query
+    unsigned long long* flops = nullptr;  // device counter of surface FLOPs (while enabled)
     cudaEvent_t get();
 };
 
@@ -100,6 +101,47 @@ struct PrepareJob {
 size_t quant_stats_bytes();
 int max_filter_width();
 cudaError_t launch_prepare(const PrepareJob& job, cudaStream_t stream, long long* launches);
+
+// The parameters of correlate_multichip (the Params fields src/multichip.jl reads).
+struct MultichipParams {
+    int64_t chip_base, chip_min, chip_max;
+    double aspect;
+    int64_t min_radius, stride, buffer;
+    double min_frac;
+    int up, measure;
+    int outliers;  // 0 NoOutlierFilter, 1 GardnerFilter
+    int64_t gwindow, giterations;
+    double gfrac, gtol, gmad;
+    int64_t fill_window;
+};
+
+// One multichip run: a prepared pair, a gr x gc point grid (device, column-major), outputs
+// (device) and a scratch block of multichip_arena_bytes(gr, gc).
+struct MultichipJob {
+    int dtype;
+    const void* ref;
+    const void* sec;
+    const uint8_t* valid;
+    int64_t nrows, ncols;
+    const double* gx;
+    const double* gy;
+    const int64_t* grx;
+    const int64_t* gry;
+    const double* gdx0;
+    const double* gdy0;
+    int64_t gr, gc;
+    MultichipParams P;
+    float* dx;
+    float* dy;
+    float* corr;
+    uint16_t* chip;
+    uint8_t* interp;
+    void* arena;
+    size_t arena_bytes;
+};
+size_t multichip_arena_bytes(int64_t gr, int64_t gc);
+cudaError_t run_multichip(const MultichipJob& job, TrackScratch& scratch, int num_sms,
+                          cudaStream_t stream, std::string* errmsg);
 
 // Refine `count` patches already on the device.
 cudaError_t launch_refine_patches(const float* patches, int64_t count, int up, int32_t* row,

@@ -192,6 +192,7 @@ struct CorrArgs {
     int32_t* sub_origin;
     float* sub_patch;
     float* surf_out;  // optional: each point's surface, NRS x NCM floats per point
+    unsigned long long* flops;  // optional: algorithmic FLOPs of the surfaces computed
 };
 
 template <typename T>
@@ -455,6 +456,8 @@ __global__ void __launch_bounds__(kCorrThreads, 2) k_corr(const CorrArgs A) {
             }
         }
         __syncthreads();
+        if (A.flops && tid == 0)
+            atomicAdd(A.flops, 2ull * static_cast<unsigned long long>(ch) * cw * nr * nc);
         if (A.surf_out) {
             float* so = A.surf_out + k * static_cast<int64_t>(A.NRS) * A.NCM;
             for (int e = tid; e < nr * nc; e += bd) so[e] = s_surf[(e % nr) + (e / nr) * A.NRS];
@@ -1114,6 +1117,7 @@ cudaError_t launch_track(int dtype, const void* ref, const void* sec, const uint
     A.sub_origin = scratch.sub_origin;
     A.sub_patch = scratch.sub_patch;
     A.surf_out = surf_out;
+    A.flops = scratch.timer.enabled ? scratch.timer.flops : nullptr;
 
     KernelTimer& T = scratch.timer;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;

@@ -230,7 +230,7 @@ def gpu_arm(args):
             e.synchronize()
             total_ms += s.elapsed_time(e)
     torch.cuda.synchronize()
-    corr_ms, refine_ms, tracks, launches = ctx.kernel_times()
+    corr_ms, refine_ms, tracks, launches, corr_flops = ctx.kernel_times()
     ctx.set_timing(False)
     t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
     if dist:
@@ -244,10 +244,14 @@ def gpu_arm(args):
     fin = torch.isfinite(out[0])
     med_dx = float(out[0][fin].median().item()) if fin.any() else float("nan")
 
-    # Roofline of the dominant kernel (the correlation): algorithmic FLOPs per launch over its
-    # event-timed average duration, against the measured cuBLAS FP32 rate.
+    # Roofline of the dominant kernel (the correlation): algorithmic FLOPs per launch (counted
+    # by the kernel: 2 * chip area * surface area per searched point) over its event-timed
+    # average duration, against the measured cuBLAS FP32 rate.
     corr_avg = corr_ms / max(tracks, 1)
-    achieved = flops_per_point() * nsearched / (corr_avg * 1e-3) / 1e12
+    flops_launch = corr_flops / max(tracks, 1)
+    assert abs(flops_launch - flops_per_point() * nsearched) <= 1e-9 * flops_launch + 1, \
+        (flops_launch, flops_per_point() * nsearched)
+    achieved = flops_launch / (corr_avg * 1e-3) / 1e12
     if args.profile:  # an ncu capture: the device steps only
         if rank == 0:
             print(json.dumps({"profile_run": True, "points": n, "ms_per_step": ms_per_step,

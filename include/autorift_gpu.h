@@ -151,6 +151,31 @@ int ar_track_device_static(const void* ref, const void* sec, const uint8_t* vali
                            int measure, float* dx_dev, float* dy_dev, float* correlation_dev,
                            uint8_t* searched_dev, void* stream, char* err, size_t err_size);
 
+/* The parameters correlate_multichip reads (Params, src/types.jl:781-829). */
+typedef struct {
+    int chip_size_base, chip_size_min, chip_size_max; /* levels chip_size_base * 2^k */
+    double chip_aspect;
+    int min_search_radius, coarse_stride, coarse_buffer;
+    double min_coarse_valid_fraction;
+    int upsampling;      /* PyramidRefine factor, or 1 for NoRefine */
+    int measure;         /* AR_ZNCC or AR_NCC */
+    int outliers;        /* 0 NoOutlierFilter, 1 GardnerFilter */
+    int outlier_window, outlier_iterations;
+    double min_agree_fraction, agree_tolerance, mad_scale;
+    int fill_window;
+} ar_multichip_params;
+
+/*
+ * correlate_multichip (src/multichip.jl:106-137) on a prepared pair over a gridded point set
+ * (PointSet{2}, grid_rows x grid_cols, fields flattened column-major; its chip-size fields are
+ * ignored: each level sets them). Host grid and host outputs of grid_rows*grid_cols elements:
+ * the fields of MultichipResult (src/multichip.jl:74-80) -- dx, dy, correlation (NaN where no
+ * level resolved the point), chip_size (0 there) and interpolated (0/1).
+ */
+int ar_multichip(ar_ctx* ctx, const ar_pair* pair, const ar_points* grid, int64_t grid_rows,
+                 int64_t grid_cols, const ar_multichip_params* params, float* dx, float* dy,
+                 float* correlation, uint16_t* chip_size, uint8_t* interpolated);
+
 /*
  * The surface of one chip against one search window (correlate!, src/correlate.jl:528-557),
  * for host arrays: `search` is (ch+2ry-1) x (cw+2rx-1), `chip` ch x cw, `surface` 2ry x 2rx,
@@ -172,14 +197,16 @@ int ar_refine_patches(ar_ctx* ctx, const float* patches, int64_t count, int upsa
 
 /*
  * Kernel timing, for benchmarks: when enabled, every track launch records CUDA events on its
- * stream around the correlation kernel and the refinement kernel. ar_kernel_times waits for
- * the recorded events and returns the summed milliseconds of each kernel, the number of
- * track launches timed and the number of kernels the library launched, then resets. No
- * reference counterpart (the reference times from Julia: benchmark/run.jl).
+ * stream around the correlation kernel and the refinement kernel, and the correlation kernel
+ * counts the algorithmic FLOPs of the surfaces it computes (2 * chip area * surface area per
+ * point). ar_kernel_times waits for the recorded events and returns the summed milliseconds
+ * of each kernel, the number of track launches timed, the number of kernels the library
+ * launched and the FLOP count, then resets. No reference counterpart (the reference times
+ * from Julia: benchmark/run.jl).
  */
 int ar_ctx_set_timing(ar_ctx* ctx, int enable);
 int ar_kernel_times(ar_ctx* ctx, double* corr_ms, double* refine_ms, int64_t* tracks,
-                    int64_t* launches);
+                    int64_t* launches, double* corr_flops);
 
 /* Block until all work the context enqueued has finished. */
 int ar_synchronize(ar_ctx* ctx);

@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #ifdef _OPENMP
@@ -652,6 +653,316 @@ void prepare_one(const T* img, const uint8_t* mask, int64_t nr, int64_t nc, int 
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// The multi-chip-size search: src/multichip.jl:106-422, src/outliers.jl:38-172, the window
+// reductions of src/window.jl:474-637 and src/resample.jl:56-71, 190-325. Grid fields are
+// column-major nr x nc.
+
+struct MCParams {
+    int64_t chip_base, chip_min, chip_max;
+    double aspect;
+    int64_t min_radius, stride, buffer;
+    double min_frac;
+    int up, measure;
+    int outliers;  // 0 NoOutlierFilter, 1 GardnerFilter
+    int64_t gwindow, giterations;
+    double gfrac, gtol, gmad;
+    int64_t fill_window;
+};
+
+// src/window.jl:565-582.
+void insertion_sort(float* b, int64_t n) {
+    for (int64_t k = 1; k < n; ++k) {
+        const float v = b[k];
+        int64_t m = k - 1;
+        while (m >= 0 && b[m] > v) { b[m + 1] = b[m]; --m; }
+        b[m + 1] = v;
+    }
+}
+float sorted_median(const float* b, int64_t n) {
+    return (n % 2 == 1) ? b[(n + 1) / 2 - 1] : (b[n / 2 - 1] + b[n / 2]) / 2.0f;
+}
+
+// src/window.jl:594-619 -- neighbours within tol of the centre (itself included).
+void count_agreeing(const float* A, int64_t nr, int64_t nc, int64_t w, float t, float* out) {
+    const Margins m = margins(std::min(w, nc), std::min(w, nr));
+    for (int64_t j = 0; j < nc; ++j)
+        for (int64_t i = 0; i < nr; ++i) {
+            const float c = A[i + j * nr];
+            if (std::isnan(c)) { out[i + j * nr] = 0.0f; continue; }
+            int64_t n = 0;
+            for (int64_t jj = std::max<int64_t>(j - m.lx, 0); jj <= std::min(j + m.rx, nc - 1); ++jj)
+                for (int64_t ii = std::max<int64_t>(i - m.ly, 0); ii <= std::min(i + m.ry, nr - 1); ++ii)
+                    if (std::fabs(A[ii + jj * nr] - c) < t) ++n;
+            out[i + j * nr] = static_cast<float>(n);
+        }
+}
+
+// src/window.jl:501-563 -- median and MAD over the window, NaN skipped, NaN when empty.
+void windowmedmad(const float* A, int64_t nr, int64_t nc, int64_t w, float* med, float* mad) {
+    const Margins m = margins(std::min(w, nc), std::min(w, nr));
+    std::vector<float> buf(static_cast<size_t>((m.lx + m.rx + 1) * (m.ly + m.ry + 1)));
+    for (int64_t j = 0; j < nc; ++j)
+        for (int64_t i = 0; i < nr; ++i) {
+            int64_t n = 0;
+            for (int64_t jj = std::max<int64_t>(j - m.lx, 0); jj <= std::min(j + m.rx, nc - 1); ++jj)
+                for (int64_t ii = std::max<int64_t>(i - m.ly, 0); ii <= std::min(i + m.ry, nr - 1); ++ii) {
+                    const float v = A[ii + jj * nr];
+                    if (!std::isnan(v)) buf[n++] = v;
+                }
+            if (n == 0) { med[i + j * nr] = NAN; mad[i + j * nr] = NAN; continue; }
+            insertion_sort(buf.data(), n);
+            const float md = sorted_median(buf.data(), n);
+            for (int64_t k = 0; k < n; ++k) buf[k] = std::fabs(buf[k] - md);
+            insertion_sort(buf.data(), n);
+            med[i + j * nr] = md;
+            mad[i + j * nr] = sorted_median(buf.data(), n);
+        }
+}
+
+// src/outliers.jl:38-172 -- which displacements to keep.
+void reject_outliers(const float* dx, const float* dy, const int64_t* rx, const int64_t* ry,
+                     const uint8_t* valid, int64_t nr, int64_t nc, int up, const MCParams& P,
+                     int64_t iterations, uint8_t* keep) {
+    const int64_t n = nr * nc;
+    for (int64_t i = 0; i < n; ++i) keep[i] = valid[i];
+    if (P.outliers == 0) return;
+    std::vector<float> nx(n), ny(n), ax(n), ay(n), mx(n), sx(n), my(n), sy(n);
+    for (int64_t i = 0; i < n; ++i) {
+        nx[i] = rx[i] > 0 ? dx[i] / static_cast<float>(rx[i]) : NAN;
+        ny[i] = ry[i] > 0 ? dy[i] / static_cast<float>(ry[i]) : NAN;
+    }
+    const int64_t w = P.gwindow;
+    const float needed = static_cast<float>(P.gfrac * static_cast<double>(w * w));
+    const float tol = static_cast<float>(P.gtol);
+    auto mask_to_nan = [&]() {
+        for (int64_t i = 0; i < n; ++i)
+            if (!keep[i]) { nx[i] = NAN; ny[i] = NAN; }
+    };
+    for (int64_t it = 0; it < iterations; ++it) {
+        mask_to_nan();
+        count_agreeing(nx.data(), nr, nc, w, tol, ax.data());
+        count_agreeing(ny.data(), nr, nc, w, tol, ay.data());
+        for (int64_t i = 0; i < n; ++i) keep[i] = (ax[i] >= needed && ay[i] >= needed) ? 1 : 0;
+    }
+    const int64_t n2 = std::max<int64_t>(iterations - 1, 1);
+    for (int64_t it = 0; it < n2; ++it) {
+        mask_to_nan();
+        windowmedmad(nx.data(), nr, nc, w, mx.data(), sx.data());
+        windowmedmad(ny.data(), nr, nc, w, my.data(), sy.data());
+        for (int64_t i = 0; i < n; ++i) {
+            if (!keep[i]) continue;
+            const double floor_x = rx[i] > 0 ? 2.0 / static_cast<double>(up * rx[i]) : INFINITY;
+            const double floor_y = ry[i] > 0 ? 2.0 / static_cast<double>(up * ry[i]) : INFINITY;
+            const double tolx = std::max(P.gmad * static_cast<double>(sx[i]), floor_x);
+            const double toly = std::max(P.gmad * static_cast<double>(sy[i]), floor_y);
+            const bool kx = static_cast<double>(std::fabs(nx[i] - mx[i])) <= tolx;
+            const bool ky = static_cast<double>(std::fabs(ny[i] - my[i])) <= toly;
+            keep[i] = (kx && ky) ? 1 : 0;
+        }
+    }
+}
+
+// src/resample.jl:190-325 -- every position within Euclidean `radius` of a true (the exact
+// squared-distance test the transform answers, evaluated directly over the disc).
+void dilate_within(const uint8_t* m, int64_t nr, int64_t nc, int64_t radius, uint8_t* out) {
+    const int64_t r2 = radius * radius;
+    for (int64_t j = 0; j < nc; ++j)
+        for (int64_t i = 0; i < nr; ++i) {
+            uint8_t v = 0;
+            for (int64_t dj = -radius; dj <= radius && !v; ++dj)
+                for (int64_t di = -radius; di <= radius; ++di) {
+                    if (di * di + dj * dj > r2) continue;
+                    const int64_t ii = i + di, jj = j + dj;
+                    if (ii < 0 || ii >= nr || jj < 0 || jj >= nc) continue;
+                    if (m[ii + jj * nr]) { v = 1; break; }
+                }
+            out[i + j * nr] = v;
+        }
+}
+
+// src/resample.jl:56-71 -- nearest, half-sample convention, a mask to a mask.
+void resample_nearest(const uint8_t* A, int64_t sr, int64_t sc, int64_t dr, int64_t dc,
+                      uint8_t* out) {
+    const double ys = static_cast<double>(sr) / static_cast<double>(dr);
+    const double xs = static_cast<double>(sc) / static_cast<double>(dc);
+    for (int64_t j = 1; j <= dc; ++j) {
+        const int64_t sj = std::clamp<int64_t>(floor_i((static_cast<double>(j) - 0.5) * xs) + 1, 1, sc);
+        for (int64_t i = 1; i <= dr; ++i) {
+            const int64_t si = std::clamp<int64_t>(floor_i((static_cast<double>(i) - 0.5) * ys) + 1, 1, sr);
+            out[(i - 1) + (j - 1) * dr] = A[(si - 1) + (sj - 1) * sr];
+        }
+    }
+}
+
+// src/multichip.jl:347-390 -- three passes of two-phase median filling of NaN holes.
+void fill_holes(float* dx, float* dy, int64_t nr, int64_t nc, int64_t w, std::vector<uint8_t>& filled) {
+    const int64_t lo = w / 2, hi = w - 1 - lo;
+    const int64_t needed = 2 * w * w / 3;
+    std::vector<float> bx(static_cast<size_t>(w * w)), by(static_cast<size_t>(w * w));
+    struct Pend { int64_t idx; float x, y; };
+    for (int pass = 0; pass < 3; ++pass) {
+        std::vector<Pend> pending;
+        for (int64_t j = 0; j < nc; ++j)
+            for (int64_t i = 0; i < nr; ++i) {
+                if (!std::isnan(dx[i + j * nr])) continue;
+                int64_t n = 0;
+                for (int64_t jj = std::max<int64_t>(j - lo, 0); jj <= std::min(j + hi, nc - 1); ++jj)
+                    for (int64_t ii = std::max<int64_t>(i - lo, 0); ii <= std::min(i + hi, nr - 1); ++ii) {
+                        const float v = dx[ii + jj * nr];
+                        if (std::isnan(v)) continue;
+                        bx[n] = v;
+                        by[n] = dy[ii + jj * nr];
+                        ++n;
+                    }
+                if (n < needed) continue;
+                insertion_sort(bx.data(), n);
+                insertion_sort(by.data(), n);
+                pending.push_back({i + j * nr, sorted_median(bx.data(), n), sorted_median(by.data(), n)});
+            }
+        if (pending.empty()) break;
+        for (const auto& q : pending) {
+            dx[q.idx] = q.x;
+            dy[q.idx] = q.y;
+            filled[q.idx] = 1;
+        }
+    }
+}
+
+template <class T>
+struct MCImages {
+    const T* ref;
+    const T* sec;
+    const uint8_t* refv;
+    const uint8_t* secv;
+    int64_t nrows, ncols;
+};
+
+template <class T>
+void run_track(const MCImages<T>& I, const double* x, const double* y, const int64_t* rx,
+               const int64_t* ry, const double* dx0, const double* dy0, const int64_t* csx,
+               const int64_t* csy, int64_t n, int up, int measure, float* odx, float* ody,
+               float* oc, uint8_t* os, int nthreads) {
+    Points p{x, y, dx0, dy0, rx, ry, csx, csy, n};
+    track_impl(I.ref, I.sec, I.refv, I.secv, I.nrows, I.ncols, p, up, measure, odx, ody, oc, os,
+               nthreads);
+}
+
+// src/multichip.jl:106-422 -- correlate_multichip over a gridded point set (gr x gc).
+template <class T>
+void multichip(const MCImages<T>& I, const double* gx, const double* gy, const int64_t* grx,
+               const int64_t* gry, const double* gdx0, const double* gdy0, int64_t gr, int64_t gc,
+               const MCParams& P, float* rdx, float* rdy, float* rcorr, uint16_t* rcs,
+               uint8_t* rinterp, int nthreads) {
+    const int64_t n = gr * gc;
+    for (int64_t i = 0; i < n; ++i) {
+        rdx[i] = NAN; rdy[i] = NAN; rcorr[i] = NAN; rcs[i] = 0; rinterp[i] = 0;
+    }
+    std::vector<int64_t> sizes;
+    for (int64_t cs = P.chip_base; cs <= P.chip_max; cs *= 2)
+        if (cs >= P.chip_min) sizes.push_back(cs);
+    for (int64_t cs : sizes) {
+        bool any = false;
+        for (int64_t i = 0; i < n; ++i) any = any || rcs[i] == 0;
+        if (!any) break;
+        const int64_t csx = cs;
+        const int64_t csy = 2 * static_cast<int64_t>(std::nearbyint(static_cast<double>(cs) * P.aspect / 2.0));
+        // _level_points (src/multichip.jl:193-213) with sanitize! (src/points.jl:332-346).
+        std::vector<int64_t> rx(n), ry(n), vcsx(n, csx), vcsy(n, csy);
+        int64_t nsearch = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            rx[i] = rcs[i] == 0 ? grx[i] : 0;
+            ry[i] = rcs[i] == 0 ? gry[i] : 0;
+            if (rx[i] <= 0 || ry[i] <= 0) { rx[i] = 0; ry[i] = 0; }
+            else { rx[i] = std::max(rx[i], P.min_radius); ry[i] = std::max(ry[i], P.min_radius); ++nsearch; }
+        }
+        if (nsearch == 0) continue;
+        // _coarse_pass (src/multichip.jl:224-288).
+        std::vector<uint8_t> cmask(n, 1);
+        bool level_off = false;
+        {
+            const int64_t st = P.stride;
+            const int64_t cr = gr / st, cc = gc / st;  // rows stride:stride:gr
+            const int64_t w = P.outliers == 1 ? P.gwindow : 0;
+            if (!(cr < w || cc < w)) {
+                const int64_t m = cr * cc;
+                std::vector<double> cx(m), cy(m), cdx0(m), cdy0(m);
+                std::vector<int64_t> crx(m), cry(m), ccsx(m, csx), ccsy(m, csy);
+                const int64_t lo = st / 2, hi = st - 1 - lo;
+                int64_t csearch = 0;
+                for (int64_t jo = 0; jo < cc; ++jo)
+                    for (int64_t io = 0; io < cr; ++io) {
+                        const int64_t i = (io + 1) * st - 1, j = (jo + 1) * st - 1;  // 0-based fine index
+                        const int64_t k = io + jo * cr, f = i + j * gr;
+                        cx[k] = gx[f]; cy[k] = gy[f]; cdx0[k] = gdx0[f]; cdy0[k] = gdy0[f];
+                        int64_t mx = 0, my = 0;
+                        for (int64_t jj = std::max<int64_t>(j - lo, 0); jj <= std::min(j + hi, gc - 1); ++jj)
+                            for (int64_t ii = std::max<int64_t>(i - lo, 0); ii <= std::min(i + hi, gr - 1); ++ii) {
+                                mx = std::max(mx, rx[ii + jj * gr]);
+                                my = std::max(my, ry[ii + jj * gr]);
+                            }
+                        crx[k] = mx; cry[k] = my;
+                        if (mx > 0 && my > 0) ++csearch;
+                    }
+                if (csearch == 0) { level_off = true; }
+                else {
+                    std::vector<float> cdx(m), cdy(m), ccor(m);
+                    std::vector<uint8_t> cs_(m), measured(m), keep(m), grown(m);
+                    run_track(I, cx.data(), cy.data(), crx.data(), cry.data(), cdx0.data(), cdy0.data(),
+                              ccsx.data(), ccsy.data(), m, 1, P.measure, cdx.data(), cdy.data(),
+                              ccor.data(), cs_.data(), nthreads);
+                    bool anym = false;
+                    for (int64_t k = 0; k < m; ++k) { measured[k] = !std::isnan(cdx[k]); anym = anym || measured[k]; }
+                    if (!anym) level_off = true;
+                    else {
+                        // relax(filter): one fewer stage-1 iteration, at least one.
+                        const int64_t iters = std::max<int64_t>(P.giterations - 1, 1);
+                        reject_outliers(cdx.data(), cdy.data(), crx.data(), cry.data(), measured.data(),
+                                        cr, cc, P.up, P, iters, keep.data());
+                        int64_t denom = 0, numer = 0;
+                        for (int64_t k = 0; k < m; ++k) {
+                            if (!measured[k]) keep[k] = 0;
+                            if (crx[k] > 0 && measured[k]) { ++denom; if (keep[k]) ++numer; }
+                        }
+                        if (denom == 0 || static_cast<double>(numer) / static_cast<double>(denom) < P.min_frac)
+                            level_off = true;
+                        else {
+                            dilate_within(keep.data(), cr, cc, P.buffer, grown.data());
+                            resample_nearest(grown.data(), cr, cc, gr, gc, cmask.data());
+                        }
+                    }
+                }
+            }
+        }
+        if (level_off) continue;
+        nsearch = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            if (!cmask[i]) { rx[i] = 0; ry[i] = 0; }
+            if (rx[i] > 0 && ry[i] > 0) ++nsearch;
+        }
+        if (nsearch == 0) continue;
+        std::vector<float> fdx(n), fdy(n), fc(n);
+        std::vector<uint8_t> fs(n), measured(n), keep(n), filled(n, 0);
+        run_track(I, gx, gy, rx.data(), ry.data(), gdx0, gdy0, vcsx.data(), vcsy.data(), n, P.up,
+                  P.measure, fdx.data(), fdy.data(), fc.data(), fs.data(), nthreads);
+        // _reject_and_fill! (src/multichip.jl:318-330).
+        for (int64_t i = 0; i < n; ++i) measured[i] = !std::isnan(fdx[i]);
+        reject_outliers(fdx.data(), fdy.data(), rx.data(), ry.data(), measured.data(), gr, gc, P.up, P,
+                        P.giterations, keep.data());
+        for (int64_t i = 0; i < n; ++i)
+            if (!keep[i]) { fdx[i] = NAN; fdy[i] = NAN; fc[i] = NAN; }
+        fill_holes(fdx.data(), fdy.data(), gr, gc, P.fill_window, filled);
+        // _merge_level! (src/multichip.jl:401-422).
+        for (int64_t i = 0; i < n; ++i) {
+            if (rcs[i] != 0) continue;
+            if (std::isnan(fdx[i])) continue;
+            rdx[i] = fdx[i]; rdy[i] = fdy[i]; rcorr[i] = fc[i];
+            rcs[i] = static_cast<uint16_t>(cs);
+            rinterp[i] = filled[i];
+        }
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -756,6 +1067,60 @@ int or_prepare(const void* img, const uint8_t* mask, int64_t nrows, int64_t ncol
         case OR_F64: run(static_cast<const double*>(img)); break;
         default: return -1;
     }
+    return 0;
+}
+
+// correlate_multichip (src/multichip.jl:106-137) over a gridded point set of gr x gc points
+// (column-major fields). params (doubles): chip_base, chip_min, chip_max, aspect, min_radius,
+// stride, buffer, min_frac, up, measure, outliers, window, iterations, min_agree_fraction,
+// agree_tolerance, mad_scale, fill_window.
+int or_multichip(const void* ref, const void* sec, const uint8_t* refv, const uint8_t* secv,
+                 int64_t nrows, int64_t ncols, int dtype, const double* gx, const double* gy,
+                 const int64_t* grx, const int64_t* gry, const double* gdx0, const double* gdy0,
+                 int64_t gr, int64_t gc, const double* prm, float* dx, float* dy, float* corr,
+                 uint16_t* chip, uint8_t* interp, int nthreads) {
+    MCParams P;
+    P.chip_base = static_cast<int64_t>(prm[0]);
+    P.chip_min = static_cast<int64_t>(prm[1]);
+    P.chip_max = static_cast<int64_t>(prm[2]);
+    P.aspect = prm[3];
+    P.min_radius = static_cast<int64_t>(prm[4]);
+    P.stride = static_cast<int64_t>(prm[5]);
+    P.buffer = static_cast<int64_t>(prm[6]);
+    P.min_frac = prm[7];
+    P.up = static_cast<int>(prm[8]);
+    P.measure = static_cast<int>(prm[9]);
+    P.outliers = static_cast<int>(prm[10]);
+    P.gwindow = static_cast<int64_t>(prm[11]);
+    P.giterations = static_cast<int64_t>(prm[12]);
+    P.gfrac = prm[13];
+    P.gtol = prm[14];
+    P.gmad = prm[15];
+    P.fill_window = static_cast<int64_t>(prm[16]);
+    auto run = [&](auto* r, auto* s) {
+        using T = std::remove_const_t<std::remove_pointer_t<decltype(r)>>;
+        MCImages<T> I{r, s, refv, secv, nrows, ncols};
+        multichip(I, gx, gy, grx, gry, gdx0, gdy0, gr, gc, P, dx, dy, corr, chip, interp, nthreads);
+    };
+    switch (dtype) {
+        case OR_U8: run(static_cast<const uint8_t*>(ref), static_cast<const uint8_t*>(sec)); break;
+        case OR_U16: run(static_cast<const uint16_t*>(ref), static_cast<const uint16_t*>(sec)); break;
+        case OR_F32: run(static_cast<const float*>(ref), static_cast<const float*>(sec)); break;
+        case OR_I16: run(static_cast<const int16_t*>(ref), static_cast<const int16_t*>(sec)); break;
+        default: return -1;
+    }
+    return 0;
+}
+
+// Gardner / NoOutlierFilter rejection alone (src/outliers.jl:38-160), for tests.
+int or_reject_outliers(const float* dx, const float* dy, const int64_t* rx, const int64_t* ry,
+                       const uint8_t* valid, int64_t nr, int64_t nc, int up, int outliers,
+                       int64_t window, int64_t iterations, double frac, double tol, double mad,
+                       uint8_t* keep) {
+    MCParams P{};
+    P.outliers = outliers; P.gwindow = window; P.giterations = iterations;
+    P.gfrac = frac; P.gtol = tol; P.gmad = mad;
+    reject_outliers(dx, dy, rx, ry, valid, nr, nc, up, P, iterations, keep);
     return 0;
 }
 

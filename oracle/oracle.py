@@ -55,6 +55,11 @@ def lib():
         L.or_track.restype = i32
         L.or_prepare.argtypes = [p, p, i64, i64, i32, i32, i64, ctypes.c_double, i32, p, p]
         L.or_prepare.restype = i32
+        L.or_multichip.argtypes = [p, p, p, p, i64, i64, i32] + [p] * 6 + [i64, i64, p] + [p] * 5 + [i32]
+        L.or_multichip.restype = i32
+        L.or_reject_outliers.argtypes = [p, p, p, p, p, i64, i64, i32, i32, i64, i64,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_double, p]
+        L.or_reject_outliers.restype = i32
         L.or_max_threads.argtypes = []
         L.or_max_threads.restype = i32
         _lib = L
@@ -181,6 +186,64 @@ def prepare(img, mask=None, preprocess: str = "highpass", width: int = 5, min_st
     if rc != 0:
         raise ValueError("unsupported dtype")
     return out, vout.astype(bool)
+
+
+def multichip(reference, secondary, grid, params: dict, reference_valid=None,
+              secondary_valid=None, nthreads: int = 0):
+    """correlate_multichip (src/multichip.jl:106-137) over a gridded point set.
+
+    ``grid`` maps the PointSet fields to (gr, gc) arrays; ``params`` holds chip_base, chip_min,
+    chip_max, aspect, min_radius, stride, buffer, min_frac, up, measure (0/1), outliers (0/1),
+    window, iterations, min_agree_fraction, agree_tolerance, mad_scale, fill_window.
+    Returns (dx, dy, correlation, chip_size, interpolated) as (gr, gc) arrays.
+    """
+    ref = _f(reference)
+    sec = _f(secondary, ref.dtype)
+    nrows, ncols = ref.shape
+    if reference_valid is None:
+        reference_valid = np.isfinite(ref) if ref.dtype.kind == "f" else np.ones(ref.shape, bool)
+    if secondary_valid is None:
+        secondary_valid = np.isfinite(sec) if sec.dtype.kind == "f" else np.ones(sec.shape, bool)
+    rv = _f(reference_valid, np.uint8)
+    sv = _f(secondary_valid, np.uint8)
+    gr, gc = np.shape(grid["x"])
+
+    def fld(name, dt):
+        return np.ascontiguousarray(np.asarray(grid[name], dtype=dt).ravel(order="F"))
+
+    keys = ["chip_base", "chip_min", "chip_max", "aspect", "min_radius", "stride", "buffer",
+            "min_frac", "up", "measure", "outliers", "window", "iterations",
+            "min_agree_fraction", "agree_tolerance", "mad_scale", "fill_window"]
+    prm = np.array([float(params[k]) for k in keys], dtype=np.float64)
+    cols = [fld("x", np.float64), fld("y", np.float64), fld("radius_x", np.int64),
+            fld("radius_y", np.int64), fld("dx_prior", np.float64), fld("dy_prior", np.float64)]
+    n = gr * gc
+    dx = np.empty(n, np.float32)
+    dy = np.empty(n, np.float32)
+    c = np.empty(n, np.float32)
+    cs = np.empty(n, np.uint16)
+    it = np.empty(n, np.uint8)
+    rc = lib().or_multichip(_ptr(ref), _ptr(sec), _ptr(rv), _ptr(sv), nrows, ncols,
+                            DTYPE_CODES[ref.dtype], *[_ptr(a) for a in cols], gr, gc, _ptr(prm),
+                            _ptr(dx), _ptr(dy), _ptr(c), _ptr(cs), _ptr(it), int(nthreads))
+    if rc != 0:
+        raise ValueError("unsupported dtype")
+    shp = lambda a: a.reshape((gr, gc), order="F")
+    return shp(dx), shp(dy), shp(c), shp(cs), shp(it).astype(bool)
+
+
+def reject_outliers(dx, dy, rx, ry, valid, up: int, outliers: str = "gardner", window: int = 5,
+                    iterations: int = 3, min_agree_fraction: float = 8 / 25,
+                    agree_tolerance: float = 0.2, mad_scale: float = 4.0):
+    """reject_outliers (src/outliers.jl:38-160) on (nr, nc) fields: the keep mask."""
+    dx = _f(dx, np.float32)
+    nr, nc = dx.shape
+    keep = np.empty((nr, nc), np.uint8, order="F")
+    lib().or_reject_outliers(_ptr(dx), _ptr(_f(dy, np.float32)), _ptr(_f(rx, np.int64)),
+                             _ptr(_f(ry, np.int64)), _ptr(_f(valid, np.uint8)), nr, nc, int(up),
+                             1 if outliers == "gardner" else 0, window, iterations,
+                             min_agree_fraction, agree_tolerance, mad_scale, _ptr(keep))
+    return keep.astype(bool)
 
 
 def max_threads() -> int:
