@@ -75,6 +75,9 @@ SIGNATURES = {
     "ar_refine_patches": (_i32, [_p, _p, _i64, _i32, _p, _p, _p]),
     "ar_multichip": (_i32, [_p, _p, ctypes.POINTER(ArPoints), _i64, _i64,
                             ctypes.POINTER(ArMultichipParams), _p, _p, _p, _p, _p]),
+    "ar_multichip_device": (_i32, [_p, _p, ctypes.POINTER(ArPoints), _i64, _i64,
+                                   ctypes.POINTER(ArMultichipParams), _p, _p, _p, _p, _p, _p]),
+    "ar_ctx_stream": (_i32, [_p, ctypes.POINTER(_p)]),
     "ar_ctx_set_timing": (_i32, [_p, _i32]),
     "ar_kernel_times": (_i32, [_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                ctypes.POINTER(_i64), ctypes.POINTER(_i64),
@@ -133,6 +136,12 @@ class Context:
 
     def set_timing(self, enable: bool):
         self.check(self.lib.ar_ctx_set_timing(self.handle, int(bool(enable))))
+
+    def stream(self) -> int:
+        """The context's CUDA stream handle."""
+        h = ctypes.c_void_p()
+        self.check(self.lib.ar_ctx_stream(self.handle, ctypes.byref(h)))
+        return h.value or 0
 
     def kernel_times(self):
         """(corr_ms, refine_ms, track_launches, kernel_launches, corr_flops) since the last

@@ -31,6 +31,9 @@ struct ar_ctx {
     // Scratch of the multichip search, grown on demand.
     void* arena = nullptr;
     size_t arena_bytes = 0;
+    // Stream-ordered pool for pair images and per-call scratch: freed blocks stay with the
+    // context and are reused without a device-wide synchronisation.
+    cudaMemPool_t pool = nullptr;
 };
 
 struct ar_pair {
@@ -204,6 +207,29 @@ cudaError_t launch_make_valid(ar_pair* p, bool have_rv, bool have_sv, cudaStream
 
 bool is_pow2(int v) { return v >= 1 && (v & (v - 1)) == 0; }
 
+// Pool allocations, ordered on the context stream.
+cudaError_t dalloc(ar_ctx* c, void** p, size_t bytes) {
+    *p = nullptr;
+    return cudaMallocFromPoolAsync(p, std::max<size_t>(bytes, 256), c->pool, c->stream);
+}
+template <typename T>
+cudaError_t dalloc(ar_ctx* c, T** p, size_t bytes) {
+    void* q = nullptr;
+    cudaError_t e = dalloc(c, &q, bytes);
+    *p = static_cast<T*>(q);
+    return e;
+}
+void dfree(ar_ctx* c, void* p) {
+    if (p) cudaFreeAsync(p, c->stream);
+}
+void pair_free(ar_pair* p) {
+    dfree(p->ctx, p->ref);
+    dfree(p->ctx, p->sec);
+    dfree(p->ctx, p->valid);
+    p->ref = p->sec = nullptr;
+    p->valid = p->ref_valid = p->sec_valid = nullptr;
+}
+
 }  // namespace
 
 extern "C" {
@@ -221,7 +247,20 @@ int ar_ctx_create(int device, ar_ctx** out) {
     c->device = device;
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        e = cudaMemPoolCreate(&c->pool, &props);
+    }
+    if (e == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;  // never trim: the context reuses what it frees
+        e = cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     if (e != cudaSuccess) {
+        if (c->pool) cudaMemPoolDestroy(c->pool);
+        if (c->stream) cudaStreamDestroy(c->stream);
         delete c;
         return AR_ERR_CUDA;
     }
@@ -244,11 +283,14 @@ int ar_ctx_destroy(ar_ctx* c) {
             for (auto ev : r) c->scratch.timer.pool.push_back(ev);
         for (auto ev : c->scratch.timer.pool) cudaEventDestroy(ev);
         cudaFree(c->scratch.timer.flops);
+        if (c->scratch.done) cudaEventDestroy(c->scratch.done);
         cudaFree(c->dbuf);
         cudaFree(c->arena);
         if (c->pinned) cudaFreeHost(c->pinned);
         for (auto& ev : c->staged)
             if (ev) cudaEventDestroy(ev);
+        cudaStreamSynchronize(c->stream);
+        cudaMemPoolDestroy(c->pool);
         cudaStreamDestroy(c->stream);
     }
     delete c;
@@ -279,9 +321,9 @@ int ar_pair_upload(ar_ctx* c, const void* ref, const void* sec, const uint8_t* r
     p->dtype = dtype;
     p->nrows = nrows;
     p->ncols = ncols;
-    cudaError_t e = cudaMalloc(&p->ref, n * es);
-    if (e == cudaSuccess) e = cudaMalloc(&p->sec, n * es);
-    if (e == cudaSuccess) e = cudaMalloc(&p->valid, 3 * n);
+    cudaError_t e = dalloc(c, &p->ref, n * es);
+    if (e == cudaSuccess) e = dalloc(c, &p->sec, n * es);
+    if (e == cudaSuccess) e = dalloc(c, &p->valid, 3 * n);
     if (e == cudaSuccess) {
         p->ref_valid = p->valid + n;
         p->sec_valid = p->valid + 2 * n;
@@ -300,9 +342,7 @@ int ar_pair_upload(ar_ctx* c, const void* ref, const void* sec, const uint8_t* r
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) {
-        cudaFree(p->ref);
-        cudaFree(p->sec);
-        cudaFree(p->valid);
+        pair_free(p);
         delete p;
         return cuda_fail(c, e, "ar_pair_upload");
     }
@@ -315,10 +355,10 @@ int ar_pair_destroy(ar_pair* p) {
     {
         DeviceGuard g(p->ctx->device);
         std::lock_guard<std::mutex> lk(p->ctx->mu);
-        cudaStreamSynchronize(p->ctx->stream);
-        cudaFree(p->ref);
-        cudaFree(p->sec);
-        cudaFree(p->valid);
+        // The library's own work on the pair is ordered before the frees on the context
+        // stream; work the caller queued on its own streams must have completed.
+        if (p->ctx->scratch.done) cudaStreamWaitEvent(p->ctx->stream, p->ctx->scratch.done, 0);
+        pair_free(p);
     }
     delete p;
     return AR_OK;
@@ -545,9 +585,10 @@ int ar_prepare(ar_ctx* c, const ar_pair* raw, const ar_prepare_opts* opts, ar_pa
     p->dtype = odt;
     p->nrows = raw->nrows;
     p->ncols = raw->ncols;
-    cudaError_t e = cudaMalloc(&p->ref, n * oes);
-    if (e == cudaSuccess) e = cudaMalloc(&p->sec, n * oes);
-    if (e == cudaSuccess) e = cudaMalloc(&p->valid, 3 * n);
+    if (c->scratch.done) cudaStreamWaitEvent(c->stream, c->scratch.done, 0);
+    cudaError_t e = dalloc(c, &p->ref, n * oes);
+    if (e == cudaSuccess) e = dalloc(c, &p->sec, n * oes);
+    if (e == cudaSuccess) e = dalloc(c, &p->valid, 3 * n);
     if (e == cudaSuccess) {
         p->ref_valid = p->valid + n;
         p->sec_valid = p->valid + 2 * n;
@@ -556,7 +597,7 @@ int ar_prepare(ar_ctx* c, const ar_pair* raw, const ar_prepare_opts* opts, ar_pa
     const bool need_m = opts->preprocess == AR_PRE_WALLIS;
     const size_t scratch = (need_f ? n * 4 : 0) + (need_m ? n * 4 : 0) + ar::quant_stats_bytes() + 256;
     unsigned char* tmp = nullptr;
-    if (e == cudaSuccess) e = cudaMalloc(&tmp, scratch);
+    if (e == cudaSuccess) e = dalloc(c, &tmp, scratch);
     for (int side = 0; side < 2 && e == cudaSuccess; ++side) {
         ar::PrepareJob J{};
         J.dtype = raw->dtype;
@@ -584,12 +625,10 @@ int ar_prepare(ar_ctx* c, const ar_pair* raw, const ar_prepare_opts* opts, ar_pa
             p->ref_valid, p->sec_valid, p->valid, n);
         e = cudaGetLastError();
     }
+    dfree(c, tmp);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    cudaFree(tmp);
     if (e != cudaSuccess) {
-        cudaFree(p->ref);
-        cudaFree(p->sec);
-        cudaFree(p->valid);
+        pair_free(p);
         delete p;
         return cuda_fail(c, e, "ar_prepare");
     }
@@ -612,66 +651,44 @@ int ar_pair_download(ar_ctx* c, const ar_pair* p, void* ref, void* sec, uint8_t*
     return e == cudaSuccess ? AR_OK : cuda_fail(c, e, "ar_pair_download");
 }
 
-int ar_multichip(ar_ctx* c, const ar_pair* p, const ar_points* grid, int64_t gr, int64_t gc,
-                 const ar_multichip_params* prm, float* dx, float* dy, float* corr,
-                 uint16_t* chip, uint8_t* interp) {
+}  // extern "C"
+
+namespace {
+
+int check_multichip_args(ar_ctx* c, const ar_pair* p, const ar_points* grid, int64_t gr,
+                         int64_t gc, const ar_multichip_params* prm) {
     if (!c || !p || !grid || !prm) return fail(c, AR_ERR_ARG, "null argument");
     if (p->ctx != c) return fail(c, AR_ERR_ARG, "the pair belongs to another context");
     if (gr < 0 || gc < 0 || grid->n != gr * gc)
         return fail(c, AR_ERR_SIZE, "grid extents do not match the point count");
-    const int64_t n = grid->n;
-    if (n == 0) return AR_OK;
-    if (!dx || !dy || !corr || !chip || !interp || !grid->x || !grid->y || !grid->radius_x ||
-        !grid->radius_y || !grid->dx_prior || !grid->dy_prior)
-        return fail(c, AR_ERR_ARG, "null grid field or output");
+    if (grid->n > 0 && (!grid->x || !grid->y || !grid->radius_x || !grid->radius_y ||
+                        !grid->dx_prior || !grid->dy_prior))
+        return fail(c, AR_ERR_ARG, "null grid field");
     if (!is_pow2(prm->upsampling) || prm->upsampling > 128)
         return fail(c, AR_ERR_ARG, "`upsampling` must be 1 or a power of 2 up to 128");
     if (prm->measure != AR_ZNCC && prm->measure != AR_NCC) return fail(c, AR_ERR_ARG, "unknown measure");
     if (prm->chip_size_base <= 0 || prm->chip_size_max < prm->chip_size_base || prm->coarse_stride <= 0)
         return fail(c, AR_ERR_ARG, "invalid chip-size levels or coarse stride");
-    for (int64_t k = 0; k < n; ++k)
-        if (!std::isfinite(grid->x[k]) || !std::isfinite(grid->y[k]) ||
-            !std::isfinite(grid->dx_prior[k]) || !std::isfinite(grid->dy_prior[k]))
-            return fail(c, AR_ERR_ARG, "grid coordinates and priors must be finite");
-    std::lock_guard<std::mutex> lk(c->mu);
-    DeviceGuard g(c->device);
-    // Device copies of the six grid fields and the five outputs.
-    const size_t need = static_cast<size_t>(n) * (6 * 8 + 3 * 4 + 2 + 1) + 16 * 256;
-    cudaError_t e = ensure_dbuf(c, need);
-    if (e != cudaSuccess) return cuda_fail(c, e, "ar_multichip: device buffers");
+    return AR_OK;
+}
+
+// The search over a grid whose fields and outputs are device arrays; the caller holds the
+// context lock. Returns once the search has completed on `s`.
+int multichip_run(ar_ctx* c, const ar_pair* p, const double* gx, const double* gy,
+                  const int64_t* grx, const int64_t* gry, const double* gdx0, const double* gdy0,
+                  int64_t gr, int64_t gc, const ar_multichip_params* prm, float* dx, float* dy,
+                  float* corr, uint16_t* chip, uint8_t* interp, cudaStream_t s) {
     const size_t ab = ar::multichip_arena_bytes(gr, gc);
     if (c->arena_bytes < ab) {
+        cudaDeviceSynchronize();
         cudaFree(c->arena);
         c->arena = nullptr;
         c->arena_bytes = 0;
-        e = cudaMalloc(&c->arena, ab);
+        cudaError_t e = cudaMalloc(&c->arena, ab);
         if (e != cudaSuccess) return cuda_fail(c, e, "ar_multichip: scratch");
         c->arena_bytes = ab;
     }
-    unsigned char* base = static_cast<unsigned char*>(c->dbuf);
-    size_t off = 0;
-    auto take = [&](size_t bytes) {
-        off = (off + 255) & ~size_t(255);
-        unsigned char* q = base + off;
-        off += bytes;
-        return q;
-    };
     ar::MultichipJob J{};
-    double* gx = reinterpret_cast<double*>(take(n * 8));
-    double* gy = reinterpret_cast<double*>(take(n * 8));
-    int64_t* grx = reinterpret_cast<int64_t*>(take(n * 8));
-    int64_t* gry = reinterpret_cast<int64_t*>(take(n * 8));
-    double* gdx0 = reinterpret_cast<double*>(take(n * 8));
-    double* gdy0 = reinterpret_cast<double*>(take(n * 8));
-    J.dx = reinterpret_cast<float*>(take(n * 4));
-    J.dy = reinterpret_cast<float*>(take(n * 4));
-    J.corr = reinterpret_cast<float*>(take(n * 4));
-    J.chip = reinterpret_cast<uint16_t*>(take(n * 2));
-    J.interp = take(n);
-    const void* srcs[6] = {grid->x, grid->y, grid->radius_x, grid->radius_y, grid->dx_prior, grid->dy_prior};
-    void* dsts[6] = {gx, gy, grx, gry, gdx0, gdy0};
-    for (int f = 0; f < 6 && e == cudaSuccess; ++f) e = stage_h2d(c, dsts[f], srcs[f], n * 8);
-    if (e != cudaSuccess) return cuda_fail(c, e, "ar_multichip: upload grid");
     J.dtype = p->dtype;
     J.ref = p->ref;
     J.sec = p->sec;
@@ -686,6 +703,11 @@ int ar_multichip(ar_ctx* c, const ar_pair* p, const ar_points* grid, int64_t gr,
     J.gdy0 = gdy0;
     J.gr = gr;
     J.gc = gc;
+    J.dx = dx;
+    J.dy = dy;
+    J.corr = corr;
+    J.chip = chip;
+    J.interp = interp;
     ar::MultichipParams& P = J.P;
     P.chip_base = prm->chip_size_base;
     P.chip_min = prm->chip_size_min;
@@ -707,15 +729,87 @@ int ar_multichip(ar_ctx* c, const ar_pair* p, const ar_points* grid, int64_t gr,
     J.arena = c->arena;
     J.arena_bytes = c->arena_bytes;
     std::string err;
-    e = ar::run_multichip(J, c->scratch, c->num_sms, c->stream, &err);
+    cudaError_t e = ar::run_multichip(J, c->scratch, c->num_sms, s, &err);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess)
         return err.empty() ? cuda_fail(c, e, "ar_multichip") : fail(c, AR_ERR_UNSUPPORTED, err);
-    e = stage_d2h(c, dx, J.dx, n * 4);
-    if (e == cudaSuccess) e = stage_d2h(c, dy, J.dy, n * 4);
-    if (e == cudaSuccess) e = stage_d2h(c, corr, J.corr, n * 4);
-    if (e == cudaSuccess) e = stage_d2h(c, chip, J.chip, n * 2);
-    if (e == cudaSuccess) e = stage_d2h(c, interp, J.interp, n);
+    return AR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ar_multichip(ar_ctx* c, const ar_pair* p, const ar_points* grid, int64_t gr, int64_t gc,
+                 const ar_multichip_params* prm, float* dx, float* dy, float* corr,
+                 uint16_t* chip, uint8_t* interp) {
+    int rc = check_multichip_args(c, p, grid, gr, gc, prm);
+    if (rc != AR_OK) return rc;
+    const int64_t n = grid->n;
+    if (n == 0) return AR_OK;
+    if (!dx || !dy || !corr || !chip || !interp) return fail(c, AR_ERR_ARG, "null output");
+    for (int64_t k = 0; k < n; ++k)
+        if (!std::isfinite(grid->x[k]) || !std::isfinite(grid->y[k]) ||
+            !std::isfinite(grid->dx_prior[k]) || !std::isfinite(grid->dy_prior[k]))
+            return fail(c, AR_ERR_ARG, "grid coordinates and priors must be finite");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    // Device copies of the six grid fields and the five outputs.
+    const size_t need = static_cast<size_t>(n) * (6 * 8 + 3 * 4 + 2 + 1) + 16 * 256;
+    cudaError_t e = ensure_dbuf(c, need);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ar_multichip: device buffers");
+    unsigned char* base = static_cast<unsigned char*>(c->dbuf);
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        off = (off + 255) & ~size_t(255);
+        unsigned char* q = base + off;
+        off += bytes;
+        return q;
+    };
+    double* gx = reinterpret_cast<double*>(take(n * 8));
+    double* gy = reinterpret_cast<double*>(take(n * 8));
+    int64_t* grx = reinterpret_cast<int64_t*>(take(n * 8));
+    int64_t* gry = reinterpret_cast<int64_t*>(take(n * 8));
+    double* gdx0 = reinterpret_cast<double*>(take(n * 8));
+    double* gdy0 = reinterpret_cast<double*>(take(n * 8));
+    float* ddx = reinterpret_cast<float*>(take(n * 4));
+    float* ddy = reinterpret_cast<float*>(take(n * 4));
+    float* dcorr = reinterpret_cast<float*>(take(n * 4));
+    uint16_t* dchip = reinterpret_cast<uint16_t*>(take(n * 2));
+    uint8_t* dint = take(n);
+    const void* srcs[6] = {grid->x, grid->y, grid->radius_x, grid->radius_y, grid->dx_prior, grid->dy_prior};
+    void* dsts[6] = {gx, gy, grx, gry, gdx0, gdy0};
+    for (int f = 0; f < 6 && e == cudaSuccess; ++f) e = stage_h2d(c, dsts[f], srcs[f], n * 8);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ar_multichip: upload grid");
+    rc = multichip_run(c, p, gx, gy, grx, gry, gdx0, gdy0, gr, gc, prm, ddx, ddy, dcorr, dchip,
+                       dint, c->stream);
+    if (rc != AR_OK) return rc;
+    e = stage_d2h(c, dx, ddx, n * 4);
+    if (e == cudaSuccess) e = stage_d2h(c, dy, ddy, n * 4);
+    if (e == cudaSuccess) e = stage_d2h(c, corr, dcorr, n * 4);
+    if (e == cudaSuccess) e = stage_d2h(c, chip, dchip, n * 2);
+    if (e == cudaSuccess) e = stage_d2h(c, interp, dint, n);
     if (e != cudaSuccess) return cuda_fail(c, e, "ar_multichip: download");
+    return AR_OK;
+}
+
+int ar_multichip_device(ar_ctx* c, const ar_pair* p, const ar_points* grid, int64_t gr,
+                        int64_t gc, const ar_multichip_params* prm, float* dx, float* dy,
+                        float* corr, uint16_t* chip, uint8_t* interp, void* stream) {
+    int rc = check_multichip_args(c, p, grid, gr, gc, prm);
+    if (rc != AR_OK) return rc;
+    if (grid->n == 0) return AR_OK;
+    if (!dx || !dy || !corr || !chip || !interp) return fail(c, AR_ERR_ARG, "null output");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    return multichip_run(c, p, grid->x, grid->y, grid->radius_x, grid->radius_y, grid->dx_prior,
+                         grid->dy_prior, gr, gc, prm, dx, dy, corr, chip, interp, s);
+}
+
+int ar_ctx_stream(ar_ctx* c, void** stream) {
+    if (!c || !stream) return AR_ERR_ARG;
+    *stream = c->stream;
     return AR_OK;
 }
 

@@ -60,6 +60,9 @@ struct TrackScratch {
     int64_t capacity = 0;
     int64_t* geom = nullptr;        // device-side pass geometry (8 int64)
     KernelTimer timer;
+    // Recorded after the last pass that used these buffers; a pass on another stream waits
+    // for it before reusing them.
+    cudaEvent_t done = nullptr;
 };
 
 // Host-side pass geometry of a host point set.

@@ -1032,9 +1032,13 @@ PassGeometry pass_geometry_host(const ar_points& p, int64_t nrows, int64_t ncols
     return g;
 }
 
+cudaError_t scratch_acquire(TrackScratch& s, cudaStream_t stream);
+
 cudaError_t pass_geometry_device(const DevPoints& pts, int64_t nrows, int64_t ncols,
                                  TrackScratch& scratch, cudaStream_t stream, PassGeometry* out) {
-    cudaError_t e = ensure_scratch(scratch, 0);
+    cudaError_t e = scratch_acquire(scratch, stream);
+    if (e != cudaSuccess) return e;
+    e = ensure_scratch(scratch, 0);
     if (e != cudaSuccess) return e;
     long long init[8] = {0, 0, 0, 0, 0, 0, 1, 0};
     e = cudaMemcpyAsync(scratch.geom, init, sizeof(init), cudaMemcpyHostToDevice, stream);
@@ -1064,11 +1068,18 @@ cudaError_t pass_geometry_device(const DevPoints& pts, int64_t nrows, int64_t nc
     return cudaSuccess;
 }
 
-cudaError_t launch_track(int dtype, const void* ref, const void* sec, const uint8_t* valid,
-                         int64_t nrows, int64_t ncols, const DevPoints& pts,
-                         const PassGeometry& geom, int up, int measure, const DevOutputs& out,
-                         TrackScratch& scratch, int num_sms, cudaStream_t stream,
-                         std::string* err, float* surf_out) {
+// The scratch buffers are shared by the passes of a context; a pass on one stream waits for
+// the last pass that used them, whichever stream that ran on.
+cudaError_t scratch_acquire(TrackScratch& s, cudaStream_t stream) {
+    if (!s.done) return cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
+    return cudaStreamWaitEvent(stream, s.done, 0);
+}
+
+cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const uint8_t* valid,
+                              int64_t nrows, int64_t ncols, const DevPoints& pts,
+                              const PassGeometry& geom, int up, int measure,
+                              const DevOutputs& out, TrackScratch& scratch, int num_sms,
+                              cudaStream_t stream, std::string* err, float* surf_out) {
     cudaError_t e = ensure_scratch(scratch, pts.n);
     if (e != cudaSuccess) return e;
     if (pts.n > 0) {
@@ -1178,6 +1189,19 @@ cudaError_t launch_track(int dtype, const void* ref, const void* sec, const uint
         T.recs.push_back({ev0, ev1, ev2});
     }
     return e;
+}
+
+cudaError_t launch_track(int dtype, const void* ref, const void* sec, const uint8_t* valid,
+                         int64_t nrows, int64_t ncols, const DevPoints& pts,
+                         const PassGeometry& geom, int up, int measure, const DevOutputs& out,
+                         TrackScratch& scratch, int num_sms, cudaStream_t stream,
+                         std::string* err, float* surf_out) {
+    cudaError_t e = scratch_acquire(scratch, stream);
+    if (e != cudaSuccess) return e;
+    e = launch_track_impl(dtype, ref, sec, valid, nrows, ncols, pts, geom, up, measure, out,
+                          scratch, num_sms, stream, err, surf_out);
+    const cudaError_t r = cudaEventRecord(scratch.done, stream);
+    return e != cudaSuccess ? e : r;
 }
 
 cudaError_t launch_refine_patches(const float* patches, int64_t count, int up, int32_t* row,

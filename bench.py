@@ -1,19 +1,24 @@
 #!/usr/bin/env python
-"""Benchmark: points/s of the dense ZNCC track pass on B200.
+"""Benchmark: points/s of AutoRIFT.jl's default pipeline at chip 32 / radius 25 on B200.
 
-Workload (one step): the fine track pass of AutoRIFT.jl (`track`, src/track.jl:103-152) at
-chip 32, search radius 25, PyramidRefine(64), ZNCC, over the 490 x 490 grid (spacing 8,
-margin from chip_size_max 128) of a 4096^2 synthetic 8-bit pair (filtered noise, mean 128,
-std 40; secondary warped by a 6-bump field up to 15 px, 2% noise, 3% no-data blobs masked
-invalid). The two 16.8 MB images fit in L2, so L2 is flushed before every timed step by writing
-a 256 MiB buffer (outside the timed interval).
+Workload (one step): `autorift(image1, image2; grid_spacing=8)` with the reference's defaults
+(src/api.jl:210-274) on a 4096^2 synthetic UInt16 pair: highpass (width 5) and UInt8
+quantisation of both images (src/api.jl:305-311), then the multi-chip-size search
+(src/multichip.jl:106-422) over the 490 x 490 grid (spacing 8, margin from chip_size_max 128)
+at chip sizes 32/64/128, search radius 25, PyramidRefine(64), ZNCC, Gardner outlier filter and
+hole filling. Scene: seeded filtered noise (sigma 2, mean 8000, std 1500) and its bicubic warp
+by a 6-bump field up to 15 px, 2% noise, 3% no-data blobs passed as the secondary's mask.
+
+`value` times the device work with the raw pair and the grid resident in HBM; `e2e` times the
+same pipeline through the C ABI from host buffers (pair upload, grid upload, result download).
+L2 (126 MB) is flushed before every timed step by writing a 256 MiB buffer.
 
 Arms:
-  default            our library (libautorift_gpu.so, sm_100a), N GPUs as N independent
+  default            our library (libautorift_gpu.so, sm_100a); N GPUs run N independent
                      replicas (one pair per rank, no collective on the data path).
   --impl reference   the reference's algorithm on the host cores: Julia is not installed, so
-                     the CPU restatement (oracle/, C++ + OpenMP, all host threads) times a
-                     bounded sample of the same workload.
+                     the CPU restatement (oracle/, C++ + OpenMP, all host threads) runs the
+                     same pipeline on a 2048^2 crop of the scene per step.
 
 Prints one JSON line (rank 0).
 """
@@ -21,6 +26,7 @@ Prints one JSON line (rank 0).
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -36,21 +42,20 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "points/sec at chip32/r25 vs plain GPU path; p50/p99 pair latency"
 UNIT = "points/s"
-CHIP, RADIUS, UP, SPACING, N = 32, 25, 64, 8, 4096
-WORKLOAD = (f"track pass (fine, ZNCC, chip {CHIP}, radius {RADIUS}, PyramidRefine({UP})) over the "
-            f"490x490 spacing-{SPACING} grid of a {N}^2 synthetic UInt8 pair")
+N, SPACING, CHIP, RADIUS, UP = 4096, 8, 32, 25, 64
+CROP = 2048  # host sample: the same pipeline on a centred crop of the scene
+WORKLOAD = (f"autorift() default pipeline (highpass 5, UInt8, multichip 32/64/128, Gardner, fill) "
+            f"on a {N}^2 synthetic UInt16 pair, 490x490 grid spacing {SPACING}, radius {RADIUS}, "
+            f"PyramidRefine({UP})")
 
 
-def load_workload(ar, spacing=SPACING):
-    a, b, valid, _ = ar.synthetic.scale_u16_pair(N, mean=128.0, std=40.0, dtype=np.uint8)
-    pts = ar.gridpoints((N, N), spacing, chip_size=4 * CHIP, search_radius=RADIUS)
-    pts = ar.pointset(pts.x, pts.y, chip_size=CHIP, search_radius=RADIUS)
-    return a, b, valid, pts
+def scene(ar, n=N):
+    a, b, valid, _ = ar.synthetic.scale_u16_pair(n)
+    return a, b, valid
 
 
-def flops_per_point():
-    # Algorithmic FLOPs of one point evaluation: 2 * chip area * surface size.
-    return 2.0 * CHIP * CHIP * (2 * RADIUS) * (2 * RADIUS)
+def pipeline_params(ar):
+    return ar.params(grid_spacing=SPACING, chip_size=CHIP, search_radius=RADIUS, upsampling=UP)
 
 
 class ClockSampler:
@@ -136,40 +141,46 @@ def measure_fp32_peak(torch, device):
     return best
 
 
-def profile_traffic():
-    """DRAM bytes per launch of the correlation kernel from the committed ncu summary."""
+def profile_traffic(points):
+    """DRAM bytes of one correlation launch over `points` searched points, from the committed
+    ncu capture of the same kernel (bytes per point measured on a smaller grid)."""
     f = ROOT / "profiles" / "k_corr_traffic.json"
     try:
         d = json.loads(f.read_text())
-        return d.get("bytes_per_point") * d.get("points_per_launch_full", 0) or None
-    except (OSError, ValueError, TypeError):
+        return float(d["bytes_per_point"]) * points
+    except (OSError, ValueError, TypeError, KeyError):
         return None
 
 
-def oracle_rate(O, a, b, valid, pts, target_s=12.0):
-    """Points/s of the oracle (all host threads) over a random sample sized for ~target_s."""
-    from autorift_b200.points import FIELDS
+def crop(a, n):
+    r0 = (a.shape[0] - n) // 2
+    return np.ascontiguousarray(a[r0:r0 + n, r0:r0 + n])
 
-    n = len(pts)
-    rng = np.random.default_rng(0)
-    order = rng.permutation(n)
 
-    def run(k):
-        idx = order[:k]
-        sub = {f: pts.flat(f)[idx] for f in FIELDS}
-        t = time.perf_counter()
-        O.track(a, b, sub, upsampling=UP, secondary_valid=valid, nthreads=0)
-        return time.perf_counter() - t
+def oracle_params(ar, p):
+    """The oracle's multichip parameter dict for a Params."""
+    o = p.outliers
+    g = isinstance(o, ar.GardnerFilter)
+    return dict(chip_base=p.chip_size_base, chip_min=p.chip_size_min, chip_max=p.chip_size_max,
+                aspect=p.chip_aspect, min_radius=p.min_search_radius, stride=p.coarse_stride,
+                buffer=p.coarse_buffer, min_frac=p.min_coarse_valid_fraction,
+                up=ar.upsampling(p.subpixel), measure=0, outliers=1 if g else 0,
+                window=o.window if g else 5, iterations=o.iterations if g else 3,
+                min_agree_fraction=o.min_agree_fraction if g else 0.32,
+                agree_tolerance=o.agree_tolerance if g else 0.2,
+                mad_scale=o.mad_scale if g else 4.0, fill_window=p.fill_window)
 
-    k = 64
-    dt = run(k)
-    while dt < 1.0 and k < n:
-        k = min(n, k * 4)
-        dt = run(k)
-    k2 = int(min(n, max(k, k * target_s / max(dt, 1e-6))))
-    if k2 > k:
-        k, dt = k2, run(k2)
-    return k / dt, k, dt
+
+def host_pipeline(O, ar, a, b, valid, p):
+    """The oracle's pipeline on the host cores (prepare both images, multichip over the
+    default grid); returns (grid points, seconds)."""
+    grid = ar.build_grid(a.shape, p)
+    fields = {f: getattr(grid, f) for f in ar.points.FIELDS}
+    t = time.perf_counter()
+    wr, wrm = O.prepare(a, None, "highpass", p.preprocess.width)
+    ws, wsm = O.prepare(b, valid, "highpass", p.preprocess.width)
+    O.multichip(wr, ws, fields, oracle_params(ar, p), wrm, wsm)
+    return len(grid), time.perf_counter() - t
 
 
 def gpu_arm(args):
@@ -187,49 +198,58 @@ def gpu_arm(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     ge.build()
     ar = ge.load_package()
-    ctx = ar._lib.Context(local)
-    a, b, valid, pts = load_workload(ar, args.spacing)
-    n = len(pts)
-    pair = ar.ImagePair(a, b, None, valid)
-    dp = pair.device(ctx)
+    L = ar._lib
+    ctx = L.Context(local)
+    lib = ctx.lib
+    a, b, valid = scene(ar, args.size)
+    p = pipeline_params(ar)
+    grid = ar.build_grid(a.shape, p)
+    gr, gc = grid.shape
+    n = gr * gc
     dev = torch.device("cuda", local)
-    cols = {f: torch.from_numpy(pts.flat(f)).to(dev) for f in ar.points.FIELDS}
-    dpts = ar._lib.ArPoints(*(cols[f].data_ptr() for f in ar.points.FIELDS), n)
-    out = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3)]
-    searched = torch.empty(n, dtype=torch.uint8, device=dev)
+    raw = ar.ImagePair(a, b, None, valid).device(ctx)  # resident before timing
+    cols = {f: torch.from_numpy(grid.flat(f)).to(dev) for f in ar.points.FIELDS}
+    dgrid = L.ArPoints(*(cols[f].data_ptr() for f in ar.points.FIELDS), n)
+    outs = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3)]
+    ochip = torch.empty(n, dtype=torch.int16, device=dev)
+    oint = torch.empty(n, dtype=torch.uint8, device=dev)
+    prm = ar.api.multichip_params(p)
+    opts = ar.track.prepare_options(p)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    # A created stream: its handle is non-null, so the library launches on it (a null handle
-    # would mean the library's own stream) and the events below bracket exactly its kernels.
-    stream = torch.cuda.Stream(dev)
-    torch.cuda.set_stream(stream)
-
-    import ctypes
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    torch.cuda.synchronize()
 
     def step():
-        ctx.check(ctx.lib.ar_track_device(
-            ctx.handle, dp.handle, ctypes.byref(dpts), UP, ar._lib.AR_ZNCC,
-            out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), searched.data_ptr(),
-            ctypes.c_void_p(stream.cuda_stream)))
+        prep = ctypes.c_void_p()
+        ctx.check(lib.ar_prepare(ctx.handle, raw.handle, ctypes.byref(opts), ctypes.byref(prep)))
+        try:
+            ctx.check(lib.ar_multichip_device(
+                ctx.handle, prep, ctypes.byref(dgrid), gr, gc, ctypes.byref(prm),
+                outs[0].data_ptr(), outs[1].data_ptr(), outs[2].data_ptr(), ochip.data_ptr(),
+                oint.data_ptr(), None))
+        finally:
+            lib.ar_pair_destroy(prep)
 
-    for _ in range(args.warmup):
-        flush.fill_(1)
-        step()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    ctx.set_timing(True)
-    ctx.kernel_times()
-    total_ms = 0.0
-    with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            flush.fill_(1)  # L2 flush outside the timed interval of each step
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record(stream)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            flush.fill_(1)
             step()
-            e.record(stream)
-            e.synchronize()
-            total_ms += s.elapsed_time(e)
-    torch.cuda.synchronize()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ctx.set_timing(True)
+        ctx.kernel_times()
+        total_ms = 0.0
+        with ClockSampler(local) as clk:
+            for _ in range(args.steps):
+                flush.fill_(1)  # L2 flush outside the timed interval of each step
+                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s.record(stream)
+                step()
+                e.record(stream)
+                e.synchronize()
+                total_ms += s.elapsed_time(e)
+        torch.cuda.synchronize()
     corr_ms, refine_ms, tracks, launches, corr_flops = ctx.kernel_times()
     ctx.set_timing(False)
     t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
@@ -240,76 +260,100 @@ def gpu_arm(args):
     ms_per_step = total_ms / args.steps
     value = world * n * args.steps / (total_ms * 1e-3)
 
-    nsearched = int(searched.sum().item())
-    fin = torch.isfinite(out[0])
-    med_dx = float(out[0][fin].median().item()) if fin.any() else float("nan")
+    dx = outs[0].cpu().numpy()
+    chip = ochip.cpu().numpy().view(np.uint16)
+    resolved = int(np.count_nonzero(chip))
+    levels = {int(c): int(np.count_nonzero(chip == c)) for c in np.unique(chip) if c}
+    med_dx = float(np.nanmedian(dx)) if resolved else float("nan")
 
-    # Roofline of the dominant kernel (the correlation): algorithmic FLOPs per launch (counted
-    # by the kernel: 2 * chip area * surface area per searched point) over its event-timed
-    # average duration, against the measured cuBLAS FP32 rate.
-    corr_avg = corr_ms / max(tracks, 1)
-    flops_launch = corr_flops / max(tracks, 1)
-    assert abs(flops_launch - flops_per_point() * nsearched) <= 1e-9 * flops_launch + 1, \
-        (flops_launch, flops_per_point() * nsearched)
-    achieved = flops_launch / (corr_avg * 1e-3) / 1e12
-    if args.profile:  # an ncu capture: the device steps only
+    # Roofline of the dominant kernel (the correlation): algorithmic FLOPs counted by the
+    # kernel (2 * chip area * surface area per searched point) over its event-timed duration,
+    # summed over the step's correlation launches, against the measured cuBLAS FP32 rate.
+    achieved = corr_flops / (corr_ms * 1e-3) / 1e12 if corr_ms > 0 else None
+    if args.profile:
         if rank == 0:
             print(json.dumps({"profile_run": True, "points": n, "ms_per_step": ms_per_step,
-                              "k_corr_ms": corr_avg, "k_refine_ms": refine_ms / max(tracks, 1)}))
+                              "k_corr_ms": corr_ms / args.steps,
+                              "k_refine_ms": refine_ms / args.steps}))
         if dist:
             dist.destroy_process_group()
         return
     fp32_peak = measure_fp32_peak(torch, dev)
-    traffic = profile_traffic()
+    eval_flops = 2.0 * CHIP * CHIP * (2 * RADIUS) ** 2
+    fine_points = corr_flops / max(tracks, 1) / eval_flops  # chip-32 evaluations per launch
 
-    # End to end through the C ABI with host buffers (pair upload, point upload, download).
-    host_pts = pts
+    # End to end through the C ABI from host buffers: the caller's column-major arrays (the
+    # Julia layout) and grid, pair upload, prepare, multichip, download; per-pair latency.
+    ha = np.asfortranarray(a)
+    hb = np.asfortranarray(b)
+    hv = np.asfortranarray(valid.astype(np.uint8))
+    hcols = {f: np.ascontiguousarray(grid.flat(f)) for f in ar.points.FIELDS}
+    hgrid = L.ArPoints(*(hcols[f].ctypes.data for f in ar.points.FIELDS), n)
+    hout = [np.empty(n, np.float32) for _ in range(3)]
+    hchip = np.empty(n, np.uint16)
+    hint = np.empty(n, np.uint8)
     e2e_times = []
     for it in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        p2 = ar.ImagePair(a, b, None, valid)
-        d = ar.track(p2, host_pts, ar.params(preprocess="none", quantize="none", upsampling=UP),
-                     ctx=ctx)
-        p2._device.clear()
+        rp, pp = ctypes.c_void_p(), ctypes.c_void_p()
+        ctx.check(lib.ar_pair_upload(ctx.handle, ha.ctypes.data, hb.ctypes.data, None,
+                                     hv.ctypes.data, args.size, args.size, L.AR_U16,
+                                     ctypes.byref(rp)))
+        ctx.check(lib.ar_prepare(ctx.handle, rp, ctypes.byref(opts), ctypes.byref(pp)))
+        ctx.check(lib.ar_multichip(ctx.handle, pp, ctypes.byref(hgrid), gr, gc, ctypes.byref(prm),
+                                   hout[0].ctypes.data, hout[1].ctypes.data, hout[2].ctypes.data,
+                                   hchip.ctypes.data, hint.ctypes.data))
+        lib.ar_pair_destroy(pp)
+        lib.ar_pair_destroy(rp)
         t1 = time.perf_counter()
         if it >= args.warmup:
             e2e_times.append(t1 - t0)
     e2e_value = world * n / float(np.mean(e2e_times))
-    e2e_p50 = float(np.percentile(e2e_times, 50)) * 1e3
-    e2e_p99 = float(np.percentile(e2e_times, 99)) * 1e3
-    h2d = a.nbytes + b.nbytes + 2 * a.size + n * 48
-    d2h = n * 13
+    h2d = ha.nbytes + hb.nbytes + hv.nbytes + 6 * 8 * n
+    d2h = n * (4 + 4 + 4 + 2 + 1)
+    same = bool(np.array_equal(hchip, chip)) and bool(
+        np.array_equal(hout[0].view(np.uint32), dx.view(np.uint32)))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
-        rate, k, dt = oracle_rate(O, a, b, valid, pts)
-        cpu = {"value": rate, "unit": UNIT, "cores": O.max_threads(), "kind": "port",
-               "sample": f"{k} of {n} points of the same workload, {dt:.1f} s"}
+        O.build()
+        pts, dt = host_pipeline(O, ar, crop(a, CROP), crop(b, CROP), crop(valid, CROP), p)
+        cpu = {"value": pts / dt, "unit": UNIT, "cores": O.max_threads(), "kind": "port",
+               "sample": f"the same pipeline on a centred {CROP}^2 crop ({pts} grid points), "
+                         f"{dt:.1f} s"}
 
     peaks = measured_peaks()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "points": n, "searched": nsearched,
-                       "chip": CHIP, "radius": RADIUS, "upsampling": UP, "image": [N, N],
-                       "element_type": "uint8", "l2": "flushed (256 MiB write) between steps",
-                       "parallelism": f"{world} independent replicas",
-                       "median_dx": med_dx},
+            "config": {"workload": WORKLOAD, "points": n, "grid": [gr, gc],
+                       "resolved": resolved, "points_per_chip_size": levels,
+                       "chip": CHIP, "radius": RADIUS, "upsampling": UP,
+                       "image": [args.size, args.size], "element_type": "uint16 -> uint8",
+                       "masks": "secondary no-data mask passed",
+                       "l2": "flushed (256 MiB write) between steps",
+                       "parallelism": f"{world} independent replicas", "median_dx": med_dx},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
-                         "unit": "TFLOP/s", "frac": achieved / fp32_peak if fp32_peak else None,
-                         "traffic": traffic, "kernel": "k_corr",
+                         "unit": "TFLOP/s",
+                         "frac": achieved / fp32_peak if (achieved and fp32_peak) else None,
+                         "traffic": profile_traffic(fine_points), "kernel": "k_corr",
                          "peak_source": "measured cuBLAS FP32 SGEMM (TF32 off) in this run; "
                                         "no FP32 figure in MEASURED_PEAKS.json",
-                         "kernel_ms": {"k_corr": corr_avg, "k_refine": refine_ms / max(tracks, 1)},
+                         "kernel_ms_per_step": {"k_corr": corr_ms / args.steps,
+                                                "k_refine": refine_ms / args.steps},
+                         "correlation_launches_per_step": tracks / args.steps,
                          "measured_peaks": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops")}},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "p50_ms": e2e_p50, "p99_ms": e2e_p99,
-                    "path": "ar_pair_upload + ar_track (host buffers) per step"},
+                    "d2h_bytes_per_step": d2h,
+                    "p50_ms": float(np.percentile(e2e_times, 50)) * 1e3,
+                    "p99_ms": float(np.percentile(e2e_times, 99)) * 1e3,
+                    "path": "ar_pair_upload + ar_prepare + ar_multichip (host buffers) per pair",
+                    "same_result_as_device_run": same},
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
         }
@@ -330,24 +374,29 @@ def reference_arm(args):
     from oracle import oracle as O
 
     O.build()
-    a, b, valid, pts = load_workload(ar)
-    n = len(pts)
+    a, b, valid = scene(ar, args.size)
+    p = pipeline_params(ar)
+    ca, cb, cv = crop(a, CROP), crop(b, CROP), crop(valid, CROP)
     rates = []
+    pts = 0
     for it in range(args.warmup + args.steps):
-        rate, k, dt = oracle_rate(O, a, b, valid, pts, target_s=max(2.0, 30.0 / (args.steps + args.warmup)))
+        pts, dt = host_pipeline(O, ar, ca, cb, cv, p)
         if it >= args.warmup:
-            rates.append(rate)
+            rates.append(pts / dt)
     value = float(np.mean(rates))
+    n = len(ar.build_grid(a.shape, p))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": n / value * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": pts / value * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "points": n, "chip": CHIP, "radius": RADIUS,
-                   "upsampling": UP, "image": [N, N], "element_type": "uint8"},
+                   "upsampling": UP, "image": [args.size, args.size],
+                   "element_type": "uint16 -> uint8"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": O.max_threads(), "kind": "port",
-                         "sample": f"{k} of {n} points per step (Julia is not installed; the "
-                                   "C++ restatement of the reference's algorithm)"},
+                         "sample": f"the same pipeline on a centred {CROP}^2 crop ({pts} grid "
+                                   "points) per step (Julia is not installed; the C++ "
+                                   "restatement of the reference's algorithm)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -360,8 +409,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--spacing", type=int, default=SPACING,
-                    help="grid spacing; the benchmark line uses 8, profiles use a sparser grid")
+    ap.add_argument("--size", type=int, default=N,
+                    help="image side; the benchmark line uses 4096, profiles a smaller scene")
     ap.add_argument("--profile", action="store_true",
                     help="time the device steps only (for ncu captures); no JSON bench line")
     args = ap.parse_args()

@@ -177,6 +177,21 @@ int ar_multichip(ar_ctx* ctx, const ar_pair* pair, const ar_points* grid, int64_
                  float* correlation, uint16_t* chip_size, uint8_t* interpolated);
 
 /*
+ * ar_multichip with the grid fields and the outputs in device memory, run on `stream` (NULL:
+ * the context's stream). The grid coordinates and priors must be finite (not re-checked on
+ * the device). Each level reads a few counters back to take the reference's early exits, so
+ * the call returns once the search has completed on `stream`.
+ */
+int ar_multichip_device(ar_ctx* ctx, const ar_pair* pair, const ar_points* grid_dev,
+                        int64_t grid_rows, int64_t grid_cols, const ar_multichip_params* params,
+                        float* dx_dev, float* dy_dev, float* correlation_dev,
+                        uint16_t* chip_size_dev, uint8_t* interpolated_dev, void* stream);
+
+/* The context's own CUDA stream (cudaStream_t), on which calls without a stream argument run;
+ * for callers that order their own work or timing events after the library's. */
+int ar_ctx_stream(ar_ctx* ctx, void** stream);
+
+/*
  * The surface of one chip against one search window (correlate!, src/correlate.jl:528-557),
  * for host arrays: `search` is (ch+2ry-1) x (cw+2rx-1), `chip` ch x cw, `surface` 2ry x 2rx,
  * all column-major of `dtype`/float. `degenerate` receives 1 for a constant chip

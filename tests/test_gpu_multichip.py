@@ -59,7 +59,7 @@ def test_multilevel_banded_scene(ar, O, gpu_lib):
 
 
 def test_no_outlier_filter_and_ncc(ar, O, gpu_lib):
-    a, b, sv = u16_scene(ar, n=480, seed=9)
+    a, b, sv = u16_scene(ar, n=640, seed=9)
     for kw in (dict(outliers="none"), dict(similarity="ncc"), dict(fill_window=5, mad_scale=3.0)):
         p = ar.params(grid_spacing=16, **kw)
         prep = ar.prepare(ar.ImagePair(a, b, None, sv), p)
