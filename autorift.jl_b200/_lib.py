@@ -45,6 +45,7 @@ class ArMultichipParams(ctypes.Structure):
 
 
 AR_PRE_NONE, AR_PRE_HIGHPASS, AR_PRE_WALLIS = 0, 1, 2
+AR_OPT_TENSOR_CORES = 1
 AR_QUANT_NONE, AR_QUANT_UINT8 = 0, 1
 
 
@@ -78,6 +79,8 @@ SIGNATURES = {
     "ar_multichip_device": (_i32, [_p, _p, ctypes.POINTER(ArPoints), _i64, _i64,
                                    ctypes.POINTER(ArMultichipParams), _p, _p, _p, _p, _p, _p]),
     "ar_ctx_stream": (_i32, [_p, ctypes.POINTER(_p)]),
+    "ar_ctx_set_option": (_i32, [_p, ctypes.c_int, ctypes.c_int]),
+    "ar_tc_selftest": (_i32, [_p, _p, ctypes.c_int, _p, ctypes.c_int, _p, _p]),
     "ar_ctx_set_timing": (_i32, [_p, _i32]),
     "ar_kernel_times": (_i32, [_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                ctypes.POINTER(_i64), ctypes.POINTER(_i64),
@@ -136,6 +139,9 @@ class Context:
 
     def set_timing(self, enable: bool):
         self.check(self.lib.ar_ctx_set_timing(self.handle, int(bool(enable))))
+
+    def set_option(self, option: int, value: int):
+        self.check(self.lib.ar_ctx_set_option(self.handle, int(option), int(value)))
 
     def stream(self) -> int:
         """The context's CUDA stream handle."""

@@ -279,6 +279,7 @@ int ar_ctx_destroy(ar_ctx* c) {
         cudaFree(c->scratch.sub_origin);
         cudaFree(c->scratch.sub_patch);
         cudaFree(c->scratch.geom);
+        cudaFree(c->scratch.status);
         for (auto& r : c->scratch.timer.recs)
             for (auto ev : r) c->scratch.timer.pool.push_back(ev);
         for (auto ev : c->scratch.timer.pool) cudaEventDestroy(ev);
@@ -437,6 +438,10 @@ int ar_track(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up, int meas
     if (e == cudaSuccess) e = stage_d2h(c, corr, dout.corr, n * 4);
     if (e == cudaSuccess) e = stage_d2h(c, searched, dout.searched, n);
     if (e != cudaSuccess) return cuda_fail(c, e, "ar_track: download results");
+    int st = 0;
+    e = ar::read_status(c->scratch, c->stream, &st);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ar_track: status");
+    if (st) return fail(c, AR_ERR_TIMEOUT, "ar_track: a device wait ran out; results incomplete");
     return AR_OK;
 }
 
@@ -733,6 +738,10 @@ int multichip_run(ar_ctx* c, const ar_pair* p, const double* gx, const double* g
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess)
         return err.empty() ? cuda_fail(c, e, "ar_multichip") : fail(c, AR_ERR_UNSUPPORTED, err);
+    int st = 0;
+    e = ar::read_status(c->scratch, s, &st);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ar_multichip: status");
+    if (st) return fail(c, AR_ERR_TIMEOUT, "ar_multichip: a device wait ran out; results incomplete");
     return AR_OK;
 }
 
@@ -805,6 +814,52 @@ int ar_multichip_device(ar_ctx* c, const ar_pair* p, const ar_points* grid, int6
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
     return multichip_run(c, p, grid->x, grid->y, grid->radius_x, grid->radius_y, grid->dx_prior,
                          grid->dy_prior, gr, gc, prm, dx, dy, corr, chip, interp, s);
+}
+
+int ar_tc_selftest(ar_ctx* c, const uint8_t* a_img, int a_bytes, const uint8_t* b_img,
+                   int b_bytes, const int* params, int32_t* d_out) {
+    if (!c || !a_img || !b_img || !params || !d_out) return fail(c, AR_ERR_ARG, "null argument");
+    if (a_bytes <= 0 || b_bytes <= 0 || a_bytes > 96 * 1024 || b_bytes > 96 * 1024)
+        return fail(c, AR_ERR_SIZE, "operand images must be 1..96 KiB");
+    const int N = params[9];
+    if (N < 8 || N > 256) return fail(c, AR_ERR_ARG, "invalid N");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    unsigned char *da = nullptr, *db = nullptr, *dd = nullptr;
+    const size_t dbytes = static_cast<size_t>(128) * N * 4 + 16;
+    cudaError_t e = dalloc(c, &da, a_bytes);
+    if (e == cudaSuccess) e = dalloc(c, &db, b_bytes);
+    if (e == cudaSuccess) e = dalloc(c, &dd, dbytes);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(da, a_img, a_bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(db, b_img, b_bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dd, 0, dbytes, c->stream);
+    int* status = reinterpret_cast<int*>(dd + static_cast<size_t>(128) * N * 4);
+    std::string err;
+    if (e == cudaSuccess)
+        e = ar::tc_probe(da, a_bytes, db, b_bytes, params, reinterpret_cast<int32_t*>(dd), status,
+                         c->stream, &err);
+    int hstatus = 0;
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_out, dd, static_cast<size_t>(128) * N * 4, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    dfree(c, da);
+    dfree(c, db);
+    dfree(c, dd);
+    if (e != cudaSuccess)
+        return err.empty() ? cuda_fail(c, e, "ar_tc_selftest") : fail(c, AR_ERR_ARG, err);
+    if (hstatus != 0) return fail(c, AR_ERR_TIMEOUT, "the tensor-core product did not complete in time");
+    return AR_OK;
+}
+
+int ar_ctx_set_option(ar_ctx* c, int option, int value) {
+    if (!c) return AR_ERR_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    switch (option) {
+        case AR_OPT_TENSOR_CORES: c->scratch.tensor_cores = value != 0; return AR_OK;
+        default: return fail(c, AR_ERR_ARG, "unknown option");
+    }
 }
 
 int ar_ctx_stream(ar_ctx* c, void** stream) {

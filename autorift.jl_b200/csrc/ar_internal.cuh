@@ -63,7 +63,14 @@ struct TrackScratch {
     // Recorded after the last pass that used these buffers; a pass on another stream waits
     // for it before reusing them.
     cudaEvent_t done = nullptr;
+    // Set by a kernel whose bounded wait ran out (read and cleared by the synchronous calls).
+    int* status = nullptr;
+    // UInt8 passes use the tensor-core correlation when their geometry fits it.
+    bool tensor_cores = true;
 };
+
+// Reads and clears the pass status; AR-style: 0 ok, 1 a bounded device wait ran out.
+cudaError_t read_status(TrackScratch& scratch, cudaStream_t stream, int* status);
 
 // Host-side pass geometry of a host point set.
 PassGeometry pass_geometry_host(const ar_points& p, int64_t nrows, int64_t ncols);
@@ -143,6 +150,12 @@ struct MultichipJob {
     size_t arena_bytes;
 };
 size_t multichip_arena_bytes(int64_t gr, int64_t gc);
+
+// One tensor-core product of two shared-memory operand images (the layout self-test):
+// params = {a_off, a_lbo, a_sbo, a_kstep, b_off, b_lbo, b_sbo, b_kstep, M, N, nk}.
+cudaError_t tc_probe(const uint8_t* a_img, int a_bytes, const uint8_t* b_img, int b_bytes,
+                     const int* params, int32_t* d_out, int* status, cudaStream_t s,
+                     std::string* err);
 cudaError_t run_multichip(const MultichipJob& job, TrackScratch& scratch, int num_sms,
                           cudaStream_t stream, std::string* errmsg);
 

@@ -32,6 +32,7 @@
 #include <string>
 
 #include "ar_internal.cuh"
+#include "ar_tc.cuh"
 
 namespace ar {
 namespace {
@@ -511,6 +512,423 @@ __global__ void __launch_bounds__(kCorrThreads, 2) k_corr(const CorrArgs A) {
 }
 
 // ----------------------------------------------------------------------------------------------
+// Tensor-core correlation for UInt8 imagery (tcgen05.mma kind::i8, exact 32-bit accumulation).
+//
+// The numerator S[i, j] = sum_{a,b} C[a, b] W[i + a, j + b] (C the chip, W the window, i the
+// surface row, j the surface column) is one product D[j, i] = sum_k A[j, k] B[i, k] over
+// K = (16-row block q of the window, chip column b, row r within the block):
+//   A[j, (q, b, r)] = W'[16 q + r, j + b]          the window as 16-byte blocks s_W[q][x][r];
+//                                                  row j of A starts 16 bytes after row j - 1,
+//                                                  so A is read in place;
+//   B[i, (q, b, r)] = C[16 q + r - delta - i, b]    the chip as 16-byte rows per column b,
+//                                                  E_b[u][r] = C[r - u - delta, b] with
+//                                                  u = i - 16 q, built once per point.
+// W' starts at the 16-aligned image row `delta` rows above the window's first row, so each
+// 16-byte block of a column-major image with 16-aligned columns is one aligned load. One MMA
+// (M = 64 surface columns, N surface rows rounded to 16, K = 32: two chip columns) per
+// (q, column pair), accumulated in Tensor Memory. The products are exact (u8 x u8 summed below
+// 2^31), so the numerator equals the CUDA-core kernel's and every surface value, the peak and
+// the patch are bit-identical to it.
+//
+// Normalising all 2ry x 2rx values in FP64 would cost as much as the products, and only the
+// peak and its 5 x 5 patch are read. So every value is first estimated in FP32 from exact
+// integers (numerator nn*D - sum(C)*s1 and variance nn*s2 - s1^2 as 64-bit integers): the
+// estimate is within 10 * 2^-24 relative of the FP32 surface value. Values whose estimate
+// cannot reach the largest one are not evaluated; the others, the patch and any value whose
+// variance is too small for the bound get the exact FP64 normalisation of the reference.
+
+constexpr int kTcThreads = 256;
+constexpr int kPadL = 32;            // zero bytes before each staged chip column
+constexpr uint32_t kTcWaitPolls = 1u << 22;
+
+struct TcArgs {
+    const uint8_t* ref;
+    const uint8_t* sec;
+    const uint8_t* valid;
+    int64_t nrows, ncols;
+    DevPoints pts;
+    int64_t padx, pady;
+    int up, measure;
+    int NMMA, QM, QS, PS, PC, XS, NRS, NRM, NCM, CHM;
+    int u_min;                       // lowest stored row of the E planes
+    unsigned off_W, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
+    uint32_t tmem_cols;
+    DevOutputs out;
+    int* sub_count;
+    int64_t* sub_point;
+    int32_t* sub_origin;
+    float* sub_patch;
+    float* surf_out;
+    unsigned long long* flops;
+    int* status;                     // set to 1 when a tensor-core wait ran out
+};
+
+// The reference's normalisation of one value from its exact integer numerator and box sums
+// (the raw-numerator branch of k_corr).
+__device__ __forceinline__ float tc_exact(uint32_t D, uint32_t S1, uint32_t S2, double mean,
+                                          double nn, double cnorm, int measure) {
+    const double s1 = static_cast<double>(S1), s2 = static_cast<double>(S2);
+    const double num = __dsub_rn(static_cast<double>(D), __dmul_rn(mean, s1));
+    double den;
+    if (measure == AR_NCC) {
+        den = __dmul_rn(cnorm, __dsqrt_rn(s2 > 0.0 ? s2 : 0.0));
+    } else {
+        double wvar = __dsub_rn(s2, __ddiv_rn(__dmul_rn(s1, s1), nn));
+        if (!(wvar > 0.0)) wvar = 0.0;
+        den = __dmul_rn(cnorm, __dsqrt_rn(wvar));
+    }
+    return den > 0.0 ? __double2float_rn(__ddiv_rn(num, den)) : 0.0f;
+}
+
+// FP32 estimate of the same value; NaN when the variance is too small for the error bound.
+__device__ __forceinline__ float tc_estimate(uint32_t D, uint32_t S1, uint32_t S2, long long nn,
+                                             long long csum, float k, int measure) {
+    const long long nx = nn * static_cast<long long>(D) - csum * static_cast<long long>(S1);
+    const long long sq = nn * static_cast<long long>(S2);
+    const long long vx = measure == AR_NCC ? static_cast<long long>(S2)
+                                           : sq - static_cast<long long>(S1) * S1;
+    if (measure != AR_NCC && vx < (sq >> 20)) return __int_as_float(0x7fc00000);
+    if (vx <= 0 || nx == 0) return 0.0f;
+    return __fmul_rn(__fmul_rn(static_cast<float>(nx), rsqrtf(static_cast<float>(vx))), k);
+}
+
+__device__ __forceinline__ float tc_tol(float v) {
+    return fabsf(v) * 7.152557373046875e-07f + 1e-30f;  // 12 * 2^-24 relative
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) k_corr_tc(const TcArgs A) {
+    extern __shared__ __align__(1024) unsigned char smem_tc[];
+    __shared__ uint64_t s_mbar;
+    __shared__ uint32_t s_taddr;
+    __shared__ int s_slot;
+    __shared__ float s_fmax[kTcThreads / 32];
+    uint8_t* s_E = smem_tc;
+    uint8_t* s_W = smem_tc + A.off_W;
+    uint8_t* s_P = smem_tc + A.off_P;
+    uint32_t* s_V1 = reinterpret_cast<uint32_t*>(smem_tc + A.off_V);
+    uint32_t* s_S1 = reinterpret_cast<uint32_t*>(smem_tc + A.off_S1);
+    uint32_t* s_S2 = reinterpret_cast<uint32_t*>(smem_tc + A.off_S2);
+    uint32_t* s_num = reinterpret_cast<uint32_t*>(smem_tc + A.off_num);
+    float* s_est = reinterpret_cast<float*>(smem_tc + A.off_est);
+    double* s_red = reinterpret_cast<double*>(smem_tc + A.off_red);
+
+    const int tid = threadIdx.x, bd = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int64_t NR = A.nrows + 2 * A.pady, NC = A.ncols + 2 * A.padx;
+    const double shx = static_cast<double>(A.padx) + 0.5;
+    const double shy = static_cast<double>(A.pady) + 0.5;
+
+    // E rows outside each point's band stay zero for the whole launch.
+    for (int e = tid * 16; e < static_cast<int>(A.off_W); e += bd * 16)
+        *reinterpret_cast<uint4*>(s_E + e) = make_uint4(0, 0, 0, 0);
+    if (warp == 0) {
+        tc::tmem_alloc(&s_taddr, A.tmem_cols);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0) {
+        tc::mbar_init(&s_mbar, 1);
+        tc::fence_mbar_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t taddr = s_taddr;
+    uint32_t phase = 0;
+    bool failed = false;
+
+    for (int64_t k = blockIdx.x; k < A.pts.n; k += gridDim.x) {
+        tc::fence_before_sync();
+        __syncthreads();  // the previous point's buffers and accumulator are no longer read
+        tc::fence_after_sync();
+        const int64_t prx = A.pts.rx[k], pry = A.pts.ry[k];
+        if (!(prx > 0 && pry > 0)) continue;
+        const double xs = A.pts.x[k] + shx, ys = A.pts.y[k] + shy;
+        const int64_t hx = A.pts.csx[k] / 2, hy = A.pts.csy[k] / 2;
+        const int64_t ccx = static_cast<int64_t>(floor(__dsub_rn(xs, A.pts.dx0[k])));
+        const int64_t ccy = static_cast<int64_t>(floor(__dsub_rn(ys, A.pts.dy0[k])));
+        const int64_t wcx = static_cast<int64_t>(floor(xs)), wcy = static_cast<int64_t>(floor(ys));
+        const int64_t cr0 = ccy - hy, cr1 = ccy + hy - 1, cc0 = ccx - hx, cc1 = ccx + hx - 1;
+        const int64_t wr0 = wcy - hy - pry, wr1 = wcy + hy + pry - 2;
+        const int64_t wc0 = wcx - hx - prx, wc1 = wcx + hx + prx - 2;
+        const bool chip_in = (cr1 < cr0 || cc1 < cc0) ||
+                             (cr0 >= 1 && cr1 <= NR && cc0 >= 1 && cc1 <= NC);
+        const bool win_in = (wr1 < wr0 || wc1 < wc0) ||
+                            (wr0 >= 1 && wr1 <= NR && wc0 >= 1 && wc1 <= NC);
+        if (!chip_in || !win_in) continue;
+        const int ch = static_cast<int>(2 * hy), cw = static_cast<int>(2 * hx);
+        const int nr = static_cast<int>(2 * pry), nc = static_cast<int>(2 * prx);
+        if (ch <= 0 || cw <= 0) continue;
+        if (ch > A.CHM || nr > A.NRM || nc > A.NCM || nc > 64) continue;  // not sized for
+        const int64_t chip_r = cr0 - 1 - A.pady, chip_c = cc0 - 1 - A.padx;
+        const int64_t win_r = wr0 - 1 - A.pady, win_c = wc0 - 1 - A.padx;
+
+        // _any_valid over the chip (src/track.jl:416-421).
+        int any = 0;
+        for (int e = tid; e < ch * cw; e += bd) {
+            const int64_t r = chip_r + e % ch, c = chip_c + e / ch;
+            if (r >= 0 && r < A.nrows && c >= 0 && c < A.ncols && A.valid[r + c * A.nrows])
+                any = 1;
+        }
+        if (!__syncthreads_or(any)) continue;
+        if (tid == 0) A.out.searched[k] = 1;
+
+        // prepare_chip! statistics in the CUDA-core kernel's order (bit-identical sums), and
+        // the chip staged as zero-padded byte columns.
+        double st[1] = {0.0};
+        for (int e = tid; e < ch * cw; e += bd)
+            st[0] = __dadd_rn(st[0], pixel(A.sec, A.nrows, A.ncols, chip_r + e % ch, chip_c + e / ch));
+        block_sum_f64<1>(st, s_red);
+        const double nn = static_cast<double>(ch * cw);
+        const double mean = __ddiv_rn(st[0], nn);
+        const int chp = (ch + kUA - 1) & ~(kUA - 1);
+        double acc2[1] = {0.0};
+        for (int e = tid; e < chp * cw; e += bd) {
+            const int a = e % chp, b = e / chp;
+            if (a < ch) {
+                const double v = pixel(A.sec, A.nrows, A.ncols, chip_r + a, chip_c + b);
+                const double d = __dsub_rn(v, mean);
+                acc2[0] = __dadd_rn(acc2[0], __dmul_rn(d, d));
+                s_P[b * A.PC + kPadL + a] = static_cast<uint8_t>(v);
+            }
+        }
+        for (int e = tid; e < cw * A.PC; e += bd) {
+            const int b = e / A.PC, o = e % A.PC;
+            if (o < kPadL || o >= kPadL + ch) s_P[b * A.PC + o] = 0;
+        }
+        block_sum_f64<1>(acc2, s_red);
+        const double sq = acc2[0];
+        if (!(sq > __dmul_rn(__dmul_rn(DBL_EPSILON, static_cast<double>(ch)), static_cast<double>(cw))))
+            continue;  // degenerate chip: searched, no measurement (src/track.jl:286)
+        const double cnorm = __dsqrt_rn(sq);
+        const long long csum = static_cast<long long>(st[0]);
+        const long long nnl = static_cast<long long>(ch) * cw;
+
+        // Window blocks W'[16 q + r][x], x in [0, XS): 16 image rows from base_r per block.
+        const int64_t delta = ((win_r % 16) + 16) % 16;
+        const int64_t base_r = win_r - delta;
+        const int Q = static_cast<int>((delta + ch + nr - 1 + 15) / 16);
+        for (int e = tid; e < Q * A.XS; e += bd) {
+            const int q = e / A.XS, x = e % A.XS;
+            const int64_t r0 = base_r + 16 * q, c = win_c + x;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (c >= 0 && c < A.ncols) {
+                const uint8_t* col = A.ref + c * A.nrows;
+                if (r0 >= 0 && r0 + 16 <= A.nrows &&
+                    (reinterpret_cast<uintptr_t>(col + r0) & 15) == 0) {
+                    v = __ldg(reinterpret_cast<const uint4*>(col + r0));
+                } else {
+                    uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+                    for (int t = 0; t < 16; ++t) {
+                        const int64_t r = r0 + t;
+                        const uint32_t b = (r >= 0 && r < A.nrows) ? col[r] : 0u;
+                        w[t >> 2] |= b << (8 * (t & 3));
+                    }
+                    v = make_uint4(w[0], w[1], w[2], w[3]);
+                }
+            }
+            *reinterpret_cast<uint4*>(s_W + q * A.QS + x * 16) = v;
+        }
+        __syncthreads();  // s_P complete
+        // The band of E rows a chip of height <= CHM can reach for any delta.
+        const int u_lo = -(A.CHM + 15), nband = A.CHM + 31;
+        for (int e = tid; e < cw * nband; e += bd) {
+            const int b = e / nband, u = u_lo + e % nband;
+            const int src = b * A.PC + kPadL - u - static_cast<int>(delta);
+            const uint32_t* w = reinterpret_cast<const uint32_t*>(s_P + (src & ~3));
+            const uint32_t sh = static_cast<uint32_t>(src & 3) * 8u;
+            uint4 o;
+            o.x = __funnelshift_r(w[0], w[1], sh);
+            o.y = __funnelshift_r(w[1], w[2], sh);
+            o.z = __funnelshift_r(w[2], w[3], sh);
+            o.w = __funnelshift_r(w[3], w[4], sh);
+            *reinterpret_cast<uint4*>(s_E + b * A.PS + (u - A.u_min) * 16) = o;
+        }
+        tc::fence_proxy_async_smem();
+        __syncthreads();
+
+        if (tid == 0) {
+            tc::fence_after_sync();
+            const uint32_t sW = tc::smem_u32(s_W), sE = tc::smem_u32(s_E);
+            const uint32_t idesc = tc::idesc_u8_s32(64, A.NMMA);
+            bool acc = false;
+            for (int q = 0; q < Q; ++q)
+                for (int t = 0; t < cw / 2; ++t) {
+                    const uint64_t da = tc::smem_desc(sW + q * A.QS + 32 * t, 16, 128);
+                    const uint64_t db = tc::smem_desc(
+                        sE + 2 * t * A.PS + (-16 * q - A.u_min) * 16, A.PS, 128);
+                    tc::mma_u8(taddr, da, db, idesc, acc);
+                    acc = true;
+                }
+            tc::mma_commit(&s_mbar);
+        }
+
+        // While the tensor core runs: box sums of W and W^2 (integral_both!, boxsum,
+        // src/integral.jl:141-170, 244-247) as exact integers. V[i][x] sums ch rows down
+        // column x; S[j][i] sums cw columns of V.
+        const int XW = cw + nc - 1;
+        uint32_t* s_V2 = s_V1 + A.NRM * XW;
+        const int nseg = (nr + 15) >> 4;
+        for (int task = tid; task < XW * nseg; task += bd) {
+            const int x = task % XW, seg = task / XW;
+            const int i0 = seg << 4, i1 = min(i0 + 16, nr);
+            auto wat = [&](int rr) -> uint32_t {
+                const int rp = rr + static_cast<int>(delta);
+                return s_W[(rp >> 4) * A.QS + x * 16 + (rp & 15)];
+            };
+            uint32_t h1 = 0, h2 = 0;
+            for (int a = 0; a < ch; ++a) {
+                const uint32_t w = wat(i0 + a);
+                h1 += w;
+                h2 += w * w;
+            }
+            for (int i = i0; i < i1; ++i) {
+                s_V1[i * XW + x] = h1;
+                s_V2[i * XW + x] = h2;
+                if (i + 1 < i1) {
+                    const uint32_t wn = wat(i + ch), wo = wat(i);
+                    h1 = h1 + wn - wo;
+                    h2 = h2 + wn * wn - wo * wo;
+                }
+            }
+        }
+        __syncthreads();
+        const int jseg = (nc + 15) >> 4;
+        for (int task = tid; task < nr * jseg; task += bd) {
+            const int i = task % nr, seg = task / nr;
+            const int j0 = seg << 4, j1 = min(j0 + 16, nc);
+            uint32_t g1 = 0, g2 = 0;
+            for (int b = 0; b < cw; ++b) {
+                g1 += s_V1[i * XW + j0 + b];
+                g2 += s_V2[i * XW + j0 + b];
+            }
+            for (int j = j0; j < j1; ++j) {
+                s_S1[j * A.NRS + i] = g1;
+                s_S2[j * A.NRS + i] = g2;
+                if (j + 1 < j1) {
+                    g1 = g1 + s_V1[i * XW + j + cw] - s_V1[i * XW + j];
+                    g2 = g2 + s_V2[i * XW + j + cw] - s_V2[i * XW + j];
+                }
+            }
+        }
+
+        // Wait for the products (bounded; every thread polls the same barrier phase).
+        const bool ok = tc::mbar_wait(&s_mbar, phase, kTcWaitPolls);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicExch(A.status, 1);
+            failed = true;
+            break;
+        }
+        tc::fence_after_sync();
+
+        // Pass 1: numerators out of Tensor Memory, estimates, their maximum. Rows j of the
+        // M = 64 accumulator live in lanes (j % 16) + 32 (j / 16); warp w reads its quarter's
+        // first 16 lanes, columns from 32 (w / 4) in steps of 64.
+        const float kk = __double2float_rn(
+            A.measure == AR_NCC ? __drcp_rn(__dmul_rn(cnorm, nn))
+                                : __drcp_rn(__dmul_rn(cnorm, __dsqrt_rn(nn))));
+        const int quarter = warp & 3, half = warp >> 2;
+        const int j = 16 * quarter + (lane & 15);
+        const bool jv = lane < 16 && j < nc;
+        float lmax = -INFINITY;
+        for (int i0 = 32 * half; i0 < nr; i0 += 64) {
+            for (int c = 0; c < 32; c += 16) {
+                const int ii = i0 + c;
+                if (ii >= nr) break;  // warp-uniform
+                uint32_t r[16];
+                tc::tmem_ld16(taddr + (static_cast<uint32_t>(32 * quarter) << 16) +
+                                  static_cast<uint32_t>(ii), r);
+                tc::tmem_wait_ld();
+#pragma unroll
+                for (int m = 0; m < 16; ++m) {
+                    const int i = ii + m;
+                    if (jv && i < nr) {
+                        const int o = j * A.NRS + i;
+                        const float est = tc_estimate(r[m], s_S1[o], s_S2[o], nnl, csum, kk, A.measure);
+                        s_num[o] = r[m];
+                        s_est[o] = est;
+                        lmax = fmaxf(lmax, est);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(kFull, lmax, o));
+        if (lane == 0) s_fmax[warp] = lmax;
+        __syncthreads();
+        float M = s_fmax[0];
+        for (int w = 1; w < kTcThreads / 32; ++w) M = fmaxf(M, s_fmax[w]);
+        const float floor_v = M - tc_tol(M);
+
+        // Pass 2: exact values where the estimate can reach the maximum; the peak key.
+        unsigned long long best = 0ull;
+        for (int e = tid; e < nr * nc; e += bd) {
+            const int i = e % nr, jj = e / nr;
+            const int o = jj * A.NRS + i;
+            const float est = s_est[o];
+            if (!(est + tc_tol(est) >= floor_v) && !isnan(est)) continue;
+            const float v = tc_exact(s_num[o], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+            const unsigned long long kk2 = argmax_key(v, static_cast<unsigned>(i * nc + jj));
+            best = kk2 > best ? kk2 : best;
+        }
+        best = block_max_u64(best, reinterpret_cast<unsigned long long*>(s_red));
+        if (A.flops && tid == 0)
+            atomicAdd(A.flops, 2ull * static_cast<unsigned long long>(ch) * cw * nr * nc);
+        if (A.surf_out) {
+            float* so = A.surf_out + k * static_cast<int64_t>(A.NRM) * A.NCM;
+            for (int e = tid; e < nr * nc; e += bd) {
+                const int o = (e / nr) * A.NRS + (e % nr);
+                so[e] = tc_exact(s_num[o], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+            }
+        }
+        unsigned rm = 0;
+        float pv = 0.0f;
+        int pi = 0, pj = 0;
+        if (key_decode(best, &rm, &pv)) {
+            pi = static_cast<int>(rm / nc);
+            pj = static_cast<int>(rm % nc);
+        }
+        if (A.up == 1 || nr < 5 || nc < 5) {
+            if (tid == 0) {
+                const int o = pj * A.NRS + pi;
+                const float v = tc_exact(s_num[o], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+                A.out.dx[k] = __double2float_rn(
+                    __dadd_rn(static_cast<double>(pj - static_cast<int>(prx)), A.pts.dx0[k]));
+                A.out.dy[k] = __double2float_rn(
+                    __dadd_rn(static_cast<double>(pi - static_cast<int>(pry)), A.pts.dy0[k]));
+                A.out.corr[k] = v;
+            }
+        } else {
+            const int pi0 = min(max(pi - 2, 0), max(nr - 5, 0));
+            const int pj0 = min(max(pj - 2, 0), max(nc - 5, 0));
+            if (tid == 0) s_slot = atomicAdd(A.sub_count, 1);
+            __syncthreads();
+            const int slot = s_slot;
+            if (tid < 25) {
+                const int a = tid % 5, b = tid / 5;
+                const int o = (pj0 + b) * A.NRS + (pi0 + a);
+                A.sub_patch[static_cast<int64_t>(slot) * 25 + tid] =
+                    tc_exact(s_num[o], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+            }
+            if (tid == 0) {
+                A.sub_point[slot] = k;
+                A.sub_origin[2 * slot] = pi0;
+                A.sub_origin[2 * slot + 1] = pj0;
+            }
+        }
+    }
+    if (failed) {
+        // Products may still be in flight: give them a bounded time before freeing the
+        // accumulator.
+        tc::mbar_wait(&s_mbar, phase ^ 1u, kTcWaitPolls);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(taddr, A.tmem_cols);
+}
+
+// ----------------------------------------------------------------------------------------------
 // Sub-pixel cascade kernel (src/peak.jl:456-522 from the patch onward).
 //
 // Levels up to (5 * up / 4)^2 are materialised in shared memory. The last two levels -- 90%
@@ -959,6 +1377,58 @@ RefinePlan plan_refine(int up) {
     return R;
 }
 
+struct TcPlan {
+    int NMMA, QM, QS, PS, PC, XS, NRS, NRM, NCM, CHM, CWM, u_min;
+    unsigned off_W, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
+    uint32_t tmem_cols;
+    size_t smem;
+};
+
+// Shared-memory plan of k_corr_tc for a pass's largest geometry; false when the pass does not
+// fit the kernel (surface wider than 64 columns, more than 256 rows, or buffers too large).
+bool plan_corr_tc(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
+    const int ch = static_cast<int>(g.max_ch), cw = static_cast<int>(g.max_cw);
+    const int nr = static_cast<int>(g.max_nr), nc = static_cast<int>(g.max_nc);
+    if (nc > 64 || nr > 256 || nr < 1 || nc < 1 || cw < 2 || ch < 2 || (cw & 1)) return false;
+    P->CHM = ch;
+    P->CWM = cw;
+    P->NRM = nr;
+    P->NCM = nc;
+    P->NMMA = std::max(16, round_up(nr, 16));
+    P->QM = std::max((15 + ch + nr - 1 + 15) / 16, (ch + 15 + 15) / 16 + 1);
+    const int U = P->NMMA + 16 * (P->QM - 1);
+    P->u_min = -16 * (P->QM - 1);
+    P->PS = U * 16;
+    P->XS = 64 + cw;
+    P->QS = P->XS * 16;
+    P->PC = round_up(kPadL + ch + 52, 16);
+    P->NRS = nr | 1;
+    size_t off = static_cast<size_t>(cw) * P->PS;
+    P->off_W = static_cast<unsigned>(off);
+    off += static_cast<size_t>(P->QM) * P->QS;
+    P->off_P = static_cast<unsigned>(off);
+    off += static_cast<size_t>(cw) * P->PC;
+    off = (off + 15) & ~size_t(15);
+    P->off_V = static_cast<unsigned>(off);
+    const size_t vbytes = 2ull * nr * (cw + nc - 1) * 4;
+    const size_t nbytes = static_cast<size_t>(nc) * P->NRS * 4;
+    P->off_num = P->off_V;
+    P->off_est = static_cast<unsigned>(off + ((nbytes + 15) & ~size_t(15)));
+    off += std::max(vbytes, 2 * ((nbytes + 15) & ~size_t(15)));
+    off = (off + 15) & ~size_t(15);
+    P->off_S1 = static_cast<unsigned>(off);
+    off += (nbytes + 15) & ~size_t(15);
+    P->off_S2 = static_cast<unsigned>(off);
+    off += (nbytes + 15) & ~size_t(15);
+    P->off_red = static_cast<unsigned>(off);
+    off += 3 * 32 * 8;
+    P->smem = off;
+    uint32_t cols = 32;
+    while (static_cast<int>(cols) < P->NMMA) cols <<= 1;
+    P->tmem_cols = cols;
+    return off <= smem_cap;
+}
+
 template <typename T>
 cudaError_t launch_corr_t(const CorrArgs& A, const CorrPlan& P, int grid, cudaStream_t stream) {
     cudaError_t e = cudaFuncSetAttribute(k_corr<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -975,6 +1445,11 @@ cudaError_t ensure_scratch(TrackScratch& s, int64_t n) {
     }
     if (!s.sub_count) {
         cudaError_t e = cudaMalloc(&s.sub_count, sizeof(int));
+        if (e != cudaSuccess) return e;
+    }
+    if (!s.status) {
+        cudaError_t e = cudaMalloc(&s.status, sizeof(int));
+        if (e == cudaSuccess) e = cudaMemset(s.status, 0, sizeof(int));
         if (e != cudaSuccess) return e;
     }
     if (s.capacity >= n) return cudaSuccess;
@@ -1033,6 +1508,15 @@ PassGeometry pass_geometry_host(const ar_points& p, int64_t nrows, int64_t ncols
 }
 
 cudaError_t scratch_acquire(TrackScratch& s, cudaStream_t stream);
+
+cudaError_t read_status(TrackScratch& scratch, cudaStream_t stream, int* status) {
+    *status = 0;
+    if (!scratch.status) return cudaSuccess;
+    cudaError_t e = cudaMemcpyAsync(status, scratch.status, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess && *status) e = cudaMemsetAsync(scratch.status, 0, sizeof(int), stream);
+    return e;
+}
 
 cudaError_t pass_geometry_device(const DevPoints& pts, int64_t nrows, int64_t ncols,
                                  TrackScratch& scratch, cudaStream_t stream, PassGeometry* out) {
@@ -1138,10 +1622,63 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         ev2 = T.get();
         cudaEventRecord(ev0, stream);
     }
+    TcPlan TP{};
+    const bool use_tc = dtype == AR_U8 && scratch.tensor_cores &&
+                        plan_corr_tc(geom, 200 * 1024, &TP);
+    if (use_tc) {
+        TcArgs B{};
+        B.ref = static_cast<const uint8_t*>(ref);
+        B.sec = static_cast<const uint8_t*>(sec);
+        B.valid = valid;
+        B.nrows = nrows;
+        B.ncols = ncols;
+        B.pts = pts;
+        B.padx = geom.padx;
+        B.pady = geom.pady;
+        B.up = up;
+        B.measure = measure;
+        B.NMMA = TP.NMMA;
+        B.QM = TP.QM;
+        B.QS = TP.QS;
+        B.PS = TP.PS;
+        B.PC = TP.PC;
+        B.XS = TP.XS;
+        B.NRS = TP.NRS;
+        B.NRM = TP.NRM;
+        B.NCM = TP.NCM;
+        B.CHM = TP.CHM;
+        B.u_min = TP.u_min;
+        B.off_W = TP.off_W;
+        B.off_P = TP.off_P;
+        B.off_V = TP.off_V;
+        B.off_S1 = TP.off_S1;
+        B.off_S2 = TP.off_S2;
+        B.off_num = TP.off_num;
+        B.off_est = TP.off_est;
+        B.off_red = TP.off_red;
+        B.tmem_cols = TP.tmem_cols;
+        B.out = out;
+        B.sub_count = scratch.sub_count;
+        B.sub_point = scratch.sub_point;
+        B.sub_origin = scratch.sub_origin;
+        B.sub_patch = scratch.sub_patch;
+        B.surf_out = surf_out;
+        B.flops = A.flops;
+        B.status = scratch.status;
+        // At least half of an SM's shared memory per CTA: one CTA per SM, so the Tensor Memory
+        // each CTA holds for its lifetime (<= 256 of 512 columns) never waits on another's.
+        const size_t tc_smem = std::max<size_t>(TP.smem, 116 * 1024);
+        e = cudaFuncSetAttribute(k_corr_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(tc_smem));
+        if (e != cudaSuccess) return e;
+        const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(pts.n, num_sms)));
+        k_corr_tc<<<grid, kTcThreads, tc_smem, stream>>>(B);
+        e = cudaGetLastError();
+    }
     const int per_sm = P.smem <= 100 * 1024 ? 2 : 1;
     const int64_t want = static_cast<int64_t>(num_sms) * per_sm * 8;
     const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(pts.n, want)));
-    switch (dtype) {
+    if (!use_tc) switch (dtype) {
         case AR_U8: e = launch_corr_t<uint8_t>(A, P, grid, stream); break;
         case AR_U16: e = launch_corr_t<uint16_t>(A, P, grid, stream); break;
         case AR_I16: e = launch_corr_t<int16_t>(A, P, grid, stream); break;

@@ -213,8 +213,8 @@ def gpu_arm(args):
     outs = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3)]
     ochip = torch.empty(n, dtype=torch.int16, device=dev)
     oint = torch.empty(n, dtype=torch.uint8, device=dev)
-    prm = ar.api.multichip_params(p)
-    opts = ar.track.prepare_options(p)
+    prm = ar.multichip_params(p)
+    opts = ar.prepare_options(p)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
     torch.cuda.synchronize()

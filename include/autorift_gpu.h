@@ -187,6 +187,28 @@ int ar_multichip_device(ar_ctx* ctx, const ar_pair* pair, const ar_points* grid_
                         float* dx_dev, float* dy_dev, float* correlation_dev,
                         uint16_t* chip_size_dev, uint8_t* interpolated_dev, void* stream);
 
+/*
+ * Diagnostic: one tensor-core product (tcgen05.mma kind::i8, unsigned 8-bit operands, 32-bit
+ * integer accumulator) of two operand images placed in shared memory as given, read through
+ * SWIZZLE_NONE K-major descriptors. params = {a_off, a_lbo, a_sbo, a_kstep, b_off, b_lbo,
+ * b_sbo, b_kstep, M, N, nk}: byte offsets and strides (multiples of 16), M in {64, 128}, N, and
+ * nk K-steps of 32 accumulated, step s reading at offset + s * kstep. `d_out` receives the
+ * accumulator as 128 Tensor Memory lanes x N columns (int32, lane-major). Descriptors that
+ * would read outside an image are rejected. It validates on a device the operand layouts the
+ * correlation kernel builds; no reference counterpart.
+ */
+int ar_tc_selftest(ar_ctx* ctx, const uint8_t* a_img, int a_bytes, const uint8_t* b_img,
+                   int b_bytes, const int* params, int32_t* d_out);
+
+/*
+ * Context options. AR_OPT_TENSOR_CORES (default 1): UInt8 passes whose geometry fits (surface
+ * at most 64 columns and 256 rows) compute the correlation numerator on the tensor cores
+ * (exact 8-bit products, bit-identical results); 0 keeps every pass on the CUDA-core kernel.
+ * No reference counterpart.
+ */
+enum { AR_OPT_TENSOR_CORES = 1 };
+int ar_ctx_set_option(ar_ctx* ctx, int option, int value);
+
 /* The context's own CUDA stream (cudaStream_t), on which calls without a stream argument run;
  * for callers that order their own work or timing events after the library's. */
 int ar_ctx_stream(ar_ctx* ctx, void** stream);
