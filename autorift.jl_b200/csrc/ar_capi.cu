@@ -821,26 +821,29 @@ int ar_tc_selftest(ar_ctx* c, const uint8_t* a_img, int a_bytes, const uint8_t* 
     if (!c || !a_img || !b_img || !params || !d_out) return fail(c, AR_ERR_ARG, "null argument");
     if (a_bytes <= 0 || b_bytes <= 0 || a_bytes > 96 * 1024 || b_bytes > 96 * 1024)
         return fail(c, AR_ERR_SIZE, "operand images must be 1..96 KiB");
-    const int N = params[9];
-    if (N < 8 || N > 256) return fail(c, AR_ERR_ARG, "invalid N");
+    const int N = params[9], nk = params[10], dstep = params[11];
+    if (N < 8 || N > 256 || nk < 1 || nk > 64 || dstep < 0 || dstep > 512)
+        return fail(c, AR_ERR_ARG, "invalid N, nk or dstep");
+    const int dcols = N + (nk - 1) * dstep;
+    if (dcols > 512) return fail(c, AR_ERR_ARG, "the accumulator columns exceed Tensor Memory");
     std::lock_guard<std::mutex> lk(c->mu);
     DeviceGuard g(c->device);
     unsigned char *da = nullptr, *db = nullptr, *dd = nullptr;
-    const size_t dbytes = static_cast<size_t>(128) * N * 4 + 16;
+    const size_t dbytes = static_cast<size_t>(128) * dcols * 4 + 16;
     cudaError_t e = dalloc(c, &da, a_bytes);
     if (e == cudaSuccess) e = dalloc(c, &db, b_bytes);
     if (e == cudaSuccess) e = dalloc(c, &dd, dbytes);
     if (e == cudaSuccess) e = cudaMemcpyAsync(da, a_img, a_bytes, cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(db, b_img, b_bytes, cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(dd, 0, dbytes, c->stream);
-    int* status = reinterpret_cast<int*>(dd + static_cast<size_t>(128) * N * 4);
+    int* status = reinterpret_cast<int*>(dd + static_cast<size_t>(128) * dcols * 4);
     std::string err;
     if (e == cudaSuccess)
         e = ar::tc_probe(da, a_bytes, db, b_bytes, params, reinterpret_cast<int32_t*>(dd), status,
                          c->stream, &err);
     int hstatus = 0;
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(d_out, dd, static_cast<size_t>(128) * N * 4, cudaMemcpyDeviceToHost, c->stream);
+        e = cudaMemcpyAsync(d_out, dd, static_cast<size_t>(128) * dcols * 4, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);

@@ -19,8 +19,8 @@ struct ProbeArgs {
     int b_base;
     int a_off, a_lbo, a_sbo, a_kstep;
     int b_off, b_lbo, b_sbo, b_kstep;
-    int M, N, nk, ncols;
-    int32_t* d_out;            // 128 lanes x N columns
+    int M, N, nk, ncols, dstep, dcols;
+    int32_t* d_out;            // 128 lanes x dcols columns
     int* status;               // 0 ok, 1 the MMA did not complete in time
 };
 
@@ -44,13 +44,26 @@ __global__ void __launch_bounds__(128, 1) k_tc_probe(const ProbeArgs P) {
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t taddr = tbase;
+    if (P.dstep > 0) {
+        // Steps write overlapping column windows: clear the accumulator and always add.
+        uint32_t z[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) z[k] = 0u;
+        for (int c = 0; c < P.dcols; c += 16)
+            tc::tmem_st16(taddr + (static_cast<uint32_t>(32 * warp) << 16) + c, z);
+        tc::tmem_wait_st();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
     if (tid == 0) {
         const uint32_t sa = tc::smem_u32(smem), sb = tc::smem_u32(smem + P.b_base);
         const uint32_t idesc = tc::idesc_u8_s32(P.M, P.N);
         for (int s = 0; s < P.nk; ++s) {
             const uint64_t da = tc::smem_desc(sa + P.a_off + s * P.a_kstep, P.a_lbo, P.a_sbo);
             const uint64_t db = tc::smem_desc(sb + P.b_off + s * P.b_kstep, P.b_lbo, P.b_sbo);
-            tc::mma_u8(taddr, da, db, idesc, s > 0);
+            tc::mma_u8(taddr + static_cast<uint32_t>(s * P.dstep), da, db, idesc,
+                       P.dstep > 0 || s > 0);
         }
         tc::mma_commit(&mbar);
     }
@@ -58,13 +71,13 @@ __global__ void __launch_bounds__(128, 1) k_tc_probe(const ProbeArgs P) {
     if (!ok && tid == 0) *P.status = 1;
     tc::fence_after_sync();
     if (ok) {
-        for (int c = 0; c < P.N; c += 16) {
+        for (int c = 0; c < P.dcols; c += 16) {
             uint32_t r[16];
             tc::tmem_ld16(taddr + (static_cast<uint32_t>(32 * warp) << 16) + c, r);
             tc::tmem_wait_ld();
 #pragma unroll
             for (int k = 0; k < 16; ++k)
-                P.d_out[(32 * warp + lane) * P.N + c + k] = static_cast<int32_t>(r[k]);
+                P.d_out[(32 * warp + lane) * P.dcols + c + k] = static_cast<int32_t>(r[k]);
         }
     }
     tc::fence_before_sync();
@@ -101,6 +114,7 @@ cudaError_t tc_probe(const uint8_t* a_img, int a_bytes, const uint8_t* b_img, in
     P.M = params[8];
     P.N = params[9];
     P.nk = params[10];
+    P.dstep = params[11];
     auto bad = [&](const char* m) {
         if (err) *err = m;
         return cudaErrorInvalidValue;
@@ -116,9 +130,12 @@ cudaError_t tc_probe(const uint8_t* a_img, int a_bytes, const uint8_t* b_img, in
         return bad("A descriptor reads past its image");
     if (operand_extent(P.b_off, P.b_lbo, P.b_sbo, P.b_kstep, P.N, P.nk) > b_bytes)
         return bad("B descriptor reads past its image");
+    if (P.dstep < 0 || (P.dstep & 15)) return bad("dstep must be a non-negative multiple of 16");
+    P.dcols = P.N + (P.nk - 1) * P.dstep;
+    if (P.dcols > 512) return bad("the accumulator columns exceed Tensor Memory");
     P.b_base = (a_bytes + 1023) & ~1023;
     int ncols = 32;
-    while (ncols < P.N) ncols <<= 1;
+    while (ncols < P.dcols) ncols <<= 1;
     P.ncols = ncols;
     P.d_out = d_out;
     P.status = status;

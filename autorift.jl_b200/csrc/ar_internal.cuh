@@ -152,7 +152,7 @@ struct MultichipJob {
 size_t multichip_arena_bytes(int64_t gr, int64_t gc);
 
 // One tensor-core product of two shared-memory operand images (the layout self-test):
-// params = {a_off, a_lbo, a_sbo, a_kstep, b_off, b_lbo, b_sbo, b_kstep, M, N, nk}.
+// params = {a_off, a_lbo, a_sbo, a_kstep, b_off, b_lbo, b_sbo, b_kstep, M, N, nk, dstep}.
 cudaError_t tc_probe(const uint8_t* a_img, int a_bytes, const uint8_t* b_img, int b_bytes,
                      const int* params, int32_t* d_out, int* status, cudaStream_t s,
                      std::string* err);

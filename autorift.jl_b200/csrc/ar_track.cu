@@ -515,27 +515,26 @@ __global__ void __launch_bounds__(kCorrThreads, 2) k_corr(const CorrArgs A) {
 // Tensor-core correlation for UInt8 imagery (tcgen05.mma kind::i8, exact 32-bit accumulation).
 //
 // The numerator S[i, j] = sum_{a,b} C[a, b] W[i + a, j + b] (C the chip, W the window, i the
-// surface row, j the surface column) is one product D[j, i] = sum_k A[j, k] B[i, k] over
+// surface row, j the surface column) is a sum of products D[j, i] += sum_k A[j, k] B[i, k] over
 // K = (16-row block q of the window, chip column b, row r within the block):
-//   A[j, (q, b, r)] = W'[16 q + r, j + b]          the window as 16-byte blocks s_W[q][x][r];
-//                                                  row j of A starts 16 bytes after row j - 1,
-//                                                  so A is read in place;
-//   B[i, (q, b, r)] = C[16 q + r - delta - i, b]    the chip as 16-byte rows per column b,
-//                                                  E_b[u][r] = C[r - u - delta, b] with
-//                                                  u = i - 16 q, built once per point.
+//   A[j, (q, b, r)] = W'[16 q + r, j + b]     the window as 16-byte blocks s_W[q][x][r]; row j
+//                                             of A starts 16 bytes after row j - 1, so A is
+//                                             read in place;
+//   B[i, (q, b, r)] = E_b[i - 16 q][r]        with E_b[u][r] = C[r - u - delta, b], the chip as
+//                                             16-byte rows per column b, built once per point.
 // W' starts at the 16-aligned image row `delta` rows above the window's first row, so each
-// 16-byte block of a column-major image with 16-aligned columns is one aligned load. One MMA
-// (M = 64 surface columns, N surface rows rounded to 16, K = 32: two chip columns) per
-// (q, column pair), accumulated in Tensor Memory. The products are exact (u8 x u8 summed below
-// 2^31), so the numerator equals the CUDA-core kernel's and every surface value, the peak and
-// the patch are bit-identical to it.
+// 16-byte block of a column-major image with 16-aligned columns is one aligned load. The chip
+// rows a block q can meet are surface rows i in [16 q + 16 - NB, 16 q + 16), i.e. the same
+// NB = 16 * ceil((ch + 30) / 16) rows u = i - 16 q of E for every q: each block's product
+// (M = 64 surface columns, N = NB, K = 32: two chip columns) adds into accumulator columns
+// [16 q, 16 q + NB), surface row i living in column i + NB - 16 of a cleared accumulator. The
+// products are exact (u8 x u8 summed below 2^31), so the numerator equals the CUDA-core
+// kernel's and every surface value, the peak and the patch are bit-identical to it.
 //
 // Normalising all 2ry x 2rx values in FP64 would cost as much as the products, and only the
-// peak and its 5 x 5 patch are read. So every value is first estimated in FP32 from exact
-// integers (numerator nn*D - sum(C)*s1 and variance nn*s2 - s1^2 as 64-bit integers): the
-// estimate is within 10 * 2^-24 relative of the FP32 surface value. Values whose estimate
-// cannot reach the largest one are not evaluated; the others, the patch and any value whose
-// variance is too small for the bound get the exact FP64 normalisation of the reference.
+// peak and its 5 x 5 patch are read. So each value is first estimated in FP32 together with a
+// rigorous bound on its distance from the FP32 surface value; only values whose bound reaches
+// the largest estimate, and the patch, get the reference's exact FP64 normalisation.
 
 constexpr int kTcThreads = 256;
 constexpr int kPadL = 32;            // zero bytes before each staged chip column
@@ -549,9 +548,8 @@ struct TcArgs {
     DevPoints pts;
     int64_t padx, pady;
     int up, measure;
-    int NMMA, QM, QS, PS, PC, XS, NRS, NRM, NCM, CHM;
-    int u_min;                       // lowest stored row of the E planes
-    unsigned off_W, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
+    int NB, QM, QS, PS, PC, XS, XT, NRS, NRM, NCM, CHM, CWM;
+    unsigned off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
     uint32_t tmem_cols;
     DevOutputs out;
     int* sub_count;
@@ -580,30 +578,60 @@ __device__ __forceinline__ float tc_exact(uint32_t D, uint32_t S1, uint32_t S2, 
     return den > 0.0 ? __double2float_rn(__ddiv_rn(num, den)) : 0.0f;
 }
 
-// FP32 estimate of the same value; NaN when the variance is too small for the error bound.
-__device__ __forceinline__ float tc_estimate(uint32_t D, uint32_t S1, uint32_t S2, long long nn,
-                                             long long csum, float k, int measure) {
-    const long long nx = nn * static_cast<long long>(D) - csum * static_cast<long long>(S1);
-    const long long sq = nn * static_cast<long long>(S2);
-    const long long vx = measure == AR_NCC ? static_cast<long long>(S2)
-                                           : sq - static_cast<long long>(S1) * S1;
-    if (measure != AR_NCC && vx < (sq >> 20)) return __int_as_float(0x7fc00000);
-    if (vx <= 0 || nx == 0) return 0.0f;
-    return __fmul_rn(__fmul_rn(static_cast<float>(nx), rsqrtf(static_cast<float>(vx))), k);
+// Exact FP32 value of an unsigned integer below 2^32 rounded once: the two 16-bit halves are
+// exact floats, their sum one rounding.
+__device__ __forceinline__ float u32_to_f(uint32_t v) {
+    const float hi = __int_as_float(0x4B000000 | (v >> 16)) - 8388608.0f;
+    const float lo = __int_as_float(0x4B000000 | (v & 0xFFFFu)) - 8388608.0f;
+    return __fmaf_rn(hi, 65536.0f, lo);
 }
 
-__device__ __forceinline__ float tc_tol(float v) {
-    return fabsf(v) * 7.152557373046875e-07f + 1e-30f;  // 12 * 2^-24 relative
+// FP32 estimate of one surface value and a bound on its distance from the value tc_exact
+// returns. With nn, C = sum(chip), s1, s2, D exact integers, the value is
+//   ZNCC: (nn D - C s1) / (cnorm sqrt(nn) sqrt(nn s2 - s1^2)),  NCC: (nn D - C s1) / (cnorm nn sqrt(s2)).
+// The numerator and the variance are each formed with three roundings of relative size
+// u = 2^-24 on terms no larger than `tn` and `tv`, so their absolute errors are below
+// 3u tn and 3u tv; rsqrt (2 ulp), the scale and two products add < 6u relative, and the final
+// Float32 rounding of the reference 1u. The bound returned covers all of it with slack; NaN
+// marks a value whose variance is too small for the bound (evaluated exactly).
+__device__ __forceinline__ float tc_estimate(uint32_t D, uint32_t S1, uint32_t S2, float nnf,
+                                             float csum, float k, int measure, float* bound) {
+    const float d = u32_to_f(D), s1 = u32_to_f(S1), s2 = u32_to_f(S2);
+    const float p = __fmul_rn(csum, s1);
+    const float nx = __fmaf_rn(nnf, d, -p);
+    const float tn = __fmaf_rn(nnf, d, p);  // |nn D| + |C s1| (both non-negative)
+    float vx, tv;
+    if (measure == AR_NCC) {
+        vx = s2;
+        tv = s2;
+    } else {
+        const float q = __fmul_rn(s1, s1);
+        vx = __fmaf_rn(nnf, s2, -q);
+        tv = __fmaf_rn(nnf, s2, q);
+    }
+    const float ev = 3.5762786865234375e-07f * tv;  // 6u tv
+    if (!(vx > 64.0f * ev)) {
+        *bound = 0.0f;
+        return __int_as_float(0x7fc00000);
+    }
+    const float r = rsqrtf(vx);
+    const float est = __fmul_rn(__fmul_rn(nx, r), k);
+    // |err| <= |est| (8u + ev / vx) + 3.5u tn r k  (u = 2^-24), doubled for slack.
+    const float rel = __fmaf_rn(ev, __frcp_rn(vx), 9.5367431640625e-07f);  // 16u + ev/vx
+    *bound = __fmaf_rn(fabsf(est), 2.0f * rel, 4.172325134277344e-07f * tn * r * k) + 1e-30f;
+    return est;
 }
 
-__global__ void __launch_bounds__(kTcThreads, 1) k_corr_tc(const TcArgs A) {
+__global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
     extern __shared__ __align__(1024) unsigned char smem_tc[];
     __shared__ uint64_t s_mbar;
     __shared__ uint32_t s_taddr;
     __shared__ int s_slot;
     __shared__ float s_fmax[kTcThreads / 32];
+    __shared__ unsigned long long s_isum[2][2];
     uint8_t* s_E = smem_tc;
     uint8_t* s_W = smem_tc + A.off_W;
+    uint8_t* s_T = smem_tc + A.off_T;
     uint8_t* s_P = smem_tc + A.off_P;
     uint32_t* s_V1 = reinterpret_cast<uint32_t*>(smem_tc + A.off_V);
     uint32_t* s_S1 = reinterpret_cast<uint32_t*>(smem_tc + A.off_S1);
@@ -613,14 +641,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_corr_tc(const TcArgs A) {
     double* s_red = reinterpret_cast<double*>(smem_tc + A.off_red);
 
     const int tid = threadIdx.x, bd = blockDim.x;
-    const int lane = tid & 31, warp = tid >> 5;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = bd >> 5;
     const int64_t NR = A.nrows + 2 * A.pady, NC = A.ncols + 2 * A.padx;
     const double shx = static_cast<double>(A.padx) + 0.5;
     const double shy = static_cast<double>(A.pady) + 0.5;
 
-    // E rows outside each point's band stay zero for the whole launch.
-    for (int e = tid * 16; e < static_cast<int>(A.off_W); e += bd * 16)
-        *reinterpret_cast<uint4*>(s_E + e) = make_uint4(0, 0, 0, 0);
     if (warp == 0) {
         tc::tmem_alloc(&s_taddr, A.tmem_cols);
         tc::tmem_relinquish();
@@ -635,11 +660,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_corr_tc(const TcArgs A) {
     const uint32_t taddr = s_taddr;
     uint32_t phase = 0;
     bool failed = false;
+    if (tid < 4) s_isum[tid >> 1][tid & 1] = 0ull;
+    int iter = 0;
 
-    for (int64_t k = blockIdx.x; k < A.pts.n; k += gridDim.x) {
+    for (int64_t k = blockIdx.x; k < A.pts.n; k += gridDim.x, ++iter) {
         tc::fence_before_sync();
         __syncthreads();  // the previous point's buffers and accumulator are no longer read
         tc::fence_after_sync();
+        // The chip sums of this iteration go to s_isum[ib]; the other buffer, last read
+        // before the barrier above, is cleared for the next iteration.
+        const int ib = iter & 1;
+        if (tid < 2) s_isum[ib ^ 1][tid] = 0ull;
         const int64_t prx = A.pts.rx[k], pry = A.pts.ry[k];
         if (!(prx > 0 && pry > 0)) continue;
         const double xs = A.pts.x[k] + shx, ys = A.pts.y[k] + shy;
@@ -658,82 +689,123 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_corr_tc(const TcArgs A) {
         const int ch = static_cast<int>(2 * hy), cw = static_cast<int>(2 * hx);
         const int nr = static_cast<int>(2 * pry), nc = static_cast<int>(2 * prx);
         if (ch <= 0 || cw <= 0) continue;
-        if (ch > A.CHM || nr > A.NRM || nc > A.NCM || nc > 64) continue;  // not sized for
+        if (ch > A.CHM || cw > A.CWM || nr > A.NRM || nc > A.NCM || nc > 64) continue;
         const int64_t chip_r = cr0 - 1 - A.pady, chip_c = cc0 - 1 - A.padx;
         const int64_t win_r = wr0 - 1 - A.pady, win_c = wc0 - 1 - A.padx;
+        const long long nnl = static_cast<long long>(ch) * cw;
+        // Power-of-two areas up to 4096: every term of the reference's FP64 chip sums is exact.
+        const bool pow2 = (nnl & (nnl - 1)) == 0 && nnl <= 4096;
 
-        // _any_valid over the chip (src/track.jl:416-421).
+        // The chip as zero-padded byte columns, _any_valid over it (src/track.jl:416-421) and,
+        // for power-of-two areas, its exact integer sums; a warp per chip column.
         int any = 0;
-        for (int e = tid; e < ch * cw; e += bd) {
-            const int64_t r = chip_r + e % ch, c = chip_c + e / ch;
-            if (r >= 0 && r < A.nrows && c >= 0 && c < A.ncols && A.valid[r + c * A.nrows])
-                any = 1;
+        unsigned long long isum = 0ull, isq = 0ull;
+        for (int b = warp; b < cw; b += nwarps) {
+            const int64_t c = chip_c + b;
+            const bool cin = c >= 0 && c < A.ncols;
+            for (int o = lane; o < A.PC; o += 32) {
+                const int a = o - kPadL;
+                uint32_t v = 0;
+                if (a >= 0 && a < ch) {
+                    const int64_t r = chip_r + a;
+                    if (cin && r >= 0 && r < A.nrows) {
+                        v = A.sec[r + c * A.nrows];
+                        any |= A.valid[r + c * A.nrows];
+                    }
+                    isum += v;
+                    isq += v * v;
+                }
+                s_P[b * A.PC + o] = static_cast<uint8_t>(v);
+            }
+        }
+        if (pow2) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                isum += __shfl_xor_sync(kFull, isum, o);
+                isq += __shfl_xor_sync(kFull, isq, o);
+            }
+            if (lane == 0) {
+                atomicAdd(&s_isum[ib][0], isum);
+                atomicAdd(&s_isum[ib][1], isq);
+            }
         }
         if (!__syncthreads_or(any)) continue;
         if (tid == 0) A.out.searched[k] = 1;
 
-        // prepare_chip! statistics in the CUDA-core kernel's order (bit-identical sums), and
-        // the chip staged as zero-padded byte columns.
-        double st[1] = {0.0};
-        for (int e = tid; e < ch * cw; e += bd)
-            st[0] = __dadd_rn(st[0], pixel(A.sec, A.nrows, A.ncols, chip_r + e % ch, chip_c + e / ch));
-        block_sum_f64<1>(st, s_red);
-        const double nn = static_cast<double>(ch * cw);
-        const double mean = __ddiv_rn(st[0], nn);
-        const int chp = (ch + kUA - 1) & ~(kUA - 1);
-        double acc2[1] = {0.0};
-        for (int e = tid; e < chp * cw; e += bd) {
-            const int a = e % chp, b = e / chp;
-            if (a < ch) {
-                const double v = pixel(A.sec, A.nrows, A.ncols, chip_r + a, chip_c + b);
-                const double d = __dsub_rn(v, mean);
-                acc2[0] = __dadd_rn(acc2[0], __dmul_rn(d, d));
-                s_P[b * A.PC + kPadL + a] = static_cast<uint8_t>(v);
+        // prepare_chip! statistics. Power-of-two areas: every term of the reference's FP64
+        // sums is exact, so mean = sum/nn and sq = (nn sum(C^2) - sum(C)^2)/nn exactly;
+        // otherwise the CUDA-core kernel's FP64 loops, in its order (bit-identical sums).
+        double mean, sq, csum_d;
+        if (pow2) {
+            const long long cs = static_cast<long long>(s_isum[ib][0]);
+            const long long c2 = static_cast<long long>(s_isum[ib][1]);
+            csum_d = static_cast<double>(cs);
+            mean = __ddiv_rn(csum_d, static_cast<double>(nnl));
+            sq = __ddiv_rn(static_cast<double>(nnl * c2 - cs * cs), static_cast<double>(nnl));
+        } else {
+            double st[1] = {0.0};
+            for (int e = tid; e < ch * cw; e += bd)
+                st[0] = __dadd_rn(st[0], pixel(A.sec, A.nrows, A.ncols, chip_r + e % ch, chip_c + e / ch));
+            block_sum_f64<1>(st, s_red);
+            csum_d = st[0];
+            mean = __ddiv_rn(st[0], static_cast<double>(nnl));
+            const int chp = (ch + kUA - 1) & ~(kUA - 1);
+            double acc2[1] = {0.0};
+            for (int e = tid; e < chp * cw; e += bd) {
+                const int a = e % chp, b = e / chp;
+                if (a < ch) {
+                    const double v = pixel(A.sec, A.nrows, A.ncols, chip_r + a, chip_c + b);
+                    const double d = __dsub_rn(v, mean);
+                    acc2[0] = __dadd_rn(acc2[0], __dmul_rn(d, d));
+                }
             }
+            block_sum_f64<1>(acc2, s_red);
+            sq = acc2[0];
         }
-        for (int e = tid; e < cw * A.PC; e += bd) {
-            const int b = e / A.PC, o = e % A.PC;
-            if (o < kPadL || o >= kPadL + ch) s_P[b * A.PC + o] = 0;
-        }
-        block_sum_f64<1>(acc2, s_red);
-        const double sq = acc2[0];
         if (!(sq > __dmul_rn(__dmul_rn(DBL_EPSILON, static_cast<double>(ch)), static_cast<double>(cw))))
             continue;  // degenerate chip: searched, no measurement (src/track.jl:286)
         const double cnorm = __dsqrt_rn(sq);
-        const long long csum = static_cast<long long>(st[0]);
-        const long long nnl = static_cast<long long>(ch) * cw;
+        const double nn = static_cast<double>(nnl);
 
-        // Window blocks W'[16 q + r][x], x in [0, XS): 16 image rows from base_r per block.
+        // Window blocks W'[16 q + r][x] (x < XS) from 16 image rows at base_r + 16 q, and the
+        // same window transposed, s_T[row][x], for the box sums.
         const int64_t delta = ((win_r % 16) + 16) % 16;
         const int64_t base_r = win_r - delta;
         const int Q = static_cast<int>((delta + ch + nr - 1 + 15) / 16);
-        for (int e = tid; e < Q * A.XS; e += bd) {
-            const int q = e / A.XS, x = e % A.XS;
-            const int64_t r0 = base_r + 16 * q, c = win_c + x;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (c >= 0 && c < A.ncols) {
-                const uint8_t* col = A.ref + c * A.nrows;
-                if (r0 >= 0 && r0 + 16 <= A.nrows &&
-                    (reinterpret_cast<uintptr_t>(col + r0) & 15) == 0) {
-                    v = __ldg(reinterpret_cast<const uint4*>(col + r0));
-                } else {
-                    uint32_t w[4] = {0, 0, 0, 0};
+        const int XW = cw + nc - 1;
+        for (int q = warp; q < Q; q += nwarps) {
+            for (int x = lane; x < A.XS; x += 32) {
+                const int64_t r0 = base_r + 16 * q, c = win_c + x;
+                uint4 v = make_uint4(0, 0, 0, 0);
+                if (c >= 0 && c < A.ncols) {
+                    const uint8_t* col = A.ref + c * A.nrows;
+                    if (r0 >= 0 && r0 + 16 <= A.nrows &&
+                        (reinterpret_cast<uintptr_t>(col + r0) & 15) == 0) {
+                        v = __ldg(reinterpret_cast<const uint4*>(col + r0));
+                    } else {
+                        uint32_t w[4] = {0, 0, 0, 0};
 #pragma unroll
-                    for (int t = 0; t < 16; ++t) {
-                        const int64_t r = r0 + t;
-                        const uint32_t b = (r >= 0 && r < A.nrows) ? col[r] : 0u;
-                        w[t >> 2] |= b << (8 * (t & 3));
+                        for (int t = 0; t < 16; ++t) {
+                            const int64_t r = r0 + t;
+                            const uint32_t bb = (r >= 0 && r < A.nrows) ? col[r] : 0u;
+                            w[t >> 2] |= bb << (8 * (t & 3));
+                        }
+                        v = make_uint4(w[0], w[1], w[2], w[3]);
                     }
-                    v = make_uint4(w[0], w[1], w[2], w[3]);
+                }
+                *reinterpret_cast<uint4*>(s_W + q * A.QS + x * 16) = v;
+                if (x < XW) {
+                    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                    for (int t = 0; t < 16; ++t)
+                        s_T[(16 * q + t) * A.XT + x] = static_cast<uint8_t>(w[t >> 2] >> (8 * (t & 3)));
                 }
             }
-            *reinterpret_cast<uint4*>(s_W + q * A.QS + x * 16) = v;
         }
         __syncthreads();  // s_P complete
-        // The band of E rows a chip of height <= CHM can reach for any delta.
-        const int u_lo = -(A.CHM + 15), nband = A.CHM + 31;
-        for (int e = tid; e < cw * nband; e += bd) {
-            const int b = e / nband, u = u_lo + e % nband;
+        // E: NB rows u = 16 - NB ... 15 per chip column, row u at (u - 16 + NB) * 16.
+        for (int e = tid; e < cw * A.NB; e += bd) {
+            const int b = e / A.NB, u = 16 - A.NB + e % A.NB;
             const int src = b * A.PC + kPadL - u - static_cast<int>(delta);
             const uint32_t* w = reinterpret_cast<const uint32_t*>(s_P + (src & ~3));
             const uint32_t sh = static_cast<uint32_t>(src & 3) * 8u;
@@ -742,23 +814,31 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_corr_tc(const TcArgs A) {
             o.y = __funnelshift_r(w[1], w[2], sh);
             o.z = __funnelshift_r(w[2], w[3], sh);
             o.w = __funnelshift_r(w[3], w[4], sh);
-            *reinterpret_cast<uint4*>(s_E + b * A.PS + (u - A.u_min) * 16) = o;
+            *reinterpret_cast<uint4*>(s_E + b * A.PS + (e % A.NB) * 16) = o;
+        }
+        // Clear the accumulator columns the products add into (warps 0-3: one lane quarter each).
+        const int dcols = 16 * (Q - 1) + A.NB;
+        if (warp < 4) {
+            uint32_t z[16];
+#pragma unroll
+            for (int t = 0; t < 16; ++t) z[t] = 0u;
+            for (int c = 0; c < dcols; c += 16)
+                tc::tmem_st16(taddr + (static_cast<uint32_t>(32 * warp) << 16) + static_cast<uint32_t>(c), z);
+            tc::tmem_wait_st();
         }
         tc::fence_proxy_async_smem();
+        tc::fence_before_sync();
         __syncthreads();
 
         if (tid == 0) {
             tc::fence_after_sync();
             const uint32_t sW = tc::smem_u32(s_W), sE = tc::smem_u32(s_E);
-            const uint32_t idesc = tc::idesc_u8_s32(64, A.NMMA);
-            bool acc = false;
+            const uint32_t idesc = tc::idesc_u8_s32(64, A.NB);
             for (int q = 0; q < Q; ++q)
                 for (int t = 0; t < cw / 2; ++t) {
                     const uint64_t da = tc::smem_desc(sW + q * A.QS + 32 * t, 16, 128);
-                    const uint64_t db = tc::smem_desc(
-                        sE + 2 * t * A.PS + (-16 * q - A.u_min) * 16, A.PS, 128);
-                    tc::mma_u8(taddr, da, db, idesc, acc);
-                    acc = true;
+                    const uint64_t db = tc::smem_desc(sE + 2 * t * A.PS, A.PS, 128);
+                    tc::mma_u8(taddr + static_cast<uint32_t>(16 * q), da, db, idesc, true);
                 }
             tc::mma_commit(&s_mbar);
         }
@@ -766,19 +846,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_corr_tc(const TcArgs A) {
         // While the tensor core runs: box sums of W and W^2 (integral_both!, boxsum,
         // src/integral.jl:141-170, 244-247) as exact integers. V[i][x] sums ch rows down
         // column x; S[j][i] sums cw columns of V.
-        const int XW = cw + nc - 1;
         uint32_t* s_V2 = s_V1 + A.NRM * XW;
         const int nseg = (nr + 15) >> 4;
         for (int task = tid; task < XW * nseg; task += bd) {
             const int x = task % XW, seg = task / XW;
             const int i0 = seg << 4, i1 = min(i0 + 16, nr);
-            auto wat = [&](int rr) -> uint32_t {
-                const int rp = rr + static_cast<int>(delta);
-                return s_W[(rp >> 4) * A.QS + x * 16 + (rp & 15)];
-            };
+            const uint8_t* col = s_T + static_cast<int>(delta) * A.XT + x;
             uint32_t h1 = 0, h2 = 0;
             for (int a = 0; a < ch; ++a) {
-                const uint32_t w = wat(i0 + a);
+                const uint32_t w = col[(i0 + a) * A.XT];
                 h1 += w;
                 h2 += w * w;
             }
@@ -786,7 +862,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_corr_tc(const TcArgs A) {
                 s_V1[i * XW + x] = h1;
                 s_V2[i * XW + x] = h2;
                 if (i + 1 < i1) {
-                    const uint32_t wn = wat(i + ch), wo = wat(i);
+                    const uint32_t wn = col[(i + ch) * A.XT], wo = col[i * A.XT];
                     h1 = h1 + wn - wo;
                     h2 = h2 + wn * wn - wo * wo;
                 }
@@ -822,22 +898,26 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_corr_tc(const TcArgs A) {
         }
         tc::fence_after_sync();
 
-        // Pass 1: numerators out of Tensor Memory, estimates, their maximum. Rows j of the
-        // M = 64 accumulator live in lanes (j % 16) + 32 (j / 16); warp w reads its quarter's
+        // Pass 1: numerators out of Tensor Memory, estimates and bounds, the largest estimate.
+        // Surface column j is accumulator row j (lane (j % 16) + 32 (j / 16) of the M = 64
+        // layout); surface row i is accumulator column i + NB - 16. Warp w reads its quarter's
         // first 16 lanes, columns from 32 (w / 4) in steps of 64.
         const float kk = __double2float_rn(
             A.measure == AR_NCC ? __drcp_rn(__dmul_rn(cnorm, nn))
                                 : __drcp_rn(__dmul_rn(cnorm, __dsqrt_rn(nn))));
+        const float nnf = static_cast<float>(nnl);
+        const float csf = static_cast<float>(csum_d);
         const int quarter = warp & 3, half = warp >> 2;
         const int j = 16 * quarter + (lane & 15);
         const bool jv = lane < 16 && j < nc;
+        const uint32_t col0 = static_cast<uint32_t>(A.NB - 16);
         float lmax = -INFINITY;
         for (int i0 = 32 * half; i0 < nr; i0 += 64) {
             for (int c = 0; c < 32; c += 16) {
                 const int ii = i0 + c;
                 if (ii >= nr) break;  // warp-uniform
                 uint32_t r[16];
-                tc::tmem_ld16(taddr + (static_cast<uint32_t>(32 * quarter) << 16) +
+                tc::tmem_ld16(taddr + (static_cast<uint32_t>(32 * quarter) << 16) + col0 +
                                   static_cast<uint32_t>(ii), r);
                 tc::tmem_wait_ld();
 #pragma unroll
@@ -845,10 +925,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_corr_tc(const TcArgs A) {
                     const int i = ii + m;
                     if (jv && i < nr) {
                         const int o = j * A.NRS + i;
-                        const float est = tc_estimate(r[m], s_S1[o], s_S2[o], nnl, csum, kk, A.measure);
+                        float bnd;
+                        const float est = tc_estimate(r[m], s_S1[o], s_S2[o], nnf, csf, kk,
+                                                      A.measure, &bnd);
                         s_num[o] = r[m];
                         s_est[o] = est;
-                        lmax = fmaxf(lmax, est);
+                        s_est[o + A.NCM * A.NRS] = bnd;
+                        lmax = fmaxf(lmax, est - bnd);
                     }
                 }
             }
@@ -859,18 +942,20 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_corr_tc(const TcArgs A) {
         __syncthreads();
         float M = s_fmax[0];
         for (int w = 1; w < kTcThreads / 32; ++w) M = fmaxf(M, s_fmax[w]);
-        const float floor_v = M - tc_tol(M);
+        // M: the largest lower bound of any value. A value whose upper bound is below it is
+        // strictly below some other value: it cannot be the (first) maximum.
 
-        // Pass 2: exact values where the estimate can reach the maximum; the peak key.
+        // Pass 2: exact values where the upper bound reaches M; the peak key.
         unsigned long long best = 0ull;
-        for (int e = tid; e < nr * nc; e += bd) {
-            const int i = e % nr, jj = e / nr;
-            const int o = jj * A.NRS + i;
-            const float est = s_est[o];
-            if (!(est + tc_tol(est) >= floor_v) && !isnan(est)) continue;
-            const float v = tc_exact(s_num[o], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
-            const unsigned long long kk2 = argmax_key(v, static_cast<unsigned>(i * nc + jj));
-            best = kk2 > best ? kk2 : best;
+        for (int jj = warp; jj < nc; jj += nwarps) {
+            for (int i = lane; i < nr; i += 32) {
+                const int o = jj * A.NRS + i;
+                const float est = s_est[o], bnd = s_est[o + A.NCM * A.NRS];
+                if (!(est + bnd >= M) && !isnan(est)) continue;
+                const float v = tc_exact(s_num[o], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+                const unsigned long long key = argmax_key(v, static_cast<unsigned>(i * nc + jj));
+                best = key > best ? key : best;
+            }
         }
         best = block_max_u64(best, reinterpret_cast<unsigned long long*>(s_red));
         if (A.flops && tid == 0)
@@ -1378,8 +1463,8 @@ RefinePlan plan_refine(int up) {
 }
 
 struct TcPlan {
-    int NMMA, QM, QS, PS, PC, XS, NRS, NRM, NCM, CHM, CWM, u_min;
-    unsigned off_W, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
+    int NB, QM, QS, PS, PC, XS, XT, NRS, NRM, NCM, CHM, CWM;
+    unsigned off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
     uint32_t tmem_cols;
     size_t smem;
 };
@@ -1394,37 +1479,42 @@ bool plan_corr_tc(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
     P->CWM = cw;
     P->NRM = nr;
     P->NCM = nc;
-    P->NMMA = std::max(16, round_up(nr, 16));
-    P->QM = std::max((15 + ch + nr - 1 + 15) / 16, (ch + 15 + 15) / 16 + 1);
-    const int U = P->NMMA + 16 * (P->QM - 1);
-    P->u_min = -16 * (P->QM - 1);
-    P->PS = U * 16;
+    P->NB = round_up(ch + 30, 16);
+    if (P->NB > 256) return false;
+    P->QM = (15 + ch + nr - 1 + 15) / 16;
+    P->PS = P->NB * 16;
     P->XS = 64 + cw;
     P->QS = P->XS * 16;
-    P->PC = round_up(kPadL + ch + 52, 16);
+    P->XT = round_up(cw + nc - 1, 4) + 4;
+    P->PC = round_up(kPadL + P->NB + 20, 16);
     P->NRS = nr | 1;
     size_t off = static_cast<size_t>(cw) * P->PS;
     P->off_W = static_cast<unsigned>(off);
     off += static_cast<size_t>(P->QM) * P->QS;
+    P->off_T = static_cast<unsigned>(off);
+    off += static_cast<size_t>(16 * P->QM) * P->XT;
+    off = (off + 15) & ~size_t(15);
     P->off_P = static_cast<unsigned>(off);
     off += static_cast<size_t>(cw) * P->PC;
     off = (off + 15) & ~size_t(15);
     P->off_V = static_cast<unsigned>(off);
     const size_t vbytes = 2ull * nr * (cw + nc - 1) * 4;
-    const size_t nbytes = static_cast<size_t>(nc) * P->NRS * 4;
+    const size_t nbytes = (static_cast<size_t>(nc) * P->NRS * 4 + 15) & ~size_t(15);
     P->off_num = P->off_V;
-    P->off_est = static_cast<unsigned>(off + ((nbytes + 15) & ~size_t(15)));
-    off += std::max(vbytes, 2 * ((nbytes + 15) & ~size_t(15)));
+    P->off_est = static_cast<unsigned>(off + nbytes);  // estimates, then bounds
+    off += std::max(vbytes, 3 * nbytes);
     off = (off + 15) & ~size_t(15);
     P->off_S1 = static_cast<unsigned>(off);
-    off += (nbytes + 15) & ~size_t(15);
+    off += nbytes;
     P->off_S2 = static_cast<unsigned>(off);
-    off += (nbytes + 15) & ~size_t(15);
+    off += nbytes;
     P->off_red = static_cast<unsigned>(off);
     off += 3 * 32 * 8;
     P->smem = off;
+    const int dcols = 16 * (P->QM - 1) + P->NB;
     uint32_t cols = 32;
-    while (static_cast<int>(cols) < P->NMMA) cols <<= 1;
+    while (static_cast<int>(cols) < dcols) cols <<= 1;
+    if (cols > 512) return false;
     P->tmem_cols = cols;
     return off <= smem_cap;
 }
@@ -1624,7 +1714,7 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
     }
     TcPlan TP{};
     const bool use_tc = dtype == AR_U8 && scratch.tensor_cores &&
-                        plan_corr_tc(geom, 200 * 1024, &TP);
+                        plan_corr_tc(geom, 220 * 1024, &TP);
     if (use_tc) {
         TcArgs B{};
         B.ref = static_cast<const uint8_t*>(ref);
@@ -1637,18 +1727,20 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         B.pady = geom.pady;
         B.up = up;
         B.measure = measure;
-        B.NMMA = TP.NMMA;
+        B.NB = TP.NB;
         B.QM = TP.QM;
         B.QS = TP.QS;
         B.PS = TP.PS;
         B.PC = TP.PC;
         B.XS = TP.XS;
+        B.XT = TP.XT;
         B.NRS = TP.NRS;
         B.NRM = TP.NRM;
         B.NCM = TP.NCM;
         B.CHM = TP.CHM;
-        B.u_min = TP.u_min;
+        B.CWM = TP.CWM;
         B.off_W = TP.off_W;
+        B.off_T = TP.off_T;
         B.off_P = TP.off_P;
         B.off_V = TP.off_V;
         B.off_S1 = TP.off_S1;
@@ -1665,13 +1757,16 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         B.surf_out = surf_out;
         B.flops = A.flops;
         B.status = scratch.status;
-        // At least half of an SM's shared memory per CTA: one CTA per SM, so the Tensor Memory
-        // each CTA holds for its lifetime (<= 256 of 512 columns) never waits on another's.
-        const size_t tc_smem = std::max<size_t>(TP.smem, 116 * 1024);
+        // Each CTA holds its Tensor Memory columns for its lifetime, so the CTAs one SM can
+        // hold must fit its 512 columns together: at most two CTAs of <= 256 columns (at least
+        // 76 KB of shared memory each), otherwise one (at least 116 KB).
+        const int per_sm_tc = TP.tmem_cols <= 256 && TP.smem <= 112 * 1024 ? 2 : 1;
+        const size_t tc_smem = std::max<size_t>(TP.smem, per_sm_tc == 2 ? 76 * 1024 : 116 * 1024);
         e = cudaFuncSetAttribute(k_corr_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(tc_smem));
         if (e != cudaSuccess) return e;
-        const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(pts.n, num_sms)));
+        const int grid = static_cast<int>(
+            std::max<int64_t>(1, std::min<int64_t>(pts.n, static_cast<int64_t>(num_sms) * per_sm_tc)));
         k_corr_tc<<<grid, kTcThreads, tc_smem, stream>>>(B);
         e = cudaGetLastError();
     }

@@ -191,11 +191,12 @@ int ar_multichip_device(ar_ctx* ctx, const ar_pair* pair, const ar_points* grid_
  * Diagnostic: one tensor-core product (tcgen05.mma kind::i8, unsigned 8-bit operands, 32-bit
  * integer accumulator) of two operand images placed in shared memory as given, read through
  * SWIZZLE_NONE K-major descriptors. params = {a_off, a_lbo, a_sbo, a_kstep, b_off, b_lbo,
- * b_sbo, b_kstep, M, N, nk}: byte offsets and strides (multiples of 16), M in {64, 128}, N, and
- * nk K-steps of 32 accumulated, step s reading at offset + s * kstep. `d_out` receives the
- * accumulator as 128 Tensor Memory lanes x N columns (int32, lane-major). Descriptors that
- * would read outside an image are rejected. It validates on a device the operand layouts the
- * correlation kernel builds; no reference counterpart.
+ * b_sbo, b_kstep, M, N, nk, dstep}: byte offsets and strides (multiples of 16), M in {64, 128},
+ * N, and nk K-steps of 32 accumulated, step s reading at offset + s * kstep and, when dstep > 0,
+ * adding into accumulator columns [s * dstep, s * dstep + N) of a cleared accumulator. `d_out`
+ * receives the accumulator as 128 Tensor Memory lanes x (N + (nk - 1) * dstep) columns (int32,
+ * lane-major). Descriptors that would read outside an image are rejected. It validates on a
+ * device the operand layouts the correlation kernel builds; no reference counterpart.
  */
 int ar_tc_selftest(ar_ctx* ctx, const uint8_t* a_img, int a_bytes, const uint8_t* b_img,
                    int b_bytes, const int* params, int32_t* d_out);

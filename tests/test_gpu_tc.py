@@ -17,9 +17,10 @@ def run(ar, a_img, b_img, params):
     ctx = ar._lib.default_context()
     a_img = np.ascontiguousarray(a_img, np.uint8)
     b_img = np.ascontiguousarray(b_img, np.uint8)
-    N = params[9]
-    out = np.zeros((128, N), np.int32)
-    prm = (ctypes.c_int * 11)(*params)
+    params = list(params) + [0] * (12 - len(params))
+    N, nk, dstep = params[9], params[10], params[11]
+    out = np.zeros((128, N + (nk - 1) * dstep), np.int32)
+    prm = (ctypes.c_int * 12)(*params)
     ctx.check(ctx.lib.ar_tc_selftest(ctx.handle, a_img.ctypes.data, a_img.size, b_img.ctypes.data,
                                      b_img.size, prm, out.ctypes.data))
     return out
@@ -81,6 +82,21 @@ def test_accumulate_over_k_steps(ar, gpu_lib):
     D = run(ar, TA.reshape(-1), TB.reshape(-1),
             [0, 16, 128, 32, 0, 40 * 16, 128, 48, M, N, nk])
     assert np.array_equal(lanes(D, M)[:, :N], want)
+
+
+def test_column_offset_accumulation(ar, gpu_lib):
+    """Step s adds into accumulator columns [16 s, 16 s + N): the correlation kernel's compact
+    chip operand, whose N rows are the same for every window block."""
+    rng = np.random.default_rng(6)
+    M, N, nk, dstep = 64, 64, 6, 16
+    TA = rng.integers(0, 256, (M + 2 * nk + 1, 16), dtype=np.uint8)
+    B = rng.integers(0, 256, (N, 32), dtype=np.uint8)
+    want = np.zeros((M, N + (nk - 1) * dstep), np.int64)
+    for st in range(nk):
+        A = np.concatenate([TA[2 * st:2 * st + M], TA[2 * st + 1:2 * st + 1 + M]], axis=1)
+        want[:, st * dstep:st * dstep + N] += A.astype(np.int64) @ B.astype(np.int64).T
+    D = run(ar, TA.reshape(-1), planes(B), [0, 16, 128, 32, 0, N * 16, 128, 0, M, N, nk, dstep])
+    assert np.array_equal(lanes(D, M), want)
 
 
 def test_out_of_image_descriptor_rejected(ar, gpu_lib):
