@@ -549,7 +549,9 @@ struct TcArgs {
     int64_t padx, pady;
     int up, measure;
     int NB, QM, QS, PS, PC, XS, XT, NRS, NRM, NCM, CHM, CWM;
-    unsigned off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
+    int BC;                          // chip columns per chunk of the chip operand (even)
+    int big;                         // 1: box sums before the products, chunks reuse their space
+    unsigned off_E, off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
     uint32_t tmem_cols;
     DevOutputs out;
     int* sub_count;
@@ -629,7 +631,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
     __shared__ int s_slot;
     __shared__ float s_fmax[kTcThreads / 32];
     __shared__ unsigned long long s_isum[2][2];
-    uint8_t* s_E = smem_tc;
+    uint8_t* s_E = smem_tc + A.off_E;
     uint8_t* s_W = smem_tc + A.off_W;
     uint8_t* s_T = smem_tc + A.off_T;
     uint8_t* s_P = smem_tc + A.off_P;
@@ -802,95 +804,116 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                 }
             }
         }
-        __syncthreads();  // s_P complete
-        // E: NB rows u = 16 - NB ... 15 per chip column, row u at (u - 16 + NB) * 16.
-        for (int e = tid; e < cw * A.NB; e += bd) {
-            const int b = e / A.NB, u = 16 - A.NB + e % A.NB;
-            const int src = b * A.PC + kPadL - u - static_cast<int>(delta);
-            const uint32_t* w = reinterpret_cast<const uint32_t*>(s_P + (src & ~3));
-            const uint32_t sh = static_cast<uint32_t>(src & 3) * 8u;
-            uint4 o;
-            o.x = __funnelshift_r(w[0], w[1], sh);
-            o.y = __funnelshift_r(w[1], w[2], sh);
-            o.z = __funnelshift_r(w[2], w[3], sh);
-            o.w = __funnelshift_r(w[3], w[4], sh);
-            *reinterpret_cast<uint4*>(s_E + b * A.PS + (e % A.NB) * 16) = o;
+        __syncthreads();  // s_P, s_W, s_T complete
+
+        // Box sums of W and W^2 (integral_both!, boxsum, src/integral.jl:141-170, 244-247) as
+        // exact integers: V[i][x] sums ch rows down column x, S[j][i] sums cw columns of V.
+        // They run while the tensor core works on the first chunk, or, when the chip operand
+        // comes in several chunks that reuse their space, before it.
+        auto box_sums = [&]() {
+            uint32_t* s_V2 = s_V1 + A.NRM * XW;
+            const int nseg = (nr + 15) >> 4;
+            for (int task = tid; task < XW * nseg; task += bd) {
+                const int x = task % XW, seg = task / XW;
+                const int i0 = seg << 4, i1 = min(i0 + 16, nr);
+                const uint8_t* col = s_T + static_cast<int>(delta) * A.XT + x;
+                uint32_t h1 = 0, h2 = 0;
+                for (int a = 0; a < ch; ++a) {
+                    const uint32_t w = col[(i0 + a) * A.XT];
+                    h1 += w;
+                    h2 += w * w;
+                }
+                for (int i = i0; i < i1; ++i) {
+                    s_V1[i * XW + x] = h1;
+                    s_V2[i * XW + x] = h2;
+                    if (i + 1 < i1) {
+                        const uint32_t wn = col[(i + ch) * A.XT], wo = col[i * A.XT];
+                        h1 = h1 + wn - wo;
+                        h2 = h2 + wn * wn - wo * wo;
+                    }
+                }
+            }
+            __syncthreads();
+            const int jseg = (nc + 15) >> 4;
+            for (int task = tid; task < nr * jseg; task += bd) {
+                const int i = task % nr, seg = task / nr;
+                const int j0 = seg << 4, j1 = min(j0 + 16, nc);
+                uint32_t g1 = 0, g2 = 0;
+                for (int b = 0; b < cw; ++b) {
+                    g1 += s_V1[i * XW + j0 + b];
+                    g2 += s_V2[i * XW + j0 + b];
+                }
+                for (int j = j0; j < j1; ++j) {
+                    s_S1[j * A.NRS + i] = g1;
+                    s_S2[j * A.NRS + i] = g2;
+                    if (j + 1 < j1) {
+                        g1 = g1 + s_V1[i * XW + j + cw] - s_V1[i * XW + j];
+                        g2 = g2 + s_V2[i * XW + j + cw] - s_V2[i * XW + j];
+                    }
+                }
+            }
+        };
+        if (A.big) {
+            box_sums();
+            __syncthreads();  // the chip chunks overwrite s_T and s_V
         }
-        // Clear the accumulator columns the products add into (warps 0-3: one lane quarter each).
+
         const int dcols = 16 * (Q - 1) + A.NB;
-        if (warp < 4) {
-            uint32_t z[16];
+        const int nchunk = (cw + A.BC - 1) / A.BC;
+        bool ok = true;
+        for (int cc = 0; cc < nchunk; ++cc) {
+            const int b0 = cc * A.BC, b1 = min(cw, b0 + A.BC);
+            if (cc > 0) {
+                // The previous chunk's products must be done before its rows are replaced.
+                ok = tc::mbar_wait(&s_mbar, phase, kTcWaitPolls);
+                phase ^= 1u;
+                if (__syncthreads_or(!ok)) break;
+                tc::fence_after_sync();
+            }
+            // E: NB rows u = 16 - NB ... 15 per chip column, row u at (u - 16 + NB) * 16.
+            for (int e = tid; e < (b1 - b0) * A.NB; e += bd) {
+                const int bl = e / A.NB, b = b0 + bl, u = 16 - A.NB + e % A.NB;
+                const int src = b * A.PC + kPadL - u - static_cast<int>(delta);
+                const uint32_t* w = reinterpret_cast<const uint32_t*>(s_P + (src & ~3));
+                const uint32_t sh = static_cast<uint32_t>(src & 3) * 8u;
+                uint4 o;
+                o.x = __funnelshift_r(w[0], w[1], sh);
+                o.y = __funnelshift_r(w[1], w[2], sh);
+                o.z = __funnelshift_r(w[2], w[3], sh);
+                o.w = __funnelshift_r(w[3], w[4], sh);
+                *reinterpret_cast<uint4*>(s_E + bl * A.PS + (e % A.NB) * 16) = o;
+            }
+            if (cc == 0 && warp < 4) {
+                // Clear the accumulator columns the products add into (one lane quarter each).
+                uint32_t z[16];
 #pragma unroll
-            for (int t = 0; t < 16; ++t) z[t] = 0u;
-            for (int c = 0; c < dcols; c += 16)
-                tc::tmem_st16(taddr + (static_cast<uint32_t>(32 * warp) << 16) + static_cast<uint32_t>(c), z);
-            tc::tmem_wait_st();
-        }
-        tc::fence_proxy_async_smem();
-        tc::fence_before_sync();
-        __syncthreads();
-
-        if (tid == 0) {
-            tc::fence_after_sync();
-            const uint32_t sW = tc::smem_u32(s_W), sE = tc::smem_u32(s_E);
-            const uint32_t idesc = tc::idesc_u8_s32(64, A.NB);
-            for (int q = 0; q < Q; ++q)
-                for (int t = 0; t < cw / 2; ++t) {
-                    const uint64_t da = tc::smem_desc(sW + q * A.QS + 32 * t, 16, 128);
-                    const uint64_t db = tc::smem_desc(sE + 2 * t * A.PS, A.PS, 128);
-                    tc::mma_u8(taddr + static_cast<uint32_t>(16 * q), da, db, idesc, true);
-                }
-            tc::mma_commit(&s_mbar);
-        }
-
-        // While the tensor core runs: box sums of W and W^2 (integral_both!, boxsum,
-        // src/integral.jl:141-170, 244-247) as exact integers. V[i][x] sums ch rows down
-        // column x; S[j][i] sums cw columns of V.
-        uint32_t* s_V2 = s_V1 + A.NRM * XW;
-        const int nseg = (nr + 15) >> 4;
-        for (int task = tid; task < XW * nseg; task += bd) {
-            const int x = task % XW, seg = task / XW;
-            const int i0 = seg << 4, i1 = min(i0 + 16, nr);
-            const uint8_t* col = s_T + static_cast<int>(delta) * A.XT + x;
-            uint32_t h1 = 0, h2 = 0;
-            for (int a = 0; a < ch; ++a) {
-                const uint32_t w = col[(i0 + a) * A.XT];
-                h1 += w;
-                h2 += w * w;
+                for (int t = 0; t < 16; ++t) z[t] = 0u;
+                for (int c = 0; c < dcols; c += 16)
+                    tc::tmem_st16(taddr + (static_cast<uint32_t>(32 * warp) << 16) + static_cast<uint32_t>(c), z);
+                tc::tmem_wait_st();
             }
-            for (int i = i0; i < i1; ++i) {
-                s_V1[i * XW + x] = h1;
-                s_V2[i * XW + x] = h2;
-                if (i + 1 < i1) {
-                    const uint32_t wn = col[(i + ch) * A.XT], wo = col[i * A.XT];
-                    h1 = h1 + wn - wo;
-                    h2 = h2 + wn * wn - wo * wo;
-                }
+            tc::fence_proxy_async_smem();
+            tc::fence_before_sync();
+            __syncthreads();
+            if (tid == 0) {
+                tc::fence_after_sync();
+                const uint32_t sW = tc::smem_u32(s_W), sE = tc::smem_u32(s_E);
+                const uint32_t idesc = tc::idesc_u8_s32(64, A.NB);
+                for (int q = 0; q < Q; ++q)
+                    for (int t = b0 / 2; t < b1 / 2; ++t) {
+                        const uint64_t da = tc::smem_desc(sW + q * A.QS + 32 * t, 16, 128);
+                        const uint64_t db = tc::smem_desc(sE + (2 * t - b0) * A.PS, A.PS, 128);
+                        tc::mma_u8(taddr + static_cast<uint32_t>(16 * q), da, db, idesc, true);
+                    }
+                tc::mma_commit(&s_mbar);
             }
+            if (cc == 0 && !A.big) box_sums();
         }
-        __syncthreads();
-        const int jseg = (nc + 15) >> 4;
-        for (int task = tid; task < nr * jseg; task += bd) {
-            const int i = task % nr, seg = task / nr;
-            const int j0 = seg << 4, j1 = min(j0 + 16, nc);
-            uint32_t g1 = 0, g2 = 0;
-            for (int b = 0; b < cw; ++b) {
-                g1 += s_V1[i * XW + j0 + b];
-                g2 += s_V2[i * XW + j0 + b];
-            }
-            for (int j = j0; j < j1; ++j) {
-                s_S1[j * A.NRS + i] = g1;
-                s_S2[j * A.NRS + i] = g2;
-                if (j + 1 < j1) {
-                    g1 = g1 + s_V1[i * XW + j + cw] - s_V1[i * XW + j];
-                    g2 = g2 + s_V2[i * XW + j + cw] - s_V2[i * XW + j];
-                }
-            }
+        if (ok) {
+            // Wait for the last chunk's products (bounded; every thread polls the same phase).
+            ok = tc::mbar_wait(&s_mbar, phase, kTcWaitPolls);
+            phase ^= 1u;
         }
-
-        // Wait for the products (bounded; every thread polls the same barrier phase).
-        const bool ok = tc::mbar_wait(&s_mbar, phase, kTcWaitPolls);
-        phase ^= 1u;
         if (__syncthreads_or(!ok)) {
             if (tid == 0) atomicExch(A.status, 1);
             failed = true;
@@ -1463,14 +1486,17 @@ RefinePlan plan_refine(int up) {
 }
 
 struct TcPlan {
-    int NB, QM, QS, PS, PC, XS, XT, NRS, NRM, NCM, CHM, CWM;
-    unsigned off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
+    int NB, QM, QS, PS, PC, XS, XT, NRS, NRM, NCM, CHM, CWM, BC, big;
+    unsigned off_E, off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
     uint32_t tmem_cols;
     size_t smem;
 };
 
 // Shared-memory plan of k_corr_tc for a pass's largest geometry; false when the pass does not
-// fit the kernel (surface wider than 64 columns, more than 256 rows, or buffers too large).
+// fit the kernel (surface wider than 64 columns, more than 256 rows, chips taller than 226).
+// The whole chip operand and separate box-sum buffers when they fit ("overlap": the box sums
+// run beside the products); otherwise the box sums first and the chip operand in chunks of BC
+// columns in the space they used.
 bool plan_corr_tc(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
     const int ch = static_cast<int>(g.max_ch), cw = static_cast<int>(g.max_cw);
     const int nr = static_cast<int>(g.max_nr), nc = static_cast<int>(g.max_nc);
@@ -1488,35 +1514,73 @@ bool plan_corr_tc(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
     P->XT = round_up(cw + nc - 1, 4) + 4;
     P->PC = round_up(kPadL + P->NB + 20, 16);
     P->NRS = nr | 1;
-    size_t off = static_cast<size_t>(cw) * P->PS;
-    P->off_W = static_cast<unsigned>(off);
-    off += static_cast<size_t>(P->QM) * P->QS;
-    P->off_T = static_cast<unsigned>(off);
-    off += static_cast<size_t>(16 * P->QM) * P->XT;
-    off = (off + 15) & ~size_t(15);
-    P->off_P = static_cast<unsigned>(off);
-    off += static_cast<size_t>(cw) * P->PC;
-    off = (off + 15) & ~size_t(15);
-    P->off_V = static_cast<unsigned>(off);
-    const size_t vbytes = 2ull * nr * (cw + nc - 1) * 4;
-    const size_t nbytes = (static_cast<size_t>(nc) * P->NRS * 4 + 15) & ~size_t(15);
-    P->off_num = P->off_V;
-    P->off_est = static_cast<unsigned>(off + nbytes);  // estimates, then bounds
-    off += std::max(vbytes, 3 * nbytes);
-    off = (off + 15) & ~size_t(15);
-    P->off_S1 = static_cast<unsigned>(off);
-    off += nbytes;
-    P->off_S2 = static_cast<unsigned>(off);
-    off += nbytes;
-    P->off_red = static_cast<unsigned>(off);
-    off += 3 * 32 * 8;
-    P->smem = off;
     const int dcols = 16 * (P->QM - 1) + P->NB;
     uint32_t cols = 32;
     while (static_cast<int>(cols) < dcols) cols <<= 1;
     if (cols > 512) return false;
     P->tmem_cols = cols;
-    return off <= smem_cap;
+    auto a16 = [](size_t v) { return (v + 15) & ~size_t(15); };
+    const size_t Eb = static_cast<size_t>(cw) * P->PS;
+    const size_t Wb = static_cast<size_t>(P->QM) * P->QS;
+    const size_t Tb = a16(static_cast<size_t>(16 * P->QM) * P->XT);
+    const size_t Pb = a16(static_cast<size_t>(cw) * P->PC);
+    const size_t Vb = a16(2ull * nr * (cw + nc - 1) * 4);
+    const size_t nbytes = a16(static_cast<size_t>(nc) * P->NRS * 4);
+    const size_t red = 3 * 32 * 8;
+    // Overlap layout: [E][W][T][P][V | num, est, bound][S1][S2][red].
+    {
+        size_t off = 0;
+        P->off_E = 0;
+        off += Eb;
+        P->off_W = static_cast<unsigned>(off);
+        off += Wb;
+        P->off_T = static_cast<unsigned>(off);
+        off += Tb;
+        P->off_P = static_cast<unsigned>(off);
+        off += Pb;
+        P->off_V = static_cast<unsigned>(off);
+        P->off_num = P->off_V;
+        P->off_est = static_cast<unsigned>(off + nbytes);
+        off += std::max(Vb, 3 * nbytes);
+        P->off_S1 = static_cast<unsigned>(off);
+        off += nbytes;
+        P->off_S2 = static_cast<unsigned>(off);
+        off += nbytes;
+        P->off_red = static_cast<unsigned>(off);
+        off += red;
+        if (off <= smem_cap) {
+            P->smem = off;
+            P->BC = cw;
+            P->big = 0;
+            return true;
+        }
+    }
+    // Chunked layout: [W][P][S1][S2][red][zone], the zone holding T and V for the box sums,
+    // then the chunks of the chip operand, then num, estimates and bounds.
+    size_t off = 0;
+    P->off_W = 0;
+    off += Wb;
+    P->off_P = static_cast<unsigned>(off);
+    off += Pb;
+    P->off_S1 = static_cast<unsigned>(off);
+    off += nbytes;
+    P->off_S2 = static_cast<unsigned>(off);
+    off += nbytes;
+    P->off_red = static_cast<unsigned>(off);
+    off += red;
+    off = a16(off);
+    const size_t zone_min = std::max(Tb + Vb, 3 * nbytes);
+    if (off + std::max(zone_min, 2 * static_cast<size_t>(P->PS)) > smem_cap) return false;
+    const size_t avail = smem_cap - off;
+    int bc = static_cast<int>(std::min<size_t>(cw, avail / P->PS)) & ~1;
+    if (bc < 2) return false;
+    P->BC = bc;
+    P->big = 1;
+    P->off_E = P->off_T = P->off_num = static_cast<unsigned>(off);
+    P->off_V = static_cast<unsigned>(off + Tb);
+    P->off_est = static_cast<unsigned>(off + nbytes);
+    P->smem = off + std::max(zone_min, static_cast<size_t>(bc) * P->PS);
+    return true;
 }
 
 template <typename T>
@@ -1739,6 +1803,9 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         B.NCM = TP.NCM;
         B.CHM = TP.CHM;
         B.CWM = TP.CWM;
+        B.BC = TP.BC;
+        B.big = TP.big;
+        B.off_E = TP.off_E;
         B.off_W = TP.off_W;
         B.off_T = TP.off_T;
         B.off_P = TP.off_P;

@@ -65,6 +65,21 @@ def test_track_identical(ar, gpu_lib, case):
     assert np.count_nonzero(~np.isnan(a.dx)) > n // 3
 
 
+@pytest.mark.parametrize("chip,r", [(64, 25), (128, 25), (96, 20), (128, 6)])
+def test_track_large_chips_identical(ar, gpu_lib, chip, r):
+    """Chips whose operand is built and multiplied in several chunks."""
+    ref, sec = ar.synthetic.shifted_pair(640, (-5.3, 3.7), seed=29, dtype=np.uint8)
+    rng = np.random.default_rng(chip + r)
+    n = 300
+    pts = ar.pointset(rng.uniform(60, 580, n), rng.uniform(60, 580, n), chip_size=chip,
+                      search_radius=r, dy_prior=np.round(rng.uniform(-2, 2, n)))
+    pair = ar.ImagePair(ref, sec)
+    p = ar.params(preprocess="none", quantize="none", upsampling=16)
+    a, b = both(ar, lambda ctx: ar.track(pair, pts, p, ctx=ctx))
+    check_fields(a, b)
+    assert np.count_nonzero(~np.isnan(a.dx)) > n // 2
+
+
 def test_track_mixed_geometry(ar, gpu_lib):
     """Per-point radii (including 0: not searchable) and chip sizes in one pass."""
     ref, sec = ar.synthetic.shifted_pair(320, (-3.2, 5.4), seed=23, dtype=np.uint8)
