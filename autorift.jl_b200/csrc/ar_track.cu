@@ -40,7 +40,6 @@ namespace {
 constexpr int kMI = 10;        // surface rows per thread item
 constexpr int kUA = 16;        // chip rows per inner step
 constexpr int kCorrThreads = 256;
-constexpr int kRefineThreads = 256;
 constexpr unsigned kFull = 0xffffffffu;
 
 template <typename T>
@@ -1037,20 +1036,23 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
 }
 
 // ----------------------------------------------------------------------------------------------
-// Sub-pixel cascade kernel (src/peak.jl:456-522 from the patch onward).
+// Sub-pixel cascade kernel (src/peak.jl:456-522 from the patch onward), one warp per patch.
 //
-// Levels up to (5 * up / 4)^2 are materialised in shared memory. The last two levels -- 90%
-// of the samples at up = 64 -- are produced in blocks of the final level, and a block is
-// evaluated only if it can hold the maximum: every pyrUp sample is a rounded convex
-// combination of its taps, so a final sample cannot exceed the largest materialised sample
-// under its two-level footprint by more than a few ulps. Blocks are visited in decreasing
-// order of that bound and the search stops once the best remaining bound is strictly below
-// the maximum found, so the result (value and row-major-first position) is exactly that of
-// the full cascade.
+// Levels 1 and 2 of the cascade (10^2, 20^2) are materialised in the warp's shared memory. Up to
+// 8x the final level is materialised too. Beyond, the final level is cut into 16 x 16 blocks and
+// a block's samples are computed through its dependency cone only: the rows and columns of each
+// coarser level its taps reach, down to level 2. Every pyrUp sample is a rounded convex
+// combination of its taps, so no sample of a block exceeds the largest level-2 sample of its
+// cone by more than the accumulated rounding (bounded by k * 2^-20 * max|level 2| over k
+// levels). Blocks are visited in decreasing order of that bound; a visited block is first
+// carried to level L - 2, where the largest cone sample gives a tighter two-level bound, and is
+// finished only if that bound still reaches the best value found. The search ends when the best
+// remaining bound is strictly below the best value, so the result (value and row-major-first
+// position) is exactly the full cascade's: each computed sample is the same function of the same
+// inputs as in the full cascade.
 
-constexpr int kQB = 16;  // penultimate-level rows per final block (32 final rows)
-constexpr int kCB = 64;  // final-level columns per final block
-constexpr int kMaxBlocks = 256;
+constexpr int kRefineWarps = 8;
+constexpr int kFB = 16;  // final-level block side
 
 struct RefineArgs {
     const int* count;       // device count of queued items (or null: use n_items)
@@ -1064,8 +1066,7 @@ struct RefineArgs {
     int32_t* ocol;
     float* oval;
     int levels;             // log2(upsampling) >= 1
-    int nmat;               // size of the last materialised level
-    unsigned off_B, off_T, off_P, off_C;  // float offsets: A at 0
+    int warp_floats;        // shared floats per warp
 };
 
 // Taps of output position p on an axis whose source has n >= 2 samples: the closed form of
@@ -1082,31 +1083,33 @@ __device__ __forceinline__ int taps(int p, int n, int& m, int& c, int& q) {
     return 3;
 }
 
-// One pyrUp step over shared memory, src (sh x sw) -> dst (2sh x 2sw) via tmp (2sh x sw);
-// all column-major. Vertical then horizontal, as src/peak.jl:261-292. Warps own columns,
-// lanes rows, so no index division is needed.
-__device__ void pyrup_block(const float* src, int sh, int sw, float* dst, float* tmp) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int th = 2 * sh;
-    for (int j = warp; j < sw; j += nw) {
-        const float* s = src + j * sh;
-        for (int i = lane; i < th; i += 32) {
-            int m, c, q;
-            const int nt = taps(i, sh, m, c, q);
-            tmp[i + j * th] = pyr_sample(nt, s[m], s[c], s[q]);
-        }
-    }
-    __syncthreads();
-    for (int j = warp; j < 2 * sw; j += nw) {
+// Source index range [lo, hi] the taps of outputs [p0, p1] read (source size n).
+__device__ __forceinline__ void tap_range(int p0, int p1, int n, int& lo, int& hi) {
+    lo = (p0 & 1) ? (p0 >> 1) : max((p0 >> 1) - 1, 0);
+    hi = min((p1 >> 1) + 1, n - 1);
+}
+
+// One full pyrUp step by a warp: src (S x S, column-major) -> dst (2S x 2S) via tmp (2S x S).
+// Vertical then horizontal, as src/peak.jl:261-292.
+template <int S>
+__device__ void pyrup_warp(const float* src, float* dst, float* tmp) {
+    const int lane = threadIdx.x & 31;
+    constexpr int D = 2 * S;
+    for (int e = lane; e < D * S; e += 32) {
+        const int i = e % D, j = e / D;
         int m, c, q;
-        const int nt = taps(j, sw, m, c, q);
-        const float* tm = tmp + m * th;
-        const float* tc = tmp + c * th;
-        const float* tq = tmp + q * th;
-        float* d = dst + j * th;
-        for (int i = lane; i < th; i += 32) d[i] = pyr_sample(nt, tm[i], tc[i], tq[i]);
+        const int nt = taps(i, S, m, c, q);
+        const float* s = src + j * S;
+        tmp[e] = pyr_sample(nt, s[m], s[c], s[q]);
     }
-    __syncthreads();
+    __syncwarp();
+    for (int e = lane; e < D * D; e += 32) {
+        const int i = e % D, j = e / D;
+        int m, c, q;
+        const int nt = taps(j, S, m, c, q);
+        dst[e] = pyr_sample(nt, tmp[i + m * D], tmp[i + c * D], tmp[i + q * D]);
+    }
+    __syncwarp();
 }
 
 // (value, row-major index) pairs: larger value wins, equal values go to the smaller index;
@@ -1118,22 +1121,7 @@ __device__ __forceinline__ void best_update(float v, int idx, float& bv, int& bi
     }
 }
 
-__device__ void block_best(float& bv, int& bi, float* rv, int* ri) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const float v2 = __shfl_xor_sync(kFull, bv, o);
-        const int i2 = __shfl_xor_sync(kFull, bi, o);
-        best_update(v2, i2, bv, bi);
-    }
-    __syncthreads();
-    if (lane == 0) {
-        rv[warp] = bv;
-        ri[warp] = bi;
-    }
-    __syncthreads();
-    bv = lane < nw ? rv[lane] : -INFINITY;
-    bi = lane < nw ? ri[lane] : INT_MAX;
+__device__ __forceinline__ void warp_best(float& bv, int& bi) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         const float v2 = __shfl_xor_sync(kFull, bv, o);
@@ -1142,177 +1130,229 @@ __device__ void block_best(float& bv, int& bi, float* rv, int* ri) {
     }
 }
 
-// Upper bound on any sample two pyrUp levels above values <= m: rounding in
-// fl(fl(0.75b) + fl(0.125 fl(a+c))) can exceed the largest tap by under 2^-23 relative per
-// level; the slack here is 2^-20 relative plus the smallest normal.
-__device__ __forceinline__ float two_level_bound(float m) {
-    return m + fabsf(m) * 9.5367431640625e-07f + 1.17549435e-38f;
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(kFull, v, o));
+    return v;
 }
 
-__global__ void __launch_bounds__(kRefineThreads) k_refine(const RefineArgs A) {
+// A cone level: rows [r0, r1] and columns [c0, c1] of a level of size n.
+struct ConeLevel {
+    int r0, r1, c0, c1;
+};
+
+// Level region `dst` (rows d.r0..d.r1, columns d.c0..d.c1) of a level computed from the source
+// region `s` of the level below (size n), stored column-major from its first element with
+// leading dimension lds; tmp holds the vertical pass (dst rows x source columns). Regions have
+// at most 16 rows: lanes 0-15 and 16-31 take alternate columns.
+__device__ void cone_step(const float* src, int lds, const ConeLevel& s, int n,
+                          const ConeLevel& d, float* tmp, float* dst) {
+    const int lane = threadIdx.x & 31;
+    const int r = lane & 15, cpar = lane >> 4;
+    const int rows = d.r1 - d.r0 + 1, scols = s.c1 - s.c0 + 1;
+    if (r < rows) {
+        int m, c, q;
+        const int nt = taps(d.r0 + r, n, m, c, q);
+        m -= s.r0;
+        c -= s.r0;
+        q -= s.r0;
+        for (int cc = cpar; cc < scols; cc += 2) {
+            const float* col = src + cc * lds;
+            tmp[r + cc * rows] = pyr_sample(nt, col[m], col[c], col[q]);
+        }
+    }
+    __syncwarp();
+    if (r < rows) {
+        for (int cc = cpar; cc <= d.c1 - d.c0; cc += 2) {
+            int m, c, q;
+            const int nt = taps(d.c0 + cc, n, m, c, q);
+            dst[r + cc * rows] = pyr_sample(nt, tmp[r + (m - s.c0) * rows],
+                                            tmp[r + (c - s.c0) * rows], tmp[r + (q - s.c0) * rows]);
+        }
+    }
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(kRefineWarps * 32) k_refine(const RefineArgs A) {
     extern __shared__ __align__(16) float rsm[];
-    float* sA = rsm;
-    float* sB = rsm + A.off_B;
-    float* sT = rsm + A.off_T;
-    float* sP = rsm + A.off_P;
-    float* sC = rsm + A.off_C;  // block buffers (alias sB/sT once materialised)
-    __shared__ float rv[32];
-    __shared__ int ri[32];
-    __shared__ float sbound[kMaxBlocks];
-    __shared__ float s_best;
-    __shared__ int s_sel;
-
-    const int tid = threadIdx.x, bd = blockDim.x;
-    const int lane = tid & 31, warp = tid >> 5, nw = bd >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float* W = rsm + warp * A.warp_floats;
+    float* P0 = W;            // 5 x 5 (32)
+    float* L1 = W + 32;       // 10 x 10
+    float* L2 = L1 + 100;     // 20 x 20
+    float* WK = L2 + 400;     // level-3 materialisation, or bounds and cone buffers
     const int64_t count = A.count ? static_cast<int64_t>(*A.count) : A.n_items;
     const int L = A.levels;
-    const int nmat_levels = L <= 2 ? L : L - 2;
 
-    for (int64_t item = blockIdx.x; item < count; item += gridDim.x) {
-        __syncthreads();
-        if (tid < 25) sP[tid] = A.patch[item * 25 + tid];
-        __syncthreads();
-        const float* cur = sP;
-        int n = 5;
-        for (int lev = 1; lev <= nmat_levels; ++lev) {
-            float* dst = ((nmat_levels - lev) & 1) == 0 ? sA : sB;
-            pyrup_block(cur, n, n, dst, sT);
-            cur = dst;
-            n *= 2;
-        }
+    for (int64_t item = static_cast<int64_t>(blockIdx.x) * kRefineWarps + warp; item < count;
+         item += static_cast<int64_t>(gridDim.x) * kRefineWarps) {
+        if (lane < 25) P0[lane] = A.patch[item * 25 + lane];
+        __syncwarp();
         float bv = -INFINITY;
         int bi = INT_MAX;
-        int nfinal;
-        if (L <= 2) {
-            nfinal = n;
-            for (int j = warp; j < n; j += nw)
-                for (int i = lane; i < n; i += 32) best_update(cur[i + j * n], i * n + j, bv, bi);
-            block_best(bv, bi, rv, ri);
+        int nfinal = 5 << L;
+        float v0 = 0.0f;  // the final level's first sample, reported when nothing beats -Inf
+        if (L <= 3) {
+            // Materialise every level; argmax of the last.
+            const float* fin;
+            if (L == 1) {
+                pyrup_warp<5>(P0, L1, WK);
+                fin = L1;
+            } else {
+                pyrup_warp<5>(P0, L1, WK);
+                pyrup_warp<10>(L1, L2, WK);
+                fin = L2;
+                if (L == 3) {
+                    float* L3 = WK + 800;
+                    pyrup_warp<20>(L2, L3, WK);
+                    fin = L3;
+                }
+            }
+            for (int e = lane; e < nfinal * nfinal; e += 32) {
+                const int i = e % nfinal, j = e / nfinal;
+                best_update(fin[e], i * nfinal + j, bv, bi);
+            }
+            warp_best(bv, bi);
+            v0 = fin[0];
         } else {
-            const int N1 = 2 * n, N2 = 4 * n;
-            nfinal = N2;
-            const int nqb = (N1 + kQB - 1) / kQB, ncb = (N2 + kCB - 1) / kCB;
-            const int nblk = nqb * ncb;
-            // Bounds: the largest materialised sample under each final block's footprint.
-            for (int blk = warp; blk < nblk; blk += nw) {
-                const int qi = blk % nqb, cj = blk / nqb;
-                const int q0 = qi * kQB, q1 = min(q0 + kQB, N1);
-                const int c0 = cj * kCB, c1 = min(c0 + kCB, N2);
-                const int pr0 = max(q0 - 1, 0), pr1 = min(q1, N1 - 1);
-                const int pc0 = max(c0 / 2 - 1, 0), pc1 = min((c1 - 1) / 2 + 1, N1 - 1);
-                const int sr0 = max(pr0 / 2 - 1, 0), sr1 = min(pr1 / 2 + 1, n - 1);
-                const int sc0 = max(pc0 / 2 - 1, 0), sc1 = min(pc1 / 2 + 1, n - 1);
-                const int nr_ = sr1 - sr0 + 1;
+            pyrup_warp<5>(P0, L1, WK);
+            pyrup_warp<10>(L1, L2, WK);
+            // Scale of the rounding slack: the largest magnitude of level 2 bounds every later
+            // level's (up to the growth of rounding itself, covered by the factor 2).
+            float amax = 0.0f;
+            for (int e = lane; e < 400; e += 32) amax = fmaxf(amax, fabsf(L2[e]));
+            amax = warp_max(amax);
+            const float ulp_scale = amax * 9.5367431640625e-07f;  // 2^-20 * max|level 2|
+            auto slack = [&](int k) { return k * ulp_scale + k * 2.3509887e-38f; };
+            const int nb = nfinal / kFB;      // blocks per side
+            float* BND = WK;                  // nb * nb bounds
+            float* CB = WK + nb * nb;         // cone buffers
+            // Cone buffer offsets per level distance d = L - level (regions <= 16, 10, 7, 6, 5 rows).
+            // R_d (region) and T_d (vertical pass) for d = 0 .. L - 3.
+            const int cap[6] = {16, 10, 7, 6, 5, 5};
+            int roff[6], toff[6], off = 0;
+            for (int d = 0; d <= L - 3; ++d) {
+                roff[d] = off;
+                off += cap[d] * cap[d];
+                toff[d] = off;
+                off += cap[d] * cap[d + 1];
+            }
+            // Loose bound of every final block: its level-2 cone maximum plus L - 2 levels of slack.
+            for (int blk = lane; blk < nb * nb; blk += 32) {
+                const int bi_ = blk % nb, bj_ = blk / nb;
+                int r0 = bi_ * kFB, r1 = r0 + kFB - 1, c0 = bj_ * kFB, c1 = c0 + kFB - 1;
+                for (int lev = L - 1; lev >= 2; --lev) {
+                    const int n = 5 << lev;
+                    int a, b;
+                    tap_range(r0, r1, n, a, b);
+                    r0 = a;
+                    r1 = b;
+                    tap_range(c0, c1, n, a, b);
+                    c0 = a;
+                    c1 = b;
+                }
                 float mx = -INFINITY;
-                for (int jj = sc0; jj <= sc1; ++jj)
-                    for (int ii = lane; ii < nr_; ii += 32) mx = fmaxf(mx, cur[(sr0 + ii) + jj * n]);
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, o));
-                if (lane == 0) sbound[blk] = two_level_bound(mx);
+                for (int j = c0; j <= c1; ++j)
+                    for (int i = r0; i <= r1; ++i) mx = fmaxf(mx, L2[i + j * 20]);
+                BND[blk] = mx + slack(L - 2);
             }
-            if (tid == 0) s_best = -INFINITY;
-            __syncthreads();
-            float* TA = sC;                         // (kQB+2) x (kCB/4+4): penultimate rows over S columns
-            float* RB = TA + (kQB + 2) * (kCB / 4 + 4);   // (kQB+2) x (kCB/2+2): penultimate samples
-            float* TB = RB + (kQB + 2) * (kCB / 2 + 2);   // 2kQB x (kCB/2+2): final rows over penultimate columns
-            const int TAS = kCB / 4 + 4, RBS = kCB / 2 + 2;
-            for (int it = 0; it < nblk; ++it) {
-                // Pick the unvisited block with the largest bound (lowest index on ties).
-                if (warp == 0) {
-                    float m = -INFINITY;
-                    int sel = INT_MAX;
-                    for (int b = lane; b < nblk; b += 32) {
-                        const float v = sbound[b];
-                        if (v > m || (v == m && b < sel)) {
-                            m = v;
-                            sel = b;
+            __syncwarp();
+            while (true) {
+                // The unvisited block with the largest bound (lowest index on ties).
+                float m = -INFINITY;
+                int sel = INT_MAX;
+                for (int b = lane; b < nb * nb; b += 32) {
+                    const float v = BND[b];
+                    if (v > m || (v == m && b < sel)) {
+                        m = v;
+                        sel = b;
+                    }
+                }
+                warp_best(m, sel);
+                if (sel == INT_MAX || m == -INFINITY || m < bv) break;
+                __syncwarp();
+                if (lane == 0) BND[sel] = -INFINITY;
+                // The block's cone, from the final level down to level 2.
+                ConeLevel cl[8];
+                {
+                    const int bi_ = sel % nb, bj_ = sel / nb;
+                    cl[0] = {bi_ * kFB, bi_ * kFB + kFB - 1, bj_ * kFB, bj_ * kFB + kFB - 1};
+                    for (int d = 1; d <= L - 2; ++d) {
+                        const int n = 5 << (L - d);
+                        tap_range(cl[d - 1].r0, cl[d - 1].r1, n, cl[d].r0, cl[d].r1);
+                        tap_range(cl[d - 1].c0, cl[d - 1].c1, n, cl[d].c0, cl[d].c1);
+                    }
+                }
+                // Levels 3 .. L - 1 (d = L - 3 .. 1) into the cone buffers.
+                ConeLevel sreg = cl[L - 2];
+                const float* src = L2 + sreg.r0 + sreg.c0 * 20;
+                int lds = 20;
+                bool pruned = false;
+                for (int d = L - 3; d >= 1; --d) {
+                    const int n = 5 << (L - d - 1);  // source level size
+                    float* dst = CB + roff[d];
+                    cone_step(src, lds, sreg, n, cl[d], CB + toff[d], dst);
+                    src = dst;
+                    sreg = cl[d];
+                    lds = cl[d].r1 - cl[d].r0 + 1;
+                    if (d == 2) {
+                        // Level L - 2: the tighter bound for the last two levels.
+                        const int cnt = (cl[2].r1 - cl[2].r0 + 1) * (cl[2].c1 - cl[2].c0 + 1);
+                        float mx = -INFINITY;
+                        for (int e = lane; e < cnt; e += 32) mx = fmaxf(mx, dst[e]);
+                        mx = warp_max(mx);
+                        if (mx + slack(2) < bv) {
+                            pruned = true;
+                            break;
                         }
                     }
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) {
-                        const float m2 = __shfl_xor_sync(kFull, m, o);
-                        const int s2 = __shfl_xor_sync(kFull, sel, o);
-                        if (m2 > m || (m2 == m && s2 < sel)) {
-                            m = m2;
-                            sel = s2;
+                }
+                if (pruned) continue;
+                // The final level: vertical pass, then each sample into the running best.
+                {
+                    const int n = 5 << (L - 1);
+                    const ConeLevel& dl = cl[0];
+                    float* tmp = CB + toff[0];
+                    const int r = lane & 15, cpar = lane >> 4;
+                    const int scols = sreg.c1 - sreg.c0 + 1;
+                    {
+                        int m2, c2, q2;
+                        const int nt = taps(dl.r0 + r, n, m2, c2, q2);
+                        m2 -= sreg.r0;
+                        c2 -= sreg.r0;
+                        q2 -= sreg.r0;
+                        for (int cc = cpar; cc < scols; cc += 2) {
+                            const float* col = src + cc * lds;
+                            tmp[r + cc * kFB] = pyr_sample(nt, col[m2], col[c2], col[q2]);
                         }
                     }
-                    if (lane == 0) {
-                        // Stop once nothing left can reach the maximum found so far.
-                        const bool go = m != -INFINITY && sel < nblk && !(m < s_best);
-                        s_sel = go ? sel : -1;
-                        if (go) sbound[sel] = -INFINITY;
+                    __syncwarp();
+                    float lv = -INFINITY;
+                    int li = INT_MAX;
+                    for (int cc = cpar; cc < kFB; cc += 2) {
+                        int m2, c2, q2;
+                        const int col = dl.c0 + cc;
+                        const int nt = taps(col, n, m2, c2, q2);
+                        const float v = pyr_sample(nt, tmp[r + (m2 - sreg.c0) * kFB],
+                                                   tmp[r + (c2 - sreg.c0) * kFB],
+                                                   tmp[r + (q2 - sreg.c0) * kFB]);
+                        best_update(v, (dl.r0 + r) * nfinal + col, lv, li);
                     }
+                    warp_best(lv, li);
+                    best_update(lv, li, bv, bi);
+                    __syncwarp();
                 }
-                __syncthreads();
-                const int blk = s_sel;
-                if (blk < 0) break;
-                const int qi = blk % nqb, cj = blk / nqb;
-                const int q0 = qi * kQB, q1 = min(q0 + kQB, N1);
-                const int c0 = cj * kCB, c1 = min(c0 + kCB, N2);
-                const int pr0 = max(q0 - 1, 0), pr1 = min(q1, N1 - 1);
-                const int pc0 = max(c0 / 2 - 1, 0), pc1 = min((c1 - 1) / 2 + 1, N1 - 1);
-                const int sc0 = max(pc0 / 2 - 1, 0), sc1 = min(pc1 / 2 + 1, n - 1);
-                const int nq = pr1 - pr0 + 1, nsc = sc1 - sc0 + 1, npc = pc1 - pc0 + 1;
-                const int np = 2 * (q1 - q0), ncl = c1 - c0;
-                // Penultimate rows pr0..pr1: vertical taps over the materialised level.
-                for (int e = tid; e < nq * TAS; e += bd) {
-                    const int qq = e / TAS, jj = e - qq * TAS;
-                    if (jj < nsc) {
-                        int m, c, q;
-                        const int nt = taps(pr0 + qq, n, m, c, q);
-                        const float* col = cur + (sc0 + jj) * n;
-                        TA[qq * TAS + jj] = pyr_sample(nt, col[m], col[c], col[q]);
-                    }
-                }
-                __syncthreads();
-                // Horizontal: the penultimate samples.
-                for (int e = tid; e < nq * RBS; e += bd) {
-                    const int qq = e / RBS, cc = e - qq * RBS;
-                    if (cc < npc) {
-                        int m, c, q;
-                        const int nt = taps(pc0 + cc, n, m, c, q);
-                        const float* row = TA + qq * TAS - sc0;
-                        RB[qq * RBS + cc] = pyr_sample(nt, row[m], row[c], row[q]);
-                    }
-                }
-                __syncthreads();
-                // Final rows 2q0 .. 2q1-1: vertical taps over the penultimate rows.
-                for (int e = tid; e < np * RBS; e += bd) {
-                    const int pp = e / RBS, cc = e - pp * RBS;
-                    if (cc < npc) {
-                        int m, c, q;
-                        const int nt = taps(2 * q0 + pp, N1, m, c, q);
-                        TB[pp * RBS + cc] = pyr_sample(nt, RB[(m - pr0) * RBS + cc],
-                                                       RB[(c - pr0) * RBS + cc],
-                                                       RB[(q - pr0) * RBS + cc]);
-                    }
-                }
-                __syncthreads();
-                // Final samples, reduced to the row-major first maximum.
-                for (int e = tid; e < np * kCB; e += bd) {
-                    const int pp = e / kCB, cl = e - pp * kCB;
-                    if (cl < ncl) {
-                        int m, c, q;
-                        const int c4 = c0 + cl;
-                        const int nt = taps(c4, N1, m, c, q);
-                        const float* row = TB + pp * RBS - pc0;
-                        best_update(pyr_sample(nt, row[m], row[c], row[q]),
-                                    (2 * q0 + pp) * N2 + c4, bv, bi);
-                    }
-                }
-                block_best(bv, bi, rv, ri);
-                if (tid == 0) s_best = bv;
             }
+            v0 = NAN;
         }
-        if (tid == 0) {
+        if (lane == 0) {
             int si = 0, sj = 0;
             float v = bv;
             if (bi != INT_MAX && bv != -INFINITY) {
                 si = bi / nfinal;
                 sj = bi - si * nfinal;
             } else {
-                v = L <= 2 ? cur[0] : NAN;  // nothing above -Inf: the reference reports (1,1)
+                v = v0;  // nothing above -Inf: the reference reports (1,1)
             }
             if (A.point) {
                 const int64_t k = A.point[item];
@@ -1331,6 +1371,7 @@ __global__ void __launch_bounds__(kRefineThreads) k_refine(const RefineArgs A) {
                 A.oval[item] = v;
             }
         }
+        __syncwarp();
     }
 }
 
@@ -1458,30 +1499,27 @@ int ilog2_exact(int up) {
 }
 
 struct RefinePlan {
-    int levels, nmat;
-    unsigned off_B, off_T, off_P, off_C;
+    int levels, warp_floats;
     size_t smem;
 };
 
+// Shared floats per warp of k_refine: patch, levels 1 and 2, then either the level-3
+// materialisation (up <= 8) or the block bounds and cone buffers.
 RefinePlan plan_refine(int up) {
     RefinePlan R{};
     R.levels = ilog2_exact(up);
     const int L = R.levels;
-    const int nm = L <= 2 ? 5 << L : 5 << (L - 2);
-    R.nmat = nm;
-    const size_t a = static_cast<size_t>(nm) * nm;
-    const size_t b = static_cast<size_t>(nm / 2) * (nm / 2);
-    const size_t t = static_cast<size_t>(nm) * (nm / 2);
-    size_t blocks = 0;
-    if (L > 2)
-        blocks = static_cast<size_t>(kQB + 2) * (kCB / 4 + 4) + static_cast<size_t>(kQB + 2) * (kCB / 2 + 2) +
-                 static_cast<size_t>(2 * kQB) * (kCB / 2 + 2);
-    R.off_B = static_cast<unsigned>(a);
-    R.off_T = static_cast<unsigned>(a + b);
-    R.off_C = static_cast<unsigned>(a);  // the block buffers reuse B and T once materialised
-    const size_t tail = std::max(b + t, blocks);
-    R.off_P = static_cast<unsigned>(a + tail);
-    R.smem = (a + tail + 32) * sizeof(float);
+    int wk;
+    if (L <= 3) {
+        wk = 800 + 1600;
+    } else {
+        const int nb = (5 << L) / kFB;
+        const int cap[7] = {16, 10, 7, 6, 5, 5, 5};
+        wk = nb * nb;
+        for (int d = 0; d <= L - 3; ++d) wk += cap[d] * cap[d] + cap[d] * cap[d + 1];
+    }
+    R.warp_floats = 32 + 100 + 400 + wk;
+    R.smem = static_cast<size_t>(kRefineWarps) * R.warp_floats * sizeof(float);
     return R;
 }
 
@@ -1870,17 +1908,14 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
     B.pts = pts;
     B.out = out;
     B.levels = R.levels;
-    B.nmat = R.nmat;
-    B.off_B = R.off_B;
-    B.off_T = R.off_T;
-    B.off_P = R.off_P;
-    B.off_C = R.off_C;
+    B.warp_floats = R.warp_floats;
     e = cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(R.smem));
     if (e != cudaSuccess) return e;
+    const int64_t rper_sm = std::max<int64_t>(1, std::min<int64_t>(4, (200 * 1024) / R.smem));
     const int rgrid = static_cast<int>(std::max<int64_t>(
-        1, std::min<int64_t>(pts.n, static_cast<int64_t>(num_sms) * 4)));
-    k_refine<<<rgrid, kRefineThreads, R.smem, stream>>>(B);
+        1, std::min<int64_t>((pts.n + kRefineWarps - 1) / kRefineWarps, num_sms * rper_sm)));
+    k_refine<<<rgrid, kRefineWarps * 32, R.smem, stream>>>(B);
     e = cudaGetLastError();
     T.launches += 1;
     if (T.enabled) {
@@ -1917,17 +1952,14 @@ cudaError_t launch_refine_patches(const float* patches, int64_t count, int up, i
     B.ocol = col;
     B.oval = value;
     B.levels = R.levels;
-    B.nmat = R.nmat;
-    B.off_B = R.off_B;
-    B.off_T = R.off_T;
-    B.off_P = R.off_P;
-    B.off_C = R.off_C;
+    B.warp_floats = R.warp_floats;
     cudaError_t e = cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(R.smem));
     if (e != cudaSuccess) return e;
+    const int64_t per_sm = std::max<int64_t>(1, std::min<int64_t>(4, (200 * 1024) / R.smem));
     const int grid = static_cast<int>(std::max<int64_t>(
-        1, std::min<int64_t>(count, static_cast<int64_t>(num_sms) * 4)));
-    k_refine<<<grid, kRefineThreads, R.smem, stream>>>(B);
+        1, std::min<int64_t>((count + kRefineWarps - 1) / kRefineWarps, num_sms * per_sm)));
+    k_refine<<<grid, kRefineWarps * 32, R.smem, stream>>>(B);
     return cudaGetLastError();
 }
 
