@@ -17,7 +17,7 @@ CSRC = PKG / "csrc"
 INCLUDE = ROOT / "include"
 LIB = PKG / "libautorift_gpu.so"
 
-SOURCES = ["ar_track.cu", "ar_corr_tc.cu", "ar_prepare.cu", "ar_multichip.cu", "ar_capi.cu"]
+SOURCES = ["ar_track.cu", "ar_corr_tc.cu", "ar_prepare.cu", "ar_multichip.cu", "ar_serve.cu", "ar_capi.cu"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -34,6 +34,11 @@ struct ar_ctx {
     // Stream-ordered pool for pair images and per-call scratch: freed blocks stay with the
     // context and are reused without a device-wide synchronisation.
     cudaMemPool_t pool = nullptr;
+    // The request loop, started by the first ar_submit.
+    std::mutex serve_mu;
+    ar::ServeEngine* serve = nullptr;
+    int serve_slots = 4;
+    size_t serve_budget = 0;
 };
 
 struct ar_pair {
@@ -270,6 +275,11 @@ int ar_ctx_create(int device, ar_ctx** out) {
 
 int ar_ctx_destroy(ar_ctx* c) {
     if (!c) return AR_ERR_ARG;
+    {
+        std::lock_guard<std::mutex> lk(c->serve_mu);
+        ar::serve_destroy(c->serve);  // completes every queued request first
+        c->serve = nullptr;
+    }
     {
         DeviceGuard g(c->device);
         std::lock_guard<std::mutex> lk(c->mu);
@@ -822,6 +832,7 @@ int ar_tc_selftest(ar_ctx* c, const uint8_t* a_img, int a_bytes, const uint8_t* 
     if (a_bytes <= 0 || b_bytes <= 0 || a_bytes > 96 * 1024 || b_bytes > 96 * 1024)
         return fail(c, AR_ERR_SIZE, "operand images must be 1..96 KiB");
     const int N = params[9], nk = params[10], dstep = params[11];
+    // params[12]: 0 reads the accumulator lane by lane (32x32b), 1 with the 16x256b pattern.
     if (N < 8 || N > 256 || nk < 1 || nk > 64 || dstep < 0 || dstep > 512)
         return fail(c, AR_ERR_ARG, "invalid N, nk or dstep");
     const int dcols = N + (nk - 1) * dstep;
@@ -861,8 +872,83 @@ int ar_ctx_set_option(ar_ctx* c, int option, int value) {
     std::lock_guard<std::mutex> lk(c->mu);
     switch (option) {
         case AR_OPT_TENSOR_CORES: c->scratch.tensor_cores = value != 0; return AR_OK;
+        case AR_OPT_SERVE_SLOTS:
+        case AR_OPT_SERVE_MEMORY_MB: {
+            std::lock_guard<std::mutex> sk(c->serve_mu);
+            if (c->serve) return fail(c, AR_ERR_ARG, "the request loop has already started");
+            if (option == AR_OPT_SERVE_SLOTS) {
+                if (value < 1 || value > 64) return fail(c, AR_ERR_ARG, "slots must be in 1..64");
+                c->serve_slots = value;
+            } else {
+                if (value < 0) return fail(c, AR_ERR_ARG, "the memory budget must be >= 0");
+                c->serve_budget = static_cast<size_t>(value) << 20;
+            }
+            return AR_OK;
+        }
         default: return fail(c, AR_ERR_ARG, "unknown option");
     }
+}
+
+int ar_submit(ar_ctx* c, const ar_request* req, ar_ticket* ticket) {
+    if (!c || !req || !ticket) return fail(c, AR_ERR_ARG, "null argument");
+    ar::ServeEngine* E;
+    {
+        std::lock_guard<std::mutex> lk(c->serve_mu);
+        if (!c->serve) {
+            std::string err;
+            c->serve = ar::serve_create(c->device, c->serve_slots, c->serve_budget, &err);
+            if (!c->serve) return fail(c, AR_ERR_CUDA, "ar_submit: " + err);
+        }
+        E = c->serve;
+    }
+    std::string err;
+    int64_t t = 0;
+    const int rc = ar::serve_submit(E, req, &t, &err);
+    if (rc != AR_OK) return fail(c, rc, "ar_submit: " + err);
+    *ticket = t;
+    return AR_OK;
+}
+
+namespace {
+ar::ServeEngine* engine_of(ar_ctx* c) {
+    std::lock_guard<std::mutex> lk(c->serve_mu);
+    return c->serve;
+}
+}  // namespace
+
+int ar_poll(ar_ctx* c, ar_ticket ticket, int* done) {
+    if (!c || !done) return fail(c, AR_ERR_ARG, "null argument");
+    ar::ServeEngine* E = engine_of(c);
+    if (!E) return fail(c, AR_ERR_ARG, "no request has been submitted");
+    std::string err;
+    const int rc = ar::serve_poll(E, ticket, done, &err);
+    return rc == AR_OK ? AR_OK : fail(c, rc, err);
+}
+
+int ar_wait(ar_ctx* c, ar_ticket ticket, int timeout_ms) {
+    if (!c) return AR_ERR_ARG;
+    ar::ServeEngine* E = engine_of(c);
+    if (!E) return fail(c, AR_ERR_ARG, "no request has been submitted");
+    std::string err;
+    const int rc = ar::serve_wait(E, ticket, timeout_ms, &err);
+    return rc == AR_OK ? AR_OK : fail(c, rc, err);
+}
+
+int ar_request_times(ar_ctx* c, ar_ticket ticket, double* queued_ms, double* run_ms) {
+    if (!c) return AR_ERR_ARG;
+    ar::ServeEngine* E = engine_of(c);
+    if (!E) return fail(c, AR_ERR_ARG, "no request has been submitted");
+    const int rc = ar::serve_times(E, ticket, queued_ms, run_ms);
+    return rc == AR_OK ? AR_OK : fail(c, rc, "unknown or pending ticket");
+}
+
+int ar_release(ar_ctx* c, ar_ticket ticket) {
+    if (!c) return AR_ERR_ARG;
+    ar::ServeEngine* E = engine_of(c);
+    if (!E) return fail(c, AR_ERR_ARG, "no request has been submitted");
+    std::string err;
+    const int rc = ar::serve_release(E, ticket, &err);
+    return rc == AR_OK ? AR_OK : fail(c, rc, err);
 }
 
 int ar_ctx_stream(ar_ctx* c, void** stream) {

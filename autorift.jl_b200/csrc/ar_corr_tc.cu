@@ -19,7 +19,7 @@ struct ProbeArgs {
     int b_base;
     int a_off, a_lbo, a_sbo, a_kstep;
     int b_off, b_lbo, b_sbo, b_kstep;
-    int M, N, nk, ncols, dstep, dcols;
+    int M, N, nk, ncols, dstep, dcols, mode;
     int32_t* d_out;            // 128 lanes x dcols columns
     int* status;               // 0 ok, 1 the MMA did not complete in time
 };
@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(128, 1) k_tc_probe(const ProbeArgs P) {
     const bool ok = tc::mbar_wait(&mbar, 0, 1u << 24);
     if (!ok && tid == 0) *P.status = 1;
     tc::fence_after_sync();
-    if (ok) {
+    if (ok && P.mode == 0) {
         for (int c = 0; c < P.dcols; c += 16) {
             uint32_t r[16];
             tc::tmem_ld16(taddr + (static_cast<uint32_t>(32 * warp) << 16) + c, r);
@@ -79,6 +79,15 @@ __global__ void __launch_bounds__(128, 1) k_tc_probe(const ProbeArgs P) {
             for (int k = 0; k < 16; ++k)
                 P.d_out[(32 * warp + lane) * P.dcols + c + k] = static_cast<int32_t>(r[k]);
         }
+    } else if (ok) {
+        // The 16x256b pattern: each warp reads the first 16 lanes of its quarter, columns
+        // [0, 32); thread t's register k goes to d_out[(32 warp + t) * dcols + k].
+        uint32_t r[16];
+        tc::tmem_ld16dp(taddr + (static_cast<uint32_t>(32 * warp) << 16), r);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+            P.d_out[(32 * warp + lane) * P.dcols + k] = static_cast<int32_t>(r[k]);
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -115,6 +124,7 @@ cudaError_t tc_probe(const uint8_t* a_img, int a_bytes, const uint8_t* b_img, in
     P.N = params[9];
     P.nk = params[10];
     P.dstep = params[11];
+    P.mode = params[12];
     auto bad = [&](const char* m) {
         if (err) *err = m;
         return cudaErrorInvalidValue;
@@ -133,6 +143,8 @@ cudaError_t tc_probe(const uint8_t* a_img, int a_bytes, const uint8_t* b_img, in
     if (P.dstep < 0 || (P.dstep & 15)) return bad("dstep must be a non-negative multiple of 16");
     P.dcols = P.N + (P.nk - 1) * P.dstep;
     if (P.dcols > 512) return bad("the accumulator columns exceed Tensor Memory");
+    if (P.mode != 0 && P.mode != 1) return bad("mode must be 0 or 1");
+    if (P.mode == 1 && P.dcols < 32) return bad("mode 1 reads 32 columns");
     P.b_base = (a_bytes + 1023) & ~1023;
     int ncols = 32;
     while (ncols < P.dcols) ncols <<= 1;

@@ -151,6 +151,16 @@ struct MultichipJob {
 };
 size_t multichip_arena_bytes(int64_t gr, int64_t gc);
 
+// The request loop (ar_serve.cu).
+struct ServeEngine;
+ServeEngine* serve_create(int device, int slots, size_t budget, std::string* err);
+void serve_destroy(ServeEngine* engine);
+int serve_submit(ServeEngine* engine, const ar_request* req, int64_t* ticket, std::string* err);
+int serve_poll(ServeEngine* engine, int64_t ticket, int* done, std::string* err);
+int serve_wait(ServeEngine* engine, int64_t ticket, int timeout_ms, std::string* err);
+int serve_times(ServeEngine* engine, int64_t ticket, double* queued_ms, double* run_ms);
+int serve_release(ServeEngine* engine, int64_t ticket, std::string* err);
+
 // One tensor-core product of two shared-memory operand images (the layout self-test):
 // params = {a_off, a_lbo, a_sbo, a_kstep, b_off, b_lbo, b_sbo, b_kstep, M, N, nk, dstep}.
 cudaError_t tc_probe(const uint8_t* a_img, int a_bytes, const uint8_t* b_img, int b_bytes,

@@ -96,6 +96,20 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
         : "r"(taddr)
         : "memory");
 }
+// 16 lanes x 32 columns (four 16x256b patterns): thread t gets lanes L = t / 4 and L + 8 of
+// the warp's lane base, columns 8 k + 2 (t % 4) and 8 k + 2 (t % 4) + 1 for k = 0..3, in
+// registers r[4 k + 0] (L, even column), r[4 k + 1] (L, odd), r[4 k + 2] (L + 8, even),
+// r[4 k + 3] (L + 8, odd). This is the M = 64 accumulator's half of a lane quarter.
+__device__ __forceinline__ void tmem_ld16dp(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.16x256b.x4.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+}
 // 32 lanes x 16 consecutive 32-bit columns from registers (the layout of tmem_ld16).
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
     asm volatile(

@@ -662,7 +662,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
     uint32_t phase = 0;
     bool failed = false;
     if (tid < 4) s_isum[tid >> 1][tid & 1] = 0ull;
+    for (int e = tid; e < A.CWM * A.PC; e += bd) s_P[e] = 0;
     int iter = 0;
+    int dirty_ch = 0;
 
     for (int64_t k = blockIdx.x; k < A.pts.n; k += gridDim.x, ++iter) {
         tc::fence_before_sync();
@@ -698,25 +700,41 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         const bool pow2 = (nnl & (nnl - 1)) == 0 && nnl <= 4096;
 
         // The chip as zero-padded byte columns, _any_valid over it (src/track.jl:416-421) and,
-        // for power-of-two areas, its exact integer sums; a warp per chip column.
+        // for power-of-two areas, its exact integer sums: warps over chip columns, lanes over
+        // rows, all loads of a lane issued before their uses. Rows a taller chip left behind
+        // are cleared (the padding itself is never written).
         int any = 0;
         unsigned long long isum = 0ull, isq = 0ull;
-        for (int b = warp; b < cw; b += nwarps) {
-            const int64_t c = chip_c + b;
-            const bool cin = c >= 0 && c < A.ncols;
-            for (int o = lane; o < A.PC; o += 32) {
-                const int a = o - kPadL;
-                uint32_t v = 0;
-                if (a >= 0 && a < ch) {
-                    const int64_t r = chip_r + a;
-                    if (cin && r >= 0 && r < A.nrows) {
-                        v = A.sec[r + c * A.nrows];
-                        any |= A.valid[r + c * A.nrows];
-                    }
-                    isum += v;
-                    isq += v * v;
+        // Invariant: chip rows at or beyond `dirty_ch` are zero in every column.
+        if (ch < dirty_ch)
+            for (int b = warp; b < A.CWM; b += nwarps)
+                for (int a = ch + lane; a < dirty_ch; a += 32) s_P[b * A.PC + kPadL + a] = 0;
+        dirty_ch = ch;
+        for (int a0 = 0; a0 < ch; a0 += 32) {
+            const int a = a0 + lane;
+            const int64_t r = chip_r + a;
+            const bool rin = a < ch && r >= 0 && r < A.nrows;
+            constexpr int kU = 4;
+            for (int b0 = warp; b0 < cw; b0 += kU * nwarps) {
+                uint32_t v[kU], m[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int b = b0 + u * nwarps;
+                    const int64_t c = chip_c + b;
+                    const bool in = rin && b < cw && c >= 0 && c < A.ncols;
+                    v[u] = in ? A.sec[r + c * A.nrows] : 0u;
+                    m[u] = in ? A.valid[r + c * A.nrows] : 0u;
                 }
-                s_P[b * A.PC + o] = static_cast<uint8_t>(v);
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int b = b0 + u * nwarps;
+                    if (a < ch && b < cw) {
+                        s_P[b * A.PC + kPadL + a] = static_cast<uint8_t>(v[u]);
+                        any |= m[u];
+                        isum += v[u];
+                        isq += v[u] * v[u];
+                    }
+                }
             }
         }
         if (pow2) {
@@ -809,10 +827,12 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         // exact integers: V[i][x] sums ch rows down column x, S[j][i] sums cw columns of V.
         // They run while the tensor core works on the first chunk, or, when the chip operand
         // comes in several chunks that reuse their space, before it.
+        // Warps 0-6 only (named barrier 1): warp 7 issues the products meanwhile.
         auto box_sums = [&]() {
+            constexpr int kBT = kTcThreads - 32;
             uint32_t* s_V2 = s_V1 + A.NRM * XW;
             const int nseg = (nr + 15) >> 4;
-            for (int task = tid; task < XW * nseg; task += bd) {
+            for (int task = tid; task < XW * nseg; task += kBT) {
                 const int x = task % XW, seg = task / XW;
                 const int i0 = seg << 4, i1 = min(i0 + 16, nr);
                 const uint8_t* col = s_T + static_cast<int>(delta) * A.XT + x;
@@ -832,9 +852,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                     }
                 }
             }
-            __syncthreads();
+            asm volatile("bar.sync 1, %0;" ::"r"(kBT) : "memory");
             const int jseg = (nc + 15) >> 4;
-            for (int task = tid; task < nr * jseg; task += bd) {
+            for (int task = tid; task < nr * jseg; task += kBT) {
                 const int i = task % nr, seg = task / nr;
                 const int j0 = seg << 4, j1 = min(j0 + 16, nc);
                 uint32_t g1 = 0, g2 = 0;
@@ -853,7 +873,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             }
         };
         if (A.big) {
-            box_sums();
+            if (warp < 7) box_sums();
             __syncthreads();  // the chip chunks overwrite s_T and s_V
         }
 
@@ -894,7 +914,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             tc::fence_proxy_async_smem();
             tc::fence_before_sync();
             __syncthreads();
-            if (tid == 0) {
+            if (tid == kTcThreads - 32) {
                 tc::fence_after_sync();
                 const uint32_t sW = tc::smem_u32(s_W), sE = tc::smem_u32(s_E);
                 const uint32_t idesc = tc::idesc_u8_s32(64, A.NB);
@@ -906,7 +926,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                     }
                 tc::mma_commit(&s_mbar);
             }
-            if (cc == 0 && !A.big) box_sums();
+            if (cc == 0 && !A.big && warp < 7) box_sums();
         }
         if (ok) {
             // Wait for the last chunk's products (bounded; every thread polls the same phase).
@@ -920,41 +940,37 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         }
         tc::fence_after_sync();
 
-        // Pass 1: numerators out of Tensor Memory, estimates and bounds, the largest estimate.
+        // Pass 1: numerators out of Tensor Memory, estimates and bounds, the largest lower bound.
         // Surface column j is accumulator row j (lane (j % 16) + 32 (j / 16) of the M = 64
         // layout); surface row i is accumulator column i + NB - 16. Warp w reads its quarter's
-        // first 16 lanes, columns from 32 (w / 4) in steps of 64.
+        // 16 lanes (16x256b: thread t gets rows 16 q + t/4 and + 8, columns 2 (t % 4) + {0, 1}
+        // + 8 k), columns from 32 (w / 4) in steps of 64.
         const float kk = __double2float_rn(
             A.measure == AR_NCC ? __drcp_rn(__dmul_rn(cnorm, nn))
                                 : __drcp_rn(__dmul_rn(cnorm, __dsqrt_rn(nn))));
         const float nnf = static_cast<float>(nnl);
         const float csf = static_cast<float>(csum_d);
         const int quarter = warp & 3, half = warp >> 2;
-        const int j = 16 * quarter + (lane & 15);
-        const bool jv = lane < 16 && j < nc;
         const uint32_t col0 = static_cast<uint32_t>(A.NB - 16);
         float lmax = -INFINITY;
         for (int i0 = 32 * half; i0 < nr; i0 += 64) {
-            for (int c = 0; c < 32; c += 16) {
-                const int ii = i0 + c;
-                if (ii >= nr) break;  // warp-uniform
-                uint32_t r[16];
-                tc::tmem_ld16(taddr + (static_cast<uint32_t>(32 * quarter) << 16) + col0 +
-                                  static_cast<uint32_t>(ii), r);
-                tc::tmem_wait_ld();
+            uint32_t r[16];
+            tc::tmem_ld16dp(taddr + (static_cast<uint32_t>(32 * quarter) << 16) + col0 +
+                                static_cast<uint32_t>(i0), r);
+            tc::tmem_wait_ld();
 #pragma unroll
-                for (int m = 0; m < 16; ++m) {
-                    const int i = ii + m;
-                    if (jv && i < nr) {
-                        const int o = j * A.NRS + i;
-                        float bnd;
-                        const float est = tc_estimate(r[m], s_S1[o], s_S2[o], nnf, csf, kk,
-                                                      A.measure, &bnd);
-                        s_num[o] = r[m];
-                        s_est[o] = est;
-                        s_est[o + A.NCM * A.NRS] = bnd;
-                        lmax = fmaxf(lmax, est - bnd);
-                    }
+            for (int v = 0; v < 16; ++v) {
+                const int j = 16 * quarter + (lane >> 2) + ((v & 2) ? 8 : 0);
+                const int i = i0 + 8 * (v >> 2) + 2 * (lane & 3) + (v & 1);
+                if (j < nc && i < nr) {
+                    const int o = j * A.NRS + i;
+                    float bnd;
+                    const float est = tc_estimate(r[v], s_S1[o], s_S2[o], nnf, csf, kk,
+                                                  A.measure, &bnd);
+                    s_num[o] = r[v];
+                    s_est[o] = est;
+                    s_est[o + A.NCM * A.NRS] = bnd;
+                    lmax = fmaxf(lmax, est - bnd);
                 }
             }
         }

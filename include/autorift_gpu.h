@@ -191,23 +191,73 @@ int ar_multichip_device(ar_ctx* ctx, const ar_pair* pair, const ar_points* grid_
  * Diagnostic: one tensor-core product (tcgen05.mma kind::i8, unsigned 8-bit operands, 32-bit
  * integer accumulator) of two operand images placed in shared memory as given, read through
  * SWIZZLE_NONE K-major descriptors. params = {a_off, a_lbo, a_sbo, a_kstep, b_off, b_lbo,
- * b_sbo, b_kstep, M, N, nk, dstep}: byte offsets and strides (multiples of 16), M in {64, 128},
+ * b_sbo, b_kstep, M, N, nk, dstep, mode}: byte offsets and strides (multiples of 16), M in {64, 128},
  * N, and nk K-steps of 32 accumulated, step s reading at offset + s * kstep and, when dstep > 0,
  * adding into accumulator columns [s * dstep, s * dstep + N) of a cleared accumulator. `d_out`
  * receives the accumulator as 128 Tensor Memory lanes x (N + (nk - 1) * dstep) columns (int32,
- * lane-major). Descriptors that would read outside an image are rejected. It validates on a
- * device the operand layouts the correlation kernel builds; no reference counterpart.
+ * lane-major) for mode 0; for mode 1, row (32 w + t) holds the 16 registers thread t of warp w
+ * reads with the 16x256b.x4 pattern from its quarter's first 16 lanes, columns 0..31.
+ * Descriptors that would read outside an image are rejected. It validates on a device the
+ * operand and accumulator layouts the correlation kernel uses; no reference counterpart.
  */
 int ar_tc_selftest(ar_ctx* ctx, const uint8_t* a_img, int a_bytes, const uint8_t* b_img,
                    int b_bytes, const int* params, int32_t* d_out);
 
 /*
+ * Serving: whole autorift() requests (src/api.jl:210-274 -- prepare both images, then the
+ * multi-chip-size search over `grid`) queued on a context and run with continuous batching.
+ * The context starts its request loop on the first ar_submit: AR_OPT_SERVE_SLOTS slots (each
+ * a stream with its own scratch and memory, driven by its own host thread; default 4) take
+ * requests in submission order as soon as the device memory the running requests hold (an
+ * estimate of each request's footprint) leaves room within AR_OPT_SERVE_MEMORY_MB (default:
+ * three quarters of the memory free when serving starts); a request larger than the budget
+ * runs alone. Requests that arrive while others run overlap with them on the device; each
+ * result is bit-identical to the same request run alone (ar_pair_upload, ar_prepare,
+ * ar_multichip). Every array a request names -- images, masks (may be NULL), the grid's
+ * fields and the outputs (grid_rows * grid_cols each) -- must stay valid until the request
+ * has completed. No reference counterpart (the reference serves one pair per call).
+ */
+typedef struct {
+    const void* reference;
+    const void* secondary;
+    const uint8_t* reference_valid;
+    const uint8_t* secondary_valid;
+    int64_t nrows, ncols;
+    int dtype;
+    ar_prepare_opts prepare;
+    ar_multichip_params params;
+    const ar_points* grid;
+    int64_t grid_rows, grid_cols;
+    float* dx;
+    float* dy;
+    float* correlation;
+    uint16_t* chip_size;
+    uint8_t* interpolated;
+} ar_request;
+
+typedef int64_t ar_ticket;
+
+/* Queue a request; `ticket` identifies it. Thread-safe. */
+int ar_submit(ar_ctx* ctx, const ar_request* request, ar_ticket* ticket);
+/* Non-blocking: *done = 0 while pending; once complete *done = 1 and the request's status is
+ * returned (its message through ar_last_error). */
+int ar_poll(ar_ctx* ctx, ar_ticket ticket, int* done);
+/* Block until the request completes (timeout_ms < 0: no limit) and return its status, or
+ * AR_ERR_TIMEOUT if it has not completed within timeout_ms. */
+int ar_wait(ar_ctx* ctx, ar_ticket ticket, int timeout_ms);
+/* Milliseconds a completed request spent queued and running. */
+int ar_request_times(ar_ctx* ctx, ar_ticket ticket, double* queued_ms, double* run_ms);
+/* Forget a completed request (its ticket becomes unknown). */
+int ar_release(ar_ctx* ctx, ar_ticket ticket);
+
+/*
  * Context options. AR_OPT_TENSOR_CORES (default 1): UInt8 passes whose geometry fits (surface
  * at most 64 columns and 256 rows) compute the correlation numerator on the tensor cores
  * (exact 8-bit products, bit-identical results); 0 keeps every pass on the CUDA-core kernel.
- * No reference counterpart.
+ * AR_OPT_SERVE_SLOTS and AR_OPT_SERVE_MEMORY_MB configure the request loop (see ar_submit);
+ * they must be set before the first ar_submit. No reference counterpart.
  */
-enum { AR_OPT_TENSOR_CORES = 1 };
+enum { AR_OPT_TENSOR_CORES = 1, AR_OPT_SERVE_SLOTS = 2, AR_OPT_SERVE_MEMORY_MB = 3 };
 int ar_ctx_set_option(ar_ctx* ctx, int option, int value);
 
 /* The context's own CUDA stream (cudaStream_t), on which calls without a stream argument run;

@@ -17,10 +17,10 @@ def run(ar, a_img, b_img, params):
     ctx = ar._lib.default_context()
     a_img = np.ascontiguousarray(a_img, np.uint8)
     b_img = np.ascontiguousarray(b_img, np.uint8)
-    params = list(params) + [0] * (12 - len(params))
+    params = list(params) + [0] * (13 - len(params))
     N, nk, dstep = params[9], params[10], params[11]
     out = np.zeros((128, N + (nk - 1) * dstep), np.int32)
-    prm = (ctypes.c_int * 12)(*params)
+    prm = (ctypes.c_int * 13)(*params)
     ctx.check(ctx.lib.ar_tc_selftest(ctx.handle, a_img.ctypes.data, a_img.size, b_img.ctypes.data,
                                      b_img.size, prm, out.ctypes.data))
     return out
@@ -97,6 +97,24 @@ def test_column_offset_accumulation(ar, gpu_lib):
         want[:, st * dstep:st * dstep + N] += A.astype(np.int64) @ B.astype(np.int64).T
     D = run(ar, TA.reshape(-1), planes(B), [0, 16, 128, 32, 0, N * 16, 128, 0, M, N, nk, dstep])
     assert np.array_equal(lanes(D, M), want)
+
+
+def test_16x256b_read_pattern(ar, gpu_lib):
+    """The epilogue's accumulator read: thread t of warp w gets rows 16 w + t // 4 (+ 8) and
+    columns 8 k + 2 (t % 4) (+ 1) of the M = 64 accumulator, in registers 4 k + 0..3."""
+    rng = np.random.default_rng(8)
+    M, N = 64, 64
+    A = rng.integers(0, 256, (M, 32), dtype=np.uint8)
+    B = rng.integers(0, 256, (N, 32), dtype=np.uint8)
+    D = run(ar, planes(A), planes(B), [0, M * 16, 128, 0, 0, N * 16, 128, 0, M, N, 1, 0, 1])
+    want = A.astype(np.int64) @ B.astype(np.int64).T
+    for w in range(4):
+        for t in range(32):
+            for k in range(4):
+                for v in range(4):
+                    row = 16 * w + t // 4 + (8 if v >= 2 else 0)
+                    col = 8 * k + 2 * (t % 4) + (v & 1)
+                    assert D[32 * w + t, 4 * k + v] == want[row, col], (w, t, k, v)
 
 
 def test_out_of_image_descriptor_rejected(ar, gpu_lib):
