@@ -10,7 +10,7 @@ from .methods import (GardnerFilter, Highpass, NCC, NoOutlierFilter, NoPreproces
                       params, upsampling)
 from .points import (PointSet, gridpoints, gridpoints_xy, nsearchable, npoints, pointset,
                      sanitize)
-from .api import (multichip_params, Cache, MultichipResult, autorift, autorift_, build_grid, correlate_multichip,
+from .api import (Ticket, submit, multichip_params, Cache, MultichipResult, autorift, autorift_, build_grid, correlate_multichip,
                   init, reinit_)
 from .track import (DisplacementField, ImagePair, PreparedPair, correlate, displacement_field,
                     nmeasured, prepare, prepare_options, refine_patches, track)
@@ -22,5 +22,5 @@ __all__ = [
     "pointset", "sanitize", "DisplacementField", "ImagePair", "correlate", "displacement_field",
     "nmeasured", "refine_patches", "track", "PreparedPair", "prepare", "Cache",
     "MultichipResult", "autorift", "autorift_", "build_grid", "correlate_multichip", "init",
-    "reinit_", "prepare_options", "multichip_params",
+    "reinit_", "prepare_options", "multichip_params", "submit", "Ticket",
 ]

@@ -44,17 +44,28 @@ class ArMultichipParams(ctypes.Structure):
                 ("fill_window", _i32)]
 
 
-AR_PRE_NONE, AR_PRE_HIGHPASS, AR_PRE_WALLIS = 0, 1, 2
-AR_OPT_TENSOR_CORES = 1
-AR_QUANT_NONE, AR_QUANT_UINT8 = 0, 1
-
-
 class ArPoints(ctypes.Structure):
     """`ar_points`: the eight PointSet fields (src/points.jl:50-74) plus the count."""
 
     _fields_ = [("x", _p), ("y", _p), ("radius_x", _p), ("radius_y", _p),
                 ("dx_prior", _p), ("dy_prior", _p), ("chip_size_x", _p), ("chip_size_y", _p),
                 ("n", _i64)]
+
+
+class ArRequest(ctypes.Structure):
+    """`ar_request` (include/autorift_gpu.h): one autorift() request for the request loop."""
+
+    _fields_ = [("reference", _p), ("secondary", _p), ("reference_valid", _p),
+                ("secondary_valid", _p), ("nrows", _i64), ("ncols", _i64),
+                ("dtype", ctypes.c_int), ("prepare", ArPrepareOpts),
+                ("params", ArMultichipParams), ("grid", ctypes.POINTER(ArPoints)),
+                ("grid_rows", _i64), ("grid_cols", _i64), ("dx", _p), ("dy", _p),
+                ("correlation", _p), ("chip_size", _p), ("interpolated", _p)]
+
+
+AR_PRE_NONE, AR_PRE_HIGHPASS, AR_PRE_WALLIS = 0, 1, 2
+AR_OPT_TENSOR_CORES, AR_OPT_SERVE_SLOTS, AR_OPT_SERVE_MEMORY_MB = 1, 2, 3
+AR_QUANT_NONE, AR_QUANT_UINT8 = 0, 1
 
 
 SIGNATURES = {
@@ -80,6 +91,12 @@ SIGNATURES = {
                                    ctypes.POINTER(ArMultichipParams), _p, _p, _p, _p, _p, _p]),
     "ar_ctx_stream": (_i32, [_p, ctypes.POINTER(_p)]),
     "ar_ctx_set_option": (_i32, [_p, ctypes.c_int, ctypes.c_int]),
+    "ar_submit": (_i32, [_p, ctypes.POINTER(ArRequest), ctypes.POINTER(_i64)]),
+    "ar_poll": (_i32, [_p, _i64, ctypes.POINTER(ctypes.c_int)]),
+    "ar_wait": (_i32, [_p, _i64, ctypes.c_int]),
+    "ar_request_times": (_i32, [_p, _i64, ctypes.POINTER(ctypes.c_double),
+                                ctypes.POINTER(ctypes.c_double)]),
+    "ar_release": (_i32, [_p, _i64]),
     "ar_tc_selftest": (_i32, [_p, _p, ctypes.c_int, _p, ctypes.c_int, _p, _p]),
     "ar_ctx_set_timing": (_i32, [_p, _i32]),
     "ar_kernel_times": (_i32, [_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),

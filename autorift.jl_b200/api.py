@@ -15,7 +15,7 @@ from . import _lib
 from .methods import (GardnerFilter, NoOutlierFilter, Params, chip_sizes, params as make_params,
                       upsampling)
 from .points import PointSet, gridpoints
-from .track import ImagePair, PreparedPair, _measure_code, points_struct, prepare
+from .track import ImagePair, PreparedPair, _measure_code, points_struct, prepare, prepare_options
 
 
 @dataclass
@@ -174,3 +174,109 @@ def autorift(reference, secondary, grid: PointSet | None = None, *, reference_va
     if grid.ndim == 2:
         return correlate_multichip(prepared, grid, p, ctx)
     return track(prepared, grid, p, ctx=ctx)
+
+
+class Ticket:
+    """A queued autorift() request (ar_submit). Holds the request's host arrays until it has
+    completed; `wait` returns its MultichipResult."""
+
+    def __init__(self, ctx, ticket: int, keep, outs, shape):
+        self.ctx = ctx
+        self.ticket = int(ticket)
+        self._keep = keep
+        self._outs = outs
+        self._shape = shape
+        self._status = None
+
+    def done(self) -> bool:
+        """True once the request has completed (ar_poll)."""
+        if self._status is not None:
+            return True
+        flag = ctypes.c_int(0)
+        rc = self.ctx.lib.ar_poll(self.ctx.handle, self.ticket, ctypes.byref(flag))
+        if flag.value:
+            self._status = rc
+            return True
+        self.ctx.check(rc)
+        return False
+
+    def wait(self, timeout: float | None = None) -> MultichipResult:
+        """Block until the request completes (ar_wait) and return its result; raises
+        TimeoutError if it has not completed within `timeout` seconds, ArError if it failed."""
+        if self._status is None:
+            ms = -1 if timeout is None else max(0, int(round(timeout * 1000)))
+            rc = self.ctx.lib.ar_wait(self.ctx.handle, self.ticket, ms)
+            if rc == _lib.AR_ERR_TIMEOUT:
+                raise TimeoutError(f"request {self.ticket} has not completed in {timeout} s")
+            self._status = rc
+        if self._status != _lib.AR_OK:
+            self.ctx.check(self._status)
+        gr, gc = self._shape
+        shp = lambda a: a.reshape((gr, gc), order="F")
+        o = self._outs
+        return MultichipResult(shp(o[0]), shp(o[1]), shp(o[2]), shp(o[3]), shp(o[4]).astype(bool))
+
+    def times(self):
+        """(queued_ms, run_ms) of a completed request."""
+        q, r = ctypes.c_double(), ctypes.c_double()
+        self.ctx.check(self.ctx.lib.ar_request_times(self.ctx.handle, self.ticket, ctypes.byref(q),
+                                                     ctypes.byref(r)))
+        return q.value, r.value
+
+    def release(self):
+        if self._keep is not None and self.done():
+            self.ctx.lib.ar_release(self.ctx.handle, self.ticket)
+            self._keep = None
+
+    def __del__(self):
+        try:
+            if self._keep is not None:
+                if not self.done():
+                    self.ctx.lib.ar_wait(self.ctx.handle, self.ticket, -1)  # buffers in use
+                self.ctx.lib.ar_release(self.ctx.handle, self.ticket)
+        except Exception:
+            pass
+
+
+def submit(reference, secondary, grid: PointSet | None = None, *, reference_valid=None,
+           secondary_valid=None, ctx=None, **kw) -> Ticket:
+    """Queue `autorift(reference, secondary; kw...)` on the context's request loop (ar_submit)
+    and return at once; requests submitted together run concurrently on the device."""
+    from .track import DTYPES, _colmajor
+    p = make_params(**kw)
+    ctx = ctx or _lib.default_context()
+    ref = np.asarray(reference)
+    sec = np.asarray(secondary)
+    if ref.shape != sec.shape or ref.ndim != 2:
+        raise ValueError(f"reference is {ref.shape} but secondary is {sec.shape}")
+    if sec.dtype != ref.dtype:
+        sec = sec.astype(ref.dtype)
+    if ref.dtype not in DTYPES:
+        raise TypeError(f"element type {ref.dtype} is not supported by the GPU correlator")
+    grid = grid if grid is not None else build_grid(ref.shape, p)
+    if grid.ndim != 2:
+        raise ValueError("a request needs a gridded PointSet{2}")
+    gr, gc = grid.shape
+    n = gr * gc
+    arrays = [_colmajor(ref), _colmajor(sec)]
+    masks = []
+    for m, img in ((reference_valid, ref), (secondary_valid, sec)):
+        if m is None:
+            masks.append(None)
+        else:
+            m = np.asarray(m, dtype=bool)
+            if m.shape != img.shape:
+                raise ValueError(f"a mask is {m.shape} but the image is {img.shape}")
+            masks.append(_colmajor(m, np.uint8))
+    st, cols = points_struct(grid)
+    outs = [np.empty(n, np.float32) for _ in range(3)] + [np.empty(n, np.uint16),
+                                                           np.empty(n, np.uint8)]
+    req = _lib.ArRequest(
+        arrays[0].ctypes.data, arrays[1].ctypes.data,
+        masks[0].ctypes.data if masks[0] is not None else None,
+        masks[1].ctypes.data if masks[1] is not None else None,
+        ref.shape[0], ref.shape[1], DTYPES[ref.dtype], prepare_options(p), multichip_params(p),
+        ctypes.pointer(st), gr, gc, *(o.ctypes.data for o in outs))
+    t = _lib._i64()
+    ctx.check(ctx.lib.ar_submit(ctx.handle, ctypes.byref(req), ctypes.byref(t)))
+    return Ticket(ctx, t.value, (arrays, masks, st, cols, req), outs, (gr, gc))

@@ -106,6 +106,7 @@ def gaussian_bumps(shape, n_bumps: int, max_amp: float, widths=(300.0, 800.0), b
     the edge (tapered), peak amplitude up to `max_amp`."""
     rng = np.random.default_rng(seed)
     nr, nc = shape
+    border = min(border, int(0.2 * min(nr, nc)))  # small scenes keep a proportional border
     yy = np.arange(nr, dtype=np.float64)[:, None]
     xx = np.arange(nc, dtype=np.float64)[None, :]
     fx = np.zeros(shape)

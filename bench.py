@@ -183,6 +183,80 @@ def host_pipeline(O, ar, a, b, valid, p):
     return len(grid), time.perf_counter() - t
 
 
+def serving_requests(ar, rng, n_req, sizes, weights, base=None):
+    """A mixed request stream in the proportions of the serving configuration: image sides
+    `sizes` with relative frequencies `weights`, grid spacing from {8, 16, 32}, chip from
+    {16, 32, 64}, search radius uniform in [8, 48]. Scenes are generated once per side (host
+    arrays in the column-major layout a Julia caller holds)."""
+    scenes = {}
+    for n in sizes:
+        a, b, v = base if (base is not None and base[0].shape[0] == n) else scene(ar, n)
+        scenes[n] = (np.asfortranarray(a), np.asfortranarray(b), np.asfortranarray(v))
+    w = np.asarray(weights, float) / np.sum(weights)
+    reqs = []
+    for _ in range(n_req):
+        n = int(rng.choice(sizes, p=w))
+        kw = dict(grid_spacing=int(rng.choice([8, 16, 32])), chip_size=int(rng.choice([16, 32, 64])),
+                  search_radius=int(rng.integers(8, 49)), upsampling=UP)
+        reqs.append((n, kw))
+    return scenes, reqs
+
+
+def serving_measure(ar, scenes, reqs, device, slots=4, rate=None):
+    """The stream through the plain one-pair-at-a-time path and through the request loop.
+    Returns points/s of each, and per-request latency (queued + running, from the loop's own
+    clock) for a Poisson stream at `rate` requests/s (default: 70% of the measured capacity)."""
+    L = ar._lib
+    points = [len(ar.build_grid(scenes[n][0].shape, ar.params(**kw))) for n, kw in reqs]
+    plain_ctx = L.Context(device)
+    a, b, v = scenes[reqs[0][0]]
+    ar.autorift(a, b, secondary_valid=v, ctx=plain_ctx, **reqs[0][1])  # warm-up
+    t0 = time.perf_counter()
+    for n, kw in reqs:
+        a, b, v = scenes[n]
+        ar.autorift(a, b, secondary_valid=v, ctx=plain_ctx, **kw)
+    plain_s = time.perf_counter() - t0
+    plain_ctx.close()
+
+    ctx = L.Context(device)
+    ctx.set_option(L.AR_OPT_SERVE_SLOTS, slots)
+    a, b, v = scenes[reqs[0][0]]
+    ar.submit(a, b, secondary_valid=v, ctx=ctx, **reqs[0][1]).wait()  # warm-up: starts the loop
+    t0 = time.perf_counter()
+    tickets = [ar.submit(*scenes[n][:2], secondary_valid=scenes[n][2], ctx=ctx, **kw)
+               for n, kw in reqs]
+    for t in tickets:
+        t.wait()
+    burst_s = time.perf_counter() - t0
+    del tickets
+    cap = len(reqs) / burst_s
+    rate = rate or 0.7 * cap
+    rng = np.random.default_rng(1)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+    t0 = time.perf_counter()
+    tickets = []
+    for (n, kw), at in zip(reqs, arrivals):
+        dt = at - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        tickets.append(ar.submit(*scenes[n][:2], secondary_valid=scenes[n][2], ctx=ctx, **kw))
+    lat = []
+    for t in tickets:
+        t.wait()
+        q, r = t.times()
+        lat.append(q + r)
+    stream_s = time.perf_counter() - t0
+    del tickets
+    ctx.close()
+    total = float(sum(points))
+    return {"requests": len(reqs), "points": int(total), "slots": slots,
+            "plain_points_per_s": total / plain_s, "plain_pairs_per_s": len(reqs) / plain_s,
+            "batched_points_per_s": total / burst_s, "batched_pairs_per_s": cap,
+            "speedup_vs_plain": plain_s / burst_s,
+            "stream_rate_pairs_per_s": rate, "stream_points_per_s": total / stream_s,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
+
+
 def gpu_arm(args):
     import torch
     import __graft_entry__ as ge
@@ -314,6 +388,17 @@ def gpu_arm(args):
     same = bool(np.array_equal(hchip, chip)) and bool(
         np.array_equal(hout[0].view(np.uint32), dx.view(np.uint32)))
 
+    serving = None
+    if not args.no_serving:
+        # A short mixed stream (image sides 512, 2048, 4096 in proportion 8:4:2) through the
+        # plain path and the request loop.
+        sc, reqs = serving_requests(ar, np.random.default_rng(5), 14, (512, 2048, N), (8, 4, 2),
+                                    base=(a, b, valid))
+        serving = serving_measure(ar, sc, reqs, local)
+        serving["workload"] = ("14 requests, sides 512/2048/4096 (8:4:2), spacing {8,16,32}, chip "
+                               "{16,32,64}, radius U[8,48], PyramidRefine(64); latency from "
+                               "submission to completion at a Poisson rate of 70% of capacity")
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
@@ -354,6 +439,7 @@ def gpu_arm(args):
                     "p99_ms": float(np.percentile(e2e_times, 99)) * 1e3,
                     "path": "ar_pair_upload + ar_prepare + ar_multichip (host buffers) per pair",
                     "same_result_as_device_run": same},
+            "serving": serving,
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
         }
@@ -361,6 +447,23 @@ def gpu_arm(args):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def serve_arm(args):
+    """The serving configuration: a seeded Poisson stream of UInt16 pairs of sides 512, 2048,
+    4096 and 10980 in proportion 8:4:2:1, each with its own grid spacing, chip and radius;
+    sustained points/s of the request loop against the plain one-pair-at-a-time path, and
+    p50/p99 pair latency."""
+    import __graft_entry__ as ge
+
+    ge.build()
+    ar = ge.load_package()
+    sc, reqs = serving_requests(ar, np.random.default_rng(7), args.steps * 15,
+                                (512, 2048, 4096, 10980), (8, 4, 2, 1))
+    res = serving_measure(ar, sc, reqs, 0)
+    print(json.dumps({"metric": "serving: sustained points/s and p50/p99 pair latency",
+                      "value": res["batched_points_per_s"], "unit": UNIT, "n_gpus": 1,
+                      "higher_is_better": True, "data": "synthetic", "serving": res}))
 
 
 def reference_arm(args):
@@ -409,6 +512,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true",
+                    help="skip the mixed-stream serving measurement")
+    ap.add_argument("--serve", action="store_true",
+                    help="only the serving measurement, on a longer stream with 10980^2 pairs")
     ap.add_argument("--size", type=int, default=N,
                     help="image side; the benchmark line uses 4096, profiles a smaller scene")
     ap.add_argument("--profile", action="store_true",
@@ -418,6 +525,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         reference_arm(args)
+    elif args.serve:
+        serve_arm(args)
     else:
         gpu_arm(args)
 

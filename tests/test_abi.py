@@ -53,3 +53,32 @@ def test_no_gpu_fails_cleanly(ar):
     # Null-argument handling never touches the device.
     assert lib.ar_ctx_destroy(None) == ar._lib.AR_ERR_ARG
     assert lib.ar_pair_destroy(None) == ar._lib.AR_ERR_ARG
+
+
+def test_struct_layouts_match_the_header(ar, tmp_path):
+    """ctypes mirrors of the header's structs have the C sizes and field offsets."""
+    import ctypes
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    from pathlib import Path
+    inc = Path(__file__).resolve().parents[1] / "include"
+    src = tmp_path / "sz.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "autorift_gpu.h"\n'
+        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu\\n\", sizeof(ar_points),"
+        " sizeof(ar_prepare_opts), sizeof(ar_multichip_params), sizeof(ar_request),"
+        " offsetof(ar_request, prepare), offsetof(ar_request, params), offsetof(ar_request, grid));"
+        "return 0;}\n")
+    exe = tmp_path / "sz"
+    subprocess.run([cc, f"-I{inc}", str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True,
+                                          check=True).stdout.split()]
+    L = ar._lib
+    want = [ctypes.sizeof(L.ArPoints), ctypes.sizeof(L.ArPrepareOpts),
+            ctypes.sizeof(L.ArMultichipParams), ctypes.sizeof(L.ArRequest),
+            L.ArRequest.prepare.offset, L.ArRequest.params.offset, L.ArRequest.grid.offset]
+    assert got == want
