@@ -15,7 +15,8 @@ module AutoRIFTGPU
 using AutoRIFT
 using AutoRIFT: ImagePair, PointSet, Params, DisplacementField, displacement_field,
                 ZNCC, NCC, NoRefine, PyramidRefine, upsampling, scatter,
-                Highpass, Wallis, NoPreprocess, QuantizeUInt8, NoQuantize
+                Highpass, Wallis, NoPreprocess, QuantizeUInt8, NoQuantize,
+                GardnerFilter, NoOutlierFilter, MultichipResult, gridpoints
 
 const LIB = get(ENV, "AUTORIFT_GPU_LIB", joinpath(@__DIR__, "..", "libautorift_gpu.so"))
 
@@ -43,6 +44,48 @@ struct ArPrepareOpts
     width::Cint
     min_std::Float64
     quantize::Cint
+end
+
+# `ar_multichip_params`: the Params fields correlate_multichip reads (src/types.jl:781-829).
+struct ArMultichipParams
+    chip_size_base::Cint
+    chip_size_min::Cint
+    chip_size_max::Cint
+    chip_aspect::Float64
+    min_search_radius::Cint
+    coarse_stride::Cint
+    coarse_buffer::Cint
+    min_coarse_valid_fraction::Float64
+    upsampling::Cint
+    measure::Cint
+    outliers::Cint
+    outlier_window::Cint
+    outlier_iterations::Cint
+    min_agree_fraction::Float64
+    agree_tolerance::Float64
+    mad_scale::Float64
+    fill_window::Cint
+end
+
+# `ar_request`: one queued autorift() request.
+struct ArRequest
+    reference::Ptr{Cvoid}
+    secondary::Ptr{Cvoid}
+    reference_valid::Ptr{UInt8}
+    secondary_valid::Ptr{UInt8}
+    nrows::Int64
+    ncols::Int64
+    dtype::Cint
+    prepare::ArPrepareOpts
+    params::ArMultichipParams
+    grid::Ptr{ArPoints}
+    grid_rows::Int64
+    grid_cols::Int64
+    dx::Ptr{Float32}
+    dy::Ptr{Float32}
+    correlation::Ptr{Float32}
+    chip_size::Ptr{UInt16}
+    interpolated::Ptr{UInt8}
 end
 
 # One context per device, created on first use (the plan cache's role, src/plans.jl:25-47).
@@ -186,6 +229,122 @@ function prepare(pair::ImagePair, p::Params; device::Integer = 0)
     ccall((:ar_pair_destroy, LIB), Cint, (Ptr{Cvoid},), h[])
     check(ctx, rc, "ar_pair_download")
     return ImagePair(r, s, rv, sv)
+end
+
+
+outlier_fields(f::GardnerFilter) = (Cint(1), f.window, f.iterations, f.min_agree_fraction,
+                                    f.agree_tolerance, f.mad_scale)
+outlier_fields(::NoOutlierFilter) = (Cint(0), 5, 3, 8 / 25, 0.2, 4.0)
+
+function multichip_params(p::Params)
+    o = outlier_fields(p.outliers)
+    ArMultichipParams(p.chip_size_base, p.chip_size_min, p.chip_size_max, p.chip_aspect,
+                      p.min_search_radius, p.coarse_stride, p.coarse_buffer,
+                      p.min_coarse_valid_fraction, upsampling(p.subpixel),
+                      measure_code(first(p.similarity)), o[1], o[2], o[3], o[4], o[5], o[6],
+                      p.fill_window)
+end
+
+# The eight PointSet fields flattened, kept alive by the returned tuple.
+function flat_points(pts::PointSet)
+    f = scatter(pts)
+    cols = (collect(f.x), collect(f.y), collect(f.radius_x), collect(f.radius_y),
+            collect(f.dx_prior), collect(f.dy_prior), collect(f.chip_size_x),
+            collect(f.chip_size_y))
+    P = ArPoints(pointer(cols[1]), pointer(cols[2]), pointer(cols[3]), pointer(cols[4]),
+                 pointer(cols[5]), pointer(cols[6]), pointer(cols[7]), pointer(cols[8]),
+                 length(cols[1]))
+    return P, cols
+end
+
+"""
+    AutoRIFTGPU.correlate_multichip(prepared::ImagePair, grid::PointSet{2}, p) -> MultichipResult
+
+`correlate_multichip` (src/multichip.jl:106-137) on the GPU, over a prepared pair.
+"""
+function correlate_multichip(prepared::ImagePair, grid::PointSet, p::Params; device::Integer = 0)
+    ctx = context(device)
+    dp = upload(prepared, ctx)
+    gr, gc = size(grid)
+    n = gr * gc
+    dx = Matrix{Float32}(undef, gr, gc); dy = similar(dx); cc = similar(dx)
+    cs = Matrix{UInt16}(undef, gr, gc); it = Matrix{UInt8}(undef, gr, gc)
+    P, cols = flat_points(grid)
+    prm = Ref(multichip_params(p))
+    GC.@preserve cols begin
+        rc = ccall((:ar_multichip, LIB), Cint,
+                   (Ptr{Cvoid}, Ptr{Cvoid}, Ref{ArPoints}, Int64, Int64, Ref{ArMultichipParams},
+                    Ptr{Float32}, Ptr{Float32}, Ptr{Float32}, Ptr{UInt16}, Ptr{UInt8}),
+                   ctx, dp.handle, Ref(P), gr, gc, prm, dx, dy, cc, cs, it)
+        check(ctx, rc, "ar_multichip")
+    end
+    return MultichipResult(dx, dy, cc, cs, BitMatrix(it .!= 0))
+end
+
+"""
+    AutoRIFTGPU.autorift(image1, image2; kw...) -> MultichipResult
+
+`autorift` (src/api.jl:210-274) with the default grid: prepare both images, then the
+multi-chip-size search, on the GPU.
+"""
+function autorift(image1::AbstractMatrix, image2::AbstractMatrix; reference_valid = nothing,
+                  secondary_valid = nothing, device::Integer = 0, kw...)
+    p = AutoRIFT.params(; kw...)
+    pair = reference_valid === nothing && secondary_valid === nothing ? ImagePair(image1, image2) :
+           ImagePair(image1, image2, something(reference_valid, isfinite.(image1)),
+                     something(secondary_valid, isfinite.(image2)))
+    grid = gridpoints(size(image1), p.grid_spacing; chip_size = p.chip_size_max,
+                      chip_aspect = p.chip_aspect, search_radius_x = p.search_radius_x,
+                      search_radius_y = p.search_radius_y, dx_prior = p.dx_prior,
+                      dy_prior = p.dy_prior)
+    return correlate_multichip(prepare(pair, p; device), grid, p; device)
+end
+
+# A queued request and everything it references (kept alive until it completes).
+mutable struct Ticket
+    ctx::Ptr{Cvoid}
+    id::Int64
+    keep::Any
+    result::MultichipResult
+end
+
+"""
+    AutoRIFTGPU.submit(image1, image2, grid, p) -> Ticket
+
+Queue `autorift` on the context's request loop (`ar_submit`); requests submitted from several
+tasks run concurrently on the device. `fetch(ticket)` waits and returns the MultichipResult.
+"""
+function submit(image1::AbstractMatrix{T}, image2::AbstractMatrix{T}, grid::PointSet, p::Params;
+                secondary_valid = nothing, device::Integer = 0) where {T}
+    ctx = context(device)
+    ref = collect(image1); sec = collect(image2)
+    sv = secondary_valid === nothing ? nothing : collect(secondary_valid)  # Matrix{Bool}
+    gr, gc = size(grid)
+    res = MultichipResult(Matrix{Float32}(undef, gr, gc), Matrix{Float32}(undef, gr, gc),
+                          Matrix{Float32}(undef, gr, gc), Matrix{UInt16}(undef, gr, gc),
+                          falses(gr, gc))
+    it = Matrix{UInt8}(undef, gr, gc)
+    P, cols = flat_points(grid)
+    Pref = Ref(P)
+    req = Ref(ArRequest(pointer(ref), pointer(sec), C_NULL,
+                        sv === nothing ? C_NULL : Ptr{UInt8}(pointer(sv)),
+                        size(ref, 1), size(ref, 2), eltype_code(T),
+                        prepare_opts(p.preprocess, p.quantize), multichip_params(p),
+                        Base.unsafe_convert(Ptr{ArPoints}, Pref), gr, gc,
+                        pointer(res.dx), pointer(res.dy), pointer(res.correlation),
+                        pointer(res.chip_size), pointer(it)))
+    t = Ref{Int64}(0)
+    rc = ccall((:ar_submit, LIB), Cint, (Ptr{Cvoid}, Ref{ArRequest}, Ref{Int64}), ctx, req, t)
+    check(ctx, rc, "ar_submit")
+    return Ticket(ctx, t[], (ref, sec, sv, cols, Pref, req, it), res)
+end
+
+function Base.fetch(t::Ticket)
+    rc = ccall((:ar_wait, LIB), Cint, (Ptr{Cvoid}, Int64, Cint), t.ctx, t.id, -1)
+    check(t.ctx, rc, "ar_wait")
+    t.result.interpolated .= t.keep[end] .!= 0
+    ccall((:ar_release, LIB), Cint, (Ptr{Cvoid}, Int64), t.ctx, t.id)
+    return t.result
 end
 
 end # module

@@ -392,12 +392,16 @@ def gpu_arm(args):
     if not args.no_serving:
         # A short mixed stream (image sides 512, 2048, 4096 in proportion 8:4:2) through the
         # plain path and the request loop.
-        sc, reqs = serving_requests(ar, np.random.default_rng(5), 14, (512, 2048, N), (8, 4, 2),
-                                    base=(a, b, valid))
-        serving = serving_measure(ar, sc, reqs, local)
-        serving["workload"] = ("14 requests, sides 512/2048/4096 (8:4:2), spacing {8,16,32}, chip "
-                               "{16,32,64}, radius U[8,48], PyramidRefine(64); latency from "
-                               "submission to completion at a Poisson rate of 70% of capacity")
+        try:
+            sc, reqs = serving_requests(ar, np.random.default_rng(5), 14, (512, 2048, N),
+                                        (8, 4, 2), base=(a, b, valid))
+            serving = serving_measure(ar, sc, reqs, local)
+            serving["workload"] = ("14 requests, sides 512/2048/4096 (8:4:2), spacing {8,16,32}, "
+                                   "chip {16,32,64}, radius U[8,48], PyramidRefine(64); latency "
+                                   "from submission to completion at a Poisson rate of 70% of "
+                                   "capacity")
+        except Exception as exc:  # reported, not fatal to the main measurement
+            serving = {"error": f"{type(exc).__name__}: {exc}"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
