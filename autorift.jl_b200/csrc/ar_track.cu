@@ -181,6 +181,7 @@ struct CorrArgs {
     int TI, TJ;   // surface tile; TI a multiple of kMI and (TI/kMI)*TJ <= blockDim
     int CHP;      // chip smem stride (rows), >= every point's ch rounded up to 16
     int CWM;      // largest chip width
+    int BC;       // chip columns staged at a time (== CWM: the whole chip once per point)
     int WS;       // window smem stride (floats): even, WS/2 odd, >= TI + CHP
     int PHS;      // prefix-table stride (entries), >= TI + largest ch
     int NRS;      // surface smem stride (rows), >= largest nr
@@ -292,7 +293,7 @@ __global__ void __launch_bounds__(kCorrThreads, 2) k_corr(const CorrArgs A) {
                 acc2[1] = __dadd_rn(acc2[1], static_cast<double>(df));
                 staged = Tr::raw ? static_cast<float>(v) : df;
             }
-            s_chip[b * A.CHP + a] = staged;
+            if (A.BC >= cw) s_chip[b * A.CHP + a] = staged;
         }
         block_sum_f64<2>(acc2, s_red);
         const double sq = acc2[0], sumd = acc2[1];
@@ -313,109 +314,132 @@ __global__ void __launch_bounds__(kCorrThreads, 2) k_corr(const CorrArgs A) {
             const int wrows = trows + ch - 1; // rows the box sums use
             for (int tj = 0; tj < nc; tj += A.TJ) {
                 const int tcols = min(A.TJ, nc - tj);
-                const int xcols = tcols + cw - 1;
-                __syncthreads();
-                // Stage the window block column-major, zero outside the image and below the
-                // window's last row.
-                for (int e = tid; e < xcols * srows; e += bd) {
-                    const int r = e % srows, x = e / srows;
-                    float v = 0.0f;
-                    if (r < wrows) {
-                        const double pv =
-                            pixel(ref, A.nrows, A.ncols, win_r + ti + r, win_c + tj + x);
-                        v = Tr::raw ? static_cast<float>(pv)
-                                    : __double2float_rn(__dsub_rn(pv, cshift));
+                // Numerator item = (row group, column), kMI surface rows per thread; its
+                // partial sums run across the chip-column chunks.
+                const int ig = tid / A.TJ, jl = tid % A.TJ;
+                const bool item = ig * kMI < trows && jl < tcols;
+                const int il = ig * kMI;
+                float acc[kMI];
+                double acc64[kMI];
+#pragma unroll
+                for (int m = 0; m < kMI; ++m) { acc[m] = 0.0f; acc64[m] = 0.0; }
+                int fc = 0;
+                for (int b0 = 0; b0 < cw; b0 += A.BC) {
+                    const int bc = min(A.BC, cw - b0);
+                    const int xcols = tcols + bc - 1;
+                    __syncthreads();
+                    if (A.BC < cw) {
+                        // This chunk of chip columns, staged as in the unchunked case.
+                        for (int e = tid; e < chp * bc; e += bd) {
+                            const int a = e % chp, bl = e / chp;
+                            float staged = 0.0f;
+                            if (a < ch) {
+                                const double v = pixel(sec, A.nrows, A.ncols, chip_r + a, chip_c + b0 + bl);
+                                staged = Tr::raw ? static_cast<float>(v)
+                                                 : __double2float_rn(__dsub_rn(v, mean));
+                            }
+                            s_chip[bl * A.CHP + a] = staged;
+                        }
                     }
-                    s_win[x * A.WS + r] = v;
-                }
-                __syncthreads();
-                // Per-window sums of W and W^2 over cw columns for every row the tile uses
-                // (integral_both!, src/integral.jl:141-170), stored at slot r + 1.
-                const int nseg = (tcols + 15) >> 4;
-                for (int task = tid; task < wrows * nseg; task += bd) {
-                    const int r = task % wrows, seg = task / wrows;
-                    const int j0s = seg << 4, j1s = min(j0s + 16, tcols);
-                    PH h1 = 0, h2 = 0;
-                    for (int b = 0; b < cw; ++b) {
-                        const PH w = ph_of<PH>(s_win[(j0s + b) * A.WS + r]);
-                        h1 = h1 + w;
-                        h2 = h2 + w * w;
+                    // Stage the window block column-major, zero outside the image and below
+                    // the window's last row.
+                    for (int e = tid; e < xcols * srows; e += bd) {
+                        const int r = e % srows, x = e / srows;
+                        float v = 0.0f;
+                        if (r < wrows) {
+                            const double pv =
+                                pixel(ref, A.nrows, A.ncols, win_r + ti + r, win_c + tj + b0 + x);
+                            v = Tr::raw ? static_cast<float>(pv)
+                                        : __double2float_rn(__dsub_rn(pv, cshift));
+                        }
+                        s_win[x * A.WS + r] = v;
                     }
-                    s_ph1[j0s * A.PHS + r + 1] = h1;
-                    s_ph2[j0s * A.PHS + r + 1] = h2;
-                    for (int jl = j0s + 1; jl < j1s; ++jl) {
-                        const PH wo = ph_of<PH>(s_win[(jl - 1) * A.WS + r]);
-                        const PH wn = ph_of<PH>(s_win[(jl - 1 + cw) * A.WS + r]);
-                        h1 = h1 + wn - wo;
-                        h2 = h2 + wn * wn - wo * wo;
-                        s_ph1[jl * A.PHS + r + 1] = h1;
-                        s_ph2[jl * A.PHS + r + 1] = h2;
+                    __syncthreads();
+                    // Per-window sums of W and W^2 over the chunk's columns for every row the
+                    // tile uses (integral_both!, src/integral.jl:141-170), added at slot r + 1.
+                    const int nseg = (tcols + 15) >> 4;
+                    for (int task = tid; task < wrows * nseg; task += bd) {
+                        const int r = task % wrows, seg = task / wrows;
+                        const int j0s = seg << 4, j1s = min(j0s + 16, tcols);
+                        PH h1 = 0, h2 = 0;
+                        for (int b = 0; b < bc; ++b) {
+                            const PH w = ph_of<PH>(s_win[(j0s + b) * A.WS + r]);
+                            h1 = h1 + w;
+                            h2 = h2 + w * w;
+                        }
+                        for (int jj = j0s; jj < j1s; ++jj) {
+                            if (jj > j0s) {
+                                const PH wo = ph_of<PH>(s_win[(jj - 1) * A.WS + r]);
+                                const PH wn = ph_of<PH>(s_win[(jj - 1 + bc) * A.WS + r]);
+                                h1 = h1 + wn - wo;
+                                h2 = h2 + wn * wn - wo * wo;
+                            }
+                            PH* p1 = &s_ph1[jj * A.PHS + r + 1];
+                            PH* p2 = &s_ph2[jj * A.PHS + r + 1];
+                            *p1 = b0 == 0 ? h1 : *p1 + h1;
+                            *p2 = b0 == 0 ? h2 : *p2 + h2;
+                        }
+                    }
+                    // The chunk's share of the numerator.
+                    if (item) {
+                        const float* wbase = s_win + jl * A.WS + il;
+                        for (int b = 0; b < bc; ++b) {
+                            const float* wc = wbase + b * A.WS;
+                            const float* cc = s_chip + b * A.CHP;
+                            for (int a0 = 0; a0 < chp; a0 += kUA) {
+                                float c[kUA];
+                                float w[kUA + kMI];
+#pragma unroll
+                                for (int q = 0; q < kUA / 4; ++q) {
+                                    const float4 v = *reinterpret_cast<const float4*>(cc + a0 + 4 * q);
+                                    c[4 * q] = v.x; c[4 * q + 1] = v.y; c[4 * q + 2] = v.z; c[4 * q + 3] = v.w;
+                                }
+#pragma unroll
+                                for (int q = 0; q < (kUA + kMI) / 2; ++q) {
+                                    const float2 v = *reinterpret_cast<const float2*>(wc + a0 + 2 * q);
+                                    w[2 * q] = v.x; w[2 * q + 1] = v.y;
+                                }
+#pragma unroll
+                                for (int a = 0; a < kUA; ++a)
+#pragma unroll
+                                    for (int m = 0; m < kMI; ++m) acc[m] = fmaf(c[a], w[m + a], acc[m]);
+                            }
+                            if (++fc == F) {
+#pragma unroll
+                                for (int m = 0; m < kMI; ++m) {
+                                    acc64[m] = __dadd_rn(acc64[m], static_cast<double>(acc[m]));
+                                    acc[m] = 0.0f;
+                                }
+                                fc = 0;
+                            }
+                        }
                     }
                 }
                 __syncthreads();
                 // Exclusive prefix down each column by warp scans: ph[jl][q] = sum_{r<q} H[r].
-                for (int jl = warp; jl < tcols; jl += nwarps) {
+                for (int jw = warp; jw < tcols; jw += nwarps) {
                     PH c1 = 0, c2 = 0;
                     for (int q = 1; q <= wrows; q += 32) {
                         const int idx = q + lane;
-                        PH v1 = idx <= wrows ? s_ph1[jl * A.PHS + idx] : PH(0);
-                        PH v2 = idx <= wrows ? s_ph2[jl * A.PHS + idx] : PH(0);
+                        PH v1 = idx <= wrows ? s_ph1[jw * A.PHS + idx] : PH(0);
+                        PH v2 = idx <= wrows ? s_ph2[jw * A.PHS + idx] : PH(0);
                         v1 = warp_inclusive_scan(v1) + c1;
                         v2 = warp_inclusive_scan(v2) + c2;
                         if (idx <= wrows) {
-                            s_ph1[jl * A.PHS + idx] = v1;
-                            s_ph2[jl * A.PHS + idx] = v2;
+                            s_ph1[jw * A.PHS + idx] = v1;
+                            s_ph2[jw * A.PHS + idx] = v2;
                         }
                         c1 = __shfl_sync(kFull, v1, 31);
                         c2 = __shfl_sync(kFull, v2, 31);
                     }
                     if (lane == 0) {
-                        s_ph1[jl * A.PHS] = PH(0);
-                        s_ph2[jl * A.PHS] = PH(0);
+                        s_ph1[jw * A.PHS] = PH(0);
+                        s_ph2[jw * A.PHS] = PH(0);
                     }
                 }
                 __syncthreads();
 
-                // Numerator: item = (row group, column), kMI surface rows per thread.
-                const int ig = tid / A.TJ, jl = tid % A.TJ;
-                if (ig * kMI < trows && jl < tcols) {
-                    const int il = ig * kMI;
-                    float acc[kMI];
-                    double acc64[kMI];
-#pragma unroll
-                    for (int m = 0; m < kMI; ++m) { acc[m] = 0.0f; acc64[m] = 0.0; }
-                    const float* wbase = s_win + jl * A.WS + il;
-                    int fc = 0;
-                    for (int b = 0; b < cw; ++b) {
-                        const float* wc = wbase + b * A.WS;
-                        const float* cc = s_chip + b * A.CHP;
-                        for (int a0 = 0; a0 < chp; a0 += kUA) {
-                            float c[kUA];
-                            float w[kUA + kMI];
-#pragma unroll
-                            for (int q = 0; q < kUA / 4; ++q) {
-                                const float4 v = *reinterpret_cast<const float4*>(cc + a0 + 4 * q);
-                                c[4 * q] = v.x; c[4 * q + 1] = v.y; c[4 * q + 2] = v.z; c[4 * q + 3] = v.w;
-                            }
-#pragma unroll
-                            for (int q = 0; q < (kUA + kMI) / 2; ++q) {
-                                const float2 v = *reinterpret_cast<const float2*>(wc + a0 + 2 * q);
-                                w[2 * q] = v.x; w[2 * q + 1] = v.y;
-                            }
-#pragma unroll
-                            for (int a = 0; a < kUA; ++a)
-#pragma unroll
-                                for (int m = 0; m < kMI; ++m) acc[m] = fmaf(c[a], w[m + a], acc[m]);
-                        }
-                        if (++fc == F) {
-#pragma unroll
-                            for (int m = 0; m < kMI; ++m) {
-                                acc64[m] = __dadd_rn(acc64[m], static_cast<double>(acc[m]));
-                                acc[m] = 0.0f;
-                            }
-                            fc = 0;
-                        }
-                    }
+                if (item) {
 #pragma unroll
                     for (int m = 0; m < kMI; ++m)
                         acc64[m] = __dadd_rn(acc64[m], static_cast<double>(acc[m]));
@@ -831,43 +855,74 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         auto box_sums = [&]() {
             constexpr int kBT = kTcThreads - 32;
             uint32_t* s_V2 = s_V1 + A.NRM * XW;
-            const int nseg = (nr + 15) >> 4;
+            // V: one round of tasks (column x, a run of rows), each an unrolled first sum with
+            // independent partials and a sliding update with the next values loaded ahead.
+            const int nseg = max(1, min((nr + 7) / 8, kBT / XW));
+            const int seglen = (nr + nseg - 1) / nseg;
             for (int task = tid; task < XW * nseg; task += kBT) {
                 const int x = task % XW, seg = task / XW;
-                const int i0 = seg << 4, i1 = min(i0 + 16, nr);
+                const int i0 = seg * seglen, i1 = min(i0 + seglen, nr);
+                if (i0 >= i1) continue;
                 const uint8_t* col = s_T + static_cast<int>(delta) * A.XT + x;
-                uint32_t h1 = 0, h2 = 0;
-                for (int a = 0; a < ch; ++a) {
-                    const uint32_t w = col[(i0 + a) * A.XT];
-                    h1 += w;
-                    h2 += w * w;
+                uint32_t p1[4] = {0, 0, 0, 0}, p2[4] = {0, 0, 0, 0};
+                int a = 0;
+                for (; a + 4 <= ch; a += 4) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const uint32_t w = col[(i0 + a + u) * A.XT];
+                        p1[u] += w;
+                        p2[u] += w * w;
+                    }
                 }
+                for (; a < ch; ++a) {
+                    const uint32_t w = col[(i0 + a) * A.XT];
+                    p1[0] += w;
+                    p2[0] += w * w;
+                }
+                uint32_t h1 = (p1[0] + p1[1]) + (p1[2] + p1[3]);
+                uint32_t h2 = (p2[0] + p2[1]) + (p2[2] + p2[3]);
+                uint32_t wo = col[i0 * A.XT], wn = col[(i0 + ch) * A.XT];
                 for (int i = i0; i < i1; ++i) {
                     s_V1[i * XW + x] = h1;
                     s_V2[i * XW + x] = h2;
                     if (i + 1 < i1) {
-                        const uint32_t wn = col[(i + ch) * A.XT], wo = col[i * A.XT];
+                        const uint32_t wo2 = col[(i + 1) * A.XT], wn2 = col[(i + 1 + ch) * A.XT];
                         h1 = h1 + wn - wo;
                         h2 = h2 + wn * wn - wo * wo;
+                        wo = wo2;
+                        wn = wn2;
                     }
                 }
             }
             asm volatile("bar.sync 1, %0;" ::"r"(kBT) : "memory");
+            // S: tasks (surface row i, a run of 16 columns), the same pattern along V's rows.
             const int jseg = (nc + 15) >> 4;
             for (int task = tid; task < nr * jseg; task += kBT) {
                 const int i = task % nr, seg = task / nr;
                 const int j0 = seg << 4, j1 = min(j0 + 16, nc);
-                uint32_t g1 = 0, g2 = 0;
-                for (int b = 0; b < cw; ++b) {
-                    g1 += s_V1[i * XW + j0 + b];
-                    g2 += s_V2[i * XW + j0 + b];
+                const uint32_t* v1 = s_V1 + i * XW;
+                const uint32_t* v2 = s_V2 + i * XW;
+                uint32_t q1[4] = {0, 0, 0, 0}, q2[4] = {0, 0, 0, 0};
+                int b = 0;
+                for (; b + 4 <= cw; b += 4) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        q1[u] += v1[j0 + b + u];
+                        q2[u] += v2[j0 + b + u];
+                    }
                 }
+                for (; b < cw; ++b) {
+                    q1[0] += v1[j0 + b];
+                    q2[0] += v2[j0 + b];
+                }
+                uint32_t g1 = (q1[0] + q1[1]) + (q1[2] + q1[3]);
+                uint32_t g2 = (q2[0] + q2[1]) + (q2[2] + q2[3]);
                 for (int j = j0; j < j1; ++j) {
                     s_S1[j * A.NRS + i] = g1;
                     s_S2[j * A.NRS + i] = g2;
                     if (j + 1 < j1) {
-                        g1 = g1 + s_V1[i * XW + j + cw] - s_V1[i * XW + j];
-                        g2 = g2 + s_V2[i * XW + j + cw] - s_V2[i * XW + j];
+                        g1 = g1 + v1[j + cw] - v1[j];
+                        g2 = g2 + v2[j + cw] - v2[j];
                     }
                 }
             }
@@ -1454,7 +1509,7 @@ inline int window_stride(int rows) {
 }
 
 struct CorrPlan {
-    int TI, TJ, CHP, CWM, WS, PHS, NRS, NCM;
+    int TI, TJ, CHP, CWM, WS, PHS, NRS, NCM, BC;
     unsigned off_win, off_ph1, off_ph2, off_surf, off_red;
     size_t smem;
 };
@@ -1466,44 +1521,51 @@ bool plan_corr(const PassGeometry& g, size_t ph_bytes, size_t smem_cap, CorrPlan
     P->CWM = std::max(cw, 1);
     P->NRS = std::max(nr, 1);
     P->NCM = std::max(nc, 1);
-    // Columns per tile: as many as fit one thread each with at least one row group, rows to
-    // fill the block. Shrink until the shared-memory budget is met.
-    for (int TJ = std::min(nc, kCorrThreads); TJ >= 1; TJ = (TJ > 8 ? TJ - 8 : TJ - 1)) {
-        const int groups = std::max(1, kCorrThreads / TJ);
-        for (int TI = std::min(round_up(nr, kMI), groups * kMI); TI >= kMI; TI -= kMI) {
-            const int WS = window_stride(TI + P->CHP);
-            const int PHS = TI + ch + 1;
-            size_t off = static_cast<size_t>(P->CHP) * P->CWM * 4;
-            off = (off + 15) & ~size_t(15);
-            const unsigned off_win = static_cast<unsigned>(off);
-            off += static_cast<size_t>(WS) * (TJ + P->CWM - 1) * 4;
-            off = (off + 15) & ~size_t(15);
-            const unsigned off_ph1 = static_cast<unsigned>(off);
-            off += static_cast<size_t>(PHS) * TJ * ph_bytes;
-            off = (off + 15) & ~size_t(15);
-            const unsigned off_ph2 = static_cast<unsigned>(off);
-            off += static_cast<size_t>(PHS) * TJ * ph_bytes;
-            off = (off + 15) & ~size_t(15);
-            const unsigned off_surf = static_cast<unsigned>(off);
-            off += static_cast<size_t>(P->NRS) * P->NCM * 4;
-            off = (off + 15) & ~size_t(15);
-            const unsigned off_red = static_cast<unsigned>(off);
-            off += 3 * 32 * 8;
-            if (off <= smem_cap) {
-                P->TI = TI;
-                P->TJ = TJ;
-                P->WS = WS;
-                P->PHS = PHS;
-                P->off_win = off_win;
-                P->off_ph1 = off_ph1;
-                P->off_ph2 = off_ph2;
-                P->off_surf = off_surf;
-                P->off_red = off_red;
-                P->smem = off;
-                return true;
+    // The whole chip staged once per point if it fits, otherwise chunks of BC chip columns
+    // (even, so FP32 partial flushes fall where they would unchunked). Within that, columns
+    // per tile: as many as fit one thread each with at least one row group, rows to fill the
+    // block; shrink until the shared-memory budget is met.
+    const int bcs[] = {P->CWM, 64, 32, 16, 8, 4, 2};
+    for (int bc : bcs) {
+        if (bc > P->CWM || (bc < P->CWM && (bc & 1))) continue;
+        for (int TJ = std::min(nc, kCorrThreads); TJ >= 1; TJ = (TJ > 8 ? TJ - 8 : TJ - 1)) {
+            const int groups = std::max(1, kCorrThreads / TJ);
+            for (int TI = std::min(round_up(nr, kMI), groups * kMI); TI >= kMI; TI -= kMI) {
+                const int WS = window_stride(TI + P->CHP);
+                const int PHS = TI + ch + 1;
+                size_t off = static_cast<size_t>(P->CHP) * bc * 4;
+                off = (off + 15) & ~size_t(15);
+                const unsigned off_win = static_cast<unsigned>(off);
+                off += static_cast<size_t>(WS) * (TJ + bc - 1) * 4;
+                off = (off + 15) & ~size_t(15);
+                const unsigned off_ph1 = static_cast<unsigned>(off);
+                off += static_cast<size_t>(PHS) * TJ * ph_bytes;
+                off = (off + 15) & ~size_t(15);
+                const unsigned off_ph2 = static_cast<unsigned>(off);
+                off += static_cast<size_t>(PHS) * TJ * ph_bytes;
+                off = (off + 15) & ~size_t(15);
+                const unsigned off_surf = static_cast<unsigned>(off);
+                off += static_cast<size_t>(P->NRS) * P->NCM * 4;
+                off = (off + 15) & ~size_t(15);
+                const unsigned off_red = static_cast<unsigned>(off);
+                off += 3 * 32 * 8;
+                if (off <= smem_cap) {
+                    P->TI = TI;
+                    P->TJ = TJ;
+                    P->WS = WS;
+                    P->PHS = PHS;
+                    P->BC = bc;
+                    P->off_win = off_win;
+                    P->off_ph1 = off_ph1;
+                    P->off_ph2 = off_ph2;
+                    P->off_surf = off_surf;
+                    P->off_red = off_red;
+                    P->smem = off;
+                    return true;
+                }
             }
+            if (TJ == 1) break;
         }
-        if (TJ == 1) break;
     }
     return false;
 }
@@ -1805,6 +1867,7 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
     A.TJ = P.TJ;
     A.CHP = P.CHP;
     A.CWM = P.CWM;
+    A.BC = P.BC;
     A.WS = P.WS;
     A.PHS = P.PHS;
     A.NRS = P.NRS;
