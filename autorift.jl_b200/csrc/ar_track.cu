@@ -573,6 +573,7 @@ struct TcArgs {
     int up, measure;
     int NB, QM, QS, PS, PC, XS, XT, NRS, NRM, NCM, CHM, CWM;
     int BC;                          // chip columns per chunk of the chip operand (even)
+    int MT;                          // MMA M: 64 or 128 surface columns
     int big;                         // 1: box sums before the products, chunks reuse their space
     unsigned off_E, off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
     uint32_t tmem_cols;
@@ -716,7 +717,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         const int ch = static_cast<int>(2 * hy), cw = static_cast<int>(2 * hx);
         const int nr = static_cast<int>(2 * pry), nc = static_cast<int>(2 * prx);
         if (ch <= 0 || cw <= 0) continue;
-        if (ch > A.CHM || cw > A.CWM || nr > A.NRM || nc > A.NCM || nc > 64) continue;
+        if (ch > A.CHM || cw > A.CWM || nr > A.NRM || nc > A.NCM || nc > A.MT) continue;
         const int64_t chip_r = cr0 - 1 - A.pady, chip_c = cc0 - 1 - A.padx;
         const int64_t win_r = wr0 - 1 - A.pady, win_c = wc0 - 1 - A.padx;
         const long long nnl = static_cast<long long>(ch) * cw;
@@ -972,7 +973,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             if (tid == kTcThreads - 32) {
                 tc::fence_after_sync();
                 const uint32_t sW = tc::smem_u32(s_W), sE = tc::smem_u32(s_E);
-                const uint32_t idesc = tc::idesc_u8_s32(64, A.NB);
+                const uint32_t idesc = tc::idesc_u8_s32(A.MT, A.NB);
                 for (int q = 0; q < Q; ++q)
                     for (int t = b0 / 2; t < b1 / 2; ++t) {
                         const uint64_t da = tc::smem_desc(sW + q * A.QS + 32 * t, 16, 128);
@@ -1008,25 +1009,37 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         const int quarter = warp & 3, half = warp >> 2;
         const uint32_t col0 = static_cast<uint32_t>(A.NB - 16);
         float lmax = -INFINITY;
-        for (int i0 = 32 * half; i0 < nr; i0 += 64) {
-            uint32_t r[16];
-            tc::tmem_ld16dp(taddr + (static_cast<uint32_t>(32 * quarter) << 16) + col0 +
-                                static_cast<uint32_t>(i0), r);
-            tc::tmem_wait_ld();
+        auto take = [&](uint32_t d, int i, int j) {
+            if (j < nc && i < nr) {
+                const int o = j * A.NRS + i;
+                float bnd;
+                const float est = tc_estimate(d, s_S1[o], s_S2[o], nnf, csf, kk, A.measure, &bnd);
+                s_num[o] = d;
+                s_est[o] = est;
+                s_est[o + A.NCM * A.NRS] = bnd;
+                lmax = fmaxf(lmax, est - bnd);
+            }
+        };
+        if (A.MT == 64) {
+            for (int i0 = 32 * half; i0 < nr; i0 += 64) {
+                uint32_t r[16];
+                tc::tmem_ld16dp(taddr + (static_cast<uint32_t>(32 * quarter) << 16) + col0 +
+                                    static_cast<uint32_t>(i0), r);
+                tc::tmem_wait_ld();
 #pragma unroll
-            for (int v = 0; v < 16; ++v) {
-                const int j = 16 * quarter + (lane >> 2) + ((v & 2) ? 8 : 0);
-                const int i = i0 + 8 * (v >> 2) + 2 * (lane & 3) + (v & 1);
-                if (j < nc && i < nr) {
-                    const int o = j * A.NRS + i;
-                    float bnd;
-                    const float est = tc_estimate(r[v], s_S1[o], s_S2[o], nnf, csf, kk,
-                                                  A.measure, &bnd);
-                    s_num[o] = r[v];
-                    s_est[o] = est;
-                    s_est[o + A.NCM * A.NRS] = bnd;
-                    lmax = fmaxf(lmax, est - bnd);
-                }
+                for (int v = 0; v < 16; ++v)
+                    take(r[v], i0 + 8 * (v >> 2) + 2 * (lane & 3) + (v & 1),
+                         16 * quarter + (lane >> 2) + ((v & 2) ? 8 : 0));
+            }
+        } else {
+            // M = 128: accumulator row j is lane j; thread = row 32 q + lane, 16 columns.
+            for (int i0 = 16 * half; i0 < nr; i0 += 32) {
+                uint32_t r[16];
+                tc::tmem_ld16(taddr + (static_cast<uint32_t>(32 * quarter) << 16) + col0 +
+                                  static_cast<uint32_t>(i0), r);
+                tc::tmem_wait_ld();
+#pragma unroll
+                for (int m = 0; m < 16; ++m) take(r[m], i0 + m, 32 * quarter + lane);
             }
         }
 #pragma unroll
@@ -1602,7 +1615,7 @@ RefinePlan plan_refine(int up) {
 }
 
 struct TcPlan {
-    int NB, QM, QS, PS, PC, XS, XT, NRS, NRM, NCM, CHM, CWM, BC, big;
+    int NB, QM, QS, PS, PC, XS, XT, NRS, NRM, NCM, CHM, CWM, BC, big, MT;
     unsigned off_E, off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
     uint32_t tmem_cols;
     size_t smem;
@@ -1616,16 +1629,17 @@ struct TcPlan {
 bool plan_corr_tc(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
     const int ch = static_cast<int>(g.max_ch), cw = static_cast<int>(g.max_cw);
     const int nr = static_cast<int>(g.max_nr), nc = static_cast<int>(g.max_nc);
-    if (nc > 64 || nr > 256 || nr < 1 || nc < 1 || cw < 2 || ch < 2 || (cw & 1)) return false;
+    if (nc > 128 || nr > 256 || nr < 1 || nc < 1 || cw < 2 || ch < 2 || (cw & 1)) return false;
     P->CHM = ch;
     P->CWM = cw;
     P->NRM = nr;
     P->NCM = nc;
+    P->MT = nc <= 64 ? 64 : 128;
     P->NB = round_up(ch + 30, 16);
     if (P->NB > 256) return false;
     P->QM = (15 + ch + nr - 1 + 15) / 16;
     P->PS = P->NB * 16;
-    P->XS = 64 + cw;
+    P->XS = P->MT + cw;
     P->QS = P->XS * 16;
     P->XT = round_up(cw + nc - 1, 4) + 4;
     P->PC = round_up(kPadL + P->NB + 20, 16);
@@ -1922,6 +1936,7 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         B.CWM = TP.CWM;
         B.BC = TP.BC;
         B.big = TP.big;
+        B.MT = TP.MT;
         B.off_E = TP.off_E;
         B.off_W = TP.off_W;
         B.off_T = TP.off_T;

@@ -41,6 +41,8 @@ CASES = [
     dict(chip=24, r=12, up=16, measure="zncc"),   # chip area 576: not a power of two
     dict(chip=16, r=(20, 8), up=8, measure="zncc"),
     dict(chip=32, r=(6, 31), up=32, measure="zncc"),
+    dict(chip=32, r=(48, 20), up=16, measure="zncc"),   # 96 surface columns: M = 128
+    dict(chip=16, r=(40, 40), up=8, measure="ncc"),
 ]
 
 
