@@ -604,25 +604,20 @@ __device__ __forceinline__ float tc_exact(uint32_t D, uint32_t S1, uint32_t S2, 
     return den > 0.0 ? __double2float_rn(__ddiv_rn(num, den)) : 0.0f;
 }
 
-// Exact FP32 value of an unsigned integer below 2^32 rounded once: the two 16-bit halves are
-// exact floats, their sum one rounding.
-__device__ __forceinline__ float u32_to_f(uint32_t v) {
-    const float hi = __int_as_float(0x4B000000 | (v >> 16)) - 8388608.0f;
-    const float lo = __int_as_float(0x4B000000 | (v & 0xFFFFu)) - 8388608.0f;
-    return __fmaf_rn(hi, 65536.0f, lo);
-}
-
 // FP32 estimate of one surface value and a bound on its distance from the value tc_exact
 // returns. With nn, C = sum(chip), s1, s2, D exact integers, the value is
 //   ZNCC: (nn D - C s1) / (cnorm sqrt(nn) sqrt(nn s2 - s1^2)),  NCC: (nn D - C s1) / (cnorm nn sqrt(s2)).
-// The numerator and the variance are each formed with three roundings of relative size
-// u = 2^-24 on terms no larger than `tn` and `tv`, so their absolute errors are below
-// 3u tn and 3u tv; rsqrt (2 ulp), the scale and two products add < 6u relative, and the final
-// Float32 rounding of the reference 1u. The bound returned covers all of it with slack; NaN
-// marks a value whose variance is too small for the bound (evaluated exactly).
+// D and s2 are converted with one rounding each (s1 < 2^24 and C are exact). The numerator and
+// the variance are then formed with three roundings of relative size u = 2^-24 on terms no
+// larger than `tn` and `tv`, so their absolute errors are below 3u tn and 3u tv; rsqrt (2 ulp),
+// the scale `k` and two products add < 6u relative, and the final Float32 rounding of the
+// reference 1u. 1/vx is taken as r^2 (within 9u of it). The bound returned covers all of it
+// with more than 3x slack; NaN marks a value whose variance is too small for the bound
+// (evaluated exactly). `k7` is 7u k.
 __device__ __forceinline__ float tc_estimate(uint32_t D, uint32_t S1, uint32_t S2, float nnf,
-                                             float csum, float k, int measure, float* bound) {
-    const float d = u32_to_f(D), s1 = u32_to_f(S1), s2 = u32_to_f(S2);
+                                             float csum, float k, float k7, int measure,
+                                             float* bound) {
+    const float d = __uint2float_rn(D), s1 = __uint2float_rn(S1), s2 = __uint2float_rn(S2);
     const float p = __fmul_rn(csum, s1);
     const float nx = __fmaf_rn(nnf, d, -p);
     const float tn = __fmaf_rn(nnf, d, p);  // |nn D| + |C s1| (both non-negative)
@@ -643,16 +638,48 @@ __device__ __forceinline__ float tc_estimate(uint32_t D, uint32_t S1, uint32_t S
     const float r = rsqrtf(vx);
     const float est = __fmul_rn(__fmul_rn(nx, r), k);
     // |err| <= |est| (8u + ev / vx) + 3.5u tn r k  (u = 2^-24), doubled for slack.
-    const float rel = __fmaf_rn(ev, __frcp_rn(vx), 9.5367431640625e-07f);  // 16u + ev/vx
-    *bound = __fmaf_rn(fabsf(est), 2.0f * rel, 4.172325134277344e-07f * tn * r * k) + 1e-30f;
+    const float rel = __fmaf_rn(ev, __fmul_rn(r, r), 9.5367431640625e-07f);  // 16u + ev/vx
+    *bound = __fmaf_rn(fabsf(est), 2.0f * rel, __fmul_rn(__fmul_rn(tn, r), k7)) + 1e-30f;
     return est;
 }
 
+// Optional phase timer (compiled in with -DAR_TC_PHASES, for profiling builds only): thread 0
+// of each CTA accumulates clock64() cycles between the marks below, per phase, and adds them to
+// g_tc_phase at exit; entry 15 counts the points that reached the output phase.
+#ifdef AR_TC_PHASES
+__device__ unsigned long long g_tc_phase[16];
+#define TC_PHASE_INIT unsigned long long tcp_t = clock64(), tcp_acc[12] = {}, tcp_n = 0;
+#define TC_PHASE(n)                              \
+    if (tid == 0) {                              \
+        const unsigned long long t_ = clock64(); \
+        tcp_acc[n] += t_ - tcp_t;                \
+        tcp_t = t_;                              \
+    }
+#define TC_PHASE_POINT \
+    if (tid == 0) ++tcp_n;
+#define TC_PHASE_FLUSH                                                           \
+    if (tid == 0) {                                                              \
+        for (int n_ = 0; n_ < 12; ++n_) atomicAdd(&g_tc_phase[n_], tcp_acc[n_]); \
+        atomicAdd(&g_tc_phase[15], tcp_n);                                       \
+    }
+#else
+#define TC_PHASE_INIT
+#define TC_PHASE(n)
+#define TC_PHASE_POINT
+#define TC_PHASE_FLUSH
+#endif
+
+// REG: every surface of the pass has at most 64 rows and 64 columns (M = 64), so one 16x256b
+// read per warp covers it and each thread keeps its 16 numerators and upper bounds in
+// registers through both passes.
+template <bool REG>
 __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
     extern __shared__ __align__(1024) unsigned char smem_tc[];
     __shared__ uint64_t s_mbar;
     __shared__ uint32_t s_taddr;
     __shared__ int s_slot;
+    __shared__ int s_ncand;
+    __shared__ uint32_t s_pd[25];
     __shared__ float s_fmax[kTcThreads / 32];
     __shared__ unsigned long long s_isum[2][2];
     uint8_t* s_E = smem_tc + A.off_E;
@@ -690,11 +717,13 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
     for (int e = tid; e < A.CWM * A.PC; e += bd) s_P[e] = 0;
     int iter = 0;
     int dirty_ch = 0;
+    TC_PHASE_INIT
 
     for (int64_t k = blockIdx.x; k < A.pts.n; k += gridDim.x, ++iter) {
         tc::fence_before_sync();
         __syncthreads();  // the previous point's buffers and accumulator are no longer read
         tc::fence_after_sync();
+        TC_PHASE(0)
         // The chip sums of this iteration go to s_isum[ib]; the other buffer, last read
         // before the barrier above, is cleared for the next iteration.
         const int ib = iter & 1;
@@ -718,6 +747,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         const int nr = static_cast<int>(2 * pry), nc = static_cast<int>(2 * prx);
         if (ch <= 0 || cw <= 0) continue;
         if (ch > A.CHM || cw > A.CWM || nr > A.NRM || nc > A.NCM || nc > A.MT) continue;
+        TC_PHASE(1)
         const int64_t chip_r = cr0 - 1 - A.pady, chip_c = cc0 - 1 - A.padx;
         const int64_t win_r = wr0 - 1 - A.pady, win_c = wc0 - 1 - A.padx;
         const long long nnl = static_cast<long long>(ch) * cw;
@@ -774,6 +804,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             }
         }
         if (!__syncthreads_or(any)) continue;
+        TC_PHASE(2)
         if (tid == 0) A.out.searched[k] = 1;
 
         // prepare_chip! statistics. Power-of-two areas: every term of the reference's FP64
@@ -808,7 +839,10 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         }
         if (!(sq > __dmul_rn(__dmul_rn(DBL_EPSILON, static_cast<double>(ch)), static_cast<double>(cw))))
             continue;  // degenerate chip: searched, no measurement (src/track.jl:286)
+        TC_PHASE(3)
         const double cnorm = __dsqrt_rn(sq);
+        // The point is measured: its refinement slot is taken now, read after later barriers.
+        if (tid == 0 && !(A.up == 1 || nr < 5 || nc < 5)) s_slot = atomicAdd(A.sub_count, 1);
         const double nn = static_cast<double>(nnl);
 
         // Window blocks W'[16 q + r][x] (x < XS) from 16 image rows at base_r + 16 q, and the
@@ -847,6 +881,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             }
         }
         __syncthreads();  // s_P, s_W, s_T complete
+        TC_PHASE(4)
 
         // Box sums of W and W^2 (integral_both!, boxsum, src/integral.jl:141-170, 244-247) as
         // exact integers: V[i][x] sums ch rows down column x, S[j][i] sums cw columns of V.
@@ -945,18 +980,29 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                 if (__syncthreads_or(!ok)) break;
                 tc::fence_after_sync();
             }
-            // E: NB rows u = 16 - NB ... 15 per chip column, row u at (u - 16 + NB) * 16.
-            for (int e = tid; e < (b1 - b0) * A.NB; e += bd) {
-                const int bl = e / A.NB, b = b0 + bl, u = 16 - A.NB + e % A.NB;
-                const int src = b * A.PC + kPadL - u - static_cast<int>(delta);
-                const uint32_t* w = reinterpret_cast<const uint32_t*>(s_P + (src & ~3));
-                const uint32_t sh = static_cast<uint32_t>(src & 3) * 8u;
-                uint4 o;
-                o.x = __funnelshift_r(w[0], w[1], sh);
-                o.y = __funnelshift_r(w[1], w[2], sh);
-                o.z = __funnelshift_r(w[2], w[3], sh);
-                o.w = __funnelshift_r(w[3], w[4], sh);
-                *reinterpret_cast<uint4*>(s_E + bl * A.PS + (e % A.NB) * 16) = o;
+            // E: NB rows u = 16 - NB ... 15 per chip column, row u at e = u - 16 + NB: 16 bytes
+            // from chip row -u - delta. Consecutive threads take consecutive rows.
+            {
+                const int nrow = (b1 - b0) * A.NB;
+                int bl = tid / A.NB, e = tid - bl * A.NB;
+                const int sbl = bd / A.NB, se = bd - sbl * A.NB;
+                for (int t = tid; t < nrow; t += bd) {
+                    const int src = (b0 + bl) * A.PC + kPadL - 16 + A.NB - static_cast<int>(delta) - e;
+                    const uint32_t* w = reinterpret_cast<const uint32_t*>(s_P + (src & ~3));
+                    const uint32_t sh = static_cast<uint32_t>(src & 3) * 8u;
+                    uint4 o;
+                    o.x = __funnelshift_r(w[0], w[1], sh);
+                    o.y = __funnelshift_r(w[1], w[2], sh);
+                    o.z = __funnelshift_r(w[2], w[3], sh);
+                    o.w = __funnelshift_r(w[3], w[4], sh);
+                    *reinterpret_cast<uint4*>(s_E + bl * A.PS + e * 16) = o;
+                    bl += sbl;
+                    e += se;
+                    if (e >= A.NB) {
+                        e -= A.NB;
+                        ++bl;
+                    }
+                }
             }
             if (cc == 0 && warp < 4) {
                 // Clear the accumulator columns the products add into (one lane quarter each).
@@ -970,6 +1016,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             tc::fence_proxy_async_smem();
             tc::fence_before_sync();
             __syncthreads();
+            TC_PHASE(5)
             if (tid == kTcThreads - 32) {
                 tc::fence_after_sync();
                 const uint32_t sW = tc::smem_u32(s_W), sE = tc::smem_u32(s_E);
@@ -983,6 +1030,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                 tc::mma_commit(&s_mbar);
             }
             if (cc == 0 && !A.big && warp < 7) box_sums();
+            TC_PHASE(6)
         }
         if (ok) {
             // Wait for the last chunk's products (bounded; every thread polls the same phase).
@@ -995,6 +1043,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             break;
         }
         tc::fence_after_sync();
+        TC_PHASE(7)
 
         // Pass 1: numerators out of Tensor Memory, estimates and bounds, the largest lower bound.
         // Surface column j is accumulator row j (lane (j % 16) + 32 (j / 16) of the M = 64
@@ -1004,16 +1053,138 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         const float kk = __double2float_rn(
             A.measure == AR_NCC ? __drcp_rn(__dmul_rn(cnorm, nn))
                                 : __drcp_rn(__dmul_rn(cnorm, __dsqrt_rn(nn))));
+        const float kk7 = 4.172325134277344e-07f * kk;  // 7u k
         const float nnf = static_cast<float>(nnl);
         const float csf = static_cast<float>(csum_d);
         const int quarter = warp & 3, half = warp >> 2;
         const uint32_t col0 = static_cast<uint32_t>(A.NB - 16);
         float lmax = -INFINITY;
+        if constexpr (REG) {
+            // One read per warp: value v of this thread is surface row
+            // i = 32 half + 8 (v / 4) + 2 (lane % 4) + v % 2, column j = 16 quarter + lane / 4
+            // (+ 8 when v % 4 >= 2). Registers keep its numerator and its upper bound.
+            const int ib0 = 32 * half + 2 * (lane & 3);
+            const int jb0 = 16 * quarter + (lane >> 2);
+            uint32_t dv[16];
+            float upb[16];
+            uint32_t vm = 0u;  // values of this thread inside the surface
+            if (32 * half < nr) {
+                tc::tmem_ld16dp(taddr + (static_cast<uint32_t>(32 * quarter) << 16) + col0 +
+                                    static_cast<uint32_t>(32 * half), dv);
+                tc::tmem_wait_ld();
+#pragma unroll
+                for (int v = 0; v < 16; ++v) {
+                    const int i = ib0 + 8 * (v >> 2) + (v & 1), j = jb0 + ((v & 2) ? 8 : 0);
+                    upb[v] = -INFINITY;
+                    if (i < nr && j < nc) {
+                        vm |= 1u << v;
+                        const int o = j * A.NRS + i;
+                        float bnd;
+                        const float est = tc_estimate(dv[v], s_S1[o], s_S2[o], nnf, csf, kk, kk7,
+                                                      A.measure, &bnd);
+                        upb[v] = est + bnd;
+                        lmax = fmaxf(lmax, est - bnd);
+                    }
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(kFull, lmax, o));
+            if (lane == 0) s_fmax[warp] = lmax;
+            if (tid == 0) s_ncand = 0;
+            __syncthreads();
+            TC_PHASE(8)
+            float M = s_fmax[0];
+            for (int w = 1; w < kTcThreads / 32; ++w) M = fmaxf(M, s_fmax[w]);
+            // Pass 2: values whose upper bound reaches M (or whose estimate was not made) go to a
+            // list -- numerator and (row, column) -- and are normalised exactly, one per thread.
+            uint32_t* s_cD = s_num;
+            uint32_t* s_cI = reinterpret_cast<uint32_t*>(s_est);
+#pragma unroll
+            for (int v = 0; v < 16; ++v) {
+                if (((vm >> v) & 1u) && (upb[v] >= M || isnan(upb[v]))) {
+                    const int c = atomicAdd(&s_ncand, 1);
+                    s_cD[c] = dv[v];
+                    s_cI[c] = (static_cast<uint32_t>(ib0 + 8 * (v >> 2) + (v & 1)) << 16) |
+                              static_cast<uint32_t>(jb0 + ((v & 2) ? 8 : 0));
+                }
+            }
+            __syncthreads();
+            const int ncand = s_ncand;
+            unsigned long long best = 0ull;
+            for (int c = tid; c < ncand; c += bd) {
+                const int i = static_cast<int>(s_cI[c] >> 16), j = static_cast<int>(s_cI[c] & 0xFFFFu);
+                const int o = j * A.NRS + i;
+                const float x = tc_exact(s_cD[c], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+                const unsigned long long key = argmax_key(x, static_cast<unsigned>(i * nc + j));
+                best = key > best ? key : best;
+            }
+            best = block_max_u64(best, reinterpret_cast<unsigned long long*>(s_red));
+            TC_PHASE(9)
+            if (A.flops && tid == 0)
+                atomicAdd(A.flops, 2ull * static_cast<unsigned long long>(ch) * cw * nr * nc);
+            if (A.surf_out) {
+                // Every value exactly (diagnostic surfaces): numerators to shared memory first.
+#pragma unroll
+                for (int v = 0; v < 16; ++v)
+                    if ((vm >> v) & 1u)
+                        s_num[(jb0 + ((v & 2) ? 8 : 0)) * A.NRS + ib0 + 8 * (v >> 2) + (v & 1)] = dv[v];
+                __syncthreads();
+                float* so = A.surf_out + k * static_cast<int64_t>(A.NRM) * A.NCM;
+                for (int e = tid; e < nr * nc; e += bd) {
+                    const int o = (e / nr) * A.NRS + (e % nr);
+                    so[e] = tc_exact(s_num[o], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+                }
+            }
+            unsigned rm = 0;
+            float pv = 0.0f;
+            int pi = 0, pj = 0;
+            if (key_decode(best, &rm, &pv)) {
+                pi = static_cast<int>(rm / nc);
+                pj = static_cast<int>(rm % nc);
+            }
+            const bool single = A.up == 1 || nr < 5 || nc < 5;
+            // The numerators of the output: the peak, or the 5 x 5 patch (all inside the surface).
+            const int pi0 = single ? pi : min(max(pi - 2, 0), max(nr - 5, 0));
+            const int pj0 = single ? pj : min(max(pj - 2, 0), max(nc - 5, 0));
+            const int span = single ? 1 : 5;
+#pragma unroll
+            for (int v = 0; v < 16; ++v) {
+                const int a = ib0 + 8 * (v >> 2) + (v & 1) - pi0, b = jb0 + ((v & 2) ? 8 : 0) - pj0;
+                if (a >= 0 && a < span && b >= 0 && b < span && ((vm >> v) & 1u)) s_pd[b * 5 + a] = dv[v];
+            }
+            __syncthreads();
+            if (single) {
+                if (tid == 0) {
+                    const int o = pj * A.NRS + pi;
+                    A.out.dx[k] = __double2float_rn(
+                        __dadd_rn(static_cast<double>(pj - static_cast<int>(prx)), A.pts.dx0[k]));
+                    A.out.dy[k] = __double2float_rn(
+                        __dadd_rn(static_cast<double>(pi - static_cast<int>(pry)), A.pts.dy0[k]));
+                    A.out.corr[k] = tc_exact(s_pd[0], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+                }
+            } else {
+                const int slot = s_slot;
+                if (tid < 25) {
+                    const int a = tid % 5, b = tid / 5;
+                    const int o = (pj0 + b) * A.NRS + (pi0 + a);
+                    A.sub_patch[static_cast<int64_t>(slot) * 25 + tid] =
+                        tc_exact(s_pd[tid], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+                }
+                if (tid == 0) {
+                    A.sub_point[slot] = k;
+                    A.sub_origin[2 * slot] = pi0;
+                    A.sub_origin[2 * slot + 1] = pj0;
+                }
+            }
+            TC_PHASE(10)
+            TC_PHASE_POINT
+            continue;
+        }
         auto take = [&](uint32_t d, int i, int j) {
             if (j < nc && i < nr) {
                 const int o = j * A.NRS + i;
                 float bnd;
-                const float est = tc_estimate(d, s_S1[o], s_S2[o], nnf, csf, kk, A.measure, &bnd);
+                const float est = tc_estimate(d, s_S1[o], s_S2[o], nnf, csf, kk, kk7, A.measure, &bnd);
                 s_num[o] = d;
                 s_est[o] = est;
                 s_est[o + A.NCM * A.NRS] = bnd;
@@ -1046,6 +1217,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(kFull, lmax, o));
         if (lane == 0) s_fmax[warp] = lmax;
         __syncthreads();
+        TC_PHASE(8)
         float M = s_fmax[0];
         for (int w = 1; w < kTcThreads / 32; ++w) M = fmaxf(M, s_fmax[w]);
         // M: the largest lower bound of any value. A value whose upper bound is below it is
@@ -1064,6 +1236,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             }
         }
         best = block_max_u64(best, reinterpret_cast<unsigned long long*>(s_red));
+        TC_PHASE(9)
         if (A.flops && tid == 0)
             atomicAdd(A.flops, 2ull * static_cast<unsigned long long>(ch) * cw * nr * nc);
         if (A.surf_out) {
@@ -1093,8 +1266,6 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         } else {
             const int pi0 = min(max(pi - 2, 0), max(nr - 5, 0));
             const int pj0 = min(max(pj - 2, 0), max(nc - 5, 0));
-            if (tid == 0) s_slot = atomicAdd(A.sub_count, 1);
-            __syncthreads();
             const int slot = s_slot;
             if (tid < 25) {
                 const int a = tid % 5, b = tid / 5;
@@ -1109,6 +1280,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             }
         }
     }
+    TC_PHASE_FLUSH
     if (failed) {
         // Products may still be in flight: give them a bounded time before freeing the
         // accumulator.
@@ -1961,12 +2133,14 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         // 76 KB of shared memory each), otherwise one (at least 116 KB).
         const int per_sm_tc = TP.tmem_cols <= 256 && TP.smem <= 112 * 1024 ? 2 : 1;
         const size_t tc_smem = std::max<size_t>(TP.smem, per_sm_tc == 2 ? 76 * 1024 : 116 * 1024);
-        e = cudaFuncSetAttribute(k_corr_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        const bool reg = TP.MT == 64 && TP.NRM <= 64;
+        auto kern = reg ? k_corr_tc<true> : k_corr_tc<false>;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(tc_smem));
         if (e != cudaSuccess) return e;
         const int grid = static_cast<int>(
             std::max<int64_t>(1, std::min<int64_t>(pts.n, static_cast<int64_t>(num_sms) * per_sm_tc)));
-        k_corr_tc<<<grid, kTcThreads, tc_smem, stream>>>(B);
+        kern<<<grid, kTcThreads, tc_smem, stream>>>(B);
         e = cudaGetLastError();
     }
     const int per_sm = P.smem <= 100 * 1024 ? 2 : 1;
@@ -2193,3 +2367,14 @@ extern "C" int ar_track_device_static(const void* ref, const void* sec, const ui
     }
     return AR_OK;
 }
+
+#ifdef AR_TC_PHASES
+// Profiling builds only: the phase counters of k_corr_tc (16 entries), then cleared.
+extern "C" int ar_tc_phase_read(unsigned long long* out) {
+    cudaDeviceSynchronize();
+    if (cudaMemcpyFromSymbol(out, ar::g_tc_phase, 16 * sizeof(unsigned long long)) != cudaSuccess)
+        return 1;
+    const unsigned long long z[16] = {};
+    return cudaMemcpyToSymbol(ar::g_tc_phase, z, sizeof(z)) == cudaSuccess ? 0 : 1;
+}
+#endif

@@ -54,8 +54,8 @@ def scene(ar, n=N):
     return a, b, valid
 
 
-def pipeline_params(ar):
-    return ar.params(grid_spacing=SPACING, chip_size=CHIP, search_radius=RADIUS, upsampling=UP)
+def pipeline_params(ar, spacing=SPACING):
+    return ar.params(grid_spacing=spacing, chip_size=CHIP, search_radius=RADIUS, upsampling=UP)
 
 
 class ClockSampler:
@@ -276,7 +276,7 @@ def gpu_arm(args):
     ctx = L.Context(local)
     lib = ctx.lib
     a, b, valid = scene(ar, args.size)
-    p = pipeline_params(ar)
+    p = pipeline_params(ar, args.spacing if args.profile else SPACING)
     grid = ar.build_grid(a.shape, p)
     gr, gc = grid.shape
     n = gr * gc
@@ -340,9 +340,10 @@ def gpu_arm(args):
     levels = {int(c): int(np.count_nonzero(chip == c)) for c in np.unique(chip) if c}
     med_dx = float(np.nanmedian(dx)) if resolved else float("nan")
 
-    # Roofline of the dominant kernel (the correlation): algorithmic FLOPs counted by the
-    # kernel (2 * chip area * surface area per searched point) over its event-timed duration,
-    # summed over the step's correlation launches, against the measured cuBLAS FP32 rate.
+    # Roofline of the dominant kernel (the tensor-core correlation, k_corr_tc): algorithmic
+    # operations counted by the kernel (2 * chip area * surface area per searched point, the
+    # reference's direct numerator) over the event-timed duration of the step's correlation
+    # launches, against the measured dense bf16 tensor rate.
     achieved = corr_flops / (corr_ms * 1e-3) / 1e12 if corr_ms > 0 else None
     if args.profile:
         if rank == 0:
@@ -413,6 +414,13 @@ def gpu_arm(args):
                          f"{dt:.1f} s"}
 
     peaks = measured_peaks()
+    if peaks.get("bf16_tflops"):
+        tensor_peak = float(peaks["bf16_tflops"])
+        peak_source = ("MEASURED_PEAKS.json bf16_tflops (burst cuBLAS bf16 GEMM; each "
+                       "correlation launch is timed on its own); of measured")
+    else:
+        tensor_peak = 1590.0
+        peak_source = "fallback 1.59 PFLOP/s bf16 (no MEASURED_PEAKS.json); of fallback"
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -426,12 +434,17 @@ def gpu_arm(args):
                        "masks": "secondary no-data mask passed",
                        "l2": "flushed (256 MiB write) between steps",
                        "parallelism": f"{world} independent replicas", "median_dx": med_dx},
-            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": tensor_peak,
                          "unit": "TFLOP/s",
-                         "frac": achieved / fp32_peak if (achieved and fp32_peak) else None,
-                         "traffic": profile_traffic(fine_points), "kernel": "k_corr",
-                         "peak_source": "measured cuBLAS FP32 SGEMM (TF32 off) in this run; "
-                                        "no FP32 figure in MEASURED_PEAKS.json",
+                         "frac": achieved / tensor_peak if achieved else None,
+                         "traffic": profile_traffic(fine_points), "kernel": "k_corr_tc",
+                         "peak_source": peak_source,
+                         "achieved_basis": "2 * chip area * surface area per searched point "
+                                           "(integer MACs of the exact u8 numerator), summed "
+                                           "over the step's correlation launches",
+                         "fp32_comparison": {"sgemm_tflops_this_run": fp32_peak,
+                                             "frac": achieved / fp32_peak
+                                             if (achieved and fp32_peak) else None},
                          "kernel_ms_per_step": {"k_corr": corr_ms / args.steps,
                                                 "k_refine": refine_ms / args.steps},
                          "correlation_launches_per_step": tracks / args.steps,
@@ -512,7 +525,7 @@ def reference_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -524,6 +537,8 @@ def main():
                     help="image side; the benchmark line uses 4096, profiles a smaller scene")
     ap.add_argument("--profile", action="store_true",
                     help="time the device steps only (for ncu captures); no JSON bench line")
+    ap.add_argument("--spacing", type=int, default=SPACING,
+                    help="grid spacing of a --profile run (the benchmark line always uses 8)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
