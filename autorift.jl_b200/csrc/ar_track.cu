@@ -576,6 +576,7 @@ struct TcArgs {
     int MT;                          // MMA M: 64 or 128 surface columns
     int big;                         // 1: box sums before the products, chunks reuse their space
     unsigned off_E, off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
+    int XV;                          // k_corr_tc2: row stride (words) of the column sums V1, V2
     uint32_t tmem_cols;
     DevOutputs out;
     int* sub_count;
@@ -1292,6 +1293,534 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
 }
 
 // ----------------------------------------------------------------------------------------------
+// Tensor-core correlation, surfaces up to 64 x 64 with the chip operand whole (k_corr_tc2).
+//
+// The window is staged from its first row (no alignment offset; each 16-byte block of a column
+// comes from two aligned loads), so block q of 16 rows meets surface rows i in
+// [16 q - ch + 1, 16 q + 15]: NB = 16 * ceil((ch + 15) / 16) rows of the chip operand
+// E_b[u][r] = C[r - u, b] (u = 16 - NB ... 15) and accumulator columns [16 q, 16 q + NB), one
+// accumulator of at most 128 columns for chip 32 / radius 25. The box sums come from the 16-byte
+// window blocks: column sums V down ch rows per 16-row block of surface rows (dp4a for the
+// first, a sliding update for the rest), then row sums of V with 16-byte loads. Estimates stay
+// in registers; candidates and the patch get the reference's FP64 normalisation.
+
+// Sixteen bytes of column `c` from row r0 (zero outside the image): two aligned 16-byte loads
+// and a byte shift when they stay inside the image, otherwise byte by byte.
+__device__ __forceinline__ uint4 load_col16(const uint8_t* img, const uint8_t* img_end,
+                                            int64_t nrows, int64_t ncols, int64_t c, int64_t r0) {
+    if (c < 0 || c >= ncols) return make_uint4(0, 0, 0, 0);
+    const uint8_t* p = img + c * nrows + r0;
+    if (r0 >= 0 && r0 + 16 <= nrows) {
+        const uintptr_t pa = reinterpret_cast<uintptr_t>(p);
+        const uint32_t s = static_cast<uint32_t>(pa & 15);
+        const uint4* a = reinterpret_cast<const uint4*>(pa - s);
+        if (s == 0) return __ldg(a);
+        if (reinterpret_cast<const uint8_t*>(a) + 32 <= img_end) {
+            const uint4 lo = __ldg(a), hi = __ldg(a + 1);
+            const uint32_t w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+            uint32_t u[6], v[5];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) u[k] = (s & 8) ? w[k + 2] : w[k];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) v[k] = (s & 4) ? u[k + 1] : u[k];
+            const uint32_t sh = (s & 3) * 8u;
+            return make_uint4(__funnelshift_r(v[0], v[1], sh), __funnelshift_r(v[1], v[2], sh),
+                              __funnelshift_r(v[2], v[3], sh), __funnelshift_r(v[3], v[4], sh));
+        }
+    }
+    uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+        const int64_t r = r0 + t;
+        const uint32_t bb = (r >= 0 && r < nrows) ? p[t] : 0u;
+        w[t >> 2] |= bb << (8 * (t & 3));
+    }
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+__global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
+    extern __shared__ __align__(1024) unsigned char smem_tc[];
+    __shared__ uint64_t s_mbar;
+    __shared__ uint32_t s_taddr;
+    __shared__ int s_slot;
+    __shared__ int s_ncand;
+    __shared__ uint32_t s_pd[25];
+    __shared__ float s_fmax[kTcThreads / 32];
+    __shared__ unsigned long long s_isum[2][2];
+    uint8_t* s_E = smem_tc + A.off_E;
+    uint8_t* s_W = smem_tc + A.off_W;
+    uint8_t* s_P = smem_tc + A.off_P;
+    uint32_t* s_V1 = reinterpret_cast<uint32_t*>(smem_tc + A.off_V);
+    uint32_t* s_V2 = s_V1 + A.NRM * A.XV + 16;
+    uint32_t* s_S1 = reinterpret_cast<uint32_t*>(smem_tc + A.off_S1);
+    uint32_t* s_S2 = reinterpret_cast<uint32_t*>(smem_tc + A.off_S2);
+    uint32_t* s_num = reinterpret_cast<uint32_t*>(smem_tc + A.off_num);
+    uint32_t* s_cI = reinterpret_cast<uint32_t*>(smem_tc + A.off_est);
+    double* s_red = reinterpret_cast<double*>(smem_tc + A.off_red);
+
+    const int tid = threadIdx.x, bd = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = bd >> 5;
+    const int64_t NR = A.nrows + 2 * A.pady, NC = A.ncols + 2 * A.padx;
+    const double shx = static_cast<double>(A.padx) + 0.5;
+    const double shy = static_cast<double>(A.pady) + 0.5;
+    const uint8_t* ref_end = A.ref + A.nrows * A.ncols;
+
+    if (warp == 0) {
+        tc::tmem_alloc(&s_taddr, A.tmem_cols);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0) {
+        tc::mbar_init(&s_mbar, 1);
+        tc::fence_mbar_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t taddr = s_taddr;
+    uint32_t phase = 0;
+    bool failed = false;
+    if (tid < 4) s_isum[tid >> 1][tid & 1] = 0ull;
+    for (int e = tid; e < A.CWM * A.PC; e += bd) s_P[e] = 0;
+    int iter = 0;
+    int dirty_ch = 0;
+    TC_PHASE_INIT
+
+    for (int64_t k = blockIdx.x; k < A.pts.n; k += gridDim.x, ++iter) {
+        tc::fence_before_sync();
+        __syncthreads();  // the previous point's buffers and accumulators are no longer read
+        tc::fence_after_sync();
+        TC_PHASE(0)
+        const int ib = iter & 1;
+        if (tid < 2) s_isum[ib ^ 1][tid] = 0ull;
+        const int64_t prx = A.pts.rx[k], pry = A.pts.ry[k];
+        if (!(prx > 0 && pry > 0)) continue;
+        const double xs = A.pts.x[k] + shx, ys = A.pts.y[k] + shy;
+        const int64_t hx = A.pts.csx[k] / 2, hy = A.pts.csy[k] / 2;
+        const int64_t ccx = static_cast<int64_t>(floor(__dsub_rn(xs, A.pts.dx0[k])));
+        const int64_t ccy = static_cast<int64_t>(floor(__dsub_rn(ys, A.pts.dy0[k])));
+        const int64_t wcx = static_cast<int64_t>(floor(xs)), wcy = static_cast<int64_t>(floor(ys));
+        const int64_t cr0 = ccy - hy, cr1 = ccy + hy - 1, cc0 = ccx - hx, cc1 = ccx + hx - 1;
+        const int64_t wr0 = wcy - hy - pry, wr1 = wcy + hy + pry - 2;
+        const int64_t wc0 = wcx - hx - prx, wc1 = wcx + hx + prx - 2;
+        const bool chip_in = (cr1 < cr0 || cc1 < cc0) ||
+                             (cr0 >= 1 && cr1 <= NR && cc0 >= 1 && cc1 <= NC);
+        const bool win_in = (wr1 < wr0 || wc1 < wc0) ||
+                            (wr0 >= 1 && wr1 <= NR && wc0 >= 1 && wc1 <= NC);
+        if (!chip_in || !win_in) continue;
+        const int ch = static_cast<int>(2 * hy), cw = static_cast<int>(2 * hx);
+        const int nr = static_cast<int>(2 * pry), nc = static_cast<int>(2 * prx);
+        if (ch <= 0 || cw <= 0) continue;
+        if (ch > A.CHM || cw > A.CWM || nr > A.NRM || nc > A.NCM) continue;
+        TC_PHASE(1)
+        const int64_t chip_r = cr0 - 1 - A.pady, chip_c = cc0 - 1 - A.padx;
+        const int64_t win_r = wr0 - 1 - A.pady, win_c = wc0 - 1 - A.padx;
+        const long long nnl = static_cast<long long>(ch) * cw;
+        const bool pow2 = (nnl & (nnl - 1)) == 0 && nnl <= 4096;
+
+        // The chip as zero-padded byte columns, _any_valid over it (src/track.jl:416-421) and,
+        // for power-of-two areas, its exact integer sums (as in k_corr_tc).
+        int any = 0;
+        unsigned long long isum = 0ull, isq = 0ull;
+        if (ch < dirty_ch)
+            for (int b = warp; b < A.CWM; b += nwarps)
+                for (int a = ch + lane; a < dirty_ch; a += 32) s_P[b * A.PC + kPadL + a] = 0;
+        dirty_ch = ch;
+        for (int a0 = 0; a0 < ch; a0 += 32) {
+            const int a = a0 + lane;
+            const int64_t r = chip_r + a;
+            const bool rin = a < ch && r >= 0 && r < A.nrows;
+            constexpr int kU = 4;
+            for (int b0 = warp; b0 < cw; b0 += kU * nwarps) {
+                uint32_t v[kU], m[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int b = b0 + u * nwarps;
+                    const int64_t c = chip_c + b;
+                    const bool in = rin && b < cw && c >= 0 && c < A.ncols;
+                    v[u] = in ? A.sec[r + c * A.nrows] : 0u;
+                    m[u] = in ? A.valid[r + c * A.nrows] : 0u;
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int b = b0 + u * nwarps;
+                    if (a < ch && b < cw) {
+                        s_P[b * A.PC + kPadL + a] = static_cast<uint8_t>(v[u]);
+                        any |= m[u];
+                        isum += v[u];
+                        isq += v[u] * v[u];
+                    }
+                }
+            }
+        }
+        if (pow2) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                isum += __shfl_xor_sync(kFull, isum, o);
+                isq += __shfl_xor_sync(kFull, isq, o);
+            }
+            if (lane == 0) {
+                atomicAdd(&s_isum[ib][0], isum);
+                atomicAdd(&s_isum[ib][1], isq);
+            }
+        }
+        if (!__syncthreads_or(any)) continue;
+        TC_PHASE(2)
+        if (tid == 0) A.out.searched[k] = 1;
+
+        double mean, sq, csum_d;
+        if (pow2) {
+            const long long cs = static_cast<long long>(s_isum[ib][0]);
+            const long long c2 = static_cast<long long>(s_isum[ib][1]);
+            csum_d = static_cast<double>(cs);
+            mean = __ddiv_rn(csum_d, static_cast<double>(nnl));
+            sq = __ddiv_rn(static_cast<double>(nnl * c2 - cs * cs), static_cast<double>(nnl));
+        } else {
+            double st[1] = {0.0};
+            for (int e = tid; e < ch * cw; e += bd)
+                st[0] = __dadd_rn(st[0], pixel(A.sec, A.nrows, A.ncols, chip_r + e % ch, chip_c + e / ch));
+            block_sum_f64<1>(st, s_red);
+            csum_d = st[0];
+            mean = __ddiv_rn(st[0], static_cast<double>(nnl));
+            const int chp = (ch + kUA - 1) & ~(kUA - 1);
+            double acc2[1] = {0.0};
+            for (int e = tid; e < chp * cw; e += bd) {
+                const int a = e % chp, b = e / chp;
+                if (a < ch) {
+                    const double v = pixel(A.sec, A.nrows, A.ncols, chip_r + a, chip_c + b);
+                    const double d = __dsub_rn(v, mean);
+                    acc2[0] = __dadd_rn(acc2[0], __dmul_rn(d, d));
+                }
+            }
+            block_sum_f64<1>(acc2, s_red);
+            sq = acc2[0];
+        }
+        if (!(sq > __dmul_rn(__dmul_rn(DBL_EPSILON, static_cast<double>(ch)), static_cast<double>(cw))))
+            continue;  // degenerate chip: searched, no measurement (src/track.jl:286)
+        TC_PHASE(3)
+        const double cnorm = __dsqrt_rn(sq);
+        if (tid == 0 && !(A.up == 1 || nr < 5 || nc < 5)) s_slot = atomicAdd(A.sub_count, 1);
+        const double nn = static_cast<double>(nnl);
+
+        // Window blocks W[16 q + r][x] (x < XS) from the window's first row.
+        const int Q = (ch + nr - 1 + 15) / 16;
+        const int XW = cw + nc - 1;
+        for (int q = warp; q < Q; q += nwarps)
+            for (int x = lane; x < A.XS; x += 32)
+                *reinterpret_cast<uint4*>(s_W + q * A.QS + x * 16) =
+                    load_col16(A.ref, ref_end, A.nrows, A.ncols, win_c + x, win_r + 16 * q);
+        // E: NB rows per chip column, row e (u = e - NB + 16) = 16 bytes from chip row -u.
+        {
+            const int nrow = cw * A.NB;
+            int bl = tid / A.NB, e = tid - bl * A.NB;
+            const int sbl = bd / A.NB, se = bd - sbl * A.NB;
+            for (int t = tid; t < nrow; t += bd) {
+                const int src = bl * A.PC + kPadL - 16 + A.NB - e;
+                const uint32_t* w = reinterpret_cast<const uint32_t*>(s_P + (src & ~3));
+                const uint32_t sh = static_cast<uint32_t>(src & 3) * 8u;
+                uint4 o;
+                o.x = __funnelshift_r(w[0], w[1], sh);
+                o.y = __funnelshift_r(w[1], w[2], sh);
+                o.z = __funnelshift_r(w[2], w[3], sh);
+                o.w = __funnelshift_r(w[3], w[4], sh);
+                *reinterpret_cast<uint4*>(s_E + bl * A.PS + e * 16) = o;
+                bl += sbl;
+                e += se;
+                if (e >= A.NB) {
+                    e -= A.NB;
+                    ++bl;
+                }
+            }
+        }
+        const int dcols = 16 * (Q - 1) + A.NB;
+        if (warp < 4) {
+            // Clear the columns the products add into (one lane quarter per warp).
+            uint32_t z[16];
+#pragma unroll
+            for (int t = 0; t < 16; ++t) z[t] = 0u;
+            const uint32_t lq = taddr + (static_cast<uint32_t>(32 * warp) << 16);
+            for (int c = 0; c < dcols; c += 16) tc::tmem_st16(lq + static_cast<uint32_t>(c), z);
+            tc::tmem_wait_st();
+        }
+        tc::fence_proxy_async_smem();
+        tc::fence_before_sync();
+        __syncthreads();  // s_P, s_W, s_E complete; accumulator cleared
+        TC_PHASE(4)
+        if (tid == kTcThreads - 32) {
+            tc::fence_after_sync();
+            const uint32_t idesc = tc::idesc_u8_s32(64, A.NB);
+            // Descriptors advance by adding to their start-address field (16-byte units; shared
+            // addresses stay below 2^18, so the field never carries).
+            const uint64_t da0 = tc::smem_desc(tc::smem_u32(s_W), 16, 128);
+            const uint64_t db0 = tc::smem_desc(tc::smem_u32(s_E), A.PS, 128);
+            const uint64_t dstep_b = static_cast<uint64_t>(2 * A.PS) >> 4;
+            for (int q = 0; q < Q; ++q) {
+                uint64_t da = da0 + (static_cast<uint64_t>(q * A.QS) >> 4);
+                uint64_t db = db0;
+                const uint32_t dn = taddr + static_cast<uint32_t>(16 * q);
+                for (int t = 0; t < cw / 2; ++t) {
+                    tc::mma_u8(dn, da, db, idesc, true);
+                    da += 2;
+                    db += dstep_b;
+                }
+            }
+            tc::mma_commit(&s_mbar);
+        }
+        TC_PHASE(5)
+        if (warp < 7) {
+            // Box sums of W and W^2 (integral_both!, boxsum, src/integral.jl:141-170, 244-247)
+            // as exact integers, warps 0-6 (named barrier 1) while warp 7 issues the products.
+            constexpr int kBT = kTcThreads - 32;
+            // V[i][x] = sums over rows i .. i + ch - 1 of column x: a task is a column and the 16
+            // rows i of one block; its outgoing rows are that block, its incoming rows start ch
+            // rows lower.
+            const int nseg = (nr + 15) >> 4;
+            const int chb = ch >> 4, chr = ch & 15;
+            for (int task = tid; task < XW * nseg; task += kBT) {
+                const int sgi = task / XW, x = task - sgi * XW;
+                const int i0 = 16 * sgi;
+                const uint8_t* colx = s_W + x * 16;
+                const uint4 bo = *reinterpret_cast<const uint4*>(colx + sgi * A.QS);
+                uint32_t h1 = 0, h2 = 0;
+                for (int bb = 0; bb < chb; ++bb) {
+                    const uint4 w = *reinterpret_cast<const uint4*>(colx + (sgi + bb) * A.QS);
+                    h1 = __dp4a(w.x, 0x01010101u, h1);
+                    h1 = __dp4a(w.y, 0x01010101u, h1);
+                    h1 = __dp4a(w.z, 0x01010101u, h1);
+                    h1 = __dp4a(w.w, 0x01010101u, h1);
+                    h2 = __dp4a(w.x, w.x, h2);
+                    h2 = __dp4a(w.y, w.y, h2);
+                    h2 = __dp4a(w.z, w.z, h2);
+                    h2 = __dp4a(w.w, w.w, h2);
+                }
+                const uint4 bi = *reinterpret_cast<const uint4*>(colx + (sgi + chb) * A.QS);
+                if (chr) {
+                    const uint32_t wv[4] = {bi.x, bi.y, bi.z, bi.w};
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        const int keep = min(max(chr - 4 * m, 0), 4);
+                        const uint32_t mk = keep == 4 ? 0xffffffffu : ((1u << (8 * keep)) - 1u);
+                        h1 = __dp4a(wv[m] & mk, 0x01010101u, h1);
+                        h2 = __dp4a(wv[m] & mk, wv[m], h2);
+                    }
+                }
+                const uint32_t wo[4] = {bo.x, bo.y, bo.z, bo.w};
+                const uint32_t wi[4] = {bi.x, bi.y, bi.z, bi.w};
+                uint32_t* v1o = s_V1 + i0 * A.XV + x;
+                uint32_t* v2o = s_V2 + i0 * A.XV + x;
+#pragma unroll
+                for (int u = 0; u < 16; ++u) {
+                    if (i0 + u < nr) {
+                        v1o[u * A.XV] = h1;
+                        v2o[u * A.XV] = h2;
+                        const uint32_t o = (wo[u >> 2] >> (8 * (u & 3))) & 0xffu;
+                        uint32_t in;
+                        if (chr == 0) {
+                            in = (wi[u >> 2] >> (8 * (u & 3))) & 0xffu;
+                        } else {
+                            const int R = i0 + u + ch;
+                            in = colx[(R >> 4) * A.QS + (R & 15)];
+                        }
+                        h1 = h1 + in - o;
+                        h2 = h2 + in * in - o * o;
+                    }
+                }
+            }
+            asm volatile("bar.sync 1, %0;" ::"r"(kBT) : "memory");
+            // S[j][i] = sums of V[i][j .. j + cw - 1]: a task is a row i and 16 columns j.
+            const int jseg = (nc + 15) >> 4;
+            const bool vec = (cw & 3) == 0;
+            for (int task = tid; task < nr * jseg; task += kBT) {
+                const int sg = task / nr, i = task - sg * nr;
+                const int j0 = 16 * sg;
+                const uint32_t* r1 = s_V1 + i * A.XV;
+                const uint32_t* r2 = s_V2 + i * A.XV;
+                uint32_t g1 = 0, g2 = 0;
+                int bb = 0;
+                for (; bb + 4 <= cw; bb += 4) {
+                    const uint4 v = *reinterpret_cast<const uint4*>(r1 + j0 + bb);
+                    const uint4 w = *reinterpret_cast<const uint4*>(r2 + j0 + bb);
+                    g1 += (v.x + v.y) + (v.z + v.w);
+                    g2 += (w.x + w.y) + (w.z + w.w);
+                }
+                for (; bb < cw; ++bb) {
+                    g1 += r1[j0 + bb];
+                    g2 += r2[j0 + bb];
+                }
+#pragma unroll
+                for (int u4 = 0; u4 < 16; u4 += 4) {
+                    const uint4 o1 = *reinterpret_cast<const uint4*>(r1 + j0 + u4);
+                    const uint4 o2 = *reinterpret_cast<const uint4*>(r2 + j0 + u4);
+                    uint4 i1, i2;
+                    if (vec) {
+                        i1 = *reinterpret_cast<const uint4*>(r1 + j0 + u4 + cw);
+                        i2 = *reinterpret_cast<const uint4*>(r2 + j0 + u4 + cw);
+                    } else {
+                        const uint32_t* p1 = r1 + j0 + u4 + cw;
+                        const uint32_t* p2 = r2 + j0 + u4 + cw;
+                        i1 = make_uint4(p1[0], p1[1], p1[2], p1[3]);
+                        i2 = make_uint4(p2[0], p2[1], p2[2], p2[3]);
+                    }
+                    const uint32_t oo1[4] = {o1.x, o1.y, o1.z, o1.w}, ii1[4] = {i1.x, i1.y, i1.z, i1.w};
+                    const uint32_t oo2[4] = {o2.x, o2.y, o2.z, o2.w}, ii2[4] = {i2.x, i2.y, i2.z, i2.w};
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        const int j = j0 + u4 + m;
+                        if (j < nc) {
+                            s_S1[j * A.NRS + i] = g1;
+                            s_S2[j * A.NRS + i] = g2;
+                            g1 = g1 + ii1[m] - oo1[m];
+                            g2 = g2 + ii2[m] - oo2[m];
+                        }
+                    }
+                }
+            }
+        }
+        TC_PHASE(6)
+        bool ok = tc::mbar_wait(&s_mbar, phase, kTcWaitPolls);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicExch(A.status, 1);
+            failed = true;
+            break;
+        }
+        tc::fence_after_sync();
+        TC_PHASE(7)
+
+        // Pass 1: numerators out of Tensor Memory (one 16x256b read per warp), box sums from
+        // shared memory; estimates and upper bounds stay in registers. Value v
+        // of a thread is surface row i = 32 half + 8 (v / 4) + 2 (lane % 4) + v % 2, column
+        // j = 16 quarter + lane / 4 (+ 8 when v % 4 >= 2).
+        const float kk = __double2float_rn(
+            A.measure == AR_NCC ? __drcp_rn(__dmul_rn(cnorm, nn))
+                                : __drcp_rn(__dmul_rn(cnorm, __dsqrt_rn(nn))));
+        const float kk7 = 4.172325134277344e-07f * kk;  // 7u k
+        const float nnf = static_cast<float>(nnl);
+        const float csf = static_cast<float>(csum_d);
+        const int quarter = warp & 3, half = warp >> 2;
+        const uint32_t col0 = static_cast<uint32_t>(A.NB - 16);
+        const int ib0 = 32 * half + 2 * (lane & 3);
+        const int jb0 = 16 * quarter + (lane >> 2);
+        uint32_t dv[16];
+        float upb[16];
+        uint32_t vm = 0u;
+        float lmax = -INFINITY;
+        if (32 * half < nr) {
+            const uint32_t base = taddr + (static_cast<uint32_t>(32 * quarter) << 16) + col0 +
+                                  static_cast<uint32_t>(32 * half);
+            tc::tmem_ld16dp(base, dv);
+            tc::tmem_wait_ld();
+#pragma unroll
+            for (int v = 0; v < 16; ++v) {
+                const int i = ib0 + 8 * (v >> 2) + (v & 1), j = jb0 + ((v & 2) ? 8 : 0);
+                upb[v] = -INFINITY;
+                if (i < nr && j < nc) {
+                    vm |= 1u << v;
+                    float bnd;
+                    const int o = j * A.NRS + i;
+                    const float est = tc_estimate(dv[v], s_S1[o], s_S2[o], nnf, csf, kk, kk7,
+                                                  A.measure, &bnd);
+                    upb[v] = est + bnd;
+                    lmax = fmaxf(lmax, est - bnd);
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(kFull, lmax, o));
+        if (lane == 0) s_fmax[warp] = lmax;
+        if (tid == 0) s_ncand = 0;
+        __syncthreads();
+        TC_PHASE(8)
+        float M = s_fmax[0];
+        for (int w = 1; w < kTcThreads / 32; ++w) M = fmaxf(M, s_fmax[w]);
+        // Pass 2: values whose upper bound reaches M (or whose estimate was not made) go to a
+        // list and are normalised exactly, one per thread.
+#pragma unroll
+        for (int v = 0; v < 16; ++v) {
+            if (((vm >> v) & 1u) && (upb[v] >= M || isnan(upb[v]))) {
+                const int c = atomicAdd(&s_ncand, 1);
+                s_num[c] = dv[v];
+                s_cI[c] = (static_cast<uint32_t>(ib0 + 8 * (v >> 2) + (v & 1)) << 16) |
+                          static_cast<uint32_t>(jb0 + ((v & 2) ? 8 : 0));
+            }
+        }
+        __syncthreads();
+        const int ncand = s_ncand;
+        unsigned long long best = 0ull;
+        for (int c = tid; c < ncand; c += bd) {
+            const int i = static_cast<int>(s_cI[c] >> 16), j = static_cast<int>(s_cI[c] & 0xFFFFu);
+            const int o = j * A.NRS + i;
+            const float x = tc_exact(s_num[c], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+            const unsigned long long key = argmax_key(x, static_cast<unsigned>(i * nc + j));
+            best = key > best ? key : best;
+        }
+        best = block_max_u64(best, reinterpret_cast<unsigned long long*>(s_red));
+        TC_PHASE(9)
+        if (A.flops && tid == 0)
+            atomicAdd(A.flops, 2ull * static_cast<unsigned long long>(ch) * cw * nr * nc);
+        if (A.surf_out) {
+            // Every value exactly (diagnostic surfaces): numerators to shared memory first.
+#pragma unroll
+            for (int v = 0; v < 16; ++v)
+                if ((vm >> v) & 1u)
+                    s_num[(jb0 + ((v & 2) ? 8 : 0)) * A.NRS + ib0 + 8 * (v >> 2) + (v & 1)] = dv[v];
+            __syncthreads();
+            float* so = A.surf_out + k * static_cast<int64_t>(A.NRM) * A.NCM;
+            for (int e = tid; e < nr * nc; e += bd) {
+                const int o = (e / nr) * A.NRS + (e % nr);
+                so[e] = tc_exact(s_num[o], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+            }
+        }
+        unsigned rm = 0;
+        float pv = 0.0f;
+        int pi = 0, pj = 0;
+        if (key_decode(best, &rm, &pv)) {
+            pi = static_cast<int>(rm / nc);
+            pj = static_cast<int>(rm % nc);
+        }
+        const bool single = A.up == 1 || nr < 5 || nc < 5;
+        const int pi0 = single ? pi : min(max(pi - 2, 0), max(nr - 5, 0));
+        const int pj0 = single ? pj : min(max(pj - 2, 0), max(nc - 5, 0));
+        const int span = single ? 1 : 5;
+#pragma unroll
+        for (int v = 0; v < 16; ++v) {
+            const int a = ib0 + 8 * (v >> 2) + (v & 1) - pi0, b = jb0 + ((v & 2) ? 8 : 0) - pj0;
+            if (a >= 0 && a < span && b >= 0 && b < span && ((vm >> v) & 1u)) s_pd[b * 5 + a] = dv[v];
+        }
+        __syncthreads();
+        if (single) {
+            if (tid == 0) {
+                A.out.dx[k] = __double2float_rn(
+                    __dadd_rn(static_cast<double>(pj - static_cast<int>(prx)), A.pts.dx0[k]));
+                A.out.dy[k] = __double2float_rn(
+                    __dadd_rn(static_cast<double>(pi - static_cast<int>(pry)), A.pts.dy0[k]));
+                const int o = pj * A.NRS + pi;
+                A.out.corr[k] = tc_exact(s_pd[0], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+            }
+        } else {
+            const int slot = s_slot;
+            if (tid < 25) {
+                const int a = tid % 5, b = tid / 5;
+                const int o = (pj0 + b) * A.NRS + (pi0 + a);
+                A.sub_patch[static_cast<int64_t>(slot) * 25 + tid] =
+                    tc_exact(s_pd[tid], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+            }
+            if (tid == 0) {
+                A.sub_point[slot] = k;
+                A.sub_origin[2 * slot] = pi0;
+                A.sub_origin[2 * slot + 1] = pj0;
+            }
+        }
+        TC_PHASE(10)
+        TC_PHASE_POINT
+    }
+    TC_PHASE_FLUSH
+    if (failed) tc::mbar_wait(&s_mbar, phase ^ 1u, kTcWaitPolls);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(taddr, A.tmem_cols);
+}
+
+// ----------------------------------------------------------------------------------------------
 // Sub-pixel cascade kernel (src/peak.jl:456-522 from the patch onward), one warp per patch.
 //
 // Levels 1 and 2 of the cascade (10^2, 20^2) are materialised in the warp's shared memory. Up to
@@ -1789,9 +2318,69 @@ RefinePlan plan_refine(int up) {
 struct TcPlan {
     int NB, QM, QS, PS, PC, XS, XT, NRS, NRM, NCM, CHM, CWM, BC, big, MT;
     unsigned off_E, off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
+    int XV = 0;
     uint32_t tmem_cols;
     size_t smem;
 };
+
+// Shared-memory and Tensor Memory plan of k_corr_tc2 for a pass's largest geometry; false when
+// the pass does not fit it (surfaces beyond 64 x 64, chip operand larger than shared memory,
+// accumulator beyond 512 columns).
+bool plan_corr_tc2(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
+    const int ch = static_cast<int>(g.max_ch), cw = static_cast<int>(g.max_cw);
+    const int nr = static_cast<int>(g.max_nr), nc = static_cast<int>(g.max_nc);
+    if (nc > 64 || nr > 64 || nr < 1 || nc < 1 || cw < 2 || ch < 2 || (cw & 1)) return false;
+    P->CHM = ch;
+    P->CWM = cw;
+    P->NRM = nr;
+    P->NCM = nc;
+    P->MT = 64;
+    P->NB = round_up(ch + 15, 16);
+    if (P->NB > 256) return false;
+    P->QM = (ch + nr - 1 + 15) / 16;
+    P->PS = P->NB * 16;
+    P->XS = 64 + cw;
+    P->QS = P->XS * 16;
+    P->XT = 0;
+    P->PC = round_up(kPadL + P->NB + 20, 16);
+    P->NRS = nr | 1;
+    P->XV = round_up(cw + nc - 1, 32) + 4;
+    const int dcols = 16 * (P->QM - 1) + P->NB;
+    const int reads = P->NB - 16 + 32 * ((nr + 31) / 32);  // columns the epilogue reads
+    uint32_t t1 = 32;
+    while (static_cast<int>(t1) < std::max(dcols, reads)) t1 <<= 1;
+    if (t1 > 512) return false;
+    P->tmem_cols = t1;
+    auto a16 = [](size_t v) { return (v + 15) & ~size_t(15); };
+    const size_t Eb = static_cast<size_t>(cw) * P->PS;
+    const size_t Wb = static_cast<size_t>(P->QM) * P->QS;
+    const size_t Pb = a16(static_cast<size_t>(cw) * P->PC);
+    const size_t Vb = a16(2 * (static_cast<size_t>(nr) * P->XV + 16) * 4);
+    const size_t nbytes = a16(static_cast<size_t>(nc) * P->NRS * 4);
+    // [E][W][P][V1, V2 | candidate numerators and indices][S1][S2][red]
+    size_t off = 0;
+    P->off_E = 0;
+    off += Eb;
+    P->off_W = static_cast<unsigned>(off);
+    off += Wb;
+    P->off_P = static_cast<unsigned>(off);
+    off += Pb;
+    P->off_V = static_cast<unsigned>(off);
+    P->off_num = P->off_V;
+    P->off_est = static_cast<unsigned>(off + nbytes);
+    off += std::max(Vb, 2 * nbytes);
+    P->off_S1 = static_cast<unsigned>(off);
+    off += nbytes;
+    P->off_S2 = static_cast<unsigned>(off);
+    off += nbytes;
+    P->off_red = static_cast<unsigned>(off);
+    off += 3 * 32 * 8;
+    P->off_T = 0;
+    P->BC = cw;
+    P->big = 0;
+    P->smem = off;
+    return off <= smem_cap;
+}
 
 // Shared-memory plan of k_corr_tc for a pass's largest geometry; false when the pass does not
 // fit the kernel (surface wider than 64 columns, more than 256 rows, chips taller than 226).
@@ -2080,8 +2669,10 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         cudaEventRecord(ev0, stream);
     }
     TcPlan TP{};
-    const bool use_tc = dtype == AR_U8 && scratch.tensor_cores &&
-                        plan_corr_tc(geom, 220 * 1024, &TP);
+    const bool tc_ok = dtype == AR_U8 && scratch.tensor_cores;
+    // k_corr_tc2 where it keeps two CTAs per SM; otherwise k_corr_tc.
+    const bool use_tc2 = tc_ok && plan_corr_tc2(geom, 112 * 1024, &TP) && TP.tmem_cols <= 256;
+    const bool use_tc = tc_ok && (use_tc2 || plan_corr_tc(geom, 220 * 1024, &TP));
     if (use_tc) {
         TcArgs B{};
         B.ref = static_cast<const uint8_t*>(ref);
@@ -2119,6 +2710,7 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         B.off_num = TP.off_num;
         B.off_est = TP.off_est;
         B.off_red = TP.off_red;
+        B.XV = TP.XV;
         B.tmem_cols = TP.tmem_cols;
         B.out = out;
         B.sub_count = scratch.sub_count;
@@ -2134,7 +2726,7 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         const int per_sm_tc = TP.tmem_cols <= 256 && TP.smem <= 112 * 1024 ? 2 : 1;
         const size_t tc_smem = std::max<size_t>(TP.smem, per_sm_tc == 2 ? 76 * 1024 : 116 * 1024);
         const bool reg = TP.MT == 64 && TP.NRM <= 64;
-        auto kern = reg ? k_corr_tc<true> : k_corr_tc<false>;
+        auto kern = use_tc2 ? k_corr_tc2 : reg ? k_corr_tc<true> : k_corr_tc<false>;
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(tc_smem));
         if (e != cudaSuccess) return e;
