@@ -1304,28 +1304,35 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
 // first, a sliding update for the rest), then row sums of V with 16-byte loads. Estimates stay
 // in registers; candidates and the patch get the reference's FP64 normalisation.
 
-// Sixteen bytes of column `c` from row r0 (zero outside the image): two aligned 16-byte loads
-// and a byte shift when they stay inside the image, otherwise byte by byte.
-__device__ __forceinline__ uint4 load_col16(const uint8_t* img, const uint8_t* img_end,
-                                            int64_t nrows, int64_t ncols, int64_t c, int64_t r0) {
-    if (c < 0 || c >= ncols) return make_uint4(0, 0, 0, 0);
+// Sixteen bytes of column `c` from row r0 (zero outside the image), in two steps so that a
+// thread can have several in flight: col16_issue starts the loads -- two aligned 16-byte loads
+// when they stay inside the image, else byte by byte -- and col16_finish shifts the bytes into
+// place.
+struct Col16 {
+    uint4 lo, hi;
+    uint32_t s;  // byte offset of row r0 in `lo` (0: `lo` is the result)
+};
+
+__device__ __forceinline__ Col16 col16_issue(const uint8_t* img, const uint8_t* img_end,
+                                             int64_t nrows, int64_t ncols, int64_t c, int64_t r0) {
+    Col16 L;
+    L.s = 0;
+    L.lo = L.hi = make_uint4(0, 0, 0, 0);
+    if (c < 0 || c >= ncols) return L;
     const uint8_t* p = img + c * nrows + r0;
     if (r0 >= 0 && r0 + 16 <= nrows) {
         const uintptr_t pa = reinterpret_cast<uintptr_t>(p);
         const uint32_t s = static_cast<uint32_t>(pa & 15);
         const uint4* a = reinterpret_cast<const uint4*>(pa - s);
-        if (s == 0) return __ldg(a);
+        if (s == 0) {
+            L.lo = __ldg(a);
+            return L;
+        }
         if (reinterpret_cast<const uint8_t*>(a) + 32 <= img_end) {
-            const uint4 lo = __ldg(a), hi = __ldg(a + 1);
-            const uint32_t w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
-            uint32_t u[6], v[5];
-#pragma unroll
-            for (int k = 0; k < 6; ++k) u[k] = (s & 8) ? w[k + 2] : w[k];
-#pragma unroll
-            for (int k = 0; k < 5; ++k) v[k] = (s & 4) ? u[k + 1] : u[k];
-            const uint32_t sh = (s & 3) * 8u;
-            return make_uint4(__funnelshift_r(v[0], v[1], sh), __funnelshift_r(v[1], v[2], sh),
-                              __funnelshift_r(v[2], v[3], sh), __funnelshift_r(v[3], v[4], sh));
+            L.lo = __ldg(a);
+            L.hi = __ldg(a + 1);
+            L.s = s;
+            return L;
         }
     }
     uint32_t w[4] = {0, 0, 0, 0};
@@ -1335,7 +1342,67 @@ __device__ __forceinline__ uint4 load_col16(const uint8_t* img, const uint8_t* i
         const uint32_t bb = (r >= 0 && r < nrows) ? p[t] : 0u;
         w[t >> 2] |= bb << (8 * (t & 3));
     }
-    return make_uint4(w[0], w[1], w[2], w[3]);
+    L.lo = make_uint4(w[0], w[1], w[2], w[3]);
+    return L;
+}
+
+__device__ __forceinline__ uint4 col16_finish(const Col16& L) {
+    const uint32_t s = L.s;
+    if (s == 0) return L.lo;
+    const uint32_t w[8] = {L.lo.x, L.lo.y, L.lo.z, L.lo.w, L.hi.x, L.hi.y, L.hi.z, L.hi.w};
+    uint32_t u[6], v[5];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) u[k] = (s & 8) ? w[k + 2] : w[k];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) v[k] = (s & 4) ? u[k + 1] : u[k];
+    const uint32_t sh = (s & 3) * 8u;
+    return make_uint4(__funnelshift_r(v[0], v[1], sh), __funnelshift_r(v[1], v[2], sh),
+                      __funnelshift_r(v[2], v[3], sh), __funnelshift_r(v[3], v[4], sh));
+}
+
+// A point's chip and window placement (src/points.jl:358-395 with the pass's padding and the
+// +0.5 shift, src/track.jl:128-138, 207-220) and whether it is searched at all.
+struct PtGeo {
+    long long k, chip_r, chip_c, win_r, win_c;
+    int ch, cw, nr, nc, prx, pry, ok;
+};
+
+__device__ __forceinline__ void pt_geometry(const TcArgs& A, int64_t k, PtGeo& g) {
+    // All eight fields are loaded before any is used.
+    const int64_t prx = A.pts.rx[k], pry = A.pts.ry[k];
+    const double x = A.pts.x[k], y = A.pts.y[k], dx0 = A.pts.dx0[k], dy0 = A.pts.dy0[k];
+    const int64_t csx = A.pts.csx[k], csy = A.pts.csy[k];
+    const int64_t NR = A.nrows + 2 * A.pady, NC = A.ncols + 2 * A.padx;
+    g.k = k;
+    g.ok = 0;
+    if (!(prx > 0 && pry > 0)) return;
+    const double xs = x + (static_cast<double>(A.padx) + 0.5);
+    const double ys = y + (static_cast<double>(A.pady) + 0.5);
+    const int64_t hx = csx / 2, hy = csy / 2;
+    const int64_t ccx = static_cast<int64_t>(floor(__dsub_rn(xs, dx0)));
+    const int64_t ccy = static_cast<int64_t>(floor(__dsub_rn(ys, dy0)));
+    const int64_t wcx = static_cast<int64_t>(floor(xs)), wcy = static_cast<int64_t>(floor(ys));
+    const int64_t cr0 = ccy - hy, cr1 = ccy + hy - 1, cc0 = ccx - hx, cc1 = ccx + hx - 1;
+    const int64_t wr0 = wcy - hy - pry, wr1 = wcy + hy + pry - 2;
+    const int64_t wc0 = wcx - hx - prx, wc1 = wcx + hx + prx - 2;
+    const bool chip_in = (cr1 < cr0 || cc1 < cc0) ||
+                         (cr0 >= 1 && cr1 <= NR && cc0 >= 1 && cc1 <= NC);
+    const bool win_in = (wr1 < wr0 || wc1 < wc0) ||
+                        (wr0 >= 1 && wr1 <= NR && wc0 >= 1 && wc1 <= NC);
+    if (!chip_in || !win_in) return;
+    g.ch = static_cast<int>(2 * hy);
+    g.cw = static_cast<int>(2 * hx);
+    g.nr = static_cast<int>(2 * pry);
+    g.nc = static_cast<int>(2 * prx);
+    g.prx = static_cast<int>(prx);
+    g.pry = static_cast<int>(pry);
+    if (g.ch <= 0 || g.cw <= 0) return;
+    if (g.ch > A.CHM || g.cw > A.CWM || g.nr > A.NRM || g.nc > A.NCM) return;
+    g.chip_r = cr0 - 1 - A.pady;
+    g.chip_c = cc0 - 1 - A.padx;
+    g.win_r = wr0 - 1 - A.pady;
+    g.win_c = wc0 - 1 - A.padx;
+    g.ok = 1;
 }
 
 __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
@@ -1347,6 +1414,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
     __shared__ uint32_t s_pd[25];
     __shared__ float s_fmax[kTcThreads / 32];
     __shared__ unsigned long long s_isum[2][2];
+    __shared__ PtGeo s_geo[2];  // by iteration parity: a point's geometry, computed ahead
     uint8_t* s_E = smem_tc + A.off_E;
     uint8_t* s_W = smem_tc + A.off_W;
     uint8_t* s_P = smem_tc + A.off_P;
@@ -1360,11 +1428,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
 
     const int tid = threadIdx.x, bd = blockDim.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = bd >> 5;
-    const int64_t NR = A.nrows + 2 * A.pady, NC = A.ncols + 2 * A.padx;
-    const double shx = static_cast<double>(A.padx) + 0.5;
-    const double shy = static_cast<double>(A.pady) + 0.5;
     const uint8_t* ref_end = A.ref + A.nrows * A.ncols;
 
+    if (tid < 2) s_geo[tid].k = -1;
     if (warp == 0) {
         tc::tmem_alloc(&s_taddr, A.tmem_cols);
         tc::tmem_relinquish();
@@ -1392,28 +1458,17 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
         TC_PHASE(0)
         const int ib = iter & 1;
         if (tid < 2) s_isum[ib ^ 1][tid] = 0ull;
-        const int64_t prx = A.pts.rx[k], pry = A.pts.ry[k];
-        if (!(prx > 0 && pry > 0)) continue;
-        const double xs = A.pts.x[k] + shx, ys = A.pts.y[k] + shy;
-        const int64_t hx = A.pts.csx[k] / 2, hy = A.pts.csy[k] / 2;
-        const int64_t ccx = static_cast<int64_t>(floor(__dsub_rn(xs, A.pts.dx0[k])));
-        const int64_t ccy = static_cast<int64_t>(floor(__dsub_rn(ys, A.pts.dy0[k])));
-        const int64_t wcx = static_cast<int64_t>(floor(xs)), wcy = static_cast<int64_t>(floor(ys));
-        const int64_t cr0 = ccy - hy, cr1 = ccy + hy - 1, cc0 = ccx - hx, cc1 = ccx + hx - 1;
-        const int64_t wr0 = wcy - hy - pry, wr1 = wcy + hy + pry - 2;
-        const int64_t wc0 = wcx - hx - prx, wc1 = wcx + hx + prx - 2;
-        const bool chip_in = (cr1 < cr0 || cc1 < cc0) ||
-                             (cr0 >= 1 && cr1 <= NR && cc0 >= 1 && cc1 <= NC);
-        const bool win_in = (wr1 < wr0 || wc1 < wc0) ||
-                            (wr0 >= 1 && wr1 <= NR && wc0 >= 1 && wc1 <= NC);
-        if (!chip_in || !win_in) continue;
-        const int ch = static_cast<int>(2 * hy), cw = static_cast<int>(2 * hx);
-        const int nr = static_cast<int>(2 * pry), nc = static_cast<int>(2 * prx);
-        if (ch <= 0 || cw <= 0) continue;
-        if (ch > A.CHM || cw > A.CWM || nr > A.NRM || nc > A.NCM) continue;
+        // The geometry: computed ahead by the previous iteration when it reached its products.
+        PtGeo g;
+        if (s_geo[ib].k == k) {
+            g = s_geo[ib];
+        } else {
+            pt_geometry(A, k, g);
+        }
+        if (!g.ok) continue;
+        const int ch = g.ch, cw = g.cw, nr = g.nr, nc = g.nc, prx = g.prx, pry = g.pry;
         TC_PHASE(1)
-        const int64_t chip_r = cr0 - 1 - A.pady, chip_c = cc0 - 1 - A.padx;
-        const int64_t win_r = wr0 - 1 - A.pady, win_c = wc0 - 1 - A.padx;
+        const int64_t chip_r = g.chip_r, chip_c = g.chip_c, win_r = g.win_r, win_c = g.win_c;
         const long long nnl = static_cast<long long>(ch) * cw;
         const bool pow2 = (nnl & (nnl - 1)) == 0 && nnl <= 4096;
 
@@ -1506,8 +1561,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
         const int XW = cw + nc - 1;
         for (int q = warp; q < Q; q += nwarps)
             for (int x = lane; x < A.XS; x += 32)
-                *reinterpret_cast<uint4*>(s_W + q * A.QS + x * 16) =
-                    load_col16(A.ref, ref_end, A.nrows, A.ncols, win_c + x, win_r + 16 * q);
+                *reinterpret_cast<uint4*>(s_W + q * A.QS + x * 16) = col16_finish(
+                    col16_issue(A.ref, ref_end, A.nrows, A.ncols, win_c + x, win_r + 16 * q));
         // E: NB rows per chip column, row e (u = e - NB + 16) = 16 bytes from chip row -u.
         {
             const int nrow = cw * A.NB;
@@ -1564,6 +1619,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
                 }
             }
             tc::mma_commit(&s_mbar);
+            // The next point's geometry, read after the next loop-top barrier.
+            const int64_t kn = k + gridDim.x;
+            if (kn < A.pts.n) pt_geometry(A, kn, s_geo[ib ^ 1]);
         }
         TC_PHASE(5)
         if (warp < 7) {
