@@ -356,6 +356,57 @@ __global__ void k_init_result(int64_t n, float* dx, float* dy, float* c, uint16_
     }
 }
 
+// Compaction of a pass to its searchable points (both radii > 0): the other points of a level
+// are skipped by the track kernels anyway, but each would still cost a CTA a loop iteration.
+__global__ void k_compact(const int64_t* rx, const int64_t* ry, int64_t n, int64_t* idx,
+                          unsigned long long* count) {
+    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const bool take = k < n && rx[k] > 0 && ry[k] > 0;
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    const int lane = threadIdx.x & 31;
+    unsigned long long base = 0;
+    if (lane == 0 && m) base = atomicAdd(count, static_cast<unsigned long long>(__popc(m)));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (take) idx[base + __popc(m & ((1u << lane) - 1u))] = k;
+}
+
+__global__ void k_gather_points(const int64_t* idx, int64_t ns, DevPoints P, double* x, double* y,
+                                int64_t* rx, int64_t* ry, double* dx0, double* dy0, int64_t* csx,
+                                int64_t* csy) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= ns) return;
+    const int64_t k = idx[i];
+    x[i] = P.x[k];
+    y[i] = P.y[k];
+    rx[i] = P.rx[k];
+    ry[i] = P.ry[k];
+    dx0[i] = P.dx0[k];
+    dy0[i] = P.dy0[k];
+    csx[i] = P.csx[k];
+    csy[i] = P.csy[k];
+}
+
+// Unmeasured outputs everywhere (src/track.jl:58-62), then the compacted results in place.
+__global__ void k_unmeasured(DevOutputs O, int64_t n) {
+    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (k < n) {
+        O.dx[k] = qnan();
+        O.dy[k] = qnan();
+        O.corr[k] = qnan();
+        O.searched[k] = 0;
+    }
+}
+
+__global__ void k_scatter_outputs(const int64_t* idx, int64_t ns, DevOutputs C, DevOutputs O) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= ns) return;
+    const int64_t k = idx[i];
+    O.dx[k] = C.dx[i];
+    O.dy[k] = C.dy[i];
+    O.corr[k] = C.corr[i];
+    O.searched[k] = C.searched[i];
+}
+
 // A bump allocator over one device block.
 struct Arena {
     unsigned char* base;
@@ -395,8 +446,9 @@ size_t multichip_arena_bytes(int64_t gr, int64_t gc) {
     const int64_t n = gr * gc;
     // Level radii and chip sizes (4 x i64), fine outputs (3 f32 + u8), Gardner scratch
     // (2 f32 + 2 u8), fill ping-pong (2 f32 + u8), coarse copies (<= n of 8 fields + outputs),
-    // counters and alignment slack.
-    return static_cast<size_t>(n) * (4 * 8 + 13 + 10 + 9 + 8 * 8 + 13 + 4 + 4) + 64 * 256 + 4096;
+    // the compacted pass (index, 8 fields, outputs), counters and alignment slack.
+    return static_cast<size_t>(n) * (4 * 8 + 13 + 10 + 9 + 8 * 8 + 13 + 4 + 4 + 8 + 8 * 8 + 13) +
+           80 * 256 + 4096;
 }
 
 cudaError_t run_multichip(const MultichipJob& J, TrackScratch& scratch, int num_sms,
@@ -435,6 +487,20 @@ cudaError_t run_multichip(const MultichipJob& J, TrackScratch& scratch, int num_
     float* ccor = A.take<float>(m);
     uint8_t* cs_ = A.take<uint8_t>(m);
     uint8_t* grown = A.take<uint8_t>(m);
+    // The compacted pass (coarse or fine, one at a time).
+    int64_t* kidx = A.take<int64_t>(n);
+    double* kx = A.take<double>(n);
+    double* ky = A.take<double>(n);
+    double* kdx0 = A.take<double>(n);
+    double* kdy0 = A.take<double>(n);
+    int64_t* krx = A.take<int64_t>(n);
+    int64_t* kry = A.take<int64_t>(n);
+    int64_t* kcsx = A.take<int64_t>(n);
+    int64_t* kcsy = A.take<int64_t>(n);
+    float* kdx = A.take<float>(n);
+    float* kdy = A.take<float>(n);
+    float* kc = A.take<float>(n);
+    uint8_t* ks = A.take<uint8_t>(n);
     if (A.off > A.size) {
         if (errmsg) *errmsg = "multichip scratch too small";
         return cudaErrorInvalidValue;
@@ -475,6 +541,30 @@ cudaError_t run_multichip(const MultichipJob& J, TrackScratch& scratch, int num_
         }
     };
 
+    // A track pass over the searchable points of P only, results scattered back into O.
+    auto track_searchable = [&](const DevPoints& P, const DevOutputs& O, int up) {
+        k_unmeasured<<<blocks(P.n), kT, 0, s>>>(O, P.n);
+        ++L;
+        C.zero();
+        k_compact<<<blocks(P.n), kT, 0, s>>>(P.rx, P.ry, P.n, kidx, C.dev);
+        ++L;
+        const int64_t ns = static_cast<int64_t>(C.read1());
+        if (ns == 0 || err != cudaSuccess) return;
+        k_gather_points<<<blocks(ns), kT, 0, s>>>(kidx, ns, P, kx, ky, krx, kry, kdx0, kdy0, kcsx,
+                                                   kcsy);
+        ++L;
+        DevPoints cp{kx, ky, krx, kry, kdx0, kdy0, kcsx, kcsy, ns};
+        DevOutputs co{kdx, kdy, kc, ks};
+        PassGeometry g;
+        err = pass_geometry_device(cp, J.nrows, J.ncols, scratch, s, &g);
+        if (err == cudaSuccess)
+            err = launch_track(J.dtype, J.ref, J.sec, J.valid, J.nrows, J.ncols, cp, g, up,
+                               J.P.measure, co, scratch, num_sms, s, errmsg);
+        if (err != cudaSuccess) return;
+        k_scatter_outputs<<<blocks(ns), kT, 0, s>>>(kidx, ns, co, O);
+        ++L;
+    };
+
     std::vector<int64_t> sizes;
     for (int64_t cs = P.chip_base; cs <= P.chip_max; cs *= 2)
         if (cs >= P.chip_min) sizes.push_back(cs);
@@ -501,12 +591,8 @@ cudaError_t run_multichip(const MultichipJob& J, TrackScratch& scratch, int num_
             ++L;
             if (C.read1() == 0) continue;
             DevPoints cp{cx, cy, crx, cry, cdx0, cdy0, ccsx, ccsy, m};
-            PassGeometry g;
-            if (err == cudaSuccess) err = pass_geometry_device(cp, J.nrows, J.ncols, scratch, s, &g);
             DevOutputs co{cdx, cdy, ccor, cs_};
-            if (err == cudaSuccess)
-                err = launch_track(J.dtype, J.ref, J.sec, J.valid, J.nrows, J.ncols, cp, g, 1,
-                                   P.measure, co, scratch, num_sms, s, errmsg);
+            if (err == cudaSuccess) track_searchable(cp, co, 1);
             C.zero();
             k_measured<<<blocks(m), kT, 0, s>>>(cdx, m, measured, C.dev);
             ++L;
@@ -529,12 +615,8 @@ cudaError_t run_multichip(const MultichipJob& J, TrackScratch& scratch, int num_
 
         // Fine pass, rejection and filling (src/multichip.jl:182-183, 318-390).
         DevPoints fp{J.gx, J.gy, rx, ry, J.gdx0, J.gdy0, csx, csy, n};
-        PassGeometry g;
-        if (err == cudaSuccess) err = pass_geometry_device(fp, J.nrows, J.ncols, scratch, s, &g);
         DevOutputs fo{fdx, fdy, fc, fs};
-        if (err == cudaSuccess)
-            err = launch_track(J.dtype, J.ref, J.sec, J.valid, J.nrows, J.ncols, fp, g, P.up,
-                               P.measure, fo, scratch, num_sms, s, errmsg);
+        if (err == cudaSuccess) track_searchable(fp, fo, static_cast<int>(P.up));
         C.zero();
         k_measured<<<blocks(n), kT, 0, s>>>(fdx, n, measured, C.dev);
         ++L;

@@ -644,6 +644,20 @@ __device__ __forceinline__ float tc_estimate(uint32_t D, uint32_t S1, uint32_t S
     return est;
 }
 
+// Rows of the chip operand that block q's product needs: operand row e holds offset
+// u = e - NB + 16 (surface row i = 16 q + u), and only surface rows 0 <= i < nr are read, so
+// e runs over [max(0, NB - 16 - 16 q), min(NB, NB - 16 + nr - 16 q)). Returned as a 16-aligned
+// start `elo` and a multiple of 16 `n` (elo + n <= NB); false when the block reaches no
+// surface row.
+__device__ __forceinline__ bool block_rows(int q, int NB, int nr, int* elo, int* n) {
+    const int lo = max(0, NB - 16 - 16 * q);
+    const int hi = min(NB, NB - 16 + nr - 16 * q);
+    if (hi <= lo) return false;
+    *elo = lo & ~15;
+    *n = (hi - *elo + 15) & ~15;
+    return true;
+}
+
 // Optional phase timer (compiled in with -DAR_TC_PHASES, for profiling builds only): thread 0
 // of each CTA accumulates clock64() cycles between the marks below, per phase, and adds them to
 // g_tc_phase at exit; entry 15 counts the points that reached the output phase.
@@ -1021,13 +1035,18 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             if (tid == kTcThreads - 32) {
                 tc::fence_after_sync();
                 const uint32_t sW = tc::smem_u32(s_W), sE = tc::smem_u32(s_E);
-                const uint32_t idesc = tc::idesc_u8_s32(A.MT, A.NB);
-                for (int q = 0; q < Q; ++q)
+                for (int q = 0; q < Q; ++q) {
+                    // Only the operand rows e in [elo, elo + n) of block q reach surface rows.
+                    int elo, n;
+                    if (!block_rows(q, A.NB, nr, &elo, &n)) continue;
+                    const uint32_t idesc = tc::idesc_u8_s32(A.MT, n);
                     for (int t = b0 / 2; t < b1 / 2; ++t) {
                         const uint64_t da = tc::smem_desc(sW + q * A.QS + 32 * t, 16, 128);
-                        const uint64_t db = tc::smem_desc(sE + (2 * t - b0) * A.PS, A.PS, 128);
-                        tc::mma_u8(taddr + static_cast<uint32_t>(16 * q), da, db, idesc, true);
+                        const uint64_t db =
+                            tc::smem_desc(sE + (2 * t - b0) * A.PS + 16 * elo, A.PS, 128);
+                        tc::mma_u8(taddr + static_cast<uint32_t>(16 * q + elo), da, db, idesc, true);
                     }
+                }
                 tc::mma_commit(&s_mbar);
             }
             if (cc == 0 && !A.big && warp < 7) box_sums();
@@ -1602,16 +1621,19 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
         TC_PHASE(4)
         if (tid == kTcThreads - 32) {
             tc::fence_after_sync();
-            const uint32_t idesc = tc::idesc_u8_s32(64, A.NB);
             // Descriptors advance by adding to their start-address field (16-byte units; shared
             // addresses stay below 2^18, so the field never carries).
             const uint64_t da0 = tc::smem_desc(tc::smem_u32(s_W), 16, 128);
             const uint64_t db0 = tc::smem_desc(tc::smem_u32(s_E), A.PS, 128);
             const uint64_t dstep_b = static_cast<uint64_t>(2 * A.PS) >> 4;
             for (int q = 0; q < Q; ++q) {
+                // Only the operand rows e in [elo, elo + n) of block q reach surface rows.
+                int elo, n;
+                if (!block_rows(q, A.NB, nr, &elo, &n)) continue;
+                const uint32_t idesc = tc::idesc_u8_s32(64, n);
                 uint64_t da = da0 + (static_cast<uint64_t>(q * A.QS) >> 4);
-                uint64_t db = db0;
-                const uint32_t dn = taddr + static_cast<uint32_t>(16 * q);
+                uint64_t db = db0 + static_cast<uint64_t>(elo);  // 16 * elo bytes
+                const uint32_t dn = taddr + static_cast<uint32_t>(16 * q + elo);
                 for (int t = 0; t < cw / 2; ++t) {
                     tc::mma_u8(dn, da, db, idesc, true);
                     da += 2;
