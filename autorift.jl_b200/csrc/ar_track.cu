@@ -2080,8 +2080,15 @@ __global__ void __launch_bounds__(kRefineWarps * 32) k_refine(const RefineArgs A
             warp_best(bv, bi);
             v0 = fin[0];
         } else {
-            pyrup_warp<5>(P0, L1, WK);
-            pyrup_warp<10>(L1, L2, WK);
+            // Levels 1-3 materialised (level 3 is 40 x 40), then the block search above them.
+            float* L3 = WK;                   // 1600 floats
+            float* BND = WK + 1600;           // nb * nb bounds
+            const int nb = nfinal / kFB;      // blocks per side
+            float* CB = BND + nb * nb;        // pyrUp scratch, row maxima, then cone buffers
+            float* RM = CB;                   // level-3 row maxima per block column (40 * nb)
+            pyrup_warp<5>(P0, L1, CB);
+            pyrup_warp<10>(L1, L2, CB);
+            pyrup_warp<20>(L2, L3, CB);
             // Scale of the rounding slack: the largest magnitude of level 2 bounds every later
             // level's (up to the growth of rounding itself, covered by the factor 2).
             float amax = 0.0f;
@@ -2089,37 +2096,46 @@ __global__ void __launch_bounds__(kRefineWarps * 32) k_refine(const RefineArgs A
             amax = warp_max(amax);
             const float ulp_scale = amax * 9.5367431640625e-07f;  // 2^-20 * max|level 2|
             auto slack = [&](int k) { return k * ulp_scale + k * 2.3509887e-38f; };
-            const int nb = nfinal / kFB;      // blocks per side
-            float* BND = WK;                  // nb * nb bounds
-            float* CB = WK + nb * nb;         // cone buffers
-            // Cone buffer offsets per level distance d = L - level (regions <= 16, 10, 7, 6, 5 rows).
-            // R_d (region) and T_d (vertical pass) for d = 0 .. L - 3.
+            // Cone buffer offsets per level distance d = L - level (regions <= 16, 10, 7, 6 rows
+            // for d = 0 .. L - 4, the levels above the materialised level 3).
             const int cap[6] = {16, 10, 7, 6, 5, 5};
             int roff[6], toff[6], off = 0;
-            for (int d = 0; d <= L - 3; ++d) {
+            for (int d = 0; d <= L - 4; ++d) {
                 roff[d] = off;
                 off += cap[d] * cap[d];
                 toff[d] = off;
                 off += cap[d] * cap[d + 1];
             }
-            // Loose bound of every final block: its level-2 cone maximum plus L - 2 levels of slack.
+            // Level-3 range of final-level rows (or columns) [16 b, 16 b + 15].
+            auto range3 = [&](int b, int& lo, int& hi) {
+                lo = b * kFB;
+                hi = lo + kFB - 1;
+                for (int lev = L - 1; lev >= 3; --lev) {
+                    int a2, b2;
+                    tap_range(lo, hi, 5 << lev, a2, b2);
+                    lo = a2;
+                    hi = b2;
+                }
+            };
+            __syncwarp();
+            // Loose bound of every final block: its level-3 cone maximum plus L - 3 levels of
+            // slack, as row maxima over each block column's range, then maxima over row ranges.
+            for (int e = lane; e < 40 * nb; e += 32) {
+                const int i = e % 40, bj_ = e / 40;
+                int c0, c1;
+                range3(bj_, c0, c1);
+                float mx = -INFINITY;
+                for (int j = c0; j <= c1; ++j) mx = fmaxf(mx, L3[i + j * 40]);
+                RM[e] = mx;
+            }
+            __syncwarp();
             for (int blk = lane; blk < nb * nb; blk += 32) {
                 const int bi_ = blk % nb, bj_ = blk / nb;
-                int r0 = bi_ * kFB, r1 = r0 + kFB - 1, c0 = bj_ * kFB, c1 = c0 + kFB - 1;
-                for (int lev = L - 1; lev >= 2; --lev) {
-                    const int n = 5 << lev;
-                    int a, b;
-                    tap_range(r0, r1, n, a, b);
-                    r0 = a;
-                    r1 = b;
-                    tap_range(c0, c1, n, a, b);
-                    c0 = a;
-                    c1 = b;
-                }
+                int r0, r1;
+                range3(bi_, r0, r1);
                 float mx = -INFINITY;
-                for (int j = c0; j <= c1; ++j)
-                    for (int i = r0; i <= r1; ++i) mx = fmaxf(mx, L2[i + j * 20]);
-                BND[blk] = mx + slack(L - 2);
+                for (int i = r0; i <= r1; ++i) mx = fmaxf(mx, RM[i + bj_ * 40]);
+                BND[blk] = mx + slack(L - 3);
             }
             __syncwarp();
             while (true) {
@@ -2137,23 +2153,24 @@ __global__ void __launch_bounds__(kRefineWarps * 32) k_refine(const RefineArgs A
                 if (sel == INT_MAX || m == -INFINITY || m < bv) break;
                 __syncwarp();
                 if (lane == 0) BND[sel] = -INFINITY;
-                // The block's cone, from the final level down to level 2.
+                // The block's cone, from the final level down to level 3.
                 ConeLevel cl[8];
                 {
                     const int bi_ = sel % nb, bj_ = sel / nb;
                     cl[0] = {bi_ * kFB, bi_ * kFB + kFB - 1, bj_ * kFB, bj_ * kFB + kFB - 1};
-                    for (int d = 1; d <= L - 2; ++d) {
+                    for (int d = 1; d <= L - 3; ++d) {
                         const int n = 5 << (L - d);
                         tap_range(cl[d - 1].r0, cl[d - 1].r1, n, cl[d].r0, cl[d].r1);
                         tap_range(cl[d - 1].c0, cl[d - 1].c1, n, cl[d].c0, cl[d].c1);
                     }
                 }
-                // Levels 3 .. L - 1 (d = L - 3 .. 1) into the cone buffers.
-                ConeLevel sreg = cl[L - 2];
-                const float* src = L2 + sreg.r0 + sreg.c0 * 20;
-                int lds = 20;
+                // Levels 4 .. L - 1 (d = L - 4 .. 1) into the cone buffers; at level L - 2 (when
+                // it is above level 3) the tighter two-level bound.
+                ConeLevel sreg = cl[L - 3];
+                const float* src = L3 + sreg.r0 + sreg.c0 * 40;
+                int lds = 40;
                 bool pruned = false;
-                for (int d = L - 3; d >= 1; --d) {
+                for (int d = L - 4; d >= 1; --d) {
                     const int n = 5 << (L - d - 1);  // source level size
                     float* dst = CB + roff[d];
                     cone_step(src, lds, sreg, n, cl[d], CB + toff[d], dst);
@@ -2161,7 +2178,6 @@ __global__ void __launch_bounds__(kRefineWarps * 32) k_refine(const RefineArgs A
                     sreg = cl[d];
                     lds = cl[d].r1 - cl[d].r0 + 1;
                     if (d == 2) {
-                        // Level L - 2: the tighter bound for the last two levels.
                         const int cnt = (cl[2].r1 - cl[2].r0 + 1) * (cl[2].c1 - cl[2].c0 + 1);
                         float mx = -INFINITY;
                         for (int e = lane; e < cnt; e += 32) mx = fmaxf(mx, dst[e]);
@@ -2376,7 +2392,7 @@ struct RefinePlan {
 };
 
 // Shared floats per warp of k_refine: patch, levels 1 and 2, then either the level-3
-// materialisation (up <= 8) or the block bounds and cone buffers.
+// materialisation (up <= 8) or level 3 with the block bounds and cone buffers.
 RefinePlan plan_refine(int up) {
     RefinePlan R{};
     R.levels = ilog2_exact(up);
@@ -2385,10 +2401,13 @@ RefinePlan plan_refine(int up) {
     if (L <= 3) {
         wk = 800 + 1600;
     } else {
+        // Level 3, the block bounds, then the largest of the pyrUp scratch (40 x 20), the
+        // level-3 row maxima (40 per block column) and the cone buffers of levels 4 .. L.
         const int nb = (5 << L) / kFB;
         const int cap[7] = {16, 10, 7, 6, 5, 5, 5};
-        wk = nb * nb;
-        for (int d = 0; d <= L - 3; ++d) wk += cap[d] * cap[d] + cap[d] * cap[d + 1];
+        int cone = 0;
+        for (int d = 0; d <= L - 4; ++d) cone += cap[d] * cap[d] + cap[d] * cap[d + 1];
+        wk = 1600 + nb * nb + std::max(std::max(800, 40 * nb), cone);
     }
     R.warp_floats = 32 + 100 + 400 + wk;
     R.smem = static_cast<size_t>(kRefineWarps) * R.warp_floats * sizeof(float);
@@ -2852,7 +2871,8 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
     e = cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(R.smem));
     if (e != cudaSuccess) return e;
-    const int64_t rper_sm = std::max<int64_t>(1, std::min<int64_t>(4, (200 * 1024) / R.smem));
+    const int64_t rper_sm =
+        std::max<int64_t>(1, std::min<int64_t>(4, (227 * 1024) / (R.smem + 1024)));
     const int rgrid = static_cast<int>(std::max<int64_t>(
         1, std::min<int64_t>((pts.n + kRefineWarps - 1) / kRefineWarps, num_sms * rper_sm)));
     k_refine<<<rgrid, kRefineWarps * 32, R.smem, stream>>>(B);
@@ -2896,7 +2916,8 @@ cudaError_t launch_refine_patches(const float* patches, int64_t count, int up, i
     cudaError_t e = cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(R.smem));
     if (e != cudaSuccess) return e;
-    const int64_t per_sm = std::max<int64_t>(1, std::min<int64_t>(4, (200 * 1024) / R.smem));
+    const int64_t per_sm =
+        std::max<int64_t>(1, std::min<int64_t>(4, (227 * 1024) / (R.smem + 1024)));
     const int grid = static_cast<int>(std::max<int64_t>(
         1, std::min<int64_t>((count + kRefineWarps - 1) / kRefineWarps, num_sms * per_sm)));
     k_refine<<<grid, kRefineWarps * 32, R.smem, stream>>>(B);

@@ -1,13 +1,14 @@
 """The block search of the sub-pixel cascade kernel (k_refine), restated in numpy float32 with
 the kernel's operation order, against the full cascade.
 
-k_refine computes only the 16 x 16 final-level blocks whose bound can reach the maximum, each
-through its dependency cone, and stops when no remaining bound reaches the best value. This
-test replays exactly that search (bounds from level 2 with k * 2^-20 * max|level 2| slack, the
-two-level bound at level L - 2, the region sizes the kernel's buffers hold) on peaked, random,
-flat and tied 5 x 5 patches and checks that it returns the full cascade's value and
-row-major-first position (src/peak.jl:456-522). The GPU tests check the kernel itself against
-the oracle's full cascade.
+k_refine materialises levels 1-3, then computes only the 16 x 16 final-level blocks whose bound
+can reach the maximum, each through its dependency cone above level 3, and stops when no
+remaining bound reaches the best value. This test replays exactly that search (bounds from the
+level-3 cone with k * 2^-20 * max|level 2| slack over the L - 3 levels above it, the two-level
+bound at level L - 2 when it is above level 3, the region sizes the kernel's buffers hold) on
+peaked, random, flat and tied 5 x 5 patches and checks that it returns the full cascade's value
+and row-major-first position (src/peak.jl:456-522). The GPU tests check the kernel itself
+against the oracle's full cascade.
 """
 
 import numpy as np
@@ -59,19 +60,21 @@ def tap_range(p0, p1, n):
     return lo, min((p1 >> 1) + 1, n - 1)
 cap = [16, 10, 7, 6, 5, 5]
 def pruned(P, L, stats):
-    L1 = pyrup_fast(P); L2 = pyrup_fast(L1)
+    L1 = pyrup_fast(P); L2 = pyrup_fast(L1); L3 = pyrup_fast(L2)
     amax = f32(np.max(np.abs(L2)))
     ulp = f32(amax * f32(9.5367431640625e-07))
     slack = lambda k: f32(f32(k * ulp) + f32(k * 2.3509887e-38))
     nfinal = 5 << L; nb = nfinal // 16
+    def range3(b):
+        lo, hi = b * 16, b * 16 + 15
+        for lev in range(L - 1, 2, -1):
+            lo, hi = tap_range(lo, hi, 5 << lev)
+        return lo, hi
     BND = np.zeros(nb * nb, f32)
     for blk in range(nb * nb):
         bi, bj = blk % nb, blk // nb
-        r0, r1, c0, c1 = bi * 16, bi * 16 + 15, bj * 16, bj * 16 + 15
-        for lev in range(L - 1, 1, -1):
-            n = 5 << lev
-            r0, r1 = tap_range(r0, r1, n); c0, c1 = tap_range(c0, c1, n)
-        BND[blk] = f32(L2[r0:r1 + 1, c0:c1 + 1].max() + slack(L - 2))
+        r0, r1 = range3(bi); c0, c1 = range3(bj)
+        BND[blk] = f32(L3[r0:r1 + 1, c0:c1 + 1].max() + slack(L - 3))
     bv, bi_ = f32(-np.inf), 2**31 - 1
     visited = full = 0
     while True:
@@ -80,17 +83,17 @@ def pruned(P, L, stats):
         BND[sel] = -np.inf; visited += 1
         bI, bJ = sel % nb, sel // nb
         cl = [(bI * 16, bI * 16 + 15, bJ * 16, bJ * 16 + 15)]
-        for d in range(1, L - 1):
+        for d in range(1, L - 2):
             n = 5 << (L - d)
             r0, r1 = tap_range(cl[-1][0], cl[-1][1], n); c0, c1 = tap_range(cl[-1][2], cl[-1][3], n)
             cl.append((r0, r1, c0, c1))
         for d in range(len(cl)):
             assert cl[d][1] - cl[d][0] + 1 <= cap[d] and cl[d][3] - cl[d][2] + 1 <= cap[d], (d, cl[d])
-        # compute the cone: region values at each level via full-level sample function on demand
-        # (equivalent: compute the dst region from the src region with the same taps)
-        sreg = cl[L - 2]; src = {(i, j): L2[i, j] for i in range(sreg[0], sreg[1] + 1) for j in range(sreg[2], sreg[3] + 1)}
+        # the cone above level 3: region values at each level from the region below, with the
+        # same taps (cl[L - 3] is the level-3 region)
+        sreg = cl[L - 3]; src = {(i, j): L3[i, j] for i in range(sreg[0], sreg[1] + 1) for j in range(sreg[2], sreg[3] + 1)}
         pr = False
-        for d in range(L - 3, -1, -1):
+        for d in range(L - 4, -1, -1):
             n = 5 << (L - d - 1)
             r0, r1, c0, c1 = cl[d]
             tmp = {}
