@@ -152,7 +152,9 @@ cudaError_t tc_probe(const uint8_t* a_img, int a_bytes, const uint8_t* b_img, in
     P.d_out = d_out;
     P.status = status;
     const int smem = P.b_base + b_bytes;
-    cudaError_t e = cudaFuncSetAttribute(k_tc_probe, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (smem > kDynSmemCap) return bad("operand images exceed shared memory");
+    cudaError_t e =
+        cudaFuncSetAttribute(k_tc_probe, cudaFuncAttributeMaxDynamicSharedMemorySize, kDynSmemCap);
     if (e != cudaSuccess) return e;
     k_tc_probe<<<1, 128, smem, s>>>(P);
     return cudaGetLastError();

@@ -12,6 +12,12 @@
 
 namespace ar {
 
+// Dynamic shared memory a kernel is allowed (cudaFuncAttributeMaxDynamicSharedMemorySize). The
+// attribute belongs to the function, shared by every context and host thread of the process, so
+// it is always set to this one value and each launch checks its own size against it: a launch
+// can never find it lowered by a concurrent launch of the same kernel with a smaller plan.
+constexpr int kDynSmemCap = 220 * 1024;
+
 // Pass geometry: the summary of a point set that sizes a launch (src/track.jl:176-197).
 struct PassGeometry {
     int64_t max_ch = 0, max_cw = 0;  // effective chip extents (2 * (size / 2))

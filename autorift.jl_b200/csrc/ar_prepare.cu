@@ -415,18 +415,19 @@ cudaError_t prepare_t(const PrepareJob& J, cudaStream_t s, long long* launches) 
     const size_t smem = box_smem_bytes(wx, wy);
     float* filt = J.quantize == 1 ? J.ftmp : static_cast<float*>(J.out);
     cudaError_t e;
+    if (smem > static_cast<size_t>(kDynSmemCap)) return cudaErrorInvalidValue;
     if (J.preprocess == 1) {
         e = cudaFuncSetAttribute(k_highpass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem));
+                                 kDynSmemCap);
         if (e != cudaSuccess) return e;
         k_highpass<T><<<grid, kBoxThreads, smem, s>>>(img, J.mask, J.nrows, J.ncols, wx, wy, filt, J.vout);
         *launches += 1;
     } else {
         e = cudaFuncSetAttribute(k_boxmean<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem));
+                                 kDynSmemCap);
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(k_wallis<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem));
+                                     kDynSmemCap);
         if (e != cudaSuccess) return e;
         k_boxmean<T><<<grid, kBoxThreads, smem, s>>>(img, J.mask, J.nrows, J.ncols, wx, wy, J.mtmp);
         k_wallis<T><<<grid, kBoxThreads, smem, s>>>(img, J.mask, J.mtmp, J.nrows, J.ncols, wx, wy,

@@ -1825,15 +1825,30 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
         }
         __syncthreads();
         const int ncand = s_ncand;
-        unsigned long long best = 0ull;
-        for (int c = tid; c < ncand; c += bd) {
-            const int i = static_cast<int>(s_cI[c] >> 16), j = static_cast<int>(s_cI[c] & 0xFFFFu);
-            const int o = j * A.NRS + i;
-            const float x = tc_exact(s_num[c], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
-            const unsigned long long key = argmax_key(x, static_cast<unsigned>(i * nc + j));
-            best = key > best ? key : best;
+        unsigned rm = 0;
+        float pv = 0.0f;
+        int pi = 0, pj = 0;
+        if (ncand == 1 && M > -INFINITY) {
+            // M is finite, so the value whose lower bound is M is in the list; when it is the
+            // only entry, every other FP32 surface value is at most its upper bound, below M,
+            // and this one is at least M: it is the strict (so the first) maximum.
+            pi = static_cast<int>(s_cI[0] >> 16);
+            pj = static_cast<int>(s_cI[0] & 0xFFFFu);
+        } else {
+            unsigned long long best = 0ull;
+            for (int c = tid; c < ncand; c += bd) {
+                const int i = static_cast<int>(s_cI[c] >> 16), j = static_cast<int>(s_cI[c] & 0xFFFFu);
+                const int o = j * A.NRS + i;
+                const float x = tc_exact(s_num[c], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+                const unsigned long long key = argmax_key(x, static_cast<unsigned>(i * nc + j));
+                best = key > best ? key : best;
+            }
+            best = block_max_u64(best, reinterpret_cast<unsigned long long*>(s_red));
+            if (key_decode(best, &rm, &pv)) {
+                pi = static_cast<int>(rm / nc);
+                pj = static_cast<int>(rm % nc);
+            }
         }
-        best = block_max_u64(best, reinterpret_cast<unsigned long long*>(s_red));
         TC_PHASE(9)
         if (A.flops && tid == 0)
             atomicAdd(A.flops, 2ull * static_cast<unsigned long long>(ch) * cw * nr * nc);
@@ -1849,13 +1864,6 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
                 const int o = (e / nr) * A.NRS + (e % nr);
                 so[e] = tc_exact(s_num[o], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
             }
-        }
-        unsigned rm = 0;
-        float pv = 0.0f;
-        int pi = 0, pj = 0;
-        if (key_decode(best, &rm, &pv)) {
-            pi = static_cast<int>(rm / nc);
-            pj = static_cast<int>(rm % nc);
         }
         const bool single = A.up == 1 || nr < 5 || nc < 5;
         const int pi0 = single ? pi : min(max(pi - 2, 0), max(nr - 5, 0));
@@ -2414,6 +2422,14 @@ RefinePlan plan_refine(int up) {
     return R;
 }
 
+// Dynamic shared memory a CTA holding `cols` Tensor Memory columns reserves, for a kernel with
+// `static_smem` bytes of static shared memory (see the launch below): with the 1 KB the SM
+// charges each CTA, its footprint is at least cols/512 of the SM's 228 KB.
+size_t tmem_smem_floor(uint32_t cols, size_t static_smem) {
+    const size_t share = static_cast<size_t>(cols) * (228 * 1024) / 512;
+    return share > 1024 + static_smem ? share - 1024 - static_smem : 0;
+}
+
 struct TcPlan {
     int NB, QM, QS, PS, PC, XS, XT, NRS, NRM, NCM, CHM, CWM, BC, big, MT;
     unsigned off_E, off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
@@ -2575,8 +2591,9 @@ bool plan_corr_tc(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
 
 template <typename T>
 cudaError_t launch_corr_t(const CorrArgs& A, const CorrPlan& P, int grid, cudaStream_t stream) {
+    if (P.smem > static_cast<size_t>(kDynSmemCap)) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(k_corr<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(P.smem));
+                                         kDynSmemCap);
     if (e != cudaSuccess) return e;
     k_corr<T><<<grid, kCorrThreads, P.smem, stream>>>(A);
     return cudaGetLastError();
@@ -2819,15 +2836,25 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         B.surf_out = surf_out;
         B.flops = A.flops;
         B.status = scratch.status;
-        // Each CTA holds its Tensor Memory columns for its lifetime, so the CTAs one SM can
-        // hold must fit its 512 columns together: at most two CTAs of <= 256 columns (at least
-        // 76 KB of shared memory each), otherwise one (at least 116 KB).
-        const int per_sm_tc = TP.tmem_cols <= 256 && TP.smem <= 112 * 1024 ? 2 : 1;
-        const size_t tc_smem = std::max<size_t>(TP.smem, per_sm_tc == 2 ? 76 * 1024 : 116 * 1024);
+        // Each CTA holds its Tensor Memory columns for its lifetime, so the CTAs one SM holds
+        // must fit its 512 columns together -- including CTAs of other launches running
+        // concurrently (other streams, the request loop's slots), or an allocation would wait
+        // for a whole persistent launch to end. A CTA of T columns therefore reserves at least
+        // T/512 of the SM's 228 KB of shared memory (less the 1 KB each CTA is charged): any set
+        // of CTAs that fits an SM's shared memory fits its Tensor Memory.
         const bool reg = TP.MT == 64 && TP.NRM <= 64;
         auto kern = use_tc2 ? k_corr_tc2 : reg ? k_corr_tc<true> : k_corr_tc<false>;
+        cudaFuncAttributes fa{};
+        e = cudaFuncGetAttributes(&fa, kern);
+        if (e != cudaSuccess) return e;
+        // The per-block limit (227 KB, static included) is this kernel's fixed attribute value.
+        const size_t dyn_max = 232448 - fa.sharedSizeBytes;
+        const size_t tc_smem = std::max<size_t>(TP.smem, tmem_smem_floor(TP.tmem_cols, fa.sharedSizeBytes));
+        const int per_sm_tc = static_cast<int>(std::max<size_t>(
+            1, std::min<size_t>(2, (228 * 1024) / (tc_smem + fa.sharedSizeBytes + 1024))));
+        if (tc_smem > dyn_max) return cudaErrorInvalidValue;
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(tc_smem));
+                                 static_cast<int>(dyn_max));
         if (e != cudaSuccess) return e;
         const int grid = static_cast<int>(
             std::max<int64_t>(1, std::min<int64_t>(pts.n, static_cast<int64_t>(num_sms) * per_sm_tc)));
@@ -2868,8 +2895,8 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
     B.out = out;
     B.levels = R.levels;
     B.warp_floats = R.warp_floats;
-    e = cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(R.smem));
+    if (R.smem > static_cast<size_t>(kDynSmemCap)) return cudaErrorInvalidValue;
+    e = cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, kDynSmemCap);
     if (e != cudaSuccess) return e;
     const int64_t rper_sm =
         std::max<int64_t>(1, std::min<int64_t>(4, (227 * 1024) / (R.smem + 1024)));
@@ -2913,8 +2940,9 @@ cudaError_t launch_refine_patches(const float* patches, int64_t count, int up, i
     B.oval = value;
     B.levels = R.levels;
     B.warp_floats = R.warp_floats;
-    cudaError_t e = cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(R.smem));
+    if (R.smem > static_cast<size_t>(kDynSmemCap)) return cudaErrorInvalidValue;
+    cudaError_t e =
+        cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, kDynSmemCap);
     if (e != cudaSuccess) return e;
     const int64_t per_sm =
         std::max<int64_t>(1, std::min<int64_t>(4, (227 * 1024) / (R.smem + 1024)));

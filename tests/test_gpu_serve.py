@@ -72,6 +72,27 @@ def test_results_identical_alone_and_in_the_mix(ar, cases):
     ctx.close()
 
 
+def test_mixed_geometries_concurrently(ar, gpu_lib):
+    """Many requests whose launches of the same kernels need different shared memory (chip
+    16/32/64, radius 8..48) running at once in four slots: every result as alone."""
+    a, b, v, _ = ar.synthetic.scale_u16_pair(512, seed=11)
+    kinds = [dict(grid_spacing=16, chip_size=16, search_radius=8),
+             dict(grid_spacing=16, chip_size=32, search_radius=25),
+             dict(grid_spacing=16, chip_size=64, search_radius=10),
+             dict(grid_spacing=32, chip_size=16, search_radius=48)]
+    alone_ctx = ar._lib.Context(0)
+    alone = [ar.autorift(a, b, secondary_valid=v, ctx=alone_ctx, **kw) for kw in kinds]
+    alone_ctx.close()
+    ctx = ar._lib.Context(0)
+    ctx.set_option(ar._lib.AR_OPT_SERVE_SLOTS, 4)
+    tickets = [ar.submit(a, b, secondary_valid=v, ctx=ctx, **kinds[k % len(kinds)])
+               for k in range(24)]
+    for k, t in enumerate(tickets):
+        same(t.wait(timeout=120), alone[k % len(kinds)])
+        t.release()
+    ctx.close()
+
+
 def test_timeout_poll_and_release(ar, gpu_lib):
     ctx = ar._lib.Context(0)
     a, b, v, _ = ar.synthetic.scale_u16_pair(1024, seed=8)
