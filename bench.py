@@ -437,7 +437,7 @@ def gpu_arm(args):
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": tensor_peak,
                          "unit": "TFLOP/s",
                          "frac": achieved / tensor_peak if achieved else None,
-                         "traffic": profile_traffic(fine_points), "kernel": "k_corr_tc",
+                         "traffic": profile_traffic(fine_points), "kernel": "k_corr_tc2",
                          "peak_source": peak_source,
                          "achieved_basis": "2 * chip area * surface area per searched point "
                                            "(integer MACs of the exact u8 numerator), summed "

@@ -252,8 +252,9 @@ int ar_release(ar_ctx* ctx, ar_ticket ticket);
 
 /*
  * Context options. AR_OPT_TENSOR_CORES (default 1): UInt8 passes whose geometry fits (surface
- * at most 64 columns and 256 rows) compute the correlation numerator on the tensor cores
- * (exact 8-bit products, bit-identical results); 0 keeps every pass on the CUDA-core kernel.
+ * at most 128 columns and 256 rows, chip at most 226 rows) compute the correlation numerator
+ * on the tensor cores (exact 8-bit products, bit-identical results); 0 keeps every pass on the
+ * CUDA-core kernel.
  * AR_OPT_SERVE_SLOTS and AR_OPT_SERVE_MEMORY_MB configure the request loop (see ar_submit);
  * they must be set before the first ar_submit. No reference counterpart.
  */
