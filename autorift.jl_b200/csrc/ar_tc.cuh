@@ -58,6 +58,24 @@ __device__ __forceinline__ void mma_u8(uint32_t d_tmem, uint64_t a_desc, uint64_
         : "memory");
 }
 
+// D (+)= A * B^T with the descriptors given as 32-bit halves (lo, hi): a caller that advances
+// only the start-address field keeps the halves in registers and adds to `lo` alone.
+__device__ __forceinline__ void mma_u8_halves(uint32_t d_tmem, uint32_t a_lo, uint32_t a_hi,
+                                              uint32_t b_lo, uint32_t b_hi, uint32_t idesc) {
+    asm volatile(
+        "{\n\t"
+        ".reg .b64 da, db;\n\t"
+        ".reg .pred p;\n\t"
+        "mov.b64 da, {%1, %2};\n\t"
+        "mov.b64 db, {%3, %4};\n\t"
+        "setp.ne.b32 p, 1, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], da, db, %5, {%6, %6, %6, %6}, p;\n\t"
+        "}\n"
+        :
+        : "r"(d_tmem), "r"(a_lo), "r"(a_hi), "r"(b_lo), "r"(b_hi), "r"(idesc), "r"(0u)
+        : "memory");
+}
+
 // Arrive on `mbar` once every tcgen05.mma issued so far by this thread has completed.
 __device__ __forceinline__ void mma_commit(uint64_t* mbar) {
     asm volatile(

@@ -577,6 +577,7 @@ struct TcArgs {
     int big;                         // 1: box sums before the products, chunks reuse their space
     unsigned off_E, off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
     int XV;                          // k_corr_tc2: row stride (words) of the column sums V1, V2
+    int acc1_col;                    // k_corr_tc2: first column of its second accumulator
     uint32_t tmem_cols;
     DevOutputs out;
     int* sub_count;
@@ -1455,13 +1456,14 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
         tc::tmem_relinquish();
     }
     if (tid == 0) {
-        tc::mbar_init(&s_mbar, 1);
+        tc::mbar_init(&s_mbar, 2);  // one commit per issuing thread
         tc::fence_mbar_init();
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t taddr = s_taddr;
+    const uint32_t acc1 = static_cast<uint32_t>(A.acc1_col);  // second accumulator's first column
     uint32_t phase = 0;
     bool failed = false;
     if (tid < 4) s_isum[tid >> 1][tid & 1] = 0ull;
@@ -1469,8 +1471,20 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
     int iter = 0;
     int dirty_ch = 0;
     TC_PHASE_INIT
+#ifdef AR_TC_PHASES
+    unsigned long long tmi_issue = 0, tmi_done = 0;
+#endif
 
-    for (int64_t k = blockIdx.x; k < A.pts.n; k += gridDim.x, ++iter) {
+    // Each CTA takes a contiguous run of points: consecutive points of a grid column have the
+    // same window columns one grid step lower, so most of their box sums carry over.
+    const int64_t per = (A.pts.n + gridDim.x - 1) / gridDim.x;
+    const int64_t kbeg = static_cast<int64_t>(blockIdx.x) * per;
+    const int64_t kend = min(A.pts.n, kbeg + per);
+    // The point whose box sums s_S1 / s_S2 hold (held = false: none).
+    bool held = false;
+    int64_t h_wr = 0, h_wc = 0;
+    int h_ch = 0, h_cw = 0, h_nr = 0, h_nc = 0;
+    for (int64_t k = kbeg; k < kend; ++k, ++iter) {
         tc::fence_before_sync();
         __syncthreads();  // the previous point's buffers and accumulators are no longer read
         tc::fence_after_sync();
@@ -1612,105 +1626,83 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
 #pragma unroll
             for (int t = 0; t < 16; ++t) z[t] = 0u;
             const uint32_t lq = taddr + (static_cast<uint32_t>(32 * warp) << 16);
-            for (int c = 0; c < dcols; c += 16) tc::tmem_st16(lq + static_cast<uint32_t>(c), z);
+            for (int c = 0; c < dcols; c += 16) {
+                tc::tmem_st16(lq + static_cast<uint32_t>(c), z);
+                tc::tmem_st16(lq + acc1 + static_cast<uint32_t>(c), z);
+            }
             tc::tmem_wait_st();
         }
         tc::fence_proxy_async_smem();
         tc::fence_before_sync();
         __syncthreads();  // s_P, s_W, s_E complete; accumulator cleared
         TC_PHASE(4)
-        if (tid == kTcThreads - 32) {
+        // Two threads issue the products, each for half of the chip column pairs into its own
+        // accumulator: the MMAs of one thread run one after another, two threads' interleave.
+        if (tid == kTcThreads - 32 || tid == kTcThreads - 64) {
+            const int stream = tid == kTcThreads - 32 ? 0 : 1;
             tc::fence_after_sync();
-            // Descriptors advance by adding to their start-address field (16-byte units; shared
-            // addresses stay below 2^18, so the field never carries).
+#ifdef AR_TC_PHASES
+            const unsigned long long tmi0 = clock64();
+#endif
+            // Descriptors advance by adding to their start-address field, the low bits of the
+            // low word (16-byte units; shared addresses stay below 2^18, so nothing carries):
+            // a product costs the issuing thread two 32-bit adds and the MMA itself.
             const uint64_t da0 = tc::smem_desc(tc::smem_u32(s_W), 16, 128);
             const uint64_t db0 = tc::smem_desc(tc::smem_u32(s_E), A.PS, 128);
-            const uint64_t dstep_b = static_cast<uint64_t>(2 * A.PS) >> 4;
+            const uint32_t a_hi = static_cast<uint32_t>(da0 >> 32);
+            const uint32_t b_hi = static_cast<uint32_t>(db0 >> 32);
+            const uint32_t bstep = static_cast<uint32_t>(2 * A.PS) >> 4;
+            const int half_pairs = (cw / 2) / 2;
+            const int t_begin = stream == 0 ? 0 : half_pairs;
+            const int npairs = stream == 0 ? half_pairs : cw / 2 - half_pairs;
             for (int q = 0; q < Q; ++q) {
                 // Only the operand rows e in [elo, elo + n) of block q reach surface rows.
                 int elo, n;
                 if (!block_rows(q, A.NB, nr, &elo, &n)) continue;
                 const uint32_t idesc = tc::idesc_u8_s32(64, n);
-                uint64_t da = da0 + (static_cast<uint64_t>(q * A.QS) >> 4);
-                uint64_t db = db0 + static_cast<uint64_t>(elo);  // 16 * elo bytes
-                const uint32_t dn = taddr + static_cast<uint32_t>(16 * q + elo);
-                for (int t = 0; t < cw / 2; ++t) {
-                    tc::mma_u8(dn, da, db, idesc, true);
-                    da += 2;
-                    db += dstep_b;
+                uint32_t a_lo = static_cast<uint32_t>(da0) +
+                                static_cast<uint32_t>(q * A.QS >> 4) + 2u * static_cast<uint32_t>(t_begin);
+                uint32_t b_lo = static_cast<uint32_t>(db0) + static_cast<uint32_t>(elo) +
+                                bstep * static_cast<uint32_t>(t_begin);
+                const uint32_t dn = taddr + (stream ? acc1 : 0u) + static_cast<uint32_t>(16 * q + elo);
+                int t = 0;
+                for (; t + 4 <= npairs; t += 4) {
+                    tc::mma_u8_halves(dn, a_lo, a_hi, b_lo, b_hi, idesc);
+                    tc::mma_u8_halves(dn, a_lo + 2, a_hi, b_lo + bstep, b_hi, idesc);
+                    tc::mma_u8_halves(dn, a_lo + 4, a_hi, b_lo + 2 * bstep, b_hi, idesc);
+                    tc::mma_u8_halves(dn, a_lo + 6, a_hi, b_lo + 3 * bstep, b_hi, idesc);
+                    a_lo += 8;
+                    b_lo += 4 * bstep;
+                }
+                for (; t < npairs; ++t) {
+                    tc::mma_u8_halves(dn, a_lo, a_hi, b_lo, b_hi, idesc);
+                    a_lo += 2;
+                    b_lo += bstep;
                 }
             }
             tc::mma_commit(&s_mbar);
+#ifdef AR_TC_PHASES
+            // Profiling builds: time to issue the products, then until they complete.
+            const unsigned long long tmi1 = clock64();
+            if (stream == 0) {
+                tc::mbar_wait(&s_mbar, phase, kTcWaitPolls);
+                tmi_issue += tmi1 - tmi0;
+                tmi_done += clock64() - tmi1;
+            }
+#endif
             // The next point's geometry, read after the next loop-top barrier.
-            const int64_t kn = k + gridDim.x;
-            if (kn < A.pts.n) pt_geometry(A, kn, s_geo[ib ^ 1]);
+            const int64_t kn = k + 1;
+            if (stream == 0 && kn < kend) pt_geometry(A, kn, s_geo[ib ^ 1]);
         }
         TC_PHASE(5)
-        if (warp < 7) {
-            // Box sums of W and W^2 (integral_both!, boxsum, src/integral.jl:141-170, 244-247)
-            // as exact integers, warps 0-6 (named barrier 1) while warp 7 issues the products.
-            constexpr int kBT = kTcThreads - 32;
-            // V[i][x] = sums over rows i .. i + ch - 1 of column x: a task is a column and the 16
-            // rows i of one block; its outgoing rows are that block, its incoming rows start ch
-            // rows lower.
-            const int nseg = (nr + 15) >> 4;
-            const int chb = ch >> 4, chr = ch & 15;
-            for (int task = tid; task < XW * nseg; task += kBT) {
-                const int sgi = task / XW, x = task - sgi * XW;
-                const int i0 = 16 * sgi;
-                const uint8_t* colx = s_W + x * 16;
-                const uint4 bo = *reinterpret_cast<const uint4*>(colx + sgi * A.QS);
-                uint32_t h1 = 0, h2 = 0;
-                for (int bb = 0; bb < chb; ++bb) {
-                    const uint4 w = *reinterpret_cast<const uint4*>(colx + (sgi + bb) * A.QS);
-                    h1 = __dp4a(w.x, 0x01010101u, h1);
-                    h1 = __dp4a(w.y, 0x01010101u, h1);
-                    h1 = __dp4a(w.z, 0x01010101u, h1);
-                    h1 = __dp4a(w.w, 0x01010101u, h1);
-                    h2 = __dp4a(w.x, w.x, h2);
-                    h2 = __dp4a(w.y, w.y, h2);
-                    h2 = __dp4a(w.z, w.z, h2);
-                    h2 = __dp4a(w.w, w.w, h2);
-                }
-                const uint4 bi = *reinterpret_cast<const uint4*>(colx + (sgi + chb) * A.QS);
-                if (chr) {
-                    const uint32_t wv[4] = {bi.x, bi.y, bi.z, bi.w};
-#pragma unroll
-                    for (int m = 0; m < 4; ++m) {
-                        const int keep = min(max(chr - 4 * m, 0), 4);
-                        const uint32_t mk = keep == 4 ? 0xffffffffu : ((1u << (8 * keep)) - 1u);
-                        h1 = __dp4a(wv[m] & mk, 0x01010101u, h1);
-                        h2 = __dp4a(wv[m] & mk, wv[m], h2);
-                    }
-                }
-                const uint32_t wo[4] = {bo.x, bo.y, bo.z, bo.w};
-                const uint32_t wi[4] = {bi.x, bi.y, bi.z, bi.w};
-                uint32_t* v1o = s_V1 + i0 * A.XV + x;
-                uint32_t* v2o = s_V2 + i0 * A.XV + x;
-#pragma unroll
-                for (int u = 0; u < 16; ++u) {
-                    if (i0 + u < nr) {
-                        v1o[u * A.XV] = h1;
-                        v2o[u * A.XV] = h2;
-                        const uint32_t o = (wo[u >> 2] >> (8 * (u & 3))) & 0xffu;
-                        uint32_t in;
-                        if (chr == 0) {
-                            in = (wi[u >> 2] >> (8 * (u & 3))) & 0xffu;
-                        } else {
-                            const int R = i0 + u + ch;
-                            in = colx[(R >> 4) * A.QS + (R & 15)];
-                        }
-                        h1 = h1 + in - o;
-                        h2 = h2 + in * in - o * o;
-                    }
-                }
-            }
-            asm volatile("bar.sync 1, %0;" ::"r"(kBT) : "memory");
-            // S[j][i] = sums of V[i][j .. j + cw - 1]: a task is a row i and 16 columns j.
+        // S[j][i] = sums of V[i][j .. j + cw - 1] for rows i in [i_lo, i_lo + ni): a task is a
+        // row i and 16 columns j (warps 0-5).
+        auto box_rows = [&](int i_lo, int ni) {
+            constexpr int kBT = kTcThreads - 64;
             const int jseg = (nc + 15) >> 4;
             const bool vec = (cw & 3) == 0;
-            for (int task = tid; task < nr * jseg; task += kBT) {
-                const int sg = task / nr, i = task - sg * nr;
+            for (int task = tid; task < ni * jseg; task += kBT) {
+                const int sg = task / ni, i = i_lo + (task - sg * ni);
                 const int j0 = 16 * sg;
                 const uint32_t* r1 = s_V1 + i * A.XV;
                 const uint32_t* r2 = s_V2 + i * A.XV;
@@ -1754,7 +1746,130 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
                     }
                 }
             }
+        };
+        // Box sums of W and W^2 (integral_both!, boxsum, src/integral.jl:141-170, 244-247) as
+        // exact integers, warps 0-5 (named barrier 1) while warps 6 and 7 issue the products. When
+        // the held sums belong to the same window geometry `sh` rows higher, they move up `sh`
+        // rows and only the last `sh` rows are computed.
+        const int64_t sh64 = win_r - h_wr;
+        const bool carry = held && win_c == h_wc && ch == h_ch && cw == h_cw && nr == h_nr &&
+                           nc == h_nc && sh64 > 0 && sh64 < nr;
+        if (warp < 6) {
+            constexpr int kBT = kTcThreads - 64;
+            if (carry) {
+                const int sh = static_cast<int>(sh64);
+                // Move: a warp per surface column, 32 rows per step (all loads of a step
+                // before its stores, reading ahead of what it overwrites).
+                for (int j = warp; j < nc; j += 6) {
+                    uint32_t* c1 = s_S1 + j * A.NRS;
+                    uint32_t* c2 = s_S2 + j * A.NRS;
+                    for (int c = 0; c < nr - sh; c += 32) {
+                        const int i = c + lane;
+                        uint32_t v1 = 0, v2 = 0;
+                        if (i < nr - sh) {
+                            v1 = c1[i + sh];
+                            v2 = c2[i + sh];
+                        }
+                        __syncwarp();
+                        if (i < nr - sh) {
+                            c1[i] = v1;
+                            c2[i] = v2;
+                        }
+                        __syncwarp();
+                    }
+                }
+                // Column sums of the new rows i in [nr - sh, nr), a thread per window column.
+                const int i0 = nr - sh;
+                for (int x = tid; x < XW; x += kBT) {
+                    const uint8_t* colx = s_W + x * 16;
+                    uint32_t h1 = 0, h2 = 0;
+                    for (int a = 0; a < ch; ++a) {
+                        const int R = i0 + a;
+                        const uint32_t w = colx[(R >> 4) * A.QS + (R & 15)];
+                        h1 += w;
+                        h2 += w * w;
+                    }
+                    for (int i = i0; i < nr; ++i) {
+                        s_V1[i * A.XV + x] = h1;
+                        s_V2[i * A.XV + x] = h2;
+                        if (i + 1 < nr) {
+                            const uint32_t o = colx[(i >> 4) * A.QS + (i & 15)];
+                            const int R = i + ch;
+                            const uint32_t n = colx[(R >> 4) * A.QS + (R & 15)];
+                            h1 = h1 + n - o;
+                            h2 = h2 + n * n - o * o;
+                        }
+                    }
+                }
+                asm volatile("bar.sync 1, %0;" ::"r"(kBT) : "memory");
+                box_rows(i0, sh);
+            } else {
+                // V[i][x] = sums over rows i .. i + ch - 1 of column x: a task is a column and the 16
+                // rows i of one block; its outgoing rows are that block, its incoming rows start ch
+                // rows lower.
+                const int nseg = (nr + 15) >> 4;
+                const int chb = ch >> 4, chr = ch & 15;
+                for (int task = tid; task < XW * nseg; task += kBT) {
+                    const int sgi = task / XW, x = task - sgi * XW;
+                    const int i0 = 16 * sgi;
+                    const uint8_t* colx = s_W + x * 16;
+                    const uint4 bo = *reinterpret_cast<const uint4*>(colx + sgi * A.QS);
+                    uint32_t h1 = 0, h2 = 0;
+                    for (int bb = 0; bb < chb; ++bb) {
+                        const uint4 w = *reinterpret_cast<const uint4*>(colx + (sgi + bb) * A.QS);
+                        h1 = __dp4a(w.x, 0x01010101u, h1);
+                        h1 = __dp4a(w.y, 0x01010101u, h1);
+                        h1 = __dp4a(w.z, 0x01010101u, h1);
+                        h1 = __dp4a(w.w, 0x01010101u, h1);
+                        h2 = __dp4a(w.x, w.x, h2);
+                        h2 = __dp4a(w.y, w.y, h2);
+                        h2 = __dp4a(w.z, w.z, h2);
+                        h2 = __dp4a(w.w, w.w, h2);
+                    }
+                    const uint4 bi = *reinterpret_cast<const uint4*>(colx + (sgi + chb) * A.QS);
+                    if (chr) {
+                        const uint32_t wv[4] = {bi.x, bi.y, bi.z, bi.w};
+#pragma unroll
+                        for (int m = 0; m < 4; ++m) {
+                            const int keep = min(max(chr - 4 * m, 0), 4);
+                            const uint32_t mk = keep == 4 ? 0xffffffffu : ((1u << (8 * keep)) - 1u);
+                            h1 = __dp4a(wv[m] & mk, 0x01010101u, h1);
+                            h2 = __dp4a(wv[m] & mk, wv[m], h2);
+                        }
+                    }
+                    const uint32_t wo[4] = {bo.x, bo.y, bo.z, bo.w};
+                    const uint32_t wi[4] = {bi.x, bi.y, bi.z, bi.w};
+                    uint32_t* v1o = s_V1 + i0 * A.XV + x;
+                    uint32_t* v2o = s_V2 + i0 * A.XV + x;
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) {
+                        if (i0 + u < nr) {
+                            v1o[u * A.XV] = h1;
+                            v2o[u * A.XV] = h2;
+                            const uint32_t o = (wo[u >> 2] >> (8 * (u & 3))) & 0xffu;
+                            uint32_t in;
+                            if (chr == 0) {
+                                in = (wi[u >> 2] >> (8 * (u & 3))) & 0xffu;
+                            } else {
+                                const int R = i0 + u + ch;
+                                in = colx[(R >> 4) * A.QS + (R & 15)];
+                            }
+                            h1 = h1 + in - o;
+                            h2 = h2 + in * in - o * o;
+                        }
+                    }
+                }
+                asm volatile("bar.sync 1, %0;" ::"r"(kBT) : "memory");
+                box_rows(0, nr);
+            }
         }
+        held = true;
+        h_wr = win_r;
+        h_wc = win_c;
+        h_ch = ch;
+        h_cw = cw;
+        h_nr = nr;
+        h_nc = nc;
         TC_PHASE(6)
         bool ok = tc::mbar_wait(&s_mbar, phase, kTcWaitPolls);
         phase ^= 1u;
@@ -1787,8 +1902,12 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
         if (32 * half < nr) {
             const uint32_t base = taddr + (static_cast<uint32_t>(32 * quarter) << 16) + col0 +
                                   static_cast<uint32_t>(32 * half);
+            uint32_t dv1[16];
             tc::tmem_ld16dp(base, dv);
+            tc::tmem_ld16dp(base + acc1, dv1);
             tc::tmem_wait_ld();
+#pragma unroll
+            for (int v = 0; v < 16; ++v) dv[v] += dv1[v];  // the two halves of the chip columns
 #pragma unroll
             for (int v = 0; v < 16; ++v) {
                 const int i = ib0 + 8 * (v >> 2) + (v & 1), j = jb0 + ((v & 2) ? 8 : 0);
@@ -1902,6 +2021,12 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
         TC_PHASE_POINT
     }
     TC_PHASE_FLUSH
+#ifdef AR_TC_PHASES
+    if (tid == kTcThreads - 32) {
+        atomicAdd(&g_tc_phase[12], tmi_issue);
+        atomicAdd(&g_tc_phase[13], tmi_done);
+    }
+#endif
     if (failed) tc::mbar_wait(&s_mbar, phase ^ 1u, kTcWaitPolls);
     tc::fence_before_sync();
     __syncthreads();
@@ -2433,7 +2558,7 @@ size_t tmem_smem_floor(uint32_t cols, size_t static_smem) {
 struct TcPlan {
     int NB, QM, QS, PS, PC, XS, XT, NRS, NRM, NCM, CHM, CWM, BC, big, MT;
     unsigned off_E, off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
-    int XV = 0;
+    int XV = 0, acc1_col = 0;
     uint32_t tmem_cols;
     size_t smem;
 };
@@ -2464,8 +2589,9 @@ bool plan_corr_tc2(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
     const int reads = P->NB - 16 + 32 * ((nr + 31) / 32);  // columns the epilogue reads
     uint32_t t1 = 32;
     while (static_cast<int>(t1) < std::max(dcols, reads)) t1 <<= 1;
-    if (t1 > 512) return false;
-    P->tmem_cols = t1;
+    if (2 * t1 > 512) return false;
+    P->acc1_col = static_cast<int>(t1);  // two accumulators of t1 columns
+    P->tmem_cols = 2 * t1;
     auto a16 = [](size_t v) { return (v + 15) & ~size_t(15); };
     const size_t Eb = static_cast<size_t>(cw) * P->PS;
     const size_t Wb = static_cast<size_t>(P->QM) * P->QS;
@@ -2827,6 +2953,7 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         B.off_est = TP.off_est;
         B.off_red = TP.off_red;
         B.XV = TP.XV;
+        B.acc1_col = TP.acc1_col;
         B.tmem_cols = TP.tmem_cols;
         B.out = out;
         B.sub_count = scratch.sub_count;

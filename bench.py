@@ -202,33 +202,37 @@ def serving_requests(ar, rng, n_req, sizes, weights, base=None):
     return scenes, reqs
 
 
-def serving_measure(ar, scenes, reqs, device, slots=4, rate=None):
-    """The stream through the plain one-pair-at-a-time path and through the request loop.
-    Returns points/s of each, and per-request latency (queued + running, from the loop's own
-    clock) for a Poisson stream at `rate` requests/s (default: 70% of the measured capacity)."""
+def serving_measure(ar, scenes, reqs, device, slots=4, rate=None, repeats=3):
+    """The stream through the plain one-pair-at-a-time path and through the request loop,
+    alternated `repeats` times (medians reported: the plain path of small pairs is bound by host
+    round trips, so single runs vary with the host). Returns points/s of each, and per-request
+    latency (queued + running, from the loop's own clock) for a Poisson stream at `rate`
+    requests/s (default: 70% of the measured capacity)."""
     L = ar._lib
     points = [len(ar.build_grid(scenes[n][0].shape, ar.params(**kw))) for n, kw in reqs]
     plain_ctx = L.Context(device)
-    a, b, v = scenes[reqs[0][0]]
-    ar.autorift(a, b, secondary_valid=v, ctx=plain_ctx, **reqs[0][1])  # warm-up
-    t0 = time.perf_counter()
-    for n, kw in reqs:
-        a, b, v = scenes[n]
-        ar.autorift(a, b, secondary_valid=v, ctx=plain_ctx, **kw)
-    plain_s = time.perf_counter() - t0
-    plain_ctx.close()
-
     ctx = L.Context(device)
     ctx.set_option(L.AR_OPT_SERVE_SLOTS, slots)
     a, b, v = scenes[reqs[0][0]]
+    ar.autorift(a, b, secondary_valid=v, ctx=plain_ctx, **reqs[0][1])  # warm-up
     ar.submit(a, b, secondary_valid=v, ctx=ctx, **reqs[0][1]).wait()  # warm-up: starts the loop
-    t0 = time.perf_counter()
-    tickets = [ar.submit(*scenes[n][:2], secondary_valid=scenes[n][2], ctx=ctx, **kw)
-               for n, kw in reqs]
-    for t in tickets:
-        t.wait()
-    burst_s = time.perf_counter() - t0
-    del tickets
+    plain_runs, burst_runs = [], []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        for n, kw in reqs:
+            a, b, v = scenes[n]
+            ar.autorift(a, b, secondary_valid=v, ctx=plain_ctx, **kw)
+        plain_runs.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        tickets = [ar.submit(*scenes[n][:2], secondary_valid=scenes[n][2], ctx=ctx, **kw)
+                   for n, kw in reqs]
+        for t in tickets:
+            t.wait()
+        burst_runs.append(time.perf_counter() - t0)
+        del tickets
+    plain_ctx.close()
+    plain_s = float(np.median(plain_runs))
+    burst_s = float(np.median(burst_runs))
     cap = len(reqs) / burst_s
     rate = rate or 0.7 * cap
     rng = np.random.default_rng(1)
@@ -249,10 +253,11 @@ def serving_measure(ar, scenes, reqs, device, slots=4, rate=None):
     del tickets
     ctx.close()
     total = float(sum(points))
-    return {"requests": len(reqs), "points": int(total), "slots": slots,
+    return {"requests": len(reqs), "points": int(total), "slots": slots, "repeats": repeats,
             "plain_points_per_s": total / plain_s, "plain_pairs_per_s": len(reqs) / plain_s,
             "batched_points_per_s": total / burst_s, "batched_pairs_per_s": cap,
             "speedup_vs_plain": plain_s / burst_s,
+            "speedup_per_repeat": [p / q for p, q in zip(plain_runs, burst_runs)],
             "stream_rate_pairs_per_s": rate, "stream_points_per_s": total / stream_s,
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
 
@@ -394,11 +399,12 @@ def gpu_arm(args):
         # A short mixed stream (image sides 512, 2048, 4096 in proportion 8:4:2) through the
         # plain path and the request loop.
         try:
-            sc, reqs = serving_requests(ar, np.random.default_rng(5), 14, (512, 2048, N),
+            sc, reqs = serving_requests(ar, np.random.default_rng(5), 28, (512, 2048, N),
                                         (8, 4, 2), base=(a, b, valid))
             serving = serving_measure(ar, sc, reqs, local)
-            serving["workload"] = ("14 requests, sides 512/2048/4096 (8:4:2), spacing {8,16,32}, "
-                                   "chip {16,32,64}, radius U[8,48], PyramidRefine(64); latency "
+            serving["workload"] = ("28 requests, sides 512/2048/4096 (8:4:2), spacing {8,16,32}, "
+                                   "chip {16,32,64}, radius U[8,48], PyramidRefine(64); plain "
+                                   "and batched passes alternated 3 times (medians); latency "
                                    "from submission to completion at a Poisson rate of 70% of "
                                    "capacity")
         except Exception as exc:  # reported, not fatal to the main measurement
