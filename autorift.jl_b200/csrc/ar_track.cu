@@ -1754,45 +1754,76 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
         const int64_t sh64 = win_r - h_wr;
         const bool carry = held && win_c == h_wc && ch == h_ch && cw == h_cw && nr == h_nr &&
                            nc == h_nc && sh64 > 0 && sh64 < nr;
+#ifdef AR_TC_PHASES
+        if (tid == 0 && carry) atomicAdd(&g_tc_phase[14], 1ull);
+#endif
         if (warp < 6) {
             constexpr int kBT = kTcThreads - 64;
             if (carry) {
                 const int sh = static_cast<int>(sh64);
-                // Move: a warp per surface column, 32 rows per step (all loads of a step
-                // before its stores, reading ahead of what it overwrites).
+                // Move: a warp per surface column, 64 rows per step (all loads of a step before
+                // its stores, reading ahead of what it overwrites).
                 for (int j = warp; j < nc; j += 6) {
                     uint32_t* c1 = s_S1 + j * A.NRS;
                     uint32_t* c2 = s_S2 + j * A.NRS;
-                    for (int c = 0; c < nr - sh; c += 32) {
-                        const int i = c + lane;
-                        uint32_t v1 = 0, v2 = 0;
-                        if (i < nr - sh) {
-                            v1 = c1[i + sh];
-                            v2 = c2[i + sh];
+                    for (int c = 0; c < nr - sh; c += 64) {
+                        const int ia = c + lane, ib = c + 32 + lane;
+                        uint32_t a1 = 0, a2 = 0, b1 = 0, b2 = 0;
+                        if (ia < nr - sh) {
+                            a1 = c1[ia + sh];
+                            a2 = c2[ia + sh];
+                        }
+                        if (ib < nr - sh) {
+                            b1 = c1[ib + sh];
+                            b2 = c2[ib + sh];
                         }
                         __syncwarp();
-                        if (i < nr - sh) {
-                            c1[i] = v1;
-                            c2[i] = v2;
+                        if (ia < nr - sh) {
+                            c1[ia] = a1;
+                            c2[ia] = a2;
+                        }
+                        if (ib < nr - sh) {
+                            c1[ib] = b1;
+                            c2[ib] = b2;
                         }
                         __syncwarp();
                     }
                 }
-                // Column sums of the new rows i in [nr - sh, nr), a thread per window column.
+                // Column sums of the new rows i in [nr - sh, nr): an item is a window column and
+                // up to 4 consecutive rows; its first sum from 4-byte groups (dp4a), then a
+                // sliding update.
                 const int i0 = nr - sh;
-                for (int x = tid; x < XW; x += kBT) {
+                const int nparts = (sh + 3) >> 2;
+                for (int item = tid; item < XW * nparts; item += kBT) {
+                    const int pt = item / XW, x = item - pt * XW;
+                    const int ia = i0 + 4 * pt, ie = min(ia + 4, nr);
                     const uint8_t* colx = s_W + x * 16;
+                    // Rows r .. r + 3 of column x as one word (a group may cross a block).
+                    auto word = [&](int r) {
+                        const int rb = r >> 4, o = r & 15, ow = o & ~3;
+                        const uint32_t lo = *reinterpret_cast<const uint32_t*>(colx + rb * A.QS + ow);
+                        if ((o & 3) == 0) return lo;
+                        const int nb = ow + 4 < 16 ? rb : rb + 1, no = ow + 4 < 16 ? ow + 4 : 0;
+                        const uint32_t hi = nb < Q ? *reinterpret_cast<const uint32_t*>(colx + nb * A.QS + no) : 0u;
+                        return __funnelshift_r(lo, hi, 8u * static_cast<uint32_t>(o & 3));
+                    };
                     uint32_t h1 = 0, h2 = 0;
-                    for (int a = 0; a < ch; ++a) {
-                        const int R = i0 + a;
-                        const uint32_t w = colx[(R >> 4) * A.QS + (R & 15)];
-                        h1 += w;
-                        h2 += w * w;
+                    int a = 0;
+                    for (; a + 4 <= ch; a += 4) {
+                        const uint32_t w = word(ia + a);
+                        h1 = __dp4a(w, 0x01010101u, h1);
+                        h2 = __dp4a(w, w, h2);
                     }
-                    for (int i = i0; i < nr; ++i) {
+                    if (a < ch) {
+                        const uint32_t mk = (1u << (8 * (ch - a))) - 1u;
+                        const uint32_t w = word(ia + a) & mk;
+                        h1 = __dp4a(w, 0x01010101u, h1);
+                        h2 = __dp4a(w, w, h2);
+                    }
+                    for (int i = ia; i < ie; ++i) {
                         s_V1[i * A.XV + x] = h1;
                         s_V2[i * A.XV + x] = h2;
-                        if (i + 1 < nr) {
+                        if (i + 1 < ie) {
                             const uint32_t o = colx[(i >> 4) * A.QS + (i & 15)];
                             const int R = i + ch;
                             const uint32_t n = colx[(R >> 4) * A.QS + (R & 15)];
@@ -1802,7 +1833,36 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
                     }
                 }
                 asm volatile("bar.sync 1, %0;" ::"r"(kBT) : "memory");
-                box_rows(i0, sh);
+                // Row sums of the new rows: a task is a row and 4 consecutive columns j.
+                const int ng = (nc + 3) >> 2;
+                for (int task = tid; task < sh * ng; task += kBT) {
+                    const int g = task / sh, i = i0 + (task - g * sh);
+                    const int j0 = 4 * g;
+                    const uint32_t* r1 = s_V1 + i * A.XV;
+                    const uint32_t* r2 = s_V2 + i * A.XV;
+                    uint32_t g1 = 0, g2 = 0;
+                    int bb = 0;
+                    for (; bb + 4 <= cw; bb += 4) {
+                        const uint4 v = *reinterpret_cast<const uint4*>(r1 + j0 + bb);
+                        const uint4 w = *reinterpret_cast<const uint4*>(r2 + j0 + bb);
+                        g1 += (v.x + v.y) + (v.z + v.w);
+                        g2 += (w.x + w.y) + (w.z + w.w);
+                    }
+                    for (; bb < cw; ++bb) {
+                        g1 += r1[j0 + bb];
+                        g2 += r2[j0 + bb];
+                    }
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        const int j = j0 + m;
+                        if (j < nc) {
+                            s_S1[j * A.NRS + i] = g1;
+                            s_S2[j * A.NRS + i] = g2;
+                            g1 = g1 + r1[j + cw] - r1[j];
+                            g2 = g2 + r2[j + cw] - r2[j];
+                        }
+                    }
+                }
             } else {
                 // V[i][x] = sums over rows i .. i + ch - 1 of column x: a task is a column and the 16
                 // rows i of one block; its outgoing rows are that block, its incoming rows start ch
