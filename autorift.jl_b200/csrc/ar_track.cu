@@ -2972,8 +2972,8 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
     }
     TcPlan TP{};
     const bool tc_ok = dtype == AR_U8 && scratch.tensor_cores;
-    // k_corr_tc2 where it keeps two CTAs per SM; otherwise k_corr_tc.
-    const bool use_tc2 = tc_ok && plan_corr_tc2(geom, 112 * 1024, &TP) && TP.tmem_cols <= 256;
+    // k_corr_tc2 wherever its plan fits (one or two CTAs per SM); otherwise k_corr_tc.
+    const bool use_tc2 = tc_ok && plan_corr_tc2(geom, 220 * 1024, &TP);
     const bool use_tc = tc_ok && (use_tc2 || plan_corr_tc(geom, 220 * 1024, &TP));
     if (use_tc) {
         TcArgs B{};
