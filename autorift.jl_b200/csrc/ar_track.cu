@@ -645,6 +645,45 @@ __device__ __forceinline__ float tc_estimate(uint32_t D, uint32_t S1, uint32_t S
     return est;
 }
 
+// tc_estimate for two values at once on packed FP32 pairs: every operation rounds each lane as
+// the scalar form does, so the estimates and bounds are the scalar ones bit for bit.
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 tc_estimate2(uint32_t D0, uint32_t D1, uint32_t S10,
+                                               uint32_t S11, uint32_t S20, uint32_t S21,
+                                               float nnf, float csum, float k, float k7,
+                                               int measure, float2* bound) {
+    const float2 d = make_float2(__uint2float_rn(D0), __uint2float_rn(D1));
+    const float2 s1 = make_float2(__uint2float_rn(S10), __uint2float_rn(S11));
+    const float2 s2 = make_float2(__uint2float_rn(S20), __uint2float_rn(S21));
+    const float2 nn2 = make_float2(nnf, nnf);
+    const float2 p = __fmul2_rn(make_float2(csum, csum), s1);
+    const float2 nx = __ffma2_rn(nn2, d, neg2(p));
+    const float2 tn = __ffma2_rn(nn2, d, p);
+    float2 vx, tv;
+    if (measure == AR_NCC) {
+        vx = s2;
+        tv = s2;
+    } else {
+        const float2 q = __fmul2_rn(s1, s1);
+        vx = __ffma2_rn(nn2, s2, neg2(q));
+        tv = __ffma2_rn(nn2, s2, q);
+    }
+    const float2 ev = __fmul2_rn(make_float2(3.5762786865234375e-07f, 3.5762786865234375e-07f), tv);
+    const float2 ev64 = __fmul2_rn(make_float2(64.0f, 64.0f), ev);
+    const bool ok0 = vx.x > ev64.x, ok1 = vx.y > ev64.y;
+    const float2 r = make_float2(rsqrtf(ok0 ? vx.x : 1.0f), rsqrtf(ok1 ? vx.y : 1.0f));
+    const float2 est = __fmul2_rn(__fmul2_rn(nx, r), make_float2(k, k));
+    const float2 rel = __ffma2_rn(ev, __fmul2_rn(r, r),
+                                  make_float2(9.5367431640625e-07f, 9.5367431640625e-07f));
+    const float2 b = __fadd2_rn(
+        __ffma2_rn(make_float2(fabsf(est.x), fabsf(est.y)), __fmul2_rn(make_float2(2.0f, 2.0f), rel),
+                   __fmul2_rn(__fmul2_rn(tn, r), make_float2(k7, k7))),
+        make_float2(1e-30f, 1e-30f));
+    const float qn = __int_as_float(0x7fc00000);
+    *bound = make_float2(ok0 ? b.x : 0.0f, ok1 ? b.y : 0.0f);
+    return make_float2(ok0 ? est.x : qn, ok1 ? est.y : qn);
+}
+
 // Rows of the chip operand that block q's product needs: operand row e holds offset
 // u = e - NB + 16 (surface row i = 16 q + u), and only surface rows 0 <= i < nr are read, so
 // e runs over [max(0, NB - 16 - 16 q), min(NB, NB - 16 + nr - 16 q)). Returned as a 16-aligned
@@ -720,13 +759,14 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         tc::tmem_relinquish();
     }
     if (tid == 0) {
-        tc::mbar_init(&s_mbar, 1);
+        tc::mbar_init(&s_mbar, 2);  // one commit per issuing thread
         tc::fence_mbar_init();
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t taddr = s_taddr;
+    const uint32_t acc1 = static_cast<uint32_t>(A.acc1_col);  // second accumulator's first column
     uint32_t phase = 0;
     bool failed = false;
     if (tid < 4) s_isum[tid >> 1][tid & 1] = 0ull;
@@ -903,9 +943,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         // exact integers: V[i][x] sums ch rows down column x, S[j][i] sums cw columns of V.
         // They run while the tensor core works on the first chunk, or, when the chip operand
         // comes in several chunks that reuse their space, before it.
-        // Warps 0-6 only (named barrier 1): warp 7 issues the products meanwhile.
+        // Warps 0-5 only (named barrier 1): warps 6 and 7 issue the products meanwhile.
         auto box_sums = [&]() {
-            constexpr int kBT = kTcThreads - 32;
+            constexpr int kBT = kTcThreads - 64;
             uint32_t* s_V2 = s_V1 + A.NRM * XW;
             // V: one round of tasks (column x, a run of rows), each an unrolled first sum with
             // independent partials and a sliding update with the next values loaded ahead.
@@ -980,11 +1020,10 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             }
         };
         if (A.big) {
-            if (warp < 7) box_sums();
+            if (warp < 6) box_sums();
             __syncthreads();  // the chip chunks overwrite s_T and s_V
         }
 
-        const int dcols = 16 * (Q - 1) + A.NB;
         const int nchunk = (cw + A.BC - 1) / A.BC;
         bool ok = true;
         for (int cc = 0; cc < nchunk; ++cc) {
@@ -1025,32 +1064,46 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                 uint32_t z[16];
 #pragma unroll
                 for (int t = 0; t < 16; ++t) z[t] = 0u;
-                for (int c = 0; c < dcols; c += 16)
-                    tc::tmem_st16(taddr + (static_cast<uint32_t>(32 * warp) << 16) + static_cast<uint32_t>(c), z);
+                // Products land in columns [NB - 16, NB + nr) of block coordinates (their rows are
+                // trimmed to the surface rows), stored from column 0 of each accumulator.
+                const int zc = (nr + 16 + 15) & ~15;
+                const uint32_t lq = taddr + (static_cast<uint32_t>(32 * warp) << 16);
+                for (int c = 0; c < zc; c += 16) {
+                    tc::tmem_st16(lq + static_cast<uint32_t>(c), z);
+                    tc::tmem_st16(lq + acc1 + static_cast<uint32_t>(c), z);
+                }
                 tc::tmem_wait_st();
             }
             tc::fence_proxy_async_smem();
             tc::fence_before_sync();
             __syncthreads();
             TC_PHASE(5)
-            if (tid == kTcThreads - 32) {
+            // Two threads issue the products, each for half of the chunk's chip column pairs into
+            // its own accumulator (one thread's MMAs run one after another).
+            if (tid == kTcThreads - 32 || tid == kTcThreads - 64) {
+                const int stream = tid == kTcThreads - 32 ? 0 : 1;
                 tc::fence_after_sync();
                 const uint32_t sW = tc::smem_u32(s_W), sE = tc::smem_u32(s_E);
+                const int p0 = b0 / 2, p1 = b1 / 2, pm = p0 + (p1 - p0) / 2;
+                const int tb = stream == 0 ? p0 : pm, te = stream == 0 ? pm : p1;
+                const uint32_t dacc = taddr + (stream ? acc1 : 0u);
                 for (int q = 0; q < Q; ++q) {
-                    // Only the operand rows e in [elo, elo + n) of block q reach surface rows.
+                    // Only the operand rows e in [elo, elo + n) of block q reach surface rows;
+                    // their accumulator columns start at NB - 16 in block coordinates.
                     int elo, n;
                     if (!block_rows(q, A.NB, nr, &elo, &n)) continue;
                     const uint32_t idesc = tc::idesc_u8_s32(A.MT, n);
-                    for (int t = b0 / 2; t < b1 / 2; ++t) {
+                    const uint32_t dcol = static_cast<uint32_t>(16 * q + elo - (A.NB - 16));
+                    for (int t = tb; t < te; ++t) {
                         const uint64_t da = tc::smem_desc(sW + q * A.QS + 32 * t, 16, 128);
                         const uint64_t db =
                             tc::smem_desc(sE + (2 * t - b0) * A.PS + 16 * elo, A.PS, 128);
-                        tc::mma_u8(taddr + static_cast<uint32_t>(16 * q + elo), da, db, idesc, true);
+                        tc::mma_u8(dacc + dcol, da, db, idesc, true);
                     }
                 }
                 tc::mma_commit(&s_mbar);
             }
-            if (cc == 0 && !A.big && warp < 7) box_sums();
+            if (cc == 0 && !A.big && warp < 6) box_sums();
             TC_PHASE(6)
         }
         if (ok) {
@@ -1068,7 +1121,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
 
         // Pass 1: numerators out of Tensor Memory, estimates and bounds, the largest lower bound.
         // Surface column j is accumulator row j (lane (j % 16) + 32 (j / 16) of the M = 64
-        // layout); surface row i is accumulator column i + NB - 16. Warp w reads its quarter's
+        // layout); surface row i is column i of each accumulator (their sum). Warp w reads its quarter's
         // 16 lanes (16x256b: thread t gets rows 16 q + t/4 and + 8, columns 2 (t % 4) + {0, 1}
         // + 8 k), columns from 32 (w / 4) in steps of 64.
         const float kk = __double2float_rn(
@@ -1078,7 +1131,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         const float nnf = static_cast<float>(nnl);
         const float csf = static_cast<float>(csum_d);
         const int quarter = warp & 3, half = warp >> 2;
-        const uint32_t col0 = static_cast<uint32_t>(A.NB - 16);
+        const uint32_t col0 = 0u;
         float lmax = -INFINITY;
         if constexpr (REG) {
             // One read per warp: value v of this thread is surface row
@@ -1090,9 +1143,14 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             float upb[16];
             uint32_t vm = 0u;  // values of this thread inside the surface
             if (32 * half < nr) {
-                tc::tmem_ld16dp(taddr + (static_cast<uint32_t>(32 * quarter) << 16) + col0 +
-                                    static_cast<uint32_t>(32 * half), dv);
+                const uint32_t base = taddr + (static_cast<uint32_t>(32 * quarter) << 16) + col0 +
+                                      static_cast<uint32_t>(32 * half);
+                uint32_t dv1[16];
+                tc::tmem_ld16dp(base, dv);
+                tc::tmem_ld16dp(base + acc1, dv1);
                 tc::tmem_wait_ld();
+#pragma unroll
+                for (int v = 0; v < 16; ++v) dv[v] += dv1[v];
 #pragma unroll
                 for (int v = 0; v < 16; ++v) {
                     const int i = ib0 + 8 * (v >> 2) + (v & 1), j = jb0 + ((v & 2) ? 8 : 0);
@@ -1214,10 +1272,14 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         };
         if (A.MT == 64) {
             for (int i0 = 32 * half; i0 < nr; i0 += 64) {
-                uint32_t r[16];
-                tc::tmem_ld16dp(taddr + (static_cast<uint32_t>(32 * quarter) << 16) + col0 +
-                                    static_cast<uint32_t>(i0), r);
+                uint32_t r[16], r1[16];
+                const uint32_t base = taddr + (static_cast<uint32_t>(32 * quarter) << 16) + col0 +
+                                      static_cast<uint32_t>(i0);
+                tc::tmem_ld16dp(base, r);
+                tc::tmem_ld16dp(base + acc1, r1);
                 tc::tmem_wait_ld();
+#pragma unroll
+                for (int v = 0; v < 16; ++v) r[v] += r1[v];
 #pragma unroll
                 for (int v = 0; v < 16; ++v)
                     take(r[v], i0 + 8 * (v >> 2) + 2 * (lane & 3) + (v & 1),
@@ -1226,10 +1288,14 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         } else {
             // M = 128: accumulator row j is lane j; thread = row 32 q + lane, 16 columns.
             for (int i0 = 16 * half; i0 < nr; i0 += 32) {
-                uint32_t r[16];
-                tc::tmem_ld16(taddr + (static_cast<uint32_t>(32 * quarter) << 16) + col0 +
-                                  static_cast<uint32_t>(i0), r);
+                uint32_t r[16], r1[16];
+                const uint32_t base = taddr + (static_cast<uint32_t>(32 * quarter) << 16) + col0 +
+                                      static_cast<uint32_t>(i0);
+                tc::tmem_ld16(base, r);
+                tc::tmem_ld16(base + acc1, r1);
                 tc::tmem_wait_ld();
+#pragma unroll
+                for (int m = 0; m < 16; ++m) r[m] += r1[m];
 #pragma unroll
                 for (int m = 0; m < 16; ++m) take(r[m], i0 + m, 32 * quarter + lane);
             }
@@ -1968,18 +2034,25 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
             tc::tmem_wait_ld();
 #pragma unroll
             for (int v = 0; v < 16; ++v) dv[v] += dv1[v];  // the two halves of the chip columns
+            // Values v and v + 1 are surface rows i and i + 1 of one column: estimated as a pair.
 #pragma unroll
-            for (int v = 0; v < 16; ++v) {
-                const int i = ib0 + 8 * (v >> 2) + (v & 1), j = jb0 + ((v & 2) ? 8 : 0);
-                upb[v] = -INFINITY;
-                if (i < nr && j < nc) {
-                    vm |= 1u << v;
-                    float bnd;
+            for (int v = 0; v < 16; v += 2) {
+                const int i = ib0 + 8 * (v >> 2), j = jb0 + ((v & 2) ? 8 : 0);
+                upb[v] = upb[v + 1] = -INFINITY;
+                if (j < nc && i < nr) {
+                    const bool two = i + 1 < nr;
+                    vm |= (two ? 3u : 1u) << v;
                     const int o = j * A.NRS + i;
-                    const float est = tc_estimate(dv[v], s_S1[o], s_S2[o], nnf, csf, kk, kk7,
-                                                  A.measure, &bnd);
-                    upb[v] = est + bnd;
-                    lmax = fmaxf(lmax, est - bnd);
+                    const uint32_t b1 = two ? s_S1[o + 1] : 0u, b2 = two ? s_S2[o + 1] : 0u;
+                    float2 bnd;
+                    const float2 est = tc_estimate2(dv[v], dv[v + 1], s_S1[o], b1, s_S2[o], b2,
+                                                    nnf, csf, kk, kk7, A.measure, &bnd);
+                    upb[v] = est.x + bnd.x;
+                    lmax = fmaxf(lmax, est.x - bnd.x);
+                    if (two) {
+                        upb[v + 1] = est.y + bnd.y;
+                        lmax = fmaxf(lmax, est.y - bnd.y);
+                    }
                 }
             }
         }
@@ -2706,11 +2779,15 @@ bool plan_corr_tc(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
     P->XT = round_up(cw + nc - 1, 4) + 4;
     P->PC = round_up(kPadL + P->NB + 20, 16);
     P->NRS = nr | 1;
-    const int dcols = 16 * (P->QM - 1) + P->NB;
+    // Two accumulators, each holding the columns of surface rows 0 .. nr + 15 (the products'
+    // rows are trimmed to the surface rows) and whatever the epilogue's reads reach.
+    const int used = (nr + 16 + 15) & ~15;
+    const int reads = P->MT == 64 ? 32 * ((nr + 31) / 32) : 16 * ((nr + 15) / 16);
     uint32_t cols = 32;
-    while (static_cast<int>(cols) < dcols) cols <<= 1;
-    if (cols > 512) return false;
-    P->tmem_cols = cols;
+    while (static_cast<int>(cols) < std::max(used, reads)) cols <<= 1;
+    if (2 * cols > 512) return false;
+    P->acc1_col = static_cast<int>(cols);
+    P->tmem_cols = 2 * cols;
     auto a16 = [](size_t v) { return (v + 15) & ~size_t(15); };
     const size_t Eb = static_cast<size_t>(cw) * P->PS;
     const size_t Wb = static_cast<size_t>(P->QM) * P->QS;
