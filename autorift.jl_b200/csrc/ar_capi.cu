@@ -28,9 +28,6 @@ struct ar_ctx {
     // Device buffers for host point sets and outputs, grown on demand.
     void* dbuf = nullptr;
     size_t dbuf_bytes = 0;
-    // Scratch of the multichip search, grown on demand.
-    void* arena = nullptr;
-    size_t arena_bytes = 0;
     // Stream-ordered pool for pair images and per-call scratch: freed blocks stay with the
     // context and are reused without a device-wide synchronisation.
     cudaMemPool_t pool = nullptr;
@@ -172,10 +169,11 @@ cudaError_t stage_d2h(ar_ctx* c, void* dst, const void* src, size_t bytes) {
 
 cudaError_t ensure_dbuf(ar_ctx* c, size_t bytes) {
     if (c->dbuf_bytes >= bytes) return cudaSuccess;
-    cudaFree(c->dbuf);
+    // Stream-ordered on the context stream (the only one that uses these buffers).
+    if (c->dbuf) cudaFreeAsync(c->dbuf, c->stream);
     c->dbuf = nullptr;
     c->dbuf_bytes = 0;
-    cudaError_t e = cudaMalloc(&c->dbuf, bytes);
+    cudaError_t e = cudaMallocFromPoolAsync(&c->dbuf, bytes, c->pool, c->stream);
     if (e != cudaSuccess) return e;
     c->dbuf_bytes = bytes;
     return cudaSuccess;
@@ -269,6 +267,7 @@ int ar_ctx_create(int device, ar_ctx** out) {
         delete c;
         return AR_ERR_CUDA;
     }
+    c->scratch.pool = c->pool;
     *out = c;
     return AR_OK;
 }
@@ -296,7 +295,6 @@ int ar_ctx_destroy(ar_ctx* c) {
         cudaFree(c->scratch.timer.flops);
         if (c->scratch.done) cudaEventDestroy(c->scratch.done);
         cudaFree(c->dbuf);
-        cudaFree(c->arena);
         if (c->pinned) cudaFreeHost(c->pinned);
         for (auto& ev : c->staged)
             if (ev) cudaEventDestroy(ev);
@@ -693,16 +691,12 @@ int multichip_run(ar_ctx* c, const ar_pair* p, const double* gx, const double* g
                   const int64_t* grx, const int64_t* gry, const double* gdx0, const double* gdy0,
                   int64_t gr, int64_t gc, const ar_multichip_params* prm, float* dx, float* dy,
                   float* corr, uint16_t* chip, uint8_t* interp, cudaStream_t s) {
+    // The search's scratch comes from the context's pool in stream order on `s` (no
+    // device-wide synchronisation, so the request loop's slots never stall one another).
     const size_t ab = ar::multichip_arena_bytes(gr, gc);
-    if (c->arena_bytes < ab) {
-        cudaDeviceSynchronize();
-        cudaFree(c->arena);
-        c->arena = nullptr;
-        c->arena_bytes = 0;
-        cudaError_t e = cudaMalloc(&c->arena, ab);
-        if (e != cudaSuccess) return cuda_fail(c, e, "ar_multichip: scratch");
-        c->arena_bytes = ab;
-    }
+    void* arena = nullptr;
+    cudaError_t ea = cudaMallocFromPoolAsync(&arena, ab, c->pool, s);
+    if (ea != cudaSuccess) return cuda_fail(c, ea, "ar_multichip: scratch");
     ar::MultichipJob J{};
     J.dtype = p->dtype;
     J.ref = p->ref;
@@ -741,10 +735,11 @@ int multichip_run(ar_ctx* c, const ar_pair* p, const double* gx, const double* g
     P.gtol = prm->agree_tolerance;
     P.gmad = prm->mad_scale;
     P.fill_window = prm->fill_window;
-    J.arena = c->arena;
-    J.arena_bytes = c->arena_bytes;
+    J.arena = arena;
+    J.arena_bytes = ab;
     std::string err;
     cudaError_t e = ar::run_multichip(J, c->scratch, c->num_sms, s, &err);
+    cudaFreeAsync(arena, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess)
         return err.empty() ? cuda_fail(c, e, "ar_multichip") : fail(c, AR_ERR_UNSUPPORTED, err);

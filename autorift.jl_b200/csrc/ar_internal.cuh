@@ -73,6 +73,9 @@ struct TrackScratch {
     int* status = nullptr;
     // UInt8 passes use the tensor-core correlation when their geometry fits it.
     bool tensor_cores = true;
+    // When set, the sub-pixel queue grows from this pool in stream order (no device-wide
+    // synchronisation when a context first meets a larger pass).
+    cudaMemPool_t pool = nullptr;
 };
 
 // Reads and clears the pass status; AR-style: 0 ok, 1 a bounded device wait ran out.

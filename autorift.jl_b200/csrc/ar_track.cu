@@ -2862,7 +2862,7 @@ cudaError_t launch_corr_t(const CorrArgs& A, const CorrPlan& P, int grid, cudaSt
     return cudaGetLastError();
 }
 
-cudaError_t ensure_scratch(TrackScratch& s, int64_t n) {
+cudaError_t ensure_scratch(TrackScratch& s, int64_t n, cudaStream_t stream) {
     if (!s.geom) {
         cudaError_t e = cudaMalloc(&s.geom, 8 * sizeof(int64_t));
         if (e != cudaSuccess) return e;
@@ -2877,17 +2877,38 @@ cudaError_t ensure_scratch(TrackScratch& s, int64_t n) {
         if (e != cudaSuccess) return e;
     }
     if (s.capacity >= n) return cudaSuccess;
-    cudaFree(s.sub_point);
-    cudaFree(s.sub_origin);
-    cudaFree(s.sub_patch);
-    s.sub_point = nullptr;
-    s.sub_origin = nullptr;
-    s.sub_patch = nullptr;
-    s.capacity = 0;
     const int64_t cap = std::max<int64_t>(n, 1024);
-    cudaError_t e = cudaMalloc(&s.sub_point, cap * sizeof(int64_t));
-    if (e == cudaSuccess) e = cudaMalloc(&s.sub_origin, cap * 2 * sizeof(int32_t));
-    if (e == cudaSuccess) e = cudaMalloc(&s.sub_patch, cap * 25 * sizeof(float));
+    cudaError_t e = cudaSuccess;
+    if (s.pool) {
+        // Stream-ordered: the old queue is released after the work already on `stream`.
+        if (s.sub_point) cudaFreeAsync(s.sub_point, stream);
+        if (s.sub_origin) cudaFreeAsync(s.sub_origin, stream);
+        if (s.sub_patch) cudaFreeAsync(s.sub_patch, stream);
+        s.sub_point = nullptr;
+        s.sub_origin = nullptr;
+        s.sub_patch = nullptr;
+        s.capacity = 0;
+        void* a = nullptr;
+        void* b = nullptr;
+        void* c = nullptr;
+        e = cudaMallocFromPoolAsync(&a, cap * sizeof(int64_t), s.pool, stream);
+        if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&b, cap * 2 * sizeof(int32_t), s.pool, stream);
+        if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&c, cap * 25 * sizeof(float), s.pool, stream);
+        s.sub_point = static_cast<int64_t*>(a);
+        s.sub_origin = static_cast<int32_t*>(b);
+        s.sub_patch = static_cast<float*>(c);
+    } else {
+        cudaFree(s.sub_point);
+        cudaFree(s.sub_origin);
+        cudaFree(s.sub_patch);
+        s.sub_point = nullptr;
+        s.sub_origin = nullptr;
+        s.sub_patch = nullptr;
+        s.capacity = 0;
+        e = cudaMalloc(&s.sub_point, cap * sizeof(int64_t));
+        if (e == cudaSuccess) e = cudaMalloc(&s.sub_origin, cap * 2 * sizeof(int32_t));
+        if (e == cudaSuccess) e = cudaMalloc(&s.sub_patch, cap * 25 * sizeof(float));
+    }
     if (e != cudaSuccess) return e;
     s.capacity = cap;
     return cudaSuccess;
@@ -2946,7 +2967,7 @@ cudaError_t pass_geometry_device(const DevPoints& pts, int64_t nrows, int64_t nc
                                  TrackScratch& scratch, cudaStream_t stream, PassGeometry* out) {
     cudaError_t e = scratch_acquire(scratch, stream);
     if (e != cudaSuccess) return e;
-    e = ensure_scratch(scratch, 0);
+    e = ensure_scratch(scratch, 0, stream);
     if (e != cudaSuccess) return e;
     long long init[8] = {0, 0, 0, 0, 0, 0, 1, 0};
     e = cudaMemcpyAsync(scratch.geom, init, sizeof(init), cudaMemcpyHostToDevice, stream);
@@ -2988,7 +3009,7 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
                               const PassGeometry& geom, int up, int measure,
                               const DevOutputs& out, TrackScratch& scratch, int num_sms,
                               cudaStream_t stream, std::string* err, float* surf_out) {
-    cudaError_t e = ensure_scratch(scratch, pts.n);
+    cudaError_t e = ensure_scratch(scratch, pts.n, stream);
     if (e != cudaSuccess) return e;
     if (pts.n > 0) {
         const int threads = 256;
