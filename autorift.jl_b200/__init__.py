@@ -6,8 +6,8 @@ Loaded under the module name ``autorift_b200`` (the directory name is not an ide
 
 from . import _lib, synthetic
 from .methods import (GardnerFilter, Highpass, NCC, NoOutlierFilter, NoPreprocess, NoQuantize,
-                      NoRefine, Params, PyramidRefine, QuantizeUInt8, Wallis, ZNCC, chip_sizes,
-                      params, upsampling)
+                      NoRefine, NoRotationSearch, Params, PyramidRefine, QuantizeUInt8,
+                      RotationSearch, Wallis, ZNCC, angles, chip_sizes, params, upsampling)
 from .points import (PointSet, gridpoints, gridpoints_xy, nsearchable, npoints, pointset,
                      sanitize)
 from .api import (Ticket, submit, multichip_params, Cache, MultichipResult, autorift, autorift_, build_grid, correlate_multichip,
@@ -22,5 +22,6 @@ __all__ = [
     "pointset", "sanitize", "DisplacementField", "ImagePair", "correlate", "displacement_field",
     "nmeasured", "refine_patches", "track", "PreparedPair", "prepare", "Cache",
     "MultichipResult", "autorift", "autorift_", "build_grid", "correlate_multichip", "init",
-    "reinit_", "prepare_options", "multichip_params", "submit", "Ticket",
+    "reinit_", "prepare_options", "multichip_params", "submit", "Ticket", "NoRotationSearch",
+    "RotationSearch", "angles",
 ]

@@ -41,7 +41,7 @@ class ArMultichipParams(ctypes.Structure):
                 ("measure", _i32), ("outliers", _i32), ("outlier_window", _i32),
                 ("outlier_iterations", _i32), ("min_agree_fraction", ctypes.c_double),
                 ("agree_tolerance", ctypes.c_double), ("mad_scale", ctypes.c_double),
-                ("fill_window", _i32)]
+                ("fill_window", _i32), ("rotation_count", _i32), ("rotation_angles", _p)]
 
 
 class ArPoints(ctypes.Structure):
@@ -79,6 +79,8 @@ SIGNATURES = {
     "ar_pair_download": (_i32, [_p, _p, _p, _p, _p, _p]),
     "ar_pair_info": (_i32, [_p, ctypes.POINTER(_i32), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "ar_track": (_i32, [_p, _p, ctypes.POINTER(ArPoints), _i32, _i32, _p, _p, _p, _p]),
+    "ar_track_rotated": (_i32, [_p, _p, ctypes.POINTER(ArPoints), _i32, _i32, _p, _i32, _p, _p,
+                                _p, _p]),
     "ar_track_device": (_i32, [_p, _p, ctypes.POINTER(ArPoints), _i32, _i32, _p, _p, _p, _p, _p]),
     "ar_track_device_static": (_i32, [_p, _p, _p, _i64, _i64, _i32, ctypes.POINTER(ArPoints), _i32,
                                       _i32, _p, _p, _p, _p, _p, ctypes.c_char_p, _sz]),

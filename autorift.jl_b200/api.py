@@ -15,7 +15,8 @@ from . import _lib
 from .methods import (GardnerFilter, NoOutlierFilter, Params, chip_sizes, params as make_params,
                       upsampling)
 from .points import PointSet, gridpoints
-from .track import ImagePair, PreparedPair, _measure_code, points_struct, prepare, prepare_options
+from .track import (ImagePair, PreparedPair, _measure_code, points_struct, prepare,
+                    prepare_options, rotation_angles)
 
 
 @dataclass
@@ -50,11 +51,17 @@ def multichip_params(p: Params) -> "_lib.ArMultichipParams":
                          f"{len(chip_sizes(p))} chip-size levels.")
     if len({type(m) for m in p.similarity}) > 1:
         raise ValueError("per-level similarity tuples are not supported on the GPU")
-    return _lib.ArMultichipParams(
+    prm = _lib.ArMultichipParams(
         p.chip_size_base, p.chip_size_min, p.chip_size_max, p.chip_aspect,
         p.min_search_radius, p.coarse_stride, p.coarse_buffer, p.min_coarse_valid_fraction,
         upsampling(p.subpixel), _measure_code(p.similarity[0]), kind, w, it, fr, tol, mad,
         p.fill_window)
+    rot = rotation_angles(p)
+    if rot is not None:
+        prm.rotation_count = rot.size
+        prm.rotation_angles = rot.ctypes.data
+        prm._angles = rot  # the array the struct points at lives as long as the struct
+    return prm
 
 
 def correlate_multichip(pair, grid: PointSet, p: Params | None = None, ctx=None) -> MultichipResult:
@@ -271,12 +278,13 @@ def submit(reference, secondary, grid: PointSet | None = None, *, reference_vali
     st, cols = points_struct(grid)
     outs = [np.empty(n, np.float32) for _ in range(3)] + [np.empty(n, np.uint16),
                                                            np.empty(n, np.uint8)]
+    prm = multichip_params(p)  # holds the rotation angles the request points at
     req = _lib.ArRequest(
         arrays[0].ctypes.data, arrays[1].ctypes.data,
         masks[0].ctypes.data if masks[0] is not None else None,
         masks[1].ctypes.data if masks[1] is not None else None,
-        ref.shape[0], ref.shape[1], DTYPES[ref.dtype], prepare_options(p), multichip_params(p),
+        ref.shape[0], ref.shape[1], DTYPES[ref.dtype], prepare_options(p), prm,
         ctypes.pointer(st), gr, gc, *(o.ctypes.data for o in outs))
     t = _lib._i64()
     ctx.check(ctx.lib.ar_submit(ctx.handle, ctypes.byref(req), ctypes.byref(t)))
-    return Ticket(ctx, t.value, (arrays, masks, st, cols, req), outs, (gr, gc))
+    return Ticket(ctx, t.value, (arrays, masks, st, cols, req, prm), outs, (gr, gc))

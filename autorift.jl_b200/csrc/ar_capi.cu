@@ -394,8 +394,34 @@ static int check_track_args(ar_ctx* c, const ar_pair* p, const ar_points* pts, i
     return AR_OK;
 }
 
+namespace {
+
+int track_host(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up, int measure,
+               const ar::Rotation* rot, float* dx, float* dy, float* corr, uint8_t* searched);
+
+}  // namespace
+
 int ar_track(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up, int measure, float* dx,
              float* dy, float* corr, uint8_t* searched) {
+    return track_host(c, p, pts, up, measure, nullptr, dx, dy, corr, searched);
+}
+
+int ar_track_rotated(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up, int measure,
+                     const double* angles, int count, float* dx, float* dy, float* corr,
+                     uint8_t* searched) {
+    if (count == 0) return track_host(c, p, pts, up, measure, nullptr, dx, dy, corr, searched);
+    ar::Rotation rot;
+    std::string err;
+    if (!ar::make_rotation(angles, count, &rot, &err)) return fail(c, AR_ERR_ARG, err);
+    return track_host(c, p, pts, up, measure, &rot, dx, dy, corr, searched);
+}
+
+}  // extern "C"
+
+namespace {
+
+int track_host(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up, int measure,
+               const ar::Rotation* rot, float* dx, float* dy, float* corr, uint8_t* searched) {
     int rc = check_track_args(c, p, pts, up, measure);
     if (rc != AR_OK) return rc;
     const int64_t n = pts->n;
@@ -436,7 +462,7 @@ int ar_track(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up, int meas
     if (e != cudaSuccess) return cuda_fail(c, e, "ar_track: upload points");
     std::string err;
     e = ar::launch_track(p->dtype, p->ref, p->sec, p->valid, p->nrows, p->ncols, dp, geom, up,
-                         measure, dout, c->scratch, c->num_sms, c->stream, &err);
+                         measure, dout, c->scratch, c->num_sms, c->stream, &err, nullptr, rot);
     if (e != cudaSuccess)
         return err.empty() ? cuda_fail(c, e, "ar_track") : fail(c, AR_ERR_UNSUPPORTED, err);
     // The three float outputs are contiguous on the device, as is `searched`.
@@ -452,6 +478,10 @@ int ar_track(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up, int meas
     if (st) return fail(c, AR_ERR_TIMEOUT, "ar_track: a device wait ran out; results incomplete");
     return AR_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 int ar_track_device(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up, int measure,
                     float* dx, float* dy, float* corr, uint8_t* searched, void* stream) {
@@ -682,6 +712,12 @@ int check_multichip_args(ar_ctx* c, const ar_pair* p, const ar_points* grid, int
     if (prm->measure != AR_ZNCC && prm->measure != AR_NCC) return fail(c, AR_ERR_ARG, "unknown measure");
     if (prm->chip_size_base <= 0 || prm->chip_size_max < prm->chip_size_base || prm->coarse_stride <= 0)
         return fail(c, AR_ERR_ARG, "invalid chip-size levels or coarse stride");
+    if (prm->rotation_count != 0) {
+        ar::Rotation rot;
+        std::string err;
+        if (!ar::make_rotation(prm->rotation_angles, prm->rotation_count, &rot, &err))
+            return fail(c, AR_ERR_ARG, err);
+    }
     return AR_OK;
 }
 
@@ -735,6 +771,8 @@ int multichip_run(ar_ctx* c, const ar_pair* p, const double* gx, const double* g
     P.gtol = prm->agree_tolerance;
     P.gmad = prm->mad_scale;
     P.fill_window = prm->fill_window;
+    if (prm->rotation_count != 0)
+        ar::make_rotation(prm->rotation_angles, prm->rotation_count, &P.rot, nullptr);
     J.arena = arena;
     J.arena_bytes = ab;
     std::string err;

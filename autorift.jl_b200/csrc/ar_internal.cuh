@@ -39,6 +39,22 @@ struct DevPoints {
     int64_t n;
 };
 
+// Rotation search (src/track.jl:313-409): the chip rotations each point of a pass tries, as
+// sin and cos of the angle (deg * (pi / 180), C library sin and cos, computed on the host), and
+// whether the angle is nonzero (an angle of exactly 0 correlates the chip itself). count 0 is
+// NoRotationSearch. Passed to the correlation kernel by value.
+constexpr int kMaxAngles = AR_MAX_ROTATION_ANGLES;
+struct Rotation {
+    int count = 0;
+    double sn[kMaxAngles];
+    double cs[kMaxAngles];
+    unsigned char turn[kMaxAngles];
+};
+
+// Checks an angle list (finite, distinct, 1..kMaxAngles of them) and fills `out`; false with a
+// message otherwise.
+bool make_rotation(const double* deg, int count, Rotation* out, std::string* err);
+
 struct DevOutputs {
     float* dx;
     float* dy;
@@ -91,7 +107,8 @@ cudaError_t launch_track(int dtype, const void* ref, const void* sec, const uint
                          int64_t nrows, int64_t ncols, const DevPoints& pts,
                          const PassGeometry& geom, int up, int measure, const DevOutputs& out,
                          TrackScratch& scratch, int num_sms, cudaStream_t stream,
-                         std::string* err, float* surf_out = nullptr);
+                         std::string* err, float* surf_out = nullptr,
+                         const Rotation* rot = nullptr);
 
 // Device-side pass geometry for a device point set (one small synchronising read).
 cudaError_t pass_geometry_device(const DevPoints& pts, int64_t nrows, int64_t ncols,
@@ -132,6 +149,7 @@ struct MultichipParams {
     int64_t gwindow, giterations;
     double gfrac, gtol, gmad;
     int64_t fill_window;
+    Rotation rot;  // the rotation search of every track pass (count 0: none)
 };
 
 // One multichip run: a prepared pair, a gr x gc point grid (device, column-major), outputs

@@ -559,7 +559,8 @@ cudaError_t run_multichip(const MultichipJob& J, TrackScratch& scratch, int num_
         err = pass_geometry_device(cp, J.nrows, J.ncols, scratch, s, &g);
         if (err == cudaSuccess)
             err = launch_track(J.dtype, J.ref, J.sec, J.valid, J.nrows, J.ncols, cp, g, up,
-                               J.P.measure, co, scratch, num_sms, s, errmsg);
+                               J.P.measure, co, scratch, num_sms, s, errmsg, nullptr,
+                               J.P.rot.count > 0 ? &J.P.rot : nullptr);
         if (err != cudaSuccess) return;
         k_scatter_outputs<<<blocks(ns), kT, 0, s>>>(kidx, ns, co, O);
         ++L;

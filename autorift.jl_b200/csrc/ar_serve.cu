@@ -37,6 +37,7 @@ constexpr int kPending = -1;
 struct Job {
     int64_t ticket = 0;
     ar_request req{};
+    std::vector<double> angles;  // the request's rotation angles, copied at submission
     size_t footprint = 0;
     int status = kPending;
     std::string err;
@@ -196,8 +197,18 @@ int serve_submit(ServeEngine* E, const ar_request* r, int64_t* ticket, std::stri
         *err = "grid extents do not match the point count";
         return AR_ERR_SIZE;
     }
+    if (r->params.rotation_count != 0) {
+        Rotation rot;
+        if (!make_rotation(r->params.rotation_angles, r->params.rotation_count, &rot, err))
+            return AR_ERR_ARG;
+    }
     auto j = std::make_shared<Job>();
     j->req = *r;
+    if (r->params.rotation_count != 0) {
+        j->angles.assign(r->params.rotation_angles,
+                         r->params.rotation_angles + r->params.rotation_count);
+        j->req.params.rotation_angles = j->angles.data();
+    }
     j->footprint = footprint(*r);
     j->t_submit = Clock::now();
     {

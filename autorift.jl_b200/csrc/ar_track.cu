@@ -30,6 +30,7 @@
 #include <cstdint>
 #include <mutex>
 #include <string>
+#include <type_traits>
 
 #include "ar_internal.cuh"
 #include "ar_tc.cuh"
@@ -194,7 +195,10 @@ struct CorrArgs {
     float* sub_patch;
     float* surf_out;  // optional: each point's surface, NRS x NCM floats per point
     unsigned long long* flops;  // optional: algorithmic FLOPs of the surfaces computed
+    unsigned off_surf2;  // rotation search: the best surface so far (NRS x NCM floats)
+    Rotation rot;        // rotation search angles (k_corr<T, true> only)
 };
+static_assert(sizeof(CorrArgs) <= 4096, "k_corr's arguments must fit the 4 KB parameter space");
 
 template <typename T>
 __device__ __forceinline__ double pixel(const T* img, int64_t nrows, int64_t ncols, int64_t r,
@@ -214,16 +218,49 @@ __device__ __forceinline__ double ph_of<double>(float w) {
     return static_cast<double>(w);
 }
 
+// _rotate_chip (src/track.jl:377-409) at 0-based chip element (a, b) of a ch x cw chip whose
+// first element is image element (chip_r, chip_c): the source point by the inverse rotation
+// about the chip centre ((ch + 1) / 2, (cw + 1) / 2, 1-based), FP64 bilinear from its four
+// neighbours, zero when one of them falls outside the chip, rounded to Float32. Each
+// operation is rounded separately, in the reference's order (no contraction).
 template <typename T>
+__device__ __forceinline__ float rotated_sample(const T* sec, int64_t nrows, int64_t ncols,
+                                                int64_t chip_r, int64_t chip_c, int ch, int cw,
+                                                int a, int b, double sn, double cs) {
+    const double yc = static_cast<double>(ch + 1) * 0.5, xc = static_cast<double>(cw + 1) * 0.5;
+    const double dy = static_cast<double>(a + 1) - yc, dx = static_cast<double>(b + 1) - xc;
+    const double sy = __dadd_rn(__dadd_rn(yc, __dmul_rn(cs, dy)), __dmul_rn(sn, dx));
+    const double sx = __dadd_rn(__dsub_rn(xc, __dmul_rn(sn, dy)), __dmul_rn(cs, dx));
+    const double fi = floor(sy), fj = floor(sx);
+    if (!(fi >= 1.0 && fj >= 1.0 && fi + 1.0 <= static_cast<double>(ch) &&
+          fj + 1.0 <= static_cast<double>(cw)))
+        return 0.0f;
+    const int i0 = static_cast<int>(fi), j0 = static_cast<int>(fj);  // 1-based
+    const double fy = __dsub_rn(sy, fi), fx = __dsub_rn(sx, fj);
+    const double v00 = pixel(sec, nrows, ncols, chip_r + i0 - 1, chip_c + j0 - 1);
+    const double v10 = pixel(sec, nrows, ncols, chip_r + i0, chip_c + j0 - 1);
+    const double v01 = pixel(sec, nrows, ncols, chip_r + i0 - 1, chip_c + j0);
+    const double v11 = pixel(sec, nrows, ncols, chip_r + i0, chip_c + j0);
+    const double gx = __dsub_rn(1.0, fx), gy = __dsub_rn(1.0, fy);
+    const double top = __dadd_rn(__dmul_rn(gx, v00), __dmul_rn(fx, v01));
+    const double bot = __dadd_rn(__dmul_rn(gx, v10), __dmul_rn(fx, v11));
+    return __double2float_rn(__dadd_rn(__dmul_rn(gy, top), __dmul_rn(fy, bot)));
+}
+
+// ROT: the rotation search. Its chips are Float32 (turned chips are resampled), so the
+// numerator takes the FP32/FP64 branch and the box sums are FP64 for every element type.
+template <typename T, bool ROT>
 __global__ void __launch_bounds__(kCorrThreads, 2) k_corr(const CorrArgs A) {
     typedef Traits<T> Tr;
-    typedef typename Tr::ph_t PH;
+    constexpr bool RAW = Tr::raw && !ROT;
+    typedef typename std::conditional<ROT, double, typename Tr::ph_t>::type PH;
     extern __shared__ __align__(16) unsigned char smem[];
     float* s_chip = reinterpret_cast<float*>(smem);
     float* s_win = reinterpret_cast<float*>(smem + A.off_win);
     PH* s_ph1 = reinterpret_cast<PH*>(smem + A.off_ph1);
     PH* s_ph2 = reinterpret_cast<PH*>(smem + A.off_ph2);
     float* s_surf = reinterpret_cast<float*>(smem + A.off_surf);
+    float* s_surf2 = reinterpret_cast<float*>(smem + A.off_surf2);
     double* s_red = reinterpret_cast<double*>(smem + A.off_red);
     __shared__ int s_slot;
 
@@ -272,230 +309,276 @@ __global__ void __launch_bounds__(kCorrThreads, 2) k_corr(const CorrArgs A) {
         if (!__syncthreads_or(any)) continue;
         if (tid == 0) A.out.searched[k] = 1;
 
-        // prepare_chip! (src/correlate.jl:423-453): FP64 mean, then the mean-removed Float32
-        // copy, its FP64 sum of squares, and the FP64 sum of the rounded copy.
-        double st[1] = {0.0};
-        for (int e = tid; e < ch * cw; e += bd)
-            st[0] = __dadd_rn(st[0], pixel(sec, A.nrows, A.ncols, chip_r + e % ch, chip_c + e / ch));
-        block_sum_f64<1>(st, s_red);
-        const double nn = static_cast<double>(ch * cw);
-        const double mean = __ddiv_rn(st[0], nn);
-        const int chp = (ch + kUA - 1) & ~(kUA - 1);
-        double acc2[2] = {0.0, 0.0};
-        for (int e = tid; e < chp * cw; e += bd) {
-            const int a = e % chp, b = e / chp;
-            float staged = 0.0f;
-            if (a < ch) {
-                const double v = pixel(sec, A.nrows, A.ncols, chip_r + a, chip_c + b);
-                const double d = __dsub_rn(v, mean);
-                const float df = __double2float_rn(d);
-                acc2[0] = __dadd_rn(acc2[0], __dmul_rn(d, d));
-                acc2[1] = __dadd_rn(acc2[1], static_cast<double>(df));
-                staged = Tr::raw ? static_cast<float>(v) : df;
+        // One correlation, or with the rotation search one per angle with the best surface kept
+        // (_correlate_rotations!, src/track.jl:313-350): an angle whose turned chip is
+        // degenerate is skipped, and a surface replaces the best so far only if its maximum is
+        // strictly larger. s_cur receives each surface; s_best is the best one so far.
+        const int nang = ROT ? A.rot.count : 1;
+        float* s_cur = s_surf;
+        float* s_best = s_surf2;
+        float bestpk = -INFINITY;
+        unsigned long long best = 0ull;
+        bool found = false;
+        for (int ia = 0; ia < nang; ++ia) {
+            const bool turn = ROT && A.rot.turn[ia];
+            const double rsn = ROT ? A.rot.sn[ia] : 0.0, rcs = ROT ? A.rot.cs[ia] : 1.0;
+
+            // prepare_chip! (src/correlate.jl:423-453): FP64 mean, then the mean-removed
+            // Float32 copy, its FP64 sum of squares, and the FP64 sum of the rounded copy. With
+            // the rotation search the chip (turned, or itself at angle 0) is first staged as
+            // Float32 values.
+            double st[1] = {0.0};
+            for (int e = tid; e < ch * cw; e += bd) {
+                const int a = e % ch, b = e / ch;
+                double v;
+                if (turn) {
+                    v = static_cast<double>(rotated_sample(sec, A.nrows, A.ncols, chip_r,
+                                                           chip_c, ch, cw, a, b, rsn, rcs));
+                } else {
+                    v = pixel(sec, A.nrows, A.ncols, chip_r + a, chip_c + b);
+                }
+                if (ROT) s_chip[b * A.CHP + a] = static_cast<float>(v);
+                st[0] = __dadd_rn(st[0], v);
             }
-            if (A.BC >= cw) s_chip[b * A.CHP + a] = staged;
-        }
-        block_sum_f64<2>(acc2, s_red);
-        const double sq = acc2[0], sumd = acc2[1];
-        if (!(sq > __dmul_rn(__dmul_rn(DBL_EPSILON, static_cast<double>(ch)),
-                             static_cast<double>(cw))))
-            continue;  // degenerate chip: searched, no measurement (src/track.jl:286)
-        const double cnorm = __dsqrt_rn(sq);
-        // Centring constant for the window of non-raw element types.
-        double cshift = 0.0;
-        if (!Tr::raw) cshift = Tr::integer ? rint(mean) : static_cast<double>(__double2float_rn(mean));
+            block_sum_f64<1>(st, s_red);
+            const double nn = static_cast<double>(ch * cw);
+            const double mean = __ddiv_rn(st[0], nn);
+            const int chp = (ch + kUA - 1) & ~(kUA - 1);
+            double acc2[2] = {0.0, 0.0};
+            for (int e = tid; e < chp * cw; e += bd) {
+                const int a = e % chp, b = e / chp;
+                float staged = 0.0f;
+                if (a < ch) {
+                    const double v = ROT ? static_cast<double>(s_chip[b * A.CHP + a])
+                                         : pixel(sec, A.nrows, A.ncols, chip_r + a, chip_c + b);
+                    const double d = __dsub_rn(v, mean);
+                    const float df = __double2float_rn(d);
+                    acc2[0] = __dadd_rn(acc2[0], __dmul_rn(d, d));
+                    acc2[1] = __dadd_rn(acc2[1], static_cast<double>(df));
+                    staged = RAW ? static_cast<float>(v) : df;
+                }
+                if (A.BC >= cw) s_chip[b * A.CHP + a] = staged;
+            }
+            block_sum_f64<2>(acc2, s_red);
+            const double sq = acc2[0], sumd = acc2[1];
+            if (!(sq > __dmul_rn(__dmul_rn(DBL_EPSILON, static_cast<double>(ch)),
+                                 static_cast<double>(cw))))
+                continue;  // degenerate chip: no surface at this angle (src/track.jl:286, 326)
+            const double cnorm = __dsqrt_rn(sq);
+            // Centring constant for the window of non-raw element types.
+            double cshift = 0.0;
+            if (!RAW) cshift = Tr::integer ? rint(mean) : static_cast<double>(__double2float_rn(mean));
 
-        const int F = Tr::raw ? max(1, 16777216 / (chp * 65025)) : 2;
+            const int F = RAW ? max(1, 16777216 / (chp * 65025)) : 2;
+            for (int ti = 0; ti < nr; ti += A.TI) {
+                const int trows = min(A.TI, nr - ti);
+                const int trows_p = (trows + kMI - 1) / kMI * kMI;
+                const int srows = trows_p + chp;  // staged window rows (<= WS)
+                const int wrows = trows + ch - 1; // rows the box sums use
+                for (int tj = 0; tj < nc; tj += A.TJ) {
+                    const int tcols = min(A.TJ, nc - tj);
+                    // Numerator item = (row group, column), kMI surface rows per thread; its
+                    // partial sums run across the chip-column chunks.
+                    const int ig = tid / A.TJ, jl = tid % A.TJ;
+                    const bool item = ig * kMI < trows && jl < tcols;
+                    const int il = ig * kMI;
+                    float acc[kMI];
+                    double acc64[kMI];
+    #pragma unroll
+                    for (int m = 0; m < kMI; ++m) { acc[m] = 0.0f; acc64[m] = 0.0; }
+                    int fc = 0;
+                    for (int b0 = 0; b0 < cw; b0 += A.BC) {
+                        const int bc = min(A.BC, cw - b0);
+                        const int xcols = tcols + bc - 1;
+                        __syncthreads();
+                        if (!ROT && A.BC < cw) {
+                            // This chunk of chip columns, staged as in the unchunked case.
+                            for (int e = tid; e < chp * bc; e += bd) {
+                                const int a = e % chp, bl = e / chp;
+                                float staged = 0.0f;
+                                if (a < ch) {
+                                    const double v = pixel(sec, A.nrows, A.ncols, chip_r + a, chip_c + b0 + bl);
+                                    staged = RAW ? static_cast<float>(v)
+                                                     : __double2float_rn(__dsub_rn(v, mean));
+                                }
+                                s_chip[bl * A.CHP + a] = staged;
+                            }
+                        }
+                        // Stage the window block column-major, zero outside the image and below
+                        // the window's last row.
+                        for (int e = tid; e < xcols * srows; e += bd) {
+                            const int r = e % srows, x = e / srows;
+                            float v = 0.0f;
+                            if (r < wrows) {
+                                const double pv =
+                                    pixel(ref, A.nrows, A.ncols, win_r + ti + r, win_c + tj + b0 + x);
+                                v = RAW ? static_cast<float>(pv)
+                                            : __double2float_rn(__dsub_rn(pv, cshift));
+                            }
+                            s_win[x * A.WS + r] = v;
+                        }
+                        __syncthreads();
+                        // Per-window sums of W and W^2 over the chunk's columns for every row the
+                        // tile uses (integral_both!, src/integral.jl:141-170), added at slot r + 1.
+                        // They sum the image values themselves: a non-raw staged window is shifted
+                        // by cshift for the numerator's FP32 products, and adding the shift back
+                        // restores the image value (exactly for zero padding, within one Float32
+                        // rounding otherwise). A window without variance -- all zero padding, or
+                        // flat integer data -- then sums to exactly zero variance, as the
+                        // reference's FP64 integral images do; expanding shifted sums instead
+                        // leaves a rounding residue that the numerator's FP32 error turns into
+                        // arbitrary correlation values.
+                        auto wv = [&](int idx) -> PH {
+                            if constexpr (RAW) {
+                                return ph_of<PH>(s_win[idx]);
+                            } else {
+                                return static_cast<PH>(
+                                    __dadd_rn(static_cast<double>(s_win[idx]), cshift));
+                            }
+                        };
+                        const int nseg = (tcols + 15) >> 4;
+                        for (int task = tid; task < wrows * nseg; task += bd) {
+                            const int r = task % wrows, seg = task / wrows;
+                            const int j0s = seg << 4, j1s = min(j0s + 16, tcols);
+                            PH h1 = 0, h2 = 0;
+                            for (int b = 0; b < bc; ++b) {
+                                const PH w = wv((j0s + b) * A.WS + r);
+                                h1 = h1 + w;
+                                h2 = h2 + w * w;
+                            }
+                            for (int jj = j0s; jj < j1s; ++jj) {
+                                if (jj > j0s) {
+                                    const PH wo = wv((jj - 1) * A.WS + r);
+                                    const PH wn = wv((jj - 1 + bc) * A.WS + r);
+                                    h1 = h1 + wn - wo;
+                                    h2 = h2 + wn * wn - wo * wo;
+                                }
+                                PH* p1 = &s_ph1[jj * A.PHS + r + 1];
+                                PH* p2 = &s_ph2[jj * A.PHS + r + 1];
+                                *p1 = b0 == 0 ? h1 : *p1 + h1;
+                                *p2 = b0 == 0 ? h2 : *p2 + h2;
+                            }
+                        }
+                        // The chunk's share of the numerator.
+                        if (item) {
+                            const float* wbase = s_win + jl * A.WS + il;
+                            for (int b = 0; b < bc; ++b) {
+                                const float* wc = wbase + b * A.WS;
+                                const float* cc = s_chip + b * A.CHP;
+                                for (int a0 = 0; a0 < chp; a0 += kUA) {
+                                    float c[kUA];
+                                    float w[kUA + kMI];
+    #pragma unroll
+                                    for (int q = 0; q < kUA / 4; ++q) {
+                                        const float4 v = *reinterpret_cast<const float4*>(cc + a0 + 4 * q);
+                                        c[4 * q] = v.x; c[4 * q + 1] = v.y; c[4 * q + 2] = v.z; c[4 * q + 3] = v.w;
+                                    }
+    #pragma unroll
+                                    for (int q = 0; q < (kUA + kMI) / 2; ++q) {
+                                        const float2 v = *reinterpret_cast<const float2*>(wc + a0 + 2 * q);
+                                        w[2 * q] = v.x; w[2 * q + 1] = v.y;
+                                    }
+    #pragma unroll
+                                    for (int a = 0; a < kUA; ++a)
+    #pragma unroll
+                                        for (int m = 0; m < kMI; ++m) acc[m] = fmaf(c[a], w[m + a], acc[m]);
+                                }
+                                if (++fc == F) {
+    #pragma unroll
+                                    for (int m = 0; m < kMI; ++m) {
+                                        acc64[m] = __dadd_rn(acc64[m], static_cast<double>(acc[m]));
+                                        acc[m] = 0.0f;
+                                    }
+                                    fc = 0;
+                                }
+                            }
+                        }
+                    }
+                    __syncthreads();
+                    // Exclusive prefix down each column by warp scans: ph[jl][q] = sum_{r<q} H[r].
+                    for (int jw = warp; jw < tcols; jw += nwarps) {
+                        PH c1 = 0, c2 = 0;
+                        for (int q = 1; q <= wrows; q += 32) {
+                            const int idx = q + lane;
+                            PH v1 = idx <= wrows ? s_ph1[jw * A.PHS + idx] : PH(0);
+                            PH v2 = idx <= wrows ? s_ph2[jw * A.PHS + idx] : PH(0);
+                            v1 = warp_inclusive_scan(v1) + c1;
+                            v2 = warp_inclusive_scan(v2) + c2;
+                            if (idx <= wrows) {
+                                s_ph1[jw * A.PHS + idx] = v1;
+                                s_ph2[jw * A.PHS + idx] = v2;
+                            }
+                            c1 = __shfl_sync(kFull, v1, 31);
+                            c2 = __shfl_sync(kFull, v2, 31);
+                        }
+                        if (lane == 0) {
+                            s_ph1[jw * A.PHS] = PH(0);
+                            s_ph2[jw * A.PHS] = PH(0);
+                        }
+                    }
+                    __syncthreads();
 
-        for (int ti = 0; ti < nr; ti += A.TI) {
-            const int trows = min(A.TI, nr - ti);
-            const int trows_p = (trows + kMI - 1) / kMI * kMI;
-            const int srows = trows_p + chp;  // staged window rows (<= WS)
-            const int wrows = trows + ch - 1; // rows the box sums use
-            for (int tj = 0; tj < nc; tj += A.TJ) {
-                const int tcols = min(A.TJ, nc - tj);
-                // Numerator item = (row group, column), kMI surface rows per thread; its
-                // partial sums run across the chip-column chunks.
-                const int ig = tid / A.TJ, jl = tid % A.TJ;
-                const bool item = ig * kMI < trows && jl < tcols;
-                const int il = ig * kMI;
-                float acc[kMI];
-                double acc64[kMI];
-#pragma unroll
-                for (int m = 0; m < kMI; ++m) { acc[m] = 0.0f; acc64[m] = 0.0; }
-                int fc = 0;
-                for (int b0 = 0; b0 < cw; b0 += A.BC) {
-                    const int bc = min(A.BC, cw - b0);
-                    const int xcols = tcols + bc - 1;
-                    __syncthreads();
-                    if (A.BC < cw) {
-                        // This chunk of chip columns, staged as in the unchunked case.
-                        for (int e = tid; e < chp * bc; e += bd) {
-                            const int a = e % chp, bl = e / chp;
-                            float staged = 0.0f;
-                            if (a < ch) {
-                                const double v = pixel(sec, A.nrows, A.ncols, chip_r + a, chip_c + b0 + bl);
-                                staged = Tr::raw ? static_cast<float>(v)
-                                                 : __double2float_rn(__dsub_rn(v, mean));
-                            }
-                            s_chip[bl * A.CHP + a] = staged;
-                        }
-                    }
-                    // Stage the window block column-major, zero outside the image and below
-                    // the window's last row.
-                    for (int e = tid; e < xcols * srows; e += bd) {
-                        const int r = e % srows, x = e / srows;
-                        float v = 0.0f;
-                        if (r < wrows) {
-                            const double pv =
-                                pixel(ref, A.nrows, A.ncols, win_r + ti + r, win_c + tj + b0 + x);
-                            v = Tr::raw ? static_cast<float>(pv)
-                                        : __double2float_rn(__dsub_rn(pv, cshift));
-                        }
-                        s_win[x * A.WS + r] = v;
-                    }
-                    __syncthreads();
-                    // Per-window sums of W and W^2 over the chunk's columns for every row the
-                    // tile uses (integral_both!, src/integral.jl:141-170), added at slot r + 1.
-                    const int nseg = (tcols + 15) >> 4;
-                    for (int task = tid; task < wrows * nseg; task += bd) {
-                        const int r = task % wrows, seg = task / wrows;
-                        const int j0s = seg << 4, j1s = min(j0s + 16, tcols);
-                        PH h1 = 0, h2 = 0;
-                        for (int b = 0; b < bc; ++b) {
-                            const PH w = ph_of<PH>(s_win[(j0s + b) * A.WS + r]);
-                            h1 = h1 + w;
-                            h2 = h2 + w * w;
-                        }
-                        for (int jj = j0s; jj < j1s; ++jj) {
-                            if (jj > j0s) {
-                                const PH wo = ph_of<PH>(s_win[(jj - 1) * A.WS + r]);
-                                const PH wn = ph_of<PH>(s_win[(jj - 1 + bc) * A.WS + r]);
-                                h1 = h1 + wn - wo;
-                                h2 = h2 + wn * wn - wo * wo;
-                            }
-                            PH* p1 = &s_ph1[jj * A.PHS + r + 1];
-                            PH* p2 = &s_ph2[jj * A.PHS + r + 1];
-                            *p1 = b0 == 0 ? h1 : *p1 + h1;
-                            *p2 = b0 == 0 ? h2 : *p2 + h2;
-                        }
-                    }
-                    // The chunk's share of the numerator.
                     if (item) {
-                        const float* wbase = s_win + jl * A.WS + il;
-                        for (int b = 0; b < bc; ++b) {
-                            const float* wc = wbase + b * A.WS;
-                            const float* cc = s_chip + b * A.CHP;
-                            for (int a0 = 0; a0 < chp; a0 += kUA) {
-                                float c[kUA];
-                                float w[kUA + kMI];
-#pragma unroll
-                                for (int q = 0; q < kUA / 4; ++q) {
-                                    const float4 v = *reinterpret_cast<const float4*>(cc + a0 + 4 * q);
-                                    c[4 * q] = v.x; c[4 * q + 1] = v.y; c[4 * q + 2] = v.z; c[4 * q + 3] = v.w;
-                                }
-#pragma unroll
-                                for (int q = 0; q < (kUA + kMI) / 2; ++q) {
-                                    const float2 v = *reinterpret_cast<const float2*>(wc + a0 + 2 * q);
-                                    w[2 * q] = v.x; w[2 * q + 1] = v.y;
-                                }
-#pragma unroll
-                                for (int a = 0; a < kUA; ++a)
-#pragma unroll
-                                    for (int m = 0; m < kMI; ++m) acc[m] = fmaf(c[a], w[m + a], acc[m]);
-                            }
-                            if (++fc == F) {
-#pragma unroll
-                                for (int m = 0; m < kMI; ++m) {
-                                    acc64[m] = __dadd_rn(acc64[m], static_cast<double>(acc[m]));
-                                    acc[m] = 0.0f;
-                                }
-                                fc = 0;
-                            }
-                        }
-                    }
-                }
-                __syncthreads();
-                // Exclusive prefix down each column by warp scans: ph[jl][q] = sum_{r<q} H[r].
-                for (int jw = warp; jw < tcols; jw += nwarps) {
-                    PH c1 = 0, c2 = 0;
-                    for (int q = 1; q <= wrows; q += 32) {
-                        const int idx = q + lane;
-                        PH v1 = idx <= wrows ? s_ph1[jw * A.PHS + idx] : PH(0);
-                        PH v2 = idx <= wrows ? s_ph2[jw * A.PHS + idx] : PH(0);
-                        v1 = warp_inclusive_scan(v1) + c1;
-                        v2 = warp_inclusive_scan(v2) + c2;
-                        if (idx <= wrows) {
-                            s_ph1[jw * A.PHS + idx] = v1;
-                            s_ph2[jw * A.PHS + idx] = v2;
-                        }
-                        c1 = __shfl_sync(kFull, v1, 31);
-                        c2 = __shfl_sync(kFull, v2, 31);
-                    }
-                    if (lane == 0) {
-                        s_ph1[jw * A.PHS] = PH(0);
-                        s_ph2[jw * A.PHS] = PH(0);
-                    }
-                }
-                __syncthreads();
+    #pragma unroll
+                        for (int m = 0; m < kMI; ++m)
+                            acc64[m] = __dadd_rn(acc64[m], static_cast<double>(acc[m]));
 
-                if (item) {
-#pragma unroll
-                    for (int m = 0; m < kMI; ++m)
-                        acc64[m] = __dadd_rn(acc64[m], static_cast<double>(acc[m]));
-
-                    // Normalisation (src/correlate.jl:591-600, 624-628).
-#pragma unroll
-                    for (int m = 0; m < kMI; ++m) {
-                        const int ir = il + m;
-                        if (ir < trows) {
-                            const PH p1 = s_ph1[jl * A.PHS + ir + ch] - s_ph1[jl * A.PHS + ir];
-                            const PH p2 = s_ph2[jl * A.PHS + ir + ch] - s_ph2[jl * A.PHS + ir];
-                            double s1, s2, num;
-                            if (Tr::raw) {
-                                s1 = static_cast<double>(p1);
-                                s2 = static_cast<double>(p2);
-                                num = __dsub_rn(acc64[m], __dmul_rn(mean, s1));
-                            } else {
-                                const double s1c = static_cast<double>(p1);
-                                const double s2c = static_cast<double>(p2);
-                                s1 = __dadd_rn(s1c, __dmul_rn(nn, cshift));
-                                s2 = __dadd_rn(__dadd_rn(s2c, __dmul_rn(__dmul_rn(2.0, cshift), s1c)),
-                                               __dmul_rn(__dmul_rn(nn, cshift), cshift));
-                                num = __dadd_rn(acc64[m], __dmul_rn(cshift, sumd));
+                        // Normalisation (src/correlate.jl:591-600, 624-628).
+    #pragma unroll
+                        for (int m = 0; m < kMI; ++m) {
+                            const int ir = il + m;
+                            if (ir < trows) {
+                                const PH p1 = s_ph1[jl * A.PHS + ir + ch] - s_ph1[jl * A.PHS + ir];
+                                const PH p2 = s_ph2[jl * A.PHS + ir + ch] - s_ph2[jl * A.PHS + ir];
+                                const double s1 = static_cast<double>(p1);
+                                const double s2 = static_cast<double>(p2);
+                                const double num =
+                                    RAW ? __dsub_rn(acc64[m], __dmul_rn(mean, s1))
+                                        : __dadd_rn(acc64[m], __dmul_rn(cshift, sumd));
+                                double den;
+                                if (A.measure == AR_NCC) {
+                                    den = __dmul_rn(cnorm, __dsqrt_rn(s2 > 0.0 ? s2 : 0.0));
+                                } else {
+                                    double wvar = __dsub_rn(s2, __ddiv_rn(__dmul_rn(s1, s1), nn));
+                                    if (!(wvar > 0.0)) wvar = 0.0;
+                                    den = __dmul_rn(cnorm, __dsqrt_rn(wvar));
+                                }
+                                const float sv = den > 0.0 ? __double2float_rn(__ddiv_rn(num, den)) : 0.0f;
+                                s_cur[(ti + ir) + (tj + jl) * A.NRS] = sv;
                             }
-                            double den;
-                            if (A.measure == AR_NCC) {
-                                den = __dmul_rn(cnorm, __dsqrt_rn(s2 > 0.0 ? s2 : 0.0));
-                            } else {
-                                double wvar = __dsub_rn(s2, __ddiv_rn(__dmul_rn(s1, s1), nn));
-                                if (!(wvar > 0.0)) wvar = 0.0;
-                                den = __dmul_rn(cnorm, __dsqrt_rn(wvar));
-                            }
-                            const float sv = den > 0.0 ? __double2float_rn(__ddiv_rn(num, den)) : 0.0f;
-                            s_surf[(ti + ir) + (tj + jl) * A.NRS] = sv;
                         }
                     }
                 }
             }
+            __syncthreads();
+            if (A.flops && tid == 0)
+                atomicAdd(A.flops, 2ull * static_cast<unsigned long long>(ch) * cw * nr * nc);
+
+            // Integer peak (src/peak.jl:32-61), and the angle's maximum (src/track.jl:327-328).
+            unsigned long long key = 0ull;
+            for (int e = tid; e < nr * nc; e += bd) {
+                const int i = e % nr, j = e / nr;
+                const unsigned long long kk =
+                    argmax_key(s_cur[i + j * A.NRS], static_cast<unsigned>(i * nc + j));
+                key = kk > key ? kk : key;
+            }
+            key = block_max_u64(key, reinterpret_cast<unsigned long long*>(s_red));
+            const float pk = key == 0ull ? NAN : key_value(key);
+            if (!ROT || pk > bestpk) {
+                bestpk = pk;
+                best = key;
+                float* t = s_best;
+                s_best = s_cur;
+                s_cur = t;
+                found = true;
+            }
         }
-        __syncthreads();
-        if (A.flops && tid == 0)
-            atomicAdd(A.flops, 2ull * static_cast<unsigned long long>(ch) * cw * nr * nc);
+        if (!found) continue;  // every angle degenerate: searched, no measurement
         if (A.surf_out) {
             float* so = A.surf_out + k * static_cast<int64_t>(A.NRS) * A.NCM;
-            for (int e = tid; e < nr * nc; e += bd) so[e] = s_surf[(e % nr) + (e / nr) * A.NRS];
+            for (int e = tid; e < nr * nc; e += bd) so[e] = s_best[(e % nr) + (e / nr) * A.NRS];
         }
 
-        // Integer peak (src/peak.jl:32-61).
-        unsigned long long best = 0ull;
-        for (int e = tid; e < nr * nc; e += bd) {
-            const int i = e % nr, j = e / nr;
-            const unsigned long long kk =
-                argmax_key(s_surf[i + j * A.NRS], static_cast<unsigned>(i * nc + j));
-            best = kk > best ? kk : best;
-        }
-        best = block_max_u64(best, reinterpret_cast<unsigned long long*>(s_red));
         unsigned rm = 0;
         float pv = 0.0f;
         int pi = 0, pj = 0;
@@ -506,7 +589,7 @@ __global__ void __launch_bounds__(kCorrThreads, 2) k_corr(const CorrArgs A) {
         if (A.up == 1 || nr < 5 || nc < 5) {
             // peak_offset (src/peak.jl:102-106) and the output write (src/track.jl:293-295).
             if (tid == 0) {
-                const float v = s_surf[pi + pj * A.NRS];
+                const float v = s_best[pi + pj * A.NRS];
                 A.out.dx[k] = __double2float_rn(
                     __dadd_rn(static_cast<double>(pj - static_cast<int>(prx)), A.pts.dx0[k]));
                 A.out.dy[k] = __double2float_rn(
@@ -523,7 +606,7 @@ __global__ void __launch_bounds__(kCorrThreads, 2) k_corr(const CorrArgs A) {
             if (tid < 25) {
                 const int a = tid % 5, b = tid / 5;
                 A.sub_patch[static_cast<int64_t>(slot) * 25 + tid] =
-                    s_surf[(pi0 + a) + (pj0 + b) * A.NRS];
+                    s_best[(pi0 + a) + (pj0 + b) * A.NRS];
             }
             if (tid == 0) {
                 A.sub_point[slot] = k;
@@ -2586,11 +2669,14 @@ inline int window_stride(int rows) {
 
 struct CorrPlan {
     int TI, TJ, CHP, CWM, WS, PHS, NRS, NCM, BC;
-    unsigned off_win, off_ph1, off_ph2, off_surf, off_red;
+    unsigned off_win, off_ph1, off_ph2, off_surf, off_red, off_surf2;
     size_t smem;
 };
 
-bool plan_corr(const PassGeometry& g, size_t ph_bytes, size_t smem_cap, CorrPlan* P) {
+// `rot`: the rotation search, which stages the whole chip (it is resampled once per angle) and
+// holds a second surface, the best one so far.
+bool plan_corr(const PassGeometry& g, size_t ph_bytes, size_t smem_cap, CorrPlan* P,
+               bool rot = false) {
     const int ch = static_cast<int>(g.max_ch), cw = static_cast<int>(g.max_cw);
     const int nr = static_cast<int>(g.max_nr), nc = static_cast<int>(g.max_nc);
     P->CHP = round_up(std::max(ch, 1), kUA);
@@ -2603,7 +2689,7 @@ bool plan_corr(const PassGeometry& g, size_t ph_bytes, size_t smem_cap, CorrPlan
     // block; shrink until the shared-memory budget is met.
     const int bcs[] = {P->CWM, 64, 32, 16, 8, 4, 2};
     for (int bc : bcs) {
-        if (bc > P->CWM || (bc < P->CWM && (bc & 1))) continue;
+        if (bc > P->CWM || (bc < P->CWM && (bc & 1)) || (rot && bc < P->CWM)) continue;
         for (int TJ = std::min(nc, kCorrThreads); TJ >= 1; TJ = (TJ > 8 ? TJ - 8 : TJ - 1)) {
             const int groups = std::max(1, kCorrThreads / TJ);
             for (int TI = std::min(round_up(nr, kMI), groups * kMI); TI >= kMI; TI -= kMI) {
@@ -2625,6 +2711,12 @@ bool plan_corr(const PassGeometry& g, size_t ph_bytes, size_t smem_cap, CorrPlan
                 off = (off + 15) & ~size_t(15);
                 const unsigned off_red = static_cast<unsigned>(off);
                 off += 3 * 32 * 8;
+                off = (off + 15) & ~size_t(15);
+                unsigned off_surf2 = off_surf;
+                if (rot) {
+                    off_surf2 = static_cast<unsigned>(off);
+                    off += static_cast<size_t>(P->NRS) * P->NCM * 4;
+                }
                 if (off <= smem_cap) {
                     P->TI = TI;
                     P->TJ = TJ;
@@ -2636,6 +2728,7 @@ bool plan_corr(const PassGeometry& g, size_t ph_bytes, size_t smem_cap, CorrPlan
                     P->off_ph2 = off_ph2;
                     P->off_surf = off_surf;
                     P->off_red = off_red;
+                    P->off_surf2 = off_surf2;
                     P->smem = off;
                     return true;
                 }
@@ -2855,12 +2948,14 @@ bool plan_corr_tc(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
 template <typename T>
 cudaError_t launch_corr_t(const CorrArgs& A, const CorrPlan& P, int grid, cudaStream_t stream) {
     if (P.smem > static_cast<size_t>(kDynSmemCap)) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(k_corr<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    auto kern = A.rot.count > 0 ? k_corr<T, true> : k_corr<T, false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          kDynSmemCap);
     if (e != cudaSuccess) return e;
-    k_corr<T><<<grid, kCorrThreads, P.smem, stream>>>(A);
+    kern<<<grid, kCorrThreads, P.smem, stream>>>(A);
     return cudaGetLastError();
 }
+
 
 cudaError_t ensure_scratch(TrackScratch& s, int64_t n, cudaStream_t stream) {
     if (!s.geom) {
@@ -2915,6 +3010,42 @@ cudaError_t ensure_scratch(TrackScratch& s, int64_t n, cudaStream_t stream) {
 }
 
 }  // namespace
+
+bool make_rotation(const double* deg, int count, Rotation* out, std::string* err) {
+    if (count < 1 || count > kMaxAngles) {
+        if (err) *err = "the rotation search needs 1 to " + std::to_string(kMaxAngles) + " angles";
+        return false;
+    }
+    if (!deg) {
+        if (err) *err = "null rotation angles";
+        return false;
+    }
+    for (int i = 0; i < count; ++i) {
+        if (!std::isfinite(deg[i])) {
+            if (err) *err = "rotation angles must be finite";
+            return false;
+        }
+        for (int j = 0; j < i; ++j)
+            if (deg[j] == deg[i]) {
+                if (err) *err = "rotation angles must be distinct";
+                return false;
+            }
+    }
+    out->count = count;
+    for (int i = 0; i < count; ++i) {
+        // deg2rad (deg * (pi / 180)), then the C library's sin and cos.
+        const double r = deg[i] * (M_PI / 180.0);
+        out->sn[i] = std::sin(r);
+        out->cs[i] = std::cos(r);
+        out->turn[i] = deg[i] != 0.0 ? 1 : 0;
+    }
+    for (int i = count; i < kMaxAngles; ++i) {
+        out->sn[i] = 0.0;
+        out->cs[i] = 1.0;
+        out->turn[i] = 0;
+    }
+    return true;
+}
 
 cudaEvent_t KernelTimer::get() {
     if (!pool.empty()) {
@@ -3008,7 +3139,8 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
                               int64_t nrows, int64_t ncols, const DevPoints& pts,
                               const PassGeometry& geom, int up, int measure,
                               const DevOutputs& out, TrackScratch& scratch, int num_sms,
-                              cudaStream_t stream, std::string* err, float* surf_out) {
+                              cudaStream_t stream, std::string* err, float* surf_out,
+                              const Rotation* rot) {
     cudaError_t e = ensure_scratch(scratch, pts.n, stream);
     if (e != cudaSuccess) return e;
     if (pts.n > 0) {
@@ -3021,13 +3153,18 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
     }
     if (geom.searchable == 0 || geom.max_cw == 0 || geom.max_ch == 0) return cudaSuccess;
 
-    const size_t ph_bytes = dtype == AR_U8 ? 4 : 8;
+    const bool rotating = rot && rot->count > 0;
+    const size_t ph_bytes = dtype == AR_U8 && !rotating ? 4 : 8;
     CorrPlan P{};
-    if (!plan_corr(geom, ph_bytes, 220 * 1024, &P)) {
-        if (err) *err = "chip and search geometry too large for shared memory";
+    if (!plan_corr(geom, ph_bytes, 220 * 1024, &P, rotating)) {
+        if (err) *err = rotating ? "chip and search geometry too large for shared memory with "
+                                   "the rotation search"
+                                 : "chip and search geometry too large for shared memory";
         return cudaErrorInvalidValue;
     }
     CorrArgs A{};
+    if (rotating) A.rot = *rot;
+    A.off_surf2 = P.off_surf2;
     A.ref = ref;
     A.sec = sec;
     A.valid = valid;
@@ -3069,7 +3206,8 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         cudaEventRecord(ev0, stream);
     }
     TcPlan TP{};
-    const bool tc_ok = dtype == AR_U8 && scratch.tensor_cores;
+    // The rotation search correlates Float32 (resampled) chips: CUDA cores for every type.
+    const bool tc_ok = dtype == AR_U8 && scratch.tensor_cores && !rotating;
     // k_corr_tc2 wherever its plan fits (one or two CTAs per SM); otherwise k_corr_tc.
     const bool use_tc2 = tc_ok && plan_corr_tc2(geom, 220 * 1024, &TP);
     const bool use_tc = tc_ok && (use_tc2 || plan_corr_tc(geom, 220 * 1024, &TP));
@@ -3201,11 +3339,11 @@ cudaError_t launch_track(int dtype, const void* ref, const void* sec, const uint
                          int64_t nrows, int64_t ncols, const DevPoints& pts,
                          const PassGeometry& geom, int up, int measure, const DevOutputs& out,
                          TrackScratch& scratch, int num_sms, cudaStream_t stream,
-                         std::string* err, float* surf_out) {
+                         std::string* err, float* surf_out, const Rotation* rot) {
     cudaError_t e = scratch_acquire(scratch, stream);
     if (e != cudaSuccess) return e;
     e = launch_track_impl(dtype, ref, sec, valid, nrows, ncols, pts, geom, up, measure, out,
-                          scratch, num_sms, stream, err, surf_out);
+                          scratch, num_sms, stream, err, surf_out, rot);
     const cudaError_t r = cudaEventRecord(scratch.done, stream);
     return e != cudaSuccess ? e : r;
 }

@@ -10,6 +10,7 @@ Julia's ArgumentError).
 from __future__ import annotations
 
 import math
+import numbers
 from dataclasses import dataclass, field
 from typing import Tuple
 
@@ -162,7 +163,73 @@ def relax(m):
 
 @dataclass(frozen=True)
 class NoRotationSearch:
-    pass
+    """Rotation search off (src/types.jl:507-527): one correlation per point."""
+
+
+MAX_ROTATION_ANGLES = 64  # AR_MAX_ROTATION_ANGLES of the C-ABI
+
+
+@dataclass(frozen=True, init=False)
+class RotationSearch:
+    """Per-chip rotation search (src/types.jl:529-557): each point correlates its chip turned by
+    every angle of ``angles(m)`` (``m.angles`` minus ``m.about``, degrees) and keeps the surface
+    with the strictly highest peak (src/track.jl:313-350). ``about`` centres the search on a
+    scene rotation. At least one angle; angles distinct; angles and ``about`` finite; at most
+    ``MAX_ROTATION_ANGLES`` (the device limit -- the reference has none)."""
+
+    angles: Tuple[float, ...]
+    about: float
+
+    def __init__(self, angles=(-3.0, 0.0, 3.0), about=0.0):
+        if isinstance(angles, (str, bytes)) or not hasattr(angles, "__iter__"):
+            raise ValueError(f"`RotationSearch` angles must be a collection of real numbers, "
+                             f"got a {type(angles).__name__}.")
+        try:
+            t = tuple(float(a) for a in angles)
+        except (TypeError, ValueError):
+            raise ValueError("`RotationSearch` angles must be real numbers.") from None
+        if not t:
+            raise ValueError("`RotationSearch` needs at least one angle; use "
+                             "`NoRotationSearch()` to disable.")
+        if len(set(t)) != len(t):
+            raise ValueError(f"`RotationSearch` angles must be distinct, got {t} -- a repeated "
+                             "angle costs a full correlation and can never win.")
+        if isinstance(about, bool) or not isinstance(about, (int, float)):
+            raise TypeError(f"`about` must be a real number, got a {type(about).__name__}.")
+        a = float(about)
+        if not (all(math.isfinite(x) for x in t) and math.isfinite(a)):
+            raise ValueError(f"`RotationSearch` needs finite angles and a finite `about`, got "
+                             f"angles {t} about {a}.")
+        if len(t) > MAX_ROTATION_ANGLES:
+            raise ValueError(f"`RotationSearch` takes at most {MAX_ROTATION_ANGLES} angles on "
+                             f"the device, got {len(t)}.")
+        object.__setattr__(self, "angles", t)
+        object.__setattr__(self, "about", a)
+
+
+def angles(m: RotationSearch) -> Tuple[float, ...]:
+    """The chip rotations a pass tries, in degrees: ``m.angles .- m.about``
+    (src/types.jl:577)."""
+    if not isinstance(m, RotationSearch):
+        raise TypeError("`angles` is defined for RotationSearch only")
+    return tuple(a - m.about for a in m.angles)
+
+
+def _rotation(x):
+    """The rotation keyword (src/params.jl:167-180): None/False off, True the default search,
+    a collection of real angles (tuple, list, range, numpy array), or a rotation method."""
+    if x is None or x is False:
+        return NoRotationSearch()
+    if x is True:
+        return RotationSearch()
+    if isinstance(x, (NoRotationSearch, RotationSearch)):
+        return x
+    if isinstance(x, (tuple, list, range)) or (hasattr(x, "dtype") and hasattr(x, "__iter__")):
+        vals = list(x)
+        if all(isinstance(v, numbers.Real) for v in vals):
+            return RotationSearch(vals)
+    raise ValueError(f"`rotation` must be `None`, a `bool`, a collection of angles, or a "
+                     f"`RotationMethod`, got a {type(x).__name__}.")
 
 
 # ---------------------------------------------------------------------------------------------
@@ -300,8 +367,7 @@ def params(*, similarity="zncc", preprocess="highpass", quantize="uint8", subpix
                              "already carries its own parameters, so "
                              f"{', '.join(f'`{k}`' for k in given)} cannot also apply.")
         out = outliers
-    if rotation not in (None, False):
-        raise ValueError("rotation search is not part of this build (NoRotationSearch only)")
+    rot = _rotation(rotation)
 
     base = _check_chip_size("chip_size", chip_size)
     cmin = base if chip_size_min is _NOKW else _check_chip_size("chip_size_min", chip_size_min)
@@ -347,7 +413,7 @@ def params(*, similarity="zncc", preprocess="highpass", quantize="uint8", subpix
         raise ValueError(f"`fill_window` must be odd so the window has a centre pixel, "
                          f"got {fill_window}")
     return Params(similarity=sim, preprocess=pre, quantize=quant, subpixel=sub, outliers=out,
-                  threaded=bool(threaded), rotation=NoRotationSearch(), chip_size_base=base,
+                  threaded=bool(threaded), rotation=rot, chip_size_base=base,
                   chip_size_min=cmin, chip_size_max=cmax, chip_aspect=float(chip_aspect),
                   grid_spacing=spacing, search_radius_x=rx, search_radius_y=ry,
                   min_search_radius=int(min_search_radius), coarse_stride=int(coarse_stride),

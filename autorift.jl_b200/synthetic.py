@@ -61,6 +61,32 @@ def shift_bilinear(a: np.ndarray, dx: float, dy: float) -> np.ndarray:
     return out
 
 
+def rotate_bilinear(a: np.ndarray, deg: float) -> np.ndarray:
+    """`a` rotated by `deg` degrees about its centre ((nr + 1) / 2, (nc + 1) / 2, 1-based):
+    each output pixel samples `a` by the inverse rotation, bilinearly, and is zero where a
+    neighbour falls outside `a`. A scene rotation for the rotation-search workloads, in the
+    convention of the reference's `rotate_bilinear` test helper (test/utils.jl:208-224)."""
+    nr, nc = a.shape
+    ii, jj = np.meshgrid(np.arange(1, nr + 1, dtype=np.float64),
+                         np.arange(1, nc + 1, dtype=np.float64), indexing="ij")
+    yc, xc = (nr + 1) / 2, (nc + 1) / 2
+    r = np.deg2rad(deg)
+    s, c = np.sin(r), np.cos(r)
+    dy, dx = ii - yc, jj - xc
+    y = yc + c * dy + s * dx - 1
+    x = xc - s * dy + c * dx - 1
+    i0 = np.floor(y).astype(np.int64)
+    j0 = np.floor(x).astype(np.int64)
+    fy = y - i0
+    fx = x - j0
+    out = np.zeros_like(a, dtype=np.float64)
+    for di, wi in ((0, 1 - fy), (1, fy)):
+        for dj, wj in ((0, 1 - fx), (1, fx)):
+            out += wi * wj * a[np.clip(i0 + di, 0, nr - 1), np.clip(j0 + dj, 0, nc - 1)]
+    out[(i0 < 0) | (j0 < 0) | (i0 + 1 > nr - 1) | (j0 + 1 > nc - 1)] = 0.0
+    return out.astype(a.dtype) if a.dtype.kind == "f" else out
+
+
 def shifted_pair(n: int, shift, seed: int = 0, dtype=np.float32):
     """(reference, secondary) where secondary is reference displaced by shift = (dx, dy)."""
     dx, dy = shift

@@ -14,7 +14,8 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from .methods import NCC, NoRefine, Params, ZNCC, params as make_params, upsampling
+from .methods import (NCC, NoRefine, Params, RotationSearch, ZNCC, angles, params as make_params,
+                      upsampling)
 from .points import FIELDS, PointSet
 
 DTYPES = {np.dtype(np.uint8): _lib.AR_U8, np.dtype(np.uint16): _lib.AR_U16,
@@ -212,10 +213,18 @@ def _measure_code(m) -> int:
                      "with :zncc or :ncc")
 
 
+def rotation_angles(p: Params):
+    """The chip rotations of `p.rotation` as a float64 array, or None for NoRotationSearch."""
+    if isinstance(p.rotation, RotationSearch):
+        return np.ascontiguousarray(angles(p.rotation), dtype=np.float64)
+    return None
+
+
 def track(pair, pts: PointSet, p: Params | None = None, *, subpixel=None,
           measure=None, ctx: "_lib.Context | None" = None) -> DisplacementField:
     """Correlate `pair` (an ImagePair, uploaded on first use, or a PreparedPair already on the
-    device) at every searchable point of `pts` (src/track.jl:103-160)."""
+    device) at every searchable point of `pts` (src/track.jl:103-160), with `p.rotation`'s
+    chip-rotation search when it is a RotationSearch (src/track.jl:313-409)."""
     p = p if p is not None else make_params()
     sub = p.subpixel if subpixel is None else subpixel
     meas = p.similarity[0] if measure is None else measure
@@ -230,9 +239,17 @@ def track(pair, pts: PointSet, p: Params | None = None, *, subpixel=None,
     dy = np.empty(n, np.float32)
     corr = np.empty(n, np.float32)
     searched = np.empty(n, np.uint8)
-    ctx.check(ctx.lib.ar_track(ctx.handle, dp.handle, ctypes.byref(s), upsampling(sub),
-                               _measure_code(meas), dx.ctypes.data, dy.ctypes.data,
-                               corr.ctypes.data, searched.ctypes.data))
+    rot = rotation_angles(p)
+    if rot is None:
+        ctx.check(ctx.lib.ar_track(ctx.handle, dp.handle, ctypes.byref(s), upsampling(sub),
+                                   _measure_code(meas), dx.ctypes.data, dy.ctypes.data,
+                                   corr.ctypes.data, searched.ctypes.data))
+    else:
+        ctx.check(ctx.lib.ar_track_rotated(ctx.handle, dp.handle, ctypes.byref(s),
+                                           upsampling(sub), _measure_code(meas),
+                                           rot.ctypes.data, rot.size, dx.ctypes.data,
+                                           dy.ctypes.data, corr.ctypes.data,
+                                           searched.ctypes.data))
     shp = pts.shape
     out.dx = dx.reshape(shp, order="F")
     out.dy = dy.reshape(shp, order="F")

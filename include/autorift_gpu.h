@@ -118,6 +118,22 @@ int ar_track(ar_ctx* ctx, const ar_pair* pair, const ar_points* pts, int upsampl
              int measure, float* dx, float* dy, float* correlation, uint8_t* searched);
 
 /*
+ * ar_track with the rotation search (_correlate_rotations!, src/track.jl:313-409): every
+ * point correlates its chip turned by each of the `count` angles (degrees, the reference's
+ * angles(RotationSearch): `about` already subtracted; an angle of exactly 0 is the chip
+ * itself), skips angles whose turned chip is degenerate and keeps the surface with the
+ * strictly highest peak, first angle first; a point whose every angle is degenerate is
+ * searched without a measurement. The turned chip is the reference's bilinear resample about
+ * the chip centre (src/track.jl:377-409), rounded to Float32, so these passes correlate in
+ * FP32/FP64 on CUDA cores for every element type. count = 0 is ar_track. At most
+ * AR_MAX_ROTATION_ANGLES angles, finite and distinct.
+ */
+enum { AR_MAX_ROTATION_ANGLES = 64 };
+int ar_track_rotated(ar_ctx* ctx, const ar_pair* pair, const ar_points* pts, int upsampling,
+                     int measure, const double* angles, int count, float* dx, float* dy,
+                     float* correlation, uint8_t* searched);
+
+/*
  * As ar_track with device-resident points and outputs, enqueued on `stream` (a
  * cudaStream_t, or NULL for the context's stream). Returns after the kernels are enqueued;
  * one small device-to-host read of the pass geometry (src/track.jl:176-197) synchronises.
@@ -163,6 +179,12 @@ typedef struct {
     int outlier_window, outlier_iterations;
     double min_agree_fraction, agree_tolerance, mad_scale;
     int fill_window;
+    /* Rotation search (RotationSearch, src/types.jl:529-577): the chip rotations each
+     * correlation tries, in degrees with `about` already subtracted (the reference's
+     * angles(m)); rotation_count 0 is NoRotationSearch. At most AR_MAX_ROTATION_ANGLES finite,
+     * distinct angles. The array is read during the call (ar_submit copies it). */
+    int rotation_count;
+    const double* rotation_angles;
 } ar_multichip_params;
 
 /*

@@ -274,6 +274,80 @@ struct Points {
     int64_t n;
 };
 
+// src/track.jl:377-409 -- _rotate_chip: the chip turned by `deg` degrees about its centre
+// ((ch + 1) / 2, (cw + 1) / 2 in 1-based coordinates). Each destination pixel reads the source
+// by the inverse rotation, interpolates bilinearly in FP64 from its four neighbours, is zero
+// where any neighbour falls outside the chip, and is rounded to Float32 (the reference's
+// rotation buffer). The angle in radians is deg * (pi / 180), Julia's deg2rad; sin and cos come
+// from the C library. Operation order is the reference's, each operation rounded.
+template <class Get>
+void rotate_chip(Get get, int64_t ch, int64_t cw, double deg, float* dst) {
+    const double r = deg * (M_PI / 180.0);
+    const double s = std::sin(r), c = std::cos(r);
+    const double yc = static_cast<double>(ch + 1) / 2.0, xc = static_cast<double>(cw + 1) / 2.0;
+    for (int64_t j = 1; j <= cw; ++j)
+        for (int64_t i = 1; i <= ch; ++i) {
+            const double dy = static_cast<double>(i) - yc, dx = static_cast<double>(j) - xc;
+            const double sy = (yc + c * dy) + s * dx;
+            const double sx = (xc - s * dy) + c * dx;
+            const double fi = std::floor(sy), fj = std::floor(sx);
+            const int64_t i0 = static_cast<int64_t>(fi), j0 = static_cast<int64_t>(fj);
+            float v = 0.0f;
+            if (!(i0 < 1 || j0 < 1 || i0 + 1 > ch || j0 + 1 > cw)) {
+                const double fy = sy - fi, fx = sx - fj;
+                const double v00 = get(i0 - 1, j0 - 1), v10 = get(i0, j0 - 1);
+                const double v01 = get(i0 - 1, j0), v11 = get(i0, j0);
+                v = static_cast<float>((1.0 - fy) * ((1.0 - fx) * v00 + fx * v01) +
+                                       fy * ((1.0 - fx) * v10 + fx * v11));
+            }
+            dst[(i - 1) + (j - 1) * ch] = v;
+        }
+}
+
+// src/track.jl:313-350 -- _correlate_rotations! with a RotationSearch: correlate the chip
+// turned by each angle (the chip itself at an angle of exactly 0), skip the angles whose
+// turned chip is degenerate, and keep the surface whose maximum is strictly larger than every
+// earlier one. Returns false (surface zero) when every angle is degenerate.
+template <class GetW, class GetC>
+bool correlate_rotations(GetW getw, GetC getc, int64_t ch, int64_t cw, int64_t rx, int64_t ry,
+                         int measure, const double* angles, int nang, float* surface,
+                         std::vector<float>& rot, std::vector<float>& hold,
+                         std::vector<float>& chipbuf, std::vector<double>& S,
+                         std::vector<double>& S2, std::vector<double>& num) {
+    const int64_t ns = (2 * ry) * (2 * rx);
+    hold.resize(static_cast<size_t>(ns));
+    rot.resize(static_cast<size_t>(ch * cw));
+    float best = -INFINITY;
+    bool found = false;
+    for (int a = 0; a < nang; ++a) {
+        bool ok;
+        if (angles[a] == 0.0) {
+            ok = correlate(getw, getc, ch, cw, rx, ry, measure, surface, chipbuf, S, S2, num);
+        } else {
+            rotate_chip(getc, ch, cw, angles[a], rot.data());
+            auto getr = [&](int64_t i, int64_t j) {
+                return static_cast<double>(rot[static_cast<size_t>(i + j * ch)]);
+            };
+            ok = correlate(getw, getr, ch, cw, rx, ry, measure, surface, chipbuf, S, S2, num);
+        }
+        if (!ok) continue;
+        float pk = surface[0];
+        for (int64_t e = 1; e < ns; ++e)
+            if (surface[e] > pk) pk = surface[e];
+        if (pk > best) {
+            best = pk;
+            std::copy(surface, surface + ns, hold.begin());
+            found = true;
+        }
+    }
+    if (!found) {
+        std::fill(surface, surface + ns, 0.0f);
+        return false;
+    }
+    std::copy(hold.begin(), hold.end(), surface);
+    return true;
+}
+
 inline int64_t floor_i(double v) { return static_cast<int64_t>(std::floor(v)); }
 
 // Julia's `÷` on Int truncates toward zero.
@@ -282,7 +356,8 @@ inline int64_t jdiv(int64_t a, int64_t b) { return a / b; }
 template <class T>
 int track_impl(const T* ref, const T* sec, const uint8_t* refv, const uint8_t* secv,
                int64_t nrows, int64_t ncols, Points pts, int up, int measure, float* odx,
-               float* ody, float* ocorr, uint8_t* osearched, int nthreads) {
+               float* ody, float* ocorr, uint8_t* osearched, int nthreads,
+               const double* angles = nullptr, int nang = 0) {
     const int64_t n = pts.n;
     for (int64_t k = 0; k < n; ++k) {
         odx[k] = NAN;
@@ -332,7 +407,7 @@ int track_impl(const T* ref, const T* sec, const uint8_t* refv, const uint8_t* s
 #pragma omp parallel
 #endif
     {
-        std::vector<float> surface, chipbuf, ba, bb, tmp;
+        std::vector<float> surface, chipbuf, ba, bb, tmp, rot, hold;
         std::vector<double> S, S2, num;
 #ifdef _OPENMP
 #pragma omp for schedule(dynamic, 4)
@@ -367,9 +442,15 @@ int track_impl(const T* ref, const T* sec, const uint8_t* refv, const uint8_t* s
             auto getw = [&](int64_t i, int64_t j) { return pix(ref, wr0 + i, wc0 + j); };
             const int64_t nr = 2 * pry, nc = 2 * prx;
             surface.resize(static_cast<size_t>(nr * nc));
-            if (!correlate(getw, getc, ch, cw, prx, pry, measure, surface.data(), chipbuf, S, S2,
-                           num))
-                continue;  // degenerate: searched, no measurement
+            // _correlate_rotations! (src/track.jl:313-350): one correlation, or one per angle
+            // with the best kept.
+            const bool ok =
+                nang == 0
+                    ? correlate(getw, getc, ch, cw, prx, pry, measure, surface.data(), chipbuf, S,
+                                S2, num)
+                    : correlate_rotations(getw, getc, ch, cw, prx, pry, measure, angles, nang,
+                                          surface.data(), rot, hold, chipbuf, S, S2, num);
+            if (!ok) continue;  // degenerate: searched, no measurement
             double dx, dy;
             float c;
             subpixel_peak(surface.data(), nr, nc, prx, pry, up, &dx, &dy, &c, ba, bb, tmp);
@@ -668,6 +749,8 @@ struct MCParams {
     int64_t gwindow, giterations;
     double gfrac, gtol, gmad;
     int64_t fill_window;
+    const double* angles;  // RotationSearch chip rotations (degrees), nang of them; 0: none
+    int nang;
 };
 
 // src/window.jl:565-582.
@@ -842,10 +925,10 @@ template <class T>
 void run_track(const MCImages<T>& I, const double* x, const double* y, const int64_t* rx,
                const int64_t* ry, const double* dx0, const double* dy0, const int64_t* csx,
                const int64_t* csy, int64_t n, int up, int measure, float* odx, float* ody,
-               float* oc, uint8_t* os, int nthreads) {
+               float* oc, uint8_t* os, int nthreads, const double* angles, int nang) {
     Points p{x, y, dx0, dy0, rx, ry, csx, csy, n};
     track_impl(I.ref, I.sec, I.refv, I.secv, I.nrows, I.ncols, p, up, measure, odx, ody, oc, os,
-               nthreads);
+               nthreads, angles, nang);
 }
 
 // src/multichip.jl:106-422 -- correlate_multichip over a gridded point set (gr x gc).
@@ -910,7 +993,7 @@ void multichip(const MCImages<T>& I, const double* gx, const double* gy, const i
                     std::vector<uint8_t> cs_(m), measured(m), keep(m), grown(m);
                     run_track(I, cx.data(), cy.data(), crx.data(), cry.data(), cdx0.data(), cdy0.data(),
                               ccsx.data(), ccsy.data(), m, 1, P.measure, cdx.data(), cdy.data(),
-                              ccor.data(), cs_.data(), nthreads);
+                              ccor.data(), cs_.data(), nthreads, P.angles, P.nang);
                     bool anym = false;
                     for (int64_t k = 0; k < m; ++k) { measured[k] = !std::isnan(cdx[k]); anym = anym || measured[k]; }
                     if (!anym) level_off = true;
@@ -944,7 +1027,8 @@ void multichip(const MCImages<T>& I, const double* gx, const double* gy, const i
         std::vector<float> fdx(n), fdy(n), fc(n);
         std::vector<uint8_t> fs(n), measured(n), keep(n), filled(n, 0);
         run_track(I, gx, gy, rx.data(), ry.data(), gdx0, gdy0, vcsx.data(), vcsy.data(), n, P.up,
-                  P.measure, fdx.data(), fdy.data(), fc.data(), fs.data(), nthreads);
+                  P.measure, fdx.data(), fdy.data(), fc.data(), fs.data(), nthreads, P.angles,
+                  P.nang);
         // _reject_and_fill! (src/multichip.jl:318-330).
         for (int64_t i = 0; i < n; ++i) measured[i] = !std::isnan(fdx[i]);
         reject_outliers(fdx.data(), fdy.data(), rx.data(), ry.data(), measured.data(), gr, gc, P.up, P,
@@ -1015,33 +1099,42 @@ void or_subpixel_peak(const float* surface, int64_t nr, int64_t nc, int64_t rx, 
 // track! over a point set (src/track.jl:103-152). Images and masks are nrows x ncols
 // column-major; points are 8 SoA arrays of length n; outputs are prefilled by this call.
 // up = 1 is NoRefine, otherwise PyramidRefine(up). nthreads <= 0 uses the OpenMP default.
+// `angles` (nang of them, degrees, `about` already subtracted: the reference's angles(m)) turns
+// on the rotation search (src/track.jl:313-350); nang = 0 is NoRotationSearch.
 int or_track(const void* ref, const void* sec, const uint8_t* refv, const uint8_t* secv,
              int64_t nrows, int64_t ncols, int dtype, const double* x, const double* y,
              const int64_t* rx, const int64_t* ry, const double* dx0, const double* dy0,
              const int64_t* csx, const int64_t* csy, int64_t n, int up, int measure,
-             float* dx, float* dy, float* corr, uint8_t* searched, int nthreads) {
+             float* dx, float* dy, float* corr, uint8_t* searched, int nthreads,
+             const double* angles, int nang) {
     Points p{x, y, dx0, dy0, rx, ry, csx, csy, n};
+    auto run = [&](auto* r, auto* s) {
+        return track_impl(r, s, refv, secv, nrows, ncols, p, up, measure, dx, dy, corr, searched,
+                          nthreads, angles, nang);
+    };
     switch (dtype) {
-        case OR_U8:
-            return track_impl(static_cast<const uint8_t*>(ref), static_cast<const uint8_t*>(sec),
-                              refv, secv, nrows, ncols, p, up, measure, dx, dy, corr, searched,
-                              nthreads);
+        case OR_U8: return run(static_cast<const uint8_t*>(ref), static_cast<const uint8_t*>(sec));
         case OR_U16:
-            return track_impl(static_cast<const uint16_t*>(ref),
-                              static_cast<const uint16_t*>(sec), refv, secv, nrows, ncols, p, up,
-                              measure, dx, dy, corr, searched, nthreads);
-        case OR_F32:
-            return track_impl(static_cast<const float*>(ref), static_cast<const float*>(sec),
-                              refv, secv, nrows, ncols, p, up, measure, dx, dy, corr, searched,
-                              nthreads);
-        case OR_I16:
-            return track_impl(static_cast<const int16_t*>(ref), static_cast<const int16_t*>(sec),
-                              refv, secv, nrows, ncols, p, up, measure, dx, dy, corr, searched,
-                              nthreads);
-        case OR_F64:
-            return track_impl(static_cast<const double*>(ref), static_cast<const double*>(sec),
-                              refv, secv, nrows, ncols, p, up, measure, dx, dy, corr, searched,
-                              nthreads);
+            return run(static_cast<const uint16_t*>(ref), static_cast<const uint16_t*>(sec));
+        case OR_F32: return run(static_cast<const float*>(ref), static_cast<const float*>(sec));
+        case OR_I16: return run(static_cast<const int16_t*>(ref), static_cast<const int16_t*>(sec));
+        case OR_F64: return run(static_cast<const double*>(ref), static_cast<const double*>(sec));
+        default: return -1;
+    }
+}
+
+// _rotate_chip (src/track.jl:377-409) of one ch x cw chip into `out` (Float32, ch x cw).
+int or_rotate_chip(const void* chip, int dtype, int64_t ch, int64_t cw, double deg, float* out) {
+    auto run = [&](auto* c) {
+        rotate_chip([&](int64_t i, int64_t j) { return as_f64(c[i + j * ch]); }, ch, cw, deg, out);
+        return 0;
+    };
+    switch (dtype) {
+        case OR_U8: return run(static_cast<const uint8_t*>(chip));
+        case OR_U16: return run(static_cast<const uint16_t*>(chip));
+        case OR_F32: return run(static_cast<const float*>(chip));
+        case OR_I16: return run(static_cast<const int16_t*>(chip));
+        case OR_F64: return run(static_cast<const double*>(chip));
         default: return -1;
     }
 }
@@ -1073,13 +1166,16 @@ int or_prepare(const void* img, const uint8_t* mask, int64_t nrows, int64_t ncol
 // correlate_multichip (src/multichip.jl:106-137) over a gridded point set of gr x gc points
 // (column-major fields). params (doubles): chip_base, chip_min, chip_max, aspect, min_radius,
 // stride, buffer, min_frac, up, measure, outliers, window, iterations, min_agree_fraction,
-// agree_tolerance, mad_scale, fill_window.
+// agree_tolerance, mad_scale, fill_window. `angles`, `nang`: the rotation search, as or_track.
 int or_multichip(const void* ref, const void* sec, const uint8_t* refv, const uint8_t* secv,
                  int64_t nrows, int64_t ncols, int dtype, const double* gx, const double* gy,
                  const int64_t* grx, const int64_t* gry, const double* gdx0, const double* gdy0,
                  int64_t gr, int64_t gc, const double* prm, float* dx, float* dy, float* corr,
-                 uint16_t* chip, uint8_t* interp, int nthreads) {
+                 uint16_t* chip, uint8_t* interp, int nthreads, const double* angles,
+                 int nang) {
     MCParams P;
+    P.angles = angles;
+    P.nang = nang;
     P.chip_base = static_cast<int64_t>(prm[0]);
     P.chip_min = static_cast<int64_t>(prm[1]);
     P.chip_max = static_cast<int64_t>(prm[2]);

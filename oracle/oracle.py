@@ -51,11 +51,15 @@ def lib():
         L.or_pyrup.restype = None
         L.or_subpixel_peak.argtypes = [p, i64, i64, i64, i64, i32, f64p, f64p, p]
         L.or_subpixel_peak.restype = None
-        L.or_track.argtypes = [p, p, p, p, i64, i64, i32] + [p] * 8 + [i64, i32, i32] + [p] * 4 + [i32]
+        L.or_track.argtypes = ([p, p, p, p, i64, i64, i32] + [p] * 8 + [i64, i32, i32] + [p] * 4
+                               + [i32, p, i32])
         L.or_track.restype = i32
         L.or_prepare.argtypes = [p, p, i64, i64, i32, i32, i64, ctypes.c_double, i32, p, p]
         L.or_prepare.restype = i32
-        L.or_multichip.argtypes = [p, p, p, p, i64, i64, i32] + [p] * 6 + [i64, i64, p] + [p] * 5 + [i32]
+        L.or_multichip.argtypes = ([p, p, p, p, i64, i64, i32] + [p] * 6 + [i64, i64, p] + [p] * 5
+                                   + [i32, p, i32])
+        L.or_rotate_chip.argtypes = [p, i32, i64, i64, ctypes.c_double, p]
+        L.or_rotate_chip.restype = i32
         L.or_multichip.restype = i32
         L.or_reject_outliers.argtypes = [p, p, p, p, p, i64, i64, i32, i32, i64, i64,
                                          ctypes.c_double, ctypes.c_double, ctypes.c_double, p]
@@ -124,13 +128,33 @@ def subpixel_peak(surface, radius, upsampling):
     return dx.value, dy.value, float(v[0])
 
 
+def _angles(angles):
+    """(pointer, count) of a rotation-search angle list; None or empty is NoRotationSearch."""
+    if angles is None or len(angles) == 0:
+        return None, 0, None
+    a = np.ascontiguousarray(np.asarray(angles, dtype=np.float64).ravel())
+    return _ptr(a), int(a.size), a
+
+
+def rotate_chip(chip, deg: float):
+    """_rotate_chip (src/track.jl:377-409): the chip turned by ``deg`` degrees, Float32."""
+    c = _f(chip)
+    ch, cw = c.shape
+    out = np.empty((ch, cw), dtype=np.float32, order="F")
+    rc = lib().or_rotate_chip(_ptr(c), DTYPE_CODES[c.dtype], ch, cw, float(deg), _ptr(out))
+    if rc != 0:
+        raise ValueError("unsupported dtype")
+    return out
+
+
 def track(reference, secondary, points, upsampling: int = 64, measure: str = "zncc",
-          reference_valid=None, secondary_valid=None, nthreads: int = 0):
+          reference_valid=None, secondary_valid=None, nthreads: int = 0, angles=None):
     """track! over a point set (src/track.jl:103-152).
 
     ``points`` is a mapping with the eight PointSet fields ``x, y, radius_x, radius_y,
     dx_prior, dy_prior, chip_size_x, chip_size_y`` (any shape; flattened column-major).
-    Returns ``(dx, dy, correlation, searched)`` as flat arrays.
+    ``angles`` (degrees, the reference's ``angles(RotationSearch)``) turns on the rotation
+    search (src/track.jl:313-350). Returns ``(dx, dy, correlation, searched)`` as flat arrays.
     """
     ref = _f(reference)
     sec = _f(secondary, ref.dtype)
@@ -160,7 +184,7 @@ def track(reference, secondary, points, upsampling: int = 64, measure: str = "zn
                         DTYPE_CODES[ref.dtype], _ptr(x), _ptr(y), _ptr(rx), _ptr(ry),
                         _ptr(dx0), _ptr(dy0), _ptr(csx), _ptr(csy), n, int(upsampling),
                         MEASURES[measure], _ptr(dx), _ptr(dy), _ptr(corr), _ptr(searched),
-                        int(nthreads))
+                        int(nthreads), *_angles(angles)[:2])
     if rc != 0:
         raise ValueError(f"or_track failed with {rc}")
     return dx, dy, corr, searched.astype(bool)
@@ -189,12 +213,13 @@ def prepare(img, mask=None, preprocess: str = "highpass", width: int = 5, min_st
 
 
 def multichip(reference, secondary, grid, params: dict, reference_valid=None,
-              secondary_valid=None, nthreads: int = 0):
+              secondary_valid=None, nthreads: int = 0, angles=None):
     """correlate_multichip (src/multichip.jl:106-137) over a gridded point set.
 
     ``grid`` maps the PointSet fields to (gr, gc) arrays; ``params`` holds chip_base, chip_min,
     chip_max, aspect, min_radius, stride, buffer, min_frac, up, measure (0/1), outliers (0/1),
     window, iterations, min_agree_fraction, agree_tolerance, mad_scale, fill_window.
+    ``angles`` turns on the rotation search at every level, as in ``track``.
     Returns (dx, dy, correlation, chip_size, interpolated) as (gr, gc) arrays.
     """
     ref = _f(reference)
@@ -225,7 +250,8 @@ def multichip(reference, secondary, grid, params: dict, reference_valid=None,
     it = np.empty(n, np.uint8)
     rc = lib().or_multichip(_ptr(ref), _ptr(sec), _ptr(rv), _ptr(sv), nrows, ncols,
                             DTYPE_CODES[ref.dtype], *[_ptr(a) for a in cols], gr, gc, _ptr(prm),
-                            _ptr(dx), _ptr(dy), _ptr(c), _ptr(cs), _ptr(it), int(nthreads))
+                            _ptr(dx), _ptr(dy), _ptr(c), _ptr(cs), _ptr(it), int(nthreads),
+                            *_angles(angles)[:2])
     if rc != 0:
         raise ValueError("unsupported dtype")
     shp = lambda a: a.reshape((gr, gc), order="F")

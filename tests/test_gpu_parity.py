@@ -153,6 +153,28 @@ def test_uint16_grid(ar, O, gpu_lib):
     _float_checks(g, w)
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.uint16])
+def test_float_scattered_padding_priors_masks(ar, O, gpu_lib, dtype):
+    """Points beyond the image edge: windows partly or wholly in the zero padding. A window
+    without variance must give a zero surface value, as the oracle's exact sums do, never an
+    arbitrary one."""
+    rng = np.random.default_rng(3)
+    ref, sec = ar.synthetic.shifted_pair(200, (2.5, -1.5), seed=11, dtype=dtype)
+    n = 300
+    pts = ar.pointset(rng.uniform(-5, 206, n), rng.uniform(-5, 206, n),
+                      chip_size=rng.choice([16, 20, 32], n), chip_size_y=rng.choice([16, 24, 32], n),
+                      search_radius_x=rng.integers(0, 10, n), search_radius_y=rng.integers(1, 10, n),
+                      dx_prior=np.round(rng.normal(0, 3, n)), dy_prior=rng.normal(0, 2, n))
+    rv = np.ones(ref.shape, bool)
+    rv[60:90, 20:70] = False
+    sv = np.ones(ref.shape, bool)
+    sv[:, 160:] = False
+    for up in (1, 16):
+        g, w = run_both(ar, O, ref, sec, pts, up=up, rv=rv, sv=sv)
+        assert np.nanmax(np.abs(g[2])) <= 1.0 + 1e-6
+        _float_checks(g, w)
+
+
 def test_integer_peaks_match_where_margin_is_clear(ar, O, gpu_lib):
     """Float32 surfaces: identical integer peaks wherever the oracle's top-two margin > 1e-4."""
     a, b, _ = ar.synthetic.plain_512_pair(seed=5)
