@@ -82,6 +82,8 @@ SIGNATURES = {
     "ar_track_rotated": (_i32, [_p, _p, ctypes.POINTER(ArPoints), _i32, _i32, _p, _i32, _p, _p,
                                 _p, _p]),
     "ar_track_device": (_i32, [_p, _p, ctypes.POINTER(ArPoints), _i32, _i32, _p, _p, _p, _p, _p]),
+    "ar_track_device_rotated": (_i32, [_p, _p, ctypes.POINTER(ArPoints), _i32, _i32, _p, _i32,
+                                       _p, _p, _p, _p, _p]),
     "ar_track_device_static": (_i32, [_p, _p, _p, _i64, _i64, _i32, ctypes.POINTER(ArPoints), _i32,
                                       _i32, _p, _p, _p, _p, _p, ctypes.c_char_p, _sz]),
     "ar_correlate": (_i32, [_p, _p, _p, _i32, _i64, _i64, _i64, _i64, _i32, _p,

@@ -28,6 +28,9 @@ struct ar_ctx {
     // Device buffers for host point sets and outputs, grown on demand.
     void* dbuf = nullptr;
     size_t dbuf_bytes = 0;
+    // Scratch of the multichip search, grown on demand and kept between calls.
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
     // Stream-ordered pool for pair images and per-call scratch: freed blocks stay with the
     // context and are reused without a device-wide synchronisation.
     cudaMemPool_t pool = nullptr;
@@ -295,6 +298,7 @@ int ar_ctx_destroy(ar_ctx* c) {
         cudaFree(c->scratch.timer.flops);
         if (c->scratch.done) cudaEventDestroy(c->scratch.done);
         cudaFree(c->dbuf);
+        cudaFree(c->arena);
         if (c->pinned) cudaFreeHost(c->pinned);
         for (auto& ev : c->staged)
             if (ev) cudaEventDestroy(ev);
@@ -483,8 +487,37 @@ int track_host(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up, int me
 
 extern "C" {
 
+namespace {
+
+int track_device(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up, int measure,
+                 const ar::Rotation* rot, float* dx, float* dy, float* corr, uint8_t* searched,
+                 void* stream);
+
+}  // namespace
+
 int ar_track_device(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up, int measure,
                     float* dx, float* dy, float* corr, uint8_t* searched, void* stream) {
+    return track_device(c, p, pts, up, measure, nullptr, dx, dy, corr, searched, stream);
+}
+
+int ar_track_device_rotated(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up,
+                            int measure, const double* angles, int count, float* dx, float* dy,
+                            float* corr, uint8_t* searched, void* stream) {
+    if (count == 0)
+        return track_device(c, p, pts, up, measure, nullptr, dx, dy, corr, searched, stream);
+    ar::Rotation rot;
+    std::string err;
+    if (!ar::make_rotation(angles, count, &rot, &err)) return fail(c, AR_ERR_ARG, err);
+    return track_device(c, p, pts, up, measure, &rot, dx, dy, corr, searched, stream);
+}
+
+}  // extern "C"
+
+namespace {
+
+int track_device(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up, int measure,
+                 const ar::Rotation* rot, float* dx, float* dy, float* corr, uint8_t* searched,
+                 void* stream) {
     int rc = check_track_args(c, p, pts, up, measure);
     if (rc != AR_OK) return rc;
     const int64_t n = pts->n;
@@ -501,11 +534,15 @@ int ar_track_device(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up, i
     ar::DevOutputs dout{dx, dy, corr, searched};
     std::string err;
     e = ar::launch_track(p->dtype, p->ref, p->sec, p->valid, p->nrows, p->ncols, dp, geom, up,
-                         measure, dout, c->scratch, c->num_sms, s, &err);
+                         measure, dout, c->scratch, c->num_sms, s, &err, nullptr, rot);
     if (e != cudaSuccess)
         return err.empty() ? cuda_fail(c, e, "ar_track_device") : fail(c, AR_ERR_UNSUPPORTED, err);
     return AR_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 int ar_correlate(ar_ctx* c, const void* search, const void* chip, int dtype, int64_t ch,
                  int64_t cw, int64_t rx, int64_t ry, int measure, float* surface,
@@ -727,12 +764,21 @@ int multichip_run(ar_ctx* c, const ar_pair* p, const double* gx, const double* g
                   const int64_t* grx, const int64_t* gry, const double* gdx0, const double* gdy0,
                   int64_t gr, int64_t gc, const ar_multichip_params* prm, float* dx, float* dy,
                   float* corr, uint16_t* chip, uint8_t* interp, cudaStream_t s) {
-    // The search's scratch comes from the context's pool in stream order on `s` (no
-    // device-wide synchronisation, so the request loop's slots never stall one another).
+    // The search's scratch is kept by the context and grows from its pool in stream order on
+    // `s` (no device-wide synchronisation, so the request loop's slots never stall one
+    // another). Every call ends with its stream synchronised, so the scratch is idle when the
+    // next call (on any stream) takes it. Kept rather than taken and returned per call: a
+    // block of this size returned to the pool between calls made later allocations slower.
     const size_t ab = ar::multichip_arena_bytes(gr, gc);
-    void* arena = nullptr;
-    cudaError_t ea = cudaMallocFromPoolAsync(&arena, ab, c->pool, s);
-    if (ea != cudaSuccess) return cuda_fail(c, ea, "ar_multichip: scratch");
+    if (c->arena_bytes < ab) {
+        if (c->arena) cudaFreeAsync(c->arena, s);
+        c->arena = nullptr;
+        c->arena_bytes = 0;
+        cudaError_t ea = cudaMallocFromPoolAsync(&c->arena, ab, c->pool, s);
+        if (ea != cudaSuccess) return cuda_fail(c, ea, "ar_multichip: scratch");
+        c->arena_bytes = ab;
+    }
+    void* arena = c->arena;
     ar::MultichipJob J{};
     J.dtype = p->dtype;
     J.ref = p->ref;
@@ -777,7 +823,6 @@ int multichip_run(ar_ctx* c, const ar_pair* p, const double* gx, const double* g
     J.arena_bytes = ab;
     std::string err;
     cudaError_t e = ar::run_multichip(J, c->scratch, c->num_sms, s, &err);
-    cudaFreeAsync(arena, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess)
         return err.empty() ? cuda_fail(c, e, "ar_multichip") : fail(c, AR_ERR_UNSUPPORTED, err);

@@ -267,6 +267,102 @@ def serving_measure(ar, scenes, reqs, device, slots=4, rate=None, repeats=3):
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
 
 
+ROT_ANGLES = (-3.0, 0.0, 3.0)  # RotationSearch()'s default, src/types.jl:557
+
+
+def rotation_measure(ar, ctx, raw, opts, grid, args, dev, stream, flush, fp32_peak, rank, world):
+    """The rotation search (src/track.jl:313-409) over the fine level's point set: every grid
+    point at chip 32 / radius 25 with RotationSearch() (angles -3, 0, 3), on the prepared pair,
+    PyramidRefine(64). Device-timed like the main step, beside the same pass without rotation,
+    and the oracle's restatement timed on a sample of the same points."""
+    import torch
+    L = ar._lib
+    lib = ctx.lib
+    prep = ctypes.c_void_p()
+    ctx.check(lib.ar_prepare(ctx.handle, raw.handle, ctypes.byref(opts), ctypes.byref(prep)))
+    n = len(grid)
+    cols = {f: torch.from_numpy(grid.flat(f)).to(dev) for f in ar.points.FIELDS}
+    cols["chip_size_x"].fill_(CHIP)
+    cols["chip_size_y"].fill_(CHIP)
+    pts = L.ArPoints(*(cols[f].data_ptr() for f in ar.points.FIELDS), n)
+    outs = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3)]
+    osr = torch.empty(n, dtype=torch.uint8, device=dev)
+    angs = np.asarray(ROT_ANGLES, dtype=np.float64)
+    res = {}
+    steps = max(3, args.steps // 4)
+    try:
+        for name, count in (("rotation", angs.size), ("plain", 0)):
+            def call():
+                ctx.check(lib.ar_track_device_rotated(
+                    ctx.handle, prep, ctypes.byref(pts), UP, L.AR_ZNCC, angs.ctypes.data, count,
+                    outs[0].data_ptr(), outs[1].data_ptr(), outs[2].data_ptr(), osr.data_ptr(),
+                    None))
+            with torch.cuda.stream(stream):
+                for _ in range(args.warmup):
+                    flush.fill_(1)
+                    call()
+                torch.cuda.synchronize()
+                ctx.set_timing(True)
+                ctx.kernel_times()
+                tot = 0.0
+                for _ in range(steps):
+                    flush.fill_(1)
+                    ev0 = torch.cuda.Event(enable_timing=True)
+                    ev1 = torch.cuda.Event(enable_timing=True)
+                    ev0.record(stream)
+                    call()
+                    ev1.record(stream)
+                    ev1.synchronize()
+                    tot += ev0.elapsed_time(ev1)
+                corr_ms, refine_ms, _, launches, flops = ctx.kernel_times()
+                ctx.set_timing(False)
+            res[name] = {"points_per_s": world * n * steps / (tot * 1e-3),
+                         "ms_per_pass": tot / steps, "k_corr_ms": corr_ms / steps,
+                         "k_refine_ms": refine_ms / steps,
+                         "corr_tflops": flops / (corr_ms * 1e-3) / 1e12 if corr_ms > 0 else None,
+                         "launches_per_pass": launches / steps}
+        rot_dx = outs[0].cpu().numpy()
+        cpu = None
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            from oracle import oracle as O
+            O.build()
+            ref, sec = (np.empty((args.size, args.size), np.uint8, order="F") for _ in range(2))
+            rv, sv = (np.empty((args.size, args.size), np.uint8, order="F") for _ in range(2))
+            ctx.check(lib.ar_pair_download(ctx.handle, prep, ref.ctypes.data, sec.ctypes.data,
+                                           rv.ctypes.data, sv.ctypes.data))
+            idx = np.linspace(0, n - 1, 10000).astype(np.int64)
+            fl = {f: grid.flat(f)[idx] for f in ar.points.FIELDS}
+            fl["chip_size_x"] = np.full(idx.size, CHIP, np.int64)
+            fl["chip_size_y"] = np.full(idx.size, CHIP, np.int64)
+            t0 = time.perf_counter()
+            wdx = O.track(ref, sec, fl, upsampling=UP, reference_valid=rv, secondary_valid=sv,
+                          angles=ROT_ANGLES)[0]
+            dt = time.perf_counter() - t0
+            m = ~np.isnan(wdx) & ~np.isnan(rot_dx[idx])
+            cpu = {"value": idx.size / dt, "unit": UNIT, "cores": O.max_threads(), "kind": "port",
+                   "sample": f"{idx.size} of the {n} points (evenly spaced), three angles, "
+                             f"{dt:.1f} s",
+                   "dx_agree_1e-3px": float(np.mean(np.abs(wdx[m] - rot_dx[idx][m]) <= 1e-3))
+                   if m.any() else None}
+    finally:
+        lib.ar_pair_destroy(prep)
+    r = res["rotation"]
+    return {"workload": f"track over the {n} grid points at chip {CHIP}, radius {RADIUS}, "
+                        f"PyramidRefine({UP}), RotationSearch() angles {list(ROT_ANGLES)}, on the "
+                        "prepared UInt8 pair; L2 flushed before each pass",
+            "points_per_s": r["points_per_s"], "ms_per_pass": r["ms_per_pass"],
+            "kernel_ms_per_pass": {"k_corr": r["k_corr_ms"], "k_refine": r["k_refine_ms"]},
+            "plain_points_per_s": res["plain"]["points_per_s"],
+            "cost_vs_plain": res["plain"]["points_per_s"] / r["points_per_s"],
+            "roofline": {"bound": "fp32", "kernel": "k_corr (rotation instantiation)",
+                         "achieved": r["corr_tflops"], "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": r["corr_tflops"] / fp32_peak if (r["corr_tflops"] and fp32_peak)
+                         else None,
+                         "peak_source": "cuBLAS SGEMM (TF32 off) measured in this run",
+                         "achieved_basis": "2 * chip area * surface area per point and angle"},
+            "cpu_baseline": cpu, "gpu_launches_per_pass": r["launches_per_pass"]}
+
+
 def gpu_arm(args):
     import torch
     import __graft_entry__ as ge
@@ -399,6 +495,14 @@ def gpu_arm(args):
     same = bool(np.array_equal(hchip, chip)) and bool(
         np.array_equal(hout[0].view(np.uint32), dx.view(np.uint32)))
 
+    rotation = None
+    if not args.no_rotation:
+        try:
+            rotation = rotation_measure(ar, ctx, raw, opts, grid, args, dev, stream, flush,
+                                        fp32_peak, rank, world)
+        except Exception as exc:  # reported, not fatal to the main measurement
+            rotation = {"error": f"{type(exc).__name__}: {exc}"}
+
     serving = None
     if not args.no_serving:
         # A short mixed stream (image sides 512, 2048, 4096 in proportion 8:4:2) through the
@@ -469,6 +573,7 @@ def gpu_arm(args):
                     "path": "ar_pair_upload + ar_prepare + ar_multichip (host buffers) per pair",
                     "same_result_as_device_run": same},
             "serving": serving,
+            "rotation_search": rotation,
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
         }
@@ -541,6 +646,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-rotation", action="store_true",
+                    help="skip the rotation-search measurement")
     ap.add_argument("--no-serving", action="store_true",
                     help="skip the mixed-stream serving measurement")
     ap.add_argument("--serve", action="store_true",

@@ -142,6 +142,12 @@ int ar_track_device(ar_ctx* ctx, const ar_pair* pair, const ar_points* pts_dev,
                     int upsampling, int measure, float* dx_dev, float* dy_dev,
                     float* correlation_dev, uint8_t* searched_dev, void* stream);
 
+/* ar_track_device with the rotation search of ar_track_rotated (`angles`: host array). */
+int ar_track_device_rotated(ar_ctx* ctx, const ar_pair* pair, const ar_points* pts_dev,
+                            int upsampling, int measure, const double* angles, int count,
+                            float* dx_dev, float* dy_dev, float* correlation_dev,
+                            uint8_t* searched_dev, void* stream);
+
 /*
  * ar_track_device without any device allocation. No counterpart in the reference: it exists
  * for callers that cannot allocate device memory when they correlate -- a host that owns the

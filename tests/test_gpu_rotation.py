@@ -240,3 +240,30 @@ def test_invalid_angles_are_rejected(ar, gpu_lib):
     rc = ctx.lib.ar_multichip(ctx.handle, pair.handle, ctypes.byref(gs), gr, gc,
                               ctypes.byref(prm), *(o.ctypes.data for o in o5))
     assert rc == 1
+
+
+def test_device_entry_matches_host_entry(ar, gpu_lib):
+    """ar_track_device_rotated (device points and outputs) gives ar_track_rotated's results."""
+    import torch
+    ctx = ar._lib.default_context()
+    ref, sec = rotated_scene(ar, n=256, deg=2.0, seed=12, dtype=np.uint8)
+    pts = ar.gridpoints(ref.shape, 12, chip_size=32, search_radius=8)
+    p = ar.params(preprocess="none", quantize="none", rotation=True)
+    pair = ar.ImagePair(ref, sec)
+    host = ar.track(pair, pts, p, ctx=ctx)
+    from autorift_b200.points import FIELDS
+    dev = torch.device("cuda", 0)
+    cols = {f: torch.from_numpy(pts.flat(f)).to(dev) for f in FIELDS}
+    st = ar._lib.ArPoints(*(cols[f].data_ptr() for f in FIELDS), len(pts))
+    n = len(pts)
+    outs = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3)]
+    srch = torch.empty(n, dtype=torch.uint8, device=dev)
+    angs = np.asarray(ar.angles(p.rotation), np.float64)
+    ctx.check(ctx.lib.ar_track_device_rotated(
+        ctx.handle, pair.device(ctx).handle, ctypes.byref(st), 64, 0, angs.ctypes.data,
+        angs.size, *(o.data_ptr() for o in outs), srch.data_ptr(), None))
+    ctx.check(ctx.lib.ar_synchronize(ctx.handle))
+    for got, want in zip(outs, (host.dx, host.dy, host.correlation)):
+        assert np.array_equal(got.cpu().numpy().view(np.uint32),
+                              want.ravel(order="F").view(np.uint32))
+    assert np.array_equal(srch.cpu().numpy().astype(bool), host.searched.ravel(order="F"))
