@@ -16,7 +16,8 @@ using AutoRIFT
 using AutoRIFT: ImagePair, PointSet, Params, DisplacementField, displacement_field,
                 ZNCC, NCC, NoRefine, PyramidRefine, upsampling, scatter,
                 Highpass, Wallis, NoPreprocess, QuantizeUInt8, NoQuantize,
-                GardnerFilter, NoOutlierFilter, MultichipResult, gridpoints
+                GardnerFilter, NoOutlierFilter, MultichipResult, gridpoints,
+                RotationSearch, NoRotationSearch
 
 const LIB = get(ENV, "AUTORIFT_GPU_LIB", joinpath(@__DIR__, "..", "libautorift_gpu.so"))
 
@@ -65,7 +66,13 @@ struct ArMultichipParams
     agree_tolerance::Float64
     mad_scale::Float64
     fill_window::Cint
+    rotation_count::Cint              # 0: NoRotationSearch
+    rotation_angles::Ptr{Float64}     # AutoRIFT.angles(p.rotation), read during the call
 end
+
+# The chip rotations of a rotation method (src/types.jl:577), as the C ABI takes them.
+rotation_angles(::NoRotationSearch) = Float64[]
+rotation_angles(m::RotationSearch) = collect(Float64, AutoRIFT.angles(m))
 
 # `ar_request`: one queued autorift() request.
 struct ArRequest
@@ -177,14 +184,16 @@ function track!(out::DisplacementField, pair::ImagePair, pts::PointSet, p::Param
     dy = Vector{Float32}(undef, n)
     cc = Vector{Float32}(undef, n)
     sr = Vector{UInt8}(undef, n)
-    GC.@preserve x y rx ry dx0 dy0 csx csy begin
+    angs = rotation_angles(p.rotation)  # _correlate_rotations! (src/track.jl:313-409)
+    GC.@preserve x y rx ry dx0 dy0 csx csy angs begin
         P = Ref(ArPoints(pointer(x), pointer(y), pointer(rx), pointer(ry), pointer(dx0),
                          pointer(dy0), pointer(csx), pointer(csy), n))
-        rc = ccall((:ar_track, LIB), Cint,
-                   (Ptr{Cvoid}, Ptr{Cvoid}, Ref{ArPoints}, Cint, Cint, Ptr{Float32},
-                    Ptr{Float32}, Ptr{Float32}, Ptr{UInt8}),
-                   ctx, dp.handle, P, upsampling(subpixel), measure_code(measure), dx, dy, cc, sr)
-        check(ctx, rc, "ar_track")
+        rc = ccall((:ar_track_rotated, LIB), Cint,
+                   (Ptr{Cvoid}, Ptr{Cvoid}, Ref{ArPoints}, Cint, Cint, Ptr{Float64}, Cint,
+                    Ptr{Float32}, Ptr{Float32}, Ptr{Float32}, Ptr{UInt8}),
+                   ctx, dp.handle, P, upsampling(subpixel), measure_code(measure), angs,
+                   length(angs), dx, dy, cc, sr)
+        check(ctx, rc, "ar_track_rotated")
     end
     vec(out.dx) .= dx
     vec(out.dy) .= dy
@@ -236,13 +245,14 @@ outlier_fields(f::GardnerFilter) = (Cint(1), f.window, f.iterations, f.min_agree
                                     f.agree_tolerance, f.mad_scale)
 outlier_fields(::NoOutlierFilter) = (Cint(0), 5, 3, 8 / 25, 0.2, 4.0)
 
-function multichip_params(p::Params)
+# `angs` = rotation_angles(p.rotation), preserved by the caller for the duration of the call.
+function multichip_params(p::Params, angs::Vector{Float64})
     o = outlier_fields(p.outliers)
     ArMultichipParams(p.chip_size_base, p.chip_size_min, p.chip_size_max, p.chip_aspect,
                       p.min_search_radius, p.coarse_stride, p.coarse_buffer,
                       p.min_coarse_valid_fraction, upsampling(p.subpixel),
                       measure_code(first(p.similarity)), o[1], o[2], o[3], o[4], o[5], o[6],
-                      p.fill_window)
+                      p.fill_window, length(angs), isempty(angs) ? C_NULL : pointer(angs))
 end
 
 # The eight PointSet fields flattened, kept alive by the returned tuple.
@@ -270,8 +280,9 @@ function correlate_multichip(prepared::ImagePair, grid::PointSet, p::Params; dev
     dx = Matrix{Float32}(undef, gr, gc); dy = similar(dx); cc = similar(dx)
     cs = Matrix{UInt16}(undef, gr, gc); it = Matrix{UInt8}(undef, gr, gc)
     P, cols = flat_points(grid)
-    prm = Ref(multichip_params(p))
-    GC.@preserve cols begin
+    angs = rotation_angles(p.rotation)
+    prm = Ref(multichip_params(p, angs))
+    GC.@preserve cols angs begin
         rc = ccall((:ar_multichip, LIB), Cint,
                    (Ptr{Cvoid}, Ptr{Cvoid}, Ref{ArPoints}, Int64, Int64, Ref{ArMultichipParams},
                     Ptr{Float32}, Ptr{Float32}, Ptr{Float32}, Ptr{UInt16}, Ptr{UInt8}),
@@ -326,15 +337,17 @@ function submit(image1::AbstractMatrix{T}, image2::AbstractMatrix{T}, grid::Poin
     it = Matrix{UInt8}(undef, gr, gc)
     P, cols = flat_points(grid)
     Pref = Ref(P)
+    angs = rotation_angles(p.rotation)  # copied by ar_submit
     req = Ref(ArRequest(pointer(ref), pointer(sec), C_NULL,
                         sv === nothing ? C_NULL : Ptr{UInt8}(pointer(sv)),
                         size(ref, 1), size(ref, 2), eltype_code(T),
-                        prepare_opts(p.preprocess, p.quantize), multichip_params(p),
+                        prepare_opts(p.preprocess, p.quantize), multichip_params(p, angs),
                         Base.unsafe_convert(Ptr{ArPoints}, Pref), gr, gc,
                         pointer(res.dx), pointer(res.dy), pointer(res.correlation),
                         pointer(res.chip_size), pointer(it)))
     t = Ref{Int64}(0)
-    rc = ccall((:ar_submit, LIB), Cint, (Ptr{Cvoid}, Ref{ArRequest}, Ref{Int64}), ctx, req, t)
+    rc = GC.@preserve angs ccall((:ar_submit, LIB), Cint, (Ptr{Cvoid}, Ref{ArRequest}, Ref{Int64}),
+                                 ctx, req, t)
     check(ctx, rc, "ar_submit")
     return Ticket(ctx, t[], (ref, sec, sv, cols, Pref, req, it), res)
 end
