@@ -5,14 +5,120 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstdint>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "ar_internal.cuh"
+
+namespace {
+
+// Host threads that split large copies between caller-owned (pageable) arrays and the pinned
+// staging buffers. One core copies at roughly a fifth of what the PCIe link carries, so a
+// single-threaded copy, not the DMA, set the pace of uploads. A copy is cut into pieces that
+// the calling thread and the workers claim from one counter; the counter carries the copy's
+// generation in its upper half, so a worker that wakes late can never claim a piece of a
+// later copy with an earlier copy's pointers.
+class CopyPool {
+public:
+    explicit CopyPool(int workers) {
+        for (int i = 0; i < workers; ++i) threads_.emplace_back([this] { work(); });
+    }
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_job_.notify_all();
+        for (auto& t : threads_) t.join();
+    }
+    // memcpy(dst, src, bytes), shared with the workers when it is large. One copy at a time
+    // (the owning context's lock serialises its callers).
+    void copy(void* dst, const void* src, size_t bytes) {
+        constexpr size_t kMinSplit = 512u << 10, kPieceAlign = 64u << 10;
+        if (threads_.empty() || bytes < kMinSplit) {
+            std::memcpy(dst, src, bytes);
+            return;
+        }
+        const size_t ways = threads_.size() + 1;
+        Job j;
+        j.dst = static_cast<unsigned char*>(dst);
+        j.src = static_cast<const unsigned char*>(src);
+        j.bytes = bytes;
+        j.piece = (bytes / ways + kPieceAlign - 1) / kPieceAlign * kPieceAlign;
+        j.parts = static_cast<uint32_t>((bytes + j.piece - 1) / j.piece);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            j.gen = ++gen_;
+            job_ = j;
+            done_ = 0;
+            next_.store(static_cast<uint64_t>(j.gen) << 32);
+        }
+        cv_job_.notify_all();
+        run(j);
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_done_.wait(lk, [&] { return done_ == j.parts; });
+    }
+
+private:
+    struct Job {
+        unsigned char* dst = nullptr;
+        const unsigned char* src = nullptr;
+        size_t bytes = 0, piece = 0;
+        uint32_t parts = 0, gen = 0;
+    };
+    void run(const Job& j) {
+        uint32_t mine = 0;
+        uint64_t cur = next_.load();
+        while ((cur >> 32) == j.gen && static_cast<uint32_t>(cur) < j.parts) {
+            if (!next_.compare_exchange_weak(cur, cur + 1)) continue;
+            const size_t off = static_cast<size_t>(static_cast<uint32_t>(cur)) * j.piece;
+            std::memcpy(j.dst + off, j.src + off, std::min(j.piece, j.bytes - off));
+            ++mine;
+            cur = next_.load();
+        }
+        if (mine) {
+            std::lock_guard<std::mutex> lk(mu_);
+            if (gen_ == j.gen) done_ += mine;
+            if (done_ == j.parts) cv_done_.notify_all();
+        }
+    }
+    void work() {
+        uint32_t seen = 0;
+        for (;;) {
+            Job j;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_job_.wait(lk, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+                j = job_;
+            }
+            run(j);
+        }
+    }
+    std::vector<std::thread> threads_;
+    std::mutex mu_;
+    std::condition_variable cv_job_, cv_done_;
+    Job job_;
+    uint32_t gen_ = 0, done_ = 0;
+    std::atomic<uint64_t> next_{0};
+    bool stop_ = false;
+};
+
+int copy_workers() {
+    const unsigned hw = std::thread::hardware_concurrency();
+    return static_cast<int>(std::min(15u, hw > 1 ? hw - 1 : 0u));
+}
+
+}  // namespace
 
 struct ar_ctx {
     int device = 0;
@@ -25,6 +131,7 @@ struct ar_ctx {
     unsigned char* pinned = nullptr;
     size_t pinned_bytes = 0;
     cudaEvent_t staged[2] = {nullptr, nullptr};
+    std::unique_ptr<CopyPool> copier;  // host threads for the staging copies
     // Device buffers for host point sets and outputs, grown on demand.
     void* dbuf = nullptr;
     size_t dbuf_bytes = 0;
@@ -95,6 +202,7 @@ cudaError_t ensure_pinned(ar_ctx* c) {
     cudaError_t e = cudaMallocHost(&c->pinned, kStageBytes);
     if (e != cudaSuccess) return e;
     c->pinned_bytes = kStageBytes;
+    c->copier.reset(new CopyPool(copy_workers()));
     for (auto& ev : c->staged) {
         e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
         if (e != cudaSuccess) return e;
@@ -116,7 +224,7 @@ cudaError_t stage_h2d(ar_ctx* c, void* dst, const void* src, size_t bytes) {
         e = cudaEventSynchronize(c->staged[slot]);  // the slot's previous DMA has finished
         if (e != cudaSuccess) return e;
         unsigned char* buf = c->pinned + slot * half;
-        std::memcpy(buf, static_cast<const unsigned char*>(src) + off, n);
+        c->copier->copy(buf, static_cast<const unsigned char*>(src) + off, n);
         e = cudaMemcpyAsync(static_cast<unsigned char*>(dst) + off, buf, n, cudaMemcpyHostToDevice,
                             c->stream);
         if (e != cudaSuccess) return e;
@@ -142,8 +250,8 @@ cudaError_t stage_d2h(ar_ctx* c, void* dst, const void* src, size_t bytes) {
             e = cudaEventSynchronize(c->staged[slot]);
             if (e != cudaSuccess) return e;
             if (pending_n[slot]) {
-                std::memcpy(static_cast<unsigned char*>(dst) + pending_off[slot],
-                            c->pinned + slot * half, pending_n[slot]);
+                c->copier->copy(static_cast<unsigned char*>(dst) + pending_off[slot],
+                                c->pinned + slot * half, pending_n[slot]);
                 pending_n[slot] = 0;
             }
             const size_t n = std::min(half, bytes - off);
@@ -161,8 +269,8 @@ cudaError_t stage_d2h(ar_ctx* c, void* dst, const void* src, size_t bytes) {
                 if (!pending_n[s]) continue;
                 e = cudaEventSynchronize(c->staged[s]);
                 if (e != cudaSuccess) return e;
-                std::memcpy(static_cast<unsigned char*>(dst) + pending_off[s], c->pinned + s * half,
-                            pending_n[s]);
+                c->copier->copy(static_cast<unsigned char*>(dst) + pending_off[s],
+                                c->pinned + s * half, pending_n[s]);
                 pending_n[s] = 0;
             }
         }
