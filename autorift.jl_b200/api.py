@@ -137,9 +137,9 @@ def reinit_(cache: Cache, *, reference=None, secondary=None, reference_valid=Non
 
     def maskfor(img):
         if img is old.reference:
-            return old.reference_valid
+            return old.given_reference_valid
         if img is old.secondary:
-            return old.secondary_valid
+            return old.given_secondary_valid
         return None
 
     rv = maskfor(ref) if reference_valid is None else reference_valid
@@ -249,7 +249,7 @@ def submit(reference, secondary, grid: PointSet | None = None, *, reference_vali
            secondary_valid=None, ctx=None, **kw) -> Ticket:
     """Queue `autorift(reference, secondary; kw...)` on the context's request loop (ar_submit)
     and return at once; requests submitted together run concurrently on the device."""
-    from .track import DTYPES, _colmajor
+    from .track import DTYPES, _colmajor, _mask_bytes
     p = make_params(**kw)
     ctx = ctx or _lib.default_context()
     ref = np.asarray(reference)
@@ -274,7 +274,7 @@ def submit(reference, secondary, grid: PointSet | None = None, *, reference_vali
             m = np.asarray(m, dtype=bool)
             if m.shape != img.shape:
                 raise ValueError(f"a mask is {m.shape} but the image is {img.shape}")
-            masks.append(_colmajor(m, np.uint8))
+            masks.append(_mask_bytes(m))
     st, cols = points_struct(grid)
     outs = [np.empty(n, np.float32) for _ in range(3)] + [np.empty(n, np.uint16),
                                                            np.empty(n, np.uint8)]

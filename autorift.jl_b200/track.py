@@ -27,6 +27,15 @@ def _colmajor(a, dtype=None) -> np.ndarray:
     return np.asfortranarray(a)
 
 
+def _mask_bytes(m) -> np.ndarray:
+    """A validity mask as the column-major bytes the C ABI reads: a bool array is viewed as
+    its bytes (0/1) without a copy when it is already column-major."""
+    m = np.asarray(m)
+    if m.dtype == np.bool_:
+        return np.asfortranarray(m).view(np.uint8)
+    return _colmajor(m != 0).view(np.uint8)
+
+
 class ImagePair:
     """The two images to correlate with their validity masks (src/preprocess.jl:41-106).
 
@@ -46,18 +55,33 @@ class ImagePair:
             sec = sec.astype(ref.dtype)
         self.reference = ref
         self.secondary = sec
-        self.reference_valid = self._mask(reference_valid, ref, "reference_valid")
-        self.secondary_valid = self._mask(secondary_valid, sec, "secondary_valid")
+        # Masks the caller gave (None: the default, finiteness, which the device computes).
+        self.given_reference_valid = self._mask(reference_valid, ref, "reference_valid")
+        self.given_secondary_valid = self._mask(secondary_valid, sec, "secondary_valid")
         self._device = {}
 
     @staticmethod
     def _mask(m, img, name):
         if m is None:
-            return np.isfinite(img) if img.dtype.kind in "fc" else np.ones(img.shape, bool)
+            return None
         m = np.asarray(m, dtype=bool)
         if m.shape != img.shape:
             raise ValueError(f"{name} is {m.shape} but the image is {img.shape}")
         return m
+
+    @staticmethod
+    def _default(img):
+        return np.isfinite(img) if img.dtype.kind in "fc" else np.ones(img.shape, bool)
+
+    @property
+    def reference_valid(self) -> np.ndarray:
+        m = self.given_reference_valid
+        return self._default(self.reference) if m is None else m
+
+    @property
+    def secondary_valid(self) -> np.ndarray:
+        m = self.given_secondary_valid
+        return self._default(self.secondary) if m is None else m
 
     @property
     def shape(self):
@@ -80,11 +104,14 @@ class ImagePair:
                             f"(supported: {', '.join(str(d) for d in DTYPES)})")
         ref = _colmajor(self.reference)
         sec = _colmajor(self.secondary)
-        rv = _colmajor(self.reference_valid, np.uint8)
-        sv = _colmajor(self.secondary_valid, np.uint8)
+        # A mask left to its default is not uploaded: the device evaluates the same finiteness
+        # test (ar_pair_upload with a NULL mask).
+        rv, sv = (None if m is None else _mask_bytes(m)
+                  for m in (self.given_reference_valid, self.given_secondary_valid))
         out = ctypes.c_void_p()
         ctx.check(ctx.lib.ar_pair_upload(ctx.handle, ref.ctypes.data, sec.ctypes.data,
-                                         rv.ctypes.data, sv.ctypes.data, ref.shape[0],
+                                         None if rv is None else rv.ctypes.data,
+                                         None if sv is None else sv.ctypes.data, ref.shape[0],
                                          ref.shape[1], DTYPES[self.dtype], ctypes.byref(out)))
         h = _DevicePair(ctx, out)
         self._device[id(ctx)] = h

@@ -203,42 +203,53 @@ def serving_requests(ar, rng, n_req, sizes, weights, base=None):
 
 
 def serving_measure(ar, scenes, reqs, device, slots=4, rate=None, repeats=3):
-    """The stream through the plain one-pair-at-a-time path and through the request loop,
-    alternated `repeats` times (medians reported: the plain path of small pairs is bound by host
-    round trips, so single runs vary with the host). Returns points/s of each, and per-request
-    latency (queued + running, from the loop's own clock) for a Poisson stream at `rate`
-    requests/s (default: 70% of the measured capacity)."""
+    """The stream three ways: the plain GPU path (one pair at a time, the direct FP32
+    correlation on CUDA cores -- tensor cores off), the same one-pair-at-a-time loop with the
+    tensor-core kernels the server runs ("sequential"), and the request loop (continuous
+    batching, `slots` slots). The three are alternated `repeats` times and medians reported
+    (small pairs are bound by host round trips, so single runs vary with the host). Also the
+    per-request latency (queued + running, from the loop's own clock) for a Poisson stream at
+    `rate` requests/s (default: 70% of the measured capacity)."""
     L = ar._lib
     points = [len(ar.build_grid(scenes[n][0].shape, ar.params(**kw))) for n, kw in reqs]
     plain_ctx = L.Context(device)
+    plain_ctx.set_option(L.AR_OPT_TENSOR_CORES, 0)
+    seq_ctx = L.Context(device)
     ctx = L.Context(device)
     ctx.set_option(L.AR_OPT_SERVE_SLOTS, slots)
-    # Warm-up: the whole stream once through both paths (untimed), so every slot has met the
-    # largest request and the timed passes see the steady state of a running server.
-    for n, kw in reqs:
-        a, b, v = scenes[n]
-        ar.autorift(a, b, secondary_valid=v, ctx=plain_ctx, **kw)
-    for t in [ar.submit(*scenes[n][:2], secondary_valid=scenes[n][2], ctx=ctx, **kw)
-              for n, kw in reqs]:
-        t.wait()
-    plain_runs, burst_runs = [], []
-    for _ in range(repeats):
-        t0 = time.perf_counter()
+
+    def one_at_a_time(c):
+        out = []
         for n, kw in reqs:
             a, b, v = scenes[n]
-            ar.autorift(a, b, secondary_valid=v, ctx=plain_ctx, **kw)
-        plain_runs.append(time.perf_counter() - t0)
-        t0 = time.perf_counter()
+            out.append(ar.autorift(a, b, secondary_valid=v, ctx=c, **kw))
+        return out
+
+    def served():
         tickets = [ar.submit(*scenes[n][:2], secondary_valid=scenes[n][2], ctx=ctx, **kw)
                    for n, kw in reqs]
-        for t in tickets:
-            t.wait()
-        burst_runs.append(time.perf_counter() - t0)
-        del tickets
+        return [t.wait() for t in tickets]
+
+    # Warm-up: the whole stream once through every path (untimed), so every slot has met the
+    # largest request and the timed passes see the steady state of a running server.
+    plain_res = one_at_a_time(plain_ctx)
+    one_at_a_time(seq_ctx)
+    served_res = served()
+    # Matched accuracy: the served results against the plain path's.
+    m = [(~np.isnan(p_.dx)) & (~np.isnan(s_.dx)) for p_, s_ in zip(plain_res, served_res)]
+    dd = np.concatenate([np.maximum(np.abs(p_.dx - s_.dx), np.abs(p_.dy - s_.dy))[k]
+                         for p_, s_, k in zip(plain_res, served_res, m)])
+    runs = {"plain": [], "sequential": [], "batched": []}
+    for _ in range(repeats):
+        for name, fn in (("plain", lambda: one_at_a_time(plain_ctx)),
+                         ("sequential", lambda: one_at_a_time(seq_ctx)), ("batched", served)):
+            t0 = time.perf_counter()
+            fn()
+            runs[name].append(time.perf_counter() - t0)
     plain_ctx.close()
-    plain_s = float(np.median(plain_runs))
-    burst_s = float(np.median(burst_runs))
-    cap = len(reqs) / burst_s
+    seq_ctx.close()
+    med = {k: float(np.median(v)) for k, v in runs.items()}
+    cap = len(reqs) / med["batched"]
     rate = rate or 0.7 * cap
     rng = np.random.default_rng(1)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
@@ -259,10 +270,17 @@ def serving_measure(ar, scenes, reqs, device, slots=4, rate=None, repeats=3):
     ctx.close()
     total = float(sum(points))
     return {"requests": len(reqs), "points": int(total), "slots": slots, "repeats": repeats,
-            "plain_points_per_s": total / plain_s, "plain_pairs_per_s": len(reqs) / plain_s,
-            "batched_points_per_s": total / burst_s, "batched_pairs_per_s": cap,
-            "speedup_vs_plain": plain_s / burst_s,
-            "speedup_per_repeat": [p / q for p, q in zip(plain_runs, burst_runs)],
+            "plain_points_per_s": total / med["plain"],
+            "plain_path": "one pair at a time, direct FP32 correlation on CUDA cores "
+                          "(AR_OPT_TENSOR_CORES = 0)",
+            "sequential_points_per_s": total / med["sequential"],
+            "batched_points_per_s": total / med["batched"], "batched_pairs_per_s": cap,
+            "speedup_vs_plain": med["plain"] / med["batched"],
+            "speedup_per_repeat": [p_ / q_ for p_, q_ in zip(runs["plain"], runs["batched"])],
+            "speedup_vs_sequential": med["sequential"] / med["batched"],
+            "matched_accuracy": {"points_compared": int(dd.size),
+                                 "dx_dy_within_1e-3px": float(np.mean(dd <= 1e-3))
+                                 if dd.size else None},
             "stream_rate_pairs_per_s": rate, "stream_points_per_s": total / stream_s,
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
 
@@ -443,6 +461,41 @@ def gpu_arm(args):
     dx = outs[0].cpu().numpy()
     chip = ochip.cpu().numpy().view(np.uint16)
     resolved = int(np.count_nonzero(chip))
+
+    # The plain GPU path on the same step: the direct FP32 correlation on CUDA cores (tensor
+    # cores off), one pair at a time, timed the same way; and its agreement with the results
+    # above (integer peaks are identical -- both numerators are exact for UInt8 -- so dx/dy
+    # agree to the bit).
+    plain = None
+    if not args.profile:
+        ctx.set_option(L.AR_OPT_TENSOR_CORES, 0)
+        psteps = max(3, args.steps // 4)
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+            step()
+            torch.cuda.synchronize()
+            ptot = 0.0
+            for _ in range(psteps):
+                flush.fill_(1)
+                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s.record(stream)
+                step()
+                e.record(stream)
+                e.synchronize()
+                ptot += s.elapsed_time(e)
+        ctx.set_option(L.AR_OPT_TENSOR_CORES, 1)
+        pt = torch.tensor([ptot], dtype=torch.float64, device=dev)
+        if dist:
+            dist.all_reduce(pt, op=dist.ReduceOp.MAX)
+        ptot = float(pt.item())
+        pdx = outs[0].cpu().numpy()
+        plain = {"points_per_s": world * n * psteps / (ptot * 1e-3), "ms_per_step": ptot / psteps,
+                 "steps": psteps,
+                 "path": "the same step with AR_OPT_TENSOR_CORES = 0: the direct FP32 "
+                         "correlation on CUDA cores (k_corr), one pair at a time",
+                 "speedup": (world * n * args.steps / (total_ms * 1e-3)) /
+                            (world * n * psteps / (ptot * 1e-3)),
+                 "identical_dx": bool(np.array_equal(pdx.view(np.uint32), dx.view(np.uint32)))}
     levels = {int(c): int(np.count_nonzero(chip == c)) for c in np.unique(chip) if c}
     med_dx = float(np.nanmedian(dx)) if resolved else float("nan")
 
@@ -506,17 +559,17 @@ def gpu_arm(args):
     serving = None
     if not args.no_serving:
         # A short mixed stream (image sides 512, 2048, 4096 in proportion 8:4:2) through the
-        # plain path and the request loop.
+        # plain path, the sequential path and the request loop.
         try:
             sc, reqs = serving_requests(ar, np.random.default_rng(5), 28, (512, 2048, N),
                                         (8, 4, 2), base=(a, b, valid))
             serving = serving_measure(ar, sc, reqs, local)
             serving["workload"] = ("28 requests, sides 512/2048/4096 (8:4:2), spacing {8,16,32}, "
                                    "chip {16,32,64}, radius U[8,48], PyramidRefine(64); after one "
-                                   "untimed pass of the stream through both paths, plain "
-                                   "and batched passes alternated 3 times (medians); latency "
-                                   "from submission to completion at a Poisson rate of 70% of "
-                                   "capacity")
+                                   "untimed pass of the stream through every path, plain, "
+                                   "sequential and batched passes alternated 3 times (medians); "
+                                   "latency from submission to completion at a Poisson rate of "
+                                   "70% of capacity")
         except Exception as exc:  # reported, not fatal to the main measurement
             serving = {"error": f"{type(exc).__name__}: {exc}"}
 
@@ -572,6 +625,7 @@ def gpu_arm(args):
                     "p99_ms": float(np.percentile(e2e_times, 99)) * 1e3,
                     "path": "ar_pair_upload + ar_prepare + ar_multichip (host buffers) per pair",
                     "same_result_as_device_run": same},
+            "plain_gpu_path": plain,
             "serving": serving,
             "rotation_search": rotation,
             "clocks": clk.summary(),
