@@ -113,6 +113,19 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def replicas_rate(dist, elapsed_ms, points_per_rank, steps, device=None):
+    """Whole-job rate of independent replicas: every rank processed `points_per_rank` points per
+    step for `steps` steps; the job took as long as its slowest rank (max over ranks; no data
+    moves between ranks). Returns (max elapsed ms, points/s of the whole job)."""
+    import torch
+    world = dist.get_world_size() if dist else 1
+    t = torch.tensor([float(elapsed_ms)], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    return ms, world * points_per_rank * steps / (ms * 1e-3)
+
+
 def measured_peaks():
     try:
         return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -450,13 +463,10 @@ def gpu_arm(args):
         torch.cuda.synchronize()
     corr_ms, refine_ms, tracks, launches, corr_flops = ctx.kernel_times()
     ctx.set_timing(False)
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
     if dist:
         dist.barrier()
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms, value = replicas_rate(dist, total_ms, n, args.steps, dev)
     ms_per_step = total_ms / args.steps
-    value = world * n * args.steps / (total_ms * 1e-3)
 
     dx = outs[0].cpu().numpy()
     chip = ochip.cpu().numpy().view(np.uint16)
@@ -484,17 +494,12 @@ def gpu_arm(args):
                 e.synchronize()
                 ptot += s.elapsed_time(e)
         ctx.set_option(L.AR_OPT_TENSOR_CORES, 1)
-        pt = torch.tensor([ptot], dtype=torch.float64, device=dev)
-        if dist:
-            dist.all_reduce(pt, op=dist.ReduceOp.MAX)
-        ptot = float(pt.item())
+        ptot, prate = replicas_rate(dist, ptot, n, psteps, dev)
         pdx = outs[0].cpu().numpy()
-        plain = {"points_per_s": world * n * psteps / (ptot * 1e-3), "ms_per_step": ptot / psteps,
-                 "steps": psteps,
+        plain = {"points_per_s": prate, "ms_per_step": ptot / psteps, "steps": psteps,
                  "path": "the same step with AR_OPT_TENSOR_CORES = 0: the direct FP32 "
                          "correlation on CUDA cores (k_corr), one pair at a time",
-                 "speedup": (world * n * args.steps / (total_ms * 1e-3)) /
-                            (world * n * psteps / (ptot * 1e-3)),
+                 "speedup": value / prate,
                  "identical_dx": bool(np.array_equal(pdx.view(np.uint32), dx.view(np.uint32)))}
     levels = {int(c): int(np.count_nonzero(chip == c)) for c in np.unique(chip) if c}
     med_dx = float(np.nanmedian(dx)) if resolved else float("nan")
