@@ -298,6 +298,41 @@ def serving_measure(ar, scenes, reqs, device, slots=4, rate=None, repeats=3):
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
 
 
+def oracle_sample(ar, ctx, raw, opts, grid, size, seed=1):
+    """The oracle on a seeded 1% sample of the step's points: the chip-32 pass (radius 25,
+    PyramidRefine(64), ZNCC) on the prepared pair, the library against the oracle's FP64
+    numerator on the same points and inputs."""
+    from oracle import oracle as O
+    L = ar._lib
+    lib = ctx.lib
+    O.build()
+    prep = ctypes.c_void_p()
+    ctx.check(lib.ar_prepare(ctx.handle, raw.handle, ctypes.byref(opts), ctypes.byref(prep)))
+    try:
+        ref, sec = (np.empty((size, size), np.uint8, order="F") for _ in range(2))
+        rv, sv = (np.empty((size, size), np.uint8, order="F") for _ in range(2))
+        ctx.check(lib.ar_pair_download(ctx.handle, prep, ref.ctypes.data, sec.ctypes.data,
+                                       rv.ctypes.data, sv.ctypes.data))
+        n = len(grid)
+        idx = np.sort(np.random.default_rng(seed).choice(n, n // 100, replace=False))
+        fl = {f: np.ascontiguousarray(grid.flat(f)[idx]) for f in ar.points.FIELDS}
+        fl["chip_size_x"] = np.full(idx.size, CHIP, np.int64)
+        fl["chip_size_y"] = np.full(idx.size, CHIP, np.int64)
+        st = L.ArPoints(*(fl[f].ctypes.data for f in ar.points.FIELDS), idx.size)
+        g = [np.empty(idx.size, np.float32) for _ in range(3)] + [np.empty(idx.size, np.uint8)]
+        ctx.check(lib.ar_track(ctx.handle, prep, ctypes.byref(st), UP, L.AR_ZNCC,
+                               *(a.ctypes.data for a in g)))
+        w = O.track(ref, sec, fl, upsampling=UP, reference_valid=rv, secondary_valid=sv)
+    finally:
+        lib.ar_pair_destroy(prep)
+    same = [bool(np.array_equal(a.view(np.uint32), b.view(np.uint32))) for a, b in zip(g[:3], w[:3])]
+    return {"points": int(idx.size), "seed": seed,
+            "pass": f"chip {CHIP}, radius {RADIUS}, PyramidRefine({UP}) on the prepared pair",
+            "dx_dy_correlation_bit_identical": all(same),
+            "searched_identical": bool(np.array_equal(g[3].astype(bool), w[3])),
+            "measured": int(np.count_nonzero(~np.isnan(w[0])))}
+
+
 ROT_ANGLES = (-3.0, 0.0, 3.0)  # RotationSearch()'s default, src/types.jl:557
 
 
@@ -553,6 +588,13 @@ def gpu_arm(args):
     same = bool(np.array_equal(hchip, chip)) and bool(
         np.array_equal(hout[0].view(np.uint32), dx.view(np.uint32)))
 
+    parity = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            parity = oracle_sample(ar, ctx, raw, opts, grid, args.size)
+        except Exception as exc:  # reported, not fatal to the main measurement
+            parity = {"error": f"{type(exc).__name__}: {exc}"}
+
     rotation = None
     if not args.no_rotation:
         try:
@@ -631,6 +673,7 @@ def gpu_arm(args):
                     "path": "ar_pair_upload + ar_prepare + ar_multichip (host buffers) per pair",
                     "same_result_as_device_run": same},
             "plain_gpu_path": plain,
+            "oracle_sample": parity,
             "serving": serving,
             "rotation_search": rotation,
             "clocks": clk.summary(),
