@@ -2304,24 +2304,31 @@ __device__ __forceinline__ void tap_range(int p0, int p1, int n, int& lo, int& h
 }
 
 // One full pyrUp step by a warp: src (S x S, column-major) -> dst (2S x 2S) via tmp (2S x S).
-// Vertical then horizontal, as src/peak.jl:261-292.
+// Vertical then horizontal, as src/peak.jl:261-292. Outputs 2c and 2c + 1 of an axis read the
+// same source samples (c - 1, or 1 at the edge; c; c + 1, clamped), so each lane produces such a
+// pair from three loads: `taps` in closed form, with the same rounded operations per sample.
+// `tmp` must be 8-byte aligned.
 template <int S>
 __device__ void pyrup_warp(const float* src, float* dst, float* tmp) {
     const int lane = threadIdx.x & 31;
     constexpr int D = 2 * S;
-    for (int e = lane; e < D * S; e += 32) {
-        const int i = e % D, j = e / D;
-        int m, c, q;
-        const int nt = taps(i, S, m, c, q);
+    for (int e = lane; e < S * S; e += 32) {
+        const int c = e % S, j = e / S;
+        const int m = c == 0 ? 1 : c - 1, q = min(c + 1, S - 1);
         const float* s = src + j * S;
-        tmp[e] = pyr_sample(nt, s[m], s[c], s[q]);
+        const float a = s[m], b = s[c], d = s[q];
+        float2 v;
+        v.x = pyr_sample(3, a, b, d);
+        v.y = pyr_sample(2, b, b, d);
+        *reinterpret_cast<float2*>(tmp + 2 * c + j * D) = v;
     }
     __syncwarp();
-    for (int e = lane; e < D * D; e += 32) {
-        const int i = e % D, j = e / D;
-        int m, c, q;
-        const int nt = taps(j, S, m, c, q);
-        dst[e] = pyr_sample(nt, tmp[i + m * D], tmp[i + c * D], tmp[i + q * D]);
+    for (int e = lane; e < D * S; e += 32) {
+        const int i = e % D, c = e / D;
+        const int m = c == 0 ? 1 : c - 1, q = min(c + 1, S - 1);
+        const float a = tmp[i + m * D], b = tmp[i + c * D], d = tmp[i + q * D];
+        dst[i + 2 * c * D] = pyr_sample(3, a, b, d);
+        dst[i + (2 * c + 1) * D] = pyr_sample(2, b, b, d);
     }
     __syncwarp();
 }
@@ -2389,17 +2396,51 @@ __device__ void cone_step(const float* src, int lds, const ConeLevel& s, int n,
 
 __global__ void __launch_bounds__(kRefineWarps * 32) k_refine(const RefineArgs A) {
     extern __shared__ __align__(16) float rsm[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float* W = rsm + warp * A.warp_floats;
-    float* P0 = W;            // 5 x 5 (32)
-    float* L1 = W + 32;       // 10 x 10
-    float* L2 = L1 + 100;     // 20 x 20
-    float* WK = L2 + 400;     // level-3 materialisation, or bounds and cone buffers
-    const int64_t count = A.count ? static_cast<int64_t>(*A.count) : A.n_items;
+    // Level-3 rows (or columns) each final block row (or column) reaches, shared by the CTA.
+    __shared__ int s_rlo[64], s_rhi[64];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
     const int L = A.levels;
-
-    for (int64_t item = static_cast<int64_t>(blockIdx.x) * kRefineWarps + warp; item < count;
-         item += static_cast<int64_t>(gridDim.x) * kRefineWarps) {
+    float* W = rsm + warp * A.warp_floats;
+    // Per-warp layout. Up to 8x: the patch, levels 1 and 2, then the pyrUp scratch and level 3.
+    // Beyond: level 3 (1600 floats), then a scratch that first holds the patch, levels 1 and 2
+    // and the pyrUp temporaries, and after level 3 is built the block bounds, the level-3 row
+    // maxima and the cone buffers (regions that are never live at the same time overlap).
+    float *P0, *L1, *L2, *WK, *T5, *T10, *T20, *L3, *B;
+    if (L <= 3) {
+        P0 = W;
+        L1 = W + 32;
+        L2 = L1 + 100;
+        WK = L2 + 400;
+        T5 = T10 = T20 = WK;
+        L3 = WK + 800;
+        B = nullptr;
+    } else {
+        L3 = W;
+        B = W + 1600;
+        L2 = B;          // [0, 400)
+        T20 = B + 400;   // [400, 1200): the 40 x 20 vertical pass of level 3
+        T10 = B + 400;   // [400, 600)
+        L1 = B + 1000;   // [1000, 1100)
+        P0 = B + 1100;   // [1100, 1125)
+        T5 = B + 400;    // [400, 450)
+        WK = nullptr;
+        const int nb = (5 << L) / kFB;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+            int lo = b * kFB, hi = lo + kFB - 1;
+            for (int lev = L - 1; lev >= 3; --lev) {
+                int a2, b2;
+                tap_range(lo, hi, 5 << lev, a2, b2);
+                lo = a2;
+                hi = b2;
+            }
+            s_rlo[b] = lo;
+            s_rhi[b] = hi;
+        }
+        __syncthreads();
+    }
+    const int64_t count = A.count ? static_cast<int64_t>(*A.count) : A.n_items;
+    for (int64_t item = static_cast<int64_t>(blockIdx.x) * warps + warp; item < count;
+         item += static_cast<int64_t>(gridDim.x) * warps) {
         if (lane < 25) P0[lane] = A.patch[item * 25 + lane];
         __syncwarp();
         float bv = -INFINITY;
@@ -2410,15 +2451,14 @@ __global__ void __launch_bounds__(kRefineWarps * 32) k_refine(const RefineArgs A
             // Materialise every level; argmax of the last.
             const float* fin;
             if (L == 1) {
-                pyrup_warp<5>(P0, L1, WK);
+                pyrup_warp<5>(P0, L1, T5);
                 fin = L1;
             } else {
-                pyrup_warp<5>(P0, L1, WK);
-                pyrup_warp<10>(L1, L2, WK);
+                pyrup_warp<5>(P0, L1, T5);
+                pyrup_warp<10>(L1, L2, T10);
                 fin = L2;
                 if (L == 3) {
-                    float* L3 = WK + 800;
-                    pyrup_warp<20>(L2, L3, WK);
+                    pyrup_warp<20>(L2, L3, T20);
                     fin = L3;
                 }
             }
@@ -2430,14 +2470,13 @@ __global__ void __launch_bounds__(kRefineWarps * 32) k_refine(const RefineArgs A
             v0 = fin[0];
         } else {
             // Levels 1-3 materialised (level 3 is 40 x 40), then the block search above them.
-            float* L3 = WK;                   // 1600 floats
-            float* BND = WK + 1600;           // nb * nb bounds
             const int nb = nfinal / kFB;      // blocks per side
-            float* CB = BND + nb * nb;        // pyrUp scratch, row maxima, then cone buffers
+            float* BND = B;                   // nb * nb bounds (over level 2, once it is read)
+            float* CB = BND + nb * nb;        // row maxima, then cone buffers
             float* RM = CB;                   // level-3 row maxima per block column (40 * nb)
-            pyrup_warp<5>(P0, L1, CB);
-            pyrup_warp<10>(L1, L2, CB);
-            pyrup_warp<20>(L2, L3, CB);
+            pyrup_warp<5>(P0, L1, T5);
+            pyrup_warp<10>(L1, L2, T10);
+            pyrup_warp<20>(L2, L3, T20);
             // Scale of the rounding slack: the largest magnitude of level 2 bounds every later
             // level's (up to the growth of rounding itself, covered by the factor 2).
             float amax = 0.0f;
@@ -2455,36 +2494,33 @@ __global__ void __launch_bounds__(kRefineWarps * 32) k_refine(const RefineArgs A
                 toff[d] = off;
                 off += cap[d] * cap[d + 1];
             }
-            // Level-3 range of final-level rows (or columns) [16 b, 16 b + 15].
-            auto range3 = [&](int b, int& lo, int& hi) {
-                lo = b * kFB;
-                hi = lo + kFB - 1;
-                for (int lev = L - 1; lev >= 3; --lev) {
-                    int a2, b2;
-                    tap_range(lo, hi, 5 << lev, a2, b2);
-                    lo = a2;
-                    hi = b2;
-                }
-            };
-            __syncwarp();
+            __syncwarp();  // level 2 is read; its space takes the bounds
             // Loose bound of every final block: its level-3 cone maximum plus L - 3 levels of
-            // slack, as row maxima over each block column's range, then maxima over row ranges.
+            // slack, as row maxima over each block column's range (s_rlo/s_rhi), then maxima
+            // over row ranges.
             for (int e = lane; e < 40 * nb; e += 32) {
                 const int i = e % 40, bj_ = e / 40;
-                int c0, c1;
-                range3(bj_, c0, c1);
+                const int c0 = s_rlo[bj_], c1 = s_rhi[bj_];
                 float mx = -INFINITY;
                 for (int j = c0; j <= c1; ++j) mx = fmaxf(mx, L3[i + j * 40]);
                 RM[e] = mx;
             }
             __syncwarp();
-            for (int blk = lane; blk < nb * nb; blk += 32) {
-                const int bi_ = blk % nb, bj_ = blk / nb;
-                int r0, r1;
-                range3(bi_, r0, r1);
-                float mx = -INFINITY;
-                for (int i = r0; i <= r1; ++i) mx = fmaxf(mx, RM[i + bj_ * 40]);
-                BND[blk] = mx + slack(L - 3);
+            {
+                int bi_ = lane % nb, bj_ = lane / nb;  // block lane + 32 t, column-major
+                const int di = 32 % nb, dj = 32 / nb;
+                for (int blk = lane; blk < nb * nb; blk += 32) {
+                    const int r0 = s_rlo[bi_], r1 = s_rhi[bi_];
+                    float mx = -INFINITY;
+                    for (int i = r0; i <= r1; ++i) mx = fmaxf(mx, RM[i + bj_ * 40]);
+                    BND[blk] = mx + slack(L - 3);
+                    bi_ += di;
+                    bj_ += dj;
+                    if (bi_ >= nb) {
+                        bi_ -= nb;
+                        ++bj_;
+                    }
+                }
             }
             __syncwarp();
             while (true) {
@@ -2747,6 +2783,8 @@ int ilog2_exact(int up) {
 
 struct RefinePlan {
     int levels, warp_floats;
+    int warps;    // warps per CTA
+    int per_sm;   // CTAs per SM
     size_t smem;
 };
 
@@ -2756,20 +2794,37 @@ RefinePlan plan_refine(int up) {
     RefinePlan R{};
     R.levels = ilog2_exact(up);
     const int L = R.levels;
-    int wk;
     if (L <= 3) {
-        wk = 800 + 1600;
+        // The patch, levels 1 and 2, the pyrUp scratch (40 x 20) and level 3.
+        R.warp_floats = 32 + 100 + 400 + 800 + 1600;
     } else {
-        // Level 3, the block bounds, then the largest of the pyrUp scratch (40 x 20), the
-        // level-3 row maxima (40 per block column) and the cone buffers of levels 4 .. L.
+        // Level 3, then a scratch of the larger of the build phase (level 2 and the 40 x 20
+        // vertical pass, with the patch and level 1 inside) and the search phase (the block
+        // bounds, then the larger of the level-3 row maxima and the cone buffers of levels
+        // 4 .. L).
         const int nb = (5 << L) / kFB;
         const int cap[7] = {16, 10, 7, 6, 5, 5, 5};
         int cone = 0;
         for (int d = 0; d <= L - 4; ++d) cone += cap[d] * cap[d] + cap[d] * cap[d + 1];
-        wk = 1600 + nb * nb + std::max(std::max(800, 40 * nb), cone);
+        R.warp_floats = 1600 + std::max(1200, nb * nb + std::max(40 * nb, cone));
     }
-    R.warp_floats = 32 + 100 + 400 + wk;
-    R.smem = static_cast<size_t>(kRefineWarps) * R.warp_floats * sizeof(float);
+    // Warps per CTA for the most resident warps per SM (228 KB of shared memory, 1 KB charged
+    // per CTA): the kernel is issue-bound on dependent shared-memory arithmetic, so resident
+    // warps, not CTA size, hide its latencies.
+    const size_t per_warp = static_cast<size_t>(R.warp_floats) * sizeof(float);
+    int best_w = 1, best_sm = 0;
+    for (int w = 1; w <= kRefineWarps; ++w) {
+        const size_t cta = w * per_warp + 1024 + 2 * 64 * sizeof(int);
+        if (w * per_warp > static_cast<size_t>(kDynSmemCap)) break;
+        const int ctas = static_cast<int>(std::min<size_t>(32, (228 * 1024) / cta));
+        if (ctas * w >= best_w * best_sm) {
+            best_w = w;
+            best_sm = ctas;
+        }
+    }
+    R.warps = best_w;
+    R.per_sm = std::max(1, best_sm);
+    R.smem = static_cast<size_t>(R.warps) * per_warp;
     return R;
 }
 
@@ -3321,11 +3376,10 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
     if (R.smem > static_cast<size_t>(kDynSmemCap)) return cudaErrorInvalidValue;
     e = cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, kDynSmemCap);
     if (e != cudaSuccess) return e;
-    const int64_t rper_sm =
-        std::max<int64_t>(1, std::min<int64_t>(4, (227 * 1024) / (R.smem + 1024)));
     const int rgrid = static_cast<int>(std::max<int64_t>(
-        1, std::min<int64_t>((pts.n + kRefineWarps - 1) / kRefineWarps, num_sms * rper_sm)));
-    k_refine<<<rgrid, kRefineWarps * 32, R.smem, stream>>>(B);
+        1, std::min<int64_t>((pts.n + R.warps - 1) / R.warps,
+                             static_cast<int64_t>(num_sms) * R.per_sm)));
+    k_refine<<<rgrid, R.warps * 32, R.smem, stream>>>(B);
     e = cudaGetLastError();
     T.launches += 1;
     if (T.enabled) {
@@ -3367,11 +3421,10 @@ cudaError_t launch_refine_patches(const float* patches, int64_t count, int up, i
     cudaError_t e =
         cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, kDynSmemCap);
     if (e != cudaSuccess) return e;
-    const int64_t per_sm =
-        std::max<int64_t>(1, std::min<int64_t>(4, (227 * 1024) / (R.smem + 1024)));
     const int grid = static_cast<int>(std::max<int64_t>(
-        1, std::min<int64_t>((count + kRefineWarps - 1) / kRefineWarps, num_sms * per_sm)));
-    k_refine<<<grid, kRefineWarps * 32, R.smem, stream>>>(B);
+        1, std::min<int64_t>((count + R.warps - 1) / R.warps,
+                             static_cast<int64_t>(num_sms) * R.per_sm)));
+    k_refine<<<grid, R.warps * 32, R.smem, stream>>>(B);
     return cudaGetLastError();
 }
 
