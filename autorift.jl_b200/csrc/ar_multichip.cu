@@ -198,6 +198,70 @@ __device__ bool medmad(const float* A, int64_t nr, int64_t nc, int64_t i, int64_
     return true;
 }
 
+// Bitonic sort of 32 register values, ascending (every index is a compile-time constant once
+// the loops unroll, so the array stays in registers).
+__device__ __forceinline__ void bitonic32(float (&v)[32]) {
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1)
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const float a = v[i], b = v[l];
+                    const bool up = (i & k) == 0;
+                    v[i] = up ? fminf(a, b) : fmaxf(a, b);
+                    v[l] = up ? fmaxf(a, b) : fminf(a, b);
+                }
+            }
+}
+
+// smedian of the first n of 32 sorted register values (n >= 1), selected without indexing.
+__device__ __forceinline__ float smedian32(const float (&v)[32], int n) {
+    const int k0 = (n & 1) ? (n + 1) / 2 - 1 : n / 2 - 1, k1 = (n & 1) ? k0 : n / 2;
+    float a = 0.0f, b = 0.0f;
+#pragma unroll
+    for (int t = 0; t < 25; ++t) {
+        if (t == k0) a = v[t];
+        if (t == k1) b = v[t];
+    }
+    return (n & 1) ? a : __fdiv_rn(__fadd_rn(a, b), 2.0f);
+}
+
+// medmad for windows of at most 5 x 5: the values in registers, NaN and absent entries as +Inf
+// (they sort after every value, and only the first n are read), sorted by a network instead of
+// an insertion sort in local memory. Same median and MAD: both are order statistics of the
+// same multiset, and signed zeros only ever enter through differences and magnitudes.
+__device__ bool medmad25(const float* A, int64_t nr, int64_t nc, int64_t i, int64_t j, Win W,
+                         float* med, float* mad) {
+    float v[32];
+    int n = 0;
+#pragma unroll
+    for (int dj = 0; dj < 5; ++dj)
+#pragma unroll
+        for (int di = 0; di < 5; ++di) {
+            const int64_t jj = j - W.lx + dj, ii = i - W.ly + di;
+            const bool in = dj <= W.lx + W.rx && di <= W.ly + W.ry && jj >= 0 && jj < nc &&
+                            ii >= 0 && ii < nr;
+            const float x = in ? A[ii + jj * nr] : __int_as_float(0x7fc00000);
+            const bool ok = !isnan(x);
+            v[dj * 5 + di] = ok ? x : INFINITY;
+            n += ok ? 1 : 0;
+        }
+#pragma unroll
+    for (int t = 25; t < 32; ++t) v[t] = INFINITY;
+    if (n == 0) return false;
+    bitonic32(v);
+    const float m = smedian32(v, n);
+#pragma unroll
+    for (int t = 0; t < 32; ++t) v[t] = t < n ? fabsf(__fsub_rn(v[t], m)) : INFINITY;
+    bitonic32(v);
+    *med = m;
+    *mad = smedian32(v, n);
+    return true;
+}
+
 // Stage 2 of the Gardner filter (src/outliers.jl:139-158).
 __global__ void k_madtest(const float* nx, const float* ny, const int64_t* rx, const int64_t* ry,
                           int64_t nr, int64_t nc, Win W, int up, double scale, uint8_t* keep) {
@@ -205,8 +269,11 @@ __global__ void k_madtest(const float* nx, const float* ny, const int64_t* rx, c
     if (k >= nr * nc || !keep[k]) return;
     const int64_t i = k % nr, j = k / nr;
     float mx = qnan(), sx = qnan(), my = qnan(), sy = qnan();
-    const bool okx = medmad(nx, nr, nc, i, j, W, &mx, &sx);
-    const bool oky = medmad(ny, nr, nc, i, j, W, &my, &sy);
+    const bool small = W.lx + W.rx < 5 && W.ly + W.ry < 5;
+    const bool okx = small ? medmad25(nx, nr, nc, i, j, W, &mx, &sx)
+                           : medmad(nx, nr, nc, i, j, W, &mx, &sx);
+    const bool oky = small ? medmad25(ny, nr, nc, i, j, W, &my, &sy)
+                           : medmad(ny, nr, nc, i, j, W, &my, &sy);
     const double fx = rx[k] > 0 ? __ddiv_rn(2.0, static_cast<double>(up * rx[k])) : INFINITY;
     const double fy = ry[k] > 0 ? __ddiv_rn(2.0, static_cast<double>(up * ry[k])) : INFINITY;
     const double tolx = fmax(__dmul_rn(scale, static_cast<double>(sx)), fx);
