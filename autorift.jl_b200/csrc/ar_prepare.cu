@@ -322,15 +322,25 @@ __global__ void __launch_bounds__(kStatThreads) k_qstats(const T* img, const uin
     }
 }
 
-// Fixed-order combination of the block partials.
+// Fixed-order combination of the block partials: the block stages them in shared memory with
+// coalesced loads, then one thread merges them in block order (the merge chain is sequential,
+// so its operands must not wait on global memory).
 template <int PASS>
 __global__ void k_qfinal(QuantStats* st, int nblocks) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    __shared__ DD s_part[kStatBlocks];
+    __shared__ long long s_cnt[kStatBlocks];
+    if (blockIdx.x != 0) return;
+    for (int k = threadIdx.x; k < nblocks; k += blockDim.x) {
+        s_part[k] = st->part[k];
+        s_cnt[k] = st->cnt[k];
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
     DD a{0.0, 0.0};
     long long c = 0;
     for (int k = 0; k < nblocks; ++k) {
-        dd_merge(a, st->part[k]);
-        c += st->cnt[k];
+        dd_merge(a, s_part[k]);
+        c += s_cnt[k];
     }
     const double s = __dadd_rn(a.hi, a.lo);
     if (PASS == 0) {
@@ -383,9 +393,9 @@ template <typename T>
 cudaError_t quantize_u8(const T* img, const uint8_t* mask, int64_t n, QuantStats* st,
                         uint8_t* out, cudaStream_t s, long long* launches) {
     k_qstats<T, 0><<<kStatBlocks, kStatThreads, 0, s>>>(img, mask, n, st);
-    k_qfinal<0><<<1, 32, 0, s>>>(st, kStatBlocks);
+    k_qfinal<0><<<1, 256, 0, s>>>(st, kStatBlocks);
     k_qstats<T, 1><<<kStatBlocks, kStatThreads, 0, s>>>(img, mask, n, st);
-    k_qfinal<1><<<1, 32, 0, s>>>(st, kStatBlocks);
+    k_qfinal<1><<<1, 256, 0, s>>>(st, kStatBlocks);
     const int threads = 256;
     k_quantize<T><<<static_cast<unsigned>((n + threads - 1) / threads), threads, 0, s>>>(img, mask, n, st, out);
     *launches += 5;

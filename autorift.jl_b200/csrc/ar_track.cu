@@ -2365,26 +2365,29 @@ struct ConeLevel {
 // Level region `dst` (rows d.r0..d.r1, columns d.c0..d.c1) of a level computed from the source
 // region `s` of the level below (size n), stored column-major from its first element with
 // leading dimension lds; tmp holds the vertical pass (dst rows x source columns). Regions have
-// at most 16 rows: lanes 0-15 and 16-31 take alternate columns.
+// at most 16 rows: the warp splits into 32 / rows groups of `rows` lanes, each group taking
+// every (32 / rows)-th column.
 __device__ void cone_step(const float* src, int lds, const ConeLevel& s, int n,
                           const ConeLevel& d, float* tmp, float* dst) {
     const int lane = threadIdx.x & 31;
-    const int r = lane & 15, cpar = lane >> 4;
     const int rows = d.r1 - d.r0 + 1, scols = s.c1 - s.c0 + 1;
-    if (r < rows) {
+    const int groups = 32 / rows;
+    const int cpar = lane / rows, r = lane - cpar * rows;
+    const bool active = cpar < groups;
+    if (active) {
         int m, c, q;
         const int nt = taps(d.r0 + r, n, m, c, q);
         m -= s.r0;
         c -= s.r0;
         q -= s.r0;
-        for (int cc = cpar; cc < scols; cc += 2) {
+        for (int cc = cpar; cc < scols; cc += groups) {
             const float* col = src + cc * lds;
             tmp[r + cc * rows] = pyr_sample(nt, col[m], col[c], col[q]);
         }
     }
     __syncwarp();
-    if (r < rows) {
-        for (int cc = cpar; cc <= d.c1 - d.c0; cc += 2) {
+    if (active) {
+        for (int cc = cpar; cc <= d.c1 - d.c0; cc += groups) {
             int m, c, q;
             const int nt = taps(d.c0 + cc, n, m, c, q);
             dst[r + cc * rows] = pyr_sample(nt, tmp[r + (m - s.c0) * rows],
