@@ -157,6 +157,9 @@ struct ar_pair {
     uint8_t* ref_valid = nullptr;
     uint8_t* sec_valid = nullptr;
     uint8_t* valid = nullptr;  // ref_valid .& sec_valid
+    // Recorded on the context stream when the pair's contents are complete (the upload or the
+    // preparation is queued, not awaited); work on another stream waits for it.
+    cudaEvent_t ready = nullptr;
 };
 
 namespace {
@@ -342,6 +345,23 @@ void pair_free(ar_pair* p) {
     dfree(p->ctx, p->valid);
     p->ref = p->sec = nullptr;
     p->valid = p->ref_valid = p->sec_valid = nullptr;
+    if (p->ready) cudaEventDestroy(p->ready);
+    p->ready = nullptr;
+}
+
+// Marks the pair complete on the context stream (its upload or preparation queued there).
+cudaError_t pair_mark_ready(ar_ctx* c, ar_pair* p) {
+    if (!p->ready) {
+        cudaError_t e = cudaEventCreateWithFlags(&p->ready, cudaEventDisableTiming);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaEventRecord(p->ready, c->stream);
+}
+
+// Orders work about to be queued on `s` after the pair's contents are complete.
+cudaError_t pair_wait(ar_ctx* c, const ar_pair* p, cudaStream_t s) {
+    if (s == c->stream || !p->ready) return cudaSuccess;
+    return cudaStreamWaitEvent(s, p->ready, 0);
 }
 
 }  // namespace
@@ -461,7 +481,9 @@ int ar_pair_upload(ar_ctx* c, const void* ref, const void* sec, const uint8_t* r
             case AR_F32: e = launch_make_valid<float>(p, ref_valid != nullptr, sec_valid != nullptr, c->stream); break;
         }
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    // The caller's arrays are copied into the staging buffers by now; the transfers and the
+    // mask kernel complete in stream order (later calls on other streams wait for `ready`).
+    if (e == cudaSuccess) e = pair_mark_ready(c, p);
     if (e != cudaSuccess) {
         pair_free(p);
         delete p;
@@ -637,7 +659,9 @@ int track_device(ar_ctx* c, const ar_pair* p, const ar_points* pts, int up, int 
     ar::DevPoints dp{pts->x, pts->y, pts->radius_x, pts->radius_y, pts->dx_prior,
                      pts->dy_prior, pts->chip_size_x, pts->chip_size_y, n};
     ar::PassGeometry geom;
-    cudaError_t e = ar::pass_geometry_device(dp, p->nrows, p->ncols, c->scratch, s, &geom);
+    cudaError_t e = pair_wait(c, p, s);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ar_track_device: pair");
+    e = ar::pass_geometry_device(dp, p->nrows, p->ncols, c->scratch, s, &geom);
     if (e != cudaSuccess) return cuda_fail(c, e, "ar_track_device: pass geometry");
     ar::DevOutputs dout{dx, dy, corr, searched};
     std::string err;
@@ -814,7 +838,7 @@ int ar_prepare(ar_ctx* c, const ar_pair* raw, const ar_prepare_opts* opts, ar_pa
         e = cudaGetLastError();
     }
     dfree(c, tmp);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess) e = pair_mark_ready(c, p);
     if (e != cudaSuccess) {
         pair_free(p);
         delete p;
@@ -872,6 +896,8 @@ int multichip_run(ar_ctx* c, const ar_pair* p, const double* gx, const double* g
                   const int64_t* grx, const int64_t* gry, const double* gdx0, const double* gdy0,
                   int64_t gr, int64_t gc, const ar_multichip_params* prm, float* dx, float* dy,
                   float* corr, uint16_t* chip, uint8_t* interp, cudaStream_t s) {
+    const cudaError_t ew = pair_wait(c, p, s);
+    if (ew != cudaSuccess) return cuda_fail(c, ew, "ar_multichip: pair");
     // The search's scratch is kept by the context and grows from its pool in stream order on
     // `s` (no device-wide synchronisation, so the request loop's slots never stall one
     // another). Every call ends with its stream synchronised, so the scratch is idle when the

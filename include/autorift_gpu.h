@@ -73,7 +73,9 @@ int ar_last_error(const ar_ctx* ctx, char* buf, size_t size);
  * Upload an image pair (ImagePair, src/preprocess.jl:74-79). `ref` and `sec` are
  * nrows x ncols column-major arrays of `dtype`. `ref_valid`/`sec_valid` may be NULL, which
  * means finiteness for float types and all-valid for integer types, as ImagePair's default.
- * The pair keeps `valid(pair) = ref_valid .& sec_valid` (src/preprocess.jl:106).
+ * The pair keeps `valid(pair) = ref_valid .& sec_valid` (src/preprocess.jl:106). Returns once
+ * the caller's arrays have been copied out (they may be reused at once); the transfers finish
+ * in the background, ordered before every later use of the pair on any stream.
  */
 int ar_pair_upload(ar_ctx* ctx, const void* ref, const void* sec, const uint8_t* ref_valid,
                    const uint8_t* sec_valid, int64_t nrows, int64_t ncols, int dtype,
@@ -95,7 +97,9 @@ typedef struct {
  * `_prepare(pair, p)` (src/api.jl:305-311): preprocess then quantize each image of `raw`
  * (src/preprocess.jl:131-160, 275-460, 477-592) into a new device pair. The result's element
  * type is UInt8 under AR_QUANT_UINT8, Float32 when a filter ran without quantisation, else the
- * input type; its masks are the filtered (eroded) masks. `raw` is unchanged.
+ * input type; its masks are the filtered (eroded) masks. `raw` is unchanged. Returns once the
+ * work is queued on the context's stream; every later use of the new pair, on any stream, is
+ * ordered after it (ar_synchronize waits for it).
  */
 int ar_prepare(ar_ctx* ctx, const ar_pair* raw, const ar_prepare_opts* opts, ar_pair** out);
 
