@@ -256,3 +256,44 @@ def test_empty_and_unsearchable_sets(ar, gpu_lib):
     pts = ar.pointset([50.0, 60.0], [50.0, 60.0], search_radius=0)
     d = ar.track(pair, pts)
     assert not d.searched.any() and np.isnan(d.dx).all()
+
+
+def test_pair_ready_orders_other_streams(ar, gpu_lib):
+    """ar_pair_upload and ar_prepare return once queued; a track on another stream right after
+    them must still see the complete pair (the pair's ready event orders it)."""
+    import ctypes
+
+    import torch
+    L = ar._lib
+    ctx = L.Context(0)
+    lib = ctx.lib
+    a, b = ar.synthetic.shifted_pair(1024, (3.2, -1.7), seed=8, dtype=np.uint16)
+    pts = ar.gridpoints(a.shape, 16, chip_size=32, search_radius=12)
+    p = ar.params()
+    want = ar.track(ar.prepare(ar.ImagePair(a, b), p, ctx), pts, p, ctx=ctx)
+    from autorift_b200.points import FIELDS
+    dev = torch.device("cuda", 0)
+    side = torch.cuda.Stream(device=dev)
+    cols = {f: torch.from_numpy(pts.flat(f)).to(dev) for f in FIELDS}
+    torch.cuda.synchronize()
+    st = L.ArPoints(*(cols[f].data_ptr() for f in FIELDS), len(pts))
+    n = len(pts)
+    outs = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3)]
+    srch = torch.empty(n, dtype=torch.uint8, device=dev)
+    fa, fb = np.asfortranarray(a), np.asfortranarray(b)
+    for _ in range(3):
+        raw, prep = ctypes.c_void_p(), ctypes.c_void_p()
+        ctx.check(lib.ar_pair_upload(ctx.handle, fa.ctypes.data, fb.ctypes.data, None, None,
+                                     a.shape[0], a.shape[1], L.AR_U16, ctypes.byref(raw)))
+        ctx.check(lib.ar_prepare(ctx.handle, raw, ctypes.byref(ar.prepare_options(p)),
+                                 ctypes.byref(prep)))
+        lib.ar_pair_destroy(raw)
+        ctx.check(lib.ar_track_device(ctx.handle, prep, ctypes.byref(st), 64, L.AR_ZNCC,
+                                      *(o.data_ptr() for o in outs), srch.data_ptr(),
+                                      ctypes.c_void_p(side.cuda_stream)))
+        side.synchronize()
+        lib.ar_pair_destroy(prep)
+        for got, w in zip(outs, (want.dx, want.dy, want.correlation)):
+            assert np.array_equal(got.cpu().numpy().view(np.uint32),
+                                  w.ravel(order="F").view(np.uint32))
+    ctx.close()
