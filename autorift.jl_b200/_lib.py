@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import ctypes
 import threading
+import weakref
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -151,6 +152,9 @@ class Context:
             raise ArError(rc, f"ar_ctx_create(device={device}) failed: no usable CUDA device")
         self.handle = h
         self.device = int(device)
+        # Device pairs of this context, released before it is destroyed (a pair cannot outlive
+        # its context's memory pool).
+        self._pairs = weakref.WeakSet()
 
     def check(self, rc: int):
         if rc != AR_OK:
@@ -181,6 +185,8 @@ class Context:
 
     def close(self):
         if getattr(self, "handle", None):
+            for pair in list(getattr(self, "_pairs", ())):
+                pair.release()
             self.lib.ar_ctx_destroy(self.handle)
             self.handle = None
 

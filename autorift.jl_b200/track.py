@@ -122,6 +122,13 @@ class _DevicePair:
     def __init__(self, ctx, handle):
         self.ctx = ctx
         self.handle = handle
+        ctx._pairs.add(self)
+
+    def release(self):
+        """Destroy the device pair (idempotent; a closed context already freed it)."""
+        if self.handle and getattr(self.ctx, "handle", None):
+            self.ctx.lib.ar_pair_destroy(self.handle)
+        self.handle = None
 
     def info(self):
         dt = ctypes.c_int()
@@ -133,9 +140,7 @@ class _DevicePair:
 
     def __del__(self):
         try:
-            if self.handle:
-                self.ctx.lib.ar_pair_destroy(self.handle)
-                self.handle = None
+            self.release()
         except Exception:
             pass
 

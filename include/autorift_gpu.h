@@ -64,6 +64,7 @@ int ar_version(void);
 /* Create a context on `device` (a CUDA ordinal). Replaces the reference's process-wide FFT
  * plan cache and workspace pools (src/plans.jl:25-47, src/correlate.jl:294-350). */
 int ar_ctx_create(int device, ar_ctx** out);
+/* Destroy a context. Its pairs live in its memory pool: destroy them first. */
 int ar_ctx_destroy(ar_ctx* ctx);
 
 /* Copy the last error message of `ctx` (NUL-terminated, truncated to `size`). */
