@@ -42,7 +42,8 @@ class ArMultichipParams(ctypes.Structure):
                 ("measure", _i32), ("outliers", _i32), ("outlier_window", _i32),
                 ("outlier_iterations", _i32), ("min_agree_fraction", ctypes.c_double),
                 ("agree_tolerance", ctypes.c_double), ("mad_scale", ctypes.c_double),
-                ("fill_window", _i32), ("rotation_count", _i32), ("rotation_angles", _p)]
+                ("fill_window", _i32), ("rotation_count", _i32), ("rotation_angles", _p),
+                ("level_measure_count", _i32), ("level_measures", _i32 * 8)]
 
 
 class ArPoints(ctypes.Structure):

@@ -49,13 +49,16 @@ def multichip_params(p: Params) -> "_lib.ArMultichipParams":
     if len(p.similarity) > len(chip_sizes(p)):
         raise ValueError(f"`similarity` names {len(p.similarity)} measures but there are only "
                          f"{len(chip_sizes(p))} chip-size levels.")
-    if len({type(m) for m in p.similarity}) > 1:
-        raise ValueError("per-level similarity tuples are not supported on the GPU")
+    levels = [_measure_code(m) for m in p.similarity]  # measure_at (src/types.jl:893-894)
     prm = _lib.ArMultichipParams(
         p.chip_size_base, p.chip_size_min, p.chip_size_max, p.chip_aspect,
         p.min_search_radius, p.coarse_stride, p.coarse_buffer, p.min_coarse_valid_fraction,
         upsampling(p.subpixel), _measure_code(p.similarity[0]), kind, w, it, fr, tol, mad,
         p.fill_window)
+    if len(levels) > 1:
+        prm.level_measure_count = len(levels)
+        for i, m in enumerate(levels):
+            prm.level_measures[i] = m
     rot = rotation_angles(p)
     if rot is not None:
         prm.rotation_count = rot.size

@@ -887,6 +887,16 @@ int check_multichip_args(ar_ctx* c, const ar_pair* p, const ar_points* grid, int
         if (!ar::make_rotation(prm->rotation_angles, prm->rotation_count, &rot, &err))
             return fail(c, AR_ERR_ARG, err);
     }
+    if (prm->level_measure_count < 0 || prm->level_measure_count > 8)
+        return fail(c, AR_ERR_ARG, "level_measure_count must be in [0, 8]");
+    int levels = 0;
+    for (int64_t cs = prm->chip_size_base; cs <= prm->chip_size_max; cs *= 2)
+        if (cs >= prm->chip_size_min) ++levels;
+    if (prm->level_measure_count > levels)
+        return fail(c, AR_ERR_ARG, "more per-level measures than chip-size levels");
+    for (int i = 0; i < prm->level_measure_count; ++i)
+        if (prm->level_measures[i] != AR_ZNCC && prm->level_measures[i] != AR_NCC)
+            return fail(c, AR_ERR_ARG, "unknown per-level measure");
     return AR_OK;
 }
 
@@ -953,6 +963,9 @@ int multichip_run(ar_ctx* c, const ar_pair* p, const double* gx, const double* g
     P.fill_window = prm->fill_window;
     if (prm->rotation_count != 0)
         ar::make_rotation(prm->rotation_angles, prm->rotation_count, &P.rot, nullptr);
+    P.n_level_measures = prm->level_measure_count;
+    for (int i = 0; i < 8; ++i)
+        P.level_measures[i] = i < prm->level_measure_count ? prm->level_measures[i] : prm->measure;
     J.arena = arena;
     J.arena_bytes = ab;
     std::string err;

@@ -150,6 +150,8 @@ struct MultichipParams {
     double gfrac, gtol, gmad;
     int64_t fill_window;
     Rotation rot;  // the rotation search of every track pass (count 0: none)
+    int n_level_measures;  // 0: `measure` at every level
+    int level_measures[8];  // measure_at(p, k) = level_measures[min(k, n) - 1]
 };
 
 // One multichip run: a prepared pair, a gr x gc point grid (device, column-major), outputs

@@ -608,6 +608,9 @@ cudaError_t run_multichip(const MultichipJob& J, TrackScratch& scratch, int num_
         }
     };
 
+    // The level's similarity measure (measure_at, src/types.jl:893-894), set per level below.
+    int level_measure = P.measure;
+
     // A track pass over the searchable points of P only, results scattered back into O.
     auto track_searchable = [&](const DevPoints& P, const DevOutputs& O, int up) {
         k_unmeasured<<<blocks(P.n), kT, 0, s>>>(O, P.n);
@@ -626,7 +629,7 @@ cudaError_t run_multichip(const MultichipJob& J, TrackScratch& scratch, int num_
         err = pass_geometry_device(cp, J.nrows, J.ncols, scratch, s, &g);
         if (err == cudaSuccess)
             err = launch_track(J.dtype, J.ref, J.sec, J.valid, J.nrows, J.ncols, cp, g, up,
-                               J.P.measure, co, scratch, num_sms, s, errmsg, nullptr,
+                               level_measure, co, scratch, num_sms, s, errmsg, nullptr,
                                J.P.rot.count > 0 ? &J.P.rot : nullptr);
         if (err != cudaSuccess) return;
         k_scatter_outputs<<<blocks(ns), kT, 0, s>>>(kidx, ns, co, O);
@@ -637,8 +640,13 @@ cudaError_t run_multichip(const MultichipJob& J, TrackScratch& scratch, int num_
     for (int64_t cs = P.chip_base; cs <= P.chip_max; cs *= 2)
         if (cs >= P.chip_min) sizes.push_back(cs);
     unsigned long long unresolved = static_cast<unsigned long long>(n);
-    for (int64_t cs : sizes) {
+    for (size_t li = 0; li < sizes.size(); ++li) {
+        const int64_t cs = sizes[li];
         if (unresolved == 0) break;  // any(wanted) || break (src/multichip.jl:130-131)
+        level_measure = P.n_level_measures > 0
+                            ? P.level_measures[std::min(static_cast<int>(li),
+                                                        P.n_level_measures - 1)]
+                            : P.measure;
         const int64_t lcsx = cs;
         const int64_t lcsy = 2 * static_cast<int64_t>(std::nearbyint(static_cast<double>(cs) * P.aspect / 2.0));
         C.zero();

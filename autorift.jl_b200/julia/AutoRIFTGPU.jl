@@ -68,6 +68,8 @@ struct ArMultichipParams
     fill_window::Cint
     rotation_count::Cint              # 0: NoRotationSearch
     rotation_angles::Ptr{Float64}     # AutoRIFT.angles(p.rotation), read during the call
+    level_measure_count::Cint         # 0: `measure` at every level
+    level_measures::NTuple{8,Cint}    # measure_at(p, k) for a `similarity` tuple
 end
 
 # The chip rotations of a rotation method (src/types.jl:577), as the C ABI takes them.
@@ -252,7 +254,9 @@ function multichip_params(p::Params, angs::Vector{Float64})
                       p.min_search_radius, p.coarse_stride, p.coarse_buffer,
                       p.min_coarse_valid_fraction, upsampling(p.subpixel),
                       measure_code(first(p.similarity)), o[1], o[2], o[3], o[4], o[5], o[6],
-                      p.fill_window, length(angs), isempty(angs) ? C_NULL : pointer(angs))
+                      p.fill_window, length(angs), isempty(angs) ? C_NULL : pointer(angs),
+                      length(p.similarity) > 1 ? length(p.similarity) : 0,
+                      ntuple(k -> measure_code(p.similarity[min(k, length(p.similarity))]), 8))
 end
 
 # The eight PointSet fields flattened, kept alive by the returned tuple.

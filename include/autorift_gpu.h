@@ -196,6 +196,11 @@ typedef struct {
      * distinct angles. The array is read during the call (ar_submit copies it). */
     int rotation_count;
     const double* rotation_angles;
+    /* Per-level similarity (a `similarity` tuple; measure_at, src/types.jl:893-894): level k
+     * (1 = finest) uses level_measures[min(k, count) - 1], AR_ZNCC or AR_NCC; count 0 uses
+     * `measure` at every level. At most 8 entries, no more than the chip-size levels. */
+    int level_measure_count;
+    int level_measures[8];
 } ar_multichip_params;
 
 /*

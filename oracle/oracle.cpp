@@ -751,6 +751,8 @@ struct MCParams {
     int64_t fill_window;
     const double* angles;  // RotationSearch chip rotations (degrees), nang of them; 0: none
     int nang;
+    int nlev;     // per-level measures (measure_at, src/types.jl:893-894); 0: `measure` always
+    int lev[8];
 };
 
 // src/window.jl:565-582.
@@ -944,10 +946,14 @@ void multichip(const MCImages<T>& I, const double* gx, const double* gy, const i
     std::vector<int64_t> sizes;
     for (int64_t cs = P.chip_base; cs <= P.chip_max; cs *= 2)
         if (cs >= P.chip_min) sizes.push_back(cs);
-    for (int64_t cs : sizes) {
+    for (size_t li = 0; li < sizes.size(); ++li) {
+        const int64_t cs = sizes[li];
         bool any = false;
         for (int64_t i = 0; i < n; ++i) any = any || rcs[i] == 0;
         if (!any) break;
+        // measure_at(p, k) (src/types.jl:893-894): the level's entry, the last one repeating.
+        const int measure =
+            P.nlev > 0 ? P.lev[std::min(static_cast<int>(li), P.nlev - 1)] : P.measure;
         const int64_t csx = cs;
         const int64_t csy = 2 * static_cast<int64_t>(std::nearbyint(static_cast<double>(cs) * P.aspect / 2.0));
         // _level_points (src/multichip.jl:193-213) with sanitize! (src/points.jl:332-346).
@@ -992,7 +998,7 @@ void multichip(const MCImages<T>& I, const double* gx, const double* gy, const i
                     std::vector<float> cdx(m), cdy(m), ccor(m);
                     std::vector<uint8_t> cs_(m), measured(m), keep(m), grown(m);
                     run_track(I, cx.data(), cy.data(), crx.data(), cry.data(), cdx0.data(), cdy0.data(),
-                              ccsx.data(), ccsy.data(), m, 1, P.measure, cdx.data(), cdy.data(),
+                              ccsx.data(), ccsy.data(), m, 1, measure, cdx.data(), cdy.data(),
                               ccor.data(), cs_.data(), nthreads, P.angles, P.nang);
                     bool anym = false;
                     for (int64_t k = 0; k < m; ++k) { measured[k] = !std::isnan(cdx[k]); anym = anym || measured[k]; }
@@ -1027,7 +1033,7 @@ void multichip(const MCImages<T>& I, const double* gx, const double* gy, const i
         std::vector<float> fdx(n), fdy(n), fc(n);
         std::vector<uint8_t> fs(n), measured(n), keep(n), filled(n, 0);
         run_track(I, gx, gy, rx.data(), ry.data(), gdx0, gdy0, vcsx.data(), vcsy.data(), n, P.up,
-                  P.measure, fdx.data(), fdy.data(), fc.data(), fs.data(), nthreads, P.angles,
+                  measure, fdx.data(), fdy.data(), fc.data(), fs.data(), nthreads, P.angles,
                   P.nang);
         // _reject_and_fill! (src/multichip.jl:318-330).
         for (int64_t i = 0; i < n; ++i) measured[i] = !std::isnan(fdx[i]);
@@ -1166,7 +1172,8 @@ int or_prepare(const void* img, const uint8_t* mask, int64_t nrows, int64_t ncol
 // correlate_multichip (src/multichip.jl:106-137) over a gridded point set of gr x gc points
 // (column-major fields). params (doubles): chip_base, chip_min, chip_max, aspect, min_radius,
 // stride, buffer, min_frac, up, measure, outliers, window, iterations, min_agree_fraction,
-// agree_tolerance, mad_scale, fill_window. `angles`, `nang`: the rotation search, as or_track.
+// agree_tolerance, mad_scale, fill_window, the per-level measure count and 8 per-level
+// measures. `angles`, `nang`: the rotation search, as or_track.
 int or_multichip(const void* ref, const void* sec, const uint8_t* refv, const uint8_t* secv,
                  int64_t nrows, int64_t ncols, int dtype, const double* gx, const double* gy,
                  const int64_t* grx, const int64_t* gry, const double* gdx0, const double* gdy0,
@@ -1193,6 +1200,8 @@ int or_multichip(const void* ref, const void* sec, const uint8_t* refv, const ui
     P.gtol = prm[14];
     P.gmad = prm[15];
     P.fill_window = static_cast<int64_t>(prm[16]);
+    P.nlev = static_cast<int>(prm[17]);
+    for (int i = 0; i < 8; ++i) P.lev[i] = static_cast<int>(prm[18 + i]);
     auto run = [&](auto* r, auto* s) {
         using T = std::remove_const_t<std::remove_pointer_t<decltype(r)>>;
         MCImages<T> I{r, s, refv, secv, nrows, ncols};

@@ -218,7 +218,8 @@ def multichip(reference, secondary, grid, params: dict, reference_valid=None,
 
     ``grid`` maps the PointSet fields to (gr, gc) arrays; ``params`` holds chip_base, chip_min,
     chip_max, aspect, min_radius, stride, buffer, min_frac, up, measure (0/1), outliers (0/1),
-    window, iterations, min_agree_fraction, agree_tolerance, mad_scale, fill_window.
+    window, iterations, min_agree_fraction, agree_tolerance, mad_scale, fill_window, and
+    optionally ``level_measures`` (0/1 per chip-size level, the last repeating).
     ``angles`` turns on the rotation search at every level, as in ``track``.
     Returns (dx, dy, correlation, chip_size, interpolated) as (gr, gc) arrays.
     """
@@ -239,7 +240,11 @@ def multichip(reference, secondary, grid, params: dict, reference_valid=None,
     keys = ["chip_base", "chip_min", "chip_max", "aspect", "min_radius", "stride", "buffer",
             "min_frac", "up", "measure", "outliers", "window", "iterations",
             "min_agree_fraction", "agree_tolerance", "mad_scale", "fill_window"]
-    prm = np.array([float(params[k]) for k in keys], dtype=np.float64)
+    lev = list(params.get("level_measures", ()))
+    if len(lev) > 8:
+        raise ValueError("at most 8 per-level measures")
+    prm = np.array([float(params[k]) for k in keys] + [float(len(lev))]
+                   + [float(v) for v in lev] + [0.0] * (8 - len(lev)), dtype=np.float64)
     cols = [fld("x", np.float64), fld("y", np.float64), fld("radius_x", np.int64),
             fld("radius_y", np.int64), fld("dx_prior", np.float64), fld("dy_prior", np.float64)]
     n = gr * gc

@@ -99,3 +99,20 @@ def test_scattered_points_run_one_scale(ar, gpu_lib):
                       search_radius=25)
     d = ar.autorift(ref, sec, pts, preprocess="none", quantize="none")
     assert d.dx.shape == (4,) and np.all(np.abs(-d.dx - 3) <= 0.05)
+
+
+def test_per_level_similarity(ar, O, gpu_lib):
+    """A `similarity` tuple: level k uses its k-th measure, the last repeating (measure_at,
+    src/types.jl:893-894) -- the coarse and fine passes of each level alike. The banded scene
+    leaves points to the coarser levels."""
+    ref, sec = banded_pair(ar, 512, (6, -4), slice(199, 290))
+    ref8 = np.round(ref * 255).astype(np.uint8)
+    sec8 = np.round(sec * 255).astype(np.uint8)
+    grid = ar.gridpoints((512, 512), 16, chip_size=32, search_radius=25)
+    for sim in (("zncc", "ncc"), ("ncc", "zncc", "ncc"), ("ncc", "zncc")):
+        p = ar.params(chip_size=32, chip_size_max=128, preprocess="none", quantize="none",
+                      similarity=sim)
+        got = ar.correlate_multichip(ar.ImagePair(ref8, sec8), grid, p)
+        want = O.multichip(ref8, sec8, fields(grid), mc_params(ar, p))
+        check_identical(got, want)
+        assert (got.chip_size > 32).any()  # the later levels ran

@@ -82,3 +82,14 @@ def test_decimation_copies(ar):
     coarse = pts[3::4, 3::4]
     coarse.radius_x[:] = 0
     assert np.all(pts.radius_x == 25)
+
+
+def test_per_level_similarity_params(ar):
+    prm = ar.multichip_params(ar.params(similarity=("zncc", "ncc")))
+    assert prm.level_measure_count == 2 and list(prm.level_measures)[:2] == [0, 1]
+    assert ar.multichip_params(ar.params()).level_measure_count == 0
+    assert ar.multichip_params(ar.params(similarity=("ncc",))).measure == 1
+    with pytest.raises(ValueError):
+        ar.multichip_params(ar.params(similarity=("zncc", "ncc", "zncc", "ncc")))
+    with pytest.raises(ValueError):
+        ar.multichip_params(ar.params(similarity=("zncc", "coherence")))

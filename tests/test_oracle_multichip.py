@@ -14,11 +14,15 @@ def mc_params(ar, p):
     return dict(chip_base=p.chip_size_base, chip_min=p.chip_size_min, chip_max=p.chip_size_max,
                 aspect=p.chip_aspect, min_radius=p.min_search_radius, stride=p.coarse_stride,
                 buffer=p.coarse_buffer, min_frac=p.min_coarse_valid_fraction,
-                up=ar.upsampling(p.subpixel), measure=0, outliers=1 if g else 0,
+                up=ar.upsampling(p.subpixel),
+                measure=1 if type(p.similarity[0]).__name__ == "NCC" else 0,
+                outliers=1 if g else 0,
                 window=o.window if g else 5, iterations=o.iterations if g else 3,
                 min_agree_fraction=o.min_agree_fraction if g else 0.32,
                 agree_tolerance=o.agree_tolerance if g else 0.2,
-                mad_scale=o.mad_scale if g else 4.0, fill_window=p.fill_window)
+                mad_scale=o.mad_scale if g else 4.0, fill_window=p.fill_window,
+                level_measures=[1 if type(m).__name__ == "NCC" else 0 for m in p.similarity]
+                if len(p.similarity) > 1 else [])
 
 
 def coherent_field(n, outliers=()):
