@@ -5,7 +5,8 @@ Loaded under the module name ``autorift_b200`` (the directory name is not an ide
 """
 
 from . import _lib, synthetic
-from .methods import (GardnerFilter, Highpass, NCC, NoOutlierFilter, NoPreprocess, NoQuantize,
+from .methods import (Coherence, GardnerFilter, Highpass, NCC, NoOutlierFilter, NoPreprocess,
+                      NoQuantize,
                       NoRefine, NoRotationSearch, Params, PyramidRefine, QuantizeUInt8,
                       RotationSearch, Wallis, ZNCC, angles, chip_sizes, params, upsampling)
 from .points import (PointSet, gridpoints, gridpoints_xy, nsearchable, npoints, pointset,
@@ -23,5 +24,5 @@ __all__ = [
     "nmeasured", "refine_patches", "track", "PreparedPair", "prepare", "Cache",
     "MultichipResult", "autorift", "autorift_", "build_grid", "correlate_multichip", "init",
     "reinit_", "prepare_options", "multichip_params", "submit", "Ticket", "NoRotationSearch",
-    "RotationSearch", "angles",
+    "RotationSearch", "angles", "Coherence",
 ]
