@@ -234,7 +234,9 @@ int ar_multichip_device(ar_ctx* ctx, const ar_pair* pair, const ar_points* grid_
  * adding into accumulator columns [s * dstep, s * dstep + N) of a cleared accumulator. `d_out`
  * receives the accumulator as 128 Tensor Memory lanes x (N + (nk - 1) * dstep) columns (int32,
  * lane-major) for mode 0; for mode 1, row (32 w + t) holds the 16 registers thread t of warp w
- * reads with the 16x256b.x4 pattern from its quarter's first 16 lanes, columns 0..31.
+ * reads with the 16x256b.x4 pattern from its quarter's first 16 lanes, columns 0..31; mode 2
+ * issues no product, so the kernel's bounded completion wait runs out and the call returns
+ * AR_ERR_TIMEOUT with the context still usable (the failure path every tensor-core wait takes).
  * Descriptors that would read outside an image are rejected. It validates on a device the
  * operand and accumulator layouts the correlation kernel uses; no reference counterpart.
  */

@@ -122,3 +122,25 @@ def test_out_of_image_descriptor_rejected(ar, gpu_lib):
     B = np.zeros(64 * 32, np.uint8)
     with pytest.raises(ar._lib.ArError):
         run(ar, A, B, [16, 64 * 16, 128, 0, 0, 64 * 16, 128, 0, 64, 64, 1])
+
+
+def test_bounded_wait_runs_out_and_context_survives(ar, gpu_lib):
+    """Failure detection without a fault: a product that is never issued leaves the kernel's
+    bounded completion wait to run out; the call reports AR_ERR_TIMEOUT, the kernel returns
+    normally, and the same context then computes correctly."""
+    ctx = ar._lib.default_context()
+    rng = np.random.default_rng(0)
+    A = rng.integers(0, 256, (64, 32), dtype=np.uint8)
+    B = rng.integers(0, 256, (16, 32), dtype=np.uint8)
+    a, b = planes(A), planes(B)
+    prm = (ctypes.c_int * 13)(0, 64 * 16, 128, 0, 0, 16 * 16, 128, 0, 64, 16, 1, 0, 2)
+    out = np.zeros((128, 16), np.int32)
+    rc = ctx.lib.ar_tc_selftest(ctx.handle, a.ctypes.data, a.size, b.ctypes.data, b.size, prm,
+                                out.ctypes.data)
+    assert rc == 4  # AR_ERR_TIMEOUT
+    D = run(ar, a, b, [0, 64 * 16, 128, 0, 0, 16 * 16, 128, 0, 64, 16, 1])
+    assert np.array_equal(lanes(D, 64)[:, :16], A.astype(np.int64) @ B.astype(np.int64).T)
+    ref, sec = ar.synthetic.shifted_pair(128, (2, 1), dtype=np.uint8)
+    d = ar.track(ar.ImagePair(ref, sec), ar.gridpoints(ref.shape, 32, chip_size=16,
+                                                        search_radius=6))
+    assert np.isfinite(d.dx).all()
