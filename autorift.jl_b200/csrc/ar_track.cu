@@ -213,10 +213,6 @@ template <>
 __device__ __forceinline__ uint32_t ph_of<uint32_t>(float w) {
     return static_cast<uint32_t>(w);
 }
-template <>
-__device__ __forceinline__ double ph_of<double>(float w) {
-    return static_cast<double>(w);
-}
 
 // _rotate_chip (src/track.jl:377-409) at 0-based chip element (a, b) of a ch x cw chip whose
 // first element is image element (chip_r, chip_c): the source point by the inverse rotation
