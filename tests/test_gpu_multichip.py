@@ -45,6 +45,39 @@ def test_default_pipeline_identical_to_oracle(ar, O, gpu_lib):
     assert np.isfinite(got.dx).mean() > 0.8
 
 
+@pytest.mark.parametrize("kind", ["int16_highpass", "float32_wallis"])
+def test_other_input_types_default_pipeline(ar, O, gpu_lib, kind):
+    """Int16 imagery (highpass) and Float32 imagery (Wallis), quantised to UInt8, through the
+    multichip search: the GPU-prepared pair agrees with the oracle's preparation to within the
+    quantiser's rounding-boundary allowance, and the multichip search on that prepared pair is
+    identical to the oracle's."""
+    a, b, sv = u16_scene(ar, n=512, seed=13)
+    if kind == "int16_highpass":
+        a = (a.astype(np.int32) - 32768).astype(np.int16)
+        b = (b.astype(np.int32) - 32768).astype(np.int16)
+        p = ar.params(grid_spacing=8)
+        pre = "highpass"
+    else:
+        a = a.astype(np.float32) / 65535
+        b = b.astype(np.float32) / 65535
+        p = ar.params(grid_spacing=8, preprocess="wallis")
+        pre = "wallis"
+    prep = ar.prepare(ar.ImagePair(a, b, None, sv), p)
+    ref, sec, rv, svv = prep.download()
+    assert ref.dtype == np.uint8
+    allow = 2 if kind == "int16_highpass" else a.size // 1000
+    for img, mask, g, gm in ((a, None, ref, rv), (b, sv, sec, svv)):
+        w, wm = O.prepare(img, mask, pre, 5)
+        assert np.array_equal(gm, wm)
+        d = np.abs(g.astype(np.int32) - w.astype(np.int32))
+        assert d.max() <= 1 and np.count_nonzero(d) <= allow
+    grid = ar.build_grid(a.shape, p)
+    got = ar.correlate_multichip(prep, grid, p)
+    want = O.multichip(ref, sec, fields(grid), mc_params(ar, p), rv, svv)
+    check_identical(got, want)
+    assert np.isfinite(got.dx).mean() > 0.8
+
+
 def test_multilevel_banded_scene(ar, O, gpu_lib):
     ref, sec = banded_pair(ar, 512, (6, -4), slice(199, 290))
     ref8 = np.round(ref * 255).astype(np.uint8)
