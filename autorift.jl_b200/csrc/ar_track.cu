@@ -1936,11 +1936,12 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
                 }
                 // Column sums of the new rows i in [nr - sh, nr): an item is a window column and
                 // up to 4 consecutive rows; its first sum from 4-byte groups (dp4a), then a
-                // sliding update.
+                // sliding update. The row groups of a column are adjacent lanes: their words lie
+                // in different banks of the column's 16-byte block.
                 const int i0 = nr - sh;
                 const int nparts = (sh + 3) >> 2;
                 for (int item = tid; item < XW * nparts; item += kBT) {
-                    const int pt = item / XW, x = item - pt * XW;
+                    const int x = item / nparts, pt = item - x * nparts;
                     const int ia = i0 + 4 * pt, ie = min(ia + 4, nr);
                     const uint8_t* colx = s_W + x * 16;
                     // Rows r .. r + 3 of column x as one word (a group may cross a block).
@@ -1997,14 +1998,29 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
                         g1 += r1[j0 + bb];
                         g2 += r2[j0 + bb];
                     }
+                    // Outgoing and incoming columns as 16-byte loads (rows stay inside XV).
+                    const uint4 o1 = *reinterpret_cast<const uint4*>(r1 + j0);
+                    const uint4 o2 = *reinterpret_cast<const uint4*>(r2 + j0);
+                    uint4 i1, i2;
+                    if ((cw & 3) == 0) {
+                        i1 = *reinterpret_cast<const uint4*>(r1 + j0 + cw);
+                        i2 = *reinterpret_cast<const uint4*>(r2 + j0 + cw);
+                    } else {
+                        const uint32_t* p1 = r1 + j0 + cw;
+                        const uint32_t* p2 = r2 + j0 + cw;
+                        i1 = make_uint4(p1[0], p1[1], p1[2], p1[3]);
+                        i2 = make_uint4(p2[0], p2[1], p2[2], p2[3]);
+                    }
+                    const uint32_t oo1[4] = {o1.x, o1.y, o1.z, o1.w}, ii1[4] = {i1.x, i1.y, i1.z, i1.w};
+                    const uint32_t oo2[4] = {o2.x, o2.y, o2.z, o2.w}, ii2[4] = {i2.x, i2.y, i2.z, i2.w};
 #pragma unroll
                     for (int m = 0; m < 4; ++m) {
                         const int j = j0 + m;
                         if (j < nc) {
                             s_S1[j * A.NRS + i] = g1;
                             s_S2[j * A.NRS + i] = g2;
-                            g1 = g1 + r1[j + cw] - r1[j];
-                            g2 = g2 + r2[j + cw] - r2[j];
+                            g1 = g1 + ii1[m] - oo1[m];
+                            g2 = g2 + ii2[m] - oo2[m];
                         }
                     }
                 }
