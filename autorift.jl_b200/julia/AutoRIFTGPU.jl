@@ -1,14 +1,24 @@
 # AutoRIFTGPU: the Julia side of libautorift_gpu's C ABI (include/autorift_gpu.h).
 #
-# A drop-in for AutoRIFT.jl's correlator: `track!` and `prepare` with the reference's own types
-# (ImagePair, PointSet, Params, DisplacementField), computed on a B200 through `ccall`. The FFI
-# idiom is the reference's FFTW binding (src/plans.jl:271-312): a `const` library path, raw
-# `Ptr{Cvoid}` handles cached under a `ReentrantLock`, no finalizers on the hot path, and a
-# non-zero status turned into a Julia exception naming the failure.
+# A drop-in for AutoRIFT.jl's correlator with the reference's own types (ImagePair, PointSet,
+# Params, DisplacementField, MultichipResult), computed on a B200 through `ccall`: `track!`,
+# `correlate_multichip`, the three `autorift` forms and the `init` / `reinit!` / `autorift!`
+# cache lifecycle, plus `submit` for the request loop. The FFI idiom is the reference's FFTW
+# binding (src/plans.jl:271-312): a `const` library path, raw `Ptr{Cvoid}` handles (one
+# context per device, cached under a `ReentrantLock`), no finalizers, and a non-zero status
+# turned into a Julia exception naming the failure.
+#
+# Device memory: a `Cache` owns its prepared pair on the device until `close(cache)` (or the
+# next `reinit!`, which replaces it); every other call uploads what it needs and frees it
+# before returning. Nothing is cached globally except the per-device context.
 #
 # Load after AutoRIFT:
 #     using AutoRIFT; include("AutoRIFTGPU.jl"); using .AutoRIFTGPU
 #     out = AutoRIFTGPU.track(pair, pts, p)          # same result type as AutoRIFT.track
+#     cache = AutoRIFTGPU.init(a, b; grid_spacing = 8)
+#     r = AutoRIFTGPU.autorift!(cache)               # MultichipResult
+#     AutoRIFTGPU.reinit!(cache; secondary = c); r2 = AutoRIFTGPU.autorift!(cache)
+#     close(cache)
 
 module AutoRIFTGPU
 
@@ -133,34 +143,44 @@ measure_code(::ZNCC) = AR_ZNCC
 measure_code(::NCC) = AR_NCC
 measure_code(m) = throw(ArgumentError("$(typeof(m)) has no GPU implementation"))
 
-# A device-resident pair, keyed on the identity of the arrays it was made from: the same
-# `===` reuse the reference's Cache makes (src/api.jl:325-335).
+# A pair resident on the device (`ar_pair`). Owned by whoever made it; `release!` frees it.
 mutable struct DevicePair
     handle::Ptr{Cvoid}
     ctx::Ptr{Cvoid}
 end
 
-const PAIR_LOCK = ReentrantLock()
-const PAIRS = IdDict{Any,DevicePair}()
+function release!(dp::DevicePair)
+    if dp.handle != C_NULL
+        ccall((:ar_pair_destroy, LIB), Cint, (Ptr{Cvoid},), dp.handle)
+        dp.handle = C_NULL
+    end
+    return nothing
+end
 
+# Upload a host pair (ar_pair_upload). The library copies the arrays out before returning.
 function upload(pair::ImagePair, ctx::Ptr{Cvoid})
-    key = (pair.reference, pair.secondary, pair.reference_valid, pair.secondary_valid)
-    lock(PAIR_LOCK) do
-        get!(PAIRS, key) do
-            T = eltype(pair.reference)
-            ref = collect(pair.reference)          # dense column-major copies
-            sec = collect(pair.secondary)
-            rv = collect(pair.reference_valid)     # Matrix{Bool}: one byte per pixel
-            sv = collect(pair.secondary_valid)
-            h = Ref{Ptr{Cvoid}}(C_NULL)
-            nr, nc = size(ref)
-            rc = ccall((:ar_pair_upload, LIB), Cint,
-                       (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{UInt8}, Ptr{UInt8}, Int64,
-                        Int64, Cint, Ref{Ptr{Cvoid}}),
-                       ctx, ref, sec, rv, sv, nr, nc, eltype_code(T), h)
-            check(ctx, rc, "ar_pair_upload")
-            DevicePair(h[], ctx)
-        end
+    T = eltype(pair.reference)
+    ref = collect(pair.reference)          # dense column-major copies (no-ops for Matrix)
+    sec = collect(pair.secondary)
+    rv = collect(pair.reference_valid)     # Matrix{Bool}: one byte per pixel
+    sv = collect(pair.secondary_valid)
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    nr, nc = size(ref)
+    rc = ccall((:ar_pair_upload, LIB), Cint,
+               (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{UInt8}, Ptr{UInt8}, Int64,
+                Int64, Cint, Ref{Ptr{Cvoid}}),
+               ctx, ref, sec, rv, sv, nr, nc, eltype_code(T), h)
+    check(ctx, rc, "ar_pair_upload")
+    return DevicePair(h[], ctx)
+end
+
+# Run `f(dp)` on a temporary device copy of `pair`, freed afterwards.
+function with_device(f, pair::ImagePair, ctx::Ptr{Cvoid})
+    dp = upload(pair, ctx)
+    try
+        return f(dp)
+    finally
+        release!(dp)
     end
 end
 
@@ -168,14 +188,20 @@ end
     AutoRIFTGPU.track!(out, pair, pts, p; subpixel = p.subpixel, measure = first(p.similarity))
 
 `AutoRIFT.track!` (src/track.jl:103-152) on the GPU: same arguments, same semantics, same
-`DisplacementField` written in place.
+`DisplacementField` written in place. `pair` is a host `ImagePair` (uploaded for the call) or a
+`DevicePair` already on the device.
 """
 function track!(out::DisplacementField, pair::ImagePair, pts::PointSet, p::Params;
-                subpixel = p.subpixel, measure = first(p.similarity), device::Integer = 0)
+                device::Integer = 0, kw...)
+    ctx = context(device)
+    with_device(dp -> track!(out, dp, pts, p; kw...), pair, ctx)
+end
+
+function track!(out::DisplacementField, dp::DevicePair, pts::PointSet, p::Params;
+                subpixel = p.subpixel, measure = first(p.similarity))
     length(out) == length(pts) || throw(DimensionMismatch(
         "output has $(length(out)) points but the point set has $(length(pts))"))
-    ctx = context(device)
-    dp = upload(pair, ctx)
+    ctx = dp.ctx
     flat = scatter(pts)
     x, y = collect(flat.x), collect(flat.y)
     rx, ry = collect(flat.radius_x), collect(flat.radius_y)
@@ -204,7 +230,7 @@ function track!(out::DisplacementField, pair::ImagePair, pts::PointSet, p::Param
     return out
 end
 
-track(pair::ImagePair, pts::PointSet, p::Params; kw...) =
+track(pair::Union{ImagePair,DevicePair}, pts::PointSet, p::Params; kw...) =
     track!(displacement_field(pts), pair, pts, p; kw...)
 
 prepare_opts(m::NoPreprocess, q) = ArPrepareOpts(AR_PRE_NONE, 0, 0.0, quant_code(q))
@@ -214,34 +240,52 @@ prepare_opts(m, q) = throw(ArgumentError("$(typeof(m)) has no GPU implementation
 quant_code(::QuantizeUInt8) = AR_QUANT_UINT8
 quant_code(::NoQuantize) = AR_QUANT_NONE
 
-"""
-    AutoRIFTGPU.prepare(pair, p) -> ImagePair
-
-`_prepare` (src/api.jl:305-311) on the GPU: preprocess then quantize each image, returned as a
-host `ImagePair` of the correlation element type with the filtered masks.
-"""
-function prepare(pair::ImagePair, p::Params; device::Integer = 0)
-    ctx = context(device)
-    dp = upload(pair, ctx)
+# `_prepare` (src/api.jl:305-311) on the device: the raw pair is uploaded, filtered and
+# quantised into a new device pair, and the raw copy freed. The result stays on the device.
+function device_prepare(raw::ImagePair, p::Params, ctx::Ptr{Cvoid})
     opts = Ref(prepare_opts(p.preprocess, p.quantize))
-    h = Ref{Ptr{Cvoid}}(C_NULL)
-    rc = ccall((:ar_prepare, LIB), Cint,
-               (Ptr{Cvoid}, Ptr{Cvoid}, Ref{ArPrepareOpts}, Ref{Ptr{Cvoid}}), ctx, dp.handle, opts, h)
-    check(ctx, rc, "ar_prepare")
+    with_device(raw, ctx) do dp
+        h = Ref{Ptr{Cvoid}}(C_NULL)
+        rc = ccall((:ar_prepare, LIB), Cint,
+                   (Ptr{Cvoid}, Ptr{Cvoid}, Ref{ArPrepareOpts}, Ref{Ptr{Cvoid}}),
+                   ctx, dp.handle, opts, h)
+        check(ctx, rc, "ar_prepare")
+        DevicePair(h[], ctx)
+    end
+end
+
+# A device pair's images and masks as a host ImagePair of its element type.
+function download(dp::DevicePair)
+    ctx = dp.ctx
     dt = Ref{Cint}(0); nr = Ref{Int64}(0); nc = Ref{Int64}(0)
     check(ctx, ccall((:ar_pair_info, LIB), Cint,
-                     (Ptr{Cvoid}, Ref{Cint}, Ref{Int64}, Ref{Int64}), h[], dt, nr, nc), "ar_pair_info")
+                     (Ptr{Cvoid}, Ref{Cint}, Ref{Int64}, Ref{Int64}), dp.handle, dt, nr, nc),
+          "ar_pair_info")
     T = dt[] == AR_U8 ? UInt8 : dt[] == AR_F32 ? Float32 : dt[] == AR_U16 ? UInt16 : Int16
     r = Matrix{T}(undef, nr[], nc[]); s = similar(r)
     rv = Matrix{Bool}(undef, nr[], nc[]); sv = similar(rv)
     rc = ccall((:ar_pair_download, LIB), Cint,
                (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Bool}, Ptr{Bool}),
-               ctx, h[], r, s, rv, sv)
-    ccall((:ar_pair_destroy, LIB), Cint, (Ptr{Cvoid},), h[])
+               ctx, dp.handle, r, s, rv, sv)
     check(ctx, rc, "ar_pair_download")
     return ImagePair(r, s, rv, sv)
 end
 
+"""
+    AutoRIFTGPU.prepare(pair, p) -> ImagePair
+
+`_prepare` (src/api.jl:305-311) on the GPU: preprocess then quantize each image, returned as a
+host `ImagePair` of the correlation element type with the filtered masks. (The pipeline itself
+never takes this round trip: `init` and `autorift` keep the prepared pair on the device.)
+"""
+function prepare(pair::ImagePair, p::Params; device::Integer = 0)
+    dp = device_prepare(pair, p, context(device))
+    try
+        return download(dp)
+    finally
+        release!(dp)
+    end
+end
 
 outlier_fields(f::GardnerFilter) = (Cint(1), f.window, f.iterations, f.min_agree_fraction,
                                     f.agree_tolerance, f.mad_scale)
@@ -272,15 +316,18 @@ function flat_points(pts::PointSet)
 end
 
 """
-    AutoRIFTGPU.correlate_multichip(prepared::ImagePair, grid::PointSet{2}, p) -> MultichipResult
+    AutoRIFTGPU.correlate_multichip(prepared, grid::PointSet{2}, p) -> MultichipResult
 
-`correlate_multichip` (src/multichip.jl:106-137) on the GPU, over a prepared pair.
+`correlate_multichip` (src/multichip.jl:106-137) on the GPU, over a prepared pair: a host
+`ImagePair` (uploaded for the call) or a `DevicePair` already on the device.
 """
 function correlate_multichip(prepared::ImagePair, grid::PointSet, p::Params; device::Integer = 0)
-    ctx = context(device)
-    dp = upload(prepared, ctx)
+    with_device(dp -> correlate_multichip(dp, grid, p), prepared, context(device))
+end
+
+function correlate_multichip(dp::DevicePair, grid::PointSet, p::Params)
+    ctx = dp.ctx
     gr, gc = size(grid)
-    n = gr * gc
     dx = Matrix{Float32}(undef, gr, gc); dy = similar(dx); cc = similar(dx)
     cs = Matrix{UInt16}(undef, gr, gc); it = Matrix{UInt8}(undef, gr, gc)
     P, cols = flat_points(grid)
@@ -296,24 +343,160 @@ function correlate_multichip(prepared::ImagePair, grid::PointSet, p::Params; dev
     return MultichipResult(dx, dy, cc, cs, BitMatrix(it .!= 0))
 end
 
+# The grid when the caller gives none (`_build_grid`, src/api.jl:339-347).
+build_grid(imagesize, p::Params) =
+    gridpoints(imagesize, p.grid_spacing; chip_size = p.chip_size_max,
+               chip_aspect = p.chip_aspect, search_radius_x = p.search_radius_x,
+               search_radius_y = p.search_radius_y, dx_prior = p.dx_prior,
+               dy_prior = p.dy_prior)
+
+"""
+    AutoRIFTGPU.Cache
+
+`AutoRIFT.Cache` (src/api.jl:30-44) with the prepared pair resident on the device: the
+resolved parameters, the pair as supplied (`raw`, host arrays), the prepared pair (a
+`DevicePair` owned by the cache), the grid, the last result and the dirty flag. Built by
+`init`, advanced by `reinit!`, run by `autorift!`; `close(cache)` frees its device memory.
+Not thread-safe: one cache per task, as in the reference.
+"""
+mutable struct Cache{P<:Params}
+    params::P
+    raw::ImagePair
+    prepared::DevicePair
+    grid::PointSet{2}
+    result::Union{Nothing,MultichipResult}
+    isfresh::Bool
+end
+
+"""
+    AutoRIFTGPU.init(reference, secondary; reference_valid, secondary_valid, device, kw...) -> Cache
+
+`init` (src/api.jl:66-76): resolve the keywords, filter and quantise both images on the device
+(the prepared pair stays there), build the grid.
+"""
+function init(reference::AbstractMatrix, secondary::AbstractMatrix;
+              reference_valid = nothing, secondary_valid = nothing, device::Integer = 0, kw...)
+    p = AutoRIFT.params(; kw...)
+    raw = ImagePair(reference, secondary; reference_valid, secondary_valid)
+    prepared = device_prepare(raw, p, context(device))
+    grid = build_grid(size(raw.reference), p)
+    return Cache{typeof(p)}(p, raw, prepared, grid, nothing, true)
+end
+
+# The mask the cache holds for `img` (in either slot), or `nothing` (src/api.jl:325-328).
+maskfor(img, old::ImagePair) =
+    img === old.reference ? old.reference_valid :
+    img === old.secondary ? old.secondary_valid : nothing
+
+"""
+    AutoRIFTGPU.reinit!(cache; reference, secondary, reference_valid, secondary_valid) -> cache
+
+`reinit!` (src/api.jl:104-134): point the cache at a new pair of the same size. An omitted
+image keeps its value; an omitted mask follows its image (kept only when the cache holds that
+same image, matched by identity in either slot, else derived from finiteness). When nothing
+changed identity the prepared pair is kept; otherwise the new pair is prepared on the device and
+the old prepared pair freed. (The reference re-filters only the image that changed; the device
+prepares both in a fraction of a millisecond, with the same result.)
+"""
+function reinit!(cache::Cache; reference = nothing, secondary = nothing,
+                 reference_valid = nothing, secondary_valid = nothing)
+    isnothing(reference) && isnothing(secondary) &&
+        isnothing(reference_valid) && isnothing(secondary_valid) && return cache
+    old = cache.raw
+    ref = isnothing(reference) ? old.reference : reference
+    sec = isnothing(secondary) ? old.secondary : secondary
+    rv = isnothing(reference_valid) ? maskfor(ref, old) : reference_valid
+    sv = isnothing(secondary_valid) ? maskfor(sec, old) : secondary_valid
+    size(ref) == size(old.reference) && size(sec) == size(old.reference) ||
+        throw(DimensionMismatch(
+            "new images are $(size(ref)) and $(size(sec)) but the cache was built for " *
+            "$(size(old.reference)); the grid and output arrays are sized to that. Build a " *
+            "new cache with `init` for a different image size."))
+    raw = ImagePair(ref, sec; reference_valid = rv, secondary_valid = sv)
+    same = raw.reference === old.reference && raw.secondary === old.secondary &&
+           raw.reference_valid === old.reference_valid &&
+           raw.secondary_valid === old.secondary_valid
+    if !same
+        prepared = device_prepare(raw, cache.params, cache.prepared.ctx)
+        release!(cache.prepared)
+        cache.prepared = prepared
+    end
+    cache.raw = raw
+    cache.isfresh |= true
+    cache.result = nothing
+    return cache
+end
+
+"""
+    AutoRIFTGPU.autorift!(cache) -> MultichipResult
+
+`autorift!` (src/api.jl:165-170): correlate the cache's current pair on the device; calling
+it again before the next `reinit!` returns the same result without recomputing.
+"""
+function autorift!(cache::Cache)
+    cache.isfresh || isnothing(cache.result) || return cache.result
+    cache.result = correlate_multichip(cache.prepared, cache.grid, cache.params)
+    cache.isfresh = false
+    return cache.result
+end
+
+"""
+    AutoRIFTGPU.imagepair(cache) -> ImagePair
+
+The pair the correlator sees (`imagepair`, src/api.jl:52), copied back from the device.
+"""
+imagepair(cache::Cache) = download(cache.prepared)
+
+"""
+    close(cache)
+
+Free the cache's prepared pair on the device. The cache cannot run again afterwards.
+"""
+Base.close(cache::Cache) = release!(cache.prepared)
+
 """
     AutoRIFTGPU.autorift(image1, image2; kw...) -> MultichipResult
+    AutoRIFTGPU.autorift(image1, image2, p::Params) -> MultichipResult
+    AutoRIFTGPU.autorift(image1, image2, grid::PointSet; kw...) -> MultichipResult or DisplacementField
 
-`autorift` (src/api.jl:210-274) with the default grid: prepare both images, then the
-multi-chip-size search, on the GPU.
+The three forms of `autorift` (src/api.jl:210-274) on the GPU. The keyword form is
+`autorift!(init(...))` with the cache closed afterwards; a gridded `PointSet{2}` runs the
+multi-chip-size search over it, a scattered `PointSet{1}` runs one scale with `track`.
 """
-function autorift(image1::AbstractMatrix, image2::AbstractMatrix; reference_valid = nothing,
-                  secondary_valid = nothing, device::Integer = 0, kw...)
-    p = AutoRIFT.params(; kw...)
-    pair = reference_valid === nothing && secondary_valid === nothing ? ImagePair(image1, image2) :
-           ImagePair(image1, image2, something(reference_valid, isfinite.(image1)),
-                     something(secondary_valid, isfinite.(image2)))
-    grid = gridpoints(size(image1), p.grid_spacing; chip_size = p.chip_size_max,
-                      chip_aspect = p.chip_aspect, search_radius_x = p.search_radius_x,
-                      search_radius_y = p.search_radius_y, dx_prior = p.dx_prior,
-                      dy_prior = p.dy_prior)
-    return correlate_multichip(prepare(pair, p; device), grid, p; device)
+function autorift(image1::AbstractMatrix, image2::AbstractMatrix; kw...)
+    cache = init(image1, image2; kw...)
+    try
+        return autorift!(cache)
+    finally
+        close(cache)
+    end
 end
+
+function autorift(image1::AbstractMatrix, image2::AbstractMatrix, p::Params; device::Integer = 0)
+    dp = device_prepare(ImagePair(image1, image2), p, context(device))
+    try
+        return correlate_multichip(dp, build_grid(size(image1), p), p)
+    finally
+        release!(dp)
+    end
+end
+
+function autorift(image1::AbstractMatrix, image2::AbstractMatrix, grid::PointSet;
+                  reference_valid = nothing, secondary_valid = nothing, device::Integer = 0,
+                  kw...)
+    p = AutoRIFT.params(; kw...)
+    raw = ImagePair(image1, image2; reference_valid, secondary_valid)
+    dp = device_prepare(raw, p, context(device))
+    try
+        return run_points(dp, grid, p)
+    finally
+        release!(dp)
+    end
+end
+
+# Dispatch on the point set's dimensionality (`_run`, src/api.jl:273-274).
+run_points(dp::DevicePair, grid::PointSet{2}, p::Params) = correlate_multichip(dp, grid, p)
+run_points(dp::DevicePair, pts::PointSet{1}, p::Params) = track(dp, pts, p)
 
 # A queued request and everything it references (kept alive until it completes).
 mutable struct Ticket
@@ -324,16 +507,20 @@ mutable struct Ticket
 end
 
 """
-    AutoRIFTGPU.submit(image1, image2, grid, p) -> Ticket
+    AutoRIFTGPU.submit(image1, image2, grid, p; reference_valid, secondary_valid) -> Ticket
 
 Queue `autorift` on the context's request loop (`ar_submit`); requests submitted from several
 tasks run concurrently on the device. `fetch(ticket)` waits and returns the MultichipResult.
+Masks default to all-valid for integer images and to finiteness for float images, as
+`ImagePair`'s default.
 """
 function submit(image1::AbstractMatrix{T}, image2::AbstractMatrix{T}, grid::PointSet, p::Params;
-                secondary_valid = nothing, device::Integer = 0) where {T}
+                reference_valid = nothing, secondary_valid = nothing,
+                device::Integer = 0) where {T}
     ctx = context(device)
     ref = collect(image1); sec = collect(image2)
-    sv = secondary_valid === nothing ? nothing : collect(secondary_valid)  # Matrix{Bool}
+    rv = reference_valid === nothing ? nothing : collect(Bool, reference_valid)  # one byte per pixel
+    sv = secondary_valid === nothing ? nothing : collect(Bool, secondary_valid)
     gr, gc = size(grid)
     res = MultichipResult(Matrix{Float32}(undef, gr, gc), Matrix{Float32}(undef, gr, gc),
                           Matrix{Float32}(undef, gr, gc), Matrix{UInt16}(undef, gr, gc),
@@ -342,7 +529,8 @@ function submit(image1::AbstractMatrix{T}, image2::AbstractMatrix{T}, grid::Poin
     P, cols = flat_points(grid)
     Pref = Ref(P)
     angs = rotation_angles(p.rotation)  # copied by ar_submit
-    req = Ref(ArRequest(pointer(ref), pointer(sec), C_NULL,
+    req = Ref(ArRequest(pointer(ref), pointer(sec),
+                        rv === nothing ? C_NULL : Ptr{UInt8}(pointer(rv)),
                         sv === nothing ? C_NULL : Ptr{UInt8}(pointer(sv)),
                         size(ref, 1), size(ref, 2), eltype_code(T),
                         prepare_opts(p.preprocess, p.quantize), multichip_params(p, angs),
@@ -353,7 +541,7 @@ function submit(image1::AbstractMatrix{T}, image2::AbstractMatrix{T}, grid::Poin
     rc = GC.@preserve angs ccall((:ar_submit, LIB), Cint, (Ptr{Cvoid}, Ref{ArRequest}, Ref{Int64}),
                                  ctx, req, t)
     check(ctx, rc, "ar_submit")
-    return Ticket(ctx, t[], (ref, sec, sv, cols, Pref, req, it), res)
+    return Ticket(ctx, t[], (ref, sec, rv, sv, cols, Pref, req, it), res)
 end
 
 function Base.fetch(t::Ticket)
