@@ -88,6 +88,7 @@ SIGNATURES = {
                                        _p, _p, _p, _p, _p]),
     "ar_track_device_static": (_i32, [_p, _p, _p, _i64, _i64, _i32, ctypes.POINTER(ArPoints), _i32,
                                       _i32, _p, _p, _p, _p, _p, ctypes.c_char_p, _sz]),
+    "ar_scratch_allocations": (_i32, [ctypes.POINTER(_i64)]),
     "ar_correlate": (_i32, [_p, _p, _p, _i32, _i64, _i64, _i64, _i64, _i32, _p,
                             ctypes.POINTER(_i32)]),
     "ar_refine_patches": (_i32, [_p, _p, _i64, _i32, _p, _p, _p]),

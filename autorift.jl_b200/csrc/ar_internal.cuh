@@ -92,7 +92,15 @@ struct TrackScratch {
     // When set, the sub-pixel queue grows from this pool in stream order (no device-wide
     // synchronisation when a context first meets a larger pass).
     cudaMemPool_t pool = nullptr;
+    // Set for a view of caller-provided memory (the allocation-free entry point): every buffer
+    // above is already in place, nothing is ever allocated or created for it, and a pass that
+    // would need more fails instead of growing it.
+    bool fixed = false;
 };
+
+// Number of device buffers and events the track scratch has allocated or created in this
+// process (a diagnostic: the allocation-free entry point must never add to it).
+long long scratch_allocations();
 
 // Reads and clears the pass status; AR-style: 0 ok, 1 a bounded device wait ran out.
 cudaError_t read_status(TrackScratch& scratch, cudaStream_t stream, int* status);

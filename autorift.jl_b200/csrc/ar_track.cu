@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <climits>
 #include <cmath>
@@ -3027,23 +3028,35 @@ cudaError_t launch_corr_t(const CorrArgs& A, const CorrPlan& P, int grid, cudaSt
 }
 
 
+std::atomic<long long> g_scratch_allocs{0};
+
 cudaError_t ensure_scratch(TrackScratch& s, int64_t n, cudaStream_t stream) {
+    if (s.fixed) {
+        // Caller-provided buffers: never allocate; a pass beyond them is an error.
+        if (!s.geom || !s.sub_count || !s.status || !s.sub_point || !s.sub_origin || !s.sub_patch)
+            return cudaErrorInvalidValue;
+        return s.capacity >= n ? cudaSuccess : cudaErrorMemoryAllocation;
+    }
     if (!s.geom) {
         cudaError_t e = cudaMalloc(&s.geom, 8 * sizeof(int64_t));
         if (e != cudaSuccess) return e;
+        ++g_scratch_allocs;
     }
     if (!s.sub_count) {
         cudaError_t e = cudaMalloc(&s.sub_count, sizeof(int));
         if (e != cudaSuccess) return e;
+        ++g_scratch_allocs;
     }
     if (!s.status) {
         cudaError_t e = cudaMalloc(&s.status, sizeof(int));
         if (e == cudaSuccess) e = cudaMemset(s.status, 0, sizeof(int));
         if (e != cudaSuccess) return e;
+        ++g_scratch_allocs;
     }
     if (s.capacity >= n) return cudaSuccess;
     const int64_t cap = std::max<int64_t>(n, 1024);
     cudaError_t e = cudaSuccess;
+    g_scratch_allocs += 3;
     if (s.pool) {
         // Stream-ordered: the old queue is released after the work already on `stream`.
         if (s.sub_point) cudaFreeAsync(s.sub_point, stream);
@@ -3201,9 +3214,15 @@ cudaError_t pass_geometry_device(const DevPoints& pts, int64_t nrows, int64_t nc
 // The scratch buffers are shared by the passes of a context; a pass on one stream waits for
 // the last pass that used them, whichever stream that ran on.
 cudaError_t scratch_acquire(TrackScratch& s, cudaStream_t stream) {
-    if (!s.done) return cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
+    if (!s.done) {
+        if (s.fixed) return cudaSuccess;  // no event is created for a caller-provided view
+        ++g_scratch_allocs;
+        return cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
+    }
     return cudaStreamWaitEvent(stream, s.done, 0);
 }
+
+long long scratch_allocations() { return g_scratch_allocs.load(); }
 
 cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const uint8_t* valid,
                               int64_t nrows, int64_t ncols, const DevPoints& pts,
@@ -3413,7 +3432,7 @@ cudaError_t launch_track(int dtype, const void* ref, const void* sec, const uint
     if (e != cudaSuccess) return e;
     e = launch_track_impl(dtype, ref, sec, valid, nrows, ncols, pts, geom, up, measure, out,
                           scratch, num_sms, stream, err, surf_out, rot);
-    const cudaError_t r = cudaEventRecord(scratch.done, stream);
+    const cudaError_t r = scratch.done ? cudaEventRecord(scratch.done, stream) : cudaSuccess;
     return e != cudaSuccess ? e : r;
 }
 
@@ -3458,8 +3477,9 @@ cudaError_t launch_refine_patches(const float* patches, int64_t count, int up, i
 // The array is sized for kStaticMaxPoints points per call (about 3.8 MB, held by every GPU
 // that loads the library until the process exits). Calls share it and it keeps the last
 // call's contents; the queue counter and the geometry words are reset by every call before
-// use. Two calls that overlap on the GPU (different streams, or different host threads) race
-// on it and must not be issued.
+// use, and so is the status word a bounded tensor-core wait sets when it runs out. Two calls
+// that overlap on the GPU (different streams, or different host threads) race on it and must
+// not be issued.
 
 namespace ar {
 namespace {
@@ -3467,6 +3487,7 @@ namespace {
 constexpr int64_t kStaticMaxPoints = 32768;
 constexpr size_t kStaticGeomOff = 0;                                   // 8 x int64
 constexpr size_t kStaticCountOff = 64;                                 // int
+constexpr size_t kStaticStatusOff = 128;                               // int
 constexpr size_t kStaticPointOff = 256;                                // int64 per point
 constexpr size_t kStaticOriginOff = kStaticPointOff + 8 * kStaticMaxPoints;   // 2 x int32
 constexpr size_t kStaticPatchOff = kStaticOriginOff + 8 * kStaticMaxPoints;   // 25 x float
@@ -3558,8 +3579,15 @@ extern "C" int ar_track_device_static(const void* ref, const void* sec, const ui
     view.sub_point = reinterpret_cast<int64_t*>(base + kStaticPointOff);
     view.sub_origin = reinterpret_cast<int32_t*>(base + kStaticOriginOff);
     view.sub_patch = reinterpret_cast<float*>(base + kStaticPatchOff);
+    view.status = reinterpret_cast<int*>(base + kStaticStatusOff);
     view.capacity = kStaticMaxPoints;
+    view.fixed = true;  // the launch helpers then neither allocate nor create events
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    e = cudaMemsetAsync(view.status, 0, sizeof(int), s);
+    if (e != cudaSuccess) {
+        static_message(err, err_size, cudaGetErrorString(e));
+        return AR_ERR_CUDA;
+    }
     DevPoints dp{pts->x, pts->y, pts->radius_x, pts->radius_y, pts->dx_prior, pts->dy_prior,
                  pts->chip_size_x, pts->chip_size_y, pts->n};
     PassGeometry geom;
@@ -3577,6 +3605,25 @@ extern "C" int ar_track_device_static(const void* ref, const void* sec, const ui
         static_message(err, err_size, msg.empty() ? cudaGetErrorString(e) : msg.c_str());
         return msg.empty() ? AR_ERR_CUDA : AR_ERR_UNSUPPORTED;
     }
+    // Wait for the pass and read its status word: a bounded tensor-core wait that ran out
+    // leaves the outputs incomplete, which the caller must learn of.
+    int status = 0;
+    e = cudaMemcpyAsync(&status, view.status, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        static_message(err, err_size, cudaGetErrorString(e));
+        return AR_ERR_CUDA;
+    }
+    if (status) {
+        static_message(err, err_size, "a device wait ran out; results incomplete");
+        return AR_ERR_TIMEOUT;
+    }
+    return AR_OK;
+}
+
+extern "C" int ar_scratch_allocations(int64_t* count) {
+    if (!count) return AR_ERR_ARG;
+    *count = ar::scratch_allocations();
     return AR_OK;
 }
 

@@ -171,12 +171,21 @@ int ar_track_device_rotated(ar_ctx* ctx, const ar_pair* pair, const ar_points* p
  * and must not be issued. The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call before any stream
  * capture. Like ar_track_device, one small device-to-host read of the pass geometry
- * synchronises the stream. `err` (may be NULL) receives a message on failure.
+ * synchronises the stream; the call then returns once the pass has completed on `stream`,
+ * with AR_ERR_TIMEOUT if a bounded device wait ran out (the outputs are then incomplete).
+ * `err` (may be NULL) receives a message on failure.
  */
 int ar_track_device_static(const void* ref, const void* sec, const uint8_t* valid, int64_t nrows,
                            int64_t ncols, int dtype, const ar_points* pts_dev, int upsampling,
                            int measure, float* dx_dev, float* dy_dev, float* correlation_dev,
                            uint8_t* searched_dev, void* stream, char* err, size_t err_size);
+
+/*
+ * Diagnostic: how many device buffers and events the library's track scratch has allocated or
+ * created in this process so far. ar_track_device_static never adds to it. No reference
+ * counterpart.
+ */
+int ar_scratch_allocations(int64_t* count);
 
 /* The parameters correlate_multichip reads (Params, src/types.jl:781-829). */
 typedef struct {

@@ -4,9 +4,12 @@ ar_track_device_static is for callers that cannot allocate device memory when th
 correlate; it keeps the pass's scratch in a static device array of the library instead of
 context-owned buffers. This file checks, through the C ABI, that two calls in a row give the
 same dx, dy, correlation and searched as the context-based entry point on the same device
-inputs (bit-identical: the same kernels run on the same data), and that point sets beyond the
-array's capacity are rejected. It sets up everything it needs, so it runs alone in a fresh
-process as well as after the other tests; it is named to be collected last.
+inputs (bit-identical: the same kernels run on the same data), for UInt8 (tensor-core
+correlation) and UInt16 (CUDA-core correlation) images; that the calls allocate nothing (the
+library's scratch-allocation counter and the device's free memory are unchanged across them);
+and that point sets beyond the array's capacity are rejected. It sets up everything it needs,
+so it runs alone in a fresh process as well as after the other tests; it is named to be
+collected last.
 """
 
 import ctypes
@@ -34,16 +37,23 @@ def _run_context(ar, ctx, pair_handle, st, up, outs, stream):
                                       ctypes.c_void_p(stream)))
 
 
-def _run_static(ar, lib, dref, dsec, dvalid, shape, st, up, outs, stream):
+def _run_static(ar, lib, dref, dsec, dvalid, shape, dtype, st, up, outs, stream):
     err = ctypes.create_string_buffer(256)
     rc = lib.ar_track_device_static(dref.data_ptr(), dsec.data_ptr(), dvalid.data_ptr(),
-                                    shape[0], shape[1], ar._lib.AR_U8, ctypes.byref(st), up,
+                                    shape[0], shape[1], dtype, ctypes.byref(st), up,
                                     ar._lib.AR_ZNCC, *(o.data_ptr() for o in outs),
                                     ctypes.c_void_p(stream), err, 256)
     assert rc == 0, err.value.decode()
 
 
-def test_static_scratch_matches_context_entry_point_twice(ar):
+def _allocations(lib):
+    n = ctypes.c_int64(-1)
+    assert lib.ar_scratch_allocations(ctypes.byref(n)) == 0
+    return n.value
+
+
+@pytest.mark.parametrize("np_dtype", [np.uint8, np.uint16])
+def test_static_scratch_matches_context_entry_point_twice(ar, np_dtype):
     import torch
 
     import __graft_entry__ as ge
@@ -53,7 +63,8 @@ def test_static_scratch_matches_context_entry_point_twice(ar):
     ctx = ar._lib.Context(0)
     dev = torch.device("cuda", 0)
     stream = torch.cuda.Stream(dev)
-    ref, sec = ar.synthetic.shifted_pair(320, (4.4, -2.7), seed=41, dtype=np.uint8)
+    code = ar._lib.AR_U8 if np_dtype == np.uint8 else ar._lib.AR_U16
+    ref, sec = ar.synthetic.shifted_pair(320, (4.4, -2.7), seed=41, dtype=np_dtype)
     rv = np.ones(ref.shape, bool)
     rv[40:90, 200:260] = False
     pair = ar.ImagePair(ref, sec, rv, None)
@@ -73,16 +84,25 @@ def test_static_scratch_matches_context_entry_point_twice(ar):
             st, keep = _device_points(torch, ar, pts, dev)
             want = _outputs(torch, len(pts), dev)
             _run_context(ar, ctx, dp.handle, st, up, want, stream.cuda_stream)
-            for call in range(2):  # two calls in a row share the static scratch
-                got = _outputs(torch, len(pts), dev)
-                _run_static(ar, lib, dref, dsec, dvalid, ref.shape, st, up, got,
+            got = [_outputs(torch, len(pts), dev) for _ in range(2)]
+            stream.synchronize()
+            # The first static call on this device looks the array's address up; every call
+            # after it must leave both the counter and the device's free memory unchanged.
+            _run_static(ar, lib, dref, dsec, dvalid, ref.shape, code, st, up, got[0],
+                        stream.cuda_stream)
+            allocs = _allocations(lib)
+            free0 = torch.cuda.mem_get_info(dev)[0]
+            for call in range(2):  # calls in a row share the static scratch
+                _run_static(ar, lib, dref, dsec, dvalid, ref.shape, code, st, up, got[call],
                             stream.cuda_stream)
                 stream.synchronize()
-                for g, w, name in zip(got, want, ("dx", "dy", "correlation", "searched")):
+                for g, w, name in zip(got[call], want, ("dx", "dy", "correlation", "searched")):
                     a, b = g.cpu().numpy(), w.cpu().numpy()
                     same = (a == b) | (np.isnan(a) & np.isnan(b)) if a.dtype.kind == "f" else (a == b)
                     assert same.all(), f"call {call}, {name}: {np.count_nonzero(~same)} differ"
-                assert bool(got[3].any())
+                assert bool(got[call][3].any())
+            assert _allocations(lib) == allocs, "the static entry point allocated scratch"
+            assert torch.cuda.mem_get_info(dev)[0] == free0, "device free memory changed"
 
 
 def test_static_scratch_rejects_oversized_point_sets(ar):
