@@ -22,6 +22,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
+#include <type_traits>
 
 #include "ar_internal.cuh"
 
@@ -187,6 +188,167 @@ __global__ void __launch_bounds__(kBoxThreads) k_highpass(const T* img, const ui
                            });
 }
 
+// Highpass of integer imagery (UInt8, UInt16, Int16): the same stencil as k_highpass with the
+// sums carried as exact 32-bit integers (at most 63 x 63 values below 2^16 in magnitude), so
+// the mean s / cnt -- an FP64 division of exact integers rounded to Float32 -- is the reference's
+// bit for bit. A block stages a tile of TR x kHpCols outputs plus its halo in shared memory
+// with 16-byte loads of the column-major image and mask (aligned chunks of each column's linear
+// range, element-wise only where a chunk would leave the array), then slides the window down each
+// column (value sums, and the contributing and in-image-invalid counts packed in one word:
+// erosion is "no in-image neighbour is invalid") and across columns, writing the Float32 output
+// and the mask with consecutive threads on consecutive rows.
+constexpr int kHpCols = 32;
+constexpr int kHpThreads = 256;
+
+// Loads the elements [e0, e1) of `base` (nelem elements) as the aligned 16-byte chunks that
+// cover them -- scalars for a chunk that is not entirely inside [base, base + nelem) -- handing
+// each element (its index and value) to `put`. Lane `task0` of `stride` lanes takes every
+// stride-th chunk.
+template <typename T, typename Put>
+__device__ __forceinline__ void load_chunks(const T* base, int64_t nelem, int64_t e0, int64_t e1,
+                                            int task0, int stride, Put put) {
+    constexpr int64_t sz = static_cast<int64_t>(sizeof(T));
+    constexpr int per = 16 / static_cast<int>(sizeof(T));
+    const int64_t b = static_cast<int64_t>(reinterpret_cast<uintptr_t>(base));
+    const int64_t first = (b + e0 * sz) & ~int64_t{15};
+    const int64_t end = b + e1 * sz, lim = b + nelem * sz;
+    for (int64_t a = first + 16 * task0; a < end; a += 16 * stride) {
+        const int64_t ea = (a - b) / sz;  // element at the chunk's first byte (a - b is a multiple of sz)
+        if (a >= b && a + 16 <= lim) {
+            const uint4 v = __ldg(reinterpret_cast<const uint4*>(a));
+            const T* t = reinterpret_cast<const T*>(&v);
+#pragma unroll
+            for (int k = 0; k < per; ++k) {
+                const int64_t e = ea + k;
+                if (e >= e0 && e < e1) put(e, t[k]);
+            }
+        } else {
+            for (int k = 0; k < per; ++k) {
+                const int64_t e = ea + k;
+                if (e >= e0 && e < e1 && e >= 0 && e < nelem) put(e, base[e]);
+            }
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kHpThreads) k_highpass_int(const T* img, const uint8_t* mask,
+                                                             int64_t nr, int64_t nc, int wx,
+                                                             int wy, int TR, float* out,
+                                                             uint8_t* vout) {
+    extern __shared__ __align__(16) unsigned char hsm[];
+    const int ly = wy / 2, lx = wx / 2;
+    const int IR = TR + wy - 1, IC = kHpCols + wx - 1;
+    const int IRp = IR | 1;  // odd column stride: a warp's rows of different columns spread banks
+    int* sv = reinterpret_cast<int*>(hsm);                      // IC x IRp: value where contributing
+    uint32_t* sf = reinterpret_cast<uint32_t*>(sv + IC * IRp);  // 1 contributing | 1 << 16 invalid
+    int* vs = reinterpret_cast<int*>(sf + IC * IRp);            // IC x TR: column sums of values
+    uint32_t* vf = reinterpret_cast<uint32_t*>(vs + IC * TR);   // IC x TR: column sums of flags
+    const int tid = threadIdx.x;
+    const int64_t r0 = static_cast<int64_t>(blockIdx.x) * TR;
+    const int64_t c0 = static_cast<int64_t>(blockIdx.y) * kHpCols;
+    const int64_t n = nr * nc;
+
+    // Out-of-image elements: no contribution, not invalid (erosion ignores them).
+    for (int e = tid; e < IC * IRp; e += kHpThreads) {
+        sv[e] = 0;
+        sf[e] = 0u;
+    }
+    __syncthreads();
+    // Column segment cc covers rows [r0 - ly, r0 - ly + IR) of image column c0 - lx + cc; only its
+    // in-image rows are loaded. Warps take segments; lanes take 16-byte chunks.
+    const int warp = tid >> 5, lane = tid & 31;
+    for (int cc = warp; cc < IC; cc += kHpThreads / 32) {
+        const int64_t gc = c0 - lx + cc;
+        if (gc < 0 || gc >= nc) continue;
+        const int64_t rlo = r0 - ly > 0 ? r0 - ly : 0;
+        const int64_t rhi = r0 - ly + IR < nr ? r0 - ly + IR : nr;
+        if (rhi <= rlo) continue;
+        const int64_t e0 = gc * nr + rlo, e1 = gc * nr + rhi;
+        const int64_t shift = gc * nr + (r0 - ly);  // linear index of segment row 0
+        int* colv = sv + cc * IRp;
+        uint32_t* colf = sf + cc * IRp;
+        load_chunks(img, n, e0, e1, lane, 32, [&](int64_t e, T v) {
+            colv[e - shift] = static_cast<int>(v);
+        });
+        __syncwarp();
+        load_chunks(mask, n, e0, e1, lane, 32, [&](int64_t e, uint8_t m) {
+            const int i = static_cast<int>(e - shift);
+            if (m) {
+                colf[i] = 1u;
+            } else {
+                colf[i] = 1u << 16;
+                colv[i] = 0;
+            }
+        });
+    }
+    __syncthreads();
+    // Down each column: a task is a column and 16 output rows.
+    const int nseg = (TR + 15) >> 4;
+    for (int task = tid; task < IC * nseg; task += kHpThreads) {
+        const int cc = task / nseg, i0 = 16 * (task - cc * nseg);
+        const int* colv = sv + cc * IRp;
+        const uint32_t* colf = sf + cc * IRp;
+        int a = 0;
+        uint32_t f = 0u;
+        for (int k = 0; k < wy; ++k) {
+            a += colv[i0 + k];
+            f += colf[i0 + k];
+        }
+        const int iend = min(i0 + 16, TR);
+        for (int i = i0; i < iend; ++i) {
+            vs[cc * TR + i] = a;
+            vf[cc * TR + i] = f;
+            a += colv[i + wy] - colv[i];
+            f += colf[i + wy] - colf[i];
+        }
+    }
+    __syncthreads();
+    // Across columns: a thread is an output row and a share of the tile's columns.
+    const int r = tid % TR;
+    const int parts = kHpThreads / TR;  // TR divides kHpThreads
+    const int cw_ = kHpCols / parts;
+    const int cb = (tid / TR) * cw_;
+    const int64_t gr = r0 + r;
+    if (gr >= nr) return;
+    int a = 0;
+    uint32_t f = 0u;
+    for (int k = 0; k < wx; ++k) {
+        a += vs[(cb + k) * TR + r];
+        f += vf[(cb + k) * TR + r];
+    }
+    for (int c = cb; c < cb + cw_; ++c) {
+        const int64_t gc = c0 + c;
+        if (gc >= nc) break;
+        const int cnt = static_cast<int>(f & 0xFFFFu);
+        const bool eroded = (f >> 16) == 0u;
+        const float mean = cnt > 0 ? __double2float_rn(__ddiv_rn(static_cast<double>(a),
+                                                                 static_cast<double>(cnt)))
+                                   : __int_as_float(0x7fc00000);
+        const int ci = (c + lx) * IRp + (r + ly);  // the centre pixel in the staged tile
+        const bool m = (sf[ci] & 1u) != 0u;
+        float o = (m && isfinite(mean)) ? __fsub_rn(static_cast<float>(sv[ci]), mean)
+                                        : __int_as_float(0x7fc00000);
+        bool v = eroded;
+        if (!isfinite(o)) {
+            o = 0.0f;
+            v = false;
+        }
+        const int64_t g = gr + gc * nr;
+        out[g] = o;
+        vout[g] = v ? 1 : 0;
+        if (c + 1 < cb + cw_) {
+            a += vs[(c + wx) * TR + r] - vs[c * TR + r];
+            f += vf[(c + wx) * TR + r] - vf[c * TR + r];
+        }
+    }
+}
+
+size_t highpass_int_smem(int wx, int wy, int TR) {
+    const size_t IR = TR + wy - 1, IC = kHpCols + wx - 1, IRp = IR | 1;
+    return IC * IRp * 8 + IC * TR * 8;
+}
+
 // First Wallis pass: the masked box mean (src/preprocess.jl:336).
 template <typename T>
 __global__ void __launch_bounds__(kBoxThreads) k_boxmean(const T* img, const uint8_t* mask,
@@ -294,26 +456,52 @@ __device__ void block_dd(DD& a, long long& c, DD* sa, long long* sc) {
     }
 }
 
-// pass 0: sum and count of the valid finite values; pass 1: sum of squared deviations.
+// pass 0: sum and count of the valid finite values; pass 1: sum of squared deviations. Each
+// thread keeps kQU independent double-double accumulators fed by kQU coalesced loads per step
+// (more loads in flight than one dependent chain allows), merged in a fixed order.
+constexpr int kQU = 4;
+
 template <typename T, int PASS>
 __global__ void __launch_bounds__(kStatThreads) k_qstats(const T* img, const uint8_t* mask,
                                                          int64_t n, QuantStats* st) {
     __shared__ DD sa[32];
     __shared__ long long sc[32];
-    DD a{0.0, 0.0};
-    long long c = 0;
+    DD acc[kQU];
+    long long cc[kQU];
+#pragma unroll
+    for (int u = 0; u < kQU; ++u) {
+        acc[u] = DD{0.0, 0.0};
+        cc[u] = 0;
+    }
     const double mean = PASS == 1 ? st->mean : 0.0;
-    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        double v;
-        if (!q_ok(img, mask, i, &v)) continue;
-        if (PASS == 0) {
-            dd_add(a, v);
-            ++c;
-        } else {
-            const double d = __dsub_rn(v, mean);
-            dd_add(a, __dmul_rn(d, d));
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t i0 = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i0 < n;
+         i0 += kQU * stride) {
+        double v[kQU];
+        bool ok[kQU];
+#pragma unroll
+        for (int u = 0; u < kQU; ++u) {
+            const int64_t i = i0 + u * stride;
+            ok[u] = i < n && q_ok(img, mask, i, &v[u]);
         }
+#pragma unroll
+        for (int u = 0; u < kQU; ++u) {
+            if (!ok[u]) continue;
+            if (PASS == 0) {
+                dd_add(acc[u], v[u]);
+                ++cc[u];
+            } else {
+                const double d = __dsub_rn(v[u], mean);
+                dd_add(acc[u], __dmul_rn(d, d));
+            }
+        }
+    }
+    DD a = acc[0];
+    long long c = cc[0];
+#pragma unroll
+    for (int u = 1; u < kQU; ++u) {
+        dd_merge(a, acc[u]);
+        c += cc[u];
     }
     block_dd(a, c, sa, sc);
     if (threadIdx.x == 0) {
@@ -355,28 +543,52 @@ __global__ void k_qfinal(QuantStats* st, int nblocks) {
     }
 }
 
+// kQV consecutive pixels per thread: one vector load of the image where it is 16-byte aligned
+// (the filtered Float32 scratch always is), one 4-byte store of the output where aligned.
+constexpr int kQV = 4;
+
 template <typename T>
 __global__ void k_quantize(const T* img, const uint8_t* mask, int64_t n, const QuantStats* st,
                            uint8_t* out) {
-    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    if (i >= n) return;
+    const int64_t i0 = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) * kQV;
+    if (i0 >= n) return;
     const long long cnt = st->n;
-    if (cnt == 0) {
-        out[i] = 0;
-        return;
+    const double sd = st->sd, lo = st->lo, scale = st->scale;
+    T vals[kQV];
+    const bool full = i0 + kQV <= n;
+    if (full && sizeof(T) == 4 && (reinterpret_cast<uintptr_t>(img + i0) & 15) == 0) {
+        const uint4 w = __ldg(reinterpret_cast<const uint4*>(img + i0));
+        const T* t = reinterpret_cast<const T*>(&w);
+#pragma unroll
+        for (int u = 0; u < kQV; ++u) vals[u] = t[u];
+    } else {
+#pragma unroll
+        for (int u = 0; u < kQV; ++u) vals[u] = i0 + u < n ? img[i0 + u] : T(0);
     }
-    if (st->sd == 0.0) {
-        out[i] = mask[i] ? 0x80 : 0x00;
-        return;
+    uint8_t o[kQV];
+#pragma unroll
+    for (int u = 0; u < kQV; ++u) {
+        const int64_t i = i0 + u;
+        const bool m = i < n && mask[i] != 0;
+        const double v = static_cast<double>(vals[u]);
+        if (cnt == 0) {
+            o[u] = 0;
+        } else if (sd == 0.0) {
+            o[u] = m ? 0x80 : 0x00;
+        } else if (!m || !isfinite(v)) {
+            o[u] = 0;
+        } else {
+            double x = __dmul_rn(__dsub_rn(v, lo), scale);
+            x = x < 0.0 ? 0.0 : (x > 255.0 ? 255.0 : x);
+            o[u] = static_cast<uint8_t>(__double2uint_rn(x));
+        }
     }
-    double v;
-    if (!q_ok(img, mask, i, &v)) {
-        out[i] = 0;
-        return;
+    if (full && (reinterpret_cast<uintptr_t>(out + i0) & 3) == 0) {
+        *reinterpret_cast<uchar4*>(out + i0) = make_uchar4(o[0], o[1], o[2], o[3]);
+    } else {
+        for (int u = 0; u < kQV; ++u)
+            if (i0 + u < n) out[i0 + u] = o[u];
     }
-    double x = __dmul_rn(__dsub_rn(v, st->lo), st->scale);
-    x = x < 0.0 ? 0.0 : (x > 255.0 ? 255.0 : x);
-    out[i] = static_cast<uint8_t>(__double2uint_rn(x));
 }
 
 // NoQuantize of a float image: non-finite values become zero, the mask is kept
@@ -397,7 +609,9 @@ cudaError_t quantize_u8(const T* img, const uint8_t* mask, int64_t n, QuantStats
     k_qstats<T, 1><<<kStatBlocks, kStatThreads, 0, s>>>(img, mask, n, st);
     k_qfinal<1><<<1, 256, 0, s>>>(st, kStatBlocks);
     const int threads = 256;
-    k_quantize<T><<<static_cast<unsigned>((n + threads - 1) / threads), threads, 0, s>>>(img, mask, n, st, out);
+    const int64_t per_block = static_cast<int64_t>(threads) * kQV;
+    k_quantize<T><<<static_cast<unsigned>((n + per_block - 1) / per_block), threads, 0, s>>>(
+        img, mask, n, st, out);
     *launches += 5;
     return cudaGetLastError();
 }
@@ -426,7 +640,21 @@ cudaError_t prepare_t(const PrepareJob& J, cudaStream_t s, long long* launches) 
     float* filt = J.quantize == 1 ? J.ftmp : static_cast<float*>(J.out);
     cudaError_t e;
     if (smem > static_cast<size_t>(kDynSmemCap)) return cudaErrorInvalidValue;
-    if (J.preprocess == 1) {
+    if (J.preprocess == 1 && !std::is_same<T, float>::value) {
+        // Integer imagery: exact 32-bit sums, the tallest tile whose staging fits.
+        int TR = 128;
+        while (TR > 32 && highpass_int_smem(wx, wy, TR) > static_cast<size_t>(kDynSmemCap)) TR /= 2;
+        const size_t hsm = highpass_int_smem(wx, wy, TR);
+        if (hsm > static_cast<size_t>(kDynSmemCap)) return cudaErrorInvalidValue;
+        e = cudaFuncSetAttribute(k_highpass_int<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kDynSmemCap);
+        if (e != cudaSuccess) return e;
+        const dim3 hgrid(static_cast<unsigned>((J.nrows + TR - 1) / TR),
+                         static_cast<unsigned>((J.ncols + kHpCols - 1) / kHpCols));
+        k_highpass_int<T><<<hgrid, kHpThreads, hsm, s>>>(img, J.mask, J.nrows, J.ncols, wx, wy, TR,
+                                                         filt, J.vout);
+        *launches += 1;
+    } else if (J.preprocess == 1) {
         e = cudaFuncSetAttribute(k_highpass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kDynSmemCap);
         if (e != cudaSuccess) return e;
