@@ -2,25 +2,30 @@
 """Benchmark: points/s of AutoRIFT.jl's default pipeline at chip 32 / radius 25 on B200.
 
 Workload (one step): `autorift(image1, image2; grid_spacing=8)` with the reference's defaults
-(src/api.jl:210-274) on a 4096^2 synthetic UInt16 pair: highpass (width 5) and UInt8
-quantisation of both images (src/api.jl:305-311), then the multi-chip-size search
-(src/multichip.jl:106-422) over the 490 x 490 grid (spacing 8, margin from chip_size_max 128)
-at chip sizes 32/64/128, search radius 25, PyramidRefine(64), ZNCC, Gardner outlier filter and
-hole filling. Scene: seeded filtered noise (sigma 2, mean 8000, std 1500) and its bicubic warp
-by a 6-bump field up to 15 px, 2% noise, 3% no-data blobs passed as the secondary's mask.
+(src/api.jl:210-274) on a 10980^2 synthetic UInt16 pair (a Sentinel-2 tile's size): highpass
+(width 5) and UInt8 quantisation of both images (src/api.jl:305-311), then the multi-chip-size
+search (src/multichip.jl:106-422) over the 1350 x 1350 grid (spacing 8, margin from
+chip_size_max 128) at chip sizes 32/64/128, search radius 25, PyramidRefine(64), ZNCC, Gardner
+outlier filter and hole filling. Scene: seeded filtered noise (sigma 2, mean 8000, std 1500)
+and its bicubic warp by a 6-bump field up to 15 px, 2% noise, 3% no-data blobs passed as the
+secondary's mask.
 
 `value` times the device work with the raw pair and the grid resident in HBM; `e2e` times the
 same pipeline through the C ABI from host buffers (pair upload, grid upload, result download):
 its value through the request loop (ar_submit, pairs overlapping on the device), its p50/p99
 pair latency and `one_pair_at_a_time` through ar_pair_upload / ar_prepare / ar_multichip.
-L2 (126 MB) is flushed before every timed step by writing a 256 MiB buffer.
+`plain_gpu_path` is the same step with the direct FP32 correlation on CUDA cores, one pair at a
+time; `batched_vs_plain` sets the served rate against it. L2 (126 MB) is flushed before every
+timed step by writing a 256 MiB buffer. The 4096^2 pair of the at-scale configuration (490 x
+490 grid) is timed the same way and reported under `config_4096`; the serving configuration's
+Poisson sweep (sides 512/2048/4096/10980 in 8:4:2:1) under `serving`.
 
 Arms:
   default            our library (libautorift_gpu.so, sm_100a); N GPUs run N independent
                      replicas (one pair per rank, no collective on the data path).
   --impl reference   the reference's algorithm on the host cores: Julia is not installed, so
                      the CPU restatement (oracle/, C++ + OpenMP, all host threads) runs the
-                     same pipeline on a 2048^2 crop of the scene per step.
+                     same pipeline on a centred 2048^2 crop of the scene per step.
 
 Prints one JSON line (rank 0).
 """
@@ -44,11 +49,16 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "points/sec at chip32/r25 vs plain GPU path; p50/p99 pair latency"
 UNIT = "points/s"
-N, SPACING, CHIP, RADIUS, UP = 4096, 8, 32, 25, 64
+N, SPACING, CHIP, RADIUS, UP = 10980, 8, 32, 25, 64
+N_SCALE = 4096  # the at-scale configuration's pair, reported beside the headline
 CROP = 2048  # host sample: the same pipeline on a centred crop of the scene
-WORKLOAD = (f"autorift() default pipeline (highpass 5, UInt8, multichip 32/64/128, Gardner, fill) "
-            f"on a {N}^2 synthetic UInt16 pair, 490x490 grid spacing {SPACING}, radius {RADIUS}, "
-            f"PyramidRefine({UP})")
+SERVE_RATES = (5, 10, 20, 50, 100, 200)  # pairs/s of the serving sweep
+
+
+def workload(n, gr, gc):
+    return (f"autorift() default pipeline (highpass 5, UInt8, multichip 32/64/128, Gardner, "
+            f"fill) on a {n}^2 synthetic UInt16 pair, {gr}x{gc} grid spacing {SPACING}, radius "
+            f"{RADIUS}, PyramidRefine({UP})")
 
 
 def scene(ar, n=N):
@@ -188,32 +198,195 @@ def oracle_params(ar, p):
 
 def host_pipeline(O, ar, a, b, valid, p):
     """The oracle's pipeline on the host cores (prepare both images, multichip over the
-    default grid); returns (grid points, seconds)."""
+    default grid); returns (grid points, seconds, multichip outputs, prepared images)."""
     grid = ar.build_grid(a.shape, p)
     fields = {f: getattr(grid, f) for f in ar.points.FIELDS}
     t = time.perf_counter()
     wr, wrm = O.prepare(a, None, "highpass", p.preprocess.width)
     ws, wsm = O.prepare(b, valid, "highpass", p.preprocess.width)
-    O.multichip(wr, ws, fields, oracle_params(ar, p), wrm, wsm)
-    return len(grid), time.perf_counter() - t
+    out = O.multichip(wr, ws, fields, oracle_params(ar, p), wrm, wsm)
+    return len(grid), time.perf_counter() - t, out, (wr, ws, wrm, wsm)
+
+
+def crop_parity(ar, ctx, O, a, b, valid, p):
+    """The whole pipeline on a centred CROP^2 crop of the scene, on the host cores (the oracle,
+    timed: the CPU baseline) and through the library (`autorift` on the same crop, same grid
+    rule): every output of every grid point compared bit for bit."""
+    ca, cb, cv = crop(a, CROP), crop(b, CROP), crop(valid, CROP)
+    pts, dt, want, prepared = host_pipeline(O, ar, ca, cb, cv, p)
+    got = ar.autorift(ca, cb, secondary_valid=cv, ctx=ctx, grid_spacing=SPACING, chip_size=CHIP,
+                      search_radius=RADIUS, upsampling=UP)
+    names = ("dx", "dy", "correlation", "chip_size", "interpolated")
+    gv = (got.dx, got.dy, got.correlation, got.chip_size, got.interpolated)
+    same = {}
+    for nm, g, w in zip(names, gv, want):
+        g, w = np.asarray(g), np.asarray(w)
+        if g.dtype.kind == "f":
+            same[nm] = bool(np.array_equal(g.view(np.uint32), w.astype(np.float32).view(np.uint32)))
+        else:
+            same[nm] = bool(np.array_equal(g.astype(np.int64), w.astype(np.int64)))
+    cpu = {"value": pts / dt, "unit": UNIT, "cores": O.max_threads(), "kind": "port",
+           "sample": f"the same pipeline on a centred {CROP}^2 crop ({pts} grid points), "
+                     f"{dt:.1f} s",
+           "numerator": "FP64 direct sum (the reference computes it with single-precision "
+                        "FFTW, not installed here; the oracle is the exact value that "
+                        "approximates)"}
+    parity = {"crop": [CROP, CROP], "points": pts,
+              "what": "the library's autorift() on the crop against the oracle's prepare + "
+                      "multichip, every grid point",
+              "bit_identical": same, "all_bit_identical": all(same.values()),
+              "resolved": int(np.count_nonzero(np.asarray(got.chip_size)))}
+    return cpu, parity, prepared, (ca, cb, cv)
+
+
+def sample_fields(ar, grid, frac, seed, chip=CHIP):
+    n = len(grid)
+    idx = np.sort(np.random.default_rng(seed).choice(n, max(1, int(n * frac)), replace=False))
+    fl = {f: np.ascontiguousarray(grid.flat(f)[idx]) for f in ar.points.FIELDS}
+    fl["chip_size_x"] = np.full(idx.size, chip, np.int64)
+    fl["chip_size_y"] = np.full(idx.size, chip, np.int64)
+    return idx, fl
+
+
+def float_flip_rate(ar, ctx, O, ca, cb, cv, seed=3, frac=0.1):
+    """Sub-pixel agreement of the unquantised path: the crop highpass-filtered to Float32 (no
+    quantisation, so the surfaces carry FP32 products), a seeded sample of the grid at chip
+    32 / radius 25 / PyramidRefine(64), the library against the oracle's FP64 numerator. A
+    flip is a point whose dx or dy differs by more than 1e-3 px: a near-tie of the 1/64 px
+    cascade argmax decided by a last-bit surface difference."""
+    p = ar.params(grid_spacing=SPACING, chip_size=CHIP, search_radius=RADIUS, upsampling=UP,
+                  quantize="none")
+    grid = ar.build_grid(ca.shape, p)
+    idx, fl = sample_fields(ar, grid, frac, seed)
+    prep = ar.prepare(ar.ImagePair(ca, cb, None, cv), p, ctx)
+    ref, sec, rv, sv = prep.download()
+    L = ar._lib
+    st = L.ArPoints(*(fl[f].ctypes.data for f in ar.points.FIELDS), idx.size)
+    g = [np.empty(idx.size, np.float32) for _ in range(3)] + [np.empty(idx.size, np.uint8)]
+    ctx.check(ctx.lib.ar_track(ctx.handle, prep.device(ctx).handle, ctypes.byref(st), UP,
+                               L.AR_ZNCC, *(x.ctypes.data for x in g)))
+    w = O.track(ref, sec, fl, upsampling=UP, reference_valid=rv, secondary_valid=sv)
+    m = ~np.isnan(g[0]) & ~np.isnan(w[0])
+    d = np.maximum(np.abs(g[0] - w[0]), np.abs(g[1] - w[1]))[m]
+    dc = np.abs(g[2] - w[2])[m]
+    return {"what": "chip 32 / radius 25 / PyramidRefine(64) on the highpass-filtered Float32 "
+                    f"crop ({CROP}^2, quantize = :none), a seeded {int(frac * 100)}% sample, "
+                    "library (FP32 products, FP64 sums) against the oracle (FP64 numerator)",
+            "points": int(idx.size), "measured_both": int(m.sum()),
+            "same_measured_set": bool(np.array_equal(np.isnan(g[0]), np.isnan(w[0]))),
+            "flip_rate_over_1e-3px": float(np.mean(d > 1e-3)) if d.size else None,
+            "over_half_px": int(np.count_nonzero(d > 0.5)),
+            "max_abs_d_px": float(d.max()) if d.size else None,
+            "max_abs_dcorr": float(dc.max()) if dc.size else None}
+
+
+_CV = {}
+
+
+def _cv_init(ref, sec):
+    import cv2
+    cv2.setNumThreads(1)
+    _CV["ref"], _CV["sec"] = ref, sec
+
+
+def _cv_points(job):
+    """OpenCV's surface, peak and pyrUp cascade at each (row, col) chip centre of `job`
+    (0-based, after the +0.5 shift); returns each point's (dx, dy)."""
+    import cv2
+    ref, sec = _CV["ref"], _CV["sec"]
+    h, r = CHIP // 2, RADIUS
+    out = np.empty((len(job), 2))
+    for k, (y0, x0) in enumerate(job):
+        chip = sec[y0 - h:y0 + h, x0 - h:x0 + h]
+        win = ref[y0 - h - r:y0 + h + r - 1, x0 - h - r:x0 + h + r - 1]
+        s = cv2.matchTemplate(win, chip, cv2.TM_CCOEFF_NORMED)
+        i, j = np.unravel_index(int(np.argmax(s)), s.shape)
+        i0, j0 = min(max(i - 2, 0), s.shape[0] - 5), min(max(j - 2, 0), s.shape[1] - 5)
+        q = np.ascontiguousarray(s[i0:i0 + 5, j0:j0 + 5])
+        for _ in range(6):
+            q = cv2.pyrUp(q)
+        si, sj = np.unravel_index(int(np.argmax(q)), q.shape)
+        out[k] = (sj / UP + j0 - r, si / UP + i0 - r)
+    return out
+
+
+def opencv_baseline(ar, grid_fields, prepared):
+    """The per-point OpenCV loop (cv2.matchTemplate TM_CCOEFF_NORMED + six cv2.pyrUp steps +
+    argmax, the primitives the reference's fixtures come from) on the prepared UInt8 crop at
+    chip 32 / radius 25, over every interior grid point of the crop (no padding path), spread
+    over the host cores by a pool of spawned worker processes with one OpenCV thread each
+    (timed after the pool has started)."""
+    try:
+        import cv2
+    except ImportError:
+        return {"unavailable": "OpenCV is not importable"}
+    import multiprocessing as mp
+    ref = np.ascontiguousarray(prepared[0])
+    sec = np.ascontiguousarray(prepared[1])
+    nr, nc = ref.shape
+    h, r = CHIP // 2, RADIUS
+    cy = np.floor(grid_fields["y"] + 0.5).astype(np.int64) - 1  # 0-based
+    cx = np.floor(grid_fields["x"] + 0.5).astype(np.int64) - 1
+    ok = (cy - h - r >= 0) & (cy + h + r - 1 <= nr) & (cx - h - r >= 0) & (cx + h + r - 1 <= nc)
+    centres = np.stack([cy[ok], cx[ok]], axis=1)
+    procs = os.cpu_count() or 1
+    jobs = np.array_split(centres, max(1, procs * 8))
+    with mp.get_context("spawn").Pool(procs, initializer=_cv_init, initargs=(ref, sec)) as pool:
+        pool.map(_cv_points, [centres[:1]] * procs)  # workers up and warm
+        t0 = time.perf_counter()
+        res = pool.map(_cv_points, jobs)
+        dt = time.perf_counter() - t0
+    done = sum(len(j) for j in jobs)
+    return {"value": done / dt, "unit": UNIT, "cores": procs, "kind": "opencv",
+            "sample": f"all {done} interior points of the {CROP}^2 crop's grid at chip 32 / "
+                      f"radius 25 / x64 (prepared UInt8), {dt:.2f} s; cv2 {cv2.__version__}, "
+                      "one process per core, one OpenCV thread each",
+            "dxdy": np.concatenate(res) if res else None, "mask": ok}
+
+
+def opencv_agreement(ar, ctx, cv, cgrid, prepared):
+    """The OpenCV loop's offsets against the library's chip-32 pass on the same prepared crop
+    and points (OpenCV's FP32 surfaces differ from the exact ones in the last bits, so a few
+    1/64 px cascade ties flip)."""
+    dxdy, mask = cv.pop("dxdy", None), cv.pop("mask", None)
+    if dxdy is None:
+        return cv
+    fl = {f: np.ascontiguousarray(cgrid.flat(f)[mask]) for f in ar.points.FIELDS}
+    fl["chip_size_x"] = np.full(dxdy.shape[0], CHIP, np.int64)
+    fl["chip_size_y"] = np.full(dxdy.shape[0], CHIP, np.int64)
+    pair = ar.ImagePair(prepared[0], prepared[1], prepared[2], prepared[3])
+    L = ar._lib
+    st = L.ArPoints(*(fl[f].ctypes.data for f in ar.points.FIELDS), dxdy.shape[0])
+    g = [np.empty(dxdy.shape[0], np.float32) for _ in range(3)] + [np.empty(dxdy.shape[0], np.uint8)]
+    dp = pair.device(ctx)
+    ctx.check(ctx.lib.ar_track(ctx.handle, dp.handle, ctypes.byref(st), UP, L.AR_ZNCC,
+                               *(x.ctypes.data for x in g)))
+    m = ~np.isnan(g[0])
+    d = np.maximum(np.abs(dxdy[:, 0] - g[0]), np.abs(dxdy[:, 1] - g[1]))[m]
+    cv["agreement_with_library"] = {"points": int(m.sum()),
+                                    "within_1e-3px": float(np.mean(d <= 1e-3)) if d.size else None,
+                                    "within_1/32px": float(np.mean(d <= 1 / 32)) if d.size else None}
+    return cv
 
 
 def serving_requests(ar, rng, n_req, sizes, weights, base=None):
     """A mixed request stream in the proportions of the serving configuration: image sides
-    `sizes` with relative frequencies `weights`, grid spacing from {8, 16, 32}, chip from
-    {16, 32, 64}, search radius uniform in [8, 48]. Scenes are generated once per side (host
-    arrays in the column-major layout a Julia caller holds)."""
+    `sizes` in the exact relative frequencies `weights` (n_req rounded to a multiple of their
+    sum), shuffled; grid spacing from {8, 16, 32}, chip from {16, 32, 64}, search radius
+    uniform in [8, 48]. Scenes are generated once per side (host arrays in the column-major
+    layout a Julia caller holds)."""
     scenes = {}
     for n in sizes:
         a, b, v = base if (base is not None and base[0].shape[0] == n) else scene(ar, n)
         scenes[n] = (np.asfortranarray(a), np.asfortranarray(b), np.asfortranarray(v))
-    w = np.asarray(weights, float) / np.sum(weights)
+    k = max(1, int(round(n_req / sum(weights))))
+    sides = [n for n, w in zip(sizes, weights) for _ in range(k * w)]
+    rng.shuffle(sides)
     reqs = []
-    for _ in range(n_req):
-        n = int(rng.choice(sizes, p=w))
+    for n in sides:
         kw = dict(grid_spacing=int(rng.choice([8, 16, 32])), chip_size=int(rng.choice([16, 32, 64])),
                   search_radius=int(rng.integers(8, 49)), upsampling=UP)
-        reqs.append((n, kw))
+        reqs.append((int(n), kw))
     return scenes, reqs
 
 
@@ -266,14 +439,14 @@ def served_e2e(ar, device, ha, hb, hv, hgrid, gr, gc, opts, prm, size, n, pairs,
             "same_result_as_device_run": bool(same)}
 
 
-def serving_measure(ar, scenes, reqs, device, slots=4, rate=None, repeats=3):
+def serving_measure(ar, scenes, reqs, device, slots=4, rates=SERVE_RATES, repeats=2, seed=1):
     """The stream three ways: the plain GPU path (one pair at a time, the direct FP32
     correlation on CUDA cores -- tensor cores off), the same one-pair-at-a-time loop with the
     tensor-core kernels the server runs ("sequential"), and the request loop (continuous
-    batching, `slots` slots). The three are alternated `repeats` times and medians reported
-    (small pairs are bound by host round trips, so single runs vary with the host). Also the
-    per-request latency (queued + running, from the loop's own clock) for a Poisson stream at
-    `rate` requests/s (default: 70% of the measured capacity)."""
+    batching, `slots` slots), alternated `repeats` times after one untimed pass of each
+    (medians). Then the request loop under a seeded Poisson stream of the same requests at
+    each rate of `rates` (pairs/s): p50/p99 latency from submission to completion (the loop's
+    own clock) and the sustained points/s."""
     L = ar._lib
     points = [len(ar.build_grid(scenes[n][0].shape, ar.params(**kw))) for n, kw in reqs]
     plain_ctx = L.Context(device)
@@ -303,6 +476,7 @@ def serving_measure(ar, scenes, reqs, device, slots=4, rate=None, repeats=3):
     m = [(~np.isnan(p_.dx)) & (~np.isnan(s_.dx)) for p_, s_ in zip(plain_res, served_res)]
     dd = np.concatenate([np.maximum(np.abs(p_.dx - s_.dx), np.abs(p_.dy - s_.dy))[k]
                          for p_, s_, k in zip(plain_res, served_res, m)])
+    del plain_res, served_res
     runs = {"plain": [], "sequential": [], "batched": []}
     for _ in range(repeats):
         for name, fn in (("plain", lambda: one_at_a_time(plain_ctx)),
@@ -314,26 +488,35 @@ def serving_measure(ar, scenes, reqs, device, slots=4, rate=None, repeats=3):
     seq_ctx.close()
     med = {k: float(np.median(v)) for k, v in runs.items()}
     cap = len(reqs) / med["batched"]
-    rate = rate or 0.7 * cap
-    rng = np.random.default_rng(1)
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
-    t0 = time.perf_counter()
-    tickets = []
-    for (n, kw), at in zip(reqs, arrivals):
-        dt = at - (time.perf_counter() - t0)
-        if dt > 0:
-            time.sleep(dt)
-        tickets.append(ar.submit(*scenes[n][:2], secondary_valid=scenes[n][2], ctx=ctx, **kw))
-    lat = []
-    for t in tickets:
-        t.wait()
-        q, r = t.times()
-        lat.append(q + r)
-    stream_s = time.perf_counter() - t0
-    del tickets
-    ctx.close()
     total = float(sum(points))
-    return {"requests": len(reqs), "points": int(total), "slots": slots, "repeats": repeats,
+    sweep = []
+    for i, rate in enumerate(rates):
+        rng = np.random.default_rng(seed + i)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+        t0 = time.perf_counter()
+        tickets = []
+        for (n, kw), at in zip(reqs, arrivals):
+            dt = at - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            tickets.append(ar.submit(*scenes[n][:2], secondary_valid=scenes[n][2], ctx=ctx, **kw))
+        lat, big = [], []
+        for (n, _), t in zip(reqs, tickets):
+            t.wait()
+            q, r = t.times()
+            lat.append(q + r)
+            if n == max(scenes):
+                big.append(q + r)
+        stream_s = time.perf_counter() - t0
+        del tickets
+        sweep.append({"rate_pairs_per_s": rate, "p50_ms": float(np.percentile(lat, 50)),
+                      "p99_ms": float(np.percentile(lat, 99)),
+                      "largest_pairs_p50_ms": float(np.percentile(big, 50)) if big else None,
+                      "points_per_s": total / stream_s, "seconds": stream_s})
+    ctx.close()
+    counts = {str(n): sum(1 for m_, _ in reqs if m_ == n) for n in sorted(scenes)}
+    return {"requests": len(reqs), "requests_per_side": counts, "points": int(total),
+            "slots": slots, "repeats": repeats,
             "plain_points_per_s": total / med["plain"],
             "plain_path": "one pair at a time, direct FP32 correlation on CUDA cores "
                           "(AR_OPT_TENSOR_CORES = 0)",
@@ -345,8 +528,7 @@ def serving_measure(ar, scenes, reqs, device, slots=4, rate=None, repeats=3):
             "matched_accuracy": {"points_compared": int(dd.size),
                                  "dx_dy_within_1e-3px": float(np.mean(dd <= 1e-3))
                                  if dd.size else None},
-            "stream_rate_pairs_per_s": rate, "stream_points_per_s": total / stream_s,
-            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
+            "sweep": sweep}
 
 
 def oracle_sample(ar, ctx, raw, opts, grid, size, seed=1):
@@ -387,7 +569,8 @@ def oracle_sample(ar, ctx, raw, opts, grid, size, seed=1):
 ROT_ANGLES = (-3.0, 0.0, 3.0)  # RotationSearch()'s default, src/types.jl:557
 
 
-def rotation_measure(ar, ctx, raw, opts, grid, args, dev, stream, flush, fp32_peak, rank, world):
+def rotation_measure(ar, ctx, raw, opts, grid, args, dev, stream, flush, fp32_peak, rank, world,
+                     size):
     """The rotation search (src/track.jl:313-409) over the fine level's point set: every grid
     point at chip 32 / radius 25 with RotationSearch() (angles -3, 0, 3), on the prepared pair,
     PyramidRefine(64). Device-timed like the main step, beside the same pass without rotation,
@@ -443,8 +626,8 @@ def rotation_measure(ar, ctx, raw, opts, grid, args, dev, stream, flush, fp32_pe
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             from oracle import oracle as O
             O.build()
-            ref, sec = (np.empty((args.size, args.size), np.uint8, order="F") for _ in range(2))
-            rv, sv = (np.empty((args.size, args.size), np.uint8, order="F") for _ in range(2))
+            ref, sec = (np.empty((size, size), np.uint8, order="F") for _ in range(2))
+            rv, sv = (np.empty((size, size), np.uint8, order="F") for _ in range(2))
             ctx.check(lib.ar_pair_download(ctx.handle, prep, ref.ctypes.data, sec.ctypes.data,
                                            rv.ctypes.data, sv.ctypes.data))
             idx = np.linspace(0, n - 1, 10000).astype(np.int64)
@@ -480,6 +663,86 @@ def rotation_measure(ar, ctx, raw, opts, grid, args, dev, stream, flush, fp32_pe
             "cpu_baseline": cpu, "gpu_launches_per_pass": r["launches_per_pass"]}
 
 
+class DeviceStep:
+    """One step of the pipeline on a device-resident raw pair and grid: ar_prepare, then
+    ar_multichip_device, on the context's stream."""
+
+    def __init__(self, ar, ctx, torch, dev, a, b, valid, p):
+        L = ar._lib
+        self.ctx, self.lib = ctx, ctx.lib
+        self.grid = ar.build_grid(a.shape, p)
+        self.gr, self.gc = self.grid.shape
+        self.n = self.gr * self.gc
+        self.raw = ar.ImagePair(a, b, None, valid).device(ctx)  # resident before timing
+        self.cols = {f: torch.from_numpy(self.grid.flat(f)).to(dev) for f in ar.points.FIELDS}
+        self.dgrid = L.ArPoints(*(self.cols[f].data_ptr() for f in ar.points.FIELDS), self.n)
+        self.outs = [torch.empty(self.n, dtype=torch.float32, device=dev) for _ in range(3)]
+        self.ochip = torch.empty(self.n, dtype=torch.int16, device=dev)
+        self.oint = torch.empty(self.n, dtype=torch.uint8, device=dev)
+        self.prm = ar.multichip_params(p)
+        self.opts = ar.prepare_options(p)
+
+    def __call__(self):
+        ctx, lib = self.ctx, self.lib
+        prep = ctypes.c_void_p()
+        ctx.check(lib.ar_prepare(ctx.handle, self.raw.handle, ctypes.byref(self.opts),
+                                 ctypes.byref(prep)))
+        try:
+            ctx.check(lib.ar_multichip_device(
+                ctx.handle, prep, ctypes.byref(self.dgrid), self.gr, self.gc,
+                ctypes.byref(self.prm), self.outs[0].data_ptr(), self.outs[1].data_ptr(),
+                self.outs[2].data_ptr(), self.ochip.data_ptr(), self.oint.data_ptr(), None))
+        finally:
+            lib.ar_pair_destroy(prep)
+
+
+def timed_steps(torch, step, stream, flush, steps, warmup, dist=None):
+    """Device time (ms, summed over `steps`) of `step`, CUDA events on the library's stream,
+    L2 flushed before every step (outside the timed interval)."""
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            flush.fill_(1)
+            step()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        total = 0.0
+        for _ in range(steps):
+            flush.fill_(1)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            step()
+            e.record(stream)
+            e.synchronize()
+            total += s.elapsed_time(e)
+        torch.cuda.synchronize()
+    return total
+
+
+def host_e2e(ar, ctx, hostpair, hgrid, gr, gc, opts, prm, size, n, reps):
+    """One pair at a time through the C ABI from host buffers: ar_pair_upload + ar_prepare +
+    ar_multichip (results read back to host memory); seconds per pair, the outputs of the last."""
+    L, lib = ar._lib, ctx.lib
+    ha, hb, hv = hostpair
+    hout = [np.empty(n, np.float32) for _ in range(3)]
+    hchip = np.empty(n, np.uint16)
+    hint = np.empty(n, np.uint8)
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        rp, pp = ctypes.c_void_p(), ctypes.c_void_p()
+        ctx.check(lib.ar_pair_upload(ctx.handle, ha.ctypes.data, hb.ctypes.data, None,
+                                     hv.ctypes.data, size, size, L.AR_U16, ctypes.byref(rp)))
+        ctx.check(lib.ar_prepare(ctx.handle, rp, ctypes.byref(opts), ctypes.byref(pp)))
+        ctx.check(lib.ar_multichip(ctx.handle, pp, ctypes.byref(hgrid), gr, gc, ctypes.byref(prm),
+                                   hout[0].ctypes.data, hout[1].ctypes.data, hout[2].ctypes.data,
+                                   hchip.ctypes.data, hint.ctypes.data))
+        lib.ar_pair_destroy(pp)
+        lib.ar_pair_destroy(rp)
+        times.append(time.perf_counter() - t0)
+    return times, hout, hchip
+
+
 def gpu_arm(args):
     import torch
     import __graft_entry__ as ge
@@ -497,56 +760,21 @@ def gpu_arm(args):
     ar = ge.load_package()
     L = ar._lib
     ctx = L.Context(local)
-    lib = ctx.lib
     a, b, valid = scene(ar, args.size)
     p = pipeline_params(ar, args.spacing if args.profile else SPACING)
-    grid = ar.build_grid(a.shape, p)
-    gr, gc = grid.shape
-    n = gr * gc
     dev = torch.device("cuda", local)
-    raw = ar.ImagePair(a, b, None, valid).device(ctx)  # resident before timing
-    cols = {f: torch.from_numpy(grid.flat(f)).to(dev) for f in ar.points.FIELDS}
-    dgrid = L.ArPoints(*(cols[f].data_ptr() for f in ar.points.FIELDS), n)
-    outs = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3)]
-    ochip = torch.empty(n, dtype=torch.int16, device=dev)
-    oint = torch.empty(n, dtype=torch.uint8, device=dev)
-    prm = ar.multichip_params(p)
-    opts = ar.prepare_options(p)
+    step = DeviceStep(ar, ctx, torch, dev, a, b, valid, p)
+    grid, gr, gc, n = step.grid, step.gr, step.gc, step.n
+    raw, opts, prm = step.raw, step.opts, step.prm
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
     torch.cuda.synchronize()
 
-    def step():
-        prep = ctypes.c_void_p()
-        ctx.check(lib.ar_prepare(ctx.handle, raw.handle, ctypes.byref(opts), ctypes.byref(prep)))
-        try:
-            ctx.check(lib.ar_multichip_device(
-                ctx.handle, prep, ctypes.byref(dgrid), gr, gc, ctypes.byref(prm),
-                outs[0].data_ptr(), outs[1].data_ptr(), outs[2].data_ptr(), ochip.data_ptr(),
-                oint.data_ptr(), None))
-        finally:
-            lib.ar_pair_destroy(prep)
-
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            flush.fill_(1)
-            step()
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        ctx.set_timing(True)
-        ctx.kernel_times()
-        total_ms = 0.0
-        with ClockSampler(local) as clk:
-            for _ in range(args.steps):
-                flush.fill_(1)  # L2 flush outside the timed interval of each step
-                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                s.record(stream)
-                step()
-                e.record(stream)
-                e.synchronize()
-                total_ms += s.elapsed_time(e)
-        torch.cuda.synchronize()
+    timed_steps(torch, step, stream, flush, 0, args.warmup, dist)
+    ctx.set_timing(True)
+    ctx.kernel_times()
+    with ClockSampler(local) as clk:
+        total_ms = timed_steps(torch, step, stream, flush, args.steps, 0, dist)
     corr_ms, refine_ms, tracks, launches, corr_flops = ctx.kernel_times()
     ctx.set_timing(False)
     if dist:
@@ -554,46 +782,9 @@ def gpu_arm(args):
     total_ms, value = replicas_rate(dist, total_ms, n, args.steps, dev)
     ms_per_step = total_ms / args.steps
 
-    dx = outs[0].cpu().numpy()
-    chip = ochip.cpu().numpy().view(np.uint16)
+    dx = step.outs[0].cpu().numpy()
+    chip = step.ochip.cpu().numpy().view(np.uint16)
     resolved = int(np.count_nonzero(chip))
-
-    # The plain GPU path on the same step: the direct FP32 correlation on CUDA cores (tensor
-    # cores off), one pair at a time, timed the same way; and its agreement with the results
-    # above (integer peaks are identical -- both numerators are exact for UInt8 -- so dx/dy
-    # agree to the bit).
-    plain = None
-    if not args.profile:
-        ctx.set_option(L.AR_OPT_TENSOR_CORES, 0)
-        psteps = max(3, args.steps // 4)
-        with torch.cuda.stream(stream):
-            flush.fill_(1)
-            step()
-            torch.cuda.synchronize()
-            ptot = 0.0
-            for _ in range(psteps):
-                flush.fill_(1)
-                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                s.record(stream)
-                step()
-                e.record(stream)
-                e.synchronize()
-                ptot += s.elapsed_time(e)
-        ctx.set_option(L.AR_OPT_TENSOR_CORES, 1)
-        ptot, prate = replicas_rate(dist, ptot, n, psteps, dev)
-        pdx = outs[0].cpu().numpy()
-        plain = {"points_per_s": prate, "ms_per_step": ptot / psteps, "steps": psteps,
-                 "path": "the same step with AR_OPT_TENSOR_CORES = 0: the direct FP32 "
-                         "correlation on CUDA cores (k_corr), one pair at a time",
-                 "speedup": value / prate,
-                 "identical_dx": bool(np.array_equal(pdx.view(np.uint32), dx.view(np.uint32)))}
-    levels = {int(c): int(np.count_nonzero(chip == c)) for c in np.unique(chip) if c}
-    med_dx = float(np.nanmedian(dx)) if resolved else float("nan")
-
-    # Roofline of the dominant kernel (the tensor-core correlation, k_corr_tc): algorithmic
-    # operations counted by the kernel (2 * chip area * surface area per searched point, the
-    # reference's direct numerator) over the event-timed duration of the step's correlation
-    # launches, against the measured dense bf16 tensor rate.
     achieved = corr_flops / (corr_ms * 1e-3) / 1e12 if corr_ms > 0 else None
     if args.profile:
         if rank == 0:
@@ -603,84 +794,105 @@ def gpu_arm(args):
         if dist:
             dist.destroy_process_group()
         return
+
+    # The plain GPU path on the same step: the direct FP32 correlation on CUDA cores (tensor
+    # cores off), one pair at a time, timed the same way; and its agreement with the results
+    # above (both numerators are exact for UInt8, so dx agrees to the bit).
+    ctx.set_option(L.AR_OPT_TENSOR_CORES, 0)
+    psteps = 3
+    ptot = timed_steps(torch, step, stream, flush, psteps, 1, dist)
+    ctx.set_option(L.AR_OPT_TENSOR_CORES, 1)
+    ptot, prate = replicas_rate(dist, ptot, n, psteps, dev)
+    pdx = step.outs[0].cpu().numpy()
+    plain = {"points_per_s": prate, "ms_per_step": ptot / psteps, "steps": psteps,
+             "path": "the same step with AR_OPT_TENSOR_CORES = 0: the direct FP32 "
+                     "correlation on CUDA cores (k_corr), one pair at a time",
+             "speedup": value / prate,
+             "identical_dx": bool(np.array_equal(pdx.view(np.uint32), dx.view(np.uint32)))}
+    levels = {int(c): int(np.count_nonzero(chip == c)) for c in np.unique(chip) if c}
+    med_dx = float(np.nanmedian(dx)) if resolved else float("nan")
+
     fp32_peak = measure_fp32_peak(torch, dev)
     eval_flops = 2.0 * CHIP * CHIP * (2 * RADIUS) ** 2
     fine_points = corr_flops / max(tracks, 1) / eval_flops  # chip-32 evaluations per launch
 
     # End to end through the C ABI from host buffers: the caller's column-major arrays (the
     # Julia layout) and grid, pair upload, prepare, multichip, download; per-pair latency.
-    ha = np.asfortranarray(a)
-    hb = np.asfortranarray(b)
-    hv = np.asfortranarray(valid.astype(np.uint8))
+    hostpair = (np.asfortranarray(a), np.asfortranarray(b),
+                np.asfortranarray(valid.astype(np.uint8)))
     hcols = {f: np.ascontiguousarray(grid.flat(f)) for f in ar.points.FIELDS}
     hgrid = L.ArPoints(*(hcols[f].ctypes.data for f in ar.points.FIELDS), n)
-    hout = [np.empty(n, np.float32) for _ in range(3)]
-    hchip = np.empty(n, np.uint16)
-    hint = np.empty(n, np.uint8)
-    e2e_times = []
-    for it in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        rp, pp = ctypes.c_void_p(), ctypes.c_void_p()
-        ctx.check(lib.ar_pair_upload(ctx.handle, ha.ctypes.data, hb.ctypes.data, None,
-                                     hv.ctypes.data, args.size, args.size, L.AR_U16,
-                                     ctypes.byref(rp)))
-        ctx.check(lib.ar_prepare(ctx.handle, rp, ctypes.byref(opts), ctypes.byref(pp)))
-        ctx.check(lib.ar_multichip(ctx.handle, pp, ctypes.byref(hgrid), gr, gc, ctypes.byref(prm),
-                                   hout[0].ctypes.data, hout[1].ctypes.data, hout[2].ctypes.data,
-                                   hchip.ctypes.data, hint.ctypes.data))
-        lib.ar_pair_destroy(pp)
-        lib.ar_pair_destroy(rp)
-        t1 = time.perf_counter()
-        if it >= args.warmup:
-            e2e_times.append(t1 - t0)
+    e2e_times, hout, hchip = host_e2e(ar, ctx, hostpair, hgrid, gr, gc, opts, prm, args.size, n,
+                                      args.warmup + min(args.steps, 10))
+    e2e_times = e2e_times[args.warmup:]
     e2e_value = world * n / float(np.mean(e2e_times))
-    served = served_e2e(ar, local, ha, hb, hv, hgrid, gr, gc, opts, prm, args.size, n,
-                        pairs=args.steps, ref_dx=dx)
-    h2d = ha.nbytes + hb.nbytes + hv.nbytes + 6 * 8 * n
-    d2h = n * (4 + 4 + 4 + 2 + 1)
     same = bool(np.array_equal(hchip, chip)) and bool(
         np.array_equal(hout[0].view(np.uint32), dx.view(np.uint32)))
+    # The plain path end to end, one pair at a time from host buffers (tensor cores off).
+    ctx.set_option(L.AR_OPT_TENSOR_CORES, 0)
+    pe_times, _, _ = host_e2e(ar, ctx, hostpair, hgrid, gr, gc, opts, prm, args.size, n, 3)
+    ctx.set_option(L.AR_OPT_TENSOR_CORES, 1)
+    plain_e2e = world * n / float(np.mean(pe_times[1:]))
+    served = served_e2e(ar, local, *hostpair, hgrid, gr, gc, opts, prm, args.size, n,
+                        pairs=min(args.steps, 12), ref_dx=dx)
+    h2d = sum(x.nbytes for x in hostpair) + 6 * 8 * n
+    d2h = n * (4 + 4 + 4 + 2 + 1)
 
-    parity = None
+    parity = cpu = crop_check = flips = cv = None
     if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        O.build()
         try:
             parity = oracle_sample(ar, ctx, raw, opts, grid, args.size)
         except Exception as exc:  # reported, not fatal to the main measurement
             parity = {"error": f"{type(exc).__name__}: {exc}"}
+        try:
+            cpu, crop_check, prepared, cropped = crop_parity(ar, ctx, O, a, b, valid, p)
+            flips = float_flip_rate(ar, ctx, O, *cropped)
+            cgrid = ar.build_grid(cropped[0].shape, p)
+            cv = opencv_baseline(ar, {f: cgrid.flat(f) for f in ("x", "y")}, prepared)
+            cv = opencv_agreement(ar, ctx, cv, cgrid, prepared)
+        except Exception as exc:
+            crop_check = {"error": f"{type(exc).__name__}: {exc}"}
+        if world > 1:
+            cpu = None  # the host baseline is a single-process figure
+
+    # The at-scale configuration's 4096^2 pair, timed the same way (device-resident).
+    a4, b4, v4 = scene(ar, N_SCALE)
+    step4 = DeviceStep(ar, ctx, torch, dev, a4, b4, v4, p)
+    t4 = timed_steps(torch, step4, stream, flush, args.steps, args.warmup, dist)
+    t4, v4rate = replicas_rate(dist, t4, step4.n, args.steps, dev)
+    config_4096 = {"workload": workload(N_SCALE, step4.gr, step4.gc), "points": step4.n,
+                   "value": v4rate, "ms_per_step": t4 / args.steps}
 
     rotation = None
     if not args.no_rotation:
         try:
-            rotation = rotation_measure(ar, ctx, raw, opts, grid, args, dev, stream, flush,
-                                        fp32_peak, rank, world)
+            rotation = rotation_measure(ar, ctx, step4.raw, opts, step4.grid, args, dev, stream,
+                                        flush, fp32_peak, rank, world, N_SCALE)
         except Exception as exc:  # reported, not fatal to the main measurement
             rotation = {"error": f"{type(exc).__name__}: {exc}"}
+    del step4
 
     serving = None
     if not args.no_serving:
-        # A short mixed stream (image sides 512, 2048, 4096 in proportion 8:4:2) through the
-        # plain path, the sequential path and the request loop.
+        # The serving configuration's mixed stream (sides 512, 2048, 4096, 10980 in 8:4:2:1)
+        # through the plain path, the sequential path and the request loop, then the Poisson
+        # sweep.
         try:
-            sc, reqs = serving_requests(ar, np.random.default_rng(5), 28, (512, 2048, N),
-                                        (8, 4, 2), base=(a, b, valid))
+            sc, reqs = serving_requests(ar, np.random.default_rng(5), 30,
+                                        (512, 2048, N_SCALE, N), (8, 4, 2, 1),
+                                        base=(a, b, valid))
             serving = serving_measure(ar, sc, reqs, local)
-            serving["workload"] = ("28 requests, sides 512/2048/4096 (8:4:2), spacing {8,16,32}, "
-                                   "chip {16,32,64}, radius U[8,48], PyramidRefine(64); after one "
-                                   "untimed pass of the stream through every path, plain, "
-                                   "sequential and batched passes alternated 3 times (medians); "
-                                   "latency from submission to completion at a Poisson rate of "
-                                   "70% of capacity")
+            serving["workload"] = (
+                f"{len(reqs)} requests, sides 512/2048/4096/10980 (8:4:2:1), spacing "
+                "{8,16,32}, chip {16,32,64}, radius U[8,48], PyramidRefine(64); after one "
+                "untimed pass of the stream through every path, plain, sequential and batched "
+                "passes alternated (medians); then the same requests as a seeded Poisson "
+                f"stream at each of {list(SERVE_RATES)} pairs/s: latency from submission to "
+                "completion")
         except Exception as exc:  # reported, not fatal to the main measurement
             serving = {"error": f"{type(exc).__name__}: {exc}"}
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        from oracle import oracle as O
-        O.build()
-        pts, dt = host_pipeline(O, ar, crop(a, CROP), crop(b, CROP), crop(valid, CROP), p)
-        cpu = {"value": pts / dt, "unit": UNIT, "cores": O.max_threads(), "kind": "port",
-               "sample": f"the same pipeline on a centred {CROP}^2 crop ({pts} grid points), "
-                         f"{dt:.1f} s"}
 
     peaks = measured_peaks()
     if peaks.get("bf16_tflops"):
@@ -696,7 +908,7 @@ def gpu_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "points": n, "grid": [gr, gc],
+            "config": {"workload": workload(args.size, gr, gc), "points": n, "grid": [gr, gc],
                        "resolved": resolved, "points_per_chip_size": levels,
                        "chip": CHIP, "radius": RADIUS, "upsampling": UP,
                        "image": [args.size, args.size], "element_type": "uint16 -> uint8",
@@ -711,6 +923,10 @@ def gpu_arm(args):
                          "achieved_basis": "2 * chip area * surface area per searched point "
                                            "(integer MACs of the exact u8 numerator), summed "
                                            "over the step's correlation launches",
+                         "frac_of_int8_rate": achieved / (2 * tensor_peak) if achieved else None,
+                         "int8_rate_note": "the products are tcgen05.mma kind::i8, whose dense "
+                                           "rate is twice the bf16 rate: frac_of_int8_rate "
+                                           "divides by 2 x peak",
                          "fp32_comparison": {"sgemm_tflops_this_run": fp32_peak,
                                              "frac": achieved / fp32_peak
                                              if (achieved and fp32_peak) else None},
@@ -719,6 +935,7 @@ def gpu_arm(args):
                          "correlation_launches_per_step": tracks / args.steps,
                          "measured_peaks": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops")}},
             "cpu_baseline": cpu,
+            "cpu_baseline_opencv": cv,
             "e2e": {"value": world * served["value"], "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "path": f"ar_submit request loop, {served['slots']} slots: "
@@ -736,7 +953,18 @@ def gpu_arm(args):
                         "path": "ar_pair_upload + ar_prepare + ar_multichip (host buffers), "
                                 "one pair after another"}},
             "plain_gpu_path": plain,
+            "batched_vs_plain": {
+                "served_e2e_points_per_s": world * served["value"],
+                "plain_e2e_points_per_s": plain_e2e,
+                "ratio_e2e": world * served["value"] / plain_e2e,
+                "ratio_device": value / prate, "target": 3.0,
+                "plain_e2e_path": "ar_pair_upload + ar_prepare + ar_multichip from host "
+                                  "buffers with AR_OPT_TENSOR_CORES = 0, one pair at a time "
+                                  "(mean of 2 after 1 warm-up)"},
             "oracle_sample": parity,
+            "oracle_crop": crop_check,
+            "float32_subpixel": flips,
+            "config_4096": config_4096,
             "serving": serving,
             "rotation_search": rotation,
             "clocks": clk.summary(),
@@ -758,7 +986,7 @@ def serve_arm(args):
     ge.build()
     ar = ge.load_package()
     sc, reqs = serving_requests(ar, np.random.default_rng(7), args.steps * 15,
-                                (512, 2048, 4096, 10980), (8, 4, 2, 1))
+                                (512, 2048, N_SCALE, N), (8, 4, 2, 1))
     res = serving_measure(ar, sc, reqs, 0)
     print(json.dumps({"metric": "serving: sustained points/s and p50/p99 pair latency",
                       "value": res["batched_points_per_s"], "unit": UNIT, "n_gpus": 1,
@@ -782,23 +1010,30 @@ def reference_arm(args):
     rates = []
     pts = 0
     for it in range(args.warmup + args.steps):
-        pts, dt = host_pipeline(O, ar, ca, cb, cv, p)
+        pts, dt, _, _ = host_pipeline(O, ar, ca, cb, cv, p)
         if it >= args.warmup:
             rates.append(pts / dt)
     value = float(np.mean(rates))
-    n = len(ar.build_grid(a.shape, p))
+    grid = ar.build_grid(a.shape, p)
+    n = len(grid)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": pts / value * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "points": n, "chip": CHIP, "radius": RADIUS,
-                   "upsampling": UP, "image": [args.size, args.size],
-                   "element_type": "uint16 -> uint8"},
+        "config": {"workload": workload(args.size, *grid.shape), "points": n, "chip": CHIP,
+                   "radius": RADIUS, "upsampling": UP, "image": [args.size, args.size],
+                   "element_type": "uint16 -> uint8",
+                   "same_config": False,
+                   "why_a_crop": f"the whole {args.size}^2 scene ({n} grid points) takes about "
+                                 f"{n / value:.0f} s per step on these cores, so each step is "
+                                 f"the same pipeline on a centred {CROP}^2 crop of it"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": O.max_threads(), "kind": "port",
                          "sample": f"the same pipeline on a centred {CROP}^2 crop ({pts} grid "
                                    "points) per step (Julia is not installed; the C++ "
-                                   "restatement of the reference's algorithm)"},
+                                   "restatement of the reference's algorithm)",
+                         "numerator": "FP64 direct sum; the reference uses single-precision "
+                                      "FFTW (not installed here)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -818,7 +1053,7 @@ def main():
     ap.add_argument("--serve", action="store_true",
                     help="only the serving measurement, on a longer stream with 10980^2 pairs")
     ap.add_argument("--size", type=int, default=N,
-                    help="image side; the benchmark line uses 4096, profiles a smaller scene")
+                    help="image side; the benchmark line uses 10980, profiles a smaller scene")
     ap.add_argument("--profile", action="store_true",
                     help="time the device steps only (for ncu captures); no JSON bench line")
     ap.add_argument("--spacing", type=int, default=SPACING,
