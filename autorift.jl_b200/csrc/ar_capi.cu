@@ -425,6 +425,8 @@ int ar_ctx_destroy(ar_ctx* c) {
         for (auto ev : c->scratch.timer.pool) cudaEventDestroy(ev);
         cudaFree(c->scratch.timer.flops);
         if (c->scratch.done) cudaEventDestroy(c->scratch.done);
+        for (auto ev : c->scratch.tune_ev)
+            if (ev) cudaEventDestroy(ev);
         cudaFree(c->dbuf);
         cudaFree(c->arena);
         if (c->pinned) cudaFreeHost(c->pinned);
@@ -1097,6 +1099,11 @@ int ar_ctx_set_option(ar_ctx* c, int option, int value) {
     std::lock_guard<std::mutex> lk(c->mu);
     switch (option) {
         case AR_OPT_TENSOR_CORES: c->scratch.tensor_cores = value != 0; return AR_OK;
+        case AR_OPT_AUTOTUNE: c->scratch.autotune = value != 0; return AR_OK;
+        case AR_OPT_SPLIT_BF16:
+            if (value < 0 || value > 2) return fail(c, AR_ERR_ARG, "split-BF16 mode must be 0, 1 or 2");
+            c->scratch.split_bf16 = value;
+            return AR_OK;
         case AR_OPT_SERVE_SLOTS:
         case AR_OPT_SERVE_MEMORY_MB: {
             std::lock_guard<std::mutex> sk(c->serve_mu);

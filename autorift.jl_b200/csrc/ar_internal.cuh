@@ -5,6 +5,7 @@
 
 #include <array>
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -89,6 +90,15 @@ struct TrackScratch {
     int* status = nullptr;
     // UInt8 passes use the tensor-core correlation when their geometry fits it.
     bool tensor_cores = true;
+    // UInt16, Int16 and Float32 passes: 0 direct FP32 on CUDA cores, 1 split-BF16 tensor-core
+    // products for chips of 64 px and up, 2 split-BF16 for every chip size (AR_OPT_SPLIT_BF16).
+    int split_bf16 = 1;
+    // UInt8 passes of at least kTuneMinPoints points: the tensor-core and CUDA-core kernels
+    // (identical results) are timed once per pass geometry and the fastest kept in `tuned`
+    // (key: chip and surface extents) -- AR_OPT_AUTOTUNE.
+    bool autotune = true;
+    std::map<uint64_t, int> tuned;
+    cudaEvent_t tune_ev[2] = {nullptr, nullptr};
     // When set, the sub-pixel queue grows from this pool in stream order (no device-wide
     // synchronisation when a context first meets a larger pass).
     cudaMemPool_t pool = nullptr;

@@ -42,6 +42,35 @@ __host__ __device__ constexpr uint32_t idesc_u8_s32(int M, int N) {
            | (static_cast<uint32_t>(M >> 4) << 24);        // M / 16
 }
 
+// Instruction descriptor for kind::f16 with BF16 A and B and an FP32 accumulator, both operands
+// K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
+    return (1u << 4)                                       // D format F32
+           | (1u << 7) | (1u << 10)                        // A, B BF16
+           | (static_cast<uint32_t>(N >> 3) << 17)         // N / 8
+           | (static_cast<uint32_t>(M >> 4) << 24);        // M / 16
+}
+
+// D (+)= A * B^T for BF16 operands (kind::f16, K = 16 elements), descriptors as 32-bit halves;
+// `accumulate` 0 overwrites D.
+__device__ __forceinline__ void mma_bf16_halves(uint32_t d_tmem, uint32_t a_lo, uint32_t a_hi,
+                                                uint32_t b_lo, uint32_t b_hi, uint32_t idesc,
+                                                uint32_t accumulate) {
+    asm volatile(
+        "{\n\t"
+        ".reg .b64 da, db;\n\t"
+        ".reg .pred p;\n\t"
+        "mov.b64 da, {%1, %2};\n\t"
+        "mov.b64 db, {%3, %4};\n\t"
+        "setp.ne.b32 p, %6, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], da, db, %5, {%7, %7, %7, %7}, p;\n\t"
+        "}\n"
+        :
+        : "r"(d_tmem), "r"(a_lo), "r"(a_hi), "r"(b_lo), "r"(b_hi), "r"(idesc), "r"(accumulate),
+          "r"(0u)
+        : "memory");
+}
+
 // D (+)= A * B^T, issued by one thread.
 __device__ __forceinline__ void mma_u8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc,
                                        uint32_t idesc, bool accumulate) {

@@ -21,6 +21,7 @@
 //    fl(0.5*fl(b+c)) with __fmul_rn/__fadd_rn, so no step is fused into an FMA and the result
 //    is bit-identical to the reference's Float32 arithmetic on the same patch.
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -2263,6 +2264,443 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
 }
 
 // ----------------------------------------------------------------------------------------------
+// Split-BF16 tensor-core correlation for UInt16, Int16 and Float32 imagery (k_corr_bf).
+//
+// The numerator of the CUDA-core kernel, sum_{a,b} C'[a, b] W'[i + a, j + b], with C' the chip of
+// prepare_chip! (src/correlate.jl:423-453: Float32(x - mean)) and W' the window shifted by the
+// same centring constant k_corr uses (Float32(w - cshift); num = sum C' W' + cshift sum C'),
+// as products on the tensor cores (tcgen05.mma kind::f16, BF16 operands, FP32 accumulators in
+// Tensor Memory). Each operand is split into two BF16 limbs, v = hi + lo with hi = bf16(v) and
+// lo = bf16(v - hi), and the numerator is the sum of the three products hi*hi + hi*lo + lo*hi:
+// about 16 significant bits per operand, exact for the integer windows of UInt16 and Int16
+// imagery (an integer below 2^16 in magnitude is the sum of two BF16 values).
+//
+// Layout (as the UInt8 kernels, with 2-byte elements and one chip column per product):
+//   A[j, (q, b, r)] = W'[16 q + r, j + b]    r < 16, stored as two 8-row halves h:
+//                                            s_W[limb][q][h][x] (16 bytes), row j of A 16 bytes
+//                                            after row j - 1, the halves LBO apart;
+//   B[i, (q, b, r)] = E_b[i - 16 q][r]       E_b[u][r] = C'[r - u, b], stored s_E[limb][b][h][e].
+// Block q meets surface rows [16 q - ch + 1, 16 q + 15]: NB = 16 ceil((ch + 15) / 16) operand rows,
+// surface row i in accumulator column i (rows trimmed to 0 <= i < nr in steps of 16). Six
+// threads issue the products -- the three limb pairs, each for even and odd chip columns into an
+// accumulator of its own -- and the epilogue adds the six in FP32.
+// The chip columns come in chunks of BC (the window columns a chunk reaches are staged with
+// it). Box sums (integral_both!, boxsum, src/integral.jl:141-170, 244-247) are FP64 from the
+// image values, the normalisation the reference's FP64 formula (src/correlate.jl:575-630), each
+// surface value computed from its FP32 numerator. Surfaces up to 64 x 64.
+
+constexpr int kBfThreads = 256;
+constexpr int kBfAcc = 6;          // accumulators: limb pair (3) x chip-column parity (2)
+constexpr int kBfPadL = 16;        // zero elements before each staged chip column
+
+struct BfArgs {
+    const void* ref;
+    const void* sec;
+    const uint8_t* valid;
+    int64_t nrows, ncols;
+    DevPoints pts;
+    int64_t padx, pady;
+    int up, measure;
+    int CHM, CWM, NRM, NCM;
+    int NB;                          // chip operand rows per column (multiple of 16)
+    int QB;                          // window blocks of 16 rows
+    int BC;                          // chip columns per chunk (even)
+    int XC;                          // window columns staged per chunk (>= BC + 63)
+    int PC;                          // staged chip column length (elements, even)
+    int NRS;                         // box-sum and surface row stride
+    int AC;                          // columns per accumulator (multiple of 16)
+    int VR;                          // rows of column sums per box-sum chunk
+    unsigned off_W, off_E, off_P, off_S1, off_S2, off_red;
+    uint32_t tmem_cols;
+    DevOutputs out;
+    int* sub_count;
+    int64_t* sub_point;
+    int32_t* sub_origin;
+    float* sub_patch;
+    float* surf_out;
+    unsigned long long* flops;
+    int* status;
+};
+
+// The two BF16 limbs of v, as raw 16-bit patterns: hi = bf16(v), lo = bf16(v - hi).
+__device__ __forceinline__ void bf16_split(float v, uint32_t* hi, uint32_t* lo) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    const __nv_bfloat16 l = __float2bfloat16_rn(__fsub_rn(v, __bfloat162float(h)));
+    *hi = static_cast<uint32_t>(__bfloat16_as_ushort(h));
+    *lo = static_cast<uint32_t>(__bfloat16_as_ushort(l));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
+    typedef Traits<T> Tr;
+    extern __shared__ __align__(1024) unsigned char smem_bf[];
+    __shared__ uint64_t s_mbar;
+    __shared__ uint32_t s_taddr;
+    __shared__ int s_slot;
+    const int tid = threadIdx.x, bd = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const T* ref = static_cast<const T*>(A.ref);
+    const T* sec = static_cast<const T*>(A.sec);
+    // Operand buffers, two limbs each: window [limb][q][h][x], chip operand [limb][b][h][e],
+    // staged chip columns [limb][b][PC] (raw BF16 bits). Box sums S1, S2 [j][NRS] (FP64).
+    unsigned char* s_W = smem_bf + A.off_W;
+    unsigned char* s_E = smem_bf + A.off_E;
+    uint16_t* s_P = reinterpret_cast<uint16_t*>(smem_bf + A.off_P);
+    double* s_S1 = reinterpret_cast<double*>(smem_bf + A.off_S1);
+    double* s_S2 = reinterpret_cast<double*>(smem_bf + A.off_S2);
+    double* s_red = reinterpret_cast<double*>(smem_bf + A.off_red);
+    float* s_surf = reinterpret_cast<float*>(smem_bf + A.off_W);  // after the products
+    double* s_V = reinterpret_cast<double*>(smem_bf + A.off_W);   // box-sum column sums
+    const size_t wlimb = static_cast<size_t>(A.QB) * 2 * A.XC * 16;
+    const size_t elimb = static_cast<size_t>(A.BC) * 2 * A.NB * 16;
+    const int plimb = A.BC * A.PC;
+    const int64_t NR = A.nrows + 2 * A.pady, NC = A.ncols + 2 * A.padx;
+    const double shx = static_cast<double>(A.padx) + 0.5;
+    const double shy = static_cast<double>(A.pady) + 0.5;
+
+    if (warp == 0) {
+        tc::tmem_alloc(&s_taddr, A.tmem_cols);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0) {
+        tc::mbar_init(&s_mbar, kBfAcc);  // one commit per issuing thread
+        tc::fence_mbar_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t taddr = s_taddr;
+    uint32_t phase = 0;
+    bool failed = false;
+
+    for (int64_t k = blockIdx.x; k < A.pts.n; k += gridDim.x) {
+        tc::fence_before_sync();
+        __syncthreads();  // the previous point's buffers and accumulators are no longer read
+        tc::fence_after_sync();
+        const int64_t prx = A.pts.rx[k], pry = A.pts.ry[k];
+        if (!(prx > 0 && pry > 0)) continue;
+        const double xs = A.pts.x[k] + shx, ys = A.pts.y[k] + shy;
+        const int64_t hx = A.pts.csx[k] / 2, hy = A.pts.csy[k] / 2;
+        const int64_t ccx = static_cast<int64_t>(floor(__dsub_rn(xs, A.pts.dx0[k])));
+        const int64_t ccy = static_cast<int64_t>(floor(__dsub_rn(ys, A.pts.dy0[k])));
+        const int64_t wcx = static_cast<int64_t>(floor(xs)), wcy = static_cast<int64_t>(floor(ys));
+        const int64_t cr0 = ccy - hy, cr1 = ccy + hy - 1, cc0 = ccx - hx, cc1 = ccx + hx - 1;
+        const int64_t wr0 = wcy - hy - pry, wr1 = wcy + hy + pry - 2;
+        const int64_t wc0 = wcx - hx - prx, wc1 = wcx + hx + prx - 2;
+        const bool chip_in = (cr1 < cr0 || cc1 < cc0) ||
+                             (cr0 >= 1 && cr1 <= NR && cc0 >= 1 && cc1 <= NC);
+        const bool win_in = (wr1 < wr0 || wc1 < wc0) ||
+                            (wr0 >= 1 && wr1 <= NR && wc0 >= 1 && wc1 <= NC);
+        if (!chip_in || !win_in) continue;
+        const int ch = static_cast<int>(2 * hy), cw = static_cast<int>(2 * hx);
+        const int nr = static_cast<int>(2 * pry), nc = static_cast<int>(2 * prx);
+        if (ch <= 0 || cw <= 0) continue;
+        if (ch > A.CHM || cw > A.CWM || nr > A.NRM || nc > A.NCM || nr > 64 || nc > 64) continue;
+        const int64_t chip_r = cr0 - 1 - A.pady, chip_c = cc0 - 1 - A.padx;
+        const int64_t win_r = wr0 - 1 - A.pady, win_c = wc0 - 1 - A.padx;
+
+        // _any_valid over the chip (src/track.jl:416-421).
+        int any = 0;
+        for (int e = tid; e < ch * cw; e += bd) {
+            const int64_t r = chip_r + e % ch, c = chip_c + e / ch;
+            if (r >= 0 && r < A.nrows && c >= 0 && c < A.ncols && A.valid[r + c * A.nrows]) any = 1;
+        }
+        if (!__syncthreads_or(any)) continue;
+        if (tid == 0) A.out.searched[k] = 1;
+
+        // prepare_chip! as the CUDA-core kernel: FP64 mean, FP64 sum of squares of the
+        // deviations, FP64 sum of the Float32-rounded deviations.
+        double st[1] = {0.0};
+        for (int e = tid; e < ch * cw; e += bd)
+            st[0] = __dadd_rn(st[0], pixel(sec, A.nrows, A.ncols, chip_r + e % ch, chip_c + e / ch));
+        block_sum_f64<1>(st, s_red);
+        const double nn = static_cast<double>(ch * cw);
+        const double mean = __ddiv_rn(st[0], nn);
+        const int chp = (ch + kUA - 1) & ~(kUA - 1);
+        double acc2[2] = {0.0, 0.0};
+        for (int e = tid; e < chp * cw; e += bd) {
+            const int a = e % chp, b = e / chp;
+            if (a < ch) {
+                const double d = __dsub_rn(pixel(sec, A.nrows, A.ncols, chip_r + a, chip_c + b), mean);
+                acc2[0] = __dadd_rn(acc2[0], __dmul_rn(d, d));
+                acc2[1] = __dadd_rn(acc2[1], static_cast<double>(__double2float_rn(d)));
+            }
+        }
+        block_sum_f64<2>(acc2, s_red);
+        const double sq = acc2[0], sumd = acc2[1];
+        if (!(sq > __dmul_rn(__dmul_rn(DBL_EPSILON, static_cast<double>(ch)), static_cast<double>(cw))))
+            continue;  // degenerate chip: searched, no measurement (src/track.jl:286)
+        const double cnorm = __dsqrt_rn(sq);
+        const double cshift = Tr::integer ? rint(mean) : static_cast<double>(__double2float_rn(mean));
+        if (tid == 0 && !(A.up == 1 || nr < 5 || nc < 5)) s_slot = atomicAdd(A.sub_count, 1);
+
+        // Box sums in FP64 from the image values: column sums V of ch rows (a thread per window
+        // column, sliding down), in chunks of VR surface rows, then row sums of cw columns.
+        const int XW = cw + nc - 1;
+        double h1 = 0.0, h2 = 0.0;
+        if (tid < XW) {
+            for (int a = 0; a < ch; ++a) {
+                const double w = pixel(ref, A.nrows, A.ncols, win_r + a, win_c + tid);
+                h1 = __dadd_rn(h1, w);
+                h2 = __dadd_rn(h2, __dmul_rn(w, w));
+            }
+        }
+        for (int i0 = 0; i0 < nr; i0 += A.VR) {
+            const int i1 = min(nr, i0 + A.VR);
+            if (tid < XW) {
+                for (int i = i0; i < i1; ++i) {
+                    s_V[2 * ((i - i0) * XW + tid)] = h1;
+                    s_V[2 * ((i - i0) * XW + tid) + 1] = h2;
+                    if (i + 1 < nr) {
+                        const double wo = pixel(ref, A.nrows, A.ncols, win_r + i, win_c + tid);
+                        const double wn = pixel(ref, A.nrows, A.ncols, win_r + i + ch, win_c + tid);
+                        h1 = __dadd_rn(__dsub_rn(h1, wo), wn);
+                        h2 = __dadd_rn(__dsub_rn(h2, __dmul_rn(wo, wo)), __dmul_rn(wn, wn));
+                    }
+                }
+            }
+            __syncthreads();
+            // Row sums: a task is a surface row and 16 columns j, sliding along V's row.
+            const int jseg = (nc + 15) >> 4;
+            for (int task = tid; task < (i1 - i0) * jseg; task += bd) {
+                const int il = task % (i1 - i0), sg = task / (i1 - i0);
+                const int j0 = 16 * sg, j1 = min(nc, j0 + 16);
+                const double* vr = s_V + 2 * il * XW;
+                double g1 = 0.0, g2 = 0.0;
+                for (int b = 0; b < cw; ++b) {
+                    g1 = __dadd_rn(g1, vr[2 * (j0 + b)]);
+                    g2 = __dadd_rn(g2, vr[2 * (j0 + b) + 1]);
+                }
+                for (int j = j0; j < j1; ++j) {
+                    s_S1[j * A.NRS + i0 + il] = g1;
+                    s_S2[j * A.NRS + i0 + il] = g2;
+                    if (j + 1 < j1) {
+                        g1 = __dadd_rn(__dsub_rn(g1, vr[2 * j]), vr[2 * (j + cw)]);
+                        g2 = __dadd_rn(__dsub_rn(g2, vr[2 * j + 1]), vr[2 * (j + cw) + 1]);
+                    }
+                }
+            }
+            __syncthreads();
+        }
+
+        // Clear the accumulators (one lane quarter per warp).
+        if (warp < 4) {
+            uint32_t z[16];
+#pragma unroll
+            for (int t = 0; t < 16; ++t) z[t] = 0u;
+            const uint32_t lq = taddr + (static_cast<uint32_t>(32 * warp) << 16);
+            for (int c = 0; c < kBfAcc * A.AC; c += 16) tc::tmem_st16(lq + static_cast<uint32_t>(c), z);
+            tc::tmem_wait_st();
+        }
+
+        const int QB = (ch + nr - 1 + 15) / 16;
+        const int nchunk = (cw + A.BC - 1) / A.BC;
+        bool ok = true;
+        for (int cc = 0; cc < nchunk && ok; ++cc) {
+            const int b0 = cc * A.BC, bcn = min(A.BC, cw - b0);
+            if (cc > 0) {
+                // The previous chunk's products must be done before its operands are replaced.
+                ok = tc::mbar_wait(&s_mbar, phase, kTcWaitPolls);
+                phase ^= 1u;
+                if (__syncthreads_or(!ok)) break;
+                tc::fence_after_sync();
+            }
+            // The chunk's chip columns C'[a, b0 + bl] as BF16 limbs, zero-padded.
+            for (int e = tid; e < A.BC * A.PC; e += bd) {
+                const int bl = e / A.PC, t = e - bl * A.PC;
+                const int a = t - kBfPadL;
+                uint32_t hi = 0u, lo = 0u;
+                if (bl < bcn && a >= 0 && a < ch) {
+                    const double d = __dsub_rn(pixel(sec, A.nrows, A.ncols, chip_r + a, chip_c + b0 + bl), mean);
+                    bf16_split(__double2float_rn(d), &hi, &lo);
+                }
+                s_P[e] = static_cast<uint16_t>(hi);
+                s_P[plimb + e] = static_cast<uint16_t>(lo);
+            }
+            // Window blocks: item (x, q, h) = 8 consecutive rows of window column b0 + x, both
+            // limbs; consecutive threads take consecutive row groups of one column.
+            const int gpc = 2 * QB;  // row groups per column
+            for (int it = tid; it < A.XC * gpc; it += bd) {
+                const int x = it / gpc, g = it - x * gpc;
+                const int q = g >> 1, h = g & 1;
+                uint32_t hw[4] = {0, 0, 0, 0}, lw[4] = {0, 0, 0, 0};
+                if (x < bcn + nc - 1) {
+                    const int64_t c = win_c + b0 + x;
+                    const int64_t r0 = win_r + 16 * q + 8 * h;
+#pragma unroll
+                    for (int t = 0; t < 8; ++t) {
+                        const int a = 16 * q + 8 * h + t;  // window row
+                        uint32_t hi = 0u, lo = 0u;
+                        if (a < ch + nr - 1) {
+                            const double w = pixel(ref, A.nrows, A.ncols, r0 + t, c);
+                            bf16_split(__double2float_rn(__dsub_rn(w, cshift)), &hi, &lo);
+                        }
+                        hw[t >> 1] |= hi << (16 * (t & 1));
+                        lw[t >> 1] |= lo << (16 * (t & 1));
+                    }
+                }
+                const size_t o = (static_cast<size_t>(q * 2 + h) * A.XC + x) * 16;
+                *reinterpret_cast<uint4*>(s_W + o) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                *reinterpret_cast<uint4*>(s_W + wlimb + o) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+            }
+            __syncthreads();  // s_P complete
+            // Chip operand rows: E_b[h][e] = 8 elements of the staged column from element
+            // kBfPadL + 8 h - e + NB - 16 (C'[r - u, b] with u = e - NB + 16, r = 8 h + t).
+            for (int it = tid; it < A.BC * 2 * A.NB; it += bd) {
+                const int bl = it / (2 * A.NB), rem = it - bl * 2 * A.NB;
+                const int h = rem / A.NB, e = rem - h * A.NB;
+                const int src = kBfPadL + 8 * h - e + A.NB - 16;  // element index, >= 1
+                const size_t o = (static_cast<size_t>(bl * 2 + h) * A.NB + e) * 16;
+#pragma unroll
+                for (int limb = 0; limb < 2; ++limb) {
+                    const uint16_t* col = s_P + limb * plimb + bl * A.PC;
+                    const uint32_t* w = reinterpret_cast<const uint32_t*>(col + (src & ~1));
+                    const uint32_t sh = (src & 1) ? 16u : 0u;
+                    uint4 v;
+                    v.x = __funnelshift_r(w[0], w[1], sh);
+                    v.y = __funnelshift_r(w[1], w[2], sh);
+                    v.z = __funnelshift_r(w[2], w[3], sh);
+                    v.w = __funnelshift_r(w[3], w[4], sh);
+                    *reinterpret_cast<uint4*>(s_E + limb * elimb + o) = v;
+                }
+            }
+            tc::fence_proxy_async_smem();
+            tc::fence_before_sync();
+            __syncthreads();  // operands complete
+            // Six threads (lane 0 of warps 2..7) issue the chunk's products: limb pair p
+            // (hi*hi, hi*lo, lo*hi) for the chip columns of parity `par`.
+            if (lane == 0 && warp >= 2) {
+                const int s = warp - 2, p = s >> 1, par = s & 1;
+                tc::fence_after_sync();
+                const uint32_t wb = tc::smem_u32(s_W) + (p == 2 ? static_cast<uint32_t>(wlimb) : 0u);
+                const uint32_t eb = tc::smem_u32(s_E) + (p == 1 ? static_cast<uint32_t>(elimb) : 0u);
+                const uint64_t da0 = tc::smem_desc(wb, static_cast<uint32_t>(A.XC * 16), 128);
+                const uint64_t db0 = tc::smem_desc(eb, static_cast<uint32_t>(A.NB * 16), 128);
+                const uint32_t a_hi = static_cast<uint32_t>(da0 >> 32);
+                const uint32_t b_hi = static_cast<uint32_t>(db0 >> 32);
+                const uint32_t dacc = taddr + static_cast<uint32_t>(s * A.AC);
+                for (int q = 0; q < QB; ++q) {
+                    int elo, n;
+                    if (!block_rows(q, A.NB, nr, &elo, &n)) continue;
+                    const uint32_t idesc = tc::idesc_bf16_f32(64, n);
+                    const uint32_t dcol = static_cast<uint32_t>(16 * q + elo - (A.NB - 16));
+                    for (int bl = par; bl < bcn; bl += 2) {
+                        // A: block q, first half, window column x = bl (row j at x = bl + j).
+                        const uint32_t a_lo = static_cast<uint32_t>(da0) +
+                                              static_cast<uint32_t>((q * 2) * A.XC + bl);
+                        const uint32_t b_lo = static_cast<uint32_t>(db0) +
+                                              static_cast<uint32_t>((bl * 2) * A.NB + elo);
+                        tc::mma_bf16_halves(dacc + dcol, a_lo, a_hi, b_lo, b_hi, idesc, 1u);
+                    }
+                }
+                tc::mma_commit(&s_mbar);
+            }
+        }
+        if (ok) {
+            ok = tc::mbar_wait(&s_mbar, phase, kTcWaitPolls);
+            phase ^= 1u;
+        }
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicExch(A.status, 1);
+            failed = true;
+            break;
+        }
+        tc::fence_after_sync();
+
+        // Epilogue: each warp reads its lane quarter's half (16x256b) of every accumulator;
+        // value v of a thread is surface row i = 32 half + 8 (v / 4) + 2 (lane % 4) + v % 2,
+        // column j = 16 quarter + lane / 4 (+ 8 when v % 4 >= 2). Every value is normalised in
+        // FP64 (src/correlate.jl:591-600, 624-628) into the surface in shared memory.
+        {
+            const int quarter = warp & 3, half = warp >> 2;
+            const int ib0 = 32 * half + 2 * (lane & 3);
+            const int jb0 = 16 * quarter + (lane >> 2);
+            if (32 * half < nr) {
+                float sum[16];
+                const uint32_t base = taddr + (static_cast<uint32_t>(32 * quarter) << 16) +
+                                      static_cast<uint32_t>(32 * half);
+                uint32_t r[16];
+                tc::tmem_ld16dp(base, r);
+                tc::tmem_wait_ld();
+#pragma unroll
+                for (int v = 0; v < 16; ++v) sum[v] = __uint_as_float(r[v]);
+                for (int s = 1; s < kBfAcc; ++s) {
+                    tc::tmem_ld16dp(base + static_cast<uint32_t>(s * A.AC), r);
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int v = 0; v < 16; ++v) sum[v] = __fadd_rn(sum[v], __uint_as_float(r[v]));
+                }
+#pragma unroll
+                for (int v = 0; v < 16; ++v) {
+                    const int i = ib0 + 8 * (v >> 2) + (v & 1), j = jb0 + ((v & 2) ? 8 : 0);
+                    if (i < nr && j < nc) {
+                        const double s1 = s_S1[j * A.NRS + i], s2 = s_S2[j * A.NRS + i];
+                        const double num = __dadd_rn(static_cast<double>(sum[v]), __dmul_rn(cshift, sumd));
+                        double den;
+                        if (A.measure == AR_NCC) {
+                            den = __dmul_rn(cnorm, __dsqrt_rn(s2 > 0.0 ? s2 : 0.0));
+                        } else {
+                            double wvar = __dsub_rn(s2, __ddiv_rn(__dmul_rn(s1, s1), nn));
+                            if (!(wvar > 0.0)) wvar = 0.0;
+                            den = __dmul_rn(cnorm, __dsqrt_rn(wvar));
+                        }
+                        s_surf[j * A.NRS + i] = den > 0.0 ? __double2float_rn(__ddiv_rn(num, den)) : 0.0f;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (A.flops && tid == 0)
+            atomicAdd(A.flops, 2ull * static_cast<unsigned long long>(ch) * cw * nr * nc);
+        // Integer peak (src/peak.jl:32-61).
+        unsigned long long key = 0ull;
+        for (int e = tid; e < nr * nc; e += bd) {
+            const int i = e % nr, j = e / nr;
+            const unsigned long long kk = argmax_key(s_surf[j * A.NRS + i], static_cast<unsigned>(i * nc + j));
+            key = kk > key ? kk : key;
+        }
+        key = block_max_u64(key, reinterpret_cast<unsigned long long*>(s_red));
+        if (A.surf_out) {
+            float* so = A.surf_out + k * static_cast<int64_t>(A.NRM) * A.NCM;
+            for (int e = tid; e < nr * nc; e += bd) so[e] = s_surf[(e / nr) * A.NRS + (e % nr)];
+        }
+        unsigned rm = 0;
+        float pv = 0.0f;
+        int pi = 0, pj = 0;
+        if (key_decode(key, &rm, &pv)) {
+            pi = static_cast<int>(rm / nc);
+            pj = static_cast<int>(rm % nc);
+        }
+        if (A.up == 1 || nr < 5 || nc < 5) {
+            if (tid == 0) {
+                A.out.dx[k] = __double2float_rn(
+                    __dadd_rn(static_cast<double>(pj - static_cast<int>(prx)), A.pts.dx0[k]));
+                A.out.dy[k] = __double2float_rn(
+                    __dadd_rn(static_cast<double>(pi - static_cast<int>(pry)), A.pts.dy0[k]));
+                A.out.corr[k] = s_surf[pj * A.NRS + pi];
+            }
+        } else {
+            const int pi0 = min(max(pi - 2, 0), max(nr - 5, 0));
+            const int pj0 = min(max(pj - 2, 0), max(nc - 5, 0));
+            const int slot = s_slot;
+            if (tid < 25) {
+                const int a = tid % 5, b = tid / 5;
+                A.sub_patch[static_cast<int64_t>(slot) * 25 + tid] = s_surf[(pj0 + b) * A.NRS + (pi0 + a)];
+            }
+            if (tid == 0) {
+                A.sub_point[slot] = k;
+                A.sub_origin[2 * slot] = pi0;
+                A.sub_origin[2 * slot + 1] = pj0;
+            }
+        }
+    }
+    if (failed) tc::mbar_wait(&s_mbar, phase ^ 1u, kTcWaitPolls);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(taddr, A.tmem_cols);
+}
+
+// ----------------------------------------------------------------------------------------------
 // Sub-pixel cascade kernel (src/peak.jl:456-522 from the patch onward), one warp per patch.
 //
 // Levels 1 and 2 of the cascade (10^2, 20^2) are materialised in the warp's shared memory. Up to
@@ -2925,6 +3363,57 @@ bool plan_corr_tc2(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
 // The whole chip operand and separate box-sum buffers when they fit ("overlap": the box sums
 // run beside the products); otherwise the box sums first and the chip operand in chunks of BC
 // columns in the space they used.
+// Plan of k_corr_bf: the widest chunk of chip columns whose operands, with the FP64 box sums,
+// fit `smem_cap`; false when the pass's surfaces exceed 64 x 64 or its window a thread per column.
+struct BfPlan {
+    int NB, QB, BC, XC, PC, NRS, AC, VR;
+    unsigned off_W, off_E, off_P, off_S1, off_S2, off_red;
+    uint32_t tmem_cols;
+    size_t smem;
+};
+
+bool plan_corr_bf(const PassGeometry& g, size_t smem_cap, BfPlan* P) {
+    const int ch = static_cast<int>(g.max_ch), cw = static_cast<int>(g.max_cw);
+    const int nr = static_cast<int>(g.max_nr), nc = static_cast<int>(g.max_nc);
+    if (nr < 1 || nc < 1 || nr > 64 || nc > 64 || ch < 2 || cw < 2) return false;
+    const int XW = cw + nc - 1;
+    if (XW > kBfThreads) return false;  // one thread per window column for the box sums
+    P->NB = round_up(ch + 15, 16);
+    if (P->NB > 256) return false;
+    P->QB = (ch + nr - 1 + 15) / 16;
+    P->PC = round_up(kBfPadL + P->NB + 26, 8);
+    P->NRS = nr | 1;
+    P->AC = round_up(nr + 15, 16);
+    if (kBfAcc * P->AC > 512) return false;
+    P->tmem_cols = 512;
+    auto a16 = [](size_t v) { return (v + 15) & ~size_t(15); };
+    const size_t Sb = a16(static_cast<size_t>(nc) * P->NRS * 8);
+    const size_t red = 3 * 32 * 8;
+    for (int bc = cw; bc >= 2; bc -= 2) {
+        const int XC = bc + 63;
+        const size_t Wb = 2 * static_cast<size_t>(P->QB) * 2 * XC * 16;
+        const size_t Eb = 2 * static_cast<size_t>(bc) * 2 * P->NB * 16;
+        const size_t Pb = a16(2 * static_cast<size_t>(bc) * P->PC * 2);
+        const size_t alias = Wb + Eb + Pb;  // box-sum column sums, then the surface, reuse it
+        const size_t surf = static_cast<size_t>(nc) * P->NRS * 4;
+        if (alias < surf || alias < static_cast<size_t>(XW) * 16) continue;
+        const size_t total = alias + 2 * Sb + red;
+        if (total > smem_cap) continue;
+        P->BC = bc;
+        P->XC = XC;
+        P->VR = static_cast<int>(std::min<size_t>(nr, alias / (static_cast<size_t>(XW) * 16)));
+        P->off_W = 0;
+        P->off_E = static_cast<unsigned>(Wb);
+        P->off_P = static_cast<unsigned>(Wb + Eb);
+        P->off_S1 = static_cast<unsigned>(alias);
+        P->off_S2 = static_cast<unsigned>(alias + Sb);
+        P->off_red = static_cast<unsigned>(alias + 2 * Sb);
+        P->smem = total;
+        return true;
+    }
+    return false;
+}
+
 bool plan_corr_tc(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
     const int ch = static_cast<int>(g.max_ch), cw = static_cast<int>(g.max_cw);
     const int nr = static_cast<int>(g.max_nr), nc = static_cast<int>(g.max_nc);
@@ -3224,6 +3713,49 @@ cudaError_t scratch_acquire(TrackScratch& s, cudaStream_t stream) {
 
 long long scratch_allocations() { return g_scratch_allocs.load(); }
 
+// Passes of at least kTuneMinPoints points are tuned, on their first kTuneSample points.
+constexpr int64_t kTuneMinPoints = 8192;
+constexpr int64_t kTuneSample = 4096;
+
+// Times each candidate kernel (2 k_corr_tc2, 1 k_corr_tc, 0 k_corr) on the first kTuneSample
+// points of the pass without refinement (the pass itself overwrites their outputs), each
+// launched twice and the second timed, and returns the fastest in `kind` (a tie keeps the
+// earlier candidate).
+template <typename Launch>
+cudaError_t autotune_u8(TrackScratch& scratch, cudaStream_t stream, const DevPoints& pts,
+                        bool fit2, bool fit1, int* kind, Launch launch) {
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i)
+        if (!scratch.tune_ev[i]) {
+            e = cudaEventCreate(&scratch.tune_ev[i]);
+            ++g_scratch_allocs;
+        }
+    if (e != cudaSuccess) return e;
+    DevPoints ds = pts;
+    ds.n = std::min<int64_t>(pts.n, kTuneSample);
+    float best = INFINITY;
+    int chosen = fit2 ? 2 : 1;
+    const int cand[3] = {2, 1, 0};
+    for (int c : cand) {
+        if ((c == 2 && !fit2) || (c == 1 && !fit1)) continue;
+        e = launch(c, ds);
+        if (e == cudaSuccess) e = cudaEventRecord(scratch.tune_ev[0], stream);
+        if (e == cudaSuccess) e = launch(c, ds);
+        if (e == cudaSuccess) e = cudaEventRecord(scratch.tune_ev[1], stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(scratch.tune_ev[1]);
+        float ms = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, scratch.tune_ev[0], scratch.tune_ev[1]);
+        if (e != cudaSuccess) return e;
+        scratch.timer.launches += 2;
+        if (ms < best) {
+            best = ms;
+            chosen = c;
+        }
+    }
+    *kind = chosen;
+    return cudaSuccess;
+}
+
 cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const uint8_t* valid,
                               int64_t nrows, int64_t ncols, const DevPoints& pts,
                               const PassGeometry& geom, int up, int measure,
@@ -3294,13 +3826,10 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         ev2 = T.get();
         cudaEventRecord(ev0, stream);
     }
-    TcPlan TP{};
-    // The rotation search correlates Float32 (resampled) chips: CUDA cores for every type.
-    const bool tc_ok = dtype == AR_U8 && scratch.tensor_cores && !rotating;
-    // k_corr_tc2 wherever its plan fits (one or two CTAs per SM); otherwise k_corr_tc.
-    const bool use_tc2 = tc_ok && plan_corr_tc2(geom, 220 * 1024, &TP);
-    const bool use_tc = tc_ok && (use_tc2 || plan_corr_tc(geom, 220 * 1024, &TP));
-    if (use_tc) {
+    // The UInt8 tensor-core kernels: k_corr_tc2 (`tc2`, surfaces up to 64 x 64 with the chip
+    // operand whole) or k_corr_tc (surfaces up to 128 columns), planned by `TP`.
+    auto launch_tc = [&](bool tc2, const TcPlan& TP, const DevPoints& pts, int up,
+                         const DevOutputs& out, unsigned long long* flops) -> cudaError_t {
         TcArgs B{};
         B.ref = static_cast<const uint8_t*>(ref);
         B.sec = static_cast<const uint8_t*>(sec);
@@ -3346,7 +3875,7 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         B.sub_origin = scratch.sub_origin;
         B.sub_patch = scratch.sub_patch;
         B.surf_out = surf_out;
-        B.flops = A.flops;
+        B.flops = flops;
         B.status = scratch.status;
         // Each CTA holds its Tensor Memory columns for its lifetime, so the CTAs one SM holds
         // must fit its 512 columns together -- including CTAs of other launches running
@@ -3355,7 +3884,7 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         // T/512 of the SM's 228 KB of shared memory (less the 1 KB each CTA is charged): any set
         // of CTAs that fits an SM's shared memory fits its Tensor Memory.
         const bool reg = TP.MT == 64 && TP.NRM <= 64;
-        auto kern = use_tc2 ? k_corr_tc2 : reg ? k_corr_tc<true> : k_corr_tc<false>;
+        auto kern = tc2 ? k_corr_tc2 : reg ? k_corr_tc<true> : k_corr_tc<false>;
         cudaFuncAttributes fa{};
         e = cudaFuncGetAttributes(&fa, kern);
         if (e != cudaSuccess) return e;
@@ -3372,18 +3901,134 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
             std::max<int64_t>(1, std::min<int64_t>(pts.n, static_cast<int64_t>(num_sms) * per_sm_tc)));
         kern<<<grid, kTcThreads, tc_smem, stream>>>(B);
         e = cudaGetLastError();
+            return e;
+    };
+    // The CUDA-core kernel (the plain method) for any element type.
+    auto launch_direct = [&](const DevPoints& pts_, int up_, const DevOutputs& out_,
+                             unsigned long long* flops_) -> cudaError_t {
+        CorrArgs A2 = A;
+        A2.pts = pts_;
+        A2.up = up_;
+        A2.out = out_;
+        A2.flops = flops_;
+        const int per_sm = P.smem <= 100 * 1024 ? 2 : 1;
+        const int64_t want = static_cast<int64_t>(num_sms) * per_sm * 8;
+        const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(pts_.n, want)));
+        switch (dtype) {
+            case AR_U8: return launch_corr_t<uint8_t>(A2, P, grid, stream);
+            case AR_U16: return launch_corr_t<uint16_t>(A2, P, grid, stream);
+            case AR_I16: return launch_corr_t<int16_t>(A2, P, grid, stream);
+            case AR_F32: return launch_corr_t<float>(A2, P, grid, stream);
+            default: return cudaErrorInvalidValue;
+        }
+    };
+    if (dtype != AR_U8 && dtype != AR_U16 && dtype != AR_I16 && dtype != AR_F32) {
+        if (err) *err = "unsupported element type";
+        return cudaErrorInvalidValue;
     }
-    const int per_sm = P.smem <= 100 * 1024 ? 2 : 1;
-    const int64_t want = static_cast<int64_t>(num_sms) * per_sm * 8;
-    const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(pts.n, want)));
-    if (!use_tc) switch (dtype) {
-        case AR_U8: e = launch_corr_t<uint8_t>(A, P, grid, stream); break;
-        case AR_U16: e = launch_corr_t<uint16_t>(A, P, grid, stream); break;
-        case AR_I16: e = launch_corr_t<int16_t>(A, P, grid, stream); break;
-        case AR_F32: e = launch_corr_t<float>(A, P, grid, stream); break;
-        default:
-            if (err) *err = "unsupported element type";
-            return cudaErrorInvalidValue;
+    // The rotation search correlates Float32 (resampled) chips: CUDA cores for every type.
+    const bool tc_ok = dtype == AR_U8 && scratch.tensor_cores && !rotating;
+    // Split-BF16 tensor-core products for the other element types (by default for chips of
+    // 64 px and up, where the products are a dense contraction worth the limb splitting).
+    bool bf_done = false;
+    const bool bf_ok = (dtype == AR_U16 || dtype == AR_I16 || dtype == AR_F32) &&
+                       scratch.tensor_cores && !rotating && scratch.split_bf16 != 0 &&
+                       (scratch.split_bf16 == 2 || (geom.max_ch >= 64 && geom.max_cw >= 64));
+    if (bf_ok) {
+        auto kern = dtype == AR_U16 ? k_corr_bf<uint16_t> : dtype == AR_I16 ? k_corr_bf<int16_t>
+                                                                             : k_corr_bf<float>;
+        cudaFuncAttributes fa{};
+        e = cudaFuncGetAttributes(&fa, kern);
+        if (e != cudaSuccess) return e;
+        const size_t dyn_max = 232448 - fa.sharedSizeBytes;
+        BfPlan BPl{};
+        if (plan_corr_bf(geom, dyn_max, &BPl)) {
+            BfArgs B{};
+            B.ref = ref;
+            B.sec = sec;
+            B.valid = valid;
+            B.nrows = nrows;
+            B.ncols = ncols;
+            B.pts = pts;
+            B.padx = geom.padx;
+            B.pady = geom.pady;
+            B.up = up;
+            B.measure = measure;
+            B.CHM = static_cast<int>(geom.max_ch);
+            B.CWM = static_cast<int>(geom.max_cw);
+            B.NRM = static_cast<int>(geom.max_nr);
+            B.NCM = static_cast<int>(geom.max_nc);
+            B.NB = BPl.NB;
+            B.QB = BPl.QB;
+            B.BC = BPl.BC;
+            B.XC = BPl.XC;
+            B.PC = BPl.PC;
+            B.NRS = BPl.NRS;
+            B.AC = BPl.AC;
+            B.VR = BPl.VR;
+            B.off_W = BPl.off_W;
+            B.off_E = BPl.off_E;
+            B.off_P = BPl.off_P;
+            B.off_S1 = BPl.off_S1;
+            B.off_S2 = BPl.off_S2;
+            B.off_red = BPl.off_red;
+            B.tmem_cols = BPl.tmem_cols;
+            B.out = out;
+            B.sub_count = scratch.sub_count;
+            B.sub_point = scratch.sub_point;
+            B.sub_origin = scratch.sub_origin;
+            B.sub_patch = scratch.sub_patch;
+            B.surf_out = surf_out;
+            B.flops = A.flops;
+            B.status = scratch.status;
+            // 512 Tensor Memory columns: one CTA per SM, which its shared memory reserves too
+            // (no CTA of another launch can wait on this one's columns).
+            const size_t bf_smem = std::max<size_t>(BPl.smem, tmem_smem_floor(BPl.tmem_cols, fa.sharedSizeBytes));
+            if (bf_smem > dyn_max) return cudaErrorInvalidValue;
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(dyn_max));
+            if (e != cudaSuccess) return e;
+            const int bgrid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(pts.n, num_sms)));
+            kern<<<bgrid, kBfThreads, bf_smem, stream>>>(B);
+            e = cudaGetLastError();
+            bf_done = true;
+        }
+    }
+    if (!bf_done) {
+        // UInt8: the three kernels are exact and give identical results, so the one to run is
+        // a matter of speed -- by default the tensor-core kernel whose plan fits (k_corr_tc2
+        // first); for large passes the autotuner times the candidates once per geometry on a
+        // sample of the pass and the context keeps the fastest.
+        TcPlan TP2{}, TP1{};
+        const bool fit2 = tc_ok && plan_corr_tc2(geom, 220 * 1024, &TP2);
+        const bool fit1 = tc_ok && plan_corr_tc(geom, 220 * 1024, &TP1);
+        int kind = fit2 ? 2 : fit1 ? 1 : 0;
+        if ((fit2 || fit1) && scratch.autotune && !scratch.fixed && pts.n >= kTuneMinPoints) {
+            const uint64_t key = (static_cast<uint64_t>(geom.max_ch) << 48) |
+                                 (static_cast<uint64_t>(geom.max_cw) << 32) |
+                                 (static_cast<uint64_t>(geom.max_nr) << 16) |
+                                 static_cast<uint64_t>(geom.max_nc);
+            auto it = scratch.tuned.find(key);
+            if (it != scratch.tuned.end()) {
+                kind = it->second;
+            } else {
+                e = autotune_u8(scratch, stream, pts, fit2, fit1, &kind,
+                                [&](int kk, const DevPoints& ds) -> cudaError_t {
+                                    if (kk == 2) return launch_tc(true, TP2, ds, 1, out, nullptr);
+                                    if (kk == 1) return launch_tc(false, TP1, ds, 1, out, nullptr);
+                                    return launch_direct(ds, 1, out, nullptr);
+                                });
+                if (e != cudaSuccess) return e;
+                scratch.tuned[key] = kind;
+            }
+        }
+        if (kind == 2) {
+            e = launch_tc(true, TP2, pts, up, out, A.flops);
+        } else if (kind == 1) {
+            e = launch_tc(false, TP1, pts, up, out, A.flops);
+        } else {
+            e = launch_direct(pts, up, out, A.flops);
+        }
     }
     if (e != cudaSuccess) return e;
     T.launches += 1;

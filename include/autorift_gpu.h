@@ -303,11 +303,22 @@ int ar_release(ar_ctx* ctx, ar_ticket ticket);
  * Context options. AR_OPT_TENSOR_CORES (default 1): UInt8 passes whose geometry fits (surface
  * at most 128 columns and 256 rows, chip at most 226 rows) compute the correlation numerator
  * on the tensor cores (exact 8-bit products, bit-identical results); 0 keeps every pass on the
- * CUDA-core kernel.
+ * CUDA-core kernel (direct FP32 for other element types, the plain method).
+ * AR_OPT_SPLIT_BF16 (default 1; applies while AR_OPT_TENSOR_CORES is 1): UInt16, Int16 and
+ * Float32 passes whose surfaces are at most 64 x 64 compute the numerator on the tensor cores
+ * as split-BF16 products (each operand as two BF16 limbs, hi*hi + hi*lo + lo*hi accumulated in
+ * FP32) -- 1 for passes whose chips are 64 px and up, 2 for every chip size, 0 never (direct
+ * FP32). Surface values then differ from the FP64 ones by up to a few 1e-6 instead of ~1e-7;
+ * the box sums and the normalisation stay FP64.
+ * AR_OPT_AUTOTUNE (default 1): for UInt8 passes of 8192 points or more, the kernels that give
+ * identical results (the two tensor-core kernels whose plans fit and the CUDA-core kernel) are
+ * timed once per pass geometry on a sample of the pass, and the context runs the fastest from
+ * then on; 0 always takes the first tensor-core kernel that fits.
  * AR_OPT_SERVE_SLOTS and AR_OPT_SERVE_MEMORY_MB configure the request loop (see ar_submit);
  * they must be set before the first ar_submit. No reference counterpart.
  */
-enum { AR_OPT_TENSOR_CORES = 1, AR_OPT_SERVE_SLOTS = 2, AR_OPT_SERVE_MEMORY_MB = 3 };
+enum { AR_OPT_TENSOR_CORES = 1, AR_OPT_SERVE_SLOTS = 2, AR_OPT_SERVE_MEMORY_MB = 3,
+       AR_OPT_SPLIT_BF16 = 4, AR_OPT_AUTOTUNE = 5 };
 int ar_ctx_set_option(ar_ctx* ctx, int option, int value);
 
 /* The context's own CUDA stream (cudaStream_t), on which calls without a stream argument run;

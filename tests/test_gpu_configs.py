@@ -7,9 +7,9 @@
   power-of-two chip areas) and close to the imposed field.
 * The precision configuration (the benchmark scene, chips 64 and 128, radius 32): the
   tensor-core path, the direct FP32 path on CUDA cores and the FP64-numerator oracle on UInt8
-  imagery (identical), and the direct FP32 path against the oracle on unquantised Float32
-  imagery (max |dNCC|, integer-peak agreement, sub-pixel deviation), each against the known
-  displacement field too.
+  imagery (identical); on unquantised imagery the direct FP32 path and the split-BF16
+  tensor-core path each against the oracle (max |dNCC|, integer-peak agreement, sub-pixel
+  deviation) and against the known displacement field.
 """
 
 import numpy as np
@@ -103,50 +103,130 @@ def test_precision_uint8_three_ways(ar, O, gpu_lib, precision_scene, chip, spaci
     assert resolved > 0.8 * pts.x.size and err < 0.3, (err, resolved)
 
 
-@pytest.mark.parametrize("chip,spacing", [(64, 24), (128, 40)])
-def test_precision_float32_direct_vs_oracle(ar, O, gpu_lib, precision_scene, chip, spacing):
-    """Float32 (highpass, no quantisation): the direct FP32 correlation against the oracle's
-    FP64 numerator -- max |dNCC| <= 1e-5, integer peaks identical where the oracle's top-two
-    margin exceeds 1e-4, sub-pixel deviation <= 1e-3 px but for bounded near-ties."""
-    a, b, sv, fx, fy = precision_scene
-    p = ar.params(chip_size=chip, search_radius=32, quantize="none")
-    prep = ar.prepare(ar.ImagePair(a, b, None, sv), p)
-    ref, sec, rv, svv = prep.download()
-    assert ref.dtype == np.float32
-    pts = ar.gridpoints(a.shape, spacing, chip_size=chip, search_radius=32)
-    got = ar.track(prep, pts, p)
-    want = O.track(ref, sec, fields(pts), upsampling=64, reference_valid=rv,
-                   secondary_valid=svv)
-    gdx, gdy, gc = (x.ravel(order="F") for x in (got.dx, got.dy, got.correlation))
-    wdx, wdy, wc = want[:3]
-    m = ~np.isnan(wdx)
-    assert np.array_equal(m, ~np.isnan(gdx))
-    dncc = float(np.abs(gc[m] - wc[m]).max())
-    assert dncc <= 1e-5, dncc
-    # Whole surfaces of a sample of points (window and chip cut from the prepared pair; the
-    # grid is inset, so no padding): values within 1e-5 and integer peaks identical where the
-    # oracle's top-two margin exceeds 1e-4.
+def surface_sample(ar, O, ref, sec, pts, m, chip, r, ctx, count=40):
+    """Whole surfaces of a sample of measured points (window and chip cut from the prepared
+    pair; the grid is inset, so no padding): the largest |dNCC| against the oracle's FP64
+    surfaces, and the integer peaks compared where the oracle's top-two margin exceeds 1e-4
+    (returns dncc, compared, agreeing)."""
     hy = hx = chip // 2
-    r = 32
-    checked = 0
-    for k in np.flatnonzero(m)[:: max(1, m.sum() // 40)]:
+    dncc, compared, agree = 0.0, 0, 0
+    for k in np.flatnonzero(m)[:: max(1, m.sum() // count)]:
         x, y = pts.x.ravel(order="F")[k] + 0.5, pts.y.ravel(order="F")[k] + 0.5
         cx, cy = int(np.floor(x)), int(np.floor(y))
         chip_a = sec[cy - hy - 1:cy + hy - 1, cx - hx - 1:cx + hx - 1]
         win = ref[cy - hy - r - 1:cy + hy + r - 2, cx - hx - r - 1:cx + hx + r - 2]
         so, _ = O.correlate(win, chip_a, r)
-        sg, _ = ar.correlate(win, chip_a, r)
+        sg, _ = ar.correlate(win, chip_a, r, ctx=ctx)
         dncc = max(dncc, float(np.abs(sg - so).max()))
         top = np.sort(so.ravel())[-2:]
         if top[1] - top[0] > 1e-4:
-            assert O.peak_index(sg) == O.peak_index(so), k
-            checked += 1
-    assert dncc <= 1e-5, dncc
-    assert checked >= 20
-    d = np.maximum(np.abs(gdx[m] - wdx[m]), np.abs(gdy[m] - wdy[m]))
-    flips = int(np.count_nonzero(d > 1e-3))
-    assert flips <= max(1, 0.02 * m.sum()), flips
-    err, resolved = field_error(ar, got, pts, fx, fy)
-    assert err < 0.3, err
-    print(f"chip {chip}: max|dNCC| {dncc:.2e}, sub-pixel flips {flips}/{m.sum()}, "
-          f"median field error {err:.3f} px")
+            compared += 1
+            agree += int(O.peak_index(sg) == O.peak_index(so))
+    return dncc, compared, agree
+
+
+def precision_run(ar, O, scene, chip, spacing, mode, preprocess="highpass"):
+    """One precision variant: correlation mode (AR_OPT_SPLIT_BF16 0 = direct FP32, 1 = split
+    BF16) on the unquantised pair, against the oracle's FP64 numerator and the imposed field."""
+    a, b, sv, fx, fy = scene
+    L = ar._lib
+    ctx = L.Context(0)
+    ctx.set_option(L.AR_OPT_SPLIT_BF16, mode)
+    try:
+        p = ar.params(chip_size=chip, search_radius=32, quantize="none", preprocess=preprocess)
+        prep = ar.prepare(ar.ImagePair(a, b, None, sv), p, ctx)
+        ref, sec, rv, svv = prep.download()
+        pts = ar.gridpoints(a.shape, spacing, chip_size=chip, search_radius=32)
+        got = ar.track(prep, pts, p, ctx=ctx)
+        want = O.track(ref, sec, fields(pts), upsampling=64, reference_valid=rv,
+                       secondary_valid=svv)
+        gdx, gdy, gc = (x.ravel(order="F") for x in (got.dx, got.dy, got.correlation))
+        wdx, wdy, wc = want[:3]
+        m = ~np.isnan(wdx)
+        assert np.array_equal(m, ~np.isnan(gdx))
+        dncc = float(np.abs(gc[m] - wc[m]).max())
+        sdncc, compared, agree = surface_sample(ar, O, ref, sec, pts, m, chip, 32, ctx)
+        d = np.maximum(np.abs(gdx[m] - wdx[m]), np.abs(gdy[m] - wdy[m]))
+        err, resolved = field_error(ar, got, pts, fx, fy)
+    finally:
+        ctx.close()
+    return {"dncc": max(dncc, sdncc), "compared": compared, "agree": agree,
+            "flips": int(np.count_nonzero(d > 1e-3)), "measured": int(m.sum()),
+            "max_dd": float(d.max()) if d.size else 0.0, "field_err": err,
+            "median_dd": float(np.median(d)) if d.size else 0.0}
+
+
+@pytest.mark.parametrize("chip,spacing", [(64, 24), (128, 40)])
+def test_precision_float32_direct_vs_oracle(ar, O, gpu_lib, precision_scene, chip, spacing):
+    """Float32 (highpass, no quantisation): the direct FP32 correlation against the oracle's
+    FP64 numerator -- max |dNCC| <= 1e-5, integer peaks identical where the oracle's top-two
+    margin exceeds 1e-4, sub-pixel deviation <= 1e-3 px but for bounded near-ties."""
+    r = precision_run(ar, O, precision_scene, chip, spacing, mode=0)
+    assert r["dncc"] <= 1e-5, r
+    assert r["compared"] >= 20 and r["agree"] == r["compared"], r
+    assert r["flips"] <= max(1, 0.02 * r["measured"]), r
+    assert r["field_err"] < 0.3, r
+    print(f"direct FP32, chip {chip}: {r}")
+
+
+@pytest.mark.parametrize("chip,spacing,pre", [(64, 24, "highpass"), (128, 40, "highpass"),
+                                              (64, 24, "none")])
+def test_precision_split_bf16_vs_oracle(ar, O, gpu_lib, precision_scene, chip, spacing, pre):
+    """The precision configuration's split-BF16 variant: tensor-core products of two BF16
+    limbs per operand (hi*hi + hi*lo + lo*hi, FP32 accumulation), FP64 box sums and
+    normalisation, on the highpass-filtered Float32 pair and on the raw UInt16 pair. Reported:
+    max |dNCC| over measured peaks and sampled whole surfaces against the FP64-numerator oracle,
+    the integer-peak agreement where the oracle's top-two margin exceeds 1e-4, the sub-pixel
+    deviation, and the error against the imposed field. Bounds: |dNCC| <= 5e-5, every
+    compared integer peak identical, sub-pixel flips (> 1e-3 px, 1/64 px cascade near-ties)
+    at most 5% of the measured points, median field error below 0.3 px."""
+    r = precision_run(ar, O, precision_scene, chip, spacing, mode=1, preprocess=pre)
+    assert r["dncc"] <= 5e-5, r
+    assert r["compared"] >= 20 and r["agree"] == r["compared"], r
+    assert r["flips"] <= max(1, 0.05 * r["measured"]), r
+    assert r["field_err"] < 0.3, r
+    print(f"split BF16, chip {chip}, {pre}: {r}")
+
+
+def test_split_bf16_is_used_for_large_chips(ar, gpu_lib, precision_scene):
+    """With the default mode the chip-64 pass of Float32 imagery runs the split-BF16 kernel
+    (its surfaces differ from the direct FP32 ones in the low bits), and mode 0 restores the
+    direct FP32 results."""
+    a, b, sv, fx, fy = precision_scene
+    L = ar._lib
+    p = ar.params(chip_size=64, search_radius=32, quantize="none")
+    pts = ar.gridpoints(a.shape, 48, chip_size=64, search_radius=32)
+    out = {}
+    for mode in (0, 1, 0):
+        ctx = L.Context(0)
+        ctx.set_option(L.AR_OPT_SPLIT_BF16, mode)
+        prep = ar.prepare(ar.ImagePair(a, b, None, sv), p, ctx)
+        got = ar.track(prep, pts, p, ctx=ctx)
+        ctx.close()
+        out.setdefault(mode, []).append(got.correlation.copy())
+    assert np.array_equal(out[0][0], out[0][1], equal_nan=True)
+    m = ~np.isnan(out[0][0])
+    assert not np.array_equal(out[0][0][m], out[1][0][m])
+    assert np.abs(out[0][0][m] - out[1][0][m]).max() < 5e-5
+
+
+def test_autotuner_keeps_results_identical(ar, gpu_lib, precision_scene):
+    """UInt8 passes large enough to be tuned give the same results with the autotuner on and
+    off (every candidate kernel is exact)."""
+    a, b, sv, fx, fy = precision_scene
+    L = ar._lib
+    p = ar.params(chip_size=32, search_radius=25)
+    pts = ar.gridpoints(a.shape, 4, chip_size=32, search_radius=25)
+    assert len(pts) >= 8192
+    res = []
+    for tune in (0, 1, 1):
+        ctx = L.Context(0)
+        ctx.set_option(L.AR_OPT_AUTOTUNE, tune)
+        prep = ar.prepare(ar.ImagePair(a, b, None, sv), p, ctx)
+        got = ar.track(prep, pts, p, ctx=ctx)
+        got2 = ar.track(prep, pts, p, ctx=ctx)  # the tuned choice, from the context's table
+        ctx.close()
+        res += [got, got2]
+    for r in res[1:]:
+        for x, y in ((r.dx, res[0].dx), (r.dy, res[0].dy), (r.correlation, res[0].correlation)):
+            assert np.array_equal(x.view(np.uint32), y.view(np.uint32))

@@ -15,15 +15,23 @@ from conftest import fields
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("dtype,chip,r,tol", [(np.uint8, 256, 24, 1e-6), (np.float32, 192, 32, 1e-5),
-                                              (np.uint8, 128, 60, 1e-6)])
-def test_large_chip_against_oracle(ar, O, gpu_lib, dtype, chip, r, tol):
+@pytest.mark.parametrize("dtype,chip,r,tol,bf16", [(np.uint8, 256, 24, 1e-6, 1),
+                                                   (np.float32, 192, 32, 1e-5, 0),
+                                                   (np.float32, 192, 32, 5e-5, 1),
+                                                   (np.uint8, 128, 60, 1e-6, 1)])
+def test_large_chip_against_oracle(ar, O, gpu_lib, dtype, chip, r, tol, bf16):
+    """bf16 = 0: the direct FP32 correlation streams the chip in column chunks; bf16 = 1 (the
+    default) runs Float32 on the split-BF16 tensor-core kernel, whose chip operand comes in
+    chunks too."""
     ref, sec = ar.synthetic.shifted_pair(768, (2.6, -3.3), seed=31, dtype=dtype)
     rng = np.random.default_rng(chip + r)
     pts = ar.pointset(rng.uniform(330, 440, 6), rng.uniform(330, 440, 6), chip_size=chip,
                       search_radius=r)
     p = ar.params(preprocess="none", quantize="none", upsampling=16)
-    d = ar.track(ar.ImagePair(ref, sec), pts, p)
+    ctx = ar._lib.Context(0)
+    ctx.set_option(ar._lib.AR_OPT_SPLIT_BF16, bf16)
+    d = ar.track(ar.ImagePair(ref, sec), pts, p, ctx=ctx)
+    ctx.close()
     dx, dy, cc, searched = O.track(ref, sec, fields(pts), upsampling=16)
     assert np.array_equal(d.searched.ravel(order="F"), searched.astype(bool))
     got = d.correlation.ravel(order="F")
