@@ -423,12 +423,35 @@ __global__ void k_init_result(int64_t n, float* dx, float* dy, float* c, uint16_
     }
 }
 
-// Compaction of a pass to its searchable points (both radii > 0): the other points of a level
-// are skipped by the track kernels anyway, but each would still cost a CTA a loop iteration.
-__global__ void k_compact(const int64_t* rx, const int64_t* ry, int64_t n, int64_t* idx,
+// Shape bin of a point: -1 not searchable, 0 a surface of at most 64 x 64 (every tensor-core
+// kernel and the split-BF16 kernel take it), 1 a larger one. A pass whose points fall in both
+// bins runs each bin as its own launch, planned for that bin's largest surface, so a few wide
+// searches do not put the whole pass on the wide-surface kernels.
+__device__ __forceinline__ int shape_bin(int64_t rx, int64_t ry) {
+    if (!(rx > 0 && ry > 0)) return -1;
+    return (2 * rx <= 64 && 2 * ry <= 64) ? 0 : 1;
+}
+
+// Points per shape bin (count[0], count[1]), one atomic per warp and bin.
+__global__ void k_count_bins(const int64_t* rx, const int64_t* ry, int64_t n,
+                             unsigned long long* count) {
+    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const int b = k < n ? shape_bin(rx[k], ry[k]) : -1;
+    const unsigned m0 = __ballot_sync(0xffffffffu, b == 0), m1 = __ballot_sync(0xffffffffu, b == 1);
+    if ((threadIdx.x & 31) == 0) {
+        if (m0) atomicAdd(&count[0], static_cast<unsigned long long>(__popc(m0)));
+        if (m1) atomicAdd(&count[1], static_cast<unsigned long long>(__popc(m1)));
+    }
+}
+
+// Compaction of a pass to its searchable points of shape bin `bin` (-1: every searchable
+// point, both radii > 0): the other points of a level are skipped by the track kernels anyway,
+// but each would still cost a CTA a loop iteration.
+__global__ void k_compact(const int64_t* rx, const int64_t* ry, int64_t n, int bin, int64_t* idx,
                           unsigned long long* count) {
     const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    const bool take = k < n && rx[k] > 0 && ry[k] > 0;
+    const int b = k < n ? shape_bin(rx[k], ry[k]) : -1;
+    const bool take = b >= 0 && (bin < 0 || b == bin);
     const unsigned m = __ballot_sync(0xffffffffu, take);
     const int lane = threadIdx.x & 31;
     unsigned long long base = 0;
@@ -612,28 +635,38 @@ cudaError_t run_multichip(const MultichipJob& J, TrackScratch& scratch, int num_
     int level_measure = P.measure;
 
     // A track pass over the searchable points of P only, results scattered back into O.
+    // The searchable points are counted per shape bin; when both bins are occupied each runs
+    // as its own compacted launch, otherwise the whole pass runs as one.
     auto track_searchable = [&](const DevPoints& P, const DevOutputs& O, int up) {
         k_unmeasured<<<blocks(P.n), kT, 0, s>>>(O, P.n);
         ++L;
-        C.zero();
-        k_compact<<<blocks(P.n), kT, 0, s>>>(P.rx, P.ry, P.n, kidx, C.dev);
+        C.zero(2);
+        k_count_bins<<<blocks(P.n), kT, 0, s>>>(P.rx, P.ry, P.n, C.dev);
         ++L;
-        const int64_t ns = static_cast<int64_t>(C.read1());
-        if (ns == 0 || err != cudaSuccess) return;
-        k_gather_points<<<blocks(ns), kT, 0, s>>>(kidx, ns, P, kx, ky, krx, kry, kdx0, kdy0, kcsx,
-                                                   kcsy);
-        ++L;
-        DevPoints cp{kx, ky, krx, kry, kdx0, kdy0, kcsx, kcsy, ns};
-        DevOutputs co{kdx, kdy, kc, ks};
-        PassGeometry g;
-        err = pass_geometry_device(cp, J.nrows, J.ncols, scratch, s, &g);
-        if (err == cudaSuccess)
-            err = launch_track(J.dtype, J.ref, J.sec, J.valid, J.nrows, J.ncols, cp, g, up,
-                               level_measure, co, scratch, num_sms, s, errmsg, nullptr,
-                               J.P.rot.count > 0 ? &J.P.rot : nullptr);
+        unsigned long long cnt[2];
+        C.read(cnt, 2);
         if (err != cudaSuccess) return;
-        k_scatter_outputs<<<blocks(ns), kT, 0, s>>>(kidx, ns, co, O);
-        ++L;
+        const bool split = cnt[0] > 0 && cnt[1] > 0;
+        for (int bin = split ? 0 : -1; bin <= (split ? 1 : -1); ++bin) {
+            const int64_t ns = static_cast<int64_t>(bin < 0 ? cnt[0] + cnt[1] : cnt[bin]);
+            if (ns == 0) continue;
+            if (err == cudaSuccess) err = cudaMemsetAsync(C.dev + 2, 0, 8, s);
+            k_compact<<<blocks(P.n), kT, 0, s>>>(P.rx, P.ry, P.n, bin, kidx, C.dev + 2);
+            k_gather_points<<<blocks(ns), kT, 0, s>>>(kidx, ns, P, kx, ky, krx, kry, kdx0, kdy0,
+                                                       kcsx, kcsy);
+            L += 2;
+            DevPoints cp{kx, ky, krx, kry, kdx0, kdy0, kcsx, kcsy, ns};
+            DevOutputs co{kdx, kdy, kc, ks};
+            PassGeometry g;
+            if (err == cudaSuccess) err = pass_geometry_device(cp, J.nrows, J.ncols, scratch, s, &g);
+            if (err == cudaSuccess)
+                err = launch_track(J.dtype, J.ref, J.sec, J.valid, J.nrows, J.ncols, cp, g, up,
+                                   level_measure, co, scratch, num_sms, s, errmsg, nullptr,
+                                   J.P.rot.count > 0 ? &J.P.rot : nullptr);
+            if (err != cudaSuccess) return;
+            k_scatter_outputs<<<blocks(ns), kT, 0, s>>>(kidx, ns, co, O);
+            ++L;
+        }
     };
 
     std::vector<int64_t> sizes;
