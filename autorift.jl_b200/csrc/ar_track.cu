@@ -1630,6 +1630,14 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
     // The point whose box sums s_S1 / s_S2 hold (held = false: none).
     bool held = false;
     int64_t h_wr = 0, h_wc = 0;
+    // s_S1 / s_S2 are rings of NRS rows per column: surface row i of the held point is stored at
+    // row (i + rbase) mod NRS, so carrying the sums down by `sh` rows advances rbase instead of
+    // moving them.
+    int rbase = 0;
+    auto ring = [&](int i) {
+        const int r = i + rbase;
+        return r >= A.NRS ? r - A.NRS : r;
+    };
     int h_ch = 0, h_cw = 0, h_nr = 0, h_nc = 0;
     for (int64_t k = kbeg; k < kend; ++k, ++iter) {
         tc::fence_before_sync();
@@ -1896,11 +1904,18 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
         };
         // Box sums of W and W^2 (integral_both!, boxsum, src/integral.jl:141-170, 244-247) as
         // exact integers, warps 0-5 (named barrier 1) while warps 6 and 7 issue the products. When
-        // the held sums belong to the same window geometry `sh` rows higher, they move up `sh`
-        // rows and only the last `sh` rows are computed.
+        // the held sums belong to the same window geometry `sh` rows higher, the ring's base
+        // advances by `sh` (the held rows become rows 0 .. nr - sh - 1) and only the last `sh`
+        // rows are computed.
         const int64_t sh64 = win_r - h_wr;
         const bool carry = held && win_c == h_wc && ch == h_ch && cw == h_cw && nr == h_nr &&
                            nc == h_nc && sh64 > 0 && sh64 < nr;
+        if (carry) {
+            rbase += static_cast<int>(sh64);
+            if (rbase >= A.NRS) rbase -= A.NRS;
+        } else {
+            rbase = 0;
+        }
 #ifdef AR_TC_PHASES
         if (tid == 0 && carry) atomicAdd(&g_tc_phase[14], 1ull);
 #endif
@@ -1908,34 +1923,6 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
             constexpr int kBT = kTcThreads - 64;
             if (carry) {
                 const int sh = static_cast<int>(sh64);
-                // Move: a warp per surface column, 64 rows per step (all loads of a step before
-                // its stores, reading ahead of what it overwrites).
-                for (int j = warp; j < nc; j += 6) {
-                    uint32_t* c1 = s_S1 + j * A.NRS;
-                    uint32_t* c2 = s_S2 + j * A.NRS;
-                    for (int c = 0; c < nr - sh; c += 64) {
-                        const int ia = c + lane, ib = c + 32 + lane;
-                        uint32_t a1 = 0, a2 = 0, b1 = 0, b2 = 0;
-                        if (ia < nr - sh) {
-                            a1 = c1[ia + sh];
-                            a2 = c2[ia + sh];
-                        }
-                        if (ib < nr - sh) {
-                            b1 = c1[ib + sh];
-                            b2 = c2[ib + sh];
-                        }
-                        __syncwarp();
-                        if (ia < nr - sh) {
-                            c1[ia] = a1;
-                            c2[ia] = a2;
-                        }
-                        if (ib < nr - sh) {
-                            c1[ib] = b1;
-                            c2[ib] = b2;
-                        }
-                        __syncwarp();
-                    }
-                }
                 // Column sums of the new rows i in [nr - sh, nr): an item is a window column and
                 // up to 4 consecutive rows; its first sum from 4-byte groups (dp4a), then a
                 // sliding update. The row groups of a column are adjacent lanes: their words lie
@@ -2015,12 +2002,13 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
                     }
                     const uint32_t oo1[4] = {o1.x, o1.y, o1.z, o1.w}, ii1[4] = {i1.x, i1.y, i1.z, i1.w};
                     const uint32_t oo2[4] = {o2.x, o2.y, o2.z, o2.w}, ii2[4] = {i2.x, i2.y, i2.z, i2.w};
+                    const int ri = ring(i);
 #pragma unroll
                     for (int m = 0; m < 4; ++m) {
                         const int j = j0 + m;
                         if (j < nc) {
-                            s_S1[j * A.NRS + i] = g1;
-                            s_S2[j * A.NRS + i] = g2;
+                            s_S1[j * A.NRS + ri] = g1;
+                            s_S2[j * A.NRS + ri] = g2;
                             g1 = g1 + ii1[m] - oo1[m];
                             g2 = g2 + ii2[m] - oo2[m];
                         }
@@ -2139,8 +2127,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
                 if (j < nc && i < nr) {
                     const bool two = i + 1 < nr;
                     vm |= (two ? 3u : 1u) << v;
-                    const int o = j * A.NRS + i;
-                    const uint32_t b1 = two ? s_S1[o + 1] : 0u, b2 = two ? s_S2[o + 1] : 0u;
+                    const int o = j * A.NRS + ring(i), o1 = j * A.NRS + ring(i + 1);
+                    const uint32_t b1 = two ? s_S1[o1] : 0u, b2 = two ? s_S2[o1] : 0u;
                     float2 bnd;
                     const float2 est = tc_estimate2(dv[v], dv[v + 1], s_S1[o], b1, s_S2[o], b2,
                                                     nnf, csf, kk, kk7, A.measure, &bnd);
@@ -2187,7 +2175,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
             unsigned long long best = 0ull;
             for (int c = tid; c < ncand; c += bd) {
                 const int i = static_cast<int>(s_cI[c] >> 16), j = static_cast<int>(s_cI[c] & 0xFFFFu);
-                const int o = j * A.NRS + i;
+                const int o = j * A.NRS + ring(i);
                 const float x = tc_exact(s_num[c], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
                 const unsigned long long key = argmax_key(x, static_cast<unsigned>(i * nc + j));
                 best = key > best ? key : best;
@@ -2210,8 +2198,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
             __syncthreads();
             float* so = A.surf_out + k * static_cast<int64_t>(A.NRM) * A.NCM;
             for (int e = tid; e < nr * nc; e += bd) {
-                const int o = (e / nr) * A.NRS + (e % nr);
-                so[e] = tc_exact(s_num[o], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+                const int o = (e / nr) * A.NRS + (e % nr), os = (e / nr) * A.NRS + ring(e % nr);
+                so[e] = tc_exact(s_num[o], s_S1[os], s_S2[os], mean, nn, cnorm, A.measure);
             }
         }
         const bool single = A.up == 1 || nr < 5 || nc < 5;
@@ -2230,14 +2218,14 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
                     __dadd_rn(static_cast<double>(pj - static_cast<int>(prx)), A.pts.dx0[k]));
                 A.out.dy[k] = __double2float_rn(
                     __dadd_rn(static_cast<double>(pi - static_cast<int>(pry)), A.pts.dy0[k]));
-                const int o = pj * A.NRS + pi;
+                const int o = pj * A.NRS + ring(pi);
                 A.out.corr[k] = tc_exact(s_pd[0], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
             }
         } else {
             const int slot = s_slot;
             if (tid < 25) {
                 const int a = tid % 5, b = tid / 5;
-                const int o = (pj0 + b) * A.NRS + (pi0 + a);
+                const int o = (pj0 + b) * A.NRS + ring(pi0 + a);
                 A.sub_patch[static_cast<int64_t>(slot) * 25 + tid] =
                     tc_exact(s_pd[tid], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
             }
