@@ -2280,6 +2280,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
 constexpr int kBfThreads = 256;
 constexpr int kBfAcc = 6;          // accumulators: limb pair (3) x chip-column parity (2)
 constexpr int kBfPadL = 16;        // zero elements before each staged chip column
+constexpr int kBfChunk = 8;        // largest chip-column chunk (accumulators flushed after each)
 
 struct BfArgs {
     const void* ref;
@@ -2471,15 +2472,42 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
             __syncthreads();
         }
 
-        // Clear the accumulators (one lane quarter per warp).
-        if (warp < 4) {
-            uint32_t z[16];
+        // The tensor core's FP32 accumulation does not round to nearest, so a long chain of
+        // products into one accumulator drifts (by ~1e-4 of the numerator over the ~1,000
+        // products per accumulator of a 192-px chip). Each chunk's products therefore go into
+        // cleared accumulators, and after the chunk every thread adds its values of the six
+        // accumulators into FP64 sums it keeps in registers: value v of a thread is surface
+        // row i = 32 half + 8 (v / 4) + 2 (lane % 4) + v % 2, column j = 16 quarter + lane / 4
+        // (+ 8 when v % 4 >= 2) -- the 16x256b read pattern of its lane quarter's half.
+        const int quarter = warp & 3, half = warp >> 2;
+        const uint32_t qbase = taddr + (static_cast<uint32_t>(32 * quarter) << 16) +
+                               static_cast<uint32_t>(32 * half);
+        double accd[16];
 #pragma unroll
-            for (int t = 0; t < 16; ++t) z[t] = 0u;
-            const uint32_t lq = taddr + (static_cast<uint32_t>(32 * warp) << 16);
-            for (int c = 0; c < kBfAcc * A.AC; c += 16) tc::tmem_st16(lq + static_cast<uint32_t>(c), z);
-            tc::tmem_wait_st();
-        }
+        for (int v = 0; v < 16; ++v) accd[v] = 0.0;
+        auto clear_acc = [&]() {
+            if (warp < 4) {
+                uint32_t z[16];
+#pragma unroll
+                for (int t = 0; t < 16; ++t) z[t] = 0u;
+                const uint32_t lq = taddr + (static_cast<uint32_t>(32 * warp) << 16);
+                for (int c = 0; c < kBfAcc * A.AC; c += 16) tc::tmem_st16(lq + static_cast<uint32_t>(c), z);
+                tc::tmem_wait_st();
+            }
+        };
+        auto flush_acc = [&]() {
+            if (32 * half < nr) {
+                for (int s = 0; s < kBfAcc; ++s) {
+                    uint32_t r[16];
+                    tc::tmem_ld16dp(qbase + static_cast<uint32_t>(s * A.AC), r);
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int v = 0; v < 16; ++v)
+                        accd[v] = __dadd_rn(accd[v], static_cast<double>(__uint_as_float(r[v])));
+                }
+            }
+        };
+        clear_acc();
 
         const int QB = (ch + nr - 1 + 15) / 16;
         const int nchunk = (cw + A.BC - 1) / A.BC;
@@ -2487,11 +2515,17 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
         for (int cc = 0; cc < nchunk && ok; ++cc) {
             const int b0 = cc * A.BC, bcn = min(A.BC, cw - b0);
             if (cc > 0) {
-                // The previous chunk's products must be done before its operands are replaced.
+                // The previous chunk's products must be done before its operands are replaced
+                // and its accumulators read out and cleared.
                 ok = tc::mbar_wait(&s_mbar, phase, kTcWaitPolls);
                 phase ^= 1u;
                 if (__syncthreads_or(!ok)) break;
                 tc::fence_after_sync();
+                flush_acc();
+                tc::fence_before_sync();
+                __syncthreads();  // every accumulator read before any is cleared
+                tc::fence_after_sync();
+                clear_acc();
             }
             // The chunk's chip columns C'[a, b0 + bl] as BF16 limbs, zero-padded.
             for (int e = tid; e < A.BC * A.PC; e += bd) {
@@ -2594,36 +2628,20 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
             break;
         }
         tc::fence_after_sync();
+        flush_acc();
 
-        // Epilogue: each warp reads its lane quarter's half (16x256b) of every accumulator;
-        // value v of a thread is surface row i = 32 half + 8 (v / 4) + 2 (lane % 4) + v % 2,
-        // column j = 16 quarter + lane / 4 (+ 8 when v % 4 >= 2). Every value is normalised in
-        // FP64 (src/correlate.jl:591-600, 624-628) into the surface in shared memory.
+        // Epilogue: every value is normalised in FP64 (src/correlate.jl:591-600, 624-628) into
+        // the surface in shared memory.
         {
-            const int quarter = warp & 3, half = warp >> 2;
             const int ib0 = 32 * half + 2 * (lane & 3);
             const int jb0 = 16 * quarter + (lane >> 2);
             if (32 * half < nr) {
-                float sum[16];
-                const uint32_t base = taddr + (static_cast<uint32_t>(32 * quarter) << 16) +
-                                      static_cast<uint32_t>(32 * half);
-                uint32_t r[16];
-                tc::tmem_ld16dp(base, r);
-                tc::tmem_wait_ld();
-#pragma unroll
-                for (int v = 0; v < 16; ++v) sum[v] = __uint_as_float(r[v]);
-                for (int s = 1; s < kBfAcc; ++s) {
-                    tc::tmem_ld16dp(base + static_cast<uint32_t>(s * A.AC), r);
-                    tc::tmem_wait_ld();
-#pragma unroll
-                    for (int v = 0; v < 16; ++v) sum[v] = __fadd_rn(sum[v], __uint_as_float(r[v]));
-                }
 #pragma unroll
                 for (int v = 0; v < 16; ++v) {
                     const int i = ib0 + 8 * (v >> 2) + (v & 1), j = jb0 + ((v & 2) ? 8 : 0);
                     if (i < nr && j < nc) {
                         const double s1 = s_S1[j * A.NRS + i], s2 = s_S2[j * A.NRS + i];
-                        const double num = __dadd_rn(static_cast<double>(sum[v]), __dmul_rn(cshift, sumd));
+                        const double num = __dadd_rn(accd[v], __dmul_rn(cshift, sumd));
                         double den;
                         if (A.measure == AR_NCC) {
                             den = __dmul_rn(cnorm, __dsqrt_rn(s2 > 0.0 ? s2 : 0.0));
@@ -3377,7 +3395,9 @@ bool plan_corr_bf(const PassGeometry& g, size_t smem_cap, BfPlan* P) {
     auto a16 = [](size_t v) { return (v + 15) & ~size_t(15); };
     const size_t Sb = a16(static_cast<size_t>(nc) * P->NRS * 8);
     const size_t red = 3 * 32 * 8;
-    for (int bc = cw; bc >= 2; bc -= 2) {
+    // At most kBfChunk chip columns per chunk: the FP32 accumulators are flushed to FP64 after
+    // every chunk, so each accumulates at most kBfChunk / 2 columns of products.
+    for (int bc = std::min(cw, kBfChunk) & ~1; bc >= 2; bc -= 2) {
         const int XC = bc + 63;
         const size_t Wb = 2 * static_cast<size_t>(P->QB) * 2 * XC * 16;
         const size_t Eb = 2 * static_cast<size_t>(bc) * 2 * P->NB * 16;
