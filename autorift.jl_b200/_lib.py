@@ -67,7 +67,7 @@ class ArRequest(ctypes.Structure):
 
 AR_PRE_NONE, AR_PRE_HIGHPASS, AR_PRE_WALLIS = 0, 1, 2
 AR_OPT_TENSOR_CORES, AR_OPT_SERVE_SLOTS, AR_OPT_SERVE_MEMORY_MB, AR_OPT_SPLIT_BF16 = 1, 2, 3, 4
-AR_OPT_AUTOTUNE = 5
+AR_OPT_AUTOTUNE, AR_OPT_SHAPE_BINS = 5, 6
 AR_QUANT_NONE, AR_QUANT_UINT8 = 0, 1
 
 

@@ -1100,6 +1100,7 @@ int ar_ctx_set_option(ar_ctx* c, int option, int value) {
     switch (option) {
         case AR_OPT_TENSOR_CORES: c->scratch.tensor_cores = value != 0; return AR_OK;
         case AR_OPT_AUTOTUNE: c->scratch.autotune = value != 0; return AR_OK;
+        case AR_OPT_SHAPE_BINS: c->scratch.shape_bins = value != 0; return AR_OK;
         case AR_OPT_SPLIT_BF16:
             if (value < 0 || value > 2) return fail(c, AR_ERR_ARG, "split-BF16 mode must be 0, 1 or 2");
             c->scratch.split_bf16 = value;

@@ -97,6 +97,9 @@ struct TrackScratch {
     // (identical results) are timed once per pass geometry and the fastest kept in `tuned`
     // (key: chip and surface extents) -- AR_OPT_AUTOTUNE.
     bool autotune = true;
+    // Multichip passes whose searchable points have both small (up to 64 x 64) and larger
+    // surfaces run each group as its own launch (AR_OPT_SHAPE_BINS).
+    bool shape_bins = true;
     std::map<uint64_t, int> tuned;
     cudaEvent_t tune_ev[2] = {nullptr, nullptr};
     // When set, the sub-pixel queue grows from this pool in stream order (no device-wide

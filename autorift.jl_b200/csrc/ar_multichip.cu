@@ -646,7 +646,7 @@ cudaError_t run_multichip(const MultichipJob& J, TrackScratch& scratch, int num_
         unsigned long long cnt[2];
         C.read(cnt, 2);
         if (err != cudaSuccess) return;
-        const bool split = cnt[0] > 0 && cnt[1] > 0;
+        const bool split = scratch.shape_bins && cnt[0] > 0 && cnt[1] > 0;
         for (int bin = split ? 0 : -1; bin <= (split ? 1 : -1); ++bin) {
             const int64_t ns = static_cast<int64_t>(bin < 0 ? cnt[0] + cnt[1] : cnt[bin]);
             if (ns == 0) continue;

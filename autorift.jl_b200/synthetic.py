@@ -197,3 +197,23 @@ def scale_u16_pair(n: int = 4096, seed: int = 11, max_amp: float = 15.0, noise: 
         covered += int(new.sum())
     b[holes] = 0
     return img1, b, ~holes, (fx, fy)
+
+
+def batching_points(n: int, fx_down, fy_down, seed: int = 3, spacing: int = 8, margin: int = 24):
+    """The batching configuration's point set on an n x n scene: fractional centres on a
+    `spacing` px lattice with +-0.5 px jitter, per-point search radii uniform in [4, 48], and
+    integer priors from the 4x-downsampled imposed feature motion (`fx_down`, `fy_down` =
+    f[::4, ::4]) rounded, plus a uniform error of up to 3 px (the tracker reports the negative of
+    the motion). Returns the PointSet fields x, y, radius, dx_prior, dy_prior as (m, m) arrays
+    in Julia's layout."""
+    rng = np.random.default_rng(seed)
+    c = np.arange(margin, n - margin, spacing, dtype=np.float64)
+    X, Y = np.meshgrid(c, c)  # rows follow y
+    X = np.asfortranarray(X + rng.uniform(-0.5, 0.5, X.shape))
+    Y = np.asfortranarray(Y + rng.uniform(-0.5, 0.5, Y.shape))
+    r = rng.integers(4, 49, X.shape)
+    iy = np.clip(np.round(Y - 1).astype(int) // 4, 0, fx_down.shape[0] - 1)
+    ix = np.clip(np.round(X - 1).astype(int) // 4, 0, fx_down.shape[1] - 1)
+    dx0 = np.round(-fx_down[iy, ix]) + rng.integers(-3, 4, X.shape)
+    dy0 = np.round(-fy_down[iy, ix]) + rng.integers(-3, 4, X.shape)
+    return X, Y, r, dx0, dy0

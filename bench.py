@@ -61,8 +61,11 @@ def workload(n, gr, gc):
             f"{RADIUS}, PyramidRefine({UP})")
 
 
-def scene(ar, n=N):
-    a, b, valid, _ = ar.synthetic.scale_u16_pair(n)
+def scene(ar, n=N, field=False):
+    """The benchmark pair of side n; with `field`, also the imposed motion downsampled 4x."""
+    a, b, valid, (fx, fy) = ar.synthetic.scale_u16_pair(n)
+    if field:
+        return a, b, valid, (np.ascontiguousarray(fx[::4, ::4]), np.ascontiguousarray(fy[::4, ::4]))
     return a, b, valid
 
 
@@ -667,10 +670,10 @@ class DeviceStep:
     """One step of the pipeline on a device-resident raw pair and grid: ar_prepare, then
     ar_multichip_device, on the context's stream."""
 
-    def __init__(self, ar, ctx, torch, dev, a, b, valid, p):
+    def __init__(self, ar, ctx, torch, dev, a, b, valid, p, grid=None):
         L = ar._lib
         self.ctx, self.lib = ctx, ctx.lib
-        self.grid = ar.build_grid(a.shape, p)
+        self.grid = grid if grid is not None else ar.build_grid(a.shape, p)
         self.gr, self.gc = self.grid.shape
         self.n = self.gr * self.gc
         self.raw = ar.ImagePair(a, b, None, valid).device(ctx)  # resident before timing
@@ -743,6 +746,49 @@ def host_e2e(ar, ctx, hostpair, hgrid, gr, gc, opts, prm, size, n, reps):
     return times, hout, hchip
 
 
+def batching_measure(ar, ctx, torch, dev, a, b, valid, fdown, stream, flush, args):
+    """The batching configuration on the benchmark pair: chip sizes 16/32/64/128 through the
+    multichip search over ~1.9 M jittered centres on an 8 px lattice with per-point radii
+    U[4, 48] (floored to 6 by sanitize!) and integer priors from the 4x-downsampled imposed
+    field +-3 px. Timed two ways on the device -- shape-binned passes with the autotuned kernel
+    choice (the default) and one launch per pass planned for its largest surface with the
+    default kernel rule -- with bit-identical results required."""
+    L = ar._lib
+    n = a.shape[0]
+    X, Y, r, dx0, dy0 = ar.synthetic.batching_points(n, fdown[0], fdown[1])
+    grid = ar.pointset(X, Y, search_radius_x=r, search_radius_y=r, chip_size=128,
+                       dx_prior=dx0, dy_prior=dy0)
+    p = ar.params(chip_size=16, chip_size_max=128, upsampling=UP)
+    step = DeviceStep(ar, ctx, torch, dev, a, b, valid, p, grid=grid)
+    out = {}
+    res = {}
+    steps = max(3, args.steps // 4)
+    for name, bins, tune in (("binned_autotuned", 1, 1), ("one_launch_per_pass", 0, 0)):
+        ctx.set_option(L.AR_OPT_SHAPE_BINS, bins)
+        ctx.set_option(L.AR_OPT_AUTOTUNE, tune)
+        t = timed_steps(torch, step, stream, flush, steps, args.warmup)
+        out[name] = {"points_per_s": step.n * steps / (t * 1e-3), "ms_per_step": t / steps}
+        res[name] = [o.cpu().numpy() for o in step.outs] + [step.ochip.cpu().numpy()]
+    ctx.set_option(L.AR_OPT_SHAPE_BINS, 1)
+    ctx.set_option(L.AR_OPT_AUTOTUNE, 1)
+    same = all(np.array_equal(x.view(np.uint32) if x.dtype == np.float32 else x,
+                              y.view(np.uint32) if y.dtype == np.float32 else y)
+               for x, y in zip(res["binned_autotuned"], res["one_launch_per_pass"]))
+    chip = res["binned_autotuned"][3].view(np.uint16)
+    out.update({"points": step.n, "grid": list(step.grid.shape), "steps": steps,
+                "speedup": out["one_launch_per_pass"]["ms_per_step"] /
+                           out["binned_autotuned"]["ms_per_step"],
+                "bit_identical": bool(same),
+                "points_per_chip_size": {int(c): int(np.count_nonzero(chip == c))
+                                         for c in np.unique(chip) if c},
+                "workload": f"multichip 16/32/64/128 on the {n}^2 benchmark pair, jittered 8 px "
+                            "lattice, radii U[4,48], priors from the 4x-downsampled field +-3 px "
+                            "(the benchmark scene's 15 px bumps: the 40 px scene of the "
+                            "batching configuration would add another scene generation to "
+                            "the run), PyramidRefine(64)"})
+    return out
+
+
 def gpu_arm(args):
     import torch
     import __graft_entry__ as ge
@@ -760,7 +806,7 @@ def gpu_arm(args):
     ar = ge.load_package()
     L = ar._lib
     ctx = L.Context(local)
-    a, b, valid = scene(ar, args.size)
+    a, b, valid, fdown = scene(ar, args.size, field=True)
     p = pipeline_params(ar, args.spacing if args.profile else SPACING)
     dev = torch.device("cuda", local)
     step = DeviceStep(ar, ctx, torch, dev, a, b, valid, p)
@@ -865,6 +911,14 @@ def gpu_arm(args):
     config_4096 = {"workload": workload(N_SCALE, step4.gr, step4.gc), "points": step4.n,
                    "value": v4rate, "ms_per_step": t4 / args.steps}
 
+    batching = None
+    if not args.profile:
+        try:
+            batching = batching_measure(ar, ctx, torch, dev, a, b, valid, fdown, stream, flush,
+                                        args)
+        except Exception as exc:  # reported, not fatal to the main measurement
+            batching = {"error": f"{type(exc).__name__}: {exc}"}
+
     rotation = None
     if not args.no_rotation:
         try:
@@ -965,6 +1019,7 @@ def gpu_arm(args):
             "oracle_crop": crop_check,
             "float32_subpixel": flips,
             "config_4096": config_4096,
+            "batching": batching,
             "serving": serving,
             "rotation_search": rotation,
             "clocks": clk.summary(),

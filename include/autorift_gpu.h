@@ -314,11 +314,15 @@ int ar_release(ar_ctx* ctx, ar_ticket ticket);
  * identical results (the two tensor-core kernels whose plans fit and the CUDA-core kernel) are
  * timed once per pass geometry on a sample of the pass, and the context runs the fastest from
  * then on; 0 always takes the first tensor-core kernel that fits.
+ * AR_OPT_SHAPE_BINS (default 1): a multichip pass whose searchable points include both surfaces
+ * of at most 64 x 64 and larger ones runs the two groups as separate launches, each planned for
+ * its own largest surface (per-point radii); 0 runs every pass as one launch. Results are the
+ * same either way.
  * AR_OPT_SERVE_SLOTS and AR_OPT_SERVE_MEMORY_MB configure the request loop (see ar_submit);
  * they must be set before the first ar_submit. No reference counterpart.
  */
 enum { AR_OPT_TENSOR_CORES = 1, AR_OPT_SERVE_SLOTS = 2, AR_OPT_SERVE_MEMORY_MB = 3,
-       AR_OPT_SPLIT_BF16 = 4, AR_OPT_AUTOTUNE = 5 };
+       AR_OPT_SPLIT_BF16 = 4, AR_OPT_AUTOTUNE = 5, AR_OPT_SHAPE_BINS = 6 };
 int ar_ctx_set_option(ar_ctx* ctx, int option, int value);
 
 /* The context's own CUDA stream (cudaStream_t), on which calls without a stream argument run;

@@ -23,19 +23,8 @@ pytestmark = pytest.mark.gpu
 
 
 def batching_points(ar, n, fx, fy, seed=3, spacing=8, margin=24):
-    rng = np.random.default_rng(seed)
-    c = np.arange(margin, n - margin, spacing, dtype=np.float64)
-    X, Y = np.meshgrid(c, c)  # rows follow y
-    X = np.asfortranarray(X + rng.uniform(-0.5, 0.5, X.shape))
-    Y = np.asfortranarray(Y + rng.uniform(-0.5, 0.5, Y.shape))
-    r = rng.integers(4, 49, X.shape)
-    # The tracker reports the negative of the feature motion; priors from a 4x-downsampled
-    # copy of it, rounded, plus a uniform error of up to 3 px.
-    down = lambda f: f[::4, ::4]
-    iy = np.clip(np.round(Y - 1).astype(int) // 4, 0, n // 4 - 1)
-    ix = np.clip(np.round(X - 1).astype(int) // 4, 0, n // 4 - 1)
-    dx0 = np.round(-down(fx)[iy, ix]) + rng.integers(-3, 4, X.shape)
-    dy0 = np.round(-down(fy)[iy, ix]) + rng.integers(-3, 4, X.shape)
+    X, Y, r, dx0, dy0 = ar.synthetic.batching_points(n, fx[::4, ::4], fy[::4, ::4], seed,
+                                                     spacing, margin)
     return ar.pointset(X, Y, search_radius_x=r, search_radius_y=r, chip_size=128,
                        dx_prior=dx0, dy_prior=dy0)
 
