@@ -789,6 +789,103 @@ def batching_measure(ar, ctx, torch, dev, a, b, valid, fdown, stream, flush, arg
     return out
 
 
+def bf16_executed_flops(ch, cw, nr):
+    """Tensor-core FLOPs k_corr_bf executes for one point: per 16-row window block the products
+    of M = 64 surface columns, the block's trimmed operand rows and K = 16, for every chip
+    column and the three limb pairs."""
+    NB = (ch + 15 + 15) // 16 * 16
+    QB = (ch + nr - 1 + 15) // 16
+    rows = 0
+    for q in range(QB):
+        lo = max(0, NB - 16 - 16 * q)
+        hi = min(NB, NB - 16 + nr - 16 * q)
+        if hi > lo:
+            elo = lo & ~15
+            rows += (hi - elo + 15) & ~15
+    return 2.0 * 64 * 16 * rows * cw * 3
+
+
+def precision_measure(ar, ctx, torch, dev, a4, b4, v4, fdown4, stream, flush, args, tensor_peak):
+    """The precision configuration on the 4096^2 pair: the default pipeline restricted to chip
+    sizes 64 and 128 at search radius 32, unquantised (highpass Float32), its correlation
+    numerators computed three ways -- split BF16 on the tensor cores, direct FP32 on CUDA cores
+    (AR_OPT_SPLIT_BF16 = 1 / 0) and the oracle's FP64 -- on a seeded 1% sample of the chip-64
+    grid: max |dNCC|, integer-peak agreement (integer offsets identical), sub-pixel |dd|, and the
+    error against the imposed field; plus each variant's device-timed pass over the whole grid
+    and the split-BF16 kernel's rate against the tensor-pipe peak."""
+    from oracle import oracle as O
+    L = ar._lib
+    O.build()
+    out = {"workload": "chip 64 and 128, radius 32, highpass Float32 (quantize = :none) on the "
+                       "4096^2 benchmark pair: one track pass over the spacing-8 grid per chip "
+                       "size; the oracle on a seeded 1% sample"}
+    fx_d, fy_d = fdown4
+    for chip in (64, 128):
+        p = ar.params(chip_size=chip, search_radius=32, quantize="none", upsampling=UP)
+        grid = ar.gridpoints(a4.shape, 8, chip_size=chip, search_radius=32)
+        n = len(grid)
+        cols = {f: torch.from_numpy(grid.flat(f)).to(dev) for f in ar.points.FIELDS}
+        pts = L.ArPoints(*(cols[f].data_ptr() for f in ar.points.FIELDS), n)
+        outs = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3)]
+        srch = torch.empty(n, dtype=torch.uint8, device=dev)
+        idx, fl = sample_fields(ar, grid, 0.01, seed=7, chip=chip)
+        row = {"points": n}
+        want = None
+        for name, mode in (("split_bf16", 1), ("direct_fp32", 0)):
+            ctx.set_option(L.AR_OPT_SPLIT_BF16, mode)
+            prep = ar.prepare(ar.ImagePair(a4, b4, None, v4), p, ctx)
+            h = prep.device(ctx).handle
+
+            def call():
+                ctx.check(ctx.lib.ar_track_device(ctx.handle, h, ctypes.byref(pts), UP, L.AR_ZNCC,
+                                                  outs[0].data_ptr(), outs[1].data_ptr(),
+                                                  outs[2].data_ptr(), srch.data_ptr(), None))
+            timed_steps(torch, call, stream, flush, 0, 1)
+            ctx.set_timing(True)
+            ctx.kernel_times()
+            t = timed_steps(torch, call, stream, flush, 2, 0)
+            corr_ms, refine_ms, tracks, _, flops = ctx.kernel_times()
+            ctx.set_timing(False)
+            dx = outs[0].cpu().numpy()
+            r = {"points_per_s": 2 * n / (t * 1e-3), "k_corr_ms": corr_ms / 2,
+                 "k_refine_ms": refine_ms / 2,
+                 "algorithmic_tflops": flops / (corr_ms * 1e-3) / 1e12 if corr_ms > 0 else None}
+            if mode == 1 and corr_ms > 0:
+                executed = bf16_executed_flops(chip, chip, 64) * (flops / (2.0 * chip * chip * 64 * 64))
+                r["executed_tensor_tflops"] = executed / (corr_ms * 1e-3) / 1e12
+                r["frac_of_bf16_peak"] = r["executed_tensor_tflops"] / tensor_peak
+            # Accuracy on the sample, against the oracle (FP64 numerator) and the imposed field.
+            st = L.ArPoints(*(fl[f].ctypes.data for f in ar.points.FIELDS), idx.size)
+            g = [np.empty(idx.size, np.float32) for _ in range(3)] + [np.empty(idx.size, np.uint8)]
+            ctx.check(ctx.lib.ar_track(ctx.handle, h, ctypes.byref(st), UP, L.AR_ZNCC,
+                                       *(x.ctypes.data for x in g)))
+            if want is None:
+                ref, sec, rv, sv = prep.download()
+                want = O.track(ref, sec, fl, upsampling=UP, reference_valid=rv, secondary_valid=sv)
+                wi = O.track(ref, sec, fl, upsampling=1, reference_valid=rv, secondary_valid=sv)
+            gi = [np.empty(idx.size, np.float32) for _ in range(3)] + [np.empty(idx.size, np.uint8)]
+            ctx.check(ctx.lib.ar_track(ctx.handle, h, ctypes.byref(st), 1, L.AR_ZNCC,
+                                       *(x.ctypes.data for x in gi)))
+            m = ~np.isnan(g[0]) & ~np.isnan(want[0])
+            d = np.maximum(np.abs(g[0] - want[0]), np.abs(g[1] - want[1]))[m]
+            mi = ~np.isnan(gi[0]) & ~np.isnan(wi[0])
+            same_int = (gi[0][mi] == wi[0][mi]) & (gi[1][mi] == wi[1][mi])
+            iy = np.clip(np.round(fl["y"] - 1).astype(int) // 4, 0, fx_d.shape[0] - 1)
+            ix = np.clip(np.round(fl["x"] - 1).astype(int) // 4, 0, fx_d.shape[1] - 1)
+            fe = np.hypot(g[0] + fx_d[iy, ix], g[1] + fy_d[iy, ix])[~np.isnan(g[0])]
+            r.update({"sample_points": int(idx.size), "measured": int(m.sum()),
+                      "max_abs_dncc": float(np.abs(g[2] - want[2])[m].max()) if m.any() else None,
+                      "integer_peak_agreement": float(same_int.mean()) if mi.any() else None,
+                      "subpixel_max_abs_dd_px": float(d.max()) if d.size else None,
+                      "subpixel_over_1e-3px": float(np.mean(d > 1e-3)) if d.size else None,
+                      "median_error_vs_field_px": float(np.median(fe)) if fe.size else None})
+            row[name] = r
+            del prep
+        ctx.set_option(L.AR_OPT_SPLIT_BF16, 1)
+        out[f"chip_{chip}"] = row
+    return out
+
+
 def gpu_arm(args):
     import torch
     import __graft_entry__ as ge
@@ -904,12 +1001,22 @@ def gpu_arm(args):
             cpu = None  # the host baseline is a single-process figure
 
     # The at-scale configuration's 4096^2 pair, timed the same way (device-resident).
-    a4, b4, v4 = scene(ar, N_SCALE)
+    a4, b4, v4, fdown4 = scene(ar, N_SCALE, field=True)
     step4 = DeviceStep(ar, ctx, torch, dev, a4, b4, v4, p)
     t4 = timed_steps(torch, step4, stream, flush, args.steps, args.warmup, dist)
     t4, v4rate = replicas_rate(dist, t4, step4.n, args.steps, dev)
     config_4096 = {"workload": workload(N_SCALE, step4.gr, step4.gc), "points": step4.n,
                    "value": v4rate, "ms_per_step": t4 / args.steps}
+
+    peaks = measured_peaks()
+    tensor_peak = float(peaks["bf16_tflops"]) if peaks.get("bf16_tflops") else 1590.0
+    precision = None
+    if rank == 0:
+        try:
+            precision = precision_measure(ar, ctx, torch, dev, a4, b4, v4, fdown4, stream, flush,
+                                          args, tensor_peak)
+        except Exception as exc:  # reported, not fatal to the main measurement
+            precision = {"error": f"{type(exc).__name__}: {exc}"}
 
     batching = None
     if not args.profile:
@@ -1020,6 +1127,7 @@ def gpu_arm(args):
             "float32_subpixel": flips,
             "config_4096": config_4096,
             "batching": batching,
+            "precision": precision,
             "serving": serving,
             "rotation_search": rotation,
             "clocks": clk.summary(),
