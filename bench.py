@@ -1139,6 +1139,45 @@ def gpu_arm(args):
         dist.destroy_process_group()
 
 
+def profile_precision_arm(args):
+    """For ncu captures of the split-BF16 kernel: the chip-64 / radius-32 track pass over the
+    highpass-filtered Float32 --size pair at grid spacing --spacing (default pipeline otherwise),
+    `--warmup` untimed passes then `--steps` timed ones; prints one line of timings."""
+    import torch
+    import __graft_entry__ as ge
+
+    ge.build()
+    ar = ge.load_package()
+    L = ar._lib
+    ctx = L.Context(0)
+    a, b, v = scene(ar, args.size)
+    p = ar.params(chip_size=64, search_radius=32, quantize="none", upsampling=UP)
+    grid = ar.gridpoints(a.shape, args.spacing, chip_size=64, search_radius=32)
+    prep = ar.prepare(ar.ImagePair(a, b, None, v), p, ctx)
+    dev = torch.device("cuda", 0)
+    n = len(grid)
+    cols = {f: torch.from_numpy(grid.flat(f)).to(dev) for f in ar.points.FIELDS}
+    pts = L.ArPoints(*(cols[f].data_ptr() for f in ar.points.FIELDS), n)
+    outs = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3)]
+    srch = torch.empty(n, dtype=torch.uint8, device=dev)
+    h = prep.device(ctx).handle
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+
+    def call():
+        ctx.check(ctx.lib.ar_track_device(ctx.handle, h, ctypes.byref(pts), UP, L.AR_ZNCC,
+                                          outs[0].data_ptr(), outs[1].data_ptr(),
+                                          outs[2].data_ptr(), srch.data_ptr(), None))
+    timed_steps(torch, call, stream, flush, 0, args.warmup)
+    ctx.set_timing(True)
+    ctx.kernel_times()
+    t = timed_steps(torch, call, stream, flush, args.steps, 0)
+    corr_ms, refine_ms, _, _, flops = ctx.kernel_times()
+    print(json.dumps({"profile_precision": True, "points": n, "ms_per_pass": t / args.steps,
+                      "k_corr_ms": corr_ms / args.steps, "k_refine_ms": refine_ms / args.steps,
+                      "algorithmic_tflops": flops / (corr_ms * 1e-3) / 1e12 if corr_ms else None}))
+
+
 def serve_arm(args):
     """The serving configuration: a seeded Poisson stream of UInt16 pairs of sides 512, 2048,
     4096 and 10980 in proportion 8:4:2:1, each with its own grid spacing, chip and radius;
@@ -1219,6 +1258,8 @@ def main():
                     help="image side; the benchmark line uses 10980, profiles a smaller scene")
     ap.add_argument("--profile", action="store_true",
                     help="time the device steps only (for ncu captures); no JSON bench line")
+    ap.add_argument("--profile-precision", action="store_true",
+                    help="time the chip-64 split-BF16 track pass only (for ncu captures)")
     ap.add_argument("--spacing", type=int, default=SPACING,
                     help="grid spacing of a --profile run (the benchmark line always uses 8)")
     args = ap.parse_args()
@@ -1226,6 +1267,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         reference_arm(args)
+    elif args.profile_precision:
+        profile_precision_arm(args)
     elif args.serve:
         serve_arm(args)
     else:
