@@ -2258,10 +2258,12 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
 // prepare_chip! (src/correlate.jl:423-453: Float32(x - mean)) and W' the window shifted by the
 // same centring constant k_corr uses (Float32(w - cshift); num = sum C' W' + cshift sum C'),
 // as products on the tensor cores (tcgen05.mma kind::f16, BF16 operands, FP32 accumulators in
-// Tensor Memory). Each operand is split into two BF16 limbs, v = hi + lo with hi = bf16(v) and
-// lo = bf16(v - hi), and the numerator is the sum of the three products hi*hi + hi*lo + lo*hi:
-// about 16 significant bits per operand, exact for the integer windows of UInt16 and Int16
-// imagery (an integer below 2^16 in magnitude is the sum of two BF16 values).
+// Tensor Memory). Each operand is split into three BF16 limbs, v = v0 + v1 + v2 with
+// v0 = bf16(v), v1 = bf16(v - v0), v2 = bf16(v - v0 - v1) (24 significant bits: a Float32 value
+// to within 2^-24 of itself), and the numerator is the sum of the six products whose order is
+// at least 2^-16 -- c0 w0, c0 w1, c1 w0, c1 w1, c2 w0, c0 w2 -- which recovers FP32 accuracy.
+// The integer windows of UInt16 and Int16 imagery are exactly w0 + w1 (an integer below 2^16 in
+// magnitude is the sum of two BF16 values), so their c0 w2 product is skipped.
 //
 // Layout (as the UInt8 kernels, with 2-byte elements and one chip column per product):
 //   A[j, (q, b, r)] = W'[16 q + r, j + b]    r < 16, stored as two 8-row halves h:
@@ -2270,17 +2272,17 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
 //   B[i, (q, b, r)] = E_b[i - 16 q][r]       E_b[u][r] = C'[r - u, b], stored s_E[limb][b][h][e].
 // Block q meets surface rows [16 q - ch + 1, 16 q + 15]: NB = 16 ceil((ch + 15) / 16) operand rows,
 // surface row i in accumulator column i (rows trimmed to 0 <= i < nr in steps of 16). Six
-// threads issue the products -- the three limb pairs, each for even and odd chip columns into an
-// accumulator of its own -- and the epilogue adds the six in FP32.
+// threads issue the products, one limb pair each into an accumulator of its own.
 // The chip columns come in chunks of BC (the window columns a chunk reaches are staged with
 // it). Box sums (integral_both!, boxsum, src/integral.jl:141-170, 244-247) are FP64 from the
 // image values, the normalisation the reference's FP64 formula (src/correlate.jl:575-630), each
 // surface value computed from its FP32 numerator. Surfaces up to 64 x 64.
 
 constexpr int kBfThreads = 256;
-constexpr int kBfAcc = 6;          // accumulators: limb pair (3) x chip-column parity (2)
+constexpr int kBfAcc = 6;          // accumulators: one per limb pair
+constexpr int kBfLimbs = 3;        // BF16 limbs per operand
 constexpr int kBfPadL = 16;        // zero elements before each staged chip column
-constexpr int kBfChunk = 8;        // largest chip-column chunk (accumulators flushed after each)
+constexpr int kBfChunk = 4;        // largest chip-column chunk (accumulators flushed after each)
 
 struct BfArgs {
     const void* ref;
@@ -2311,12 +2313,17 @@ struct BfArgs {
     int* status;
 };
 
-// The two BF16 limbs of v, as raw 16-bit patterns: hi = bf16(v), lo = bf16(v - hi).
-__device__ __forceinline__ void bf16_split(float v, uint32_t* hi, uint32_t* lo) {
-    const __nv_bfloat16 h = __float2bfloat16_rn(v);
-    const __nv_bfloat16 l = __float2bfloat16_rn(__fsub_rn(v, __bfloat162float(h)));
-    *hi = static_cast<uint32_t>(__bfloat16_as_ushort(h));
-    *lo = static_cast<uint32_t>(__bfloat16_as_ushort(l));
+// The three BF16 limbs of v, as raw 16-bit patterns: l[0] = bf16(v), l[1] = bf16(v - l[0]),
+// l[2] = bf16(v - l[0] - l[1]). Each difference is exact in FP32 (its operands are within a
+// factor of two of each other), so v - (l[0] + l[1] + l[2]) is below 2^-24 |v|.
+__device__ __forceinline__ void bf16_split3(float v, uint32_t (&l)[kBfLimbs]) {
+    float r = v;
+#pragma unroll
+    for (int t = 0; t < kBfLimbs; ++t) {
+        const __nv_bfloat16 h = __float2bfloat16_rn(r);
+        l[t] = static_cast<uint32_t>(__bfloat16_as_ushort(h));
+        r = __fsub_rn(r, __bfloat162float(h));
+    }
 }
 
 template <typename T>
@@ -2330,7 +2337,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
     const int lane = tid & 31, warp = tid >> 5;
     const T* ref = static_cast<const T*>(A.ref);
     const T* sec = static_cast<const T*>(A.sec);
-    // Operand buffers, two limbs each: window [limb][q][h][x], chip operand [limb][b][h][e],
+    // Operand buffers, three limbs each: window [limb][q][h][x], chip operand [limb][b][h][e],
     // staged chip columns [limb][b][PC] (raw BF16 bits). Box sums S1, S2 [j][NRS] (FP64).
     unsigned char* s_W = smem_bf + A.off_W;
     unsigned char* s_E = smem_bf + A.off_E;
@@ -2531,13 +2538,13 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
             for (int e = tid; e < A.BC * A.PC; e += bd) {
                 const int bl = e / A.PC, t = e - bl * A.PC;
                 const int a = t - kBfPadL;
-                uint32_t hi = 0u, lo = 0u;
+                uint32_t l[kBfLimbs] = {0u, 0u, 0u};
                 if (bl < bcn && a >= 0 && a < ch) {
                     const double d = __dsub_rn(pixel(sec, A.nrows, A.ncols, chip_r + a, chip_c + b0 + bl), mean);
-                    bf16_split(__double2float_rn(d), &hi, &lo);
+                    bf16_split3(__double2float_rn(d), l);
                 }
-                s_P[e] = static_cast<uint16_t>(hi);
-                s_P[plimb + e] = static_cast<uint16_t>(lo);
+#pragma unroll
+                for (int limb = 0; limb < kBfLimbs; ++limb) s_P[limb * plimb + e] = static_cast<uint16_t>(l[limb]);
             }
             // Window blocks: item (x, q, h) = 8 consecutive rows of window column b0 + x, both
             // limbs; consecutive threads take consecutive row groups of one column.
@@ -2545,25 +2552,28 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
             for (int it = tid; it < A.XC * gpc; it += bd) {
                 const int x = it / gpc, g = it - x * gpc;
                 const int q = g >> 1, h = g & 1;
-                uint32_t hw[4] = {0, 0, 0, 0}, lw[4] = {0, 0, 0, 0};
+                uint32_t lw[kBfLimbs][4] = {};
                 if (x < bcn + nc - 1) {
                     const int64_t c = win_c + b0 + x;
                     const int64_t r0 = win_r + 16 * q + 8 * h;
 #pragma unroll
                     for (int t = 0; t < 8; ++t) {
                         const int a = 16 * q + 8 * h + t;  // window row
-                        uint32_t hi = 0u, lo = 0u;
+                        uint32_t l[kBfLimbs] = {0u, 0u, 0u};
                         if (a < ch + nr - 1) {
                             const double w = pixel(ref, A.nrows, A.ncols, r0 + t, c);
-                            bf16_split(__double2float_rn(__dsub_rn(w, cshift)), &hi, &lo);
+                            bf16_split3(__double2float_rn(__dsub_rn(w, cshift)), l);
                         }
-                        hw[t >> 1] |= hi << (16 * (t & 1));
-                        lw[t >> 1] |= lo << (16 * (t & 1));
+#pragma unroll
+                        for (int limb = 0; limb < kBfLimbs; ++limb)
+                            lw[limb][t >> 1] |= l[limb] << (16 * (t & 1));
                     }
                 }
                 const size_t o = (static_cast<size_t>(q * 2 + h) * A.XC + x) * 16;
-                *reinterpret_cast<uint4*>(s_W + o) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-                *reinterpret_cast<uint4*>(s_W + wlimb + o) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+#pragma unroll
+                for (int limb = 0; limb < kBfLimbs; ++limb)
+                    *reinterpret_cast<uint4*>(s_W + limb * wlimb + o) =
+                        make_uint4(lw[limb][0], lw[limb][1], lw[limb][2], lw[limb][3]);
             }
             __syncthreads();  // s_P complete
             // Chip operand rows: E_b[h][e] = 8 elements of the staged column from element
@@ -2574,7 +2584,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                 const int src = kBfPadL + 8 * h - e + A.NB - 16;  // element index, >= 1
                 const size_t o = (static_cast<size_t>(bl * 2 + h) * A.NB + e) * 16;
 #pragma unroll
-                for (int limb = 0; limb < 2; ++limb) {
+                for (int limb = 0; limb < kBfLimbs; ++limb) {
                     const uint16_t* col = s_P + limb * plimb + bl * A.PC;
                     const uint32_t* w = reinterpret_cast<const uint32_t*>(col + (src & ~1));
                     const uint32_t sh = (src & 1) ? 16u : 0u;
@@ -2589,13 +2599,17 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
             tc::fence_proxy_async_smem();
             tc::fence_before_sync();
             __syncthreads();  // operands complete
-            // Six threads (lane 0 of warps 2..7) issue the chunk's products: limb pair p
-            // (hi*hi, hi*lo, lo*hi) for the chip columns of parity `par`.
+            // Six threads (lane 0 of warps 2..7) issue the chunk's products, thread s the limb
+            // pair (chip limb, window limb) = (0,0), (0,1), (1,0), (1,1), (2,0), (0,2) into
+            // accumulator s; integer windows have no third limb.
             if (lane == 0 && warp >= 2) {
-                const int s = warp - 2, p = s >> 1, par = s & 1;
+                const int s = warp - 2;
+                const int cl = s == 2 || s == 3 ? 1 : s == 4 ? 2 : 0;
+                const int wl = s == 1 || s == 3 ? 1 : s == 5 ? 2 : 0;
+                const int bstart = (Tr::integer && s == 5) ? bcn : 0;
                 tc::fence_after_sync();
-                const uint32_t wb = tc::smem_u32(s_W) + (p == 2 ? static_cast<uint32_t>(wlimb) : 0u);
-                const uint32_t eb = tc::smem_u32(s_E) + (p == 1 ? static_cast<uint32_t>(elimb) : 0u);
+                const uint32_t wb = tc::smem_u32(s_W) + static_cast<uint32_t>(wl * wlimb);
+                const uint32_t eb = tc::smem_u32(s_E) + static_cast<uint32_t>(cl * elimb);
                 const uint64_t da0 = tc::smem_desc(wb, static_cast<uint32_t>(A.XC * 16), 128);
                 const uint64_t db0 = tc::smem_desc(eb, static_cast<uint32_t>(A.NB * 16), 128);
                 const uint32_t a_hi = static_cast<uint32_t>(da0 >> 32);
@@ -2606,7 +2620,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                     if (!block_rows(q, A.NB, nr, &elo, &n)) continue;
                     const uint32_t idesc = tc::idesc_bf16_f32(64, n);
                     const uint32_t dcol = static_cast<uint32_t>(16 * q + elo - (A.NB - 16));
-                    for (int bl = par; bl < bcn; bl += 2) {
+                    for (int bl = bstart; bl < bcn; ++bl) {
                         // A: block q, first half, window column x = bl (row j at x = bl + j).
                         const uint32_t a_lo = static_cast<uint32_t>(da0) +
                                               static_cast<uint32_t>((q * 2) * A.XC + bl);
@@ -3396,12 +3410,12 @@ bool plan_corr_bf(const PassGeometry& g, size_t smem_cap, BfPlan* P) {
     const size_t Sb = a16(static_cast<size_t>(nc) * P->NRS * 8);
     const size_t red = 3 * 32 * 8;
     // At most kBfChunk chip columns per chunk: the FP32 accumulators are flushed to FP64 after
-    // every chunk, so each accumulates at most kBfChunk / 2 columns of products.
+    // every chunk, so each accumulates at most kBfChunk columns of products.
     for (int bc = std::min(cw, kBfChunk) & ~1; bc >= 2; bc -= 2) {
         const int XC = bc + 63;
-        const size_t Wb = 2 * static_cast<size_t>(P->QB) * 2 * XC * 16;
-        const size_t Eb = 2 * static_cast<size_t>(bc) * 2 * P->NB * 16;
-        const size_t Pb = a16(2 * static_cast<size_t>(bc) * P->PC * 2);
+        const size_t Wb = kBfLimbs * static_cast<size_t>(P->QB) * 2 * XC * 16;
+        const size_t Eb = kBfLimbs * static_cast<size_t>(bc) * 2 * P->NB * 16;
+        const size_t Pb = a16(kBfLimbs * static_cast<size_t>(bc) * P->PC * 2);
         const size_t alias = Wb + Eb + Pb;  // box-sum column sums, then the surface, reuse it
         const size_t surf = static_cast<size_t>(nc) * P->NRS * 4;
         if (alias < surf || alias < static_cast<size_t>(XW) * 16) continue;
