@@ -809,8 +809,8 @@ def precision_measure(ar, ctx, torch, dev, a4, b4, v4, fdown4, stream, flush, ar
     """The precision configuration on the 4096^2 pair: the default pipeline restricted to chip
     sizes 64 and 128 at search radius 32, unquantised (highpass Float32), its correlation
     numerators computed three ways -- split BF16 on the tensor cores, direct FP32 on CUDA cores
-    (AR_OPT_SPLIT_BF16 = 1 / 0) and the oracle's FP64 -- on a seeded 1% sample of the chip-64
-    grid: max |dNCC|, integer-peak agreement (integer offsets identical), sub-pixel |dd|, and the
+    (AR_OPT_SPLIT_BF16 = 1 / 0) and the oracle's FP64 -- on a seeded sample of each grid:
+    max |dNCC|, integer-peak agreement (integer offsets identical), sub-pixel |dd|, and the
     error against the imposed field; plus each variant's device-timed pass over the whole grid
     and the split-BF16 kernel's rate against the tensor-pipe peak."""
     from oracle import oracle as O
@@ -818,7 +818,7 @@ def precision_measure(ar, ctx, torch, dev, a4, b4, v4, fdown4, stream, flush, ar
     O.build()
     out = {"workload": "chip 64 and 128, radius 32, highpass Float32 (quantize = :none) on the "
                        "4096^2 benchmark pair: one track pass over the spacing-8 grid per chip "
-                       "size; the oracle on a seeded 1% sample"}
+                       "size; the oracle on a seeded sample (0.5% at chip 64, 0.25% at 128)"}
     fx_d, fy_d = fdown4
     for chip in (64, 128):
         p = ar.params(chip_size=chip, search_radius=32, quantize="none", upsampling=UP)
@@ -828,7 +828,9 @@ def precision_measure(ar, ctx, torch, dev, a4, b4, v4, fdown4, stream, flush, ar
         pts = L.ArPoints(*(cols[f].data_ptr() for f in ar.points.FIELDS), n)
         outs = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3)]
         srch = torch.empty(n, dtype=torch.uint8, device=dev)
-        idx, fl = sample_fields(ar, grid, 0.01, seed=7, chip=chip)
+        # The oracle's FP64 numerator costs 2 chip area x surface area per point per pass:
+        # a 0.5% sample at chip 64, 0.25% at chip 128.
+        idx, fl = sample_fields(ar, grid, 0.005 if chip == 64 else 0.0025, seed=7, chip=chip)
         row = {"points": n}
         want = None
         for name, mode in (("split_bf16", 1), ("direct_fp32", 0)):
