@@ -2307,34 +2307,44 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
 // Split-BF16 tensor-core correlation for UInt16, Int16 and Float32 imagery (k_corr_bf).
 //
 // The numerator of the CUDA-core kernel, sum_{a,b} C'[a, b] W'[i + a, j + b], with C' the chip of
-// prepare_chip! (src/correlate.jl:423-453: Float32(x - mean)) and W' the window shifted by the
-// same centring constant k_corr uses (Float32(w - cshift); num = sum C' W' + cshift sum C'),
-// as products on the tensor cores (tcgen05.mma kind::f16, BF16 operands, FP32 accumulators in
-// Tensor Memory). Each operand is split into three BF16 limbs, v = v0 + v1 + v2 with
-// v0 = bf16(v), v1 = bf16(v - v0), v2 = bf16(v - v0 - v1) (24 significant bits: a Float32 value
-// to within 2^-24 of itself), and the numerator is the sum of the six products whose order is
-// at least 2^-16 -- c0 w0, c0 w1, c1 w0, c1 w1, c2 w0, c0 w2 -- which recovers FP32 accuracy.
-// The integer windows of UInt16 and Int16 imagery are exactly w0 + w1 (an integer below 2^16 in
-// magnitude is the sum of two BF16 values), so their c0 w2 product is skipped.
+// prepare_chip! (src/correlate.jl:423-453: Float32(x - mean)) and W' the window shifted by a
+// centring constant (W' = Float32(w - cshift), cshift the chip mean rounded to an integer for
+// integer imagery and to Float32 otherwise; num = sum C' W' + cshift sum C'), as products on the
+// tensor cores (tcgen05.mma kind::f16, BF16 operands, FP32 accumulators in Tensor Memory). Each
+// operand is split into three BF16 limbs, v = v0 + v1 + v2 with v0 = bf16(v), v1 = bf16(v - v0),
+// v2 = bf16(v - v0 - v1) (24 significant bits: a Float32 value exactly), and the numerator is the
+// sum of the six products whose order is at least 2^-16 -- c0 w0, c0 w1, c1 w0, c1 w1, c2 w0,
+// c0 w2 -- which recovers FP32 accuracy. The integer windows of UInt16 and Int16 imagery are
+// exactly w0 + w1 (an integer below 2^16 in magnitude is the sum of two BF16 values), so their
+// c0 w2 product is skipped.
 //
 // Layout (as the UInt8 kernels, with 2-byte elements and one chip column per product):
 //   A[j, (q, b, r)] = W'[16 q + r, j + b]    r < 16, stored as two 8-row halves h:
 //                                            s_W[limb][q][h][x] (16 bytes), row j of A 16 bytes
-//                                            after row j - 1, the halves LBO apart;
+//                                            after row j - 1, the halves LW x 16 bytes apart;
 //   B[i, (q, b, r)] = E_b[i - 16 q][r]       E_b[u][r] = C'[r - u, b], stored s_E[limb][b][h][e].
 // Block q meets surface rows [16 q - ch + 1, 16 q + 15]: NB = 16 ceil((ch + 15) / 16) operand rows,
-// surface row i in accumulator column i (rows trimmed to 0 <= i < nr in steps of 16). Six
-// threads issue the products, one limb pair each into an accumulator of its own.
-// The chip columns come in chunks of BC (the window columns a chunk reaches are staged with
-// it). Box sums (integral_both!, boxsum, src/integral.jl:141-170, 244-247) are FP64 from the
-// image values, the normalisation the reference's FP64 formula (src/correlate.jl:575-630), each
-// surface value computed from its FP32 numerator. Surfaces up to 64 x 64.
+// surface row i in accumulator column i (rows trimmed to 0 <= i < nr in steps of 16).
+//
+// Per point: the chip's statistics; the window's box sums (integral_both!, boxsum,
+// src/integral.jl:141-170, 244-247) in FP64 from the image values, a stripe of window columns
+// at a time in shared memory -- column sums of ch rows, then a running sum along each surface
+// row whose differences cw columns apart are the box sums -- and from them each surface value's
+// FP64 denominator (src/correlate.jl:575-630); then the window's limbs for as many chip columns
+// as shared memory holds (all of them up to 64-px chips), and the products chunk by chunk of BC
+// chip columns. Two accumulator sets (one for c0 w0, one for the five smaller products) take
+// alternate chunks: while the tensor core runs chunk c, the threads build chunk c + 1's chip
+// operand and add chunk c - 1's accumulators into FP64 sums they keep in registers (the tensor
+// core's FP32 accumulation does not round to nearest, so a long chain of products into one
+// accumulator drifts: ~1e-4 of the numerator over the ~1,000 products per accumulator of a 192-px
+// chip; a chunk's chain is kept near kBfChain). Surfaces up to 64 x 64.
 
 constexpr int kBfThreads = 256;
-constexpr int kBfAcc = 6;          // accumulators: one per limb pair
 constexpr int kBfLimbs = 3;        // BF16 limbs per operand
 constexpr int kBfPadL = 16;        // zero elements before each staged chip column
-constexpr int kBfChunk = 4;        // largest chip-column chunk (accumulators flushed after each)
+constexpr int kBfChain = 20;       // accumulating products per accumulator element per chunk
+constexpr int kBfPre = 4;          // staged chip elements per thread and chunk
+constexpr int kBfBatch = 8;        // global loads a thread issues before using them
 
 struct BfArgs {
     const void* ref;
@@ -2346,14 +2356,18 @@ struct BfArgs {
     int up, measure;
     int CHM, CWM, NRM, NCM;
     int NB;                          // chip operand rows per column (multiple of 16)
-    int QB;                          // window blocks of 16 rows
-    int BC;                          // chip columns per chunk (even)
-    int XC;                          // window columns staged per chunk (>= BC + 63)
+    int BC;                          // chip columns per chunk
+    int OB;                          // chip columns per window staging (multiple of BC)
+    int LW;                          // window columns staged (OB + 63)
     int PC;                          // staged chip column length (elements, even)
-    int NRS;                         // box-sum and surface row stride
+    int NRS;                         // surface, box-sum and denominator row stride
     int AC;                          // columns per accumulator (multiple of 16)
-    int VR;                          // rows of column sums per box-sum chunk
-    unsigned off_W, off_E, off_P, off_S1, off_S2, off_red;
+    int RS;                          // row stride of a box-sum stripe's window columns (odd)
+    int VS;                          // row stride of a stripe's column sums (nr + 1)
+    int XS;                          // window columns per box-sum stripe
+    unsigned off_S2, off_raw, off_V; // box-sum phase (S1 at 0)
+    unsigned off_den, off_E, off_P, off_red;
+    unsigned Eb, Pb;                 // bytes per chip-operand / staged-chip buffer
     uint32_t tmem_cols;
     DevOutputs out;
     int* sub_count;
@@ -2367,7 +2381,8 @@ struct BfArgs {
 
 // The three BF16 limbs of v, as raw 16-bit patterns: l[0] = bf16(v), l[1] = bf16(v - l[0]),
 // l[2] = bf16(v - l[0] - l[1]). Each difference is exact in FP32 (its operands are within a
-// factor of two of each other), so v - (l[0] + l[1] + l[2]) is below 2^-24 |v|.
+// factor of two of each other), and the last remainder has at most 8 significant bits, so
+// v = l[0] + l[1] + l[2] for every normal v.
 __device__ __forceinline__ void bf16_split3(float v, uint32_t (&l)[kBfLimbs]) {
     float r = v;
 #pragma unroll
@@ -2382,24 +2397,28 @@ template <typename T>
 __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
     typedef Traits<T> Tr;
     extern __shared__ __align__(1024) unsigned char smem_bf[];
-    __shared__ uint64_t s_mbar;
+    __shared__ uint64_t s_mbar[2];
     __shared__ uint32_t s_taddr;
     __shared__ int s_slot;
     const int tid = threadIdx.x, bd = blockDim.x;
     const int lane = tid & 31, warp = tid >> 5;
     const T* ref = static_cast<const T*>(A.ref);
     const T* sec = static_cast<const T*>(A.sec);
-    // Operand buffers, three limbs each: window [limb][q][h][x], chip operand [limb][b][h][e],
-    // staged chip columns [limb][b][PC] (raw BF16 bits). Box sums S1, S2 [j][NRS] (FP64).
-    unsigned char* s_W = smem_bf + A.off_W;
-    unsigned char* s_E = smem_bf + A.off_E;
-    uint16_t* s_P = reinterpret_cast<uint16_t*>(smem_bf + A.off_P);
-    double* s_S1 = reinterpret_cast<double*>(smem_bf + A.off_S1);
+    // Window limbs [limb][q][h][x] (16 bytes each) from offset 0, where the box-sum phase keeps
+    // S1 and S2 [j][NRS] (FP64) and the epilogue the surface; the stripe buffers of the box sums
+    // reach into the region of the denominators [j][NRS] (FP64), the two chip-operand buffers
+    // [limb][b][h][e] and the two staged-chip buffers [limb][b][PC] (raw BF16 bits).
+    unsigned char* s_W = smem_bf;
+    double* s_S1 = reinterpret_cast<double*>(smem_bf);
     double* s_S2 = reinterpret_cast<double*>(smem_bf + A.off_S2);
+    float* s_raw = reinterpret_cast<float*>(smem_bf + A.off_raw);
+    double* s_V = reinterpret_cast<double*>(smem_bf + A.off_V);
+    double* s_den = reinterpret_cast<double*>(smem_bf + A.off_den);
+    unsigned char* s_E = smem_bf + A.off_E;
+    unsigned char* s_Pb = smem_bf + A.off_P;
     double* s_red = reinterpret_cast<double*>(smem_bf + A.off_red);
-    float* s_surf = reinterpret_cast<float*>(smem_bf + A.off_W);  // after the products
-    double* s_V = reinterpret_cast<double*>(smem_bf + A.off_W);   // box-sum column sums
-    const size_t wlimb = static_cast<size_t>(A.QB) * 2 * A.XC * 16;
+    float* s_surf = reinterpret_cast<float*>(smem_bf);
+    const size_t wlimb = static_cast<size_t>((A.CHM + A.NRM - 1 + 15) / 16) * 2 * A.LW * 16;
     const size_t elimb = static_cast<size_t>(A.BC) * 2 * A.NB * 16;
     const int plimb = A.BC * A.PC;
     const int64_t NR = A.nrows + 2 * A.pady, NC = A.ncols + 2 * A.padx;
@@ -2411,17 +2430,46 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
         tc::tmem_relinquish();
     }
     if (tid == 0) {
-        tc::mbar_init(&s_mbar, kBfAcc);  // one commit per issuing thread
+        tc::mbar_init(&s_mbar[0], 1);  // one commit per chunk
+        tc::mbar_init(&s_mbar[1], 1);
         tc::fence_mbar_init();
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t taddr = s_taddr;
-    uint32_t phase = 0;
+    uint32_t ph[2] = {0u, 0u};
+    bool pend[2] = {false, false};
     bool failed = false;
 
-    for (int64_t k = blockIdx.x; k < A.pts.n; k += gridDim.x) {
+    // Accumulator values of a thread after a chunk: value v is surface row
+    // i = 32 half + 8 (v / 4) + 2 (lane % 4) + v % 2, column j = 16 quarter + lane / 4 (+ 8 when
+    // v % 4 >= 2) -- the 16x256b read pattern of its lane quarter's half.
+    const int quarter = warp & 3, half = warp >> 2;
+    const uint32_t qbase = taddr + (static_cast<uint32_t>(32 * quarter) << 16) +
+                           static_cast<uint32_t>(32 * half);
+    auto clear_set = [&](int s) {
+        if (warp < 4) {
+            uint32_t z[16];
+#pragma unroll
+            for (int t = 0; t < 16; ++t) z[t] = 0u;
+            const uint32_t lq = taddr + (static_cast<uint32_t>(32 * warp) << 16);
+            for (int c = 2 * s * A.AC; c < 2 * (s + 1) * A.AC; c += 16)
+                tc::tmem_st16(lq + static_cast<uint32_t>(c), z);
+            tc::tmem_wait_st();
+        }
+    };
+    // Bounded wait for set s's products; on success the set is no longer pending.
+    auto wait_set = [&](int s) -> bool {
+        const bool ok = tc::mbar_wait(&s_mbar[s], ph[s], kTcWaitPolls);
+        if (ok) {
+            ph[s] ^= 1u;
+            pend[s] = false;
+        }
+        return ok;
+    };
+
+    for (int64_t k = blockIdx.x; k < A.pts.n && !failed; k += gridDim.x) {
         tc::fence_before_sync();
         __syncthreads();  // the previous point's buffers and accumulators are no longer read
         tc::fence_after_sync();
@@ -2446,32 +2494,59 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
         if (ch > A.CHM || cw > A.CWM || nr > A.NRM || nc > A.NCM || nr > 64 || nc > 64) continue;
         const int64_t chip_r = cr0 - 1 - A.pady, chip_c = cc0 - 1 - A.padx;
         const int64_t win_r = wr0 - 1 - A.pady, win_c = wc0 - 1 - A.padx;
+        const int nn_i = ch * cw;
 
         // _any_valid over the chip (src/track.jl:416-421).
         int any = 0;
-        for (int e = tid; e < ch * cw; e += bd) {
-            const int64_t r = chip_r + e % ch, c = chip_c + e / ch;
-            if (r >= 0 && r < A.nrows && c >= 0 && c < A.ncols && A.valid[r + c * A.nrows]) any = 1;
+        for (int e0 = tid; e0 < nn_i && !any; e0 += kBfBatch * bd) {
+            uint8_t v[kBfBatch];
+#pragma unroll
+            for (int u = 0; u < kBfBatch; ++u) {
+                const int e = e0 + u * bd;
+                const int64_t r = chip_r + e % ch, c = chip_c + e / ch;
+                v[u] = (e < nn_i && r >= 0 && r < A.nrows && c >= 0 && c < A.ncols)
+                           ? A.valid[r + c * A.nrows] : static_cast<uint8_t>(0);
+            }
+#pragma unroll
+            for (int u = 0; u < kBfBatch; ++u) any |= v[u] ? 1 : 0;
         }
         if (!__syncthreads_or(any)) continue;
         if (tid == 0) A.out.searched[k] = 1;
 
-        // prepare_chip! as the CUDA-core kernel: FP64 mean, FP64 sum of squares of the
-        // deviations, FP64 sum of the Float32-rounded deviations.
+        // prepare_chip! as the CUDA-core kernel (the same per-thread order): FP64 mean, FP64 sum
+        // of squares of the deviations, FP64 sum of the Float32-rounded deviations.
         double st[1] = {0.0};
-        for (int e = tid; e < ch * cw; e += bd)
-            st[0] = __dadd_rn(st[0], pixel(sec, A.nrows, A.ncols, chip_r + e % ch, chip_c + e / ch));
+        for (int e0 = tid; e0 < nn_i; e0 += kBfBatch * bd) {
+            double v[kBfBatch];
+#pragma unroll
+            for (int u = 0; u < kBfBatch; ++u) {
+                const int e = e0 + u * bd;
+                v[u] = e < nn_i ? pixel(sec, A.nrows, A.ncols, chip_r + e % ch, chip_c + e / ch) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kBfBatch; ++u)
+                if (e0 + u * bd < nn_i) st[0] = __dadd_rn(st[0], v[u]);
+        }
         block_sum_f64<1>(st, s_red);
-        const double nn = static_cast<double>(ch * cw);
+        const double nn = static_cast<double>(nn_i);
         const double mean = __ddiv_rn(st[0], nn);
         const int chp = (ch + kUA - 1) & ~(kUA - 1);
         double acc2[2] = {0.0, 0.0};
-        for (int e = tid; e < chp * cw; e += bd) {
-            const int a = e % chp, b = e / chp;
-            if (a < ch) {
-                const double d = __dsub_rn(pixel(sec, A.nrows, A.ncols, chip_r + a, chip_c + b), mean);
-                acc2[0] = __dadd_rn(acc2[0], __dmul_rn(d, d));
-                acc2[1] = __dadd_rn(acc2[1], static_cast<double>(__double2float_rn(d)));
+        for (int e0 = tid; e0 < chp * cw; e0 += kBfBatch * bd) {
+            double v[kBfBatch];
+#pragma unroll
+            for (int u = 0; u < kBfBatch; ++u) {
+                const int e = e0 + u * bd, a = e % chp, b = e / chp;
+                v[u] = (e < chp * cw && a < ch) ? pixel(sec, A.nrows, A.ncols, chip_r + a, chip_c + b) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kBfBatch; ++u) {
+                const int e = e0 + u * bd;
+                if (e < chp * cw && e % chp < ch) {
+                    const double d = __dsub_rn(v[u], mean);
+                    acc2[0] = __dadd_rn(acc2[0], __dmul_rn(d, d));
+                    acc2[1] = __dadd_rn(acc2[1], static_cast<double>(__double2float_rn(d)));
+                }
             }
         }
         block_sum_f64<2>(acc2, s_red);
@@ -2480,224 +2555,288 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
             continue;  // degenerate chip: searched, no measurement (src/track.jl:286)
         const double cnorm = __dsqrt_rn(sq);
         const double cshift = Tr::integer ? rint(mean) : static_cast<double>(__double2float_rn(mean));
+        const float csf = static_cast<float>(cshift);
         if (tid == 0 && !(A.up == 1 || nr < 5 || nc < 5)) s_slot = atomicAdd(A.sub_count, 1);
 
-        // Box sums in FP64 from the image values: column sums V of ch rows (a thread per window
-        // column, sliding down), in chunks of VR surface rows, then row sums of cw columns.
-        const int XW = cw + nc - 1;
-        double h1 = 0.0, h2 = 0.0;
-        if (tid < XW) {
-            for (int a = 0; a < ch; ++a) {
-                const double w = pixel(ref, A.nrows, A.ncols, win_r + a, win_c + tid);
-                h1 = __dadd_rn(h1, w);
-                h2 = __dadd_rn(h2, __dmul_rn(w, w));
+        // Box sums in FP64, a stripe of window columns at a time: the stripe's image values
+        // (exact in FP32 for every element type), its column sums V(i, x) of ch rows, then the
+        // running sum Q along each surface row i (a thread per row and sum): the box sum at column
+        // j is Q after window column j + cw - 1 less Q before column j.
+        const int RW = ch + nr - 1, XW = cw + nc - 1;
+        double qrun = 0.0;
+        for (int x0 = 0; x0 < XW; x0 += A.XS) {
+            const int xn = min(A.XS, XW - x0);
+            for (int e0 = tid; e0 < xn * RW; e0 += kBfBatch * bd) {
+                double v[kBfBatch];
+#pragma unroll
+                for (int u = 0; u < kBfBatch; ++u) {
+                    const int e = e0 + u * bd;
+                    v[u] = e < xn * RW ? pixel(ref, A.nrows, A.ncols, win_r + e % RW, win_c + x0 + e / RW) : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < kBfBatch; ++u) {
+                    const int e = e0 + u * bd;
+                    if (e < xn * RW) s_raw[(e / RW) * A.RS + e % RW] = static_cast<float>(v[u]);
+                }
             }
-        }
-        for (int i0 = 0; i0 < nr; i0 += A.VR) {
-            const int i1 = min(nr, i0 + A.VR);
-            if (tid < XW) {
-                for (int i = i0; i < i1; ++i) {
-                    s_V[2 * ((i - i0) * XW + tid)] = h1;
-                    s_V[2 * ((i - i0) * XW + tid) + 1] = h2;
-                    if (i + 1 < nr) {
-                        const double wo = pixel(ref, A.nrows, A.ncols, win_r + i, win_c + tid);
-                        const double wn = pixel(ref, A.nrows, A.ncols, win_r + i + ch, win_c + tid);
-                        h1 = __dadd_rn(__dsub_rn(h1, wo), wn);
-                        h2 = __dadd_rn(__dsub_rn(h2, __dmul_rn(wo, wo)), __dmul_rn(wn, wn));
+            __syncthreads();
+            {
+                const int segs = max(1, min(nr, bd / xn));
+                const int len = (nr + segs - 1) / segs;
+                for (int t = tid; t < xn * segs; t += bd) {
+                    const int x = t % xn, i0 = (t / xn) * len, i1 = min(nr, i0 + len);
+                    if (i0 >= i1) continue;
+                    const float* col = s_raw + x * A.RS;
+                    double h1 = 0.0, h2 = 0.0;
+                    for (int a = i0; a < i0 + ch; ++a) {
+                        const double w = static_cast<double>(col[a]);
+                        h1 = __dadd_rn(h1, w);
+                        h2 = __dadd_rn(h2, __dmul_rn(w, w));
+                    }
+                    for (int i = i0; i < i1; ++i) {
+                        s_V[2 * (x * A.VS + i)] = h1;
+                        s_V[2 * (x * A.VS + i) + 1] = h2;
+                        if (i + 1 < i1) {
+                            const double wo = static_cast<double>(col[i]);
+                            const double wn = static_cast<double>(col[i + ch]);
+                            h1 = __dadd_rn(__dsub_rn(h1, wo), wn);
+                            h2 = __dadd_rn(__dsub_rn(h2, __dmul_rn(wo, wo)), __dmul_rn(wn, wn));
+                        }
                     }
                 }
             }
             __syncthreads();
-            // Row sums: a task is a surface row and 16 columns j, sliding along V's row.
-            const int jseg = (nc + 15) >> 4;
-            for (int task = tid; task < (i1 - i0) * jseg; task += bd) {
-                const int il = task % (i1 - i0), sg = task / (i1 - i0);
-                const int j0 = 16 * sg, j1 = min(nc, j0 + 16);
-                const double* vr = s_V + 2 * il * XW;
-                double g1 = 0.0, g2 = 0.0;
-                for (int b = 0; b < cw; ++b) {
-                    g1 = __dadd_rn(g1, vr[2 * (j0 + b)]);
-                    g2 = __dadd_rn(g2, vr[2 * (j0 + b) + 1]);
-                }
-                for (int j = j0; j < j1; ++j) {
-                    s_S1[j * A.NRS + i0 + il] = g1;
-                    s_S2[j * A.NRS + i0 + il] = g2;
-                    if (j + 1 < j1) {
-                        g1 = __dadd_rn(__dsub_rn(g1, vr[2 * j]), vr[2 * (j + cw)]);
-                        g2 = __dadd_rn(__dsub_rn(g2, vr[2 * j + 1]), vr[2 * (j + cw) + 1]);
-                    }
+            if (tid < 2 * nr) {
+                const int i = tid >> 1, comp = tid & 1;
+                double* S = comp ? s_S2 : s_S1;
+                for (int x = 0; x < xn; ++x) {
+                    const int xg = x0 + x;
+                    if (xg < nc) S[xg * A.NRS + i] = qrun;
+                    qrun = __dadd_rn(qrun, s_V[2 * (x * A.VS + i) + comp]);
+                    const int j = xg - cw + 1;
+                    if (j >= 0 && j < nc) S[j * A.NRS + i] = __dsub_rn(qrun, S[j * A.NRS + i]);
                 }
             }
             __syncthreads();
         }
+        // FP64 denominators (src/correlate.jl:591-600, 624-628).
+        for (int e = tid; e < nr * nc; e += bd) {
+            const int i = e % nr, j = e / nr;
+            const double s1 = s_S1[j * A.NRS + i], s2 = s_S2[j * A.NRS + i];
+            double den;
+            if (A.measure == AR_NCC) {
+                den = __dmul_rn(cnorm, __dsqrt_rn(s2 > 0.0 ? s2 : 0.0));
+            } else {
+                double wvar = __dsub_rn(s2, __ddiv_rn(__dmul_rn(s1, s1), nn));
+                if (!(wvar > 0.0)) wvar = 0.0;
+                den = __dmul_rn(cnorm, __dsqrt_rn(wvar));
+            }
+            s_den[j * A.NRS + i] = den;
+        }
+        clear_set(0);
+        clear_set(1);
+        __syncthreads();  // S1 and S2 read before the window limbs replace them
 
-        // The tensor core's FP32 accumulation does not round to nearest, so a long chain of
-        // products into one accumulator drifts (by ~1e-4 of the numerator over the ~1,000
-        // products per accumulator of a 192-px chip). Each chunk's products therefore go into
-        // cleared accumulators, and after the chunk every thread adds its values of the six
-        // accumulators into FP64 sums it keeps in registers: value v of a thread is surface
-        // row i = 32 half + 8 (v / 4) + 2 (lane % 4) + v % 2, column j = 16 quarter + lane / 4
-        // (+ 8 when v % 4 >= 2) -- the 16x256b read pattern of its lane quarter's half.
-        const int quarter = warp & 3, half = warp >> 2;
-        const uint32_t qbase = taddr + (static_cast<uint32_t>(32 * quarter) << 16) +
-                               static_cast<uint32_t>(32 * half);
         double accd[16];
 #pragma unroll
         for (int v = 0; v < 16; ++v) accd[v] = 0.0;
-        auto clear_acc = [&]() {
-            if (warp < 4) {
-                uint32_t z[16];
-#pragma unroll
-                for (int t = 0; t < 16; ++t) z[t] = 0u;
-                const uint32_t lq = taddr + (static_cast<uint32_t>(32 * warp) << 16);
-                for (int c = 0; c < kBfAcc * A.AC; c += 16) tc::tmem_st16(lq + static_cast<uint32_t>(c), z);
-                tc::tmem_wait_st();
-            }
-        };
-        auto flush_acc = [&]() {
+        auto flush_set = [&](int s) {
             if (32 * half < nr) {
-                for (int s = 0; s < kBfAcc; ++s) {
-                    uint32_t r[16];
-                    tc::tmem_ld16dp(qbase + static_cast<uint32_t>(s * A.AC), r);
-                    tc::tmem_wait_ld();
+                uint32_t hi[16], lo[16];
+                tc::tmem_ld16dp(qbase + static_cast<uint32_t>(2 * s * A.AC), hi);
+                tc::tmem_ld16dp(qbase + static_cast<uint32_t>((2 * s + 1) * A.AC), lo);
+                tc::tmem_wait_ld();
 #pragma unroll
-                    for (int v = 0; v < 16; ++v)
-                        accd[v] = __dadd_rn(accd[v], static_cast<double>(__uint_as_float(r[v])));
+                for (int v = 0; v < 16; ++v)
+                    accd[v] = __dadd_rn(__dadd_rn(accd[v], static_cast<double>(__uint_as_float(hi[v]))),
+                                        static_cast<double>(__uint_as_float(lo[v])));
+            }
+        };
+        // A chunk's chip columns C'[a, b0 + bl] as BF16 limbs, zero-padded: the loads first
+        // (into registers), the conversion after other work.
+        auto p_load = [&](int b0, int bcn, double (&pr)[kBfPre]) {
+#pragma unroll
+            for (int u = 0; u < kBfPre; ++u) {
+                const int e = tid + u * bd;
+                const int bl = e / A.PC, a = e - bl * A.PC - kBfPadL;
+                pr[u] = (e < plimb && bl < bcn && a >= 0 && a < ch)
+                            ? pixel(sec, A.nrows, A.ncols, chip_r + a, chip_c + b0 + bl) : 0.0;
+            }
+        };
+        auto p_store = [&](int buf, int bcn, const double (&pr)[kBfPre]) {
+            uint16_t* P = reinterpret_cast<uint16_t*>(s_Pb + buf * A.Pb);
+#pragma unroll
+            for (int u = 0; u < kBfPre; ++u) {
+                const int e = tid + u * bd;
+                if (e < plimb) {
+                    const int bl = e / A.PC, a = e - bl * A.PC - kBfPadL;
+                    uint32_t l[kBfLimbs] = {0u, 0u, 0u};
+                    if (bl < bcn && a >= 0 && a < ch) bf16_split3(__double2float_rn(__dsub_rn(pr[u], mean)), l);
+#pragma unroll
+                    for (int limb = 0; limb < kBfLimbs; ++limb) P[limb * plimb + e] = static_cast<uint16_t>(l[limb]);
                 }
             }
         };
-        clear_acc();
 
-        const int QB = (ch + nr - 1 + 15) / 16;
-        const int nchunk = (cw + A.BC - 1) / A.BC;
+        const int QBp = (ch + nr - 1 + 15) / 16;
+        const int gp = 2 * QBp;  // 8-row groups per window column
         bool ok = true;
-        for (int cc = 0; cc < nchunk && ok; ++cc) {
-            const int b0 = cc * A.BC, bcn = min(A.BC, cw - b0);
-            if (cc > 0) {
-                // The previous chunk's products must be done before its operands are replaced
-                // and its accumulators read out and cleared.
-                ok = tc::mbar_wait(&s_mbar, phase, kTcWaitPolls);
-                phase ^= 1u;
-                if (__syncthreads_or(!ok)) break;
-                tc::fence_after_sync();
-                flush_acc();
-                tc::fence_before_sync();
-                __syncthreads();  // every accumulator read before any is cleared
-                tc::fence_after_sync();
-                clear_acc();
-            }
-            // The chunk's chip columns C'[a, b0 + bl] as BF16 limbs, zero-padded.
-            for (int e = tid; e < A.BC * A.PC; e += bd) {
-                const int bl = e / A.PC, t = e - bl * A.PC;
-                const int a = t - kBfPadL;
-                uint32_t l[kBfLimbs] = {0u, 0u, 0u};
-                if (bl < bcn && a >= 0 && a < ch) {
-                    const double d = __dsub_rn(pixel(sec, A.nrows, A.ncols, chip_r + a, chip_c + b0 + bl), mean);
-                    bf16_split3(__double2float_rn(d), l);
+        for (int ob0 = 0; ob0 < cw && ok; ob0 += A.OB) {
+            const int obn = min(A.OB, cw - ob0);
+            const int xneed = obn + nc - 1;
+            // Window limbs of columns ob0 .. ob0 + LW - 1 (zero past the columns and rows the
+            // valid surface values read): item (x, q, h) = 8 consecutive rows of column x,
+            // consecutive threads on consecutive row groups of one column; two items' loads at once.
+            const int items = A.LW * gp;
+            for (int it0 = tid; it0 < items; it0 += 2 * bd) {
+                float wv[2][8];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int it = it0 + u * bd;
+                    const int x = it / gp, g = it - x * gp;
+                    const int r0 = 8 * g;  // 16 q + 8 h
+#pragma unroll
+                    for (int t = 0; t < 8; ++t)
+                        wv[u][t] = (it < items && x < xneed && r0 + t < RW)
+                                       ? static_cast<float>(pixel(ref, A.nrows, A.ncols, win_r + r0 + t, win_c + ob0 + x))
+                                       : 0.0f;
                 }
 #pragma unroll
-                for (int limb = 0; limb < kBfLimbs; ++limb) s_P[limb * plimb + e] = static_cast<uint16_t>(l[limb]);
-            }
-            // Window blocks: item (x, q, h) = 8 consecutive rows of window column b0 + x, both
-            // limbs; consecutive threads take consecutive row groups of one column.
-            const int gpc = 2 * QB;  // row groups per column
-            for (int it = tid; it < A.XC * gpc; it += bd) {
-                const int x = it / gpc, g = it - x * gpc;
-                const int q = g >> 1, h = g & 1;
-                uint32_t lw[kBfLimbs][4] = {};
-                if (x < bcn + nc - 1) {
-                    const int64_t c = win_c + b0 + x;
-                    const int64_t r0 = win_r + 16 * q + 8 * h;
+                for (int u = 0; u < 2; ++u) {
+                    const int it = it0 + u * bd;
+                    if (it < items) {
+                        const int x = it / gp, g = it - x * gp;
+                        const int r0 = 8 * g;
+                        uint32_t lw[kBfLimbs][4] = {};
 #pragma unroll
-                    for (int t = 0; t < 8; ++t) {
-                        const int a = 16 * q + 8 * h + t;  // window row
-                        uint32_t l[kBfLimbs] = {0u, 0u, 0u};
-                        if (a < ch + nr - 1) {
-                            const double w = pixel(ref, A.nrows, A.ncols, r0 + t, c);
-                            bf16_split3(__double2float_rn(__dsub_rn(w, cshift)), l);
+                        for (int t = 0; t < 8; ++t) {
+                            uint32_t l[kBfLimbs] = {0u, 0u, 0u};
+                            if (x < xneed && r0 + t < RW) bf16_split3(__fsub_rn(wv[u][t], csf), l);
+#pragma unroll
+                            for (int limb = 0; limb < kBfLimbs; ++limb) lw[limb][t >> 1] |= l[limb] << (16 * (t & 1));
                         }
+                        const size_t o = (static_cast<size_t>(g) * A.LW + x) * 16;
 #pragma unroll
                         for (int limb = 0; limb < kBfLimbs; ++limb)
-                            lw[limb][t >> 1] |= l[limb] << (16 * (t & 1));
+                            *reinterpret_cast<uint4*>(s_W + limb * wlimb + o) =
+                                make_uint4(lw[limb][0], lw[limb][1], lw[limb][2], lw[limb][3]);
                     }
                 }
-                const size_t o = (static_cast<size_t>(q * 2 + h) * A.XC + x) * 16;
-#pragma unroll
-                for (int limb = 0; limb < kBfLimbs; ++limb)
-                    *reinterpret_cast<uint4*>(s_W + limb * wlimb + o) =
-                        make_uint4(lw[limb][0], lw[limb][1], lw[limb][2], lw[limb][3]);
             }
-            __syncthreads();  // s_P complete
-            // Chip operand rows: E_b[h][e] = 8 elements of the staged column from element
-            // kBfPadL + 8 h - e + NB - 16 (C'[r - u, b] with u = e - NB + 16, r = 8 h + t).
-            for (int it = tid; it < A.BC * 2 * A.NB; it += bd) {
-                const int bl = it / (2 * A.NB), rem = it - bl * 2 * A.NB;
-                const int h = rem / A.NB, e = rem - h * A.NB;
-                const int src = kBfPadL + 8 * h - e + A.NB - 16;  // element index, >= 1
-                const size_t o = (static_cast<size_t>(bl * 2 + h) * A.NB + e) * 16;
-#pragma unroll
-                for (int limb = 0; limb < kBfLimbs; ++limb) {
-                    const uint16_t* col = s_P + limb * plimb + bl * A.PC;
-                    const uint32_t* w = reinterpret_cast<const uint32_t*>(col + (src & ~1));
-                    const uint32_t sh = (src & 1) ? 16u : 0u;
-                    uint4 v;
-                    v.x = __funnelshift_r(w[0], w[1], sh);
-                    v.y = __funnelshift_r(w[1], w[2], sh);
-                    v.z = __funnelshift_r(w[2], w[3], sh);
-                    v.w = __funnelshift_r(w[3], w[4], sh);
-                    *reinterpret_cast<uint4*>(s_E + limb * elimb + o) = v;
-                }
+            {
+                double pr[kBfPre];
+                p_load(ob0, min(A.BC, obn), pr);
+                p_store(0, min(A.BC, obn), pr);
             }
-            tc::fence_proxy_async_smem();
-            tc::fence_before_sync();
-            __syncthreads();  // operands complete
-            // Six threads (lane 0 of warps 2..7) issue the chunk's products, thread s the limb
-            // pair (chip limb, window limb) = (0,0), (0,1), (1,0), (1,1), (2,0), (0,2) into
-            // accumulator s; integer windows have no third limb.
-            if (lane == 0 && warp >= 2) {
-                const int s = warp - 2;
-                const int cl = s == 2 || s == 3 ? 1 : s == 4 ? 2 : 0;
-                const int wl = s == 1 || s == 3 ? 1 : s == 5 ? 2 : 0;
-                const int bstart = (Tr::integer && s == 5) ? bcn : 0;
-                tc::fence_after_sync();
-                const uint32_t wb = tc::smem_u32(s_W) + static_cast<uint32_t>(wl * wlimb);
-                const uint32_t eb = tc::smem_u32(s_E) + static_cast<uint32_t>(cl * elimb);
-                const uint64_t da0 = tc::smem_desc(wb, static_cast<uint32_t>(A.XC * 16), 128);
-                const uint64_t db0 = tc::smem_desc(eb, static_cast<uint32_t>(A.NB * 16), 128);
-                const uint32_t a_hi = static_cast<uint32_t>(da0 >> 32);
-                const uint32_t b_hi = static_cast<uint32_t>(db0 >> 32);
-                const uint32_t dacc = taddr + static_cast<uint32_t>(s * A.AC);
-                for (int q = 0; q < QB; ++q) {
-                    int elo, n;
-                    if (!block_rows(q, A.NB, nr, &elo, &n)) continue;
-                    const uint32_t idesc = tc::idesc_bf16_f32(64, n);
-                    const uint32_t dcol = static_cast<uint32_t>(16 * q + elo - (A.NB - 16));
-                    for (int bl = bstart; bl < bcn; ++bl) {
-                        // A: block q, first half, window column x = bl (row j at x = bl + j).
-                        const uint32_t a_lo = static_cast<uint32_t>(da0) +
-                                              static_cast<uint32_t>((q * 2) * A.XC + bl);
-                        const uint32_t b_lo = static_cast<uint32_t>(db0) +
-                                              static_cast<uint32_t>((bl * 2) * A.NB + elo);
-                        tc::mma_bf16_halves(dacc + dcol, a_lo, a_hi, b_lo, b_hi, idesc, 1u);
+            __syncthreads();  // limbs and the first chunk's chip columns complete
+
+            const int nch = (obn + A.BC - 1) / A.BC;
+            for (int c = 0; c < nch; ++c) {
+                const int s = c & 1;
+                const int b0 = ob0 + c * A.BC, bcn = min(A.BC, ob0 + obn - b0);
+                // Chip operand rows: E_b[h][e] = 8 elements of the staged column from element
+                // kBfPadL + 8 h - e + NB - 16 (C'[r - u, b] with u = e - NB + 16, r = 8 h + t).
+                {
+                    const uint16_t* P = reinterpret_cast<const uint16_t*>(s_Pb + s * A.Pb);
+                    unsigned char* E = s_E + s * A.Eb;
+                    for (int it = tid; it < A.BC * 2 * A.NB; it += bd) {
+                        const int bl = it / (2 * A.NB), rem = it - bl * 2 * A.NB;
+                        const int h = rem / A.NB, e = rem - h * A.NB;
+                        const int src = kBfPadL + 8 * h - e + A.NB - 16;  // element index, >= 1
+                        const size_t o = (static_cast<size_t>(bl * 2 + h) * A.NB + e) * 16;
+#pragma unroll
+                        for (int limb = 0; limb < kBfLimbs; ++limb) {
+                            const uint16_t* col = P + limb * plimb + bl * A.PC;
+                            const uint32_t* w = reinterpret_cast<const uint32_t*>(col + (src & ~1));
+                            const uint32_t sh = (src & 1) ? 16u : 0u;
+                            uint4 v;
+                            v.x = __funnelshift_r(w[0], w[1], sh);
+                            v.y = __funnelshift_r(w[1], w[2], sh);
+                            v.z = __funnelshift_r(w[2], w[3], sh);
+                            v.w = __funnelshift_r(w[3], w[4], sh);
+                            *reinterpret_cast<uint4*>(E + limb * elimb + o) = v;
+                        }
                     }
                 }
-                tc::mma_commit(&s_mbar);
+                tc::fence_proxy_async_smem();
+                tc::fence_before_sync();
+                __syncthreads();  // operands complete; accumulator set s clear
+                // One thread issues the chunk's products: limb pairs (chip, window) (0,0) into
+                // the set's first accumulator, (0,1), (1,0), (1,1), (2,0), (0,2) into its second
+                // (integer windows have no third limb).
+                if (tid == 0) {
+                    tc::fence_after_sync();
+                    const uint32_t wb = tc::smem_u32(s_W);
+                    const uint32_t eb = tc::smem_u32(s_E) + static_cast<uint32_t>(s * A.Eb);
+#pragma unroll 1
+                    for (int p = 0; p < 6; ++p) {
+                        const int cl = p == 2 || p == 3 ? 1 : p == 4 ? 2 : 0;
+                        const int wl = p == 1 || p == 3 ? 1 : p == 5 ? 2 : 0;
+                        if (Tr::integer && wl == 2) continue;
+                        const uint64_t da0 = tc::smem_desc(wb + static_cast<uint32_t>(wl * wlimb),
+                                                           static_cast<uint32_t>(A.LW * 16), 128);
+                        const uint64_t db0 = tc::smem_desc(eb + static_cast<uint32_t>(cl * elimb),
+                                                           static_cast<uint32_t>(A.NB * 16), 128);
+                        const uint32_t a_hi = static_cast<uint32_t>(da0 >> 32);
+                        const uint32_t b_hi = static_cast<uint32_t>(db0 >> 32);
+                        const uint32_t dacc = taddr + static_cast<uint32_t>((2 * s + (p ? 1 : 0)) * A.AC);
+                        for (int q = 0; q < QBp; ++q) {
+                            int elo, n;
+                            if (!block_rows(q, A.NB, nr, &elo, &n)) continue;
+                            const uint32_t idesc = tc::idesc_bf16_f32(64, n);
+                            const uint32_t dcol = static_cast<uint32_t>(16 * q + elo - (A.NB - 16));
+                            for (int bl = 0; bl < bcn; ++bl) {
+                                // A: block q, first half, window column x = b0 - ob0 + bl.
+                                const uint32_t a_lo = static_cast<uint32_t>(da0) +
+                                                      static_cast<uint32_t>((q * 2) * A.LW + (b0 - ob0) + bl);
+                                const uint32_t b_lo = static_cast<uint32_t>(db0) +
+                                                      static_cast<uint32_t>((bl * 2) * A.NB + elo);
+                                tc::mma_bf16_halves(dacc + dcol, a_lo, a_hi, b_lo, b_hi, idesc, 1u);
+                            }
+                        }
+                    }
+                    tc::mma_commit(&s_mbar[s]);
+                }
+                pend[s] = true;
+                // The next chunk's chip columns: loads now, conversion after the flush.
+                const bool more = c + 1 < nch;
+                const int bnext = min(A.BC, ob0 + obn - (b0 + A.BC));
+                double pr[kBfPre];
+                if (more) p_load(b0 + A.BC, bnext, pr);
+                if (c >= 1) {
+                    // The previous chunk's products: done (its chip operand buffer is free), its
+                    // accumulators added into the FP64 sums and cleared.
+                    ok = wait_set(s ^ 1);
+                    if (__syncthreads_or(!ok)) { ok = false; break; }
+                    tc::fence_after_sync();
+                    flush_set(s ^ 1);
+                    clear_set(s ^ 1);
+                }
+                if (more) p_store(s ^ 1, bnext, pr);
+                tc::fence_before_sync();
+                __syncthreads();
+            }
+            if (ok) {
+                const int sl = (nch - 1) & 1;
+                ok = wait_set(sl);
+                if (__syncthreads_or(!ok)) {
+                    ok = false;
+                } else {
+                    tc::fence_after_sync();
+                    flush_set(sl);
+                    clear_set(sl);
+                    tc::fence_before_sync();
+                    __syncthreads();  // the window limbs are replaced next
+                }
             }
         }
-        if (ok) {
-            ok = tc::mbar_wait(&s_mbar, phase, kTcWaitPolls);
-            phase ^= 1u;
-        }
-        if (__syncthreads_or(!ok)) {
+        if (!ok) {
             if (tid == 0) atomicExch(A.status, 1);
             failed = true;
             break;
         }
-        tc::fence_after_sync();
-        flush_acc();
 
-        // Epilogue: every value is normalised in FP64 (src/correlate.jl:591-600, 624-628) into
-        // the surface in shared memory.
+        // Epilogue: every value normalised in FP64 into the surface in shared memory.
         {
             const int ib0 = 32 * half + 2 * (lane & 3);
             const int jb0 = 16 * quarter + (lane >> 2);
@@ -2706,16 +2845,8 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                 for (int v = 0; v < 16; ++v) {
                     const int i = ib0 + 8 * (v >> 2) + (v & 1), j = jb0 + ((v & 2) ? 8 : 0);
                     if (i < nr && j < nc) {
-                        const double s1 = s_S1[j * A.NRS + i], s2 = s_S2[j * A.NRS + i];
                         const double num = __dadd_rn(accd[v], __dmul_rn(cshift, sumd));
-                        double den;
-                        if (A.measure == AR_NCC) {
-                            den = __dmul_rn(cnorm, __dsqrt_rn(s2 > 0.0 ? s2 : 0.0));
-                        } else {
-                            double wvar = __dsub_rn(s2, __ddiv_rn(__dmul_rn(s1, s1), nn));
-                            if (!(wvar > 0.0)) wvar = 0.0;
-                            den = __dmul_rn(cnorm, __dsqrt_rn(wvar));
-                        }
+                        const double den = s_den[j * A.NRS + i];
                         s_surf[j * A.NRS + i] = den > 0.0 ? __double2float_rn(__ddiv_rn(num, den)) : 0.0f;
                     }
                 }
@@ -2766,7 +2897,9 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
             }
         }
     }
-    if (failed) tc::mbar_wait(&s_mbar, phase ^ 1u, kTcWaitPolls);
+    // Products still in flight after a failed wait finish before their columns are freed.
+    for (int s = 0; s < 2; ++s)
+        if (pend[s]) tc::mbar_wait(&s_mbar[s], ph[s], kTcWaitPolls);
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) tc::tmem_dealloc(taddr, A.tmem_cols);
@@ -3433,16 +3566,13 @@ bool plan_corr_tc2(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
     return off <= smem_cap;
 }
 
-// Shared-memory plan of k_corr_tc for a pass's largest geometry; false when the pass does not
-// fit the kernel (surface wider than 64 columns, more than 256 rows, chips taller than 226).
-// The whole chip operand and separate box-sum buffers when they fit ("overlap": the box sums
-// run beside the products); otherwise the box sums first and the chip operand in chunks of BC
-// columns in the space they used.
-// Plan of k_corr_bf: the widest chunk of chip columns whose operands, with the FP64 box sums,
-// fit `smem_cap`; false when the pass's surfaces exceed 64 x 64 or its window a thread per column.
+// Plan of k_corr_bf: the chunk of chip columns whose products keep each accumulator element's
+// chain near kBfChain, the widest window staging that fits `smem_cap` beside the chip operand
+// buffers and the denominators, and the box-sum stripes in the space of both; false when the
+// pass's surfaces exceed 64 x 64 or its chips 240 px.
 struct BfPlan {
-    int NB, QB, BC, XC, PC, NRS, AC, VR;
-    unsigned off_W, off_E, off_P, off_S1, off_S2, off_red;
+    int NB, QB, BC, OB, LW, PC, NRS, AC, RS, VS, XS;
+    unsigned off_S2, off_raw, off_V, off_den, off_E, off_P, off_red, Eb, Pb;
     uint32_t tmem_cols;
     size_t smem;
 };
@@ -3451,46 +3581,70 @@ bool plan_corr_bf(const PassGeometry& g, size_t smem_cap, BfPlan* P) {
     const int ch = static_cast<int>(g.max_ch), cw = static_cast<int>(g.max_cw);
     const int nr = static_cast<int>(g.max_nr), nc = static_cast<int>(g.max_nc);
     if (nr < 1 || nc < 1 || nr > 64 || nc > 64 || ch < 2 || cw < 2) return false;
-    const int XW = cw + nc - 1;
-    if (XW > kBfThreads) return false;  // one thread per window column for the box sums
     P->NB = round_up(ch + 15, 16);
     if (P->NB > 256) return false;
     P->QB = (ch + nr - 1 + 15) / 16;
     P->PC = round_up(kBfPadL + P->NB + 26, 8);
     P->NRS = nr | 1;
     P->AC = round_up(nr + 15, 16);
-    if (kBfAcc * P->AC > 512) return false;
+    if (4 * P->AC > 512) return false;  // two sets of two accumulators
     P->tmem_cols = 512;
+    P->RS = (ch + nr - 1) | 1;
+    P->VS = nr + 1;
+    // Window blocks meeting one surface row: (ch + 15) / 16 + 1, each a product per chip column.
+    const int blocks = (ch + 15) / 16 + 1;
+    int bc = std::max(2, (kBfChain / blocks) & ~1);
+    bc = std::min(bc, round_up(cw, 2));
+    while (bc > 2 && bc * P->PC > kBfPre * kBfThreads) bc -= 2;
+    if (bc * P->PC > kBfPre * kBfThreads) return false;
+    P->BC = bc;
     auto a16 = [](size_t v) { return (v + 15) & ~size_t(15); };
     const size_t Sb = a16(static_cast<size_t>(nc) * P->NRS * 8);
+    const size_t Eb = static_cast<size_t>(kBfLimbs) * bc * 2 * P->NB * 16;
+    const size_t Pb = a16(static_cast<size_t>(kBfLimbs) * bc * P->PC * 2);
     const size_t red = 3 * 32 * 8;
-    // At most kBfChunk chip columns per chunk: the FP32 accumulators are flushed to FP64 after
-    // every chunk, so each accumulates at most kBfChunk columns of products.
-    for (int bc = std::min(cw, kBfChunk) & ~1; bc >= 2; bc -= 2) {
-        const int XC = bc + 63;
-        const size_t Wb = kBfLimbs * static_cast<size_t>(P->QB) * 2 * XC * 16;
-        const size_t Eb = kBfLimbs * static_cast<size_t>(bc) * 2 * P->NB * 16;
-        const size_t Pb = a16(kBfLimbs * static_cast<size_t>(bc) * P->PC * 2);
-        const size_t alias = Wb + Eb + Pb;  // box-sum column sums, then the surface, reuse it
-        const size_t surf = static_cast<size_t>(nc) * P->NRS * 4;
-        if (alias < surf || alias < static_cast<size_t>(XW) * 16) continue;
-        const size_t total = alias + 2 * Sb + red;
-        if (total > smem_cap) continue;
-        P->BC = bc;
-        P->XC = XC;
-        P->VR = static_cast<int>(std::min<size_t>(nr, alias / (static_cast<size_t>(XW) * 16)));
-        P->off_W = 0;
-        P->off_E = static_cast<unsigned>(Wb);
-        P->off_P = static_cast<unsigned>(Wb + Eb);
-        P->off_S1 = static_cast<unsigned>(alias);
-        P->off_S2 = static_cast<unsigned>(alias + Sb);
-        P->off_red = static_cast<unsigned>(alias + 2 * Sb);
-        P->smem = total;
-        return true;
+    const size_t X = Sb + 2 * Eb + 2 * Pb + red;
+    const size_t colb = static_cast<size_t>(kBfLimbs) * P->QB * 2 * 16;  // limb bytes per column
+    const size_t minL = std::max(2 * Sb, a16(static_cast<size_t>(nc) * P->NRS * 4));
+    auto Lof = [&](int ob) { return std::max(minL, static_cast<size_t>(ob + 63) * colb); };
+    if (X >= smem_cap) return false;
+    int OB = round_up(cw, bc);
+    if (Lof(OB) + X > smem_cap) {
+        const int lw = static_cast<int>((smem_cap - X) / colb);
+        const int ob = (lw - 63) / bc * bc;
+        if (ob < bc) return false;
+        const int nout = (cw + ob - 1) / ob;
+        OB = round_up((cw + nout - 1) / nout, bc);
     }
-    return false;
+    P->OB = OB;
+    P->LW = OB + 63;
+    const size_t L = Lof(OB);
+    if (L + X > smem_cap) return false;
+    // Box-sum stripes after S1 and S2, up to the reduction scratch.
+    const int XW = cw + nc - 1;
+    const size_t avail = L + X - red - 2 * Sb;
+    const size_t per_col = static_cast<size_t>(P->RS) * 4 + static_cast<size_t>(P->VS) * 16;
+    if (avail < per_col + 16) return false;
+    P->XS = static_cast<int>(std::min<size_t>(XW, (avail - 16) / per_col));
+    P->off_S2 = static_cast<unsigned>(Sb);
+    P->off_raw = static_cast<unsigned>(2 * Sb);
+    P->off_V = static_cast<unsigned>(a16(2 * Sb + static_cast<size_t>(P->XS) * P->RS * 4));
+    if (P->off_V + static_cast<size_t>(P->XS) * P->VS * 16 > L + X - red) return false;
+    P->off_den = static_cast<unsigned>(L);
+    P->off_E = static_cast<unsigned>(L + Sb);
+    P->off_P = static_cast<unsigned>(L + Sb + 2 * Eb);
+    P->off_red = static_cast<unsigned>(L + Sb + 2 * Eb + 2 * Pb);
+    P->Eb = static_cast<unsigned>(Eb);
+    P->Pb = static_cast<unsigned>(Pb);
+    P->smem = L + X;
+    return true;
 }
 
+// Shared-memory plan of k_corr_tc for a pass's largest geometry; false when the pass does not
+// fit the kernel (surface wider than 64 columns, more than 256 rows, chips taller than 226).
+// The whole chip operand and separate box-sum buffers when they fit ("overlap": the box sums
+// run beside the products); otherwise the box sums first and the chip operand in chunks of BC
+// columns in the space they used.
 bool plan_corr_tc(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
     const int ch = static_cast<int>(g.max_ch), cw = static_cast<int>(g.max_cw);
     const int nr = static_cast<int>(g.max_nr), nc = static_cast<int>(g.max_nc);
@@ -4037,19 +4191,24 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
             B.NRM = static_cast<int>(geom.max_nr);
             B.NCM = static_cast<int>(geom.max_nc);
             B.NB = BPl.NB;
-            B.QB = BPl.QB;
             B.BC = BPl.BC;
-            B.XC = BPl.XC;
+            B.OB = BPl.OB;
+            B.LW = BPl.LW;
             B.PC = BPl.PC;
             B.NRS = BPl.NRS;
             B.AC = BPl.AC;
-            B.VR = BPl.VR;
-            B.off_W = BPl.off_W;
+            B.RS = BPl.RS;
+            B.VS = BPl.VS;
+            B.XS = BPl.XS;
+            B.off_S2 = BPl.off_S2;
+            B.off_raw = BPl.off_raw;
+            B.off_V = BPl.off_V;
+            B.off_den = BPl.off_den;
             B.off_E = BPl.off_E;
             B.off_P = BPl.off_P;
-            B.off_S1 = BPl.off_S1;
-            B.off_S2 = BPl.off_S2;
             B.off_red = BPl.off_red;
+            B.Eb = BPl.Eb;
+            B.Pb = BPl.Pb;
             B.tmem_cols = BPl.tmem_cols;
             B.out = out;
             B.sub_count = scratch.sub_count;

@@ -789,10 +789,10 @@ def batching_measure(ar, ctx, torch, dev, a, b, valid, fdown, stream, flush, arg
     return out
 
 
-def bf16_executed_flops(ch, cw, nr):
+def bf16_executed_flops(ch, cw, nr, products=6):
     """Tensor-core FLOPs k_corr_bf executes for one point: per 16-row window block the products
     of M = 64 surface columns, the block's trimmed operand rows and K = 16, for every chip
-    column and the three limb pairs."""
+    column and limb pair (six for Float32 imagery, five for integer imagery)."""
     NB = (ch + 15 + 15) // 16 * 16
     QB = (ch + nr - 1 + 15) // 16
     rows = 0
@@ -802,7 +802,7 @@ def bf16_executed_flops(ch, cw, nr):
         if hi > lo:
             elo = lo & ~15
             rows += (hi - elo + 15) & ~15
-    return 2.0 * 64 * 16 * rows * cw * 3
+    return 2.0 * 64 * 16 * rows * cw * products
 
 
 def precision_measure(ar, ctx, torch, dev, a4, b4, v4, fdown4, stream, flush, args, tensor_peak):
