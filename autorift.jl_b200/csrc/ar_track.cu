@@ -657,7 +657,6 @@ struct TcArgs {
     int MT;                          // MMA M: 64 or 128 surface columns
     int big;                         // 1: box sums before the products, chunks reuse their space
     unsigned off_E, off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
-    unsigned off_P2;                 // k_corr_tc2: the second staged-chip buffer
     int XV;                          // k_corr_tc2: row stride (words) of the column sums V1, V2
     int acc1_col;                    // k_corr_tc2: first column of its second accumulator
     uint32_t tmem_cols;
@@ -1573,61 +1572,6 @@ __device__ __forceinline__ void pt_geometry(const TcArgs& A, int64_t k, PtGeo& g
     g.ok = 1;
 }
 
-// The chip of a point as zero-padded byte columns of `sP` (column b at b * PC + kPadL; rows at
-// or beyond `dirty` are already zero, rows [ch, dirty) are cleared), by the first `nw` warps of
-// the block (thread `tid`): returns whether the calling thread saw a valid pixel
-// (_any_valid, src/track.jl:416-421) and, for power-of-two areas, adds the exact integer sum and
-// sum of squares into isum[0], isum[1] (one atomic per warp).
-__device__ __forceinline__ int stage_chip(const TcArgs& A, uint8_t* sP, int dirty, int64_t chip_r,
-                                          int64_t chip_c, int ch, int cw, bool pow2, int tid,
-                                          int nw, unsigned long long* isums) {
-    const int lane = tid & 31, warp = tid >> 5;
-    if (ch < dirty)
-        for (int b = warp; b < A.CWM; b += nw)
-            for (int a = ch + lane; a < dirty; a += 32) sP[b * A.PC + kPadL + a] = 0;
-    int any = 0;
-    unsigned long long isum = 0ull, isq = 0ull;
-    for (int a0 = 0; a0 < ch; a0 += 32) {
-        const int a = a0 + lane;
-        const int64_t r = chip_r + a;
-        const bool rin = a < ch && r >= 0 && r < A.nrows;
-        constexpr int kU = 4;
-        for (int b0 = warp; b0 < cw; b0 += kU * nw) {
-            uint32_t v[kU], m[kU];
-#pragma unroll
-            for (int u = 0; u < kU; ++u) {
-                const int b = b0 + u * nw;
-                const int64_t c = chip_c + b;
-                const bool in = rin && b < cw && c >= 0 && c < A.ncols;
-                v[u] = in ? A.sec[r + c * A.nrows] : 0u;
-                m[u] = in ? A.valid[r + c * A.nrows] : 0u;
-            }
-#pragma unroll
-            for (int u = 0; u < kU; ++u) {
-                const int b = b0 + u * nw;
-                if (a < ch && b < cw) {
-                    sP[b * A.PC + kPadL + a] = static_cast<uint8_t>(v[u]);
-                    any |= m[u];
-                    isum += v[u];
-                    isq += v[u] * v[u];
-                }
-            }
-        }
-    }
-    if (pow2) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            isum += __shfl_xor_sync(kFull, isum, o);
-            isq += __shfl_xor_sync(kFull, isq, o);
-        }
-        if (lane == 0) {
-            atomicAdd(&isums[0], isum);
-            atomicAdd(&isums[1], isq);
-        }
-    }
-    return any;
-}
-
 __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
     extern __shared__ __align__(1024) unsigned char smem_tc[];
     __shared__ uint64_t s_mbar;
@@ -1638,14 +1582,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
     __shared__ float s_fmax[kTcThreads / 32];
     __shared__ unsigned long long s_isum[2][2];
     __shared__ PtGeo s_geo[2];  // by iteration parity: a point's geometry, computed ahead
-    // By iteration parity: the point whose chip the buffer holds, staged ahead (-1: none), its
-    // _any_valid, and the rows its columns hold (rows at or beyond it are zero in every column).
-    __shared__ long long s_pre_k[2];
-    __shared__ int s_pre_any[2];
-    __shared__ int s_dirty[2];
     uint8_t* s_E = smem_tc + A.off_E;
     uint8_t* s_W = smem_tc + A.off_W;
-    uint8_t* const s_Pbuf[2] = {smem_tc + A.off_P, smem_tc + A.off_P2};
+    uint8_t* s_P = smem_tc + A.off_P;
     uint32_t* s_V1 = reinterpret_cast<uint32_t*>(smem_tc + A.off_V);
     uint32_t* s_V2 = s_V1 + A.NRM * A.XV + 16;
     uint32_t* s_S1 = reinterpret_cast<uint32_t*>(smem_tc + A.off_S1);
@@ -1658,12 +1597,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
     const int lane = tid & 31, warp = tid >> 5, nwarps = bd >> 5;
     const uint8_t* ref_end = A.ref + A.nrows * A.ncols;
 
-    if (tid < 2) {
-        s_geo[tid].k = -1;
-        s_pre_k[tid] = -1;
-        s_pre_any[tid] = 0;
-        s_dirty[tid] = 0;
-    }
+    if (tid < 2) s_geo[tid].k = -1;
     if (warp == 0) {
         tc::tmem_alloc(&s_taddr, A.tmem_cols);
         tc::tmem_relinquish();
@@ -1680,11 +1614,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
     uint32_t phase = 0;
     bool failed = false;
     if (tid < 4) s_isum[tid >> 1][tid & 1] = 0ull;
-    for (int e = tid; e < A.CWM * A.PC; e += bd) {
-        s_Pbuf[0][e] = 0;
-        s_Pbuf[1][e] = 0;
-    }
+    for (int e = tid; e < A.CWM * A.PC; e += bd) s_P[e] = 0;
     int iter = 0;
+    int dirty_ch = 0;
     TC_PHASE_INIT
 #ifdef AR_TC_PHASES
     unsigned long long tmi_issue = 0, tmi_done = 0;
@@ -1714,8 +1646,6 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
         TC_PHASE(0)
         const int ib = iter & 1;
         if (tid < 2) s_isum[ib ^ 1][tid] = 0ull;
-        if (tid == 2) s_pre_any[ib ^ 1] = 0;
-        uint8_t* const s_P = s_Pbuf[ib];
         // The geometry: computed ahead by the previous iteration when it reached its products.
         PtGeo g;
         if (s_geo[ib].k == k) {
@@ -1731,17 +1661,52 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
         const bool pow2 = (nnl & (nnl - 1)) == 0 && nnl <= 4096;
 
         // The chip as zero-padded byte columns, _any_valid over it (src/track.jl:416-421) and,
-        // for power-of-two areas, its exact integer sums (as in k_corr_tc) -- staged by warps 0-5
-        // during the previous point's products when that point reached them (s_pre_k).
-        const bool staged = s_pre_k[ib] == k;
+        // for power-of-two areas, its exact integer sums (as in k_corr_tc).
         int any = 0;
-        if (staged) {
-            any = s_pre_any[ib];
-        } else {
-            any = stage_chip(A, s_P, s_dirty[ib], chip_r, chip_c, ch, cw, pow2, tid, nwarps,
-                             s_isum[ib]);
-        }        if (!__syncthreads_or(any)) continue;
-        if (tid == 0 && !staged) s_dirty[ib] = ch;
+        unsigned long long isum = 0ull, isq = 0ull;
+        if (ch < dirty_ch)
+            for (int b = warp; b < A.CWM; b += nwarps)
+                for (int a = ch + lane; a < dirty_ch; a += 32) s_P[b * A.PC + kPadL + a] = 0;
+        dirty_ch = ch;
+        for (int a0 = 0; a0 < ch; a0 += 32) {
+            const int a = a0 + lane;
+            const int64_t r = chip_r + a;
+            const bool rin = a < ch && r >= 0 && r < A.nrows;
+            constexpr int kU = 4;
+            for (int b0 = warp; b0 < cw; b0 += kU * nwarps) {
+                uint32_t v[kU], m[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int b = b0 + u * nwarps;
+                    const int64_t c = chip_c + b;
+                    const bool in = rin && b < cw && c >= 0 && c < A.ncols;
+                    v[u] = in ? A.sec[r + c * A.nrows] : 0u;
+                    m[u] = in ? A.valid[r + c * A.nrows] : 0u;
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int b = b0 + u * nwarps;
+                    if (a < ch && b < cw) {
+                        s_P[b * A.PC + kPadL + a] = static_cast<uint8_t>(v[u]);
+                        any |= m[u];
+                        isum += v[u];
+                        isq += v[u] * v[u];
+                    }
+                }
+            }
+        }
+        if (pow2) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                isum += __shfl_xor_sync(kFull, isum, o);
+                isq += __shfl_xor_sync(kFull, isq, o);
+            }
+            if (lane == 0) {
+                atomicAdd(&s_isum[ib][0], isum);
+                atomicAdd(&s_isum[ib][1], isq);
+            }
+        }
+        if (!__syncthreads_or(any)) continue;
         TC_PHASE(2)
         if (tid == 0) A.out.searched[k] = 1;
 
@@ -1880,6 +1845,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
                 tmi_done += clock64() - tmi1;
             }
 #endif
+            // The next point's geometry, read after the next loop-top barrier.
+            const int64_t kn = k + 1;
+            if (stream == 0 && kn < kend) pt_geometry(A, kn, s_geo[ib ^ 1]);
         }
         TC_PHASE(5)
         // S[j][i] = sums of V[i][j .. j + cw - 1] for rows i in [i_lo, i_lo + ni): a task is a
@@ -2104,26 +2072,6 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
                 }
                 asm volatile("bar.sync 1, %0;" ::"r"(kBT) : "memory");
                 box_rows(0, nr);
-            }
-            // The next point: its geometry, then its chip staged into the other buffer while
-            // the products finish (warps 0-5, named barrier 1).
-            const int64_t kn = k + 1;
-            if (kn < kend) {
-                if (tid == 0) pt_geometry(A, kn, s_geo[ib ^ 1]);
-                asm volatile("bar.sync 1, %0;" ::"r"(kBT) : "memory");
-                const PtGeo& gn = s_geo[ib ^ 1];
-                if (gn.ok) {
-                    const long long nn2 = static_cast<long long>(gn.ch) * gn.cw;
-                    const bool p2 = (nn2 & (nn2 - 1)) == 0 && nn2 <= 4096;
-                    const int an = stage_chip(A, s_Pbuf[ib ^ 1], s_dirty[ib ^ 1], gn.chip_r,
-                                              gn.chip_c, gn.ch, gn.cw, p2, tid, 6, s_isum[ib ^ 1]);
-                    if (an) atomicOr(&s_pre_any[ib ^ 1], 1);
-                    asm volatile("bar.sync 1, %0;" ::"r"(kBT) : "memory");
-                    if (tid == 0) {
-                        s_dirty[ib ^ 1] = gn.ch;
-                        s_pre_k[ib ^ 1] = kn;
-                    }
-                }
             }
         }
         held = true;
@@ -3498,7 +3446,6 @@ size_t tmem_smem_floor(uint32_t cols, size_t static_smem) {
 struct TcPlan {
     int NB, QM, QS, PS, PC, XS, XT, NRS, NRM, NCM, CHM, CWM, BC, big, MT;
     unsigned off_E, off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
-    unsigned off_P2 = 0;
     int XV = 0, acc1_col = 0;
     uint32_t tmem_cols;
     size_t smem;
@@ -3546,8 +3493,6 @@ bool plan_corr_tc2(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
     P->off_W = static_cast<unsigned>(off);
     off += Wb;
     P->off_P = static_cast<unsigned>(off);
-    off += Pb;
-    P->off_P2 = static_cast<unsigned>(off);  // the next point's chip, staged ahead
     off += Pb;
     P->off_V = static_cast<unsigned>(off);
     P->off_num = P->off_V;
@@ -4091,7 +4036,6 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         B.off_W = TP.off_W;
         B.off_T = TP.off_T;
         B.off_P = TP.off_P;
-        B.off_P2 = TP.off_P2;
         B.off_V = TP.off_V;
         B.off_S1 = TP.off_S1;
         B.off_S2 = TP.off_S2;
