@@ -344,6 +344,80 @@ __global__ void __launch_bounds__(kHpThreads) k_highpass_int(const T* img, const
     }
 }
 
+// The same filter for square windows of odd width W <= 9 (the usual highpass widths), without
+// shared memory: a warp holds 32 consecutive rows of one column (a lane per row, coalesced loads
+// and stores) and walks along its columns. Each element becomes one 64-bit word -- its value
+// (offset to be non-negative) in the low 32 bits when it contributes, a contributing count of 1
+// at bit 32 or an in-image-invalid count of 1 at bit 48 -- so the window's three sums are one
+// 64-bit sum: down the column across lanes (shuffles), then along the row across the last W
+// columns (a sliding sum over a register ring). A warp writes the 32 - (W - 1) rows whose whole
+// window it holds. The mean and output are the generic kernel's, bit for bit.
+constexpr int kHwCols = 64;     // columns per warp
+constexpr int kHwWarps = 8;     // warps (row strips) per block
+
+template <typename T, int W>
+__global__ void __launch_bounds__(kHwWarps * 32) k_highpass_w(const T* img, const uint8_t* mask,
+                                                              int64_t nr, int64_t nc, float* out,
+                                                              uint8_t* vout) {
+    constexpr int L = W / 2;
+    constexpr int RO = 32 - 2 * L;  // output rows of a strip
+    constexpr uint64_t kContrib = 1ull << 32, kInvalid = 1ull << 48;
+    constexpr int kBias = std::is_signed<T>::value ? 32768 : 0;
+    const int lane = threadIdx.x & 31;
+    const int64_t strip = static_cast<int64_t>(blockIdx.x) * kHwWarps + (threadIdx.x >> 5);
+    const int64_t r0 = strip * RO;  // first output row of the strip
+    if (r0 >= nr) return;
+    const int64_t c0 = static_cast<int64_t>(blockIdx.y) * kHwCols;
+    const int64_t c1 = c0 + kHwCols < nc ? c0 + kHwCols : nc;
+    const int64_t r = r0 - L + lane;
+    const bool rin = r >= 0 && r < nr;
+    const bool writes = lane >= L && lane < 32 - L && r < nr;
+    uint64_t ring_v[W], ring_p[W];
+#pragma unroll
+    for (int u = 0; u < W; ++u) ring_v[u] = ring_p[u] = 0ull;
+    uint64_t S = 0ull;
+    for (int64_t cb = c0 - L; cb < c1 + L; cb += W) {
+#pragma unroll
+        for (int u = 0; u < W; ++u) {
+            const int64_t c = cb + u;
+            if (c >= c1 + L) break;
+            uint64_t p = 0ull;
+            if (rin && c >= 0 && c < nc) {
+                const int64_t g = r + c * nr;
+                const int v = static_cast<int>(img[g]) + kBias;
+                p = mask[g] ? (static_cast<uint64_t>(static_cast<uint32_t>(v)) | kContrib) : kInvalid;
+            }
+            uint64_t V = p;
+#pragma unroll
+            for (int d = 1; d <= L; ++d) V += __shfl_up_sync(kFullMask, p, d) + __shfl_down_sync(kFullMask, p, d);
+            S += V - ring_v[u];
+            ring_v[u] = V;
+            ring_p[u] = p;
+            const int64_t j = c - L;  // the output column whose window ends at column c
+            if (writes && j >= c0) {
+                const int cnt = static_cast<int>((S >> 32) & 0xFFFFull);
+                const int inv = static_cast<int>(S >> 48);
+                const int a = static_cast<int>(static_cast<uint32_t>(S)) - kBias * cnt;
+                const float mean = cnt > 0 ? __double2float_rn(__ddiv_rn(static_cast<double>(a),
+                                                                         static_cast<double>(cnt)))
+                                           : __int_as_float(0x7fc00000);
+                const uint64_t pc = ring_p[(u - L + W) % W];  // column j's element
+                const bool m = ((pc >> 32) & 1ull) != 0ull;
+                const float x = static_cast<float>(static_cast<int>(static_cast<uint32_t>(pc)) - kBias);
+                float o = (m && isfinite(mean)) ? __fsub_rn(x, mean) : __int_as_float(0x7fc00000);
+                bool v = inv == 0;
+                if (!isfinite(o)) {
+                    o = 0.0f;
+                    v = false;
+                }
+                const int64_t g = r + j * nr;
+                out[g] = o;
+                vout[g] = v ? 1 : 0;
+            }
+        }
+    }
+}
+
 size_t highpass_int_smem(int wx, int wy, int TR) {
     const size_t IR = TR + wy - 1, IC = kHpCols + wx - 1, IRp = IR | 1;
     return IC * IRp * 8 + IC * TR * 8;
@@ -640,7 +714,22 @@ cudaError_t prepare_t(const PrepareJob& J, cudaStream_t s, long long* launches) 
     float* filt = J.quantize == 1 ? J.ftmp : static_cast<float*>(J.out);
     cudaError_t e;
     if (smem > static_cast<size_t>(kDynSmemCap)) return cudaErrorInvalidValue;
-    if (J.preprocess == 1 && !std::is_same<T, float>::value) {
+    if (J.preprocess == 1 && !std::is_same<T, float>::value && wx == wy && (wx & 1) && wx <= 9) {
+        // Integer imagery, square odd window up to 9: the shared-memory-free kernel.
+        constexpr int RO_of[10] = {0, 32, 0, 30, 0, 28, 0, 26, 0, 24};
+        const int RO = RO_of[wx];
+        const int64_t strips = (J.nrows + RO - 1) / RO;
+        const dim3 wgrid(static_cast<unsigned>((strips + kHwWarps - 1) / kHwWarps),
+                         static_cast<unsigned>((J.ncols + kHwCols - 1) / kHwCols));
+        switch (wx) {
+            case 1: k_highpass_w<T, 1><<<wgrid, kHwWarps * 32, 0, s>>>(img, J.mask, J.nrows, J.ncols, filt, J.vout); break;
+            case 3: k_highpass_w<T, 3><<<wgrid, kHwWarps * 32, 0, s>>>(img, J.mask, J.nrows, J.ncols, filt, J.vout); break;
+            case 5: k_highpass_w<T, 5><<<wgrid, kHwWarps * 32, 0, s>>>(img, J.mask, J.nrows, J.ncols, filt, J.vout); break;
+            case 7: k_highpass_w<T, 7><<<wgrid, kHwWarps * 32, 0, s>>>(img, J.mask, J.nrows, J.ncols, filt, J.vout); break;
+            default: k_highpass_w<T, 9><<<wgrid, kHwWarps * 32, 0, s>>>(img, J.mask, J.nrows, J.ncols, filt, J.vout); break;
+        }
+        *launches += 1;
+    } else if (J.preprocess == 1 && !std::is_same<T, float>::value) {
         // Integer imagery: exact 32-bit sums, the tallest tile whose staging fits.
         int TR = 128;
         while (TR > 32 && highpass_int_smem(wx, wy, TR) > static_cast<size_t>(kDynSmemCap)) TR /= 2;

@@ -121,3 +121,21 @@ def test_prepared_pair_tracks_like_host_prepared(ar, O, gpu_lib):
     for x, y in zip(g, want):
         same = (x == y) | (np.isnan(x) & np.isnan(y)) if x.dtype.kind == "f" else (x == y)
         assert same.mean() > 0.995
+
+
+@pytest.mark.parametrize("dtype", [np.uint8, np.uint16, np.int16])
+@pytest.mark.parametrize("width", [1, 3, 5, 9])
+def test_highpass_small_widths_exact(ar, O, gpu_lib, dtype, width):
+    """Square odd windows up to 9 on integer imagery (the warp-per-row-strip kernel): ragged
+    extents (strip and column-block remainders), invalid blocks, single pixels and image edges
+    against the oracle, bit for bit."""
+    rng = np.random.default_rng(width)
+    for shape in ((61, 70), (100, 129), (33, 5)):
+        hi = {np.uint8: 256, np.uint16: 65536, np.int16: 32768}[dtype]
+        lo = -32768 if dtype == np.int16 else 0
+        a = rng.integers(lo, hi, shape).astype(dtype)
+        m = rng.random(shape) > 0.05
+        m[10:14, :] = False
+        m[:, 3] = False
+        p = ar.params(quantize="none", filter_width=width)
+        _check(ar, O, a, a[::-1].copy(), m, m[::-1].copy(), p, "highpass", width, quant="none")
