@@ -503,12 +503,6 @@ struct QuantStats {
 
 namespace {
 
-template <typename T>
-__device__ __forceinline__ bool q_ok(const T* img, const uint8_t* mask, int64_t i, double* v) {
-    *v = static_cast<double>(img[i]);
-    return mask[i] && isfinite(*v);
-}
-
 __device__ void block_dd(DD& a, long long& c, DD* sa, long long* sc) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
@@ -530,10 +524,19 @@ __device__ void block_dd(DD& a, long long& c, DD* sa, long long* sc) {
     }
 }
 
-// pass 0: sum and count of the valid finite values; pass 1: sum of squared deviations. Each
-// thread keeps kQU independent double-double accumulators fed by kQU coalesced loads per step
-// (more loads in flight than one dependent chain allows), merged in a fixed order.
+// pass 0: sum and count of the valid finite values; pass 1: sum of squared deviations. A thread
+// takes runs of four consecutive elements (one vector load of the image and one of the mask
+// where both are aligned) and keeps kQU runs in flight, each feeding its own double-double
+// accumulator; the accumulators merge in a fixed order.
 constexpr int kQU = 4;
+
+template <typename T>
+struct alignas(4 * sizeof(T)) Run4 {
+    T x[4];
+};
+struct alignas(4) Mask4 {
+    uint8_t x[4];
+};
 
 template <typename T, int PASS>
 __global__ void __launch_bounds__(kStatThreads) k_qstats(const T* img, const uint8_t* mask,
@@ -548,25 +551,46 @@ __global__ void __launch_bounds__(kStatThreads) k_qstats(const T* img, const uin
         cc[u] = 0;
     }
     const double mean = PASS == 1 ? st->mean : 0.0;
-    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-    for (int64_t i0 = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i0 < n;
-         i0 += kQU * stride) {
-        double v[kQU];
-        bool ok[kQU];
+    const bool vec = (reinterpret_cast<uintptr_t>(img) % (4 * sizeof(T))) == 0 &&
+                     (reinterpret_cast<uintptr_t>(mask) % 4) == 0;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;  // in runs of four
+    for (int64_t r0 = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; 4 * r0 < n;
+         r0 += kQU * stride) {
+        T t[kQU][4];
+        uint8_t m[kQU][4];
 #pragma unroll
         for (int u = 0; u < kQU; ++u) {
-            const int64_t i = i0 + u * stride;
-            ok[u] = i < n && q_ok(img, mask, i, &v[u]);
+            const int64_t i = 4 * (r0 + u * stride);
+            if (vec && i + 4 <= n) {
+                const Run4<T> w = *reinterpret_cast<const Run4<T>*>(img + i);
+                const Mask4 k = *reinterpret_cast<const Mask4*>(mask + i);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    t[u][e] = w.x[e];
+                    m[u][e] = k.x[e];
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const bool in = i + e < n;
+                    t[u][e] = in ? img[i + e] : T(0);
+                    m[u][e] = in ? mask[i + e] : static_cast<uint8_t>(0);
+                }
+            }
         }
 #pragma unroll
         for (int u = 0; u < kQU; ++u) {
-            if (!ok[u]) continue;
-            if (PASS == 0) {
-                dd_add(acc[u], v[u]);
-                ++cc[u];
-            } else {
-                const double d = __dsub_rn(v[u], mean);
-                dd_add(acc[u], __dmul_rn(d, d));
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const double v = static_cast<double>(t[u][e]);
+                if (!(m[u][e] && isfinite(v))) continue;
+                if (PASS == 0) {
+                    dd_add(acc[u], v);
+                    ++cc[u];
+                } else {
+                    const double d = __dsub_rn(v, mean);
+                    dd_add(acc[u], __dmul_rn(d, d));
+                }
             }
         }
     }
