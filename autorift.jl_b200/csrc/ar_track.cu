@@ -2280,17 +2280,20 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
 // row whose differences cw columns apart are the box sums -- and from them each surface value's
 // FP64 denominator (src/correlate.jl:575-630); then the window's limbs for as many chip columns
 // as shared memory holds (all of them up to 64-px chips), and the products chunk by chunk of BC
-// chip columns. Two accumulator sets (one for c0 w0, one for the five smaller products) take
-// alternate chunks: while the tensor core runs chunk c, the threads build chunk c + 1's chip
-// operand and add chunk c - 1's accumulators into FP64 sums they keep in registers (the tensor
-// core's FP32 accumulation does not round to nearest, so a long chain of products into one
-// accumulator drifts: ~1e-4 of the numerator over the ~1,000 products per accumulator of a 192-px
-// chip; a chunk's chain is kept near kBfChain). Surfaces up to 64 x 64.
+// chip columns. Four threads issue a chunk's products, each into an accumulator of its own (one
+// thread issues an MMA about every 120 cycles, so the small M = 64 products need several issuers
+// to keep the tensor core busy). Two sets of four accumulators take alternate chunks: while the
+// tensor core runs chunk c, the threads build chunk c + 1's chip operand and add chunk c - 1's
+// accumulators into FP64 sums they keep in registers (the tensor core's FP32 accumulation does
+// not round to nearest, so a long chain of products into one accumulator drifts: ~1e-4 of the
+// numerator over the ~1,000 products per accumulator of a 192-px chip; a chunk's chain is kept
+// near kBfChain). Surfaces up to 64 x 64.
 
 constexpr int kBfThreads = 256;
 constexpr int kBfLimbs = 3;        // BF16 limbs per operand
 constexpr int kBfPadL = 16;        // zero elements before each staged chip column
-constexpr int kBfChain = 20;       // accumulating products per accumulator element per chunk
+constexpr int kBfChain = 24;       // accumulating products per accumulator element per chunk
+constexpr int kBfIssuers = 4;      // issuing threads (and accumulators) per set
 constexpr int kBfPre = 4;          // staged chip elements per thread and chunk
 constexpr int kBfBatch = 8;        // global loads a thread issues before using them
 
@@ -2378,8 +2381,8 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
         tc::tmem_relinquish();
     }
     if (tid == 0) {
-        tc::mbar_init(&s_mbar[0], 1);  // one commit per chunk
-        tc::mbar_init(&s_mbar[1], 1);
+        tc::mbar_init(&s_mbar[0], kBfIssuers);  // one commit per issuer and chunk
+        tc::mbar_init(&s_mbar[1], kBfIssuers);
         tc::fence_mbar_init();
     }
     tc::fence_before_sync();
@@ -2402,7 +2405,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
 #pragma unroll
             for (int t = 0; t < 16; ++t) z[t] = 0u;
             const uint32_t lq = taddr + (static_cast<uint32_t>(32 * warp) << 16);
-            for (int c = 2 * s * A.AC; c < 2 * (s + 1) * A.AC; c += 16)
+            for (int c = kBfIssuers * s * A.AC; c < kBfIssuers * (s + 1) * A.AC; c += 16)
                 tc::tmem_st16(lq + static_cast<uint32_t>(c), z);
             tc::tmem_wait_st();
         }
@@ -2590,14 +2593,16 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
         for (int v = 0; v < 16; ++v) accd[v] = 0.0;
         auto flush_set = [&](int s) {
             if (32 * half < nr) {
-                uint32_t hi[16], lo[16];
-                tc::tmem_ld16dp(qbase + static_cast<uint32_t>(2 * s * A.AC), hi);
-                tc::tmem_ld16dp(qbase + static_cast<uint32_t>((2 * s + 1) * A.AC), lo);
+                uint32_t r[kBfIssuers][16];
+#pragma unroll
+                for (int t = 0; t < kBfIssuers; ++t)
+                    tc::tmem_ld16dp(qbase + static_cast<uint32_t>((kBfIssuers * s + t) * A.AC), r[t]);
                 tc::tmem_wait_ld();
 #pragma unroll
                 for (int v = 0; v < 16; ++v)
-                    accd[v] = __dadd_rn(__dadd_rn(accd[v], static_cast<double>(__uint_as_float(hi[v]))),
-                                        static_cast<double>(__uint_as_float(lo[v])));
+#pragma unroll
+                    for (int t = 0; t < kBfIssuers; ++t)
+                        accd[v] = __dadd_rn(accd[v], static_cast<double>(__uint_as_float(r[t][v])));
             }
         };
         // A chunk's chip columns C'[a, b0 + bl] as BF16 limbs, zero-padded: the loads first
@@ -2709,17 +2714,21 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                 tc::fence_proxy_async_smem();
                 tc::fence_before_sync();
                 __syncthreads();  // operands complete; accumulator set s clear
-                // One thread issues the chunk's products: limb pairs (chip, window) (0,0) into
-                // the set's first accumulator, (0,1), (1,0), (1,1), (2,0), (0,2) into its second
-                // (integer windows have no third limb).
-                if (tid == 0) {
+                // Lane 0 of warps 0-3 issue the chunk's products, each into an accumulator of
+                // its own (one thread issues a product about every 120 cycles; four keep the
+                // tensor core busy): issuer t takes the window blocks q of parity t & 1 and the
+                // limb pairs (chip, window) (0,0), (1,1), (2,0) when t < 2, else (0,1), (1,0),
+                // (0,2) (integer windows have no third limb).
+                if (lane == 0 && warp < kBfIssuers) {
                     tc::fence_after_sync();
                     const uint32_t wb = tc::smem_u32(s_W);
                     const uint32_t eb = tc::smem_u32(s_E) + static_cast<uint32_t>(s * A.Eb);
+                    const int par = warp & 1;
+                    const uint32_t dacc = taddr + static_cast<uint32_t>((kBfIssuers * s + warp) * A.AC);
 #pragma unroll 1
-                    for (int p = 0; p < 6; ++p) {
-                        const int cl = p == 2 || p == 3 ? 1 : p == 4 ? 2 : 0;
-                        const int wl = p == 1 || p == 3 ? 1 : p == 5 ? 2 : 0;
+                    for (int pp = 0; pp < 3; ++pp) {
+                        const int cl = warp < 2 ? pp : (pp == 1 ? 1 : 0);
+                        const int wl = warp < 2 ? (pp == 1 ? 1 : 0) : (pp == 0 ? 1 : pp == 2 ? 2 : 0);
                         if (Tr::integer && wl == 2) continue;
                         const uint64_t da0 = tc::smem_desc(wb + static_cast<uint32_t>(wl * wlimb),
                                                            static_cast<uint32_t>(A.LW * 16), 128);
@@ -2727,8 +2736,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                                                            static_cast<uint32_t>(A.NB * 16), 128);
                         const uint32_t a_hi = static_cast<uint32_t>(da0 >> 32);
                         const uint32_t b_hi = static_cast<uint32_t>(db0 >> 32);
-                        const uint32_t dacc = taddr + static_cast<uint32_t>((2 * s + (p ? 1 : 0)) * A.AC);
-                        for (int q = 0; q < QBp; ++q) {
+                        for (int q = par; q < QBp; q += 2) {
                             int elo, n;
                             if (!block_rows(q, A.NB, nr, &elo, &n)) continue;
                             const uint32_t idesc = tc::idesc_bf16_f32(64, n);
@@ -3531,16 +3539,19 @@ bool plan_corr_bf(const PassGeometry& g, size_t smem_cap, BfPlan* P) {
     P->QB = (ch + nr - 1 + 15) / 16;
     P->PC = round_up(kBfPadL + P->NB + 26, 8);
     P->NRS = nr | 1;
-    P->AC = round_up(nr + 15, 16);
-    if (4 * P->AC > 512) return false;  // two sets of two accumulators
+    // A block's products write accumulator columns [16 q + elo - NB + 16, + n), all below
+    // round16(nr) (block_rows: elo, NB multiples of 16, the rows' end at most NB - 16 + nr - 16 q).
+    P->AC = round_up(nr, 16);
+    if (2 * kBfIssuers * P->AC > 512) return false;  // two sets of kBfIssuers accumulators
     P->tmem_cols = 512;
     P->RS = (ch + nr - 1) | 1;
     P->VS = nr + 1;
-    // Window blocks meeting one surface row: (ch + 15) / 16 + 1, each a product per chip column.
+    // Window blocks meeting one surface row: (ch + 15) / 16 + 1, half of them (one parity) into
+    // an accumulator, with three limb pairs each: 1.5 blocks accumulating steps per chip column.
     const int blocks = (ch + 15) / 16 + 1;
-    int bc = std::max(2, (kBfChain / blocks) & ~1);
-    bc = std::min(bc, round_up(cw, 2));
-    while (bc > 2 && bc * P->PC > kBfPre * kBfThreads) bc -= 2;
+    int bc = std::max(1, 2 * kBfChain / (3 * blocks));
+    bc = std::min(bc, cw);
+    while (bc > 1 && bc * P->PC > kBfPre * kBfThreads) --bc;
     if (bc * P->PC > kBfPre * kBfThreads) return false;
     P->BC = bc;
     auto a16 = [](size_t v) { return (v + 15) & ~size_t(15); };
