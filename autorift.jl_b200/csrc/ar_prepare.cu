@@ -346,12 +346,16 @@ __global__ void __launch_bounds__(kHpThreads) k_highpass_int(const T* img, const
 
 // The same filter for square windows of odd width W <= 9 (the usual highpass widths), without
 // shared memory: a warp holds 32 consecutive rows of one column (a lane per row, coalesced loads
-// and stores) and walks along its columns. Each element becomes one 64-bit word -- its value
-// (offset to be non-negative) in the low 32 bits when it contributes, a contributing count of 1
-// at bit 32 or an in-image-invalid count of 1 at bit 48 -- so the window's three sums are one
-// 64-bit sum: down the column across lanes (shuffles), then along the row across the last W
-// columns (a sliding sum over a register ring). A warp writes the 32 - (W - 1) rows whose whole
-// window it holds. The mean and output are the generic kernel's, bit for bit.
+// and stores) and walks along its columns, W columns' loads at a time. An element becomes one
+// 32-bit word -- its value (offset to be non-negative) in bits 0-19 when it contributes, a
+// contributing count of 1 at bit 20 or an in-image-invalid count of 1 at bit 24 -- so the three
+// sums down a column of the window are one 32-bit sum across lanes (shuffles); along the row they
+// are a sliding sum over a register ring of the last W columns, widened to 64 bits (value in the
+// low word, counts at bits 32 and 48). A warp writes the 32 - (W - 1) rows whose whole window it
+// holds. The mean is an FP32 division of the exact sum by the count: both are exact in FP32
+// (below 2^24) and FP64 has more than 2 x 24 + 2 bits, so it equals the generic kernel's FP64
+// quotient rounded to FP32 (double rounding is innocuous there); the output is the generic
+// kernel's, bit for bit.
 constexpr int kHwCols = 64;     // columns per warp
 constexpr int kHwWarps = 8;     // warps (row strips) per block
 
@@ -361,7 +365,7 @@ __global__ void __launch_bounds__(kHwWarps * 32) k_highpass_w(const T* img, cons
                                                               uint8_t* vout) {
     constexpr int L = W / 2;
     constexpr int RO = 32 - 2 * L;  // output rows of a strip
-    constexpr uint64_t kContrib = 1ull << 32, kInvalid = 1ull << 48;
+    constexpr uint32_t kC32 = 1u << 20, kI32 = 1u << 24;
     constexpr int kBias = std::is_signed<T>::value ? 32768 : 0;
     const int lane = threadIdx.x & 31;
     const int64_t strip = static_cast<int64_t>(blockIdx.x) * kHwWarps + (threadIdx.x >> 5);
@@ -372,38 +376,48 @@ __global__ void __launch_bounds__(kHwWarps * 32) k_highpass_w(const T* img, cons
     const int64_t r = r0 - L + lane;
     const bool rin = r >= 0 && r < nr;
     const bool writes = lane >= L && lane < 32 - L && r < nr;
-    uint64_t ring_v[W], ring_p[W];
+    uint64_t ring_v[W];
+    uint32_t ring_p[W];
 #pragma unroll
-    for (int u = 0; u < W; ++u) ring_v[u] = ring_p[u] = 0ull;
+    for (int u = 0; u < W; ++u) {
+        ring_v[u] = 0ull;
+        ring_p[u] = 0u;
+    }
     uint64_t S = 0ull;
     for (int64_t cb = c0 - L; cb < c1 + L; cb += W) {
+        uint32_t pv[W];
 #pragma unroll
         for (int u = 0; u < W; ++u) {
             const int64_t c = cb + u;
-            if (c >= c1 + L) break;
-            uint64_t p = 0ull;
+            pv[u] = 0u;
             if (rin && c >= 0 && c < nc) {
                 const int64_t g = r + c * nr;
-                const int v = static_cast<int>(img[g]) + kBias;
-                p = mask[g] ? (static_cast<uint64_t>(static_cast<uint32_t>(v)) | kContrib) : kInvalid;
+                const uint32_t v = static_cast<uint32_t>(static_cast<int>(img[g]) + kBias);
+                pv[u] = mask[g] ? (v | kC32) : kI32;
             }
-            uint64_t V = p;
+        }
+#pragma unroll
+        for (int u = 0; u < W; ++u) {
+            const uint32_t p = pv[u];
+            uint32_t V = p;
 #pragma unroll
             for (int d = 1; d <= L; ++d) V += __shfl_up_sync(kFullMask, p, d) + __shfl_down_sync(kFullMask, p, d);
-            S += V - ring_v[u];
-            ring_v[u] = V;
+            const uint64_t V64 = static_cast<uint64_t>(V & (kC32 - 1u)) |
+                                 (static_cast<uint64_t>((V >> 20) & 0xFu) << 32) |
+                                 (static_cast<uint64_t>(V >> 24) << 48);
+            S += V64 - ring_v[u];
+            ring_v[u] = V64;
             ring_p[u] = p;
-            const int64_t j = c - L;  // the output column whose window ends at column c
-            if (writes && j >= c0) {
+            const int64_t j = cb + u - L;  // the output column whose window ends at column cb + u
+            if (writes && j >= c0 && j < c1) {
                 const int cnt = static_cast<int>((S >> 32) & 0xFFFFull);
                 const int inv = static_cast<int>(S >> 48);
                 const int a = static_cast<int>(static_cast<uint32_t>(S)) - kBias * cnt;
-                const float mean = cnt > 0 ? __double2float_rn(__ddiv_rn(static_cast<double>(a),
-                                                                         static_cast<double>(cnt)))
+                const float mean = cnt > 0 ? __fdiv_rn(static_cast<float>(a), static_cast<float>(cnt))
                                            : __int_as_float(0x7fc00000);
-                const uint64_t pc = ring_p[(u - L + W) % W];  // column j's element
-                const bool m = ((pc >> 32) & 1ull) != 0ull;
-                const float x = static_cast<float>(static_cast<int>(static_cast<uint32_t>(pc)) - kBias);
+                const uint32_t pc = ring_p[(u - L + W) % W];  // column j's element
+                const bool m = (pc & kC32) != 0u;
+                const float x = static_cast<float>(static_cast<int>(pc & (kC32 - 1u)) - kBias);
                 float o = (m && isfinite(mean)) ? __fsub_rn(x, mean) : __int_as_float(0x7fc00000);
                 bool v = inv == 0;
                 if (!isfinite(o)) {
@@ -641,9 +655,10 @@ __global__ void k_qfinal(QuantStats* st, int nblocks) {
     }
 }
 
-// kQV consecutive pixels per thread: one vector load of the image where it is 16-byte aligned
-// (the filtered Float32 scratch always is), one 4-byte store of the output where aligned.
-constexpr int kQV = 4;
+// kQV consecutive pixels per thread as runs of four: one vector load of the image and one of the
+// mask per run where aligned (the filtered Float32 scratch and the masks always are), one 4-byte
+// store of the output per run.
+constexpr int kQV = 8;
 
 template <typename T>
 __global__ void k_quantize(const T* img, const uint8_t* mask, int64_t n, const QuantStats* st,
@@ -652,22 +667,35 @@ __global__ void k_quantize(const T* img, const uint8_t* mask, int64_t n, const Q
     if (i0 >= n) return;
     const long long cnt = st->n;
     const double sd = st->sd, lo = st->lo, scale = st->scale;
+    const bool vec = (reinterpret_cast<uintptr_t>(img) % (4 * sizeof(T))) == 0 &&
+                     (reinterpret_cast<uintptr_t>(mask) % 4) == 0 &&
+                     (reinterpret_cast<uintptr_t>(out) % 4) == 0;
     T vals[kQV];
-    const bool full = i0 + kQV <= n;
-    if (full && sizeof(T) == 4 && (reinterpret_cast<uintptr_t>(img + i0) & 15) == 0) {
-        const uint4 w = __ldg(reinterpret_cast<const uint4*>(img + i0));
-        const T* t = reinterpret_cast<const T*>(&w);
+    uint8_t ms[kQV];
 #pragma unroll
-        for (int u = 0; u < kQV; ++u) vals[u] = t[u];
-    } else {
+    for (int r = 0; r < kQV; r += 4) {
+        const int64_t i = i0 + r;
+        if (vec && i + 4 <= n) {
+            const Run4<T> w = *reinterpret_cast<const Run4<T>*>(img + i);
+            const Mask4 k = *reinterpret_cast<const Mask4*>(mask + i);
 #pragma unroll
-        for (int u = 0; u < kQV; ++u) vals[u] = i0 + u < n ? img[i0 + u] : T(0);
+            for (int e = 0; e < 4; ++e) {
+                vals[r + e] = w.x[e];
+                ms[r + e] = k.x[e];
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const bool in = i + e < n;
+                vals[r + e] = in ? img[i + e] : T(0);
+                ms[r + e] = in ? mask[i + e] : static_cast<uint8_t>(0);
+            }
+        }
     }
     uint8_t o[kQV];
 #pragma unroll
     for (int u = 0; u < kQV; ++u) {
-        const int64_t i = i0 + u;
-        const bool m = i < n && mask[i] != 0;
+        const bool m = ms[u] != 0;
         const double v = static_cast<double>(vals[u]);
         if (cnt == 0) {
             o[u] = 0;
@@ -681,11 +709,15 @@ __global__ void k_quantize(const T* img, const uint8_t* mask, int64_t n, const Q
             o[u] = static_cast<uint8_t>(__double2uint_rn(x));
         }
     }
-    if (full && (reinterpret_cast<uintptr_t>(out + i0) & 3) == 0) {
-        *reinterpret_cast<uchar4*>(out + i0) = make_uchar4(o[0], o[1], o[2], o[3]);
-    } else {
-        for (int u = 0; u < kQV; ++u)
-            if (i0 + u < n) out[i0 + u] = o[u];
+#pragma unroll
+    for (int r = 0; r < kQV; r += 4) {
+        const int64_t i = i0 + r;
+        if (vec && i + 4 <= n) {
+            *reinterpret_cast<uchar4*>(out + i) = make_uchar4(o[r], o[r + 1], o[r + 2], o[r + 3]);
+        } else {
+            for (int e = 0; e < 4; ++e)
+                if (i + e < n) out[i + e] = o[r + e];
+        }
     }
 }
 
