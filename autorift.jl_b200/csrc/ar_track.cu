@@ -2392,6 +2392,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
     uint32_t ph[2] = {0u, 0u};
     bool pend[2] = {false, false};
     bool failed = false;
+    TC_PHASE_INIT
 
     // Accumulator values of a thread after a chunk: value v is surface row
     // i = 32 half + 8 (v / 4) + 2 (lane % 4) + v % 2, column j = 16 quarter + lane / 4 (+ 8 when
@@ -2424,6 +2425,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
         tc::fence_before_sync();
         __syncthreads();  // the previous point's buffers and accumulators are no longer read
         tc::fence_after_sync();
+        TC_PHASE(0)
         const int64_t prx = A.pts.rx[k], pry = A.pts.ry[k];
         if (!(prx > 0 && pry > 0)) continue;
         const double xs = A.pts.x[k] + shx, ys = A.pts.y[k] + shy;
@@ -2463,6 +2465,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
         }
         if (!__syncthreads_or(any)) continue;
         if (tid == 0) A.out.searched[k] = 1;
+        TC_PHASE(1)
 
         // prepare_chip! as the CUDA-core kernel (the same per-thread order): FP64 mean, FP64 sum
         // of squares of the deviations, FP64 sum of the Float32-rounded deviations.
@@ -2508,6 +2511,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
         const double cshift = Tr::integer ? rint(mean) : static_cast<double>(__double2float_rn(mean));
         const float csf = static_cast<float>(cshift);
         if (tid == 0 && !(A.up == 1 || nr < 5 || nc < 5)) s_slot = atomicAdd(A.sub_count, 1);
+        TC_PHASE(2)
 
         // Box sums in FP64, a stripe of window columns at a time: the stripe's image values
         // (exact in FP32 for every element type), its column sums V(i, x) of ch rows, then the
@@ -2570,6 +2574,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
             }
             __syncthreads();
         }
+        TC_PHASE(3)
         // FP64 denominators (src/correlate.jl:591-600, 624-628).
         for (int e = tid; e < nr * nc; e += bd) {
             const int i = e % nr, j = e / nr;
@@ -2587,6 +2592,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
         clear_set(0);
         clear_set(1);
         __syncthreads();  // S1 and S2 read before the window limbs replace them
+        TC_PHASE(4)
 
         double accd[16];
 #pragma unroll
@@ -2682,6 +2688,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                 p_store(0, min(A.BC, obn), pr);
             }
             __syncthreads();  // limbs and the first chunk's chip columns complete
+            TC_PHASE(5)
 
             const int nch = (obn + A.BC - 1) / A.BC;
             for (int c = 0; c < nch; ++c) {
@@ -2753,6 +2760,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                     }
                     tc::mma_commit(&s_mbar[s]);
                 }
+                TC_PHASE(7)
                 pend[s] = true;
                 // The next chunk's chip columns: loads now, conversion after the flush.
                 const bool more = c + 1 < nch;
@@ -2771,6 +2779,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                 if (more) p_store(s ^ 1, bnext, pr);
                 tc::fence_before_sync();
                 __syncthreads();
+                TC_PHASE(6)
             }
             if (ok) {
                 const int sl = (nch - 1) & 1;
@@ -2785,6 +2794,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                     __syncthreads();  // the window limbs are replaced next
                 }
             }
+            TC_PHASE(8)
         }
         if (!ok) {
             if (tid == 0) atomicExch(A.status, 1);
@@ -2809,6 +2819,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
             }
         }
         __syncthreads();
+        TC_PHASE(9)
         if (A.flops && tid == 0)
             atomicAdd(A.flops, 2ull * static_cast<unsigned long long>(ch) * cw * nr * nc);
         // Integer peak (src/peak.jl:32-61).
@@ -2852,7 +2863,10 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                 A.sub_origin[2 * slot + 1] = pj0;
             }
         }
+        TC_PHASE(10)
+        TC_PHASE_POINT
     }
+    TC_PHASE_FLUSH
     // Products still in flight after a failed wait finish before their columns are freed.
     for (int s = 0; s < 2; ++s)
         if (pend[s]) tc::mbar_wait(&s_mbar[s], ph[s], kTcWaitPolls);
