@@ -641,6 +641,7 @@ __global__ void __launch_bounds__(kCorrThreads, 2) k_corr(const CorrArgs A) {
 // the largest estimate, and the patch, get the reference's exact FP64 normalisation.
 
 constexpr int kTcThreads = 256;
+constexpr int kTc2Issuers = 3;  // k_corr_tc2: threads issuing a point's products
 constexpr int kPadL = 32;            // zero bytes before each staged chip column
 constexpr uint32_t kTcWaitPolls = 1u << 22;
 
@@ -658,7 +659,8 @@ struct TcArgs {
     int big;                         // 1: box sums before the products, chunks reuse their space
     unsigned off_E, off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
     int XV;                          // k_corr_tc2: row stride (words) of the column sums V1, V2
-    int acc1_col;                    // k_corr_tc2: first column of its second accumulator
+    int acc1_col;                    // first column of the second accumulator (k_corr_tc2: the
+                                     // stride between its accumulators)
     uint32_t tmem_cols;
     DevOutputs out;
     int* sub_count;
@@ -1603,14 +1605,14 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
         tc::tmem_relinquish();
     }
     if (tid == 0) {
-        tc::mbar_init(&s_mbar, 2);  // one commit per issuing thread
+        tc::mbar_init(&s_mbar, kTc2Issuers);  // one commit per issuing thread
         tc::fence_mbar_init();
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t taddr = s_taddr;
-    const uint32_t acc1 = static_cast<uint32_t>(A.acc1_col);  // second accumulator's first column
+    const uint32_t acc1 = static_cast<uint32_t>(A.acc1_col);  // stride between accumulators
     uint32_t phase = 0;
     bool failed = false;
     if (tid < 4) s_isum[tid >> 1][tid & 1] = 0ull;
@@ -1774,27 +1776,29 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
                 }
             }
         }
-        const int dcols = 16 * (Q - 1) + A.NB;
+        // The products add into accumulator columns [0, round16(nr)): surface row i is column i.
+        const int dcols = (nr + 15) & ~15;
         if (warp < 4) {
             // Clear the columns the products add into (one lane quarter per warp).
             uint32_t z[16];
 #pragma unroll
             for (int t = 0; t < 16; ++t) z[t] = 0u;
             const uint32_t lq = taddr + (static_cast<uint32_t>(32 * warp) << 16);
-            for (int c = 0; c < dcols; c += 16) {
-                tc::tmem_st16(lq + static_cast<uint32_t>(c), z);
-                tc::tmem_st16(lq + acc1 + static_cast<uint32_t>(c), z);
-            }
+            for (int c = 0; c < dcols; c += 16)
+#pragma unroll
+                for (int t = 0; t < kTc2Issuers; ++t)
+                    tc::tmem_st16(lq + static_cast<uint32_t>(t) * acc1 + static_cast<uint32_t>(c), z);
             tc::tmem_wait_st();
         }
         tc::fence_proxy_async_smem();
         tc::fence_before_sync();
         __syncthreads();  // s_P, s_W, s_E complete; accumulator cleared
         TC_PHASE(4)
-        // Two threads issue the products, each for half of the chip column pairs into its own
-        // accumulator: the MMAs of one thread run one after another, two threads' interleave.
-        if (tid == kTcThreads - 32 || tid == kTcThreads - 64) {
-            const int stream = tid == kTcThreads - 32 ? 0 : 1;
+        // Lane 0 of the last kTc2Issuers warps issue the products, each for a share of the chip
+        // column pairs into its own accumulator (one thread issues an MMA about every 120
+        // cycles; several issuers interleave theirs).
+        if (lane == 0 && warp >= nwarps - kTc2Issuers) {
+            const int stream = nwarps - 1 - warp;
             tc::fence_after_sync();
 #ifdef AR_TC_PHASES
             const unsigned long long tmi0 = clock64();
@@ -1807,9 +1811,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
             const uint32_t a_hi = static_cast<uint32_t>(da0 >> 32);
             const uint32_t b_hi = static_cast<uint32_t>(db0 >> 32);
             const uint32_t bstep = static_cast<uint32_t>(2 * A.PS) >> 4;
-            const int half_pairs = (cw / 2) / 2;
-            const int t_begin = stream == 0 ? 0 : half_pairs;
-            const int npairs = stream == 0 ? half_pairs : cw / 2 - half_pairs;
+            const int pairs = cw / 2;
+            const int t_begin = pairs * stream / kTc2Issuers;
+            const int npairs = pairs * (stream + 1) / kTc2Issuers - t_begin;
             for (int q = 0; q < Q; ++q) {
                 // Only the operand rows e in [elo, elo + n) of block q reach surface rows.
                 int elo, n;
@@ -1819,7 +1823,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
                                 static_cast<uint32_t>(q * A.QS >> 4) + 2u * static_cast<uint32_t>(t_begin);
                 uint32_t b_lo = static_cast<uint32_t>(db0) + static_cast<uint32_t>(elo) +
                                 bstep * static_cast<uint32_t>(t_begin);
-                const uint32_t dn = taddr + (stream ? acc1 : 0u) + static_cast<uint32_t>(16 * q + elo);
+                const uint32_t dn = taddr + static_cast<uint32_t>(stream) * acc1 +
+                                    static_cast<uint32_t>(16 * q + elo - (A.NB - 16));
                 int t = 0;
                 for (; t + 4 <= npairs; t += 4) {
                     tc::mma_u8_halves(dn, a_lo, a_hi, b_lo, b_hi, idesc);
@@ -1851,9 +1856,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
         }
         TC_PHASE(5)
         // S[j][i] = sums of V[i][j .. j + cw - 1] for rows i in [i_lo, i_lo + ni): a task is a
-        // row i and 16 columns j (warps 0-5).
+        // row i and 16 columns j (the warps that do not issue products).
         auto box_rows = [&](int i_lo, int ni) {
-            constexpr int kBT = kTcThreads - 64;
+            constexpr int kBT = kTcThreads - 32 * kTc2Issuers;
             const int jseg = (nc + 15) >> 4;
             const bool vec = (cw & 3) == 0;
             for (int task = tid; task < ni * jseg; task += kBT) {
@@ -1919,8 +1924,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
 #ifdef AR_TC_PHASES
         if (tid == 0 && carry) atomicAdd(&g_tc_phase[14], 1ull);
 #endif
-        if (warp < 6) {
-            constexpr int kBT = kTcThreads - 64;
+        if (warp < nwarps - kTc2Issuers) {
+            constexpr int kBT = kTcThreads - 32 * kTc2Issuers;
             if (carry) {
                 const int sh = static_cast<int>(sh64);
                 // Column sums of the new rows i in [nr - sh, nr): an item is a window column and
@@ -2103,7 +2108,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
         const float nnf = static_cast<float>(nnl);
         const float csf = static_cast<float>(csum_d);
         const int quarter = warp & 3, half = warp >> 2;
-        const uint32_t col0 = static_cast<uint32_t>(A.NB - 16);
+        const uint32_t col0 = 0u;  // surface row i is accumulator column i
         const int ib0 = 32 * half + 2 * (lane & 3);
         const int jb0 = 16 * quarter + (lane >> 2);
         uint32_t dv[16];
@@ -2113,12 +2118,15 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
         if (32 * half < nr) {
             const uint32_t base = taddr + (static_cast<uint32_t>(32 * quarter) << 16) + col0 +
                                   static_cast<uint32_t>(32 * half);
-            uint32_t dv1[16];
+            uint32_t dv1[kTc2Issuers - 1][16];
             tc::tmem_ld16dp(base, dv);
-            tc::tmem_ld16dp(base + acc1, dv1);
+#pragma unroll
+            for (int t = 1; t < kTc2Issuers; ++t) tc::tmem_ld16dp(base + static_cast<uint32_t>(t) * acc1, dv1[t - 1]);
             tc::tmem_wait_ld();
 #pragma unroll
-            for (int v = 0; v < 16; ++v) dv[v] += dv1[v];  // the two halves of the chip columns
+            for (int t = 1; t < kTc2Issuers; ++t)
+#pragma unroll
+                for (int v = 0; v < 16; ++v) dv[v] += dv1[t - 1][v];  // the issuers' shares
             // Values v and v + 1 are surface rows i and i + 1 of one column: estimated as a pair.
 #pragma unroll
             for (int v = 0; v < 16; v += 2) {
@@ -3495,13 +3503,13 @@ bool plan_corr_tc2(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
     P->PC = round_up(kPadL + P->NB + 20, 16);
     P->NRS = nr | 1;
     P->XV = round_up(cw + nc - 1, 32) + 4;
-    const int dcols = 16 * (P->QM - 1) + P->NB;
-    const int reads = P->NB - 16 + 32 * ((nr + 31) / 32);  // columns the epilogue reads
+    // kTc2Issuers accumulators whose column i is surface row i (the products write columns below
+    // round16(nr), the epilogue reads 32 columns per half of the surface rows).
+    const int stride = nr > 32 ? 64 : 32;
     uint32_t t1 = 32;
-    while (static_cast<int>(t1) < std::max(dcols, reads)) t1 <<= 1;
-    if (2 * t1 > 512) return false;
-    P->acc1_col = static_cast<int>(t1);  // two accumulators of t1 columns
-    P->tmem_cols = 2 * t1;
+    while (static_cast<int>(t1) < kTc2Issuers * stride) t1 <<= 1;
+    P->acc1_col = stride;
+    P->tmem_cols = t1;
     auto a16 = [](size_t v) { return (v + 15) & ~size_t(15); };
     const size_t Eb = static_cast<size_t>(cw) * P->PS;
     const size_t Wb = static_cast<size_t>(P->QM) * P->QS;
