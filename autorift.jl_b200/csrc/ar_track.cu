@@ -2543,6 +2543,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                 }
             }
             __syncthreads();
+            TC_PHASE(3)
             {
                 const int segs = max(1, min(nr, bd / xn));
                 const int len = (nr + segs - 1) / segs;
@@ -2569,6 +2570,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                 }
             }
             __syncthreads();
+            TC_PHASE(4)
             if (tid < 2 * nr) {
                 const int i = tid >> 1, comp = tid & 1;
                 double* S = comp ? s_S2 : s_S1;
@@ -2581,8 +2583,9 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                 }
             }
             __syncthreads();
+            TC_PHASE(5)
         }
-        TC_PHASE(3)
+        TC_PHASE(5)
         // FP64 denominators (src/correlate.jl:591-600, 624-628).
         for (int e = tid; e < nr * nc; e += bd) {
             const int i = e % nr, j = e / nr;
@@ -2600,7 +2603,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
         clear_set(0);
         clear_set(1);
         __syncthreads();  // S1 and S2 read before the window limbs replace them
-        TC_PHASE(4)
+        TC_PHASE(6)
 
         double accd[16];
 #pragma unroll
@@ -2696,7 +2699,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                 p_store(0, min(A.BC, obn), pr);
             }
             __syncthreads();  // limbs and the first chunk's chip columns complete
-            TC_PHASE(5)
+            TC_PHASE(7)
 
             const int nch = (obn + A.BC - 1) / A.BC;
             for (int c = 0; c < nch; ++c) {
@@ -2768,7 +2771,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                     }
                     tc::mma_commit(&s_mbar[s]);
                 }
-                TC_PHASE(7)
+                TC_PHASE(9)
                 pend[s] = true;
                 // The next chunk's chip columns: loads now, conversion after the flush.
                 const bool more = c + 1 < nch;
@@ -2787,7 +2790,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                 if (more) p_store(s ^ 1, bnext, pr);
                 tc::fence_before_sync();
                 __syncthreads();
-                TC_PHASE(6)
+                TC_PHASE(8)
             }
             if (ok) {
                 const int sl = (nch - 1) & 1;
@@ -2827,7 +2830,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
             }
         }
         __syncthreads();
-        TC_PHASE(9)
+        TC_PHASE(10)
         if (A.flops && tid == 0)
             atomicAdd(A.flops, 2ull * static_cast<unsigned long long>(ch) * cw * nr * nc);
         // Integer peak (src/peak.jl:32-61).
@@ -2871,7 +2874,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                 A.sub_origin[2 * slot + 1] = pj0;
             }
         }
-        TC_PHASE(10)
+        TC_PHASE(11)
         TC_PHASE_POINT
     }
     TC_PHASE_FLUSH
