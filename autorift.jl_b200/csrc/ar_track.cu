@@ -2408,16 +2408,20 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
     const int quarter = warp & 3, half = warp >> 2;
     const uint32_t qbase = taddr + (static_cast<uint32_t>(32 * quarter) << 16) +
                            static_cast<uint32_t>(32 * half);
-    auto clear_set = [&](int s) {
-        if (warp < 4) {
-            uint32_t z[16];
+    // Zeros into this warp's lane quarter and half of the columns of set s's accumulators
+    // (columns [32 half, 32 half + 32) of each, as far as the accumulator reaches): the warps
+    // of the two halves together clear the set, each after reading its own values.
+    auto clear_half = [&](int s) {
+        uint32_t z[16];
 #pragma unroll
-            for (int t = 0; t < 16; ++t) z[t] = 0u;
-            const uint32_t lq = taddr + (static_cast<uint32_t>(32 * warp) << 16);
-            for (int c = kBfIssuers * s * A.AC; c < kBfIssuers * (s + 1) * A.AC; c += 16)
-                tc::tmem_st16(lq + static_cast<uint32_t>(c), z);
-            tc::tmem_wait_st();
+        for (int t = 0; t < 16; ++t) z[t] = 0u;
+        const int c1 = min(32 * (half + 1), A.AC);
+        for (int t = 0; t < kBfIssuers; ++t) {
+            const uint32_t a0 = qbase - static_cast<uint32_t>(32 * half) +
+                                static_cast<uint32_t>((kBfIssuers * s + t) * A.AC);
+            for (int c = 32 * half; c < c1; c += 16) tc::tmem_st16(a0 + static_cast<uint32_t>(c), z);
         }
+        tc::tmem_wait_st();
     };
     // Bounded wait for set s's products; on success the set is no longer pending.
     auto wait_set = [&](int s) -> bool {
@@ -2600,8 +2604,8 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
             }
             s_den[j * A.NRS + i] = den;
         }
-        clear_set(0);
-        clear_set(1);
+        clear_half(0);
+        clear_half(1);
         __syncthreads();  // S1 and S2 read before the window limbs replace them
         TC_PHASE(6)
 
@@ -2624,20 +2628,20 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
         };
         // A chunk's chip columns C'[a, b0 + bl] as BF16 limbs, zero-padded: the loads first
         // (into registers), the conversion after other work.
-        auto p_load = [&](int b0, int bcn, double (&pr)[kBfPre]) {
+        auto p_load = [&](int b0, int bcn, double (&pr)[kBfPre], int t0, int nt) {
 #pragma unroll
             for (int u = 0; u < kBfPre; ++u) {
-                const int e = tid + u * bd;
+                const int e = (tid - t0) + u * nt;
                 const int bl = e / A.PC, a = e - bl * A.PC - kBfPadL;
                 pr[u] = (e < plimb && bl < bcn && a >= 0 && a < ch)
                             ? pixel(sec, A.nrows, A.ncols, chip_r + a, chip_c + b0 + bl) : 0.0;
             }
         };
-        auto p_store = [&](int buf, int bcn, const double (&pr)[kBfPre]) {
+        auto p_store = [&](int buf, int bcn, const double (&pr)[kBfPre], int t0, int nt) {
             uint16_t* P = reinterpret_cast<uint16_t*>(s_Pb + buf * A.Pb);
 #pragma unroll
             for (int u = 0; u < kBfPre; ++u) {
-                const int e = tid + u * bd;
+                const int e = (tid - t0) + u * nt;
                 if (e < plimb) {
                     const int bl = e / A.PC, a = e - bl * A.PC - kBfPadL;
                     uint32_t l[kBfLimbs] = {0u, 0u, 0u};
@@ -2693,106 +2697,141 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                     }
                 }
             }
+            // Chip operand rows for the chunk in buffer `buf` (threads [t0, t0 + nt)):
+            // E_b[h][e] = 8 elements of the staged column from element kBfPadL + 8 h - e + NB - 16
+            // (C'[r - u, b] with u = e - NB + 16, r = 8 h + t).
+            auto build_E = [&](int buf, int t0, int nt) {
+                const uint16_t* P = reinterpret_cast<const uint16_t*>(s_Pb + buf * A.Pb);
+                unsigned char* E = s_E + buf * A.Eb;
+                for (int it = tid - t0; it < A.BC * 2 * A.NB; it += nt) {
+                    const int bl = it / (2 * A.NB), rem = it - bl * 2 * A.NB;
+                    const int h = rem / A.NB, e = rem - h * A.NB;
+                    const int src = kBfPadL + 8 * h - e + A.NB - 16;  // element index, >= 1
+                    const size_t o = (static_cast<size_t>(bl * 2 + h) * A.NB + e) * 16;
+#pragma unroll
+                    for (int limb = 0; limb < kBfLimbs; ++limb) {
+                        const uint16_t* col = P + limb * plimb + bl * A.PC;
+                        const uint32_t* w = reinterpret_cast<const uint32_t*>(col + (src & ~1));
+                        const uint32_t sh = (src & 1) ? 16u : 0u;
+                        uint4 v;
+                        v.x = __funnelshift_r(w[0], w[1], sh);
+                        v.y = __funnelshift_r(w[1], w[2], sh);
+                        v.z = __funnelshift_r(w[2], w[3], sh);
+                        v.w = __funnelshift_r(w[3], w[4], sh);
+                        *reinterpret_cast<uint4*>(E + limb * elimb + o) = v;
+                    }
+                }
+            };
+            const int nch = (obn + A.BC - 1) / A.BC;
+            auto chunk_b0 = [&](int c) { return ob0 + c * A.BC; };
+            auto chunk_n = [&](int c) { return min(A.BC, ob0 + obn - chunk_b0(c)); };
+            // Chunk 0's chip columns and operand, chunk 1's chip columns, by every thread.
             {
                 double pr[kBfPre];
-                p_load(ob0, min(A.BC, obn), pr);
-                p_store(0, min(A.BC, obn), pr);
+                p_load(chunk_b0(0), chunk_n(0), pr, 0, bd);
+                p_store(0, chunk_n(0), pr, 0, bd);
+                __syncthreads();
+                build_E(0, 0, bd);
+                if (nch > 1) {
+                    p_load(chunk_b0(1), chunk_n(1), pr, 0, bd);
+                    p_store(1, chunk_n(1), pr, 0, bd);
+                }
             }
-            __syncthreads();  // limbs and the first chunk's chip columns complete
+            tc::fence_proxy_async_smem();
+            tc::fence_before_sync();
+            __syncthreads();  // limbs, chunk 0's operand and chunk 1's chip columns complete
             TC_PHASE(7)
 
-            const int nch = (obn + A.BC - 1) / A.BC;
-            for (int c = 0; c < nch; ++c) {
+            // Chunk c: lane 0 of warps 0-3 issue its products into set c & 1 while warps 4-7 take
+            // chunk c - 1's values out of set c & 1 ^ 1 (their half of the columns), build chunk
+            // c + 1's operand into the buffer chunk c - 1 used and stage chunk c + 2's chip
+            // columns; warps 0-3 then take their half of chunk c - 1's values. One barrier per
+            // chunk: set c & 1 ^ 1 is clear and chunk c + 1's operand complete after it.
+            for (int c = 0; c < nch && ok; ++c) {
                 const int s = c & 1;
-                const int b0 = ob0 + c * A.BC, bcn = min(A.BC, ob0 + obn - b0);
-                // Chip operand rows: E_b[h][e] = 8 elements of the staged column from element
-                // kBfPadL + 8 h - e + NB - 16 (C'[r - u, b] with u = e - NB + 16, r = 8 h + t).
-                {
-                    const uint16_t* P = reinterpret_cast<const uint16_t*>(s_Pb + s * A.Pb);
-                    unsigned char* E = s_E + s * A.Eb;
-                    for (int it = tid; it < A.BC * 2 * A.NB; it += bd) {
-                        const int bl = it / (2 * A.NB), rem = it - bl * 2 * A.NB;
-                        const int h = rem / A.NB, e = rem - h * A.NB;
-                        const int src = kBfPadL + 8 * h - e + A.NB - 16;  // element index, >= 1
-                        const size_t o = (static_cast<size_t>(bl * 2 + h) * A.NB + e) * 16;
-#pragma unroll
-                        for (int limb = 0; limb < kBfLimbs; ++limb) {
-                            const uint16_t* col = P + limb * plimb + bl * A.PC;
-                            const uint32_t* w = reinterpret_cast<const uint32_t*>(col + (src & ~1));
-                            const uint32_t sh = (src & 1) ? 16u : 0u;
-                            uint4 v;
-                            v.x = __funnelshift_r(w[0], w[1], sh);
-                            v.y = __funnelshift_r(w[1], w[2], sh);
-                            v.z = __funnelshift_r(w[2], w[3], sh);
-                            v.w = __funnelshift_r(w[3], w[4], sh);
-                            *reinterpret_cast<uint4*>(E + limb * elimb + o) = v;
-                        }
-                    }
-                }
-                tc::fence_proxy_async_smem();
-                tc::fence_before_sync();
-                __syncthreads();  // operands complete; accumulator set s clear
-                // Lane 0 of warps 0-3 issue the chunk's products, each into an accumulator of
-                // its own (one thread issues a product about every 120 cycles; four keep the
-                // tensor core busy): issuer t takes the window blocks q of parity t & 1 and the
-                // limb pairs (chip, window) (0,0), (1,1), (2,0) when t < 2, else (0,1), (1,0),
-                // (0,2) (integer windows have no third limb).
-                if (lane == 0 && warp < kBfIssuers) {
-                    tc::fence_after_sync();
-                    const uint32_t wb = tc::smem_u32(s_W);
-                    const uint32_t eb = tc::smem_u32(s_E) + static_cast<uint32_t>(s * A.Eb);
-                    const int par = warp & 1;
-                    const uint32_t dacc = taddr + static_cast<uint32_t>((kBfIssuers * s + warp) * A.AC);
+                const int b0 = chunk_b0(c), bcn = chunk_n(c);
+                bool okc = true;
+                if (warp < kBfIssuers) {
+                    // Lane 0 of warps 0-3 issue the chunk's products, each into an accumulator of
+                    // its own (one thread issues a product about every 120 cycles; four keep the
+                    // tensor core busy): issuer t takes the window blocks q of parity t & 1 and
+                    // the limb pairs (chip, window) (0,0), (1,1), (2,0) when t < 2, else (0,1),
+                    // (1,0), (0,2) (integer windows have no third limb).
+                    if (lane == 0) {
+                        tc::fence_after_sync();
+                        const uint32_t wb = tc::smem_u32(s_W);
+                        const uint32_t eb = tc::smem_u32(s_E) + static_cast<uint32_t>(s * A.Eb);
+                        const int par = warp & 1;
+                        const uint32_t dacc = taddr + static_cast<uint32_t>((kBfIssuers * s + warp) * A.AC);
 #pragma unroll 1
-                    for (int pp = 0; pp < 3; ++pp) {
-                        const int cl = warp < 2 ? pp : (pp == 1 ? 1 : 0);
-                        const int wl = warp < 2 ? (pp == 1 ? 1 : 0) : (pp == 0 ? 1 : pp == 2 ? 2 : 0);
-                        if (Tr::integer && wl == 2) continue;
-                        const uint64_t da0 = tc::smem_desc(wb + static_cast<uint32_t>(wl * wlimb),
-                                                           static_cast<uint32_t>(A.LW * 16), 128);
-                        const uint64_t db0 = tc::smem_desc(eb + static_cast<uint32_t>(cl * elimb),
-                                                           static_cast<uint32_t>(A.NB * 16), 128);
-                        const uint32_t a_hi = static_cast<uint32_t>(da0 >> 32);
-                        const uint32_t b_hi = static_cast<uint32_t>(db0 >> 32);
-                        for (int q = par; q < QBp; q += 2) {
-                            int elo, n;
-                            if (!block_rows(q, A.NB, nr, &elo, &n)) continue;
-                            const uint32_t idesc = tc::idesc_bf16_f32(64, n);
-                            const uint32_t dcol = static_cast<uint32_t>(16 * q + elo - (A.NB - 16));
-                            for (int bl = 0; bl < bcn; ++bl) {
-                                // A: block q, first half, window column x = b0 - ob0 + bl.
-                                const uint32_t a_lo = static_cast<uint32_t>(da0) +
-                                                      static_cast<uint32_t>((q * 2) * A.LW + (b0 - ob0) + bl);
-                                const uint32_t b_lo = static_cast<uint32_t>(db0) +
-                                                      static_cast<uint32_t>((bl * 2) * A.NB + elo);
-                                tc::mma_bf16_halves(dacc + dcol, a_lo, a_hi, b_lo, b_hi, idesc, 1u);
+                        for (int pp = 0; pp < 3; ++pp) {
+                            const int cl = warp < 2 ? pp : (pp == 1 ? 1 : 0);
+                            const int wl = warp < 2 ? (pp == 1 ? 1 : 0) : (pp == 0 ? 1 : pp == 2 ? 2 : 0);
+                            if (Tr::integer && wl == 2) continue;
+                            const uint64_t da0 = tc::smem_desc(wb + static_cast<uint32_t>(wl * wlimb),
+                                                               static_cast<uint32_t>(A.LW * 16), 128);
+                            const uint64_t db0 = tc::smem_desc(eb + static_cast<uint32_t>(cl * elimb),
+                                                               static_cast<uint32_t>(A.NB * 16), 128);
+                            const uint32_t a_hi = static_cast<uint32_t>(da0 >> 32);
+                            const uint32_t b_hi = static_cast<uint32_t>(db0 >> 32);
+                            for (int q = par; q < QBp; q += 2) {
+                                int elo, n;
+                                if (!block_rows(q, A.NB, nr, &elo, &n)) continue;
+                                const uint32_t idesc = tc::idesc_bf16_f32(64, n);
+                                const uint32_t dcol = static_cast<uint32_t>(16 * q + elo - (A.NB - 16));
+                                for (int bl = 0; bl < bcn; ++bl) {
+                                    // A: block q, first half, window column x = b0 - ob0 + bl.
+                                    const uint32_t a_lo = static_cast<uint32_t>(da0) +
+                                                          static_cast<uint32_t>((q * 2) * A.LW + (b0 - ob0) + bl);
+                                    const uint32_t b_lo = static_cast<uint32_t>(db0) +
+                                                          static_cast<uint32_t>((bl * 2) * A.NB + elo);
+                                    tc::mma_bf16_halves(dacc + dcol, a_lo, a_hi, b_lo, b_hi, idesc, 1u);
+                                }
                             }
                         }
+                        tc::mma_commit(&s_mbar[s]);
                     }
-                    tc::mma_commit(&s_mbar[s]);
+                    __syncwarp();
+                    TC_PHASE(9)
+                    if (c >= 1) {
+                        okc = tc::mbar_wait(&s_mbar[s ^ 1], ph[s ^ 1], kTcWaitPolls);
+                        if (okc) {
+                            tc::fence_after_sync();
+                            flush_set(s ^ 1);
+                            clear_half(s ^ 1);
+                        }
+                    }
+                } else {
+                    if (c >= 1) {
+                        okc = tc::mbar_wait(&s_mbar[s ^ 1], ph[s ^ 1], kTcWaitPolls);
+                        if (okc) {
+                            tc::fence_after_sync();
+                            flush_set(s ^ 1);
+                            clear_half(s ^ 1);
+                        }
+                    }
+                    if (okc && c + 1 < nch) build_E(s ^ 1, 32 * kBfIssuers, bd - 32 * kBfIssuers);
+                    if (okc && c + 2 < nch) {
+                        double pr[kBfPre];
+                        p_load(chunk_b0(c + 2), chunk_n(c + 2), pr, 32 * kBfIssuers, bd - 32 * kBfIssuers);
+                        p_store(s, chunk_n(c + 2), pr, 32 * kBfIssuers, bd - 32 * kBfIssuers);
+                    }
                 }
-                TC_PHASE(9)
                 pend[s] = true;
-                // The next chunk's chip columns: loads now, conversion after the flush.
-                const bool more = c + 1 < nch;
-                const int bnext = min(A.BC, ob0 + obn - (b0 + A.BC));
-                double pr[kBfPre];
-                if (more) p_load(b0 + A.BC, bnext, pr);
-                if (c >= 1) {
-                    // The previous chunk's products: done (its chip operand buffer is free), its
-                    // accumulators added into the FP64 sums and cleared.
-                    ok = wait_set(s ^ 1);
-                    if (__syncthreads_or(!ok)) { ok = false; break; }
-                    tc::fence_after_sync();
-                    flush_set(s ^ 1);
-                    clear_set(s ^ 1);
-                }
-                if (more) p_store(s ^ 1, bnext, pr);
+                tc::fence_proxy_async_smem();
                 tc::fence_before_sync();
-                __syncthreads();
+                if (__syncthreads_or(!okc)) {
+                    ok = false;
+                    break;
+                }
+                if (c >= 1) {
+                    ph[s ^ 1] ^= 1u;
+                    pend[s ^ 1] = false;
+                }
                 TC_PHASE(8)
             }
             if (ok) {
+                // The last chunk's values; each warp clears its half of the set.
                 const int sl = (nch - 1) & 1;
                 ok = wait_set(sl);
                 if (__syncthreads_or(!ok)) {
@@ -2800,7 +2839,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                 } else {
                     tc::fence_after_sync();
                     flush_set(sl);
-                    clear_set(sl);
+                    clear_half(sl);
                     tc::fence_before_sync();
                     __syncthreads();  // the window limbs are replaced next
                 }
@@ -3576,8 +3615,10 @@ bool plan_corr_bf(const PassGeometry& g, size_t smem_cap, BfPlan* P) {
     const int blocks = (ch + 15) / 16 + 1;
     int bc = std::max(1, 2 * kBfChain / (3 * blocks));
     bc = std::min(bc, cw);
-    while (bc > 1 && bc * P->PC > kBfPre * kBfThreads) --bc;
-    if (bc * P->PC > kBfPre * kBfThreads) return false;
+    // The staged chip columns of a chunk: kBfPre elements per thread of warps 4-7.
+    const int stagers = kBfThreads - 32 * kBfIssuers;
+    while (bc > 1 && bc * P->PC > kBfPre * stagers) --bc;
+    if (bc * P->PC > kBfPre * stagers) return false;
     P->BC = bc;
     auto a16 = [](size_t v) { return (v + 15) & ~size_t(15); };
     const size_t Sb = a16(static_cast<size_t>(nc) * P->NRS * 8);
