@@ -25,7 +25,10 @@ namespace {
 // single-threaded copy, not the DMA, set the pace of uploads. A copy is cut into pieces that
 // the calling thread and the workers claim from one counter; the counter carries the copy's
 // generation in its upper half, so a worker that wakes late can never claim a piece of a
-// later copy with an earlier copy's pointers.
+// later copy with an earlier copy's pointers. One pool serves every context of the process and
+// runs one copy at a time: the host's memory bandwidth is the shared resource, and the serving
+// slots' contexts copying at once with a pool each oversubscribed the cores (three slots ran
+// slower than one pair at a time).
 class CopyPool {
 public:
     explicit CopyPool(int workers) {
@@ -39,14 +42,15 @@ public:
         cv_job_.notify_all();
         for (auto& t : threads_) t.join();
     }
-    // memcpy(dst, src, bytes), shared with the workers when it is large. One copy at a time
-    // (the owning context's lock serialises its callers).
+    // memcpy(dst, src, bytes), shared with the workers when it is large; callers from several
+    // contexts take turns.
     void copy(void* dst, const void* src, size_t bytes) {
         constexpr size_t kMinSplit = 512u << 10, kPieceAlign = 64u << 10;
         if (threads_.empty() || bytes < kMinSplit) {
             std::memcpy(dst, src, bytes);
             return;
         }
+        std::lock_guard<std::mutex> turn(turn_mu_);
         const size_t ways = threads_.size() + 1;
         Job j;
         j.dst = static_cast<unsigned char*>(dst);
@@ -105,6 +109,7 @@ private:
         }
     }
     std::vector<std::thread> threads_;
+    std::mutex turn_mu_;  // one copy at a time
     std::mutex mu_;
     std::condition_variable cv_job_, cv_done_;
     Job job_;
@@ -116,6 +121,20 @@ private:
 int copy_workers() {
     const unsigned hw = std::thread::hardware_concurrency();
     return static_cast<int>(std::min(15u, hw > 1 ? hw - 1 : 0u));
+}
+
+// The process's copy pool, created by the first context that stages a copy and released with
+// the last one.
+std::shared_ptr<CopyPool> shared_copy_pool() {
+    static std::mutex m;
+    static std::weak_ptr<CopyPool> pool;
+    std::lock_guard<std::mutex> lk(m);
+    std::shared_ptr<CopyPool> p = pool.lock();
+    if (!p) {
+        p = std::make_shared<CopyPool>(copy_workers());
+        pool = p;
+    }
+    return p;
 }
 
 }  // namespace
@@ -131,7 +150,7 @@ struct ar_ctx {
     unsigned char* pinned = nullptr;
     size_t pinned_bytes = 0;
     cudaEvent_t staged[2] = {nullptr, nullptr};
-    std::unique_ptr<CopyPool> copier;  // host threads for the staging copies
+    std::shared_ptr<CopyPool> copier;  // the process's host threads for the staging copies
     // Device buffers for host point sets and outputs, grown on demand.
     void* dbuf = nullptr;
     size_t dbuf_bytes = 0;
@@ -205,7 +224,7 @@ cudaError_t ensure_pinned(ar_ctx* c) {
     cudaError_t e = cudaMallocHost(&c->pinned, kStageBytes);
     if (e != cudaSuccess) return e;
     c->pinned_bytes = kStageBytes;
-    c->copier.reset(new CopyPool(copy_workers()));
+    c->copier = shared_copy_pool();
     for (auto& ev : c->staged) {
         e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
         if (e != cudaSuccess) return e;
