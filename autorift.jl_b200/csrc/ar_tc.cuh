@@ -206,6 +206,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
+// 16 bytes global -> shared without registers (cp.async, L2 only); both addresses 16-byte
+// aligned. Completion: cp_async_commit() then cp_async_wait_all() by the issuing thread.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gmem_src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
 // Bounded wait for phase `parity` of `mbar` to complete: false after `limit` polls.
 __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint32_t limit) {
     for (uint32_t k = 0; k < limit; ++k)

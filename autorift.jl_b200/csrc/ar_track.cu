@@ -1642,6 +1642,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
     };
     int h_ch = 0, h_cw = 0, h_nr = 0, h_nc = 0;
     for (int64_t k = kbeg; k < kend; ++k, ++iter) {
+        tc::cp_async_wait_all();  // no copy of a skipped point is still landing
         tc::fence_before_sync();
         __syncthreads();  // the previous point's buffers and accumulators are no longer read
         tc::fence_after_sync();
@@ -1661,6 +1662,34 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
         const int64_t chip_r = g.chip_r, chip_c = g.chip_c, win_r = g.win_r, win_c = g.win_c;
         const long long nnl = static_cast<long long>(ch) * cw;
         const bool pow2 = (nnl & (nnl - 1)) == 0 && nnl <= 4096;
+
+        // The window's columns as aligned 16-byte chunks, copied asynchronously (cp.async) into
+        // the column-sum buffer -- free until the box sums -- while the chip is staged: when
+        // every row of the window lies in the image, a column takes the Q + 1 chunks from the
+        // aligned address at or below its first row (columns whose chunks would leave the array,
+        // and windows that reach outside the image's rows, are staged from global memory below).
+        const int Q = (ch + nr - 1 + 15) / 16;
+        const int RQ = Q + 1;
+        uint8_t* s_Wraw = reinterpret_cast<uint8_t*>(s_V1);
+        const bool rows_in = win_r >= 0 && win_r + 16 * Q <= A.nrows;
+        auto raw_col = [&](int x, const uint8_t** first) {
+            // Column x's aligned first chunk when all its chunks are inside the array, else null.
+            const int64_t c = win_c + x;
+            if (!rows_in || c < 0 || c >= A.ncols) return false;
+            const uint8_t* p = A.ref + c * A.nrows + win_r;
+            const uint8_t* a0 = reinterpret_cast<const uint8_t*>(reinterpret_cast<uintptr_t>(p) & ~uintptr_t(15));
+            if (a0 < A.ref || a0 + 16 * RQ > ref_end) return false;
+            *first = a0;
+            return true;
+        };
+        if (rows_in) {
+            for (int it = tid; it < A.XS * RQ; it += bd) {
+                const int x = it / RQ, kq = it - x * RQ;
+                const uint8_t* a0;
+                if (raw_col(x, &a0)) tc::cp_async16(s_Wraw + static_cast<size_t>(it) * 16, a0 + 16 * kq);
+            }
+        }
+        tc::cp_async_commit();
 
         // The chip as zero-padded byte columns, _any_valid over it (src/track.jl:416-421) and,
         // for power-of-two areas, its exact integer sums (as in k_corr_tc).
@@ -1708,6 +1737,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
                 atomicAdd(&s_isum[ib][1], isq);
             }
         }
+        tc::cp_async_wait_all();  // this thread's window chunks have landed (visible after the barrier)
         if (!__syncthreads_or(any)) continue;
         TC_PHASE(2)
         if (tid == 0) A.out.searched[k] = 1;
@@ -1746,13 +1776,23 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
         if (tid == 0 && !(A.up == 1 || nr < 5 || nc < 5)) s_slot = atomicAdd(A.sub_count, 1);
         const double nn = static_cast<double>(nnl);
 
-        // Window blocks W[16 q + r][x] (x < XS) from the window's first row.
-        const int Q = (ch + nr - 1 + 15) / 16;
+        // Window blocks W[16 q + r][x] (x < XS) from the window's first row: from the chunks in
+        // shared memory, or from global memory for the columns that have none.
         const int XW = cw + nc - 1;
         for (int q = warp; q < Q; q += nwarps)
-            for (int x = lane; x < A.XS; x += 32)
-                *reinterpret_cast<uint4*>(s_W + q * A.QS + x * 16) = col16_finish(
-                    col16_issue(A.ref, ref_end, A.nrows, A.ncols, win_c + x, win_r + 16 * q));
+            for (int x = lane; x < A.XS; x += 32) {
+                const uint8_t* a0;
+                Col16 L;
+                if (raw_col(x, &a0)) {
+                    const uint4* rc = reinterpret_cast<const uint4*>(s_Wraw + static_cast<size_t>(x * RQ + q) * 16);
+                    L.lo = rc[0];
+                    L.hi = rc[1];
+                    L.s = static_cast<uint32_t>(reinterpret_cast<uintptr_t>(A.ref + (win_c + x) * A.nrows + win_r) & 15);
+                } else {
+                    L = col16_issue(A.ref, ref_end, A.nrows, A.ncols, win_c + x, win_r + 16 * q);
+                }
+                *reinterpret_cast<uint4*>(s_W + q * A.QS + x * 16) = col16_finish(L);
+            }
         // E: NB rows per chip column, row e (u = e - NB + 16) = 16 bytes from chip row -u.
         {
             const int nrow = cw * A.NB;
@@ -2802,6 +2842,11 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                         }
                     }
                 } else {
+                    // Chunk c + 2's chip columns are loaded first and converted last, so the
+                    // loads are in flight through the wait, the flush and the operand build.
+                    const bool stage = c + 2 < nch;
+                    double pr[kBfPre];
+                    if (stage) p_load(chunk_b0(c + 2), chunk_n(c + 2), pr, 32 * kBfIssuers, bd - 32 * kBfIssuers);
                     if (c >= 1) {
                         okc = tc::mbar_wait(&s_mbar[s ^ 1], ph[s ^ 1], kTcWaitPolls);
                         if (okc) {
@@ -2811,11 +2856,7 @@ __global__ void __launch_bounds__(kBfThreads, 1) k_corr_bf(const BfArgs A) {
                         }
                     }
                     if (okc && c + 1 < nch) build_E(s ^ 1, 32 * kBfIssuers, bd - 32 * kBfIssuers);
-                    if (okc && c + 2 < nch) {
-                        double pr[kBfPre];
-                        p_load(chunk_b0(c + 2), chunk_n(c + 2), pr, 32 * kBfIssuers, bd - 32 * kBfIssuers);
-                        p_store(s, chunk_n(c + 2), pr, 32 * kBfIssuers, bd - 32 * kBfIssuers);
-                    }
+                    if (okc && stage) p_store(s, chunk_n(c + 2), pr, 32 * kBfIssuers, bd - 32 * kBfIssuers);
                 }
                 pend[s] = true;
                 tc::fence_proxy_async_smem();
@@ -3569,7 +3610,9 @@ bool plan_corr_tc2(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
     P->off_V = static_cast<unsigned>(off);
     P->off_num = P->off_V;
     P->off_est = static_cast<unsigned>(off + nbytes);
-    off += std::max(Vb, 2 * nbytes);
+    // The region also takes the window's raw 16-byte chunks before the box sums.
+    const size_t rawb = static_cast<size_t>(P->XS) * (P->QM + 1) * 16;
+    off += std::max(std::max(Vb, 2 * nbytes), rawb);
     P->off_S1 = static_cast<unsigned>(off);
     off += nbytes;
     P->off_S2 = static_cast<unsigned>(off);
@@ -3966,14 +4009,19 @@ cudaError_t scratch_acquire(TrackScratch& s, cudaStream_t stream) {
 
 long long scratch_allocations() { return g_scratch_allocs.load(); }
 
-// Passes of at least kTuneMinPoints points are tuned, on their first kTuneSample points.
+// Passes of at least kTuneMinPoints points are tuned: the tensor-core kernels on their first
+// kTuneSample points, the CUDA-core kernel on the first kTuneSampleDirect.
 constexpr int64_t kTuneMinPoints = 8192;
-constexpr int64_t kTuneSample = 4096;
+constexpr int64_t kTuneSample = 32768;
+constexpr int64_t kTuneSampleDirect = 4096;
 
-// Times each candidate kernel (2 k_corr_tc2, 1 k_corr_tc, 0 k_corr) on the first kTuneSample
-// points of the pass without refinement (the pass itself overwrites their outputs), each
-// launched twice and the second timed, and returns the fastest in `kind` (a tie keeps the
-// earlier candidate).
+// Times each candidate kernel (2 k_corr_tc2, 1 k_corr_tc, 0 k_corr) on a sample of the pass's
+// first points without refinement (the pass itself overwrites their outputs), each launched
+// twice and the second timed, and returns in `kind` the one with the least time per point (a
+// tie keeps the earlier candidate). The tensor-core kernels' sample is large enough that each
+// CTA takes a run of consecutive points, as in the full pass: k_corr_tc2 carries box sums from
+// one point of a run to the next, and on a sample of 4096 points (one or two points per CTA)
+// it lost that and the tuner could pick k_corr_tc, 25 % slower on the full pass.
 template <typename Launch>
 cudaError_t autotune_u8(TrackScratch& scratch, cudaStream_t stream, const DevPoints& pts,
                         bool fit2, bool fit1, int* kind, Launch launch) {
@@ -3984,13 +4032,13 @@ cudaError_t autotune_u8(TrackScratch& scratch, cudaStream_t stream, const DevPoi
             ++g_scratch_allocs;
         }
     if (e != cudaSuccess) return e;
-    DevPoints ds = pts;
-    ds.n = std::min<int64_t>(pts.n, kTuneSample);
     float best = INFINITY;
     int chosen = fit2 ? 2 : 1;
     const int cand[3] = {2, 1, 0};
     for (int c : cand) {
         if ((c == 2 && !fit2) || (c == 1 && !fit1)) continue;
+        DevPoints ds = pts;
+        ds.n = std::min<int64_t>(pts.n, c == 0 ? kTuneSampleDirect : kTuneSample);
         e = launch(c, ds);
         if (e == cudaSuccess) e = cudaEventRecord(scratch.tune_ev[0], stream);
         if (e == cudaSuccess) e = launch(c, ds);
@@ -4000,8 +4048,9 @@ cudaError_t autotune_u8(TrackScratch& scratch, cudaStream_t stream, const DevPoi
         if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, scratch.tune_ev[0], scratch.tune_ev[1]);
         if (e != cudaSuccess) return e;
         scratch.timer.launches += 2;
-        if (ms < best) {
-            best = ms;
+        const float per_point = ms / static_cast<float>(ds.n);
+        if (per_point < best) {
+            best = per_point;
             chosen = c;
         }
     }
