@@ -1141,10 +1141,12 @@ def gpu_arm(args):
         dist.destroy_process_group()
 
 
-def profile_precision_arm(args):
-    """For ncu captures of the split-BF16 kernel: the chip-64 / radius-32 track pass over the
-    highpass-filtered Float32 --size pair at grid spacing --spacing (default pipeline otherwise),
-    `--warmup` untimed passes then `--steps` timed ones; prints one line of timings."""
+def profile_pass_arm(args, precision):
+    """For ncu captures of one correlation pass: a single track pass over the --size pair at grid
+    spacing --spacing, `--warmup` untimed passes then `--steps` timed ones; prints one line of
+    timings. precision: the split-BF16 kernel's chip-64 / radius-32 pass on the highpass-filtered
+    Float32 pair (quantize = :none); otherwise the fine chip-32 / radius-25 pass of the default
+    pipeline on the prepared UInt8 pair with the autotuner off (k_corr_tc2)."""
     import torch
     import __graft_entry__ as ge
 
@@ -1153,8 +1155,13 @@ def profile_precision_arm(args):
     L = ar._lib
     ctx = L.Context(0)
     a, b, v = scene(ar, args.size)
-    p = ar.params(chip_size=64, search_radius=32, quantize="none", upsampling=UP)
-    grid = ar.gridpoints(a.shape, args.spacing, chip_size=64, search_radius=32)
+    chip, radius = (64, 32) if precision else (32, 25)
+    if precision:
+        p = ar.params(chip_size=chip, search_radius=radius, quantize="none", upsampling=UP)
+    else:
+        p = ar.params(chip_size=chip, search_radius=radius, upsampling=UP)
+        ctx.set_option(L.AR_OPT_AUTOTUNE, 0)
+    grid = ar.gridpoints(a.shape, args.spacing, chip_size=chip, search_radius=radius)
     prep = ar.prepare(ar.ImagePair(a, b, None, v), p, ctx)
     dev = torch.device("cuda", 0)
     n = len(grid)
@@ -1175,7 +1182,8 @@ def profile_precision_arm(args):
     ctx.kernel_times()
     t = timed_steps(torch, call, stream, flush, args.steps, 0)
     corr_ms, refine_ms, _, _, flops = ctx.kernel_times()
-    print(json.dumps({"profile_precision": True, "points": n, "ms_per_pass": t / args.steps,
+    print(json.dumps({"profile_pass": "split_bf16" if precision else "u8_fine", "points": n,
+                      "chip": chip, "radius": radius, "ms_per_pass": t / args.steps,
                       "k_corr_ms": corr_ms / args.steps, "k_refine_ms": refine_ms / args.steps,
                       "algorithmic_tflops": flops / (corr_ms * 1e-3) / 1e12 if corr_ms else None}))
 
@@ -1262,6 +1270,9 @@ def main():
                     help="time the device steps only (for ncu captures); no JSON bench line")
     ap.add_argument("--profile-precision", action="store_true",
                     help="time the chip-64 split-BF16 track pass only (for ncu captures)")
+    ap.add_argument("--profile-pass", action="store_true",
+                    help="time the fine chip-32 UInt8 track pass only, autotuner off "
+                         "(k_corr_tc2; for ncu captures)")
     ap.add_argument("--spacing", type=int, default=SPACING,
                     help="grid spacing of a --profile run (the benchmark line always uses 8)")
     args = ap.parse_args()
@@ -1270,7 +1281,9 @@ def main():
     if args.impl == "reference":
         reference_arm(args)
     elif args.profile_precision:
-        profile_precision_arm(args)
+        profile_pass_arm(args, precision=True)
+    elif args.profile_pass:
+        profile_pass_arm(args, precision=False)
     elif args.serve:
         serve_arm(args)
     else:
