@@ -1465,13 +1465,15 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
 // Tensor-core correlation, surfaces up to 64 x 64 with the chip operand whole (k_corr_tc2).
 //
 // The window is staged from its first row (no alignment offset; each 16-byte block of a column
-// comes from two aligned loads), so block q of 16 rows meets surface rows i in
-// [16 q - ch + 1, 16 q + 15]: NB = 16 * ceil((ch + 15) / 16) rows of the chip operand
-// E_b[u][r] = C[r - u, b] (u = 16 - NB ... 15) and accumulator columns [16 q, 16 q + NB), one
-// accumulator of at most 128 columns for chip 32 / radius 25. The box sums come from the 16-byte
-// window blocks: column sums V down ch rows per 16-row block of surface rows (dp4a for the
-// first, a sliding update for the rest), then row sums of V with 16-byte loads. Estimates stay
-// in registers; candidates and the patch get the reference's FP64 normalisation.
+// is realigned from the aligned 16-byte chunks cp.async copied into shared memory, or from two
+// aligned global loads), so block q of 16 rows meets surface rows i in [16 q - ch + 1,
+// 16 q + 15]: NB = 16 * ceil((ch + 15) / 16) rows of the chip operand E_b[u][r] = C[r - u, b]
+// (u = 16 - NB ... 15). A block's product lands at accumulator column 16 q + e - (NB - 16) for
+// its operand row e, so surface row i is column i and the products of three issuing threads
+// write three accumulators of round16(nr) columns. The box sums come from the 16-byte window
+// blocks: column sums V down ch rows per 16-row block of surface rows (dp4a for the first, a
+// sliding update for the rest), then row sums of V with 16-byte loads. Estimates stay in
+// registers; candidates and the patch get the reference's FP64 normalisation.
 
 // Sixteen bytes of column `c` from row r0 (zero outside the image), in two steps so that a
 // thread can have several in flight: col16_issue starts the loads -- two aligned 16-byte loads
@@ -1948,7 +1950,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
             }
         };
         // Box sums of W and W^2 (integral_both!, boxsum, src/integral.jl:141-170, 244-247) as
-        // exact integers, warps 0-5 (named barrier 1) while warps 6 and 7 issue the products. When
+        // exact integers, warps 0-4 (named barrier 1) while warps 5-7 issue the products. When
         // the held sums belong to the same window geometry `sh` rows higher, the ring's base
         // advances by `sh` (the held rows become rows 0 .. nr - sh - 1) and only the last `sh`
         // rows are computed.
