@@ -809,7 +809,10 @@ __device__ unsigned long long g_tc_phase[16];
 
 // REG: every surface of the pass has at most 64 rows and 64 columns (M = 64), so one 16x256b
 // read per warp covers it and each thread keeps its 16 numerators and upper bounds in
-// registers through both passes.
+// registers through both passes. Otherwise the numerators go to shared memory and both passes
+// run over the surface in flattened order, four values per thread and step, so that every warp
+// has work even when the surface's columns fill only two or three of the M = 128 accumulator's
+// lane quarters.
 template <bool REG>
 __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
     extern __shared__ __align__(1024) unsigned char smem_tc[];
@@ -858,7 +861,23 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
     int dirty_ch = 0;
     TC_PHASE_INIT
 
-    for (int64_t k = blockIdx.x; k < A.pts.n; k += gridDim.x, ++iter) {
+    // Each CTA takes a contiguous run of points: consecutive points of a grid column have the
+    // same window columns one grid step lower, so most of their box sums carry over. s_S1 / s_S2
+    // are rings of NRS rows per column: surface row i of the held point is stored at row
+    // (i + rbase) mod NRS, and carrying the sums down by `sh` rows advances rbase.
+    const int64_t per = (A.pts.n + gridDim.x - 1) / gridDim.x;
+    const int64_t kbeg = static_cast<int64_t>(blockIdx.x) * per;
+    const int64_t kend = min(A.pts.n, kbeg + per);
+    bool held = false;  // s_S1 / s_S2 hold the sums of the geometry h_*
+    int64_t h_wr = 0, h_wc = 0;
+    int h_ch = 0, h_cw = 0, h_nr = 0, h_nc = 0;
+    int rbase = 0;
+    auto ring = [&](int i) {
+        const int r = i + rbase;
+        return r >= A.NRS ? r - A.NRS : r;
+    };
+
+    for (int64_t k = kbeg; k < kend; ++k, ++iter) {
         tc::fence_before_sync();
         __syncthreads();  // the previous point's buffers and accumulator are no longer read
         tc::fence_after_sync();
@@ -984,12 +1003,38 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         if (tid == 0 && !(A.up == 1 || nr < 5 || nc < 5)) s_slot = atomicAdd(A.sub_count, 1);
         const double nn = static_cast<double>(nnl);
 
+        // Box sums carried from the held point: same window columns and shape, `sh` rows
+        // higher; only surface rows iA .. nr - 1 are computed (iA = 0: all of them).
+        const int64_t sh64 = win_r - h_wr;
+        const bool carry = held && win_c == h_wc && ch == h_ch && cw == h_cw && nr == h_nr &&
+                           nc == h_nc && sh64 > 0 && sh64 < nr;
+        int iA = 0;
+        if (carry) {
+            iA = nr - static_cast<int>(sh64);
+            rbase += static_cast<int>(sh64);
+            if (rbase >= A.NRS) rbase -= A.NRS;
+        } else {
+            rbase = 0;
+        }
+        held = true;
+        h_wr = win_r;
+        h_wc = win_c;
+        h_ch = ch;
+        h_cw = cw;
+        h_nr = nr;
+        h_nc = nc;
+#ifdef AR_TC_PHASES
+        if (tid == 0 && carry) atomicAdd(&g_tc_phase[14], 1ull);
+#endif
+
         // Window blocks W'[16 q + r][x] (x < XS) from 16 image rows at base_r + 16 q, and the
-        // same window transposed, s_T[row][x], for the box sums.
+        // same window transposed, s_T[row][x], for the box sums (the blocks from the one that
+        // holds window row iA: the rows the box sums read).
         const int64_t delta = ((win_r % 16) + 16) % 16;
         const int64_t base_r = win_r - delta;
         const int Q = static_cast<int>((delta + ch + nr - 1 + 15) / 16);
         const int XW = cw + nc - 1;
+        const int qT = static_cast<int>((delta + iA) >> 4);
         for (int q = warp; q < Q; q += nwarps) {
             for (int x = lane; x < A.XS; x += 32) {
                 const int64_t r0 = base_r + 16 * q, c = win_c + x;
@@ -1011,7 +1056,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                     }
                 }
                 *reinterpret_cast<uint4*>(s_W + q * A.QS + x * 16) = v;
-                if (x < XW) {
+                if (x < XW && q >= qT) {
                     const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
                     for (int t = 0; t < 16; ++t)
@@ -1025,18 +1070,20 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         // Box sums of W and W^2 (integral_both!, boxsum, src/integral.jl:141-170, 244-247) as
         // exact integers: V[i][x] sums ch rows down column x, S[j][i] sums cw columns of V.
         // They run while the tensor core works on the first chunk, or, when the chip operand
-        // comes in several chunks that reuse their space, before it.
+        // comes in several chunks that reuse their space, before it. Only surface rows
+        // iA .. nr - 1 are computed (the others carried over), into ring rows.
         // Warps 0-5 only (named barrier 1): warps 6 and 7 issue the products meanwhile.
         auto box_sums = [&]() {
             constexpr int kBT = kTcThreads - 64;
             uint32_t* s_V2 = s_V1 + A.NRM * XW;
+            const int nrw = nr - iA;
             // V: one round of tasks (column x, a run of rows), each an unrolled first sum with
             // independent partials and a sliding update with the next values loaded ahead.
-            const int nseg = max(1, min((nr + 7) / 8, kBT / XW));
-            const int seglen = (nr + nseg - 1) / nseg;
+            const int nseg = max(1, min((nrw + 7) / 8, kBT / XW));
+            const int seglen = (nrw + nseg - 1) / nseg;
             for (int task = tid; task < XW * nseg; task += kBT) {
                 const int x = task % XW, seg = task / XW;
-                const int i0 = seg * seglen, i1 = min(i0 + seglen, nr);
+                const int i0 = iA + seg * seglen, i1 = min(i0 + seglen, nr);
                 if (i0 >= i1) continue;
                 const uint8_t* col = s_T + static_cast<int>(delta) * A.XT + x;
                 uint32_t p1[4] = {0, 0, 0, 0}, p2[4] = {0, 0, 0, 0};
@@ -1072,8 +1119,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             asm volatile("bar.sync 1, %0;" ::"r"(kBT) : "memory");
             // S: tasks (surface row i, a run of 16 columns), the same pattern along V's rows.
             const int jseg = (nc + 15) >> 4;
-            for (int task = tid; task < nr * jseg; task += kBT) {
-                const int i = task % nr, seg = task / nr;
+            for (int task = tid; task < nrw * jseg; task += kBT) {
+                const int i = iA + task % nrw, seg = task / nrw;
+                const int ri = ring(i);
                 const int j0 = seg << 4, j1 = min(j0 + 16, nc);
                 const uint32_t* v1 = s_V1 + i * XW;
                 const uint32_t* v2 = s_V2 + i * XW;
@@ -1093,8 +1141,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                 uint32_t g1 = (q1[0] + q1[1]) + (q1[2] + q1[3]);
                 uint32_t g2 = (q2[0] + q2[1]) + (q2[2] + q2[3]);
                 for (int j = j0; j < j1; ++j) {
-                    s_S1[j * A.NRS + i] = g1;
-                    s_S2[j * A.NRS + i] = g2;
+                    s_S1[j * A.NRS + ri] = g1;
+                    s_S2[j * A.NRS + ri] = g2;
                     if (j + 1 < j1) {
                         g1 = g1 + v1[j + cw] - v1[j];
                         g2 = g2 + v2[j + cw] - v2[j];
@@ -1240,7 +1288,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                     upb[v] = -INFINITY;
                     if (i < nr && j < nc) {
                         vm |= 1u << v;
-                        const int o = j * A.NRS + i;
+                        const int o = j * A.NRS + ring(i);
                         float bnd;
                         const float est = tc_estimate(dv[v], s_S1[o], s_S2[o], nnf, csf, kk, kk7,
                                                       A.measure, &bnd);
@@ -1275,7 +1323,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             unsigned long long best = 0ull;
             for (int c = tid; c < ncand; c += bd) {
                 const int i = static_cast<int>(s_cI[c] >> 16), j = static_cast<int>(s_cI[c] & 0xFFFFu);
-                const int o = j * A.NRS + i;
+                const int o = j * A.NRS + ring(i);
                 const float x = tc_exact(s_cD[c], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
                 const unsigned long long key = argmax_key(x, static_cast<unsigned>(i * nc + j));
                 best = key > best ? key : best;
@@ -1294,7 +1342,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                 float* so = A.surf_out + k * static_cast<int64_t>(A.NRM) * A.NCM;
                 for (int e = tid; e < nr * nc; e += bd) {
                     const int o = (e / nr) * A.NRS + (e % nr);
-                    so[e] = tc_exact(s_num[o], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+                    const int os = (e / nr) * A.NRS + ring(e % nr);
+                    so[e] = tc_exact(s_num[o], s_S1[os], s_S2[os], mean, nn, cnorm, A.measure);
                 }
             }
             unsigned rm = 0;
@@ -1317,7 +1366,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             __syncthreads();
             if (single) {
                 if (tid == 0) {
-                    const int o = pj * A.NRS + pi;
+                    const int o = pj * A.NRS + ring(pi);
                     A.out.dx[k] = __double2float_rn(
                         __dadd_rn(static_cast<double>(pj - static_cast<int>(prx)), A.pts.dx0[k]));
                     A.out.dy[k] = __double2float_rn(
@@ -1328,7 +1377,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                 const int slot = s_slot;
                 if (tid < 25) {
                     const int a = tid % 5, b = tid / 5;
-                    const int o = (pj0 + b) * A.NRS + (pi0 + a);
+                    const int o = (pj0 + b) * A.NRS + ring(pi0 + a);
                     A.sub_patch[static_cast<int64_t>(slot) * 25 + tid] =
                         tc_exact(s_pd[tid], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
                 }
@@ -1342,11 +1391,25 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             TC_PHASE_POINT
             continue;
         }
+        // The surface's values in flattened order e = i + nr j: thread t starts at e = t and
+        // steps by kTcThreads (row and column advanced without a division).
+        const int ne = nr * nc;
+        const int fj0 = tid / nr, fi0 = tid - fj0 * nr;
+        const int fdj = kTcThreads / nr, fdi = kTcThreads - fdj * nr;
+        auto fstep = [&](int& i, int& j) {
+            i += fdi;
+            j += fdj;
+            if (i >= nr) {
+                i -= nr;
+                ++j;
+            }
+        };
         auto take = [&](uint32_t d, int i, int j) {
             if (j < nc && i < nr) {
                 const int o = j * A.NRS + i;
+                const int os = j * A.NRS + ring(i);
                 float bnd;
-                const float est = tc_estimate(d, s_S1[o], s_S2[o], nnf, csf, kk, kk7, A.measure, &bnd);
+                const float est = tc_estimate(d, s_S1[os], s_S2[os], nnf, csf, kk, kk7, A.measure, &bnd);
                 s_num[o] = d;
                 s_est[o] = est;
                 s_est[o + A.NCM * A.NRS] = bnd;
@@ -1369,18 +1432,61 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                          16 * quarter + (lane >> 2) + ((v & 2) ? 8 : 0));
             }
         } else {
-            // M = 128: accumulator row j is lane j; thread = row 32 q + lane, 16 columns.
-            for (int i0 = 16 * half; i0 < nr; i0 += 32) {
-                uint32_t r[16], r1[16];
-                const uint32_t base = taddr + (static_cast<uint32_t>(32 * quarter) << 16) + col0 +
-                                      static_cast<uint32_t>(i0);
-                tc::tmem_ld16(base, r);
-                tc::tmem_ld16(base + acc1, r1);
-                tc::tmem_wait_ld();
+            // M = 128: accumulator row j is lane j; thread = row 32 q + lane, 16 columns. Only
+            // the lane quarters below nc hold surface columns (for nc <= 96, two or three of
+            // the four), so their warps move the numerators to shared memory and the estimates
+            // are spread over all warps: warp w takes columns w, w + 8, ..., lanes the rows.
+            if (32 * quarter < nc) {
+                const int j = 32 * quarter + lane;
+                for (int i0 = 16 * half; i0 < nr; i0 += 32) {
+                    uint32_t r[16], r1[16];
+                    const uint32_t base = taddr + (static_cast<uint32_t>(32 * quarter) << 16) +
+                                          col0 + static_cast<uint32_t>(i0);
+                    tc::tmem_ld16(base, r);
+                    tc::tmem_ld16(base + acc1, r1);
+                    tc::tmem_wait_ld();
+                    if (j < nc) {
 #pragma unroll
-                for (int m = 0; m < 16; ++m) r[m] += r1[m];
+                        for (int m = 0; m < 16; ++m)
+                            if (i0 + m < nr) s_num[j * A.NRS + i0 + m] = r[m] + r1[m];
+                    }
+                }
+            }
+            __syncthreads();
+            // Four values per thread and step, their loads issued before the (paired) arithmetic.
+            int fi = fi0, fj = fj0;
+            for (int e = tid; e < ne; e += 4 * kTcThreads) {
+                int o[4], os[4];
+                bool in[4];
+                uint32_t d[4], s1[4], s2[4];
 #pragma unroll
-                for (int m = 0; m < 16; ++m) take(r[m], i0 + m, 32 * quarter + lane);
+                for (int u = 0; u < 4; ++u) {
+                    in[u] = e + u * kTcThreads < ne;
+                    o[u] = fj * A.NRS + fi;
+                    os[u] = fj * A.NRS + ring(fi);
+                    fstep(fi, fj);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    d[u] = in[u] ? s_num[o[u]] : 0u;
+                    s1[u] = in[u] ? s_S1[os[u]] : 0u;
+                    s2[u] = in[u] ? s_S2[os[u]] : 0u;
+                }
+                float2 b01, b23;
+                const float2 e01 = tc_estimate2(d[0], d[1], s1[0], s1[1], s2[0], s2[1], nnf, csf,
+                                                kk, kk7, A.measure, &b01);
+                const float2 e23 = tc_estimate2(d[2], d[3], s1[2], s1[3], s2[2], s2[3], nnf, csf,
+                                                kk, kk7, A.measure, &b23);
+                const float ev[4] = {e01.x, e01.y, e23.x, e23.y};
+                const float bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (in[u]) {
+                        s_est[o[u]] = ev[u];
+                        s_est[o[u] + A.NCM * A.NRS] = bv[u];
+                        lmax = fmaxf(lmax, ev[u] - bv[u]);
+                    }
+                }
             }
         }
 #pragma unroll
@@ -1393,16 +1499,38 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         // M: the largest lower bound of any value. A value whose upper bound is below it is
         // strictly below some other value: it cannot be the (first) maximum.
 
-        // Pass 2: exact values where the upper bound reaches M; the peak key.
+        // Pass 2: exact values where the upper bound reaches M; the peak key. The same flattened
+        // order, four values per thread and step.
         unsigned long long best = 0ull;
-        for (int jj = warp; jj < nc; jj += nwarps) {
-            for (int i = lane; i < nr; i += 32) {
-                const int o = jj * A.NRS + i;
-                const float est = s_est[o], bnd = s_est[o + A.NCM * A.NRS];
-                if (!(est + bnd >= M) && !isnan(est)) continue;
-                const float v = tc_exact(s_num[o], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
-                const unsigned long long key = argmax_key(v, static_cast<unsigned>(i * nc + jj));
-                best = key > best ? key : best;
+        {
+            int fi = fi0, fj = fj0;
+            for (int e = tid; e < ne; e += 4 * kTcThreads) {
+                int o[4], ii[4], jj[4];
+                bool in[4];
+                float est[4], bnd[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    in[u] = e + u * kTcThreads < ne;
+                    ii[u] = fi;
+                    jj[u] = fj;
+                    o[u] = fj * A.NRS + fi;
+                    fstep(fi, fj);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    est[u] = in[u] ? s_est[o[u]] : 0.0f;
+                    bnd[u] = in[u] ? s_est[o[u] + A.NCM * A.NRS] : 0.0f;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (!in[u] || (!(est[u] + bnd[u] >= M) && !isnan(est[u]))) continue;
+                    const int os = jj[u] * A.NRS + ring(ii[u]);
+                    const float v =
+                        tc_exact(s_num[o[u]], s_S1[os], s_S2[os], mean, nn, cnorm, A.measure);
+                    const unsigned long long key =
+                        argmax_key(v, static_cast<unsigned>(ii[u] * nc + jj[u]));
+                    best = key > best ? key : best;
+                }
             }
         }
         best = block_max_u64(best, reinterpret_cast<unsigned long long*>(s_red));
@@ -1413,7 +1541,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             float* so = A.surf_out + k * static_cast<int64_t>(A.NRM) * A.NCM;
             for (int e = tid; e < nr * nc; e += bd) {
                 const int o = (e / nr) * A.NRS + (e % nr);
-                so[e] = tc_exact(s_num[o], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+                const int os = (e / nr) * A.NRS + ring(e % nr);
+                so[e] = tc_exact(s_num[o], s_S1[os], s_S2[os], mean, nn, cnorm, A.measure);
             }
         }
         unsigned rm = 0;
@@ -1426,7 +1555,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         if (A.up == 1 || nr < 5 || nc < 5) {
             if (tid == 0) {
                 const int o = pj * A.NRS + pi;
-                const float v = tc_exact(s_num[o], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+                const int os = pj * A.NRS + ring(pi);
+                const float v = tc_exact(s_num[o], s_S1[os], s_S2[os], mean, nn, cnorm, A.measure);
                 A.out.dx[k] = __double2float_rn(
                     __dadd_rn(static_cast<double>(pj - static_cast<int>(prx)), A.pts.dx0[k]));
                 A.out.dy[k] = __double2float_rn(
@@ -1440,8 +1570,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             if (tid < 25) {
                 const int a = tid % 5, b = tid / 5;
                 const int o = (pj0 + b) * A.NRS + (pi0 + a);
+                const int os = (pj0 + b) * A.NRS + ring(pi0 + a);
                 A.sub_patch[static_cast<int64_t>(slot) * 25 + tid] =
-                    tc_exact(s_num[o], s_S1[o], s_S2[o], mean, nn, cnorm, A.measure);
+                    tc_exact(s_num[o], s_S1[os], s_S2[os], mean, nn, cnorm, A.measure);
             }
             if (tid == 0) {
                 A.sub_point[slot] = k;
@@ -1449,6 +1580,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                 A.sub_origin[2 * slot + 1] = pj0;
             }
         }
+        TC_PHASE(10)
+        TC_PHASE_POINT
     }
     TC_PHASE_FLUSH
     if (failed) {

@@ -10,6 +10,8 @@ the kernel computes it and checks it against the direct definition:
   surface row whose differences cw columns apart are the box sums) against direct box sums;
 * the three-limb BF16 split: v == l0 + l1 + l2 for normal Float32 v, and two limbs for integers
   below 2^16 in magnitude;
+* the flattened order of `k_corr_tc`'s wide-surface epilogue (every value visited once) and the
+  ring rows of the carried box sums;
 * the FP32 mean of `k_highpass_w`: the correctly rounded FP32 quotient of an integer sum by a
   count equals the FP64 quotient rounded to FP32 (double rounding innocuous), for every count
   the kernel can see.
@@ -182,3 +184,59 @@ def test_fp32_mean_equals_fp64_mean_rounded():
         f32 = a.astype(np.float32) / np.float32(cnt)          # IEEE FP32 division
         f64 = (a.astype(np.float64) / np.float64(cnt)).astype(np.float32)
         assert np.array_equal(f32.view(np.uint32), f64.view(np.uint32)), cnt
+
+
+def flattened_visits(nr, nc, threads=256, group=4):
+    """`k_corr_tc`'s flattened epilogue order: thread t starts at e = t (row e mod nr, column
+    e div nr) and steps by `threads`, advancing the row by threads mod nr and the column by
+    threads div nr with one carry; `group` values per step, the last ones masked by e < nr nc."""
+    ne = nr * nc
+    fdj, fdi = threads // nr, threads - (threads // nr) * nr
+    seen = np.zeros((nr, nc), np.int64)
+    for t in range(threads):
+        fj, fi = t // nr, t - (t // nr) * nr
+        for e in range(t, ne, group * threads):
+            for u in range(group):
+                if e + u * threads < ne:
+                    assert fi + fj * nr == e + u * threads
+                    seen[fi, fj] += 1
+                fi += fdi
+                fj += fdj
+                if fi >= nr:
+                    fi -= nr
+                    fj += 1
+    return seen
+
+
+@pytest.mark.parametrize("nr,nc", [(66, 66), (94, 94), (80, 81), (1, 128), (256, 64), (300, 3),
+                                   (128, 128), (17, 100)])
+def test_flattened_epilogue_visits_every_value_once(nr, nc):
+    assert np.all(flattened_visits(nr, nc) == 1)
+
+
+def test_ring_rows_carry_box_sums():
+    """Carried box sums: after the held point's sums are shifted up by sh rows (ring base
+    advanced by sh, only the last sh rows recomputed), every ring row holds the new point's sums."""
+    rng = np.random.default_rng(3)
+    ch, cw, nr, nc = 12, 10, 30, 20
+    NRS = nr | 1
+    W = rng.integers(0, 256, (ch + nr - 1 + 200, cw + nc - 1)).astype(np.int64)
+
+    def box(r0, i, j):
+        return W[r0 + i:r0 + i + ch, j:j + cw].sum()
+
+    S = np.zeros((nc, NRS), np.int64)
+    rbase, r0 = 0, 0
+    ring = lambda i: (i + rbase) % NRS
+    for i in range(nr):
+        for j in range(nc):
+            S[j, ring(i)] = box(r0, i, j)
+    for sh in (8, 8, 3, 29, 1, 8):
+        r0 += sh
+        rbase = (rbase + sh) % NRS
+        for i in range(nr - sh, nr):
+            for j in range(nc):
+                S[j, ring(i)] = box(r0, i, j)
+        for i in range(nr):
+            for j in range(nc):
+                assert S[j, ring(i)] == box(r0, i, j)
