@@ -659,8 +659,9 @@ struct TcArgs {
     int big;                         // 1: box sums before the products, chunks reuse their space
     unsigned off_E, off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
     int XV;                          // k_corr_tc2: row stride (words) of the column sums V1, V2
-    int acc1_col;                    // first column of the second accumulator (k_corr_tc2: the
-                                     // stride between its accumulators)
+    int acc1_col;                    // stride between the accumulators (first column of the
+                                     // second one)
+    int issuers;                     // k_corr_tc: threads issuing the products, 2 or 4
     uint32_t tmem_cols;
     DevOutputs out;
     int* sub_count;
@@ -781,6 +782,54 @@ __device__ __forceinline__ bool block_rows(int q, int NB, int nr, int* elo, int*
     return true;
 }
 
+// prepare_chip! statistics (src/correlate.jl:423-453) of a UInt8 chip staged as zero-padded
+// byte columns (row a of column b at s_P[b * PC + kPadL + a]; rows outside the image are 0, as
+// `pixel` reads them), in the CUDA-core kernel's per-thread order -- thread t takes elements
+// t, t + bd, ... of the column-major chip, then its block sum -- so the FP64 sums are its own bit
+// for bit. Row and column advance without a division.
+__device__ __forceinline__ void staged_chip_stats(const uint8_t* s_P, int PC, int ch, int cw, int tid,
+                                                  int bd, double* s_red, double* csum, double* mean,
+                                                  double* sq) {
+    double st[1] = {0.0};
+    {
+        const int db = bd / ch, da = bd - db * ch;
+        int b = tid / ch, a = tid - b * ch;
+        for (int e = tid; e < ch * cw; e += bd) {
+            st[0] = __dadd_rn(st[0], static_cast<double>(s_P[b * PC + kPadL + a]));
+            a += da;
+            b += db;
+            if (a >= ch) {
+                a -= ch;
+                ++b;
+            }
+        }
+    }
+    block_sum_f64<1>(st, s_red);
+    *csum = st[0];
+    const double m = __ddiv_rn(st[0], static_cast<double>(ch) * static_cast<double>(cw));
+    *mean = m;
+    const int chp = (ch + kUA - 1) & ~(kUA - 1);
+    double acc2[1] = {0.0};
+    {
+        const int db = bd / chp, da = bd - db * chp;
+        int b = tid / chp, a = tid - b * chp;
+        for (int e = tid; e < chp * cw; e += bd) {
+            if (a < ch) {
+                const double d = __dsub_rn(static_cast<double>(s_P[b * PC + kPadL + a]), m);
+                acc2[0] = __dadd_rn(acc2[0], __dmul_rn(d, d));
+            }
+            a += da;
+            b += db;
+            if (a >= chp) {
+                a -= chp;
+                ++b;
+            }
+        }
+    }
+    block_sum_f64<1>(acc2, s_red);
+    *sq = acc2[0];
+}
+
 // Optional phase timer (compiled in with -DAR_TC_PHASES, for profiling builds only): thread 0
 // of each CTA accumulates clock64() cycles between the marks below, per phase, and adds them to
 // g_tc_phase at exit; entry 15 counts the points that reached the output phase.
@@ -836,6 +885,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
 
     const int tid = threadIdx.x, bd = blockDim.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = bd >> 5;
+    // Threads issuing the products (only plans of the register epilogue take four).
+    const int NI = REG ? A.issuers : 2;
     const int64_t NR = A.nrows + 2 * A.pady, NC = A.ncols + 2 * A.padx;
     const double shx = static_cast<double>(A.padx) + 0.5;
     const double shy = static_cast<double>(A.pady) + 0.5;
@@ -845,7 +896,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         tc::tmem_relinquish();
     }
     if (tid == 0) {
-        tc::mbar_init(&s_mbar, 2);  // one commit per issuing thread
+        tc::mbar_init(&s_mbar, NI);  // one commit per issuing thread
         tc::fence_mbar_init();
     }
     tc::fence_before_sync();
@@ -927,7 +978,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             const int a = a0 + lane;
             const int64_t r = chip_r + a;
             const bool rin = a < ch && r >= 0 && r < A.nrows;
-            constexpr int kU = 4;
+            constexpr int kU = REG ? 8 : 4;  // columns per step: more loads in flight for wide chips
             for (int b0 = warp; b0 < cw; b0 += kU * nwarps) {
                 uint32_t v[kU], m[kU];
 #pragma unroll
@@ -976,24 +1027,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             mean = __ddiv_rn(csum_d, static_cast<double>(nnl));
             sq = __ddiv_rn(static_cast<double>(nnl * c2 - cs * cs), static_cast<double>(nnl));
         } else {
-            double st[1] = {0.0};
-            for (int e = tid; e < ch * cw; e += bd)
-                st[0] = __dadd_rn(st[0], pixel(A.sec, A.nrows, A.ncols, chip_r + e % ch, chip_c + e / ch));
-            block_sum_f64<1>(st, s_red);
-            csum_d = st[0];
-            mean = __ddiv_rn(st[0], static_cast<double>(nnl));
-            const int chp = (ch + kUA - 1) & ~(kUA - 1);
-            double acc2[1] = {0.0};
-            for (int e = tid; e < chp * cw; e += bd) {
-                const int a = e % chp, b = e / chp;
-                if (a < ch) {
-                    const double v = pixel(A.sec, A.nrows, A.ncols, chip_r + a, chip_c + b);
-                    const double d = __dsub_rn(v, mean);
-                    acc2[0] = __dadd_rn(acc2[0], __dmul_rn(d, d));
-                }
-            }
-            block_sum_f64<1>(acc2, s_red);
-            sq = acc2[0];
+            staged_chip_stats(s_P, A.PC, ch, cw, tid, bd, s_red, &csum_d, &mean, &sq);
         }
         if (!(sq > __dmul_rn(__dmul_rn(DBL_EPSILON, static_cast<double>(ch)), static_cast<double>(cw))))
             continue;  // degenerate chip: searched, no measurement (src/track.jl:286)
@@ -1072,9 +1106,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         // They run while the tensor core works on the first chunk, or, when the chip operand
         // comes in several chunks that reuse their space, before it. Only surface rows
         // iA .. nr - 1 are computed (the others carried over), into ring rows.
-        // Warps 0-5 only (named barrier 1): warps 6 and 7 issue the products meanwhile.
-        auto box_sums = [&]() {
-            constexpr int kBT = kTcThreads - 64;
+        // Threads 0 .. kBT - 1 (named barrier 1): the warps below the issuing ones.
+        auto box_sums = [&](const int kBT) {
             uint32_t* s_V2 = s_V1 + A.NRM * XW;
             const int nrw = nr - iA;
             // V: one round of tasks (column x, a run of rows), each an unrolled first sum with
@@ -1151,7 +1184,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
             }
         };
         if (A.big) {
-            if (warp < 6) box_sums();
+            if (warp < nwarps - NI) box_sums(kTcThreads - 32 * NI);
             __syncthreads();  // the chip chunks overwrite s_T and s_V
         }
 
@@ -1199,25 +1232,27 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                 // trimmed to the surface rows), stored from column 0 of each accumulator.
                 const int zc = (nr + 16 + 15) & ~15;
                 const uint32_t lq = taddr + (static_cast<uint32_t>(32 * warp) << 16);
-                for (int c = 0; c < zc; c += 16) {
-                    tc::tmem_st16(lq + static_cast<uint32_t>(c), z);
-                    tc::tmem_st16(lq + acc1 + static_cast<uint32_t>(c), z);
-                }
+                for (int s = 0; s < NI; ++s)
+                    for (int c = 0; c < zc; c += 16)
+                        tc::tmem_st16(lq + static_cast<uint32_t>(s) * acc1 + static_cast<uint32_t>(c), z);
                 tc::tmem_wait_st();
             }
             tc::fence_proxy_async_smem();
             tc::fence_before_sync();
             __syncthreads();
             TC_PHASE(5)
-            // Two threads issue the products, each for half of the chunk's chip column pairs into
-            // its own accumulator (one thread's MMAs run one after another).
-            if (tid == kTcThreads - 32 || tid == kTcThreads - 64) {
-                const int stream = tid == kTcThreads - 32 ? 0 : 1;
+            // Lane 0 of each of the last NI warps issues the products of a share of the
+            // chunk's chip column pairs into its own accumulator (one thread's MMAs run one after
+            // another, so the products of one point are spread over two or four threads).
+            if (REG ? (lane == 0 && warp >= nwarps - NI)
+                    : (tid == kTcThreads - 32 || tid == kTcThreads - 64)) {
+                const int stream = REG ? nwarps - 1 - warp : (tid == kTcThreads - 32 ? 0 : 1);
                 tc::fence_after_sync();
                 const uint32_t sW = tc::smem_u32(s_W), sE = tc::smem_u32(s_E);
-                const int p0 = b0 / 2, p1 = b1 / 2, pm = p0 + (p1 - p0) / 2;
-                const int tb = stream == 0 ? p0 : pm, te = stream == 0 ? pm : p1;
-                const uint32_t dacc = taddr + (stream ? acc1 : 0u);
+                const int p0 = b0 / 2, p1 = b1 / 2;
+                const int tb = p0 + (p1 - p0) * stream / NI;
+                const int te = p0 + (p1 - p0) * (stream + 1) / NI;
+                const uint32_t dacc = taddr + static_cast<uint32_t>(stream) * acc1;
                 for (int q = 0; q < Q; ++q) {
                     // Only the operand rows e in [elo, elo + n) of block q reach surface rows;
                     // their accumulator columns start at NB - 16 in block coordinates.
@@ -1234,7 +1269,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                 }
                 tc::mma_commit(&s_mbar);
             }
-            if (cc == 0 && !A.big && warp < 6) box_sums();
+            if (cc == 0 && !A.big && warp < nwarps - NI) box_sums(kTcThreads - 32 * NI);
             TC_PHASE(6)
         }
         if (ok) {
@@ -1282,6 +1317,12 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                 tc::tmem_wait_ld();
 #pragma unroll
                 for (int v = 0; v < 16; ++v) dv[v] += dv1[v];
+                for (int s = 2; s < NI; ++s) {
+                    tc::tmem_ld16dp(base + static_cast<uint32_t>(s) * acc1, dv1);
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int v = 0; v < 16; ++v) dv[v] += dv1[v];
+                }
 #pragma unroll
                 for (int v = 0; v < 16; ++v) {
                     const int i = ib0 + 8 * (v >> 2) + (v & 1), j = jb0 + ((v & 2) ? 8 : 0);
@@ -1426,6 +1467,12 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                 tc::tmem_wait_ld();
 #pragma unroll
                 for (int v = 0; v < 16; ++v) r[v] += r1[v];
+                for (int s = 2; s < NI; ++s) {
+                    tc::tmem_ld16dp(base + static_cast<uint32_t>(s) * acc1, r1);
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int v = 0; v < 16; ++v) r[v] += r1[v];
+                }
 #pragma unroll
                 for (int v = 0; v < 16; ++v)
                     take(r[v], i0 + 8 * (v >> 2) + 2 * (lane & 3) + (v & 1),
@@ -1445,10 +1492,18 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
                     tc::tmem_ld16(base, r);
                     tc::tmem_ld16(base + acc1, r1);
                     tc::tmem_wait_ld();
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) r[m] += r1[m];
+                    for (int s = 2; s < NI; ++s) {
+                        tc::tmem_ld16(base + static_cast<uint32_t>(s) * acc1, r1);
+                        tc::tmem_wait_ld();
+#pragma unroll
+                        for (int m = 0; m < 16; ++m) r[m] += r1[m];
+                    }
                     if (j < nc) {
 #pragma unroll
                         for (int m = 0; m < 16; ++m)
-                            if (i0 + m < nr) s_num[j * A.NRS + i0 + m] = r[m] + r1[m];
+                            if (i0 + m < nr) s_num[j * A.NRS + i0 + m] = r[m];
                     }
                 }
             }
@@ -1885,24 +1940,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc2(const TcArgs A) {
             mean = __ddiv_rn(csum_d, static_cast<double>(nnl));
             sq = __ddiv_rn(static_cast<double>(nnl * c2 - cs * cs), static_cast<double>(nnl));
         } else {
-            double st[1] = {0.0};
-            for (int e = tid; e < ch * cw; e += bd)
-                st[0] = __dadd_rn(st[0], pixel(A.sec, A.nrows, A.ncols, chip_r + e % ch, chip_c + e / ch));
-            block_sum_f64<1>(st, s_red);
-            csum_d = st[0];
-            mean = __ddiv_rn(st[0], static_cast<double>(nnl));
-            const int chp = (ch + kUA - 1) & ~(kUA - 1);
-            double acc2[1] = {0.0};
-            for (int e = tid; e < chp * cw; e += bd) {
-                const int a = e % chp, b = e / chp;
-                if (a < ch) {
-                    const double v = pixel(A.sec, A.nrows, A.ncols, chip_r + a, chip_c + b);
-                    const double d = __dsub_rn(v, mean);
-                    acc2[0] = __dadd_rn(acc2[0], __dmul_rn(d, d));
-                }
-            }
-            block_sum_f64<1>(acc2, s_red);
-            sq = acc2[0];
+            staged_chip_stats(s_P, A.PC, ch, cw, tid, bd, s_red, &csum_d, &mean, &sq);
         }
         if (!(sq > __dmul_rn(__dmul_rn(DBL_EPSILON, static_cast<double>(ch)), static_cast<double>(cw))))
             continue;  // degenerate chip: searched, no measurement (src/track.jl:286)
@@ -3694,7 +3732,7 @@ size_t tmem_smem_floor(uint32_t cols, size_t static_smem) {
 struct TcPlan {
     int NB, QM, QS, PS, PC, XS, XT, NRS, NRM, NCM, CHM, CWM, BC, big, MT;
     unsigned off_E, off_W, off_T, off_P, off_V, off_S1, off_S2, off_num, off_est, off_red;
-    int XV = 0, acc1_col = 0;
+    int XV = 0, acc1_col = 0, issuers = 2;
     uint32_t tmem_cols;
     size_t smem;
 };
@@ -3840,6 +3878,18 @@ bool plan_corr_bf(const PassGeometry& g, size_t smem_cap, BfPlan* P) {
     return true;
 }
 
+// A k_corr_tc plan whose shared memory leaves room for one CTA per SM anyway has the SM's 512
+// Tensor Memory columns to itself: with M = 64 products (surfaces up to 64 x 64: the chip-128
+// levels), which one thread issues only about every 120 cycles, it issues them from four threads
+// into four accumulators. M = 128 products are bound by the tensor pipe and keep two.
+void four_issuers(TcPlan* P) {
+    const bool one_per_sm = 2 * (P->smem + 2048) > 228 * 1024;
+    if (one_per_sm && P->MT == 64 && P->NRM <= 64 && 4 * P->acc1_col <= 512) {
+        P->issuers = 4;
+        P->tmem_cols = static_cast<uint32_t>(4 * P->acc1_col);
+    }
+}
+
 // Shared-memory plan of k_corr_tc for a pass's largest geometry; false when the pass does not
 // fit the kernel (surface wider than 64 columns, more than 256 rows, chips taller than 226).
 // The whole chip operand and separate box-sum buffers when they fit ("overlap": the box sums
@@ -3905,6 +3955,7 @@ bool plan_corr_tc(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
             P->smem = off;
             P->BC = cw;
             P->big = 0;
+            four_issuers(P);
             return true;
         }
     }
@@ -3933,6 +3984,7 @@ bool plan_corr_tc(const PassGeometry& g, size_t smem_cap, TcPlan* P) {
     P->off_V = static_cast<unsigned>(off + Tb);
     P->off_est = static_cast<unsigned>(off + nbytes);
     P->smem = off + std::max(zone_min, static_cast<size_t>(bc) * P->PS);
+    four_issuers(P);
     return true;
 }
 
@@ -4305,6 +4357,7 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         B.off_red = TP.off_red;
         B.XV = TP.XV;
         B.acc1_col = TP.acc1_col;
+        B.issuers = TP.issuers;
         B.tmem_cols = TP.tmem_cols;
         B.out = out;
         B.sub_count = scratch.sub_count;
