@@ -782,48 +782,136 @@ __device__ __forceinline__ bool block_rows(int q, int NB, int nr, int* elo, int*
     return true;
 }
 
+// Sixteen bytes of column `c` from row r0 (zero outside the image), in two steps so that a
+// thread can have several in flight: col16_issue starts the loads -- two aligned 16-byte loads
+// when they stay inside the image, else byte by byte -- and col16_finish shifts the bytes into
+// place.
+struct Col16 {
+    uint4 lo, hi;
+    uint32_t s;  // byte offset of row r0 in `lo` (0: `lo` is the result)
+};
+
+__device__ __forceinline__ Col16 col16_issue(const uint8_t* img, const uint8_t* img_end,
+                                             int64_t nrows, int64_t ncols, int64_t c, int64_t r0) {
+    Col16 L;
+    L.s = 0;
+    L.lo = L.hi = make_uint4(0, 0, 0, 0);
+    if (c < 0 || c >= ncols) return L;
+    const uint8_t* p = img + c * nrows + r0;
+    if (r0 >= 0 && r0 + 16 <= nrows) {
+        const uintptr_t pa = reinterpret_cast<uintptr_t>(p);
+        const uint32_t s = static_cast<uint32_t>(pa & 15);
+        const uint4* a = reinterpret_cast<const uint4*>(pa - s);
+        if (s == 0) {
+            L.lo = __ldg(a);
+            return L;
+        }
+        if (reinterpret_cast<const uint8_t*>(a) + 32 <= img_end) {
+            L.lo = __ldg(a);
+            L.hi = __ldg(a + 1);
+            L.s = s;
+            return L;
+        }
+    }
+    uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+        const int64_t r = r0 + t;
+        const uint32_t bb = (r >= 0 && r < nrows) ? p[t] : 0u;
+        w[t >> 2] |= bb << (8 * (t & 3));
+    }
+    L.lo = make_uint4(w[0], w[1], w[2], w[3]);
+    return L;
+}
+
+__device__ __forceinline__ uint4 col16_finish(const Col16& L) {
+    const uint32_t s = L.s;
+    if (s == 0) return L.lo;
+    const uint32_t w[8] = {L.lo.x, L.lo.y, L.lo.z, L.lo.w, L.hi.x, L.hi.y, L.hi.z, L.hi.w};
+    uint32_t u[6], v[5];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) u[k] = (s & 8) ? w[k + 2] : w[k];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) v[k] = (s & 4) ? u[k + 1] : u[k];
+    const uint32_t sh = (s & 3) * 8u;
+    return make_uint4(__funnelshift_r(v[0], v[1], sh), __funnelshift_r(v[1], v[2], sh),
+                      __funnelshift_r(v[2], v[3], sh), __funnelshift_r(v[3], v[4], sh));
+}
+
 // prepare_chip! statistics (src/correlate.jl:423-453) of a UInt8 chip staged as zero-padded
 // byte columns (row a of column b at s_P[b * PC + kPadL + a]; rows outside the image are 0, as
-// `pixel` reads them), in the CUDA-core kernel's per-thread order -- thread t takes elements
-// t, t + bd, ... of the column-major chip, then its block sum -- so the FP64 sums are its own bit
-// for bit. Row and column advance without a division.
+// `pixel` reads them), with the CUDA-core kernel's FP64 results bit for bit: thread t takes
+// elements t, t + bd, ... of the column-major chip (rows padded to a multiple of kUA) and the
+// per-thread partial sums go through the same block sum.
+//   One pass gives each thread the count m, sum P and sum of squares Q of its elements (exact
+// integers; the sum of C is exact in any order). When the area nn is a power of two the mean
+// S/nn is exact, so is every deviation d = N/nn (N = nn C - S) and its square, and a thread's
+// FP64 running sum of squares is exactly K/nn^2 with K = sum N^2 = nn^2 Q - 2 nn S P + m S^2
+// while K stays below 2^53 -- guaranteed when (its terms) x (255 nn)^2 is: then the partial is
+// that integer scaled by 1/nn^2, the double the FP64 loop produces. Other areas take the FP64
+// loop over the staged chip.
 __device__ __forceinline__ void staged_chip_stats(const uint8_t* s_P, int PC, int ch, int cw, int tid,
                                                   int bd, double* s_red, double* csum, double* mean,
                                                   double* sq) {
-    double st[1] = {0.0};
+    const int chp = (ch + kUA - 1) & ~(kUA - 1);
+    const int ne = chp * cw;
+    const int db = bd / chp, da = bd - db * chp;
+    const int b0 = tid / chp, a0 = tid - b0 * chp;
+    auto step = [&](int& a, int& b) {
+        a += da;
+        b += db;
+        if (a >= chp) {
+            a -= chp;
+            ++b;
+        }
+    };
+    uint32_t P = 0u, Q = 0u, m = 0u;
     {
-        const int db = bd / ch, da = bd - db * ch;
-        int b = tid / ch, a = tid - b * ch;
-        for (int e = tid; e < ch * cw; e += bd) {
-            st[0] = __dadd_rn(st[0], static_cast<double>(s_P[b * PC + kPadL + a]));
-            a += da;
-            b += db;
-            if (a >= ch) {
-                a -= ch;
-                ++b;
+        int a = a0, b = b0;
+        for (int e = tid; e < ne; e += 4 * bd) {
+            int o[4];
+            bool in[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                in[u] = e + u * bd < ne && a < ch;
+                o[u] = b * PC + kPadL + a;
+                step(a, b);
+            }
+            uint32_t v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[u] = in[u] ? s_P[o[u]] : 0u;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                P += v[u];
+                Q += v[u] * v[u];
+                m += in[u] ? 1u : 0u;
             }
         }
     }
+    double st[1] = {static_cast<double>(P)};
     block_sum_f64<1>(st, s_red);
     *csum = st[0];
-    const double m = __ddiv_rn(st[0], static_cast<double>(ch) * static_cast<double>(cw));
-    *mean = m;
-    const int chp = (ch + kUA - 1) & ~(kUA - 1);
+    const int nn = ch * cw;
+    const double mn = __ddiv_rn(st[0], static_cast<double>(nn));
+    *mean = mn;
+    const int terms = (ne + bd - 1) / bd;
+    const double span = 255.0 * static_cast<double>(nn);
+    const bool exact = (nn & (nn - 1)) == 0 && static_cast<double>(terms) * span * span < 9007199254740992.0;
     double acc2[1] = {0.0};
-    {
-        const int db = bd / chp, da = bd - db * chp;
-        int b = tid / chp, a = tid - b * chp;
-        for (int e = tid; e < chp * cw; e += bd) {
+    if (exact) {
+        const long long S = static_cast<long long>(st[0]), N2 = static_cast<long long>(nn);
+        const long long K = N2 * N2 * static_cast<long long>(Q) - 2 * N2 * S * static_cast<long long>(P) +
+                            static_cast<long long>(m) * S * S;
+        const double inv = 1.0 / (static_cast<double>(nn) * static_cast<double>(nn));  // 2^-2k
+        acc2[0] = static_cast<double>(K) * inv;
+    } else {
+        int a = a0, b = b0;
+        for (int e = tid; e < ne; e += bd) {
             if (a < ch) {
-                const double d = __dsub_rn(static_cast<double>(s_P[b * PC + kPadL + a]), m);
+                const double d = __dsub_rn(static_cast<double>(s_P[b * PC + kPadL + a]), mn);
                 acc2[0] = __dadd_rn(acc2[0], __dmul_rn(d, d));
             }
-            a += da;
-            b += db;
-            if (a >= chp) {
-                a -= chp;
-                ++b;
-            }
+            step(a, b);
         }
     }
     block_sum_f64<1>(acc2, s_red);
@@ -890,6 +978,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
     const int64_t NR = A.nrows + 2 * A.pady, NC = A.ncols + 2 * A.padx;
     const double shx = static_cast<double>(A.padx) + 0.5;
     const double shy = static_cast<double>(A.pady) + 0.5;
+    const uint8_t* ref_end = A.ref + A.nrows * A.ncols;
+    const uint8_t* sec_end = A.sec + A.nrows * A.ncols;
+    const uint8_t* valid_end = A.valid + A.nrows * A.ncols;
 
     if (warp == 0) {
         tc::tmem_alloc(&s_taddr, A.tmem_cols);
@@ -967,39 +1058,52 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         // for power-of-two areas, its exact integer sums: warps over chip columns, lanes over
         // rows, all loads of a lane issued before their uses. Rows a taller chip left behind
         // are cleared (the padding itself is never written).
-        int any = 0;
-        unsigned long long isum = 0ull, isq = 0ull;
         // Invariant: chip rows at or beyond `dirty_ch` are zero in every column.
         if (ch < dirty_ch)
             for (int b = warp; b < A.CWM; b += nwarps)
                 for (int a = ch + lane; a < dirty_ch; a += 32) s_P[b * A.PC + kPadL + a] = 0;
         dirty_ch = ch;
-        for (int a0 = 0; a0 < ch; a0 += 32) {
-            const int a = a0 + lane;
-            const int64_t r = chip_r + a;
-            const bool rin = a < ch && r >= 0 && r < A.nrows;
-            constexpr int kU = REG ? 8 : 4;  // columns per step: more loads in flight for wide chips
-            for (int b0 = warp; b0 < cw; b0 += kU * nwarps) {
-                uint32_t v[kU], m[kU];
+        // A task is 16 rows of one chip column: a 16-byte block of the image and of its mask
+        // (col16_issue: aligned loads and a byte shift, zero outside the image), rows beyond ch
+        // zeroed. Each thread starts the loads of two tasks before using them.
+        int any = 0;
+        unsigned long long isum = 0ull, isq = 0ull;
+        {
+            const int nb16 = (ch + 15) >> 4, ntask = nb16 * cw;
+            uint32_t s1 = 0u, s2 = 0u;
+            for (int t0 = tid; t0 < ntask; t0 += 2 * bd) {
+                Col16 Lv[2], Lm[2];
+                int tb[2], tj[2];
 #pragma unroll
-                for (int u = 0; u < kU; ++u) {
-                    const int b = b0 + u * nwarps;
-                    const int64_t c = chip_c + b;
-                    const bool in = rin && b < cw && c >= 0 && c < A.ncols;
-                    v[u] = in ? A.sec[r + c * A.nrows] : 0u;
-                    m[u] = in ? A.valid[r + c * A.nrows] : 0u;
+                for (int u = 0; u < 2; ++u) {
+                    const int t = t0 + u * bd;
+                    tb[u] = t / nb16;
+                    tj[u] = t - tb[u] * nb16;
+                    const int64_t c = t < ntask ? chip_c + tb[u] : -1;
+                    Lv[u] = col16_issue(A.sec, sec_end, A.nrows, A.ncols, c, chip_r + 16 * tj[u]);
+                    Lm[u] = col16_issue(A.valid, valid_end, A.nrows, A.ncols, c, chip_r + 16 * tj[u]);
                 }
 #pragma unroll
-                for (int u = 0; u < kU; ++u) {
-                    const int b = b0 + u * nwarps;
-                    if (a < ch && b < cw) {
-                        s_P[b * A.PC + kPadL + a] = static_cast<uint8_t>(v[u]);
-                        any |= m[u];
-                        isum += v[u];
-                        isq += v[u] * v[u];
+                for (int u = 0; u < 2; ++u) {
+                    if (t0 + u * bd >= ntask) continue;
+                    const uint4 v = col16_finish(Lv[u]), mk = col16_finish(Lm[u]);
+                    const int keep = ch - 16 * tj[u];
+                    uint32_t w[4] = {v.x, v.y, v.z, v.w}, mw[4] = {mk.x, mk.y, mk.z, mk.w};
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const int kb = keep - 4 * i;
+                        const uint32_t m = kb >= 4 ? 0xffffffffu : kb <= 0 ? 0u : (1u << (8 * kb)) - 1u;
+                        w[i] &= m;
+                        any |= (mw[i] & m) != 0u;
+                        s1 = __dp4a(w[i], 0x01010101u, s1);
+                        s2 = __dp4a(w[i], w[i], s2);
                     }
+                    *reinterpret_cast<uint4*>(s_P + tb[u] * A.PC + kPadL + 16 * tj[u]) =
+                        make_uint4(w[0], w[1], w[2], w[3]);
                 }
             }
+            isum = s1;
+            isq = s2;
         }
         if (pow2) {
 #pragma unroll
@@ -1069,26 +1173,12 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         const int Q = static_cast<int>((delta + ch + nr - 1 + 15) / 16);
         const int XW = cw + nc - 1;
         const int qT = static_cast<int>((delta + iA) >> 4);
+        // A block is one aligned 16-byte load when the image's columns are 16-byte aligned (row
+        // counts divisible by 16), otherwise two aligned loads and a byte shift.
         for (int q = warp; q < Q; q += nwarps) {
             for (int x = lane; x < A.XS; x += 32) {
-                const int64_t r0 = base_r + 16 * q, c = win_c + x;
-                uint4 v = make_uint4(0, 0, 0, 0);
-                if (c >= 0 && c < A.ncols) {
-                    const uint8_t* col = A.ref + c * A.nrows;
-                    if (r0 >= 0 && r0 + 16 <= A.nrows &&
-                        (reinterpret_cast<uintptr_t>(col + r0) & 15) == 0) {
-                        v = __ldg(reinterpret_cast<const uint4*>(col + r0));
-                    } else {
-                        uint32_t w[4] = {0, 0, 0, 0};
-#pragma unroll
-                        for (int t = 0; t < 16; ++t) {
-                            const int64_t r = r0 + t;
-                            const uint32_t bb = (r >= 0 && r < A.nrows) ? col[r] : 0u;
-                            w[t >> 2] |= bb << (8 * (t & 3));
-                        }
-                        v = make_uint4(w[0], w[1], w[2], w[3]);
-                    }
-                }
+                const Col16 L = col16_issue(A.ref, ref_end, A.nrows, A.ncols, win_c + x, base_r + 16 * q);
+                const uint4 v = col16_finish(L);
                 *reinterpret_cast<uint4*>(s_W + q * A.QS + x * 16) = v;
                 if (x < XW && q >= qT) {
                     const uint32_t w[4] = {v.x, v.y, v.z, v.w};
@@ -1662,62 +1752,6 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
 // blocks: column sums V down ch rows per 16-row block of surface rows (dp4a for the first, a
 // sliding update for the rest), then row sums of V with 16-byte loads. Estimates stay in
 // registers; candidates and the patch get the reference's FP64 normalisation.
-
-// Sixteen bytes of column `c` from row r0 (zero outside the image), in two steps so that a
-// thread can have several in flight: col16_issue starts the loads -- two aligned 16-byte loads
-// when they stay inside the image, else byte by byte -- and col16_finish shifts the bytes into
-// place.
-struct Col16 {
-    uint4 lo, hi;
-    uint32_t s;  // byte offset of row r0 in `lo` (0: `lo` is the result)
-};
-
-__device__ __forceinline__ Col16 col16_issue(const uint8_t* img, const uint8_t* img_end,
-                                             int64_t nrows, int64_t ncols, int64_t c, int64_t r0) {
-    Col16 L;
-    L.s = 0;
-    L.lo = L.hi = make_uint4(0, 0, 0, 0);
-    if (c < 0 || c >= ncols) return L;
-    const uint8_t* p = img + c * nrows + r0;
-    if (r0 >= 0 && r0 + 16 <= nrows) {
-        const uintptr_t pa = reinterpret_cast<uintptr_t>(p);
-        const uint32_t s = static_cast<uint32_t>(pa & 15);
-        const uint4* a = reinterpret_cast<const uint4*>(pa - s);
-        if (s == 0) {
-            L.lo = __ldg(a);
-            return L;
-        }
-        if (reinterpret_cast<const uint8_t*>(a) + 32 <= img_end) {
-            L.lo = __ldg(a);
-            L.hi = __ldg(a + 1);
-            L.s = s;
-            return L;
-        }
-    }
-    uint32_t w[4] = {0, 0, 0, 0};
-#pragma unroll
-    for (int t = 0; t < 16; ++t) {
-        const int64_t r = r0 + t;
-        const uint32_t bb = (r >= 0 && r < nrows) ? p[t] : 0u;
-        w[t >> 2] |= bb << (8 * (t & 3));
-    }
-    L.lo = make_uint4(w[0], w[1], w[2], w[3]);
-    return L;
-}
-
-__device__ __forceinline__ uint4 col16_finish(const Col16& L) {
-    const uint32_t s = L.s;
-    if (s == 0) return L.lo;
-    const uint32_t w[8] = {L.lo.x, L.lo.y, L.lo.z, L.lo.w, L.hi.x, L.hi.y, L.hi.z, L.hi.w};
-    uint32_t u[6], v[5];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) u[k] = (s & 8) ? w[k + 2] : w[k];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) v[k] = (s & 4) ? u[k + 1] : u[k];
-    const uint32_t sh = (s & 3) * 8u;
-    return make_uint4(__funnelshift_r(v[0], v[1], sh), __funnelshift_r(v[1], v[2], sh),
-                      __funnelshift_r(v[2], v[3], sh), __funnelshift_r(v[3], v[4], sh));
-}
 
 // A point's chip and window placement (src/points.jl:358-395 with the pass's padding and the
 // +0.5 shift, src/track.jl:128-138, 207-220) and whether it is searched at all.

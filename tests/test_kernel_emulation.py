@@ -12,6 +12,8 @@ the kernel computes it and checks it against the direct definition:
   below 2^16 in magnitude;
 * the flattened order of `k_corr_tc`'s wide-surface epilogue (every value visited once) and the
   ring rows of the carried box sums;
+* the integer per-thread partial sums of `staged_chip_stats` against the FP64 running sums they
+  replace (bit for bit, within the kernel's bound);
 * the FP32 mean of `k_highpass_w`: the correctly rounded FP32 quotient of an integer sum by a
   count equals the FP64 quotient rounded to FP32 (double rounding innocuous), for every count
   the kernel can see.
@@ -240,3 +242,51 @@ def test_ring_rows_carry_box_sums():
         for i in range(nr):
             for j in range(nc):
                 assert S[j, ring(i)] == box(r0, i, j)
+
+
+def chip_sq_partials(C, bd=256, kUA=16):
+    """Per-thread partial sums of squared deviations as the CUDA-core kernel forms them: the FP64
+    mean S/nn, then thread t adds fl(fl(v - mean)^2) over elements t, t + bd, ... of the
+    column-major chip with rows padded to a multiple of kUA (padding skipped)."""
+    ch, cw = C.shape
+    nn = ch * cw
+    S = float(C.sum())
+    mean = S / nn
+    chp = (ch + kUA - 1) // kUA * kUA
+    part = np.zeros(bd)
+    for e in range(chp * cw):
+        a, b = e % chp, e // chp
+        if a < ch:
+            d = float(C[a, b]) - mean
+            part[e % bd] = part[e % bd] + d * d
+    return part, int(S)
+
+
+@pytest.mark.parametrize("ch,cw,scale", [(128, 128, 255), (128, 128, 40), (64, 128, 255),
+                                         (128, 64, 90), (128, 256, 255)])
+def test_integer_chip_partials_equal_fp64_partials(ch, cw, scale):
+    """`staged_chip_stats`: for power-of-two areas within its bound, the per-thread partial
+    K / nn^2 with K = sum (nn C - S)^2 = nn^2 Q - 2 nn S P + m S^2 in integers is the FP64 running
+    sum, bit for bit."""
+    rng = np.random.default_rng(ch + cw + scale)
+    C = np.clip(rng.normal(128, scale, (ch, cw)), 0, 255).astype(np.int64)
+    nn, bd, chp = ch * cw, 256, (ch + 15) // 16 * 16
+    terms = (chp * cw + bd - 1) // bd
+    exact = terms * (255.0 * nn) ** 2 < 2.0 ** 53
+    part, S = chip_sq_partials(C)
+    P, Q, m = [0] * bd, [0] * bd, [0] * bd
+    for e in range(chp * cw):
+        a, b = e % chp, e // chp
+        if a < ch:
+            v = int(C[a, b])
+            P[e % bd] += v
+            Q[e % bd] += v * v
+            m[e % bd] += 1
+    # K = sum (nn C - S)^2 over the thread's elements, from its count, sum and sum of squares.
+    K = [nn * nn * Q[t] - 2 * nn * S * P[t] + m[t] * S * S for t in range(bd)]
+    assert max(K) < 2 ** 63
+    ip = np.array([float(k) / float(nn * nn) for k in K])
+    if exact:
+        assert np.array_equal(ip.view(np.int64), part.view(np.int64))
+    else:
+        assert (ch, cw) == (128, 256)  # outside the bound: the kernel keeps the FP64 loop
