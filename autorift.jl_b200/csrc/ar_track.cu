@@ -1175,16 +1175,33 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_corr_tc(const TcArgs A) {
         const int qT = static_cast<int>((delta + iA) >> 4);
         // A block is one aligned 16-byte load when the image's columns are 16-byte aligned (row
         // counts divisible by 16), otherwise two aligned loads and a byte shift.
-        for (int q = warp; q < Q; q += nwarps) {
-            for (int x = lane; x < A.XS; x += 32) {
-                const Col16 L = col16_issue(A.ref, ref_end, A.nrows, A.ncols, win_c + x, base_r + 16 * q);
-                const uint4 v = col16_finish(L);
-                *reinterpret_cast<uint4*>(s_W + q * A.QS + x * 16) = v;
-                if (x < XW && q >= qT) {
-                    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+        // A task is block q of column x (consecutive threads on consecutive columns); each thread
+        // starts the loads of three tasks before using them.
+        {
+            const int ntask = Q * A.XS;
+            for (int t0 = tid; t0 < ntask; t0 += 3 * bd) {
+                Col16 L[3];
+                int tq[3], tx[3];
 #pragma unroll
-                    for (int t = 0; t < 16; ++t)
-                        s_T[(16 * q + t) * A.XT + x] = static_cast<uint8_t>(w[t >> 2] >> (8 * (t & 3)));
+                for (int u = 0; u < 3; ++u) {
+                    const int t = t0 + u * bd;
+                    tq[u] = t / A.XS;
+                    tx[u] = t - tq[u] * A.XS;
+                    const int64_t c = t < ntask ? win_c + tx[u] : -1;
+                    L[u] = col16_issue(A.ref, ref_end, A.nrows, A.ncols, c, base_r + 16 * tq[u]);
+                }
+#pragma unroll
+                for (int u = 0; u < 3; ++u) {
+                    if (t0 + u * bd >= ntask) continue;
+                    const int q = tq[u], x = tx[u];
+                    const uint4 v = col16_finish(L[u]);
+                    *reinterpret_cast<uint4*>(s_W + q * A.QS + x * 16) = v;
+                    if (x < XW && q >= qT) {
+                        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                        for (int t = 0; t < 16; ++t)
+                            s_T[(16 * q + t) * A.XT + x] = static_cast<uint8_t>(w[t >> 2] >> (8 * (t & 3)));
+                    }
                 }
             }
         }
