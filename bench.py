@@ -1146,7 +1146,8 @@ def profile_pass_arm(args, precision):
     spacing --spacing, `--warmup` untimed passes then `--steps` timed ones; prints one line of
     timings. precision: the split-BF16 kernel's chip-64 / radius-32 pass on the highpass-filtered
     Float32 pair (quantize = :none); otherwise the fine chip-32 / radius-25 pass of the default
-    pipeline on the prepared UInt8 pair with the autotuner off (k_corr_tc2)."""
+    pipeline on the prepared UInt8 pair with the autotuner off (k_corr_tc2). --chip / --radius
+    replace the pass's chip size and radius (a radius above 32 runs k_corr_tc)."""
     import torch
     import __graft_entry__ as ge
 
@@ -1156,6 +1157,8 @@ def profile_pass_arm(args, precision):
     ctx = L.Context(0)
     a, b, v = scene(ar, args.size)
     chip, radius = (64, 32) if precision else (32, 25)
+    chip = args.chip or chip
+    radius = args.radius or radius
     if precision:
         p = ar.params(chip_size=chip, search_radius=radius, quantize="none", upsampling=UP)
     else:
@@ -1275,6 +1278,11 @@ def main():
                          "(k_corr_tc2; for ncu captures)")
     ap.add_argument("--spacing", type=int, default=SPACING,
                     help="grid spacing of a --profile run (the benchmark line always uses 8)")
+    ap.add_argument("--chip", type=int, default=None,
+                    help="chip size of a --profile-pass run (default 32; 64 with --profile-precision)")
+    ap.add_argument("--radius", type=int, default=None,
+                    help="search radius of a --profile-pass run (default 25; 32 with "
+                         "--profile-precision); surfaces wider than 64 run k_corr_tc")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
