@@ -67,7 +67,7 @@ class ArRequest(ctypes.Structure):
 
 AR_PRE_NONE, AR_PRE_HIGHPASS, AR_PRE_WALLIS = 0, 1, 2
 AR_OPT_TENSOR_CORES, AR_OPT_SERVE_SLOTS, AR_OPT_SERVE_MEMORY_MB, AR_OPT_SPLIT_BF16 = 1, 2, 3, 4
-AR_OPT_AUTOTUNE, AR_OPT_SHAPE_BINS = 5, 6
+AR_OPT_AUTOTUNE, AR_OPT_SHAPE_BINS, AR_OPT_UINT8_KERNEL = 5, 6, 7
 AR_QUANT_NONE, AR_QUANT_UINT8 = 0, 1
 
 
@@ -110,6 +110,7 @@ SIGNATURES = {
     "ar_kernel_times": (_i32, [_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                ctypes.POINTER(_i64), ctypes.POINTER(_i64),
                                ctypes.POINTER(ctypes.c_double)]),
+    "ar_ctx_tuned": (_i32, [_p, _p, _i64, ctypes.POINTER(_i64)]),
     "ar_synchronize": (_i32, [_p]),
 }
 
@@ -185,6 +186,19 @@ class Context:
         self.check(self.lib.ar_kernel_times(self.handle, ctypes.byref(a), ctypes.byref(b),
                                             ctypes.byref(t), ctypes.byref(n), ctypes.byref(f)))
         return a.value, b.value, t.value, n.value, f.value
+
+    def tuned(self):
+        """The autotuner's choices so far: one dict per pass geometry (largest chip rows and
+        columns, surface rows and columns) with the kernel kept ("k_corr_tc2", "k_corr_tc" or
+        "k_corr")."""
+        cnt = _i64()
+        self.check(self.lib.ar_ctx_tuned(self.handle, None, 0, ctypes.byref(cnt)))
+        buf = (ctypes.c_int32 * (5 * max(cnt.value, 1)))()
+        self.check(self.lib.ar_ctx_tuned(self.handle, buf, cnt.value, ctypes.byref(cnt)))
+        names = {2: "k_corr_tc2", 1: "k_corr_tc", 0: "k_corr"}
+        return [{"chip": [buf[5 * i], buf[5 * i + 1]], "surface": [buf[5 * i + 2], buf[5 * i + 3]],
+                 "kernel": names.get(buf[5 * i + 4], str(buf[5 * i + 4]))}
+                for i in range(cnt.value)]
 
     def close(self):
         if getattr(self, "handle", None):

@@ -1120,6 +1120,10 @@ int ar_ctx_set_option(ar_ctx* c, int option, int value) {
         case AR_OPT_TENSOR_CORES: c->scratch.tensor_cores = value != 0; return AR_OK;
         case AR_OPT_AUTOTUNE: c->scratch.autotune = value != 0; return AR_OK;
         case AR_OPT_SHAPE_BINS: c->scratch.shape_bins = value != 0; return AR_OK;
+        case AR_OPT_UINT8_KERNEL:
+            if (value < -1 || value > 2) return fail(c, AR_ERR_ARG, "the UInt8 kernel must be -1, 0, 1 or 2");
+            c->scratch.uint8_kernel = value;
+            return AR_OK;
         case AR_OPT_SPLIT_BF16:
             if (value < 0 || value > 2) return fail(c, AR_ERR_ARG, "split-BF16 mode must be 0, 1 or 2");
             c->scratch.split_bf16 = value;
@@ -1253,6 +1257,25 @@ int ar_kernel_times(ar_ctx* c, double* corr_ms, double* refine_ms, int64_t* trac
     if (corr_ms) *corr_ms = sc;
     if (refine_ms) *refine_ms = sr;
     return e == cudaSuccess ? AR_OK : cuda_fail(c, e, "ar_kernel_times");
+}
+
+int ar_ctx_tuned(ar_ctx* c, int32_t* out, int64_t cap, int64_t* count) {
+    if (!c || !count || cap < 0 || (cap > 0 && !out)) return AR_ERR_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    int64_t n = 0;
+    for (const auto& kv : c->scratch.tuned) {
+        if (n < cap) {
+            int32_t* o = out + 5 * n;
+            o[0] = static_cast<int32_t>((kv.first >> 48) & 0xFFFF);
+            o[1] = static_cast<int32_t>((kv.first >> 32) & 0xFFFF);
+            o[2] = static_cast<int32_t>((kv.first >> 16) & 0xFFFF);
+            o[3] = static_cast<int32_t>(kv.first & 0xFFFF);
+            o[4] = kv.second;
+        }
+        ++n;
+    }
+    *count = n;
+    return AR_OK;
 }
 
 int ar_synchronize(ar_ctx* c) {

@@ -97,6 +97,9 @@ struct TrackScratch {
     // (identical results) are timed once per pass geometry and the fastest kept in `tuned`
     // (key: chip and surface extents) -- AR_OPT_AUTOTUNE.
     bool autotune = true;
+    // AR_OPT_UINT8_KERNEL: -1 the autotuner (or the fixed rule); 2, 1, 0 run k_corr_tc2,
+    // k_corr_tc or the CUDA-core kernel on every UInt8 pass whose plan fits it.
+    int uint8_kernel = -1;
     // Multichip passes whose searchable points have both small (up to 64 x 64) and larger
     // surfaces run each group as its own launch (AR_OPT_SHAPE_BINS).
     bool shape_bins = true;

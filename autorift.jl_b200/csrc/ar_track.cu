@@ -4253,16 +4253,22 @@ constexpr int64_t kTuneMinPoints = 8192;
 constexpr int64_t kTuneSample = 32768;
 constexpr int64_t kTuneSampleDirect = 4096;
 
-// Times each candidate kernel (2 k_corr_tc2, 1 k_corr_tc, 0 k_corr) on a sample of the pass's
-// first points without refinement (the pass itself overwrites their outputs), each launched
-// twice and the second timed, and returns in `kind` the one with the least time per point (a
-// tie keeps the earlier candidate). The tensor-core kernels' sample is large enough that each
-// CTA takes a run of consecutive points, as in the full pass: k_corr_tc2 carries box sums from
-// one point of a run to the next, and on a sample of 4096 points (one or two points per CTA)
-// it lost that and the tuner could pick k_corr_tc, 25 % slower on the full pass.
+// Times each candidate kernel (2 k_corr_tc2, 1 k_corr_tc, 0 k_corr) on a sample of the pass --
+// consecutive points from its middle, written to their own output slots, without refinement
+// (the pass itself then writes the same values there) -- each launched twice and the second
+// timed, and returns in `kind` the one with the least time per point (a tie keeps the earlier
+// candidate). The tensor-core kernels' sample is large enough that each CTA takes a run of
+// consecutive points, as in the full pass: both carry box sums from one point of a run to the
+// next, and on a sample of 4096 points (one or two points per CTA) k_corr_tc2 lost that and the
+// tuner could pick k_corr_tc, 25 % slower on the full pass. The sample comes from the middle
+// because a pass's first points (its first grid columns) lie at the image's edge, where more
+// points are skipped or clipped than elsewhere: on the 10980^2 benchmark pair the first 32 768
+// points made k_corr_tc look faster, and it was 35 % slower on the whole pass. With diagnostic
+// surfaces (`at_start`) the sample is the pass's first points, whose rows they are.
 template <typename Launch>
 cudaError_t autotune_u8(TrackScratch& scratch, cudaStream_t stream, const DevPoints& pts,
-                        bool fit2, bool fit1, int* kind, Launch launch) {
+                        const DevOutputs& out, bool at_start, bool fit2, bool fit1, int* kind,
+                        Launch launch) {
     cudaError_t e = cudaSuccess;
     for (int i = 0; i < 2 && e == cudaSuccess; ++i)
         if (!scratch.tune_ev[i]) {
@@ -4275,11 +4281,26 @@ cudaError_t autotune_u8(TrackScratch& scratch, cudaStream_t stream, const DevPoi
     const int cand[3] = {2, 1, 0};
     for (int c : cand) {
         if ((c == 2 && !fit2) || (c == 1 && !fit1)) continue;
+        const int64_t m = std::min<int64_t>(pts.n, c == 0 ? kTuneSampleDirect : kTuneSample);
+        const int64_t off = at_start ? 0 : (pts.n - m) / 2;
         DevPoints ds = pts;
-        ds.n = std::min<int64_t>(pts.n, c == 0 ? kTuneSampleDirect : kTuneSample);
-        e = launch(c, ds);
+        ds.x += off;
+        ds.y += off;
+        ds.rx += off;
+        ds.ry += off;
+        ds.dx0 += off;
+        ds.dy0 += off;
+        ds.csx += off;
+        ds.csy += off;
+        ds.n = m;
+        DevOutputs dout = out;
+        dout.dx += off;
+        dout.dy += off;
+        dout.corr += off;
+        dout.searched += off;
+        e = launch(c, ds, dout);
         if (e == cudaSuccess) e = cudaEventRecord(scratch.tune_ev[0], stream);
-        if (e == cudaSuccess) e = launch(c, ds);
+        if (e == cudaSuccess) e = launch(c, ds, dout);
         if (e == cudaSuccess) e = cudaEventRecord(scratch.tune_ev[1], stream);
         if (e == cudaSuccess) e = cudaEventSynchronize(scratch.tune_ev[1]);
         float ms = 0.0f;
@@ -4549,7 +4570,10 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
         const bool fit2 = tc_ok && plan_corr_tc2(geom, 220 * 1024, &TP2);
         const bool fit1 = tc_ok && plan_corr_tc(geom, 220 * 1024, &TP1);
         int kind = fit2 ? 2 : fit1 ? 1 : 0;
-        if ((fit2 || fit1) && scratch.autotune && !scratch.fixed && pts.n >= kTuneMinPoints) {
+        const int force = scratch.uint8_kernel;
+        if (force == 0 || (force == 1 && fit1) || (force == 2 && fit2)) kind = force;
+        if (force < 0 && (fit2 || fit1) && scratch.autotune && !scratch.fixed &&
+            pts.n >= kTuneMinPoints) {
             const uint64_t key = (static_cast<uint64_t>(geom.max_ch) << 48) |
                                  (static_cast<uint64_t>(geom.max_cw) << 32) |
                                  (static_cast<uint64_t>(geom.max_nr) << 16) |
@@ -4558,11 +4582,11 @@ cudaError_t launch_track_impl(int dtype, const void* ref, const void* sec, const
             if (it != scratch.tuned.end()) {
                 kind = it->second;
             } else {
-                e = autotune_u8(scratch, stream, pts, fit2, fit1, &kind,
-                                [&](int kk, const DevPoints& ds) -> cudaError_t {
-                                    if (kk == 2) return launch_tc(true, TP2, ds, 1, out, nullptr);
-                                    if (kk == 1) return launch_tc(false, TP1, ds, 1, out, nullptr);
-                                    return launch_direct(ds, 1, out, nullptr);
+                e = autotune_u8(scratch, stream, pts, out, surf_out != nullptr, fit2, fit1, &kind,
+                                [&](int kk, const DevPoints& ds, const DevOutputs& dout) -> cudaError_t {
+                                    if (kk == 2) return launch_tc(true, TP2, ds, 1, dout, nullptr);
+                                    if (kk == 1) return launch_tc(false, TP1, ds, 1, dout, nullptr);
+                                    return launch_direct(ds, 1, dout, nullptr);
                                 });
                 if (e != cudaSuccess) return e;
                 scratch.tuned[key] = kind;

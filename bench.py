@@ -169,15 +169,24 @@ def measure_fp32_peak(torch, device):
     return best
 
 
-def profile_traffic(points):
-    """DRAM bytes of one correlation launch over `points` searched points, from the committed
-    ncu capture of the same kernel (bytes per point measured on a smaller grid)."""
+def profile_traffic(points, kernel):
+    """DRAM bytes of one correlation launch of `kernel` over `points` searched points, from the
+    committed ncu capture of the same kernel on the same pass geometry (bytes per point measured
+    on a smaller grid); None when there is no capture of it."""
     f = ROOT / "profiles" / "k_corr_traffic.json"
     try:
         d = json.loads(f.read_text())
-        return float(d["bytes_per_point"]) * points
+        return float(d[kernel]["bytes_per_point"]) * points
     except (OSError, ValueError, TypeError, KeyError):
         return None
+
+
+def fine_pass_kernel(ctx):
+    """The kernel the autotuner kept for the fine chip-32 / radius-25 pass (surface 50 x 50)."""
+    for t in ctx.tuned():
+        if t["chip"] == [CHIP, CHIP] and t["surface"] == [2 * RADIUS, 2 * RADIUS]:
+            return t["kernel"]
+    return "k_corr_tc2"
 
 
 def crop(a, n):
@@ -960,6 +969,8 @@ def gpu_arm(args):
     fp32_peak = measure_fp32_peak(torch, dev)
     eval_flops = 2.0 * CHIP * CHIP * (2 * RADIUS) ** 2
     fine_points = corr_flops / max(tracks, 1) / eval_flops  # chip-32 evaluations per launch
+    tuned_kernels = ctx.tuned()
+    fine_kernel = fine_pass_kernel(ctx)
 
     # End to end through the C ABI from host buffers: the caller's column-major arrays (the
     # Julia layout) and grid, pair upload, prepare, multichip, download; per-pair latency.
@@ -1081,7 +1092,8 @@ def gpu_arm(args):
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": tensor_peak,
                          "unit": "TFLOP/s",
                          "frac": achieved / tensor_peak if achieved else None,
-                         "traffic": profile_traffic(fine_points), "kernel": "k_corr_tc2",
+                         "traffic": profile_traffic(fine_points, fine_kernel),
+                         "kernel": fine_kernel, "tuned_kernels": tuned_kernels,
                          "peak_source": peak_source,
                          "achieved_basis": "2 * chip area * surface area per searched point "
                                            "(integer MACs of the exact u8 numerator), summed "
@@ -1147,7 +1159,8 @@ def profile_pass_arm(args, precision):
     timings. precision: the split-BF16 kernel's chip-64 / radius-32 pass on the highpass-filtered
     Float32 pair (quantize = :none); otherwise the fine chip-32 / radius-25 pass of the default
     pipeline on the prepared UInt8 pair with the autotuner off (k_corr_tc2). --chip / --radius
-    replace the pass's chip size and radius (a radius above 32 runs k_corr_tc)."""
+    replace the pass's chip size and radius (a radius above 32 runs k_corr_tc); --kernel picks
+    the UInt8 kernel."""
     import torch
     import __graft_entry__ as ge
 
@@ -1164,6 +1177,8 @@ def profile_pass_arm(args, precision):
     else:
         p = ar.params(chip_size=chip, search_radius=radius, upsampling=UP)
         ctx.set_option(L.AR_OPT_AUTOTUNE, 0)
+        if args.kernel:
+            ctx.set_option(L.AR_OPT_UINT8_KERNEL, {"tc2": 2, "tc": 1, "direct": 0}[args.kernel])
     grid = ar.gridpoints(a.shape, args.spacing, chip_size=chip, search_radius=radius)
     prep = ar.prepare(ar.ImagePair(a, b, None, v), p, ctx)
     dev = torch.device("cuda", 0)
@@ -1186,6 +1201,7 @@ def profile_pass_arm(args, precision):
     t = timed_steps(torch, call, stream, flush, args.steps, 0)
     corr_ms, refine_ms, _, _, flops = ctx.kernel_times()
     print(json.dumps({"profile_pass": "split_bf16" if precision else "u8_fine", "points": n,
+                      "kernel": args.kernel,
                       "chip": chip, "radius": radius, "ms_per_pass": t / args.steps,
                       "k_corr_ms": corr_ms / args.steps, "k_refine_ms": refine_ms / args.steps,
                       "algorithmic_tflops": flops / (corr_ms * 1e-3) / 1e12 if corr_ms else None}))
@@ -1278,6 +1294,9 @@ def main():
                          "(k_corr_tc2; for ncu captures)")
     ap.add_argument("--spacing", type=int, default=SPACING,
                     help="grid spacing of a --profile run (the benchmark line always uses 8)")
+    ap.add_argument("--kernel", choices=["tc2", "tc", "direct"], default=None,
+                    help="UInt8 kernel of a --profile-pass run (AR_OPT_UINT8_KERNEL; default: "
+                         "k_corr_tc2 where it fits)")
     ap.add_argument("--chip", type=int, default=None,
                     help="chip size of a --profile-pass run (default 32; 64 with --profile-precision)")
     ap.add_argument("--radius", type=int, default=None,

@@ -318,11 +318,15 @@ int ar_release(ar_ctx* ctx, ar_ticket ticket);
  * of at most 64 x 64 and larger ones runs the two groups as separate launches, each planned for
  * its own largest surface (per-point radii); 0 runs every pass as one launch. Results are the
  * same either way.
+ * AR_OPT_UINT8_KERNEL (default -1: the autotuner, or the fixed rule above): 2, 1 or 0 runs
+ * every UInt8 pass on k_corr_tc2, k_corr_tc or the CUDA-core kernel where that kernel's plan
+ * fits the pass (else the usual choice) -- for benchmarks and profiles; results are identical.
  * AR_OPT_SERVE_SLOTS and AR_OPT_SERVE_MEMORY_MB configure the request loop (see ar_submit);
  * they must be set before the first ar_submit. No reference counterpart.
  */
 enum { AR_OPT_TENSOR_CORES = 1, AR_OPT_SERVE_SLOTS = 2, AR_OPT_SERVE_MEMORY_MB = 3,
-       AR_OPT_SPLIT_BF16 = 4, AR_OPT_AUTOTUNE = 5, AR_OPT_SHAPE_BINS = 6 };
+       AR_OPT_SPLIT_BF16 = 4, AR_OPT_AUTOTUNE = 5, AR_OPT_SHAPE_BINS = 6,
+       AR_OPT_UINT8_KERNEL = 7 };
 int ar_ctx_set_option(ar_ctx* ctx, int option, int value);
 
 /* The context's own CUDA stream (cudaStream_t), on which calls without a stream argument run;
@@ -360,6 +364,15 @@ int ar_refine_patches(ar_ctx* ctx, const float* patches, int64_t count, int upsa
 int ar_ctx_set_timing(ar_ctx* ctx, int enable);
 int ar_kernel_times(ar_ctx* ctx, double* corr_ms, double* refine_ms, int64_t* tracks,
                     int64_t* launches, double* corr_flops);
+
+/*
+ * The UInt8 correlation kernel the autotuner kept for each pass geometry it has timed in this
+ * context (AR_OPT_AUTOTUNE): five int32 per geometry -- largest chip rows, chip columns,
+ * surface rows, surface columns, then the kernel (2: k_corr_tc2, 1: k_corr_tc, 0: k_corr, the
+ * CUDA-core direct sum). Writes up to `cap` geometries to `out`; *count = the number tuned.
+ * Diagnostics for benchmarks; no reference counterpart.
+ */
+int ar_ctx_tuned(ar_ctx* ctx, int32_t* out, int64_t cap, int64_t* count);
 
 /* Block until all work the context enqueued has finished. */
 int ar_synchronize(ar_ctx* ctx);
