@@ -916,6 +916,12 @@ def gpu_arm(args):
     ar = ge.load_package()
     L = ar._lib
     ctx = L.Context(local)
+    if args.profile:
+        # Under a profiler every launch is serialised and cold, which distorts the autotuner's
+        # timing of its samples (under ncu it kept k_corr_tc for the fine pass, which the
+        # timed run does not): profile runs take the fixed rule, which picks the kernels the
+        # tuned run keeps on this workload (k_corr_tc2 up to chip 64, k_corr_tc at chip 128).
+        ctx.set_option(L.AR_OPT_AUTOTUNE, 0)
     a, b, valid, fdown = scene(ar, args.size, field=True)
     p = pipeline_params(ar, args.spacing if args.profile else SPACING)
     dev = torch.device("cuda", local)
@@ -1288,7 +1294,8 @@ def main():
     ap.add_argument("--size", type=int, default=N,
                     help="image side; the benchmark line uses 10980, profiles a smaller scene")
     ap.add_argument("--profile", action="store_true",
-                    help="time the device steps only (for ncu captures); no JSON bench line")
+                    help="time the device steps only, autotuner off (for ncu captures); no JSON "
+                         "bench line")
     ap.add_argument("--profile-precision", action="store_true",
                     help="time the chip-64 split-BF16 track pass only (for ncu captures)")
     ap.add_argument("--profile-pass", action="store_true",
