@@ -219,3 +219,35 @@ def test_autotuner_keeps_results_identical(ar, gpu_lib, precision_scene):
     for r in res[1:]:
         for x, y in ((r.dx, res[0].dx), (r.dy, res[0].dy), (r.correlation, res[0].correlation)):
             assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
+
+
+def test_forced_uint8_kernels_and_tuner_table(ar, gpu_lib, precision_scene):
+    """AR_OPT_UINT8_KERNEL runs the chosen exact UInt8 kernel (k_corr_tc2, k_corr_tc or the
+    CUDA-core k_corr) with results identical to the tuned run's, and ar_ctx_tuned lists the
+    autotuner's choice for the pass geometry it timed (none when a kernel is forced)."""
+    a, b, sv, fx, fy = precision_scene
+    L = ar._lib
+    p = ar.params(chip_size=32, search_radius=25)
+    pts = ar.gridpoints(a.shape, 4, chip_size=32, search_radius=25)
+    assert len(pts) >= 8192
+    res = []
+    for kern in (-1, 2, 1, 0):
+        ctx = L.Context(0)
+        ctx.set_option(L.AR_OPT_UINT8_KERNEL, kern)
+        prep = ar.prepare(ar.ImagePair(a, b, None, sv), p, ctx)
+        res.append(ar.track(prep, pts, p, ctx=ctx))
+        tuned = ctx.tuned()
+        if kern == -1:
+            assert len(tuned) == 1
+            assert tuned[0]["chip"] == [32, 32] and tuned[0]["surface"] == [50, 50]
+            assert tuned[0]["kernel"] in ("k_corr_tc2", "k_corr_tc", "k_corr")
+        else:
+            assert tuned == []
+        with pytest.raises(L.ArError):
+            ctx.set_option(L.AR_OPT_UINT8_KERNEL, 3)
+        ctx.close()
+    assert np.count_nonzero(~np.isnan(res[0].dx)) > 0
+    for r in res[1:]:
+        for x, y in ((r.dx, res[0].dx), (r.dy, res[0].dy), (r.correlation, res[0].correlation)):
+            assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
+        assert np.array_equal(r.searched, res[0].searched)
