@@ -4262,8 +4262,9 @@ constexpr int64_t kTuneSampleDirect = 4096;
 // next, and on a sample of 4096 points (one or two points per CTA) k_corr_tc2 lost that and the
 // tuner could pick k_corr_tc, 25 % slower on the full pass. The sample comes from the middle
 // because a pass's first points (its first grid columns) lie at the image's edge, where more
-// points are skipped or clipped than elsewhere: on the 10980^2 benchmark pair the first 32 768
-// points made k_corr_tc look faster, and it was 35 % slower on the whole pass. With diagnostic
+// points are skipped or clipped than elsewhere: on a 4096 x 4096 scene the first 32 768 points of
+// the chip-32 / radius-25 pass made k_corr_tc look faster, and on the whole pass it is 29 %
+// slower (12.9 against 10.0 ms). With diagnostic
 // surfaces (`at_start`) the sample is the pass's first points, whose rows they are.
 template <typename Launch>
 cudaError_t autotune_u8(TrackScratch& scratch, cudaStream_t stream, const DevPoints& pts,
