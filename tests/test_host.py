@@ -1,5 +1,8 @@
 """Host-side logic that needs no GPU: parameter resolution (src/params.jl), point sets
-(src/points.jl) and the pass geometry the library computes (src/track.jl:176-197)."""
+(src/points.jl), the pass geometry the library computes (src/track.jl:176-197) and the bench
+line's roofline helpers."""
+
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -93,3 +96,27 @@ def test_per_level_similarity_params(ar):
         ar.multichip_params(ar.params(similarity=("zncc", "ncc", "zncc", "ncc")))
     with pytest.raises(ValueError):
         ar.multichip_params(ar.params(similarity=("zncc", "coherence")))
+
+
+def test_bench_traffic_and_fine_pass_kernel():
+    """The bench line's roofline takes the fine pass's kernel from the autotuner's table and
+    that kernel's committed DRAM bytes per point (None for a kernel without a capture)."""
+    import sys
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+    import bench
+
+    class FakeCtx:
+        def __init__(self, table):
+            self.table = table
+
+        def tuned(self):
+            return self.table
+
+    fine = {"chip": [bench.CHIP, bench.CHIP], "surface": [2 * bench.RADIUS, 2 * bench.RADIUS]}
+    assert bench.fine_pass_kernel(FakeCtx([dict(fine, kernel="k_corr_tc")])) == "k_corr_tc"
+    other = {"chip": [128, 128], "surface": [50, 50], "kernel": "k_corr_tc"}
+    assert bench.fine_pass_kernel(FakeCtx([other])) == "k_corr_tc2"  # untuned: the fixed rule
+    for k in ("k_corr_tc2", "k_corr_tc"):
+        t = bench.profile_traffic(1000, k)
+        assert t is not None and 500e3 < t < 2e6
+    assert bench.profile_traffic(1000, "k_corr") is None
