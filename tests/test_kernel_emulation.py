@@ -14,6 +14,8 @@ the kernel computes it and checks it against the direct definition:
   ring rows of the carried box sums;
 * the integer per-thread partial sums of `staged_chip_stats` against the FP64 running sums they
   replace (bit for bit, within the kernel's bound);
+* `k_corr_tc`'s staging task maps (chip blocks and window blocks, each written once) and that the
+  carried box sums read only the window blocks the kernel transposed for them;
 * the FP32 mean of `k_highpass_w`: the correctly rounded FP32 quotient of an integer sum by a
   count equals the FP64 quotient rounded to FP32 (double rounding innocuous), for every count
   the kernel can see.
@@ -290,3 +292,72 @@ def test_integer_chip_partials_equal_fp64_partials(ch, cw, scale):
         assert np.array_equal(ip.view(np.int64), part.view(np.int64))
     else:
         assert (ch, cw) == (128, 256)  # outside the bound: the kernel keeps the FP64 loop
+
+
+@pytest.mark.parametrize("ch,nr,delta,sh", [(32, 66, 0, 8), (32, 94, 15, 8), (64, 80, 7, 16),
+                                            (16, 88, 3, 1), (128, 50, 9, 8), (32, 66, 4, 65)])
+def test_carried_box_sums_read_only_transposed_blocks(ch, nr, delta, sh):
+    """`k_corr_tc` with carried box sums transposes only the window blocks q >= qT, qT = (delta +
+    iA) / 16 with iA = nr - sh the first recomputed surface row; the column-sum tasks of rows
+    iA .. nr - 1 (first sums over ch rows, then a sliding update that reads one row ahead) read
+    window rows delta + iA ... delta + nr - 1 + ch, all inside those blocks."""
+    iA = nr - sh
+    qT = (delta + iA) >> 4
+    kBT, XW = 192, 97
+    nrw = nr - iA
+    nseg = max(1, min((nrw + 7) // 8, kBT // XW))
+    seglen = (nrw + nseg - 1) // nseg
+    rows = set()
+    for seg in range(nseg):
+        i0 = iA + seg * seglen
+        i1 = min(i0 + seglen, nr)
+        if i0 >= i1:
+            continue
+        rows.update(delta + i0 + a for a in range(ch))   # first sum
+        rows.update((delta + i0, delta + i0 + ch))        # outgoing / incoming before the slide
+        for i in range(i0, i1 - 1):
+            rows.update((delta + i + 1, delta + i + 1 + ch))
+    assert min(rows) >= 16 * qT
+    # The sums that are carried (rows 0 .. iA - 1) are not recomputed at all.
+    assert min(rows) >= delta + iA
+
+
+@pytest.mark.parametrize("ch,cw", [(32, 32), (17, 9), (128, 128), (64, 31), (226, 4)])
+def test_chip_block_tasks_cover_the_chip_once(ch, cw):
+    """`k_corr_tc`'s chip staging: task t is 16 rows (block j = t mod nb16) of chip column
+    b = t div nb16; two tasks per thread and step. Every row < round16(ch) of every column is
+    written once, rows >= ch as zeros (the keep mask)."""
+    nb16 = (ch + 15) >> 4
+    ntask, bd = nb16 * cw, 256
+    written = np.zeros((nb16 * 16, cw), np.int64)
+    for tid in range(bd):
+        for t0 in range(tid, ntask, 2 * bd):
+            for u in range(2):
+                t = t0 + u * bd
+                if t >= ntask:
+                    continue
+                b, j = t // nb16, t % nb16
+                keep = ch - 16 * j
+                for i in range(4):
+                    kb = keep - 4 * i
+                    nbytes = 4 if kb >= 4 else max(kb, 0)
+                    for byte in range(4):
+                        r = 16 * j + 4 * i + byte
+                        written[r, b] += 1
+                        assert (byte < nbytes) == (r < ch)
+    assert np.all(written == 1)
+
+
+@pytest.mark.parametrize("Q,XS", [(7, 160), (12, 192), (1, 96), (10, 130)])
+def test_window_block_tasks_cover_each_block_once(Q, XS):
+    """`k_corr_tc`'s window staging: task t = (block q = t div XS, column x = t mod XS), three
+    tasks per thread and step."""
+    bd, ntask = 256, Q * XS
+    seen = np.zeros((Q, XS), np.int64)
+    for tid in range(bd):
+        for t0 in range(tid, ntask, 3 * bd):
+            for u in range(3):
+                t = t0 + u * bd
+                if t < ntask:
+                    seen[t // XS, t % XS] += 1
+    assert np.all(seen == 1)
